@@ -1,0 +1,429 @@
+"""TEST INFRASTRUCTURE — Python bindings for the two oracle libraries.
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg import this,
+always as the checker, never as the thing measured or shipped.
+
+  RefLib   oracle/_ref/libbonsai_ref.so: the reference's own CPU grower
+           (src/bin_mapper.cpp, src/dataset.cpp, src/split.cpp,
+           src/grower.cpp, include/bonsai/booster.hpp, src/shap.cpp ...)
+           compiled from its sources by oracle/Makefile.
+  Oracle   oracle/_ref/liboracle.so: the C restatement bonsai_oracle.c.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libbonsai_ref.so")
+ORACLE_SO = os.path.join(HERE, "_ref", "liboracle.so")
+LEAF = 0xFFFFFFFF
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class RefCfg(C.Structure):
+    _fields_ = [
+        ("grower", C.c_int32), ("objective", C.c_int32), ("n_iters", C.c_uint32),
+        ("learning_rate", C.c_float), ("min_child_hess", C.c_float),
+        ("min_gain_to_split", C.c_float), ("lambda_l2", C.c_float),
+        ("lambda_l1", C.c_float), ("feature_fraction", C.c_float),
+        ("max_depth", C.c_uint32), ("min_data_in_leaf", C.c_uint32),
+        ("max_leaves", C.c_uint32), ("feature_seed", C.c_uint32),
+        ("subsample", C.c_float), ("random_seed", C.c_uint32),
+        ("n_threads", C.c_uint32), ("n_classes", C.c_uint32),
+        ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
+    ]
+
+
+GROWERS = {"depthwise": 0, "levelwise": 1, "leafwise": 2}
+OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2}
+
+
+@dataclass
+class TreeCfg:
+    """The reference's TreeConfig + BoosterConfig knobs the hot path reads
+    (include/bonsai/config/tree_config.hpp:9-29, booster_config.hpp)."""
+    grower: str = "depthwise"
+    objective: str = "mse"
+    n_iters: int = 100
+    learning_rate: float = 0.1
+    min_child_hess: float = 1.0
+    min_gain_to_split: float = 0.0
+    lambda_l2: float = 1.0
+    lambda_l1: float = 0.0
+    feature_fraction: float = 1.0
+    max_depth: int = 6
+    min_data_in_leaf: int = 20
+    max_leaves: int = 31
+    feature_seed: int = 2
+    subsample: float = 1.0
+    random_seed: int = 42
+    n_threads: int = 1
+    n_classes: int = 3
+    monotone: list = field(default_factory=list)
+
+    def ref(self):
+        c = RefCfg()
+        c.grower = GROWERS[self.grower]
+        c.objective = OBJECTIVES[self.objective]
+        for k in ("n_iters", "learning_rate", "min_child_hess", "min_gain_to_split",
+                  "lambda_l2", "lambda_l1", "feature_fraction", "max_depth",
+                  "min_data_in_leaf", "max_leaves", "feature_seed", "subsample",
+                  "random_seed", "n_threads", "n_classes"):
+            setattr(c, k, getattr(self, k))
+        if self.monotone:
+            self._mono = np.asarray(self.monotone, dtype=np.int32)
+            c.monotone = _p(self._mono, C.c_int32)
+            c.n_monotone = len(self.monotone)
+        return c
+
+
+@dataclass
+class Tree:
+    feature: np.ndarray
+    value: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    default_left: np.ndarray
+    gains: np.ndarray
+    covers: np.ndarray
+    split_bin: np.ndarray | None = None
+    depth: int = 0
+    n_leaves: int = 0
+
+
+class RefLib:
+    """The reference's own CPU implementation (compiled from its sources)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run make -C oracle)")
+        L = self.L = C.CDLL(path)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_dataset_create.restype = C.c_void_p
+        L.ref_train.restype = C.c_void_p
+        L.ref_grow_tree.restype = C.c_void_p
+        L.ref_model_n_trees.restype = C.c_size_t
+        L.ref_model_tree_size.restype = C.c_size_t
+        L.ref_model_init_score.restype = C.c_float
+        L.ref_model_oblivious_depth.restype = C.c_size_t
+        for name in ("ref_dataset_destroy", "ref_model_destroy"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.ref_dataset_u8.argtypes = [C.c_void_p]
+        L.ref_dataset_bins.argtypes = [C.c_void_p, C.c_void_p]
+        L.ref_model_n_trees.argtypes = [C.c_void_p]
+        L.ref_model_init_score.argtypes = [C.c_void_p]
+        L.ref_model_tree_size.argtypes = [C.c_void_p, C.c_size_t]
+        L.ref_model_tree.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 7
+        L.ref_model_oblivious_depth.argtypes = [C.c_void_p, C.c_size_t]
+        L.ref_model_oblivious.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 4
+        L.ref_model_predict_binned.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_model_contribs_binned.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_train.argtypes = [C.c_void_p, C.POINTER(RefCfg)]
+
+    def err(self):
+        return self.L.ref_last_error().decode()
+
+    def fit_cuts(self, X, max_bin=255, n_samples=200_000, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        n, F = X.shape
+        cap = F * (max_bin + 2)
+        cuts = np.empty(cap, np.float32)
+        off = np.empty(F + 1, np.uint32)
+        rc = self.L.ref_fit_cuts(_p(X, C.c_float), C.c_size_t(n), C.c_size_t(F),
+                                 C.c_int32(max_bin), C.c_size_t(n_samples),
+                                 C.c_uint64(seed), _p(cuts, C.c_float), C.c_size_t(cap),
+                                 _p(off, C.c_uint32))
+        if rc:
+            raise RuntimeError(self.err())
+        return cuts[: off[-1]].copy(), off
+
+    def cuts_from_sample(self, S, max_bin=255):
+        S = np.ascontiguousarray(S, dtype=np.float32)
+        n, F = S.shape
+        cap = F * (max_bin + 2)
+        cuts = np.empty(cap, np.float32)
+        off = np.empty(F + 1, np.uint32)
+        rc = self.L.ref_cuts_from_sample(_p(S, C.c_float), C.c_size_t(n), C.c_size_t(F),
+                                         C.c_int32(max_bin), _p(cuts, C.c_float),
+                                         C.c_size_t(cap), _p(off, C.c_uint32))
+        if rc:
+            raise RuntimeError(self.err())
+        return cuts[: off[-1]].copy(), off
+
+    def dataset(self, X, y, cuts, off):
+        return RefDataset(self, X, y, cuts, off)
+
+    def train(self, ds, cfg: TreeCfg):
+        rc = cfg.ref()
+        h = self.L.ref_train(C.c_void_p(ds.h), C.byref(rc))
+        if not h:
+            raise RuntimeError(self.err())
+        return RefModel(self, h)
+
+    def grow_tree(self, ds, cfg: TreeCfg, grad, hess, rows=None):
+        n = ds.n
+        grad = np.ascontiguousarray(grad, np.float32)
+        hess = np.ascontiguousarray(hess, np.float32)
+        rows = np.arange(n, dtype=np.uint32) if rows is None else np.ascontiguousarray(rows, np.uint32)
+        values = np.empty(n, np.float32)
+        ids = np.empty(n, np.uint32)
+        rc = cfg.ref()
+        self.L.ref_grow_tree.argtypes = [C.c_void_p, C.POINTER(RefCfg)] + [C.c_void_p] * 3 + [C.c_size_t] + [C.c_void_p] * 2
+        h = self.L.ref_grow_tree(C.c_void_p(ds.h), C.byref(rc), grad.ctypes.data,
+                                 hess.ctypes.data, rows.ctypes.data, len(rows),
+                                 values.ctypes.data, ids.ctypes.data)
+        if not h:
+            raise RuntimeError(self.err())
+        m = RefModel(self, h)
+        return m.tree(0), values, ids, m
+
+    def find_split(self, hist, n_rows, cfg: TreeCfg):
+        """hist: float32 [F, n_bins, 2]."""
+        hist = np.ascontiguousarray(hist, np.float32)
+        F, nb, _ = hist.shape
+        gain = C.c_double()
+        feat = C.c_uint32()
+        b = C.c_uint32()
+        dl = C.c_uint8()
+        valid = C.c_uint8()
+        rc = cfg.ref()
+        r = self.L.ref_find_split(_p(hist, C.c_float), C.c_size_t(F), C.c_size_t(nb),
+                                  C.c_size_t(n_rows), C.byref(rc), C.byref(gain),
+                                  C.byref(feat), C.byref(b), C.byref(dl), C.byref(valid))
+        if r:
+            raise RuntimeError(self.err())
+        return dict(gain=gain.value, feature=feat.value, bin=b.value,
+                    default_left=dl.value, valid=valid.value)
+
+
+class RefDataset:
+    def __init__(self, lib, X, y, cuts, off):
+        self.lib = lib
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        self.n, self.F = X.shape
+        self.cuts = np.ascontiguousarray(cuts, np.float32)
+        self.off = np.ascontiguousarray(off, np.uint32)
+        lib.L.ref_dataset_create.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p]
+        self.h = lib.L.ref_dataset_create(X.ctypes.data, y.ctypes.data, self.n, self.F,
+                                          self.cuts.ctypes.data, self.off.ctypes.data)
+        if not self.h:
+            raise RuntimeError(lib.err())
+
+    def bins(self):
+        out = np.empty((self.F, self.n), np.uint16)
+        if self.lib.L.ref_dataset_bins(C.c_void_p(self.h), out.ctypes.data):
+            raise RuntimeError(self.lib.err())
+        return out
+
+    def u8(self):
+        return bool(self.lib.L.ref_dataset_u8(C.c_void_p(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.ref_dataset_destroy(C.c_void_p(self.h))
+            self.h = None
+
+
+class RefModel:
+    def __init__(self, lib, h):
+        self.lib = lib
+        self.h = h
+
+    def n_trees(self):
+        return int(self.lib.L.ref_model_n_trees(C.c_void_p(self.h)))
+
+    def init_score(self):
+        return float(self.lib.L.ref_model_init_score(C.c_void_p(self.h)))
+
+    def tree(self, t):
+        n = int(self.lib.L.ref_model_tree_size(C.c_void_p(self.h), t))
+        a = dict(feature=np.empty(n, np.uint32), value=np.empty(n, np.float32),
+                 left=np.empty(n, np.uint32), right=np.empty(n, np.uint32),
+                 default_left=np.empty(n, np.uint8), gains=np.empty(n, np.float32),
+                 covers=np.empty(n, np.float32))
+        self.lib.L.ref_model_tree(C.c_void_p(self.h), t, *(a[k].ctypes.data for k in (
+            "feature", "value", "left", "right", "default_left", "gains", "covers")))
+        return Tree(**a)
+
+    def trees(self):
+        return [self.tree(t) for t in range(self.n_trees())]
+
+    def oblivious(self, t):
+        d = int(self.lib.L.ref_model_oblivious_depth(C.c_void_p(self.h), t))
+        f = np.empty(d, np.uint32)
+        thr = np.empty(d, np.float32)
+        dl = np.empty(d, np.uint8)
+        leaves = np.empty(1 << d, np.float32)
+        self.lib.L.ref_model_oblivious(C.c_void_p(self.h), t, f.ctypes.data,
+                                       thr.ctypes.data, dl.ctypes.data, leaves.ctypes.data)
+        return f, thr, dl, leaves
+
+    def predict_binned(self, ds):
+        out = np.empty(ds.n, np.float32)
+        if self.lib.L.ref_model_predict_binned(C.c_void_p(self.h), C.c_void_p(ds.h),
+                                               out.ctypes.data):
+            raise RuntimeError(self.lib.err())
+        return out
+
+    def contribs_binned(self, ds):
+        out = np.empty((ds.n, ds.F + 1), np.float64)
+        if self.lib.L.ref_model_contribs_binned(C.c_void_p(self.h), C.c_void_p(ds.h),
+                                                out.ctypes.data):
+            raise RuntimeError(self.lib.err())
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.L.ref_model_destroy(C.c_void_p(self.h))
+            self.h = None
+
+
+class OrcTreeCfg(C.Structure):
+    _fields_ = [
+        ("min_child_hess", C.c_float), ("min_gain_to_split", C.c_float),
+        ("lambda_l2", C.c_float), ("lambda_l1", C.c_float),
+        ("max_depth", C.c_uint32), ("min_data_in_leaf", C.c_uint32),
+        ("max_leaves", C.c_uint32), ("monotone", C.POINTER(C.c_int32)),
+        ("n_monotone", C.c_uint32),
+    ]
+
+
+class OrcTree(C.Structure):
+    _fields_ = [
+        ("cap", C.c_uint32), ("feature", C.POINTER(C.c_uint32)),
+        ("value", C.POINTER(C.c_float)), ("left", C.POINTER(C.c_uint32)),
+        ("right", C.POINTER(C.c_uint32)), ("default_left", C.POINTER(C.c_uint8)),
+        ("gains", C.POINTER(C.c_float)), ("covers", C.POINTER(C.c_float)),
+        ("split_bin", C.POINTER(C.c_uint32)), ("n_nodes", C.c_uint32),
+        ("depth", C.c_uint32), ("n_leaves", C.c_uint32),
+    ]
+
+
+class _TreeBuf:
+    def __init__(self, cap):
+        self.a = dict(feature=np.zeros(cap, np.uint32), value=np.zeros(cap, np.float32),
+                      left=np.zeros(cap, np.uint32), right=np.zeros(cap, np.uint32),
+                      default_left=np.zeros(cap, np.uint8), gains=np.zeros(cap, np.float32),
+                      covers=np.zeros(cap, np.float32), split_bin=np.zeros(cap, np.uint32))
+        self.s = OrcTree()
+        self.s.cap = cap
+        for k, v in self.a.items():
+            t = {np.uint32: C.c_uint32, np.float32: C.c_float, np.uint8: C.c_uint8}[v.dtype.type]
+            setattr(self.s, k, _p(v, t))
+
+    def tree(self):
+        n = self.s.n_nodes
+        return Tree(**{k: v[:n].copy() for k, v in self.a.items()},
+                    depth=self.s.depth, n_leaves=self.s.n_leaves)
+
+
+class Oracle:
+    """The C restatement (bonsai_oracle.c)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run make -C oracle oracle)")
+        self.L = C.CDLL(path)
+        self.L.orc_init_score.restype = C.c_float
+
+    @staticmethod
+    def cfg(tc: TreeCfg):
+        c = OrcTreeCfg()
+        c.min_child_hess = tc.min_child_hess
+        c.min_gain_to_split = tc.min_gain_to_split
+        c.lambda_l2 = tc.lambda_l2
+        c.lambda_l1 = tc.lambda_l1
+        c.max_depth = tc.max_depth
+        c.min_data_in_leaf = tc.min_data_in_leaf
+        c.max_leaves = tc.max_leaves
+        if tc.monotone:
+            c._mono = np.asarray(tc.monotone, dtype=np.int32)
+            c.monotone = _p(c._mono, C.c_int32)
+            c.n_monotone = len(tc.monotone)
+        return c
+
+    def transform(self, X, cuts, off):
+        X = np.ascontiguousarray(X, np.float32)
+        n, F = X.shape
+        bins = np.empty((F, n), np.uint16)
+        self.L.orc_transform(_p(X, C.c_float), C.c_size_t(n), C.c_size_t(F),
+                             _p(np.ascontiguousarray(cuts, np.float32), C.c_float),
+                             _p(np.ascontiguousarray(off, np.uint32), C.c_uint32),
+                             _p(bins, C.c_uint16))
+        return bins
+
+    def grow(self, bins, n_bins, cuts, off, grad, hess, tc: TreeCfg, rows=None,
+             selected=None):
+        F, n = bins.shape
+        bins = np.ascontiguousarray(bins, np.uint16)
+        rows = np.arange(n, dtype=np.uint32) if rows is None else np.ascontiguousarray(rows, np.uint32)
+        selected = np.arange(F, dtype=np.uint32) if selected is None else np.ascontiguousarray(selected, np.uint32)
+        nb = np.ascontiguousarray(n_bins, np.uint32)
+        cap = 4 << tc.max_depth if tc.grower == "depthwise" else 4 * max(tc.max_leaves, 2)
+        tb = _TreeBuf(cap)
+        values = np.empty(n, np.float32)
+        ids = np.empty(n, np.uint32)
+        cfg = self.cfg(tc)
+        grad = np.ascontiguousarray(grad, np.float32)
+        hess = np.ascontiguousarray(hess, np.float32)
+        cuts = np.ascontiguousarray(cuts, np.float32)
+        off = np.ascontiguousarray(off, np.uint32)
+        rc = self.L.orc_grow_depthwise(
+            _p(bins, C.c_uint16), C.c_size_t(n), C.c_size_t(F), _p(nb, C.c_uint32),
+            _p(cuts, C.c_float), _p(off, C.c_uint32), _p(grad, C.c_float),
+            _p(hess, C.c_float), _p(rows, C.c_uint32), C.c_size_t(len(rows)),
+            _p(selected, C.c_uint32), C.c_size_t(len(selected)), C.byref(cfg),
+            C.byref(tb.s), _p(values, C.c_float), _p(ids, C.c_uint32))
+        if rc:
+            raise RuntimeError("oracle tree outgrew its capacity")
+        return tb.tree(), values, ids
+
+    def train(self, bins, n_bins, cuts, off, labels, tc: TreeCfg):
+        F, n = bins.shape
+        bufs = [_TreeBuf(4 << tc.max_depth) for _ in range(tc.n_iters)]
+        arr = (OrcTree * tc.n_iters)(*[b.s for b in bufs])
+        init = C.c_float()
+        scores = np.empty(n, np.float32)
+        cfg = self.cfg(tc)
+        bins = np.ascontiguousarray(bins, np.uint16)
+        labels = np.ascontiguousarray(labels, np.float32)
+        rc = self.L.orc_train_depthwise(
+            _p(bins, C.c_uint16), C.c_size_t(n), C.c_size_t(F),
+            _p(np.ascontiguousarray(n_bins, np.uint32), C.c_uint32),
+            _p(np.ascontiguousarray(cuts, np.float32), C.c_float),
+            _p(np.ascontiguousarray(off, np.uint32), C.c_uint32),
+            _p(labels, C.c_float), C.c_int(OBJECTIVES[tc.objective]),
+            C.c_uint32(tc.n_iters), C.c_float(tc.learning_rate), C.byref(cfg),
+            arr, C.byref(init), _p(scores, C.c_float))
+        if rc:
+            raise RuntimeError("oracle tree outgrew its capacity")
+        for i, b in enumerate(bufs):
+            b.s = arr[i]
+        return [b.tree() for b in bufs], init.value, scores
+
+    def predict_binned(self, bins, n_bins, trees, init, lr):
+        F, n = bins.shape
+        bufs = []
+        for t in trees:
+            b = _TreeBuf(len(t.feature))
+            for k in b.a:
+                b.a[k][:] = getattr(t, k)
+            b.s.n_nodes = len(t.feature)
+            bufs.append(b)
+        arr = (OrcTree * len(bufs))(*[b.s for b in bufs])
+        out = np.empty(n, np.float32)
+        bins = np.ascontiguousarray(bins, np.uint16)
+        self.L.orc_predict_binned(_p(bins, C.c_uint16), C.c_size_t(n),
+                                  _p(np.ascontiguousarray(n_bins, np.uint32), C.c_uint32),
+                                  arr, C.c_size_t(len(bufs)), C.c_float(init),
+                                  C.c_float(lr), _p(out, C.c_float))
+        return out

@@ -1,0 +1,658 @@
+// TEST INFRASTRUCTURE — the oracle harness. Not part of the product.
+//
+// A C-ABI driver over the reference's own CPU implementation of the
+// CUDA-grower hot path, compiled from the reference's sources by
+// oracle/Makefile into oracle/_ref/libbonsai_ref.so. Only tests/, the smoke
+// check and bench.py's CPU-baseline leg load it, always as the checker.
+//
+// What it drives (reference files, by path within the project):
+//   BinMapper::fit / transform        src/bin_mapper.cpp:232-291
+//   Dataset::bin (host bin fill)      src/dataset.cpp:45-160
+//   Booster<Obj, Grower, Sampler>     include/bonsai/booster.hpp:484-592
+//   DepthwiseGrower / ObliviousGrower / LeafwiseGrower<CpuHistogramEngine>
+//                                     src/grower.cpp:155-157, src/grower_impl.hpp
+//   HistogramNodeSplitFinder          src/split.cpp:271-297
+//   DenseTree walk, tree_shap_binned  src/tree.cpp, src/shap.cpp
+//
+// libstdc++ 13 cannot compile src/bin_mappers.cpp (ranges::sample over an
+// iota_view), so the three BinMappers accessors the other sources call are
+// defined here, and per-column mappers are assembled with from_mappers.
+// For <= n_samples rows that equals BinMappers::fit exactly.
+
+#include "bonsai/bin_mapper.hpp"
+#include "bonsai/bin_mappers.hpp"
+#include "bonsai/booster.hpp"
+#include "bonsai/config/config.hpp"
+#include "bonsai/dataset.hpp"
+#include "bonsai/grower.hpp"
+#include "bonsai/multiclass_booster.hpp"
+#include "bonsai/objective.hpp"
+#include "bonsai/parallel.hpp"
+#include "bonsai/sampler.hpp"
+#include "bonsai/shap.hpp"
+#include "bonsai/split.hpp"
+#include "bonsai/tree.hpp"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace bonsai
+{
+BinMapper const &BinMappers::operator[](size_t fid) const
+{
+    return mappers_[fid];
+}
+size_t BinMappers::size() const
+{
+    return mappers_.size();
+}
+std::span<std::string const> BinMappers::feature_names() const
+{
+    return feature_names_;
+}
+} // namespace bonsai
+
+using namespace bonsai;
+
+namespace
+{
+
+thread_local std::string g_err;
+
+template <typename F> int guarded(F &&f)
+{
+    try
+    {
+        f();
+        return 0;
+    }
+    catch (std::exception const &e)
+    {
+        g_err = e.what();
+        return 1;
+    }
+    catch (...)
+    {
+        g_err = "unknown exception";
+        return 1;
+    }
+}
+
+BinMappers mappers_from_cuts(float const *cuts, uint32_t const *cut_off, size_t F)
+{
+    std::vector<BinMapper>   ms;
+    std::vector<std::string> names;
+    for (size_t f = 0; f < F; ++f)
+    {
+        ms.push_back(BinMapper::from_cuts(
+            std::vector<float>(cuts + cut_off[f], cuts + cut_off[f + 1])));
+        names.push_back("f" + std::to_string(f));
+    }
+    return BinMappers::from_mappers(std::move(ms), std::move(names));
+}
+
+// One flattened tree: DenseTree nodes plus their gains and covers. Oblivious
+// trees are reported through their dense equivalent and their own tables.
+struct FlatTree
+{
+    std::vector<uint32_t> feature;
+    std::vector<float>    value; // threshold (internal) or leaf value
+    std::vector<uint32_t> left, right;
+    std::vector<uint8_t>  default_left;
+    std::vector<float>    gains, covers;
+    uint32_t              depth = 0, n_leaves = 0;
+};
+
+FlatTree flatten(DenseTree const &t)
+{
+    FlatTree ft;
+    for (auto const &n : t.nodes())
+    {
+        ft.feature.push_back(n.feature_id);
+        ft.value.push_back(n.threshold_or_value);
+        ft.left.push_back(n.left);
+        ft.right.push_back(n.right);
+        ft.default_left.push_back(n.default_left ? 1 : 0);
+    }
+    ft.gains  = t.split_gains();
+    ft.covers = t.covers();
+    ft.gains.resize(ft.feature.size(), 0.0F);
+    ft.covers.resize(ft.feature.size(), 0.0F);
+    ft.depth    = static_cast<uint32_t>(t.params().depth);
+    ft.n_leaves = static_cast<uint32_t>(t.params().n_leaves);
+    return ft;
+}
+
+} // namespace
+
+struct ref_cfg
+    {
+        int32_t  grower;    // 0 depthwise, 1 levelwise (oblivious), 2 leafwise
+        int32_t  objective; // 0 mse, 1 logloss, 2 softmax
+        uint32_t n_iters;
+        float    learning_rate;
+        float    min_child_hess;
+        float    min_gain_to_split;
+        float    lambda_l2;
+        float    lambda_l1;
+        float    feature_fraction;
+        uint32_t max_depth;
+        uint32_t min_data_in_leaf;
+        uint32_t max_leaves;
+        uint32_t feature_seed;
+        float    subsample; // < 1 selects the Bernoulli sampler
+        uint32_t random_seed;
+        uint32_t n_threads;
+        uint32_t n_classes;
+        int32_t const *monotone;
+        uint32_t       n_monotone;
+    };
+
+    struct RefModel
+    {
+        std::unique_ptr<IBooster> booster;
+        std::vector<FlatTree>     trees;
+        std::vector<float>        init_scores;
+        int32_t                   grower = 0;
+        // oblivious tables, per tree
+        std::vector<std::vector<ObliviousTree::LevelSplit>> level_splits;
+        std::vector<std::vector<float>>                     leaf_tables;
+    };
+
+namespace
+{
+    Config make_config(ref_cfg const &c)
+    {
+        Config cfg;
+        cfg.tree_config.min_child_hess    = c.min_child_hess;
+        cfg.tree_config.min_gain_to_split = c.min_gain_to_split;
+        cfg.tree_config.lambda_l2         = c.lambda_l2;
+        cfg.tree_config.lambda_l1         = c.lambda_l1;
+        cfg.tree_config.feature_fraction  = c.feature_fraction;
+        cfg.tree_config.max_depth         = static_cast<uint8_t>(c.max_depth);
+        cfg.tree_config.min_data_in_leaf  = static_cast<uint8_t>(c.min_data_in_leaf);
+        cfg.tree_config.max_leaves        = c.max_leaves;
+        cfg.tree_config.feature_seed      = c.feature_seed;
+        if (c.monotone != nullptr)
+        {
+            cfg.tree_config.monotone_constraints.assign(c.monotone,
+                                                        c.monotone + c.n_monotone);
+        }
+        cfg.booster_config.n_iters       = c.n_iters;
+        cfg.booster_config.learning_rate = c.learning_rate;
+        cfg.booster_config.random_seed   = c.random_seed;
+        cfg.sampler.subsample            = c.subsample;
+        cfg.objective.n_classes          = c.n_classes;
+        return cfg;
+    }
+
+    template <typename Gr, typename Sa>
+    std::unique_ptr<IBooster> make_for_objective(ref_cfg const &c, Config const &cfg)
+    {
+        switch (c.objective)
+        {
+        case 0:
+            return std::make_unique<Booster<MSEObjective, Gr, Sa>>(cfg);
+        case 1:
+            return std::make_unique<Booster<LogLossObjective, Gr, Sa>>(cfg);
+        case 2:
+            return std::make_unique<MulticlassBooster<Gr, Sa>>(cfg);
+        default:
+            throw std::runtime_error("unknown objective");
+        }
+    }
+
+    template <typename Gr>
+    std::unique_ptr<IBooster> make_for_sampler(ref_cfg const &c, Config const &cfg)
+    {
+        if (c.subsample < 1.0F)
+        {
+            return make_for_objective<Gr, BernoulliSampler>(c, cfg);
+        }
+        return make_for_objective<Gr, AllRowsSampler>(c, cfg);
+    }
+
+    template <typename B> void harvest_dense(RefModel &m, B const &b)
+    {
+        for (auto const &t : b.trees())
+        {
+            m.trees.push_back(flatten(t));
+        }
+    }
+
+    template <typename B> void harvest_oblivious(RefModel &m, B const &b)
+    {
+        for (auto const &t : b.trees())
+        {
+            m.level_splits.push_back(t.splits());
+            m.leaf_tables.push_back(t.leaf_table());
+            m.trees.push_back(flatten(dense_equivalent(t)));
+        }
+    }
+
+    template <typename Gr> void harvest(RefModel &m, ref_cfg const &c)
+    {
+        auto *raw = m.booster.get();
+        auto  go  = [&](auto *b)
+        {
+            if (b == nullptr)
+            {
+                return false;
+            }
+            if constexpr (std::same_as<typename Gr::Tree, DenseTree>)
+            {
+                harvest_dense(m, *b);
+            }
+            else
+            {
+                harvest_oblivious(m, *b);
+            }
+            return true;
+        };
+        bool ok = false;
+        if (c.subsample < 1.0F)
+        {
+            ok = go(dynamic_cast<Booster<MSEObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<LogLossObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<MulticlassBooster<Gr, BernoulliSampler> *>(raw));
+        }
+        else
+        {
+            ok = go(dynamic_cast<Booster<MSEObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<LogLossObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<MulticlassBooster<Gr, AllRowsSampler> *>(raw));
+        }
+        if (!ok)
+        {
+            throw std::runtime_error("booster type not recognised");
+        }
+    }
+
+    template <typename B> void read_init(RefModel &m, B const *b)
+    {
+        if (b != nullptr)
+        {
+            m.init_scores = {b->init_score()};
+        }
+    }
+} // namespace
+
+
+extern "C"
+{
+
+
+
+    char const *ref_last_error()
+    {
+        return g_err.c_str();
+    }
+
+    // BinMapper::fit per column (row-major X), cuts written flattened.
+    // cut_off must hold F + 1 entries; cuts_cap bounds the cut buffer.
+    int ref_fit_cuts(float const *X, size_t n, size_t F, int32_t max_bin,
+                     size_t n_samples, uint64_t seed, float *cuts, size_t cuts_cap,
+                     uint32_t *cut_off)
+    {
+        return guarded(
+            [&]
+            {
+                BinMapperConfig cfg;
+                cfg.max_bin   = max_bin;
+                cfg.n_samples = n_samples;
+                cfg.seed      = seed;
+                size_t             pos = 0;
+                std::vector<float> col(n);
+                for (size_t f = 0; f < F; ++f)
+                {
+                    for (size_t r = 0; r < n; ++r)
+                    {
+                        col[r] = X[(r * F) + f];
+                    }
+                    BinMapper const m = BinMapper::fit(col, cfg);
+                    auto const      c = m.cuts();
+                    if (pos + c.size() > cuts_cap)
+                    {
+                        throw std::runtime_error("ref_fit_cuts: cut buffer too small");
+                    }
+                    cut_off[f] = static_cast<uint32_t>(pos);
+                    std::memcpy(cuts + pos, c.data(), c.size() * sizeof(float));
+                    pos += c.size();
+                }
+                cut_off[F] = static_cast<uint32_t>(pos);
+            });
+    }
+
+    // Cuts from an explicit NaN-free sample per column (the shared row sample
+    // for tall data), via BinMapper::from_sample.
+    int ref_cuts_from_sample(float const *sample_rowmajor, size_t n, size_t F,
+                             int32_t max_bin, float *cuts, size_t cuts_cap,
+                             uint32_t *cut_off)
+    {
+        return guarded(
+            [&]
+            {
+                BinMapperConfig cfg;
+                cfg.max_bin = max_bin;
+                size_t pos  = 0;
+                for (size_t f = 0; f < F; ++f)
+                {
+                    std::vector<float> col;
+                    for (size_t r = 0; r < n; ++r)
+                    {
+                        float const v = sample_rowmajor[(r * F) + f];
+                        if (!std::isnan(v))
+                        {
+                            col.push_back(v);
+                        }
+                    }
+                    BinMapper const m = BinMapper::from_sample(std::move(col), cfg);
+                    auto const      c = m.cuts();
+                    if (pos + c.size() > cuts_cap)
+                    {
+                        throw std::runtime_error("ref_cuts_from_sample: buffer");
+                    }
+                    cut_off[f] = static_cast<uint32_t>(pos);
+                    std::memcpy(cuts + pos, c.data(), c.size() * sizeof(float));
+                    pos += c.size();
+                }
+                cut_off[F] = static_cast<uint32_t>(pos);
+            });
+    }
+
+    // A binned Dataset over row-major X under the given cuts.
+    void *ref_dataset_create(float const *X, float const *y, size_t n, size_t F,
+                             float const *cuts, uint32_t const *cut_off)
+    {
+        Dataset *out = nullptr;
+        int const rc = guarded(
+            [&]
+            {
+                BinMappers const mappers = mappers_from_cuts(cuts, cut_off, F);
+                features_view    Xv(X, n, F);
+                std::vector<float> labels(y, y + n);
+                out = new Dataset(Dataset::bin(Xv, labels, mappers, DataConfig{}));
+            });
+        return rc == 0 ? out : nullptr;
+    }
+
+    void ref_dataset_destroy(void *ds)
+    {
+        delete static_cast<Dataset *>(ds);
+    }
+
+    int ref_dataset_u8(void const *ds)
+    {
+        return static_cast<Dataset const *>(ds)->bins_are_u8() ? 1 : 0;
+    }
+
+    // Feature-major bin codes, widened to u16.
+    int ref_dataset_bins(void const *dsp, uint16_t *out)
+    {
+        return guarded(
+            [&]
+            {
+                auto const  &ds = *static_cast<Dataset const *>(dsp);
+                size_t const n  = ds.n_rows();
+                for (size_t f = 0; f < ds.n_features(); ++f)
+                {
+                    for (size_t r = 0; r < n; ++r)
+                    {
+                        out[(f * n) + r] = ds.bin_at(f, r);
+                    }
+                }
+            });
+    }
+
+    // Trains a Booster on ds for cfg.n_iters rounds. Returns a model handle.
+    void *ref_train(void const *dsp, ref_cfg const *c)
+    {
+        RefModel *m  = nullptr;
+        int const rc = guarded(
+            [&]
+            {
+                auto const &ds  = *static_cast<Dataset const *>(dsp);
+                Config      cfg = make_config(*c);
+                parallel::set_n_threads(c->n_threads);
+                auto mm    = std::make_unique<RefModel>();
+                mm->grower = c->grower;
+                switch (c->grower)
+                {
+                case 0:
+                    mm->booster = make_for_sampler<DepthwiseGrower<>>(*c, cfg);
+                    break;
+                case 1:
+                    mm->booster = make_for_sampler<ObliviousGrower<>>(*c, cfg);
+                    break;
+                case 2:
+                    mm->booster = make_for_sampler<LeafwiseGrower<>>(*c, cfg);
+                    break;
+                default:
+                    throw std::runtime_error("unknown grower");
+                }
+                for (uint32_t i = 0; i < c->n_iters; ++i)
+                {
+                    mm->booster->update_one_iter(ds);
+                }
+                switch (c->grower)
+                {
+                case 0:
+                    harvest<DepthwiseGrower<>>(*mm, *c);
+                    break;
+                case 1:
+                    harvest<ObliviousGrower<>>(*mm, *c);
+                    break;
+                default:
+                    harvest<LeafwiseGrower<>>(*mm, *c);
+                    break;
+                }
+                auto *raw = mm->booster.get();
+                read_init(*mm, dynamic_cast<Booster<MSEObjective, DepthwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<LogLossObjective, DepthwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<MSEObjective, ObliviousGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<LogLossObjective, ObliviousGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<MSEObjective, LeafwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<LogLossObjective, LeafwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<MSEObjective, DepthwiseGrower<>,
+                                                    BernoulliSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<MSEObjective, LeafwiseGrower<>,
+                                                    BernoulliSampler> const *>(raw));
+                m = mm.release();
+            });
+        return rc == 0 ? m : nullptr;
+    }
+
+    void ref_model_destroy(void *mp)
+    {
+        delete static_cast<RefModel *>(mp);
+    }
+
+    size_t ref_model_n_trees(void const *mp)
+    {
+        return static_cast<RefModel const *>(mp)->trees.size();
+    }
+
+    float ref_model_init_score(void const *mp)
+    {
+        auto const *m = static_cast<RefModel const *>(mp);
+        return m->init_scores.empty() ? 0.0F : m->init_scores[0];
+    }
+
+    size_t ref_model_tree_size(void const *mp, size_t t)
+    {
+        return static_cast<RefModel const *>(mp)->trees[t].feature.size();
+    }
+
+    // Copies tree t's node table (n = ref_model_tree_size entries each).
+    void ref_model_tree(void const *mp, size_t t, uint32_t *feature, float *value,
+                        uint32_t *left, uint32_t *right, uint8_t *default_left,
+                        float *gains, float *covers)
+    {
+        auto const &ft = static_cast<RefModel const *>(mp)->trees[t];
+        size_t const n = ft.feature.size();
+        std::memcpy(feature, ft.feature.data(), n * 4);
+        std::memcpy(value, ft.value.data(), n * 4);
+        std::memcpy(left, ft.left.data(), n * 4);
+        std::memcpy(right, ft.right.data(), n * 4);
+        std::memcpy(default_left, ft.default_left.data(), n);
+        std::memcpy(gains, ft.gains.data(), n * 4);
+        std::memcpy(covers, ft.covers.data(), n * 4);
+    }
+
+    // Oblivious tree t: depth level splits and 2^depth leaf values.
+    size_t ref_model_oblivious_depth(void const *mp, size_t t)
+    {
+        auto const *m = static_cast<RefModel const *>(mp);
+        return t < m->level_splits.size() ? m->level_splits[t].size() : 0;
+    }
+
+    void ref_model_oblivious(void const *mp, size_t t, uint32_t *feature,
+                             float *threshold, uint8_t *default_left, float *leaves)
+    {
+        auto const *m  = static_cast<RefModel const *>(mp);
+        auto const &ls = m->level_splits[t];
+        for (size_t i = 0; i < ls.size(); ++i)
+        {
+            feature[i]      = ls[i].feature_id;
+            threshold[i]    = ls[i].threshold;
+            default_left[i] = ls[i].default_left ? 1 : 0;
+        }
+        auto const &lt = m->leaf_tables[t];
+        std::memcpy(leaves, lt.data(), lt.size() * 4);
+    }
+
+    // Binned predict over ds: init + lr * sum of leaves (predict_at_binned).
+    int ref_model_predict_binned(void const *mp, void const *dsp, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                auto const *m  = static_cast<RefModel const *>(mp);
+                auto const &ds = *static_cast<Dataset const *>(dsp);
+                m->booster->predict_at_binned(ds, {out, ds.n_rows()}, 0);
+            });
+    }
+
+    // Raw-feature predict over row-major X (predict_at).
+    int ref_model_predict(void const *mp, float const *X, size_t n, size_t F, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                auto const *m = static_cast<RefModel const *>(mp);
+                m->booster->predict(features_view(X, n, F), {out, n});
+            });
+    }
+
+    // TreeSHAP over ds in bin space: n_rows x (F + 1) doubles, bias last.
+    int ref_model_contribs_binned(void const *mp, void const *dsp, double *out)
+    {
+        return guarded(
+            [&]
+            {
+                auto const  *m  = static_cast<RefModel const *>(mp);
+                auto const  &ds = *static_cast<Dataset const *>(dsp);
+                size_t const F  = ds.n_features();
+                m->booster->pred_contribs_binned(ds, {out, ds.n_rows() * (F + 1)}, F);
+            });
+    }
+
+    // Grows ONE depthwise/levelwise/leafwise tree on given grad/hess over the
+    // given ascending rows, through the reference's CPU grower. Outputs the
+    // per-row leaf values and leaf ids over all ds rows (unsampled rows are
+    // routed, as grow does) and keeps the tree for the getters below.
+    void *ref_grow_tree(void const *dsp, ref_cfg const *c, float const *grad,
+                        float const *hess, uint32_t const *rows, size_t n_sel,
+                        float *values, uint32_t *leaf_ids)
+    {
+        RefModel *m  = nullptr;
+        int const rc = guarded(
+            [&]
+            {
+                auto const &ds  = *static_cast<Dataset const *>(dsp);
+                Config      cfg = make_config(*c);
+                parallel::set_n_threads(c->n_threads);
+                size_t const       n = ds.n_rows();
+                floats_view const  g{grad, n};
+                floats_view const  h{hess, n};
+                row_index_view const ri{rows, n_sel};
+                auto mm    = std::make_unique<RefModel>();
+                mm->grower = c->grower;
+                auto take  = [&](auto &&res)
+                {
+                    std::memcpy(values, res.values.data(), n * 4);
+                    std::memcpy(leaf_ids, res.leaf_ids.data(), n * 4);
+                    return std::move(res.tree);
+                };
+                switch (c->grower)
+                {
+                case 0:
+                {
+                    DepthwiseGrower<> gr(cfg.tree_config);
+                    mm->trees.push_back(flatten(take(gr.grow(ds, g, h, ri))));
+                    break;
+                }
+                case 1:
+                {
+                    ObliviousGrower<> gr(cfg.tree_config);
+                    ObliviousTree     t = take(gr.grow(ds, g, h, ri));
+                    mm->level_splits.push_back(t.splits());
+                    mm->leaf_tables.push_back(t.leaf_table());
+                    mm->trees.push_back(flatten(dense_equivalent(t)));
+                    break;
+                }
+                default:
+                {
+                    LeafwiseGrower<> gr(cfg.tree_config);
+                    mm->trees.push_back(flatten(take(gr.grow(ds, g, h, ri))));
+                    break;
+                }
+                }
+                m = mm.release();
+            });
+        return rc == 0 ? m : nullptr;
+    }
+
+    // The reference's node split finder on one hand-built histogram set:
+    // hist is [F][n_bins] cells of (g, h) floats, F features sharing n_bins.
+    // Writes (gain, feature, bin, default_left, valid).
+    int ref_find_split(float const *hist, size_t F, size_t n_bins, size_t n_rows,
+                       ref_cfg const *c, double *gain, uint32_t *feature,
+                       uint32_t *bin, uint8_t *default_left, uint8_t *valid)
+    {
+        return guarded(
+            [&]
+            {
+                Config     cfg = make_config(*c);
+                SplitInput in;
+                for (size_t f = 0; f < F; ++f)
+                {
+                    Histogram hh(n_bins);
+                    for (size_t b = 0; b < n_bins; ++b)
+                    {
+                        float const *cell = hist + (((f * n_bins) + b) * 2);
+                        hh.add(static_cast<bin_id_t>(b), cell[0], cell[1]);
+                    }
+                    in.hists.push_back(std::move(hh));
+                }
+                in.rows.assign(n_rows, 0);
+                SplitOutput const s = HistogramNodeSplitFinder::find(in, cfg.tree_config);
+                *gain               = s.gain;
+                *feature            = s.feature_id;
+                *bin                = s.bin_id;
+                *default_left       = s.default_left ? 1 : 0;
+                *valid              = s.valid ? 1 : 0;
+            });
+    }
+}
