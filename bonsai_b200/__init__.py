@@ -1,0 +1,264 @@
+"""bonsai_b200: B200-native (sm_100a) CUDA growers for bonsai.
+
+The hot path of bonsai's CUDA growers -- bin application, per-level
+histograms with sibling subtraction, split finding, stable row partition,
+leaf values with the fused score update, ensemble predict -- as hand-written
+CUDA behind a C ABI (include/bonsai_b200.h). This module is the Python host
+side over that ABI:
+
+    cuts, off = fit_cuts(X)                  # host mappers
+    plane = Plane(X, cuts, off)              # device bin application
+    b = Booster(plane, y, TrainParams(...))  # device-resident boosting
+    b.update(100); trees = b.trees()
+    p = predict(plane, trees, b.init_score, lr)
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import BonsaiError, ConfigError, check, lib, ptr
+from .binning import cuts_from_sample, fit_cuts, sample_rows
+
+__all__ = [
+    "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
+    "grow_tree", "predict", "fit_cuts", "cuts_from_sample", "sample_rows",
+    "available", "LEAF",
+]
+
+LEAF = 0xFFFFFFFF
+OBJECTIVES = {"mse": 0, "logloss": 1}
+HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
+
+
+def available() -> bool:
+    return bool(lib().bb_available())
+
+
+@dataclass
+class TrainParams:
+    """TreeConfig / BoosterConfig keys the device path reads (defaults are
+    the reference's: include/bonsai/config/tree_config.hpp:9-29)."""
+    objective: str = "mse"
+    learning_rate: float = 0.1
+    min_child_hess: float = 1.0
+    min_gain_to_split: float = 0.0
+    lambda_l2: float = 1.0
+    lambda_l1: float = 0.0
+    max_depth: int = 6
+    min_data_in_leaf: int = 20
+    hist_mode: str = "exact"
+    seed: int = 0
+    monotone: list = field(default_factory=list)
+    selected: list | None = None
+    use_graph: bool = False
+
+    def c(self) -> _lib.TrainCfg:
+        c = _lib.TrainCfg()
+        c.objective = OBJECTIVES[self.objective]
+        c.learning_rate = self.learning_rate
+        c.min_child_hess = self.min_child_hess
+        c.min_gain_to_split = self.min_gain_to_split
+        c.lambda_l2 = self.lambda_l2
+        c.lambda_l1 = self.lambda_l1
+        c.max_depth = self.max_depth
+        c.min_data_in_leaf = self.min_data_in_leaf
+        c.hist_mode = HIST_MODES[self.hist_mode]
+        c.seed = self.seed
+        c.use_graph = 1 if self.use_graph else 0
+        if self.monotone:
+            c._mono = np.ascontiguousarray(self.monotone, dtype=np.int8)
+            c.monotone = c._mono.ctypes.data_as(C.POINTER(C.c_int8))
+            c.n_monotone = len(self.monotone)
+        if self.selected is not None:
+            c._sel = np.ascontiguousarray(self.selected, dtype=np.uint32)
+            c.selected = c._sel.ctypes.data_as(C.POINTER(C.c_uint32))
+            c.n_selected = len(self.selected)
+        return c
+
+
+@dataclass
+class Tree:
+    """One tree in the reference's DenseTree layout (tree.hpp:38-45)."""
+    feature: np.ndarray
+    value: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    default_left: np.ndarray
+    gains: np.ndarray
+    covers: np.ndarray
+    split_bin: np.ndarray
+    depth: int = 0
+    n_leaves: int = 0
+
+
+def _tree_arrays(cap: int):
+    return dict(feature=np.zeros(cap, np.uint32), value=np.zeros(cap, np.float32),
+                left=np.zeros(cap, np.uint32), right=np.zeros(cap, np.uint32),
+                default_left=np.zeros(cap, np.uint8), gains=np.zeros(cap, np.float32),
+                covers=np.zeros(cap, np.float32), split_bin=np.zeros(cap, np.uint32))
+
+
+_ORDER = ("feature", "value", "left", "right", "default_left", "gains", "covers",
+          "split_bin")
+
+
+def _finish(a: dict, meta: np.ndarray) -> Tree:
+    n = int(meta[0])
+    return Tree(**{k: v[:n].copy() for k, v in a.items()}, depth=int(meta[1]),
+                n_leaves=int(meta[2]))
+
+
+class Plane:
+    """A device-resident binned dataset (bb_ingest)."""
+
+    def __init__(self, X, cuts, cut_off, x_on_device: bool = False):
+        if x_on_device:
+            # a torch CUDA tensor (or anything exposing data_ptr and shape)
+            n, F = X.shape
+            xp = X.data_ptr()
+            self._keep = X
+        else:
+            X = np.ascontiguousarray(X, dtype=np.float32)
+            n, F = X.shape
+            xp = ptr(X)
+            self._keep = X
+        self.cuts = np.ascontiguousarray(cuts, dtype=np.float32)
+        self.cut_off = np.ascontiguousarray(cut_off, dtype=np.uint32)
+        if len(self.cut_off) != F + 1:
+            raise ValueError("cut_off must hold n_features + 1 offsets")
+        self.n_rows, self.n_feats = int(n), int(F)
+        self.n_bins = np.diff(self.cut_off).astype(np.uint32)
+        h = C.c_void_p()
+        check(lib().bb_ingest(xp, n, F, 1 if x_on_device else 0, ptr(self.cuts),
+                              ptr(self.cut_off), C.byref(h)))
+        self.h = h.value
+        self._keep = None
+
+    @property
+    def u8(self) -> bool:
+        return bool(lib().bb_plane_is_u8(self.h))
+
+    def bins(self) -> np.ndarray:
+        out = np.empty((self.n_feats, self.n_rows), np.uint16)
+        check(lib().bb_plane_download(self.h, ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_plane_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Booster:
+    """Device-resident boosting (bb_booster_*)."""
+
+    def __init__(self, plane: Plane, labels, params: TrainParams, max_trees: int = 1000,
+                 init_scores=None):
+        self.plane = plane
+        self.params = params
+        self._labels = np.ascontiguousarray(labels, dtype=np.float32)
+        init = None if init_scores is None else np.ascontiguousarray(init_scores, np.float32)
+        h = C.c_void_p()
+        self._cfg = params.c()
+        check(lib().bb_booster_create(plane.h, ptr(self._labels),
+                                      None if init is None else ptr(init),
+                                      C.byref(self._cfg), max_trees, C.byref(h)))
+        self.h = h.value
+
+    def update(self, n_iters: int = 1, sync: bool = True):
+        check(lib().bb_booster_update(self.h, n_iters))
+        if sync:
+            self.sync()
+
+    def sync(self):
+        check(lib().bb_booster_sync(self.h))
+
+    @property
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        check(lib().bb_booster_last_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    @property
+    def init_score(self) -> float:
+        return float(lib().bb_booster_init_score(self.h))
+
+    @property
+    def n_trees(self) -> int:
+        n = C.c_uint32()
+        check(lib().bb_booster_n_trees(self.h, C.byref(n)))
+        return n.value
+
+    def tree(self, t: int) -> Tree:
+        cap = int(lib().bb_booster_tree_capacity(self.h))
+        a = _tree_arrays(cap)
+        meta = np.zeros(3, np.uint32)
+        check(lib().bb_booster_tree(self.h, t, *(ptr(a[k]) for k in _ORDER), ptr(meta)))
+        return _finish(a, meta)
+
+    def trees(self) -> list:
+        return [self.tree(t) for t in range(self.n_trees)]
+
+    def scores(self) -> np.ndarray:
+        out = np.empty(self.plane.n_rows, np.float32)
+        check(lib().bb_booster_scores(self.h, ptr(out)))
+        return out
+
+    def leaf_ids(self) -> np.ndarray:
+        out = np.empty(self.plane.n_rows, np.uint32)
+        check(lib().bb_booster_leaf_ids(self.h, ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_booster_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def grow_tree(plane: Plane, params: TrainParams, grad, hess, rows=None):
+    """One depthwise tree from given gradients (bb_grow_tree): returns
+    (tree, values, leaf_ids) over every row (unsampled rows: NaN / max)."""
+    n = plane.n_rows
+    grad = np.ascontiguousarray(grad, np.float32)
+    hess = np.ascontiguousarray(hess, np.float32)
+    cap = (2 << params.max_depth) - 1
+    a = _tree_arrays(cap)
+    meta = np.zeros(3, np.uint32)
+    values = np.full(n, np.nan, np.float32)
+    ids = np.full(n, LEAF, np.uint32)
+    r = None if rows is None else np.ascontiguousarray(rows, np.uint32)
+    cfg = params.c()
+    check(lib().bb_grow_tree(plane.h, C.byref(cfg), ptr(grad), ptr(hess),
+                             None if r is None else ptr(r), 0 if r is None else len(r),
+                             *(ptr(a[k]) for k in _ORDER), ptr(meta), ptr(values),
+                             ptr(ids)))
+    return _finish(a, meta), values, ids
+
+
+def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
+    """Ensemble predict in bin space (bb_predict)."""
+    roots = np.zeros(len(trees), np.uint32)
+    parts = {k: [] for k in ("feature", "split_bin", "left", "right", "default_left", "value")}
+    base = 0
+    for i, t in enumerate(trees):
+        roots[i] = base
+        for k in parts:
+            parts[k].append(getattr(t, k))
+        base += len(t.feature)
+    cat = {k: np.ascontiguousarray(np.concatenate(v)) for k, v in parts.items()}
+    out = np.empty(plane.n_rows, np.float32)
+    check(lib().bb_predict(plane.h, len(trees), ptr(roots), base, ptr(cat["feature"]),
+                           ptr(cat["split_bin"]), ptr(cat["left"]), ptr(cat["right"]),
+                           ptr(cat["default_left"]), ptr(cat["value"]), lr, init, ptr(out)))
+    return out

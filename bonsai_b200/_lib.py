@@ -1,0 +1,90 @@
+"""ctypes binding of libbonsai_b200.so (the C ABI in include/bonsai_b200.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbonsai_b200.so")
+
+BB_OK, BB_ERR_CUDA, BB_ERR_CONFIG, BB_ERR_ARG, BB_DECLINED = range(5)
+
+
+class BonsaiError(RuntimeError):
+    """A failed call: .code is the C ABI status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+class ConfigError(BonsaiError):
+    """A capacity or configuration refusal (the reference's ConfigError)."""
+
+
+class TrainCfg(C.Structure):
+    _fields_ = [
+        ("objective", C.c_int32), ("learning_rate", C.c_float),
+        ("min_child_hess", C.c_float), ("min_gain_to_split", C.c_float),
+        ("lambda_l2", C.c_float), ("lambda_l1", C.c_float),
+        ("max_depth", C.c_uint32), ("min_data_in_leaf", C.c_uint32),
+        ("hist_mode", C.c_int32), ("seed", C.c_uint64),
+        ("monotone", C.POINTER(C.c_int8)), ("n_monotone", C.c_uint32),
+        ("selected", C.POINTER(C.c_uint32)), ("n_selected", C.c_uint32),
+        ("use_graph", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python -m bonsai_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.bb_last_error.restype = C.c_char_p
+        L.bb_booster_init_score.restype = C.c_float
+        L.bb_booster_tree_capacity.restype = C.c_uint32
+        vp = C.c_void_p
+        L.bb_ingest.argtypes = [vp, C.c_uint64, C.c_uint32, C.c_int, vp, vp, C.POINTER(vp)]
+        L.bb_plane_is_u8.argtypes = [vp]
+        L.bb_plane_download.argtypes = [vp, vp]
+        L.bb_plane_destroy.argtypes = [vp]
+        L.bb_booster_create.argtypes = [vp, vp, vp, C.POINTER(TrainCfg), C.c_uint32,
+                                        C.POINTER(vp)]
+        L.bb_booster_update.argtypes = [vp, C.c_uint32]
+        L.bb_booster_sync.argtypes = [vp]
+        L.bb_booster_n_trees.argtypes = [vp, C.POINTER(C.c_uint32)]
+        L.bb_booster_init_score.argtypes = [vp]
+        L.bb_booster_tree_capacity.argtypes = [vp]
+        L.bb_booster_tree.argtypes = [vp, C.c_uint32] + [vp] * 9
+        L.bb_booster_scores.argtypes = [vp, vp]
+        L.bb_booster_leaf_ids.argtypes = [vp, vp]
+        L.bb_booster_last_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.bb_booster_destroy.argtypes = [vp]
+        L.bb_grow_tree.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64] + [vp] * 11
+        L.bb_predict.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 6 + [
+            C.c_float, C.c_float, vp]
+        L.bb_select_device.argtypes = [C.c_uint32]
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != BB_OK:
+        msg = lib().bb_last_error().decode()
+        if rc == BB_ERR_CONFIG:
+            raise ConfigError(rc, msg)
+        raise BonsaiError(rc, msg)
+
+
+def ptr(a: np.ndarray) -> int:
+    return a.ctypes.data

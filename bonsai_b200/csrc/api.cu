@@ -1,0 +1,820 @@
+// The C ABI (include/bonsai_b200.h): planes, the device-resident booster,
+// single-tree growth and ensemble predict.
+#include "bonsai_b200.h"
+#include "grow.cuh"
+#include "ingest.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+struct bb_plane
+{
+    bb::Plane p;
+};
+
+namespace bb
+{
+namespace
+{
+
+thread_local std::string g_err;
+
+template <typename F> int guarded(F &&f)
+{
+    try
+    {
+        f();
+        g_err.clear();
+        return BB_OK;
+    }
+    catch (CudaError const &e)
+    {
+        g_err = e.what();
+        return BB_ERR_CUDA;
+    }
+    catch (ConfigError const &e)
+    {
+        g_err = e.what();
+        return BB_ERR_CONFIG;
+    }
+    catch (std::invalid_argument const &e)
+    {
+        g_err = e.what();
+        return BB_ERR_ARG;
+    }
+    catch (std::exception const &e)
+    {
+        g_err = e.what();
+        return BB_ERR_CUDA;
+    }
+}
+
+void need(bool ok, char const *what)
+{
+    if (!ok)
+    {
+        throw std::invalid_argument(what);
+    }
+}
+
+// ---- objectives (the resident gradient kernel) ----------------------------
+// mse: g = s - y, h = 1 (src/objective.cpp:44-58); logloss: p = 1/(1+e^-s),
+// g = p - y, h = p(1-p) (src/objective.cpp:86-101).
+__global__ void gradient_kernel(int objective, float const *__restrict__ scores,
+                                float const *__restrict__ labels, float2 *__restrict__ gh,
+                                uint64_t n)
+{
+    uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (i >= n)
+    {
+        return;
+    }
+    float const s = scores[i];
+    float const y = labels[i];
+    if (objective == 0)
+    {
+        gh[i] = make_float2(s - y, 1.0F);
+    }
+    else
+    {
+        float const p = 1.0F / (1.0F + expf(-s));
+        gh[i]         = make_float2(p - y, p * (1.0F - p));
+    }
+}
+
+__global__ void iota_kernel(uint32_t *rows, uint64_t n)
+{
+    uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (i < n)
+    {
+        rows[i] = static_cast<uint32_t>(i);
+    }
+}
+
+__global__ void fill_kernel(float *x, float v, uint64_t n)
+{
+    uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (i < n)
+    {
+        x[i] = v;
+    }
+}
+
+// Copies the scratch tree into slot *round and advances the round counter,
+// so a captured boosting round needs no per-round pointer.
+__global__ void commit_tree_kernel(TreeOut scratch, TreeOut slots, uint32_t cap,
+                                   uint32_t *round)
+{
+    uint32_t const r   = *round;
+    uint64_t const off = static_cast<uint64_t>(r) * cap;
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x)
+    {
+        slots.feature[off + i]      = scratch.feature[i];
+        slots.value[off + i]        = scratch.value[i];
+        slots.left[off + i]         = scratch.left[i];
+        slots.right[off + i]        = scratch.right[i];
+        slots.default_left[off + i] = scratch.default_left[i];
+        slots.gain[off + i]         = scratch.gain[i];
+        slots.cover[off + i]        = scratch.cover[i];
+        slots.split_bin[off + i]    = scratch.split_bin[i];
+    }
+    if (threadIdx.x < 3)
+    {
+        slots.meta[(3 * static_cast<uint64_t>(r)) + threadIdx.x] = scratch.meta[threadIdx.x];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        *round = r + 1;
+    }
+}
+
+// One thread per row, every tree in order: the bin-space walk of
+// routes_left, leaves summed in float in tree order, then init + sum * lr
+// with no contraction (booster.hpp:831-845, detail/bin_walk.hpp).
+template <typename BinT>
+__global__ void predict_kernel(BinT const *__restrict__ bins, uint64_t n_pad, uint64_t n,
+                               uint32_t const *__restrict__ last_bin, uint32_t n_trees,
+                               uint32_t const *__restrict__ roots,
+                               uint32_t const *__restrict__ feature,
+                               uint32_t const *__restrict__ split_bin,
+                               uint32_t const *__restrict__ left,
+                               uint32_t const *__restrict__ right,
+                               uint8_t const *__restrict__ dl,
+                               float const *__restrict__ value, float lr, float init,
+                               float *__restrict__ out)
+{
+    uint64_t const r = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (r >= n)
+    {
+        return;
+    }
+    float acc = 0.0F;
+    for (uint32_t t = 0; t < n_trees; ++t)
+    {
+        uint32_t const base = roots[t];
+        uint32_t       idx  = base;
+        while (feature[idx] != k_leaf_flag)
+        {
+            uint32_t const f = feature[idx];
+            uint32_t const b = bins[(static_cast<uint64_t>(f) * n_pad) + r];
+            idx = base + (routes_left(b, last_bin[f], split_bin[idx], dl[idx] != 0)
+                              ? left[idx]
+                              : right[idx]);
+        }
+        acc = acc + value[idx];
+    }
+    out[r] = init + (acc * lr);
+}
+
+template <typename T> T *dmalloc(size_t n)
+{
+    void *p = nullptr;
+    BB_CHECK(cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T)));
+    return static_cast<T *>(p);
+}
+
+struct TreeStore
+{
+    uint32_t cap  = 0;
+    uint32_t n    = 0;
+    TreeOut  t{};
+    void     alloc(uint32_t capacity, uint32_t slots)
+    {
+        cap                = capacity;
+        n                  = slots;
+        size_t const total = static_cast<size_t>(capacity) * slots;
+        t.feature          = dmalloc<uint32_t>(total);
+        t.value            = dmalloc<float>(total);
+        t.left             = dmalloc<uint32_t>(total);
+        t.right            = dmalloc<uint32_t>(total);
+        t.default_left     = dmalloc<uint8_t>(total);
+        t.gain             = dmalloc<float>(total);
+        t.cover            = dmalloc<float>(total);
+        t.split_bin        = dmalloc<uint32_t>(total);
+        t.meta             = dmalloc<uint32_t>(3 * static_cast<size_t>(slots));
+    }
+    void release()
+    {
+        void *ps[] = {t.feature, t.value,     t.left, t.right, t.default_left,
+                      t.gain,    t.cover,     t.split_bin, t.meta};
+        for (void *p : ps)
+        {
+            if (p != nullptr)
+            {
+                cudaFree(p);
+            }
+        }
+        t = {};
+    }
+    void download(uint32_t slot, uint32_t *feature, float *value, uint32_t *left,
+                  uint32_t *right, uint8_t *dl, float *gain, float *cover,
+                  uint32_t *split_bin, uint32_t *meta) const
+    {
+        size_t const o = static_cast<size_t>(slot) * cap;
+        BB_CHECK(cudaMemcpy(feature, t.feature + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(value, t.value + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(left, t.left + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(right, t.right + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(dl, t.default_left + o, cap, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(gain, t.gain + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(cover, t.cover + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(split_bin, t.split_bin + o, cap * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(meta, t.meta + (3 * static_cast<size_t>(slot)), 12,
+                            cudaMemcpyDeviceToHost));
+    }
+};
+
+GrowConfig grow_config(bb_train_cfg const &c)
+{
+    need(c.max_depth <= 8, "max_depth must be <= 8 on the device level plane");
+    need(c.hist_mode >= 0 && c.hist_mode <= 2, "hist_mode must be 0, 1 or 2");
+    GrowConfig g;
+    g.tp.min_child_hess    = c.min_child_hess;
+    g.tp.min_gain_to_split = c.min_gain_to_split;
+    g.tp.lambda_l2         = c.lambda_l2;
+    g.tp.lambda_l1         = c.lambda_l1;
+    g.tp.max_depth         = c.max_depth;
+    g.tp.min_data_in_leaf  = c.min_data_in_leaf;
+    g.tp.max_leaves        = 0;
+    g.mode                 = static_cast<HistMode>(c.hist_mode);
+    return g;
+}
+
+std::vector<uint32_t> selection(bb_train_cfg const &c, uint32_t F)
+{
+    std::vector<uint32_t> sel;
+    if (c.selected == nullptr)
+    {
+        sel.resize(F);
+        std::iota(sel.begin(), sel.end(), 0U);
+        return sel;
+    }
+    sel.assign(c.selected, c.selected + c.n_selected);
+    for (size_t i = 0; i < sel.size(); ++i)
+    {
+        need(sel[i] < F, "selected feature out of range");
+        need(i == 0 || sel[i] > sel[i - 1], "selected features must be ascending");
+    }
+    return sel;
+}
+
+std::vector<int8_t> monotone(bb_train_cfg const &c)
+{
+    if (c.monotone == nullptr)
+    {
+        return {};
+    }
+    return {c.monotone, c.monotone + c.n_monotone};
+}
+
+uint32_t blocks(uint64_t n, uint32_t t = 256)
+{
+    return ceil_div(std::max<uint64_t>(n, 1), t);
+}
+
+} // namespace
+} // namespace bb
+
+using namespace bb;
+
+struct bb_booster
+{
+    bb::Plane const            *plane = nullptr;
+    cudaStream_t                stream{};
+    int                         objective = 0;
+    float                       lr        = 0.1F;
+    float                       init      = 0.0F;
+    float                      *labels    = nullptr;
+    float                      *scores    = nullptr;
+    float2                     *gh        = nullptr;
+    uint32_t                   *rows      = nullptr;
+    uint32_t                   *leaf_id   = nullptr;
+    uint32_t                   *round     = nullptr;
+    std::unique_ptr<bb::Grower> grower;
+    bb::TreeStore               scratch;
+    bb::TreeStore               trees;
+    uint32_t                    n_trees = 0;
+    bool                        use_graph = false;
+    cudaGraphExec_t             graph     = nullptr;
+    cudaEvent_t                 ev0{}, ev1{};
+    float                       last_ms = 0.0F;
+
+    void round_body()
+    {
+        uint64_t const n = plane->n_rows;
+        gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
+        BB_LAUNCH("gradient_kernel");
+        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t, leaf_id, scores, lr);
+        commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
+        BB_LAUNCH("commit_tree_kernel");
+    }
+};
+
+extern "C"
+{
+
+    char const *bb_last_error(void)
+    {
+        return g_err.c_str();
+    }
+
+    int bb_available(void)
+    {
+        int n = 0;
+        return cudaGetDeviceCount(&n) == cudaSuccess && n > 0 ? 1 : 0;
+    }
+
+    int bb_select_device(uint32_t device_id)
+    {
+        return guarded(
+            [&]
+            {
+                int n = 0;
+                BB_CHECK(cudaGetDeviceCount(&n));
+                if (device_id >= static_cast<uint32_t>(n))
+                {
+                    throw ConfigError("parallel.device_id " + std::to_string(device_id) +
+                                      " is out of range for " + std::to_string(n) +
+                                      " visible CUDA devices");
+                }
+                BB_CHECK(cudaSetDevice(static_cast<int>(device_id)));
+            });
+    }
+
+    int bb_ingest(float const *X, uint64_t n_rows, uint32_t n_feats, int x_on_device,
+                  float const *cuts, uint32_t const *cut_off, bb_plane **out)
+    {
+        return guarded(
+            [&]
+            {
+                need(out != nullptr && X != nullptr && cuts != nullptr && cut_off != nullptr,
+                     "bb_ingest: null argument");
+                need(n_rows > 0 && n_feats > 0, "bb_ingest: empty matrix");
+                need(n_rows < (1ull << 32), "bb_ingest: more than 2^32 - 1 rows");
+                auto pl = std::make_unique<bb_plane>();
+                Plane &p = pl->p;
+                p.n_rows  = n_rows;
+                p.n_pad   = ((n_rows + 63) / 64) * 64;
+                p.n_feats = n_feats;
+                BB_CHECK(cudaGetDevice(&p.device));
+                uint32_t const n_cuts = cut_off[n_feats];
+                uint32_t       max_nb = 0;
+                for (uint32_t f = 0; f < n_feats; ++f)
+                {
+                    need(cut_off[f + 1] > cut_off[f] + 1, "bb_ingest: a feature needs >= 2 bins");
+                    max_nb = std::max(max_nb, cut_off[f + 1] - cut_off[f]);
+                }
+                need(max_nb <= 65535, "bb_ingest: more than 65535 bins");
+                p.u8        = max_nb <= 256;
+                p.h_cuts    = new float[n_cuts];
+                p.h_cut_off = new uint32_t[n_feats + 1];
+                std::memcpy(p.h_cuts, cuts, n_cuts * sizeof(float));
+                std::memcpy(p.h_cut_off, cut_off, (n_feats + 1) * sizeof(uint32_t));
+                std::vector<uint32_t> nb(n_feats);
+                for (uint32_t f = 0; f < n_feats; ++f)
+                {
+                    nb[f] = cut_off[f + 1] - cut_off[f];
+                }
+                p.cuts    = dmalloc<float>(n_cuts);
+                p.cut_off = dmalloc<uint32_t>(n_feats + 1);
+                p.n_bins  = dmalloc<uint32_t>(n_feats);
+                BB_CHECK(cudaMemcpy(p.cuts, cuts, n_cuts * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(p.cut_off, cut_off, (n_feats + 1) * 4,
+                                    cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(p.n_bins, nb.data(), n_feats * 4, cudaMemcpyHostToDevice));
+                size_t const bytes = static_cast<size_t>(n_feats) * p.n_pad * (p.u8 ? 1 : 2);
+                BB_CHECK(cudaMalloc(&p.bins, bytes));
+                BB_CHECK(cudaMemset(p.bins, 0, bytes));
+                cudaStream_t s;
+                BB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                try
+                {
+                    ingest(p, X, x_on_device != 0, s);
+                    BB_CHECK(cudaStreamSynchronize(s));
+                }
+                catch (...)
+                {
+                    cudaStreamDestroy(s);
+                    throw;
+                }
+                BB_CHECK(cudaStreamDestroy(s));
+                *out = pl.release();
+            });
+    }
+
+    int bb_plane_is_u8(bb_plane const *plane)
+    {
+        return plane->p.u8 ? 1 : 0;
+    }
+
+    int bb_plane_download(bb_plane const *plane, uint16_t *out)
+    {
+        return guarded(
+            [&]
+            {
+                Plane const &p = plane->p;
+                if (p.u8)
+                {
+                    std::vector<uint8_t> tmp(p.n_rows);
+                    for (uint32_t f = 0; f < p.n_feats; ++f)
+                    {
+                        BB_CHECK(cudaMemcpy(tmp.data(),
+                                            static_cast<uint8_t const *>(p.bins) + (f * p.n_pad),
+                                            p.n_rows, cudaMemcpyDeviceToHost));
+                        for (uint64_t r = 0; r < p.n_rows; ++r)
+                        {
+                            out[(f * p.n_rows) + r] = tmp[r];
+                        }
+                    }
+                }
+                else
+                {
+                    for (uint32_t f = 0; f < p.n_feats; ++f)
+                    {
+                        BB_CHECK(cudaMemcpy(out + (f * p.n_rows),
+                                            static_cast<uint16_t const *>(p.bins) + (f * p.n_pad),
+                                            p.n_rows * 2, cudaMemcpyDeviceToHost));
+                    }
+                }
+            });
+    }
+
+    void bb_plane_destroy(bb_plane *plane)
+    {
+        if (plane == nullptr)
+        {
+            return;
+        }
+        Plane &p = plane->p;
+        cudaFree(p.bins);
+        cudaFree(p.cuts);
+        cudaFree(p.cut_off);
+        cudaFree(p.n_bins);
+        delete[] p.h_cuts;
+        delete[] p.h_cut_off;
+        delete plane;
+    }
+
+    int bb_booster_create(bb_plane const *plane, float const *labels,
+                          float const *init_scores, bb_train_cfg const *cfg,
+                          uint32_t max_trees, bb_booster **out)
+    {
+        return guarded(
+            [&]
+            {
+                need(plane != nullptr && labels != nullptr && cfg != nullptr && out != nullptr,
+                     "bb_booster_create: null argument");
+                need(cfg->objective == 0 || cfg->objective == 1,
+                     "objective must be 0 (mse) or 1 (logloss)");
+                need(max_trees > 0, "max_trees must be positive");
+                if (cfg->hist_mode != 0)
+                {
+                    throw ConfigError("quantised histograms are not built in this library");
+                }
+                auto         b = std::make_unique<bb_booster>();
+                Plane const &p = plane->p;
+                uint64_t const n = p.n_rows;
+                b->plane         = &p;
+                b->objective     = cfg->objective;
+                b->lr            = cfg->learning_rate;
+                BB_CHECK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+                // init_score: a float serial sum, as std::accumulate does
+                float sum = 0.0F;
+                for (uint64_t i = 0; i < n; ++i)
+                {
+                    sum += labels[i];
+                }
+                float const nn = static_cast<float>(n);
+                b->init        = cfg->objective == 0 ? sum / nn : std::log((sum / nn) / (1.0F - (sum / nn)));
+                b->labels      = dmalloc<float>(n);
+                b->scores      = dmalloc<float>(n);
+                b->gh          = dmalloc<float2>(n);
+                b->rows        = dmalloc<uint32_t>(n);
+                b->leaf_id     = dmalloc<uint32_t>(n);
+                b->round       = dmalloc<uint32_t>(1);
+                BB_CHECK(cudaMemcpyAsync(b->labels, labels, n * 4, cudaMemcpyHostToDevice, b->stream));
+                if (init_scores != nullptr)
+                {
+                    BB_CHECK(cudaMemcpyAsync(b->scores, init_scores, n * 4, cudaMemcpyHostToDevice,
+                                             b->stream));
+                }
+                else
+                {
+                    fill_kernel<<<blocks(n), 256, 0, b->stream>>>(b->scores, b->init, n);
+                    BB_LAUNCH("fill_kernel");
+                }
+                iota_kernel<<<blocks(n), 256, 0, b->stream>>>(b->rows, n);
+                BB_LAUNCH("iota_kernel");
+                BB_CHECK(cudaMemsetAsync(b->round, 0, 4, b->stream));
+                b->grower = std::make_unique<Grower>(p, grow_config(*cfg),
+                                                     selection(*cfg, p.n_feats),
+                                                     static_cast<uint32_t>(n), b->stream);
+                b->grower->set_monotone(monotone(*cfg));
+                b->scratch.alloc(b->grower->max_nodes(), 1);
+                b->trees.alloc(b->grower->max_nodes(), max_trees);
+                b->use_graph = cfg->use_graph != 0;
+                BB_CHECK(cudaEventCreate(&b->ev0));
+                BB_CHECK(cudaEventCreate(&b->ev1));
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                *out = b.release();
+            });
+    }
+
+    int bb_booster_update(bb_booster *b, uint32_t n_iters)
+    {
+        return guarded(
+            [&]
+            {
+                need(b->n_trees + n_iters <= b->trees.n, "bb_booster_update: tree capacity");
+                if (b->use_graph && b->graph == nullptr)
+                {
+                    cudaGraph_t g;
+                    BB_CHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+                    try
+                    {
+                        b->round_body();
+                    }
+                    catch (...)
+                    {
+                        cudaStreamEndCapture(b->stream, &g);
+                        throw;
+                    }
+                    BB_CHECK(cudaStreamEndCapture(b->stream, &g));
+                    BB_CHECK(cudaGraphInstantiate(&b->graph, g, 0));
+                    BB_CHECK(cudaGraphDestroy(g));
+                }
+                BB_CHECK(cudaEventRecord(b->ev0, b->stream));
+                for (uint32_t i = 0; i < n_iters; ++i)
+                {
+                    if (b->graph != nullptr)
+                    {
+                        BB_CHECK(cudaGraphLaunch(b->graph, b->stream));
+                    }
+                    else
+                    {
+                        b->round_body();
+                    }
+                }
+                BB_CHECK(cudaEventRecord(b->ev1, b->stream));
+                b->n_trees += n_iters;
+            });
+    }
+
+    int bb_booster_sync(bb_booster *b)
+    {
+        return guarded(
+            [&]
+            {
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                BB_CHECK(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+            });
+    }
+
+    int bb_booster_last_ms(bb_booster const *b, float *ms)
+    {
+        *ms = b->last_ms;
+        return BB_OK;
+    }
+
+    int bb_booster_n_trees(bb_booster const *b, uint32_t *n)
+    {
+        *n = b->n_trees;
+        return BB_OK;
+    }
+
+    float bb_booster_init_score(bb_booster const *b)
+    {
+        return b->init;
+    }
+
+    uint32_t bb_booster_tree_capacity(bb_booster const *b)
+    {
+        return b->trees.cap;
+    }
+
+    int bb_booster_tree(bb_booster const *b, uint32_t t, uint32_t *feature, float *value,
+                        uint32_t *left, uint32_t *right, uint8_t *default_left, float *gain,
+                        float *cover, uint32_t *split_bin, uint32_t *meta)
+    {
+        return guarded(
+            [&]
+            {
+                need(t < b->n_trees, "bb_booster_tree: tree index out of range");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                b->trees.download(t, feature, value, left, right, default_left, gain, cover,
+                                  split_bin, meta);
+            });
+    }
+
+    int bb_booster_scores(bb_booster const *b, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                BB_CHECK(cudaMemcpy(out, b->scores, b->plane->n_rows * 4, cudaMemcpyDeviceToHost));
+            });
+    }
+
+    int bb_booster_leaf_ids(bb_booster const *b, uint32_t *out)
+    {
+        return guarded(
+            [&]
+            {
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                BB_CHECK(cudaMemcpy(out, b->leaf_id, b->plane->n_rows * 4, cudaMemcpyDeviceToHost));
+            });
+    }
+
+    void bb_booster_destroy(bb_booster *b)
+    {
+        if (b == nullptr)
+        {
+            return;
+        }
+        cudaStreamSynchronize(b->stream);
+        if (b->graph != nullptr)
+        {
+            cudaGraphExecDestroy(b->graph);
+        }
+        b->grower.reset();
+        b->scratch.release();
+        b->trees.release();
+        void *ps[] = {b->labels, b->scores, b->gh, b->rows, b->leaf_id, b->round};
+        for (void *p : ps)
+        {
+            cudaFree(p);
+        }
+        cudaEventDestroy(b->ev0);
+        cudaEventDestroy(b->ev1);
+        cudaStreamDestroy(b->stream);
+        delete b;
+    }
+
+    int bb_grow_tree(bb_plane const *plane, bb_train_cfg const *cfg, float const *grad,
+                     float const *hess, uint32_t const *rows, uint64_t n_sel_rows,
+                     uint32_t *feature, float *value, uint32_t *left, uint32_t *right,
+                     uint8_t *default_left, float *gain, float *cover, uint32_t *split_bin,
+                     uint32_t *meta, float *values, uint32_t *leaf_ids)
+    {
+        return guarded(
+            [&]
+            {
+                need(plane != nullptr && cfg != nullptr && grad != nullptr && hess != nullptr,
+                     "bb_grow_tree: null argument");
+                if (cfg->hist_mode != 0)
+                {
+                    throw ConfigError("quantised histograms are not built in this library");
+                }
+                Plane const   &p = plane->p;
+                uint64_t const n = p.n_rows;
+                uint64_t const m = rows == nullptr ? n : n_sel_rows;
+                need(m <= n, "bb_grow_tree: more sampled rows than rows");
+                for (uint64_t k = 0; rows != nullptr && k < m; ++k)
+                {
+                    need(rows[k] < n && (k == 0 || rows[k] > rows[k - 1]),
+                         "bb_grow_tree: rows must be ascending row ids below n_rows");
+                }
+                cudaStream_t   s;
+                BB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                std::vector<float2> gh(n);
+                for (uint64_t i = 0; i < n; ++i)
+                {
+                    gh[i] = make_float2(grad[i], hess[i]);
+                }
+                float2   *d_gh  = dmalloc<float2>(n);
+                uint32_t *d_rows = dmalloc<uint32_t>(std::max<uint64_t>(m, 1));
+                uint32_t *d_leaf = dmalloc<uint32_t>(n);
+                float    *d_val  = dmalloc<float>(n);
+                TreeStore ts;
+                try
+                {
+                    BB_CHECK(cudaMemcpyAsync(d_gh, gh.data(), n * 8, cudaMemcpyHostToDevice, s));
+                    if (rows == nullptr)
+                    {
+                        iota_kernel<<<blocks(n), 256, 0, s>>>(d_rows, n);
+                        BB_LAUNCH("iota_kernel");
+                    }
+                    else if (m > 0)
+                    {
+                        BB_CHECK(cudaMemcpyAsync(d_rows, rows, m * 4, cudaMemcpyHostToDevice, s));
+                    }
+                    // values via the fused score update on a zeroed buffer, lr = 1
+                    BB_CHECK(cudaMemsetAsync(d_val, 0, n * 4, s));
+                    Grower g(p, grow_config(*cfg), selection(*cfg, p.n_feats),
+                             static_cast<uint32_t>(std::max<uint64_t>(m, 1)), s);
+                    g.set_monotone(monotone(*cfg));
+                    ts.alloc(g.max_nodes(), 1);
+                    g.grow(d_gh, d_rows, static_cast<uint32_t>(m), ts.t, d_leaf, d_val, 1.0F);
+                    BB_CHECK(cudaStreamSynchronize(s));
+                    ts.download(0, feature, value, left, right, default_left, gain, cover,
+                                split_bin, meta);
+                    std::vector<float>    v(n);
+                    std::vector<uint32_t> ids(n);
+                    BB_CHECK(cudaMemcpy(v.data(), d_val, n * 4, cudaMemcpyDeviceToHost));
+                    BB_CHECK(cudaMemcpy(ids.data(), d_leaf, n * 4, cudaMemcpyDeviceToHost));
+                    for (uint64_t k = 0; k < m; ++k)
+                    {
+                        uint64_t const r = rows == nullptr ? k : rows[k];
+                        values[r]        = v[r];
+                        leaf_ids[r]      = ids[r];
+                    }
+                }
+                catch (...)
+                {
+                    ts.release();
+                    cudaFree(d_gh);
+                    cudaFree(d_rows);
+                    cudaFree(d_leaf);
+                    cudaFree(d_val);
+                    cudaStreamDestroy(s);
+                    throw;
+                }
+                ts.release();
+                cudaFree(d_gh);
+                cudaFree(d_rows);
+                cudaFree(d_leaf);
+                cudaFree(d_val);
+                BB_CHECK(cudaStreamDestroy(s));
+            });
+    }
+
+    int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+                   uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
+                   uint32_t const *left, uint32_t const *right, uint8_t const *default_left,
+                   float const *value, float lr, float init, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                Plane const   &p = plane->p;
+                uint64_t const n = p.n_rows;
+                std::vector<uint32_t> last(p.n_feats);
+                for (uint32_t f = 0; f < p.n_feats; ++f)
+                {
+                    last[f] = p.h_cut_off[f + 1] - p.h_cut_off[f] - 1;
+                }
+                // every walk must end: children lie after their parent inside
+                // the tree, and split features exist
+                for (uint32_t t = 0; t < n_trees; ++t)
+                {
+                    uint32_t const b = roots[t];
+                    uint32_t const e = t + 1 < n_trees ? roots[t + 1] : n_nodes;
+                    need(b < e && e <= n_nodes, "bb_predict: bad tree roots");
+                    for (uint32_t i = b; i < e; ++i)
+                    {
+                        if (feature[i] == k_leaf_flag)
+                        {
+                            continue;
+                        }
+                        need(feature[i] < p.n_feats, "bb_predict: node feature out of range");
+                        need(left[i] > i - b && right[i] > i - b && b + left[i] < e &&
+                                 b + right[i] < e,
+                             "bb_predict: a child id must follow its parent in its tree");
+                    }
+                }
+                uint32_t *d_last  = dmalloc<uint32_t>(p.n_feats);
+                uint32_t *d_roots = dmalloc<uint32_t>(n_trees);
+                uint32_t *d_feat  = dmalloc<uint32_t>(n_nodes);
+                uint32_t *d_sb    = dmalloc<uint32_t>(n_nodes);
+                uint32_t *d_l     = dmalloc<uint32_t>(n_nodes);
+                uint32_t *d_r     = dmalloc<uint32_t>(n_nodes);
+                uint8_t  *d_dl    = dmalloc<uint8_t>(n_nodes);
+                float    *d_v     = dmalloc<float>(n_nodes);
+                float    *d_out   = dmalloc<float>(n);
+                BB_CHECK(cudaMemcpy(d_last, last.data(), p.n_feats * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_roots, roots, n_trees * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_feat, feature, n_nodes * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_sb, split_bin, n_nodes * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_l, left, n_nodes * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_r, right, n_nodes * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_dl, default_left, n_nodes, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(d_v, value, n_nodes * 4, cudaMemcpyHostToDevice));
+                if (p.u8)
+                {
+                    predict_kernel<uint8_t><<<blocks(n), 256>>>(
+                        static_cast<uint8_t const *>(p.bins), p.n_pad, n, d_last, n_trees,
+                        d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, lr, init, d_out);
+                }
+                else
+                {
+                    predict_kernel<uint16_t><<<blocks(n), 256>>>(
+                        static_cast<uint16_t const *>(p.bins), p.n_pad, n, d_last, n_trees,
+                        d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, lr, init, d_out);
+                }
+                BB_LAUNCH("predict_kernel");
+                BB_CHECK(cudaMemcpy(out, d_out, n * 4, cudaMemcpyDeviceToHost));
+                void *ps[] = {d_last, d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, d_out};
+                for (void *q : ps)
+                {
+                    cudaFree(q);
+                }
+            });
+    }
+}

@@ -1,0 +1,102 @@
+// Shared device/host definitions for the B200 growers.
+//
+// Everything here compiles with -fmad=false: the plain form promises results
+// bit-identical to the reference's CPU grower, which is built with
+// -ffp-contract=off, so no multiply-add may fuse anywhere in this library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace bb
+{
+
+constexpr uint32_t k_leaf_flag = 0xFFFFFFFFu;
+
+// The error the C ABI reports: "cuda: <what>: <cudaGetErrorString>", the
+// reference's check() text (src/cuda/detail/device_buffer.cuh:96-103).
+struct CudaError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+// A capacity or configuration refusal (the reference's ConfigError).
+struct ConfigError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+inline void check(cudaError_t e, char const *what)
+{
+    if (e != cudaSuccess)
+    {
+        throw CudaError(std::string("cuda: ") + what + ": " + cudaGetErrorString(e));
+    }
+}
+
+#define BB_CHECK(call) ::bb::check((call), #call)
+#define BB_LAUNCH(what) ::bb::check(cudaGetLastError(), what)
+
+// ---- split math, restated from include/bonsai/split.hpp:112-158 ----------
+// Double precision, IEEE round-to-nearest, no contraction (-fmad=false).
+
+__host__ __device__ inline double l1_thresholded(double g, double l1)
+{
+    if (g > l1)
+    {
+        return g - l1;
+    }
+    if (g < -l1)
+    {
+        return g + l1;
+    }
+    return 0.0;
+}
+
+__host__ __device__ inline double split_score(double g, double h, double l1, double l2)
+{
+    double const t = l1_thresholded(g, l1);
+    double const d = h + l2;
+    return d > 0.0 ? (t * t) / d : 0.0;
+}
+
+__host__ __device__ inline double bounded_leaf_weight(double g, double h, double l1,
+                                                      double l2, double lo, double hi)
+{
+    double const d = h + l2;
+    double const w = d > 0.0 ? -l1_thresholded(g, l1) / d : 0.0;
+    return w < lo ? lo : (hi < w ? hi : w);
+}
+
+// routes_left (include/bonsai/dataset.hpp:234-238): the last bin holds
+// missing values and follows default_left; otherwise bin <= split_bin.
+__host__ __device__ inline bool routes_left(uint32_t b, uint32_t last, uint32_t split,
+                                            bool dl)
+{
+    return b == last ? dl : b <= split;
+}
+
+// Tree-level knobs the device reads (TreeConfig, include/bonsai/config/
+// tree_config.hpp:9-29). Floats stay float: the reference widens them to
+// double at each use, and so does every kernel here.
+struct TreeParams
+{
+    float    min_child_hess;
+    float    min_gain_to_split;
+    float    lambda_l2;
+    float    lambda_l1;
+    uint32_t max_depth;
+    uint32_t min_data_in_leaf;
+    uint32_t max_leaves;
+};
+
+inline uint32_t ceil_div(uint64_t a, uint64_t b)
+{
+    return static_cast<uint32_t>((a + b - 1) / b);
+}
+
+} // namespace bb

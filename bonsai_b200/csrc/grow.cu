@@ -1,0 +1,1376 @@
+// Level kernels and the device-resident tree loop. See grow.cuh.
+//
+// Reference behaviour each kernel restates (paths within the project):
+//   find_kernel + plan_kernel    HistogramNodeSplitFinder::find
+//                                (src/split.cpp:101-162,271-297) and
+//                                plan_level (src/grower_impl.hpp:212-255)
+//   pcount/plan2/pscatter        host_partition (src/step/primitives.hpp:
+//                                262-374), demote_empty_splits
+//                                (src/grower_impl.hpp:262-298),
+//                                commit_children (:303-326)
+//   count/offsets/scatter/chain  the column fill's serial cell order
+//                                (src/fill/columns.hpp:31-89)
+//   subtract_totals_kernel       finish_split (src/step/primitives.hpp:
+//                                156-173), Histogram::totals
+//                                (include/bonsai/histogram.hpp:84-95),
+//                                propagate_monotone_bounds
+//                                (src/grower_impl.hpp:52-80)
+//   stamp/final kernels          finalize_as_leaf / write_leaf
+//                                (src/step/primitives.hpp:42-69)
+#include "grow.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace bb
+{
+namespace
+{
+
+constexpr uint32_t k_threads    = 256;
+constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
+constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk
+constexpr uint32_t k_warps_feat = 8;    // features per count/scatter CTA
+constexpr uint32_t k_find_warps = 4;    // features per find CTA
+constexpr uint32_t k_chain_stg  = 32;   // elements per lane per cp.async stage
+constexpr uint32_t k_chain_nst  = 4;    // cp.async stages per lane
+constexpr uint32_t k_max_bins   = 4096; // per feature, this engine's ceiling
+constexpr uint32_t k_plan_thr   = 512;  // plan kernels: one thread per node
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <typename BinT>
+__device__ __forceinline__ uint32_t bin_at(void const *bins, uint64_t n_pad, uint32_t f,
+                                           uint32_t r)
+{
+    return static_cast<BinT const *>(bins)[(static_cast<uint64_t>(f) * n_pad) + r];
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim <= 1024).
+template <uint32_t NT>
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total)
+{
+    __shared__ uint32_t warp_sums[NT / 32];
+    uint32_t const      lane = threadIdx.x & 31;
+    uint32_t const      w    = threadIdx.x >> 5;
+    uint32_t            x    = v;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1)
+    {
+        uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o)
+        {
+            x += y;
+        }
+    }
+    if (lane == 31)
+    {
+        warp_sums[w] = x;
+    }
+    __syncthreads();
+    if (w == 0)
+    {
+        uint32_t s = lane < NT / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1)
+        {
+            uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o)
+            {
+                s += y;
+            }
+        }
+        if (lane < NT / 32)
+        {
+            warp_sums[lane] = s;
+        }
+    }
+    __syncthreads();
+    uint32_t const before = w > 0 ? warp_sums[w - 1] : 0;
+    if (total != nullptr)
+    {
+        *total = warp_sums[NT / 32 - 1];
+    }
+    __syncthreads();
+    return before + x - v;
+}
+
+__device__ __forceinline__ void write_leaf_node(TreeOut const &t, uint32_t id, float v)
+{
+    t.feature[id]      = k_leaf_flag;
+    t.value[id]        = v;
+    t.left[id]         = 0;
+    t.right[id]        = 0;
+    t.default_left[id] = 0;
+    t.split_bin[id]    = 0;
+}
+
+__device__ __forceinline__ float leaf_value(Node const &nd, TreeParams const &tp)
+{
+    return static_cast<float>(bounded_leaf_weight(nd.sum_g, nd.sum_h, tp.lambda_l1,
+                                                  tp.lambda_l2, nd.lo, nd.hi));
+}
+
+// ---------------------------------------------------------------- root ----
+
+__global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk *bchunks,
+                                  uint32_t *brange, uint32_t *build, TreeOut t)
+{
+    uint32_t const nch = (n_root + k_build_rows - 1) / k_build_rows;
+    if (threadIdx.x == 0)
+    {
+        Ctl c{};
+        c.n_cur      = 1;
+        c.n_nodes    = 1;
+        c.n_build    = 1;
+        c.n_bchunks  = nch;
+        c.built_rows = n_root;
+        *ctl         = c;
+        Node nd{};
+        nd.start  = 0;
+        nd.count  = n_root;
+        nd.id     = 0;
+        nd.lo     = -INFINITY;
+        nd.hi     = INFINITY;
+        nodes[0]  = nd;
+        build[0]  = 0;
+        brange[0] = 0;
+        brange[1] = nch;
+        write_leaf_node(t, 0, 0.0F);
+        t.gain[0]  = 0.0F;
+        t.cover[0] = static_cast<float>(n_root);
+    }
+    for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x)
+    {
+        uint32_t const b = c * k_build_rows;
+        bchunks[c]       = {0, b, min(k_build_rows, n_root - b), 0};
+    }
+}
+
+// Node totals from the first selected feature's cells: double sums over
+// every cell in bin order, rounded to float once (Histogram::totals).
+__device__ __forceinline__ void totals_from_cells(float2 const *cells, uint32_t nb,
+                                                  float &g, float &h)
+{
+    double sg = 0.0;
+    double sh = 0.0;
+    for (uint32_t b = 0; b < nb; ++b)
+    {
+        float2 const c = cells[b];
+        sg += c.x;
+        sh += c.y;
+    }
+    g = static_cast<float>(sg);
+    h = static_cast<float>(sh);
+}
+
+__global__ void root_totals_kernel(Node *nodes, float2 const *hist, uint32_t const *sel_nb)
+{
+    if (threadIdx.x == 0)
+    {
+        totals_from_cells(hist, sel_nb[0], nodes[0].sum_g, nodes[0].sum_h);
+    }
+}
+
+// ------------------------------------------------------- histogram build ----
+// The plain form's cells must equal the CPU fill's serial float chains, so
+// each built node's rows are stably counting-sorted by bin per feature
+// (count -> offsets -> scatter), after which every cell's (g, h) values sit
+// contiguous in the node's row order and one lane folds each cell.
+
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    count_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *rows,
+                 void const *bins, uint64_t n_pad, uint32_t const *sel,
+                 uint32_t const *sel_nb, uint32_t nfb, uint32_t *ccount, uint32_t cs)
+{
+    extern __shared__ uint32_t cnt_s[]; // [k_warps_feat][cs]
+    uint32_t const             c = blockIdx.x;
+    if (c >= ctl->n_bchunks)
+    {
+        return;
+    }
+    Chunk const    ch   = bchunks[c];
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t const j    = (blockIdx.y * k_warps_feat) + w;
+    if (j >= nfb)
+    {
+        return;
+    }
+    uint32_t const f   = sel[j];
+    uint32_t const nb  = sel_nb[j];
+    uint32_t      *cnt = cnt_s + (w * cs);
+    for (uint32_t b = lane; b < nb; b += 32)
+    {
+        cnt[b] = 0;
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < ch.count; k += 32)
+    {
+        uint32_t const r = rows[ch.begin + k];
+        atomicAdd(&cnt[bin_at<BinT>(bins, n_pad, f, r)], 1U);
+    }
+    __syncwarp();
+    uint32_t *out = ccount + ((static_cast<uint64_t>(c) * nfb + j) * cs);
+    for (uint32_t b = lane; b < nb; b += 32)
+    {
+        out[b] = cnt[b];
+    }
+}
+
+// Per (built node, feature): bin totals over the node's chunks, their
+// exclusive scan (the bin segments of the node's sorted payload), and each
+// chunk's per-bin write base, in place of its counts.
+__global__ void __launch_bounds__(k_threads)
+    offsets_kernel(Ctl const *ctl, uint32_t const *brange, uint32_t *ccount,
+                   uint32_t *seg, uint32_t const *sel_nb, uint32_t nfb, uint32_t cs,
+                   Chunk const *bchunks)
+{
+    __shared__ uint32_t tot_s[k_max_bins];
+    __shared__ uint32_t carry_s;
+    uint32_t const      i = blockIdx.x;
+    if (i >= ctl->n_build)
+    {
+        return;
+    }
+    uint32_t const j  = blockIdx.y;
+    uint32_t const nb = sel_nb[j];
+    uint32_t const c0 = brange[i];
+    uint32_t const c1 = brange[i + 1];
+    for (uint32_t b = threadIdx.x; b < nb; b += k_threads)
+    {
+        uint32_t s = 0;
+        for (uint32_t c = c0; c < c1; ++c)
+        {
+            s += ccount[((static_cast<uint64_t>(c) * nfb + j) * cs) + b];
+        }
+        tot_s[b] = s;
+    }
+    if (threadIdx.x == 0)
+    {
+        carry_s = 0;
+    }
+    __syncthreads();
+    // exclusive scan over bins, 256 at a time
+    for (uint32_t b0 = 0; b0 < nb; b0 += k_threads)
+    {
+        uint32_t const b     = b0 + threadIdx.x;
+        uint32_t const v     = b < nb ? tot_s[b] : 0;
+        uint32_t       total = 0;
+        uint32_t const ex    = block_excl_scan<k_threads>(v, &total);
+        uint32_t const carry = carry_s;
+        if (b < nb)
+        {
+            tot_s[b] = carry + ex;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            carry_s = carry + total;
+        }
+        __syncthreads();
+    }
+    uint32_t *sg = seg + ((static_cast<uint64_t>(i) * nfb + j) * cs);
+    for (uint32_t b = threadIdx.x; b < nb; b += k_threads)
+    {
+        uint32_t run = tot_s[b];
+        sg[b]        = run;
+        for (uint32_t c = c0; c < c1; ++c)
+        {
+            uint32_t *p = ccount + ((static_cast<uint64_t>(c) * nfb + j) * cs) + b;
+            uint32_t  v = *p;
+            *p          = run;
+            run += v;
+        }
+    }
+    if (threadIdx.x == 0)
+    {
+        sg[nb] = carry_s;
+    }
+    (void)bchunks;
+}
+
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    scatter_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *rows,
+                   void const *bins, uint64_t n_pad, float2 const *gh,
+                   uint32_t const *sel, uint32_t const *sel_nb, uint32_t nfb,
+                   uint32_t const *ccount, uint32_t cs, float2 *payload,
+                   uint64_t p_stride)
+{
+    extern __shared__ unsigned char smem_raw[];
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_bchunks)
+    {
+        return;
+    }
+    Chunk const ch     = bchunks[c];
+    auto       *rows_s = reinterpret_cast<uint32_t *>(smem_raw);
+    auto       *gh_s   = reinterpret_cast<float2 *>(rows_s + k_build_rows);
+    auto       *base_s = reinterpret_cast<uint32_t *>(gh_s + k_build_rows);
+    auto       *bins_s = reinterpret_cast<BinT *>(base_s + (k_warps_feat * cs));
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        uint32_t const r = rows[ch.begin + k];
+        rows_s[k]        = r;
+        gh_s[k]          = gh[r];
+    }
+    __syncthreads();
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t const j    = (blockIdx.y * k_warps_feat) + w;
+    if (j >= nfb)
+    {
+        return;
+    }
+    uint32_t const  f    = sel[j];
+    uint32_t const  nb   = sel_nb[j];
+    uint32_t       *base = base_s + (w * cs);
+    BinT           *bw   = bins_s + (w * k_build_rows);
+    uint32_t const *off  = ccount + ((static_cast<uint64_t>(c) * nfb + j) * cs);
+    for (uint32_t b = lane; b < nb; b += 32)
+    {
+        base[b] = off[b];
+    }
+    for (uint32_t k = lane; k < ch.count; k += 32)
+    {
+        bw[k] = static_cast<BinT>(bin_at<BinT>(bins, n_pad, f, rows_s[k]));
+    }
+    __syncwarp();
+    float2 *out = payload + (static_cast<uint64_t>(j) * p_stride) + ch.aux;
+    for (uint32_t k0 = 0; k0 < ch.count; k0 += 32)
+    {
+        uint32_t const k     = k0 + lane;
+        bool const     valid = k < ch.count;
+        uint32_t const b     = valid ? static_cast<uint32_t>(bw[k]) : 0xFFFFFFFFu;
+        uint32_t const peers = __match_any_sync(0xFFFFFFFFu, b);
+        uint32_t       pos   = 0;
+        if (valid)
+        {
+            pos      = base[b] + __popc(peers & lanemask_lt());
+            out[pos] = gh_s[k];
+        }
+        __syncwarp();
+        if (valid && (peers & lanemask_lt()) == 0)
+        {
+            base[b] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ void cp_async8(void *smem_dst, void const *gsrc)
+{
+    uint32_t const s = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// One lane per cell: the serial float chain over the cell's contiguous
+// (g, h) run, streamed through a per-lane cp.async ring in shared memory so
+// that many bytes are in flight even when few cells exist (the root).
+// grid (build nodes, features, ceil(max_bins / 32)), one warp per CTA.
+__global__ void __launch_bounds__(32)
+    chain_kernel(Ctl const *ctl, uint32_t const *build, Chunk const *bchunks,
+                 uint32_t const *brange, uint32_t const *seg, float2 const *payload,
+                 uint64_t p_stride, uint32_t const *sel_nb, uint32_t const *cell_off,
+                 uint32_t nfb, uint32_t cs, float2 *hist, uint32_t total_cells)
+{
+    extern __shared__ float2 ring_s[];
+    uint32_t const i = blockIdx.x;
+    if (i >= ctl->n_build)
+    {
+        return;
+    }
+    uint32_t const j    = blockIdx.y;
+    uint32_t const nb   = sel_nb[j];
+    uint32_t const lane = threadIdx.x;
+    uint32_t const b    = (blockIdx.z * 32) + lane;
+    if (blockIdx.z * 32 >= nb)
+    {
+        return;
+    }
+    uint32_t const  slot  = build[i];
+    uint32_t const  nbase = bchunks[brange[i]].aux;
+    uint32_t const *sg    = seg + ((static_cast<uint64_t>(i) * nfb + j) * cs);
+    uint32_t        s0    = 0;
+    uint32_t        s1    = 0;
+    if (b < nb)
+    {
+        s0 = sg[b];
+        s1 = sg[b + 1];
+    }
+    float2 const *src  = payload + (static_cast<uint64_t>(j) * p_stride) + nbase;
+    float2       *ring = ring_s + (lane * k_chain_stg * k_chain_nst);
+    uint32_t      next = s0;
+    auto          issue = [&](uint32_t st)
+    {
+        float2 *dst = ring + (st * k_chain_stg);
+#pragma unroll 8
+        for (uint32_t e = 0; e < k_chain_stg; ++e)
+        {
+            if (next + e < s1)
+            {
+                cp_async8(dst + e, src + next + e);
+            }
+        }
+        next = min(s1, next + k_chain_stg);
+        cp_async_commit();
+    };
+#pragma unroll
+    for (uint32_t st = 0; st < k_chain_nst - 1; ++st)
+    {
+        issue(st);
+    }
+    float    g  = 0.0F;
+    float    h  = 0.0F;
+    uint32_t st = 0;
+    for (uint32_t s = s0; s < s1;)
+    {
+        issue((st + k_chain_nst - 1) % k_chain_nst);
+        cp_async_wait<k_chain_nst - 1>();
+        float2 const  *v = ring + (st * k_chain_stg);
+        uint32_t const n = min(k_chain_stg, s1 - s);
+        for (uint32_t e = 0; e < n; ++e)
+        {
+            float2 const x = v[e];
+            g += x.x;
+            h += x.y;
+        }
+        s += n;
+        st = (st + 1) % k_chain_nst;
+    }
+    cp_async_wait<0>();
+    if (b < nb)
+    {
+        hist[(static_cast<uint64_t>(slot) * total_cells) + cell_off[j] + b] =
+            make_float2(g, h);
+    }
+}
+
+// ------------------------------------------------------------ split find ----
+
+// The per-candidate core of update_best_for_feature_for_node
+// (src/split.cpp:55-82,101-162) for one (bin, default_left).
+__device__ __forceinline__ bool candidate_gain(double lg, double lh, float mg, float mh,
+                                               double real_g, double real_h, bool dl,
+                                               double node_score, TreeParams const &tp,
+                                               int mc, double lo, double hi,
+                                               double &gain)
+{
+    double const rg = real_g - lg;
+    double const rh = real_h - lh;
+    double const gL = lg + (dl ? static_cast<double>(mg) : 0.0);
+    double const hL = lh + (dl ? static_cast<double>(mh) : 0.0);
+    double const gR = rg + (!dl ? static_cast<double>(mg) : 0.0);
+    double const hR = rh + (!dl ? static_cast<double>(mh) : 0.0);
+    double const mch = tp.min_child_hess;
+    if (hL < mch || hR < mch)
+    {
+        return false;
+    }
+    double const l1       = tp.lambda_l1;
+    double const l2       = tp.lambda_l2;
+    double const children = split_score(gL, hL, l1, l2) + split_score(gR, hR, l1, l2);
+    if (mc != 0)
+    {
+        double const wl = bounded_leaf_weight(gL, hL, l1, l2, lo, hi);
+        double const wr = bounded_leaf_weight(gR, hR, l1, l2, lo, hi);
+        if (static_cast<double>(mc) * (wr - wl) < 0.0)
+        {
+            return false;
+        }
+    }
+    gain = children - node_score;
+    return true;
+}
+
+// Warp reduce of (gain, order): the larger gain, the earlier scan order on a
+// tie, so the winner is the serial scan's strict-> first maximum.
+__device__ __forceinline__ void warp_best(double &gain, uint32_t &order)
+{
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        double const   g2 = __shfl_xor_sync(0xFFFFFFFFu, gain, o);
+        uint32_t const o2 = __shfl_xor_sync(0xFFFFFFFFu, order, o);
+        if (g2 > gain || (g2 == gain && o2 < order))
+        {
+            gain  = g2;
+            order = o2;
+        }
+    }
+}
+
+// grid (frontier, ceil(n_sel / 4)), 4 warps: one warp per (node, feature).
+__global__ void __launch_bounds__(32 * k_find_warps)
+    find_kernel(Ctl const *ctl, Node const *nodes, float2 const *hist,
+                uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
+                uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
+                TreeParams tp, Best *cand, uint32_t max_nb)
+{
+    extern __shared__ unsigned char smem_raw[];
+    uint32_t const i = blockIdx.x;
+    if (i >= ctl->n_cur)
+    {
+        return;
+    }
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t const j    = (blockIdx.y * k_find_warps) + w;
+    if (j >= n_sel)
+    {
+        return;
+    }
+    auto *pref = reinterpret_cast<double2 *>(smem_raw) + (w * max_nb);
+    auto *cell = reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(smem_raw) +
+                                            (k_find_warps * max_nb)) +
+                 (w * max_nb);
+    Node const     nd  = nodes[i];
+    uint32_t const nb  = sel_nb[j];
+    Best           out = {0.0, j, 0, 1, 0};
+    if (nd.count < 2 * tp.min_data_in_leaf || nb < 2)
+    {
+        if (lane == 0)
+        {
+            cand[(i * n_sel) + j] = out;
+        }
+        return;
+    }
+    float2 const *src = hist + (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
+    for (uint32_t b = lane; b < nb; b += 32)
+    {
+        cell[b] = src[b];
+    }
+    __syncwarp();
+    uint32_t const n_cut = nb - 2;
+    if (lane == 0)
+    {
+        double lg = 0.0;
+        double lh = 0.0;
+        for (uint32_t b = 0; b < n_cut; ++b)
+        {
+            lg += cell[b].x;
+            lh += cell[b].y;
+            pref[b] = make_double2(lg, lh);
+        }
+    }
+    __syncwarp();
+    float const  mg      = cell[nb - 1].x;
+    float const  mh      = cell[nb - 1].y;
+    double const l1      = tp.lambda_l1;
+    double const l2      = tp.lambda_l2;
+    double const node_sc = split_score(nd.sum_g, nd.sum_h, l1, l2);
+    // float fields subtract in float, then widen (src/split.cpp:117-118)
+    double const real_g  = static_cast<double>(nd.sum_g - mg);
+    double const real_h  = static_cast<double>(nd.sum_h - mh);
+    uint32_t const f     = sel[j];
+    int const      mc    = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+    uint32_t const n_dir = (mg == 0.0F && mh == 0.0F) ? 1 : 2;
+    double         best  = 0.0;
+    uint32_t       order = 0xFFFFFFFFu;
+    double const   min_gain = tp.min_gain_to_split;
+    for (uint32_t b = lane; b < n_cut; b += 32)
+    {
+        double2 const p = pref[b];
+        for (uint32_t d = 0; d < n_dir; ++d)
+        {
+            double gain = 0.0;
+            if (candidate_gain(p.x, p.y, mg, mh, real_g, real_h, d == 0, node_sc, tp, mc,
+                               nd.lo, nd.hi, gain) &&
+                gain > best && gain >= min_gain)
+            {
+                best  = gain;
+                order = (b * 2) + d;
+            }
+        }
+    }
+    warp_best(best, order);
+    if (lane == 0)
+    {
+        if (order != 0xFFFFFFFFu)
+        {
+            out.gain  = best;
+            out.bin   = order >> 1;
+            out.dl    = (order & 1) == 0 ? 1 : 0;
+            out.valid = 1;
+        }
+        cand[(i * n_sel) + j] = out;
+    }
+}
+
+// ------------------------------------------------------------- planning ----
+
+__global__ void __launch_bounds__(k_plan_thr)
+    plan_kernel(Ctl *ctl, Node *nodes, Best const *cand, Best *best, uint32_t n_sel,
+                uint32_t const *sel, float const *cuts, uint32_t const *cut_off,
+                TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr)
+{
+    uint32_t const n_cur = ctl->n_cur;
+    uint32_t const lane  = threadIdx.x & 31;
+    uint32_t const w     = threadIdx.x >> 5;
+    // per node: the first feature (ascending) holding the largest gain
+    for (uint32_t i = w; i < n_cur; i += k_plan_thr / 32)
+    {
+        double   g = 0.0;
+        uint32_t o = 0xFFFFFFFFu;
+        for (uint32_t j = lane; j < n_sel; j += 32)
+        {
+            Best const c = cand[(i * n_sel) + j];
+            if (c.valid != 0 && (c.gain > g || (c.gain == g && j < o)))
+            {
+                g = c.gain;
+                o = j;
+            }
+        }
+        warp_best(g, o);
+        if (lane == 0)
+        {
+            best[i] = o == 0xFFFFFFFFu ? Best{0.0, 0, 0, 1, 0} : cand[(i * n_sel) + o];
+        }
+    }
+    __syncthreads();
+    uint32_t const i     = threadIdx.x;
+    bool const     live  = i < n_cur;
+    Best const     bs    = live ? best[i] : Best{};
+    bool const     split = live && bs.valid != 0;
+    uint32_t       n_split_total = 0;
+    uint32_t const rank  = block_excl_scan<k_plan_thr>(split ? 1 : 0, &n_split_total);
+    uint32_t const n_nodes0 = ctl->n_nodes;
+    Node           nd       = live ? nodes[i] : Node{};
+    if (live)
+    {
+        if (split)
+        {
+            uint32_t const f     = sel[bs.feature];
+            uint32_t const left  = n_nodes0 + (2 * rank);
+            uint32_t const right = left + 1;
+            t.feature[nd.id]      = f;
+            t.value[nd.id]        = cuts[cut_off[f] + bs.bin];
+            t.left[nd.id]         = left;
+            t.right[nd.id]        = right;
+            t.default_left[nd.id] = static_cast<uint8_t>(bs.dl);
+            t.gain[nd.id]         = static_cast<float>(bs.gain);
+            t.split_bin[nd.id]    = bs.bin;
+            write_leaf_node(t, left, 0.0F);
+            write_leaf_node(t, right, 0.0F);
+            t.gain[left]   = 0.0F;
+            t.gain[right]  = 0.0F;
+            t.cover[left]  = 0.0F;
+            t.cover[right] = 0.0F;
+            nd.flags       = 1;
+        }
+        else
+        {
+            write_leaf_node(t, nd.id, leaf_value(nd, tp));
+            nd.flags = 0;
+        }
+        nodes[i] = nd;
+    }
+    // partition chunk table over every frontier node
+    uint32_t const nch    = live ? (nd.count + k_part_rows - 1) / k_part_rows : 0;
+    uint32_t       total  = 0;
+    uint32_t const c0     = block_excl_scan<k_plan_thr>(nch, &total);
+    if (live)
+    {
+        pcr[i] = c0;
+        for (uint32_t c = 0; c < nch; ++c)
+        {
+            uint32_t const b = c * k_part_rows;
+            pchunks[c0 + c]  = {i, nd.start + b, min(k_part_rows, nd.count - b), 0};
+        }
+    }
+    if (i == 0)
+    {
+        pcr[n_cur]      = total;
+        ctl->n_pchunks  = total;
+        ctl->n_nodes    = n_nodes0 + (2 * n_split_total);
+        ctl->n_leaves  += n_cur - n_split_total;
+    }
+}
+
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    pcount_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
+                  Best const *best, uint32_t const *rows, void const *bins,
+                  uint64_t n_pad, uint32_t const *sel, uint32_t const *sel_nb,
+                  uint32_t *pleft)
+{
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_pchunks)
+    {
+        return;
+    }
+    Chunk const ch = pchunks[c];
+    if ((nodes[ch.node].flags & 1) == 0)
+    {
+        return;
+    }
+    Best const     bs   = best[ch.node];
+    uint32_t const f    = sel[bs.feature];
+    uint32_t const last = sel_nb[bs.feature] - 1;
+    uint32_t       n    = 0;
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        uint32_t const b = bin_at<BinT>(bins, n_pad, f, rows[ch.begin + k]);
+        n += routes_left(b, last, bs.bin, bs.dl != 0) ? 1 : 0;
+    }
+    uint32_t total = 0;
+    block_excl_scan<k_threads>(n, &total);
+    if (threadIdx.x == 0)
+    {
+        pleft[c] = total;
+    }
+}
+
+__global__ void __launch_bounds__(k_plan_thr)
+    plan2_kernel(Ctl *ctl, Node *nodes, Node *next, Best const *best,
+                 Chunk const *pchunks, uint32_t const *pcr, uint32_t *pleft,
+                 uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
+                 uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
+                 TreeOut t)
+{
+    uint32_t const n_cur = ctl->n_cur;
+    uint32_t const lane  = threadIdx.x & 31;
+    uint32_t const w     = threadIdx.x >> 5;
+    // per split node: left count and each chunk's left/right write base
+    for (uint32_t i = w; i < n_cur; i += k_plan_thr / 32)
+    {
+        Node const nd = nodes[i];
+        if ((nd.flags & 1) == 0)
+        {
+            continue;
+        }
+        uint32_t const c0  = pcr[i];
+        uint32_t const c1  = pcr[i + 1];
+        uint32_t       run = 0;
+        for (uint32_t cb = c0; cb < c1; cb += 32)
+        {
+            uint32_t const c = cb + lane;
+            uint32_t const v = c < c1 ? pleft[c] : 0;
+            uint32_t       x = v;
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1)
+            {
+                uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= o)
+                {
+                    x += y;
+                }
+            }
+            uint32_t const ex = run + x - v;
+            if (c < c1)
+            {
+                pleft[c]  = ex;
+                prbase[c] = (pchunks[c].begin - nd.start) - ex;
+            }
+            run += __shfl_sync(0xFFFFFFFFu, x, 31);
+        }
+        if (lane == 0)
+        {
+            nleft[i] = run;
+        }
+    }
+    __syncthreads();
+    uint32_t const i    = threadIdx.x;
+    bool const     live = i < n_cur;
+    Node           nd   = live ? nodes[i] : Node{};
+    bool           surv = false;
+    uint32_t       nl   = 0;
+    if (live && (nd.flags & 1) != 0)
+    {
+        nl = nleft[i];
+        if (nl == 0 || nl == nd.count)
+        {
+            // demote_empty_splits: the parent is a leaf after all
+            nd.flags |= 2;
+            write_leaf_node(t, nd.id, leaf_value(nd, tp));
+            t.gain[nd.id] = 0.0F;
+            nodes[i]      = nd;
+        }
+        else
+        {
+            surv = true;
+        }
+    }
+    uint32_t       n_surv = 0;
+    uint32_t const k      = block_excl_scan<k_plan_thr>(surv ? 1 : 0, &n_surv);
+    uint32_t       rows_total = 0;
+    uint32_t const start = block_excl_scan<k_plan_thr>(surv ? nd.count : 0, &rows_total);
+    uint32_t const n_demoted_before = 0;
+    (void)n_demoted_before;
+    uint32_t small_count = 0;
+    if (surv)
+    {
+        dst[i]              = start;
+        uint32_t const nr   = nd.count - nl;
+        uint32_t const lid  = t.left[nd.id];
+        uint32_t const rid  = t.right[nd.id];
+        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi};
+        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi};
+        next[2 * k]         = L;
+        next[(2 * k) + 1]   = R;
+        t.cover[lid]        = static_cast<float>(nl);
+        t.cover[rid]        = static_cast<float>(nr);
+        bool const left_sm  = nl <= nr;
+        bpair[(3 * k) + 0]  = i;
+        bpair[(3 * k) + 1]  = (2 * k) + (left_sm ? 0 : 1);
+        bpair[(3 * k) + 2]  = (2 * k) + (left_sm ? 1 : 0);
+        build[k]            = (2 * k) + (left_sm ? 0 : 1);
+        small_count         = left_sm ? nl : nr;
+    }
+    // histogram-build chunk table over the smaller children
+    uint32_t const nch   = surv ? (small_count + k_build_rows - 1) / k_build_rows : 0;
+    uint32_t       nch_t = 0;
+    uint32_t const c0    = block_excl_scan<k_plan_thr>(nch, &nch_t);
+    uint32_t       built = 0;
+    uint32_t const pbase = block_excl_scan<k_plan_thr>(small_count, &built);
+    if (surv)
+    {
+        uint32_t const sst = (nl <= nd.count - nl) ? start : start + nl;
+        brange[k]          = c0;
+        for (uint32_t c = 0; c < nch; ++c)
+        {
+            uint32_t const b = c * k_build_rows;
+            bchunks[c0 + c]  = {k, sst + b, min(k_build_rows, small_count - b), pbase};
+        }
+    }
+    if (i == 0)
+    {
+        uint32_t n_dem = 0;
+        for (uint32_t x = 0; x < n_cur; ++x)
+        {
+            n_dem += (nodes[x].flags & 2) != 0 ? 1 : 0;
+        }
+        brange[n_surv]  = nch_t;
+        ctl->n_leaves  += n_dem;
+        ctl->n_next     = 2 * n_surv;
+        ctl->n_splits   = n_surv;
+        ctl->n_build    = n_surv;
+        ctl->n_bchunks  = nch_t;
+        ctl->built_rows = built;
+        if (n_surv > 0)
+        {
+            ctl->depth += 1;
+        }
+    }
+}
+
+// Rows of this level's leaves (never split, or demoted): their leaf id and
+// the fused score update scores[r] += lr * value.
+__global__ void __launch_bounds__(k_threads)
+    stamp_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
+                 uint32_t const *rows, TreeOut t, uint32_t *leaf_id, float *scores,
+                 float lr)
+{
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_pchunks)
+    {
+        return;
+    }
+    Chunk const ch = pchunks[c];
+    Node const  nd = nodes[ch.node];
+    if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
+    {
+        return;
+    }
+    float const v = t.value[nd.id];
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        uint32_t const r = rows[ch.begin + k];
+        if (leaf_id != nullptr)
+        {
+            leaf_id[r] = nd.id;
+        }
+        if (scores != nullptr)
+        {
+            scores[r] = scores[r] + (lr * v);
+        }
+    }
+}
+
+// Stable scatter of a split node's chunk: lefts keep their order at
+// dst + left base, rights at dst + n_left + right base.
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    pscatter_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
+                    Best const *best, uint32_t const *pleft, uint32_t const *prbase,
+                    uint32_t const *nleft, uint32_t const *dst, uint32_t const *rows,
+                    uint32_t *rows_out, void const *bins, uint64_t n_pad,
+                    uint32_t const *sel, uint32_t const *sel_nb)
+{
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_pchunks)
+    {
+        return;
+    }
+    Chunk const ch = pchunks[c];
+    Node const  nd = nodes[ch.node];
+    if ((nd.flags & 1) == 0 || (nd.flags & 2) != 0)
+    {
+        return;
+    }
+    Best const     bs   = best[ch.node];
+    uint32_t const f    = sel[bs.feature];
+    uint32_t const last = sel_nb[bs.feature] - 1;
+    uint32_t const d0   = dst[ch.node];
+    uint32_t const nl   = nleft[ch.node];
+    uint32_t       lb   = d0 + pleft[c];
+    uint32_t       rb   = d0 + nl + prbase[c];
+    for (uint32_t k0 = 0; k0 < ch.count; k0 += k_threads)
+    {
+        uint32_t const k     = k0 + threadIdx.x;
+        bool const     valid = k < ch.count;
+        uint32_t       r     = 0;
+        bool           left  = false;
+        if (valid)
+        {
+            r    = rows[ch.begin + k];
+            left = routes_left(bin_at<BinT>(bins, n_pad, f, r), last, bs.bin, bs.dl != 0);
+        }
+        uint32_t       n_l = 0;
+        uint32_t const lr  = block_excl_scan<k_threads>(left ? 1 : 0, &n_l);
+        if (valid)
+        {
+            uint32_t const rr = threadIdx.x - lr;
+            rows_out[left ? lb + lr : rb + rr] = r;
+        }
+        uint32_t const tile = min(k_threads, ch.count - k0);
+        lb += n_l;
+        rb += tile - n_l;
+    }
+}
+
+// Larger child = parent - smaller child, cell by cell in float
+// (finish_split); then both children's totals and monotone bounds.
+__global__ void __launch_bounds__(k_threads)
+    subtract_totals_kernel(Ctl const *ctl, uint32_t const *bpair, float2 const *hist_cur,
+                           float2 *hist_nxt, uint32_t total_cells, uint32_t n_cells,
+                           Node const *cur, Node *next, Best const *best,
+                           uint32_t const *sel, uint32_t const *sel_nb,
+                           int8_t const *mono, uint32_t n_mono, TreeParams tp)
+{
+    uint32_t const k = blockIdx.x;
+    if (k >= ctl->n_splits)
+    {
+        return;
+    }
+    uint32_t const p  = bpair[3 * k];
+    uint32_t const s  = bpair[(3 * k) + 1];
+    uint32_t const l  = bpair[(3 * k) + 2];
+    float2 const  *hp = hist_cur + (static_cast<uint64_t>(p) * total_cells);
+    float2 const  *hs = hist_nxt + (static_cast<uint64_t>(s) * total_cells);
+    float2        *hl = hist_nxt + (static_cast<uint64_t>(l) * total_cells);
+    for (uint32_t x = threadIdx.x; x < n_cells; x += k_threads)
+    {
+        float2 const a = hp[x];
+        float2 const b = hs[x];
+        hl[x]          = make_float2(a.x - b.x, a.y - b.y);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t const nb0 = sel_nb[0];
+        Node           L   = next[2 * k];
+        Node           R   = next[(2 * k) + 1];
+        totals_from_cells(hist_nxt + (static_cast<uint64_t>(2 * k) * total_cells), nb0,
+                          L.sum_g, L.sum_h);
+        totals_from_cells(hist_nxt + (static_cast<uint64_t>((2 * k) + 1) * total_cells),
+                          nb0, R.sum_g, R.sum_h);
+        Node const     par = cur[p];
+        uint32_t const f   = sel[best[p].feature];
+        int const      mc  = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+        if (mc != 0)
+        {
+            double const l1  = tp.lambda_l1;
+            double const l2  = tp.lambda_l2;
+            double const wl  = bounded_leaf_weight(L.sum_g, L.sum_h, l1, l2, par.lo, par.hi);
+            double const wr  = bounded_leaf_weight(R.sum_g, R.sum_h, l1, l2, par.lo, par.hi);
+            double const mid = 0.5 * (wl + wr);
+            if (mc > 0)
+            {
+                L.hi = fmin(L.hi, mid);
+                R.lo = fmax(R.lo, mid);
+            }
+            else
+            {
+                L.lo = fmax(L.lo, mid);
+                R.hi = fmin(R.hi, mid);
+            }
+        }
+        next[2 * k]       = L;
+        next[(2 * k) + 1] = R;
+    }
+}
+
+// The surviving frontier after the last level: leaves (end_tree).
+__global__ void __launch_bounds__(k_plan_thr)
+    final_kernel(Ctl *ctl, Node const *nodes, TreeParams tp, TreeOut t)
+{
+    uint32_t const n = ctl->n_cur;
+    uint32_t const i = threadIdx.x;
+    uint32_t       c = 0;
+    if (i < n)
+    {
+        Node const nd = nodes[i];
+        write_leaf_node(t, nd.id, leaf_value(nd, tp));
+        c = nd.count;
+    }
+    uint32_t total = 0;
+    block_excl_scan<k_plan_thr>(c, &total);
+    if (i == 0)
+    {
+        ctl->n_leaves += n;
+        ctl->built_rows = total;
+        t.meta[0]       = ctl->n_nodes;
+        t.meta[1]       = ctl->depth;
+        t.meta[2]       = ctl->n_leaves;
+    }
+}
+
+__global__ void __launch_bounds__(k_threads)
+    final_stamp_kernel(Ctl const *ctl, Node const *nodes, uint32_t const *rows,
+                       TreeOut t, uint32_t *leaf_id, float *scores, float lr)
+{
+    uint32_t const p = (blockIdx.x * k_threads) + threadIdx.x;
+    if (p >= ctl->built_rows)
+    {
+        return;
+    }
+    uint32_t const n  = ctl->n_cur;
+    uint32_t       lo = 0;
+    uint32_t       hi = n;
+    while (hi - lo > 1)
+    {
+        uint32_t const mid = (lo + hi) >> 1;
+        if (nodes[mid].start <= p)
+        {
+            lo = mid;
+        }
+        else
+        {
+            hi = mid;
+        }
+    }
+    uint32_t const id = nodes[lo].id;
+    uint32_t const r  = rows[p];
+    if (leaf_id != nullptr)
+    {
+        leaf_id[r] = id;
+    }
+    if (scores != nullptr)
+    {
+        scores[r] = scores[r] + (lr * t.value[id]);
+    }
+}
+
+__global__ void advance_kernel(Ctl *ctl)
+{
+    ctl->n_cur = ctl->n_next;
+}
+
+template <typename T> T *dalloc(size_t n, cudaStream_t s)
+{
+    void *p = nullptr;
+    BB_CHECK(cudaMallocAsync(&p, std::max<size_t>(1, n) * sizeof(T), s));
+    return static_cast<T *>(p);
+}
+
+} // namespace
+
+Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> selected,
+               uint32_t max_root_rows, cudaStream_t stream)
+    : plane_(plane), cfg_(cfg), sel_h_(std::move(selected)), stream_(stream)
+{
+    n_sel_ = static_cast<uint32_t>(sel_h_.size());
+    if (n_sel_ == 0)
+    {
+        throw ConfigError("grower: the feature selection is empty");
+    }
+    if (cfg_.tp.max_depth > 8)
+    {
+        throw ConfigError("grower: max_depth above 8 exceeds the level plane's "
+                          "512-node frontier; use a host grower");
+    }
+    std::vector<uint32_t> off(n_sel_ + 1, 0);
+    std::vector<uint32_t> nb(n_sel_, 0);
+    for (uint32_t j = 0; j < n_sel_; ++j)
+    {
+        uint32_t const f = sel_h_[j];
+        nb[j]            = plane_.h_cut_off[f + 1] - plane_.h_cut_off[f];
+        off[j + 1]       = off[j] + nb[j];
+        max_nb_          = std::max(max_nb_, nb[j]);
+    }
+    if (max_nb_ > k_max_bins)
+    {
+        throw ConfigError("grower: a feature has more than 4096 bins; lower "
+                          "bin_mapper.max_bin or use a host grower");
+    }
+    total_cells_ = off[n_sel_];
+    off_h_       = off;
+    cell_stride_ = ((max_nb_ + 1 + 3) / 4) * 4;
+    max_front_   = 1u << cfg_.tp.max_depth;
+    max_nodes_   = (2u << cfg_.tp.max_depth) - 1;
+    max_rows_    = max_root_rows;
+    max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
+    max_bchunks_ = ceil_div(max_rows_, k_build_rows) + max_front_;
+
+    cudaStream_t s = stream_;
+    sel_      = dalloc<uint32_t>(n_sel_, s);
+    cell_off_ = dalloc<uint32_t>(n_sel_ + 1, s);
+    sel_nb_   = dalloc<uint32_t>(n_sel_, s);
+    BB_CHECK(cudaMemcpyAsync(sel_, sel_h_.data(), n_sel_ * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(cell_off_, off.data(), (n_sel_ + 1) * 4,
+                             cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(sel_nb_, nb.data(), n_sel_ * 4, cudaMemcpyHostToDevice, s));
+    ctl_      = dalloc<Ctl>(1, s);
+    nodes_[0] = dalloc<Node>(max_front_, s);
+    nodes_[1] = dalloc<Node>(max_front_, s);
+    hist_[0]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_, s);
+    hist_[1]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_, s);
+    cand_     = dalloc<Best>(static_cast<size_t>(max_front_) * n_sel_, s);
+    best_     = dalloc<Best>(max_front_, s);
+    pchunks_  = dalloc<Chunk>(max_pchunks_, s);
+    pleft_    = dalloc<uint32_t>(max_pchunks_, s);
+    prbase_   = dalloc<uint32_t>(max_pchunks_, s);
+    dst_      = dalloc<uint32_t>(max_front_ + 1, s);
+    build_    = dalloc<uint32_t>(max_front_ * 2 + 2, s);
+    bpair_    = dalloc<uint32_t>(3 * max_front_, s);
+    brange_   = dalloc<uint32_t>(max_front_ + 2, s);
+    bchunks_  = dalloc<Chunk>(max_bchunks_, s);
+    ccount_   = dalloc<uint32_t>(static_cast<size_t>(max_bchunks_) * n_sel_ * cell_stride_, s);
+    seg_      = dalloc<uint32_t>(static_cast<size_t>(max_front_) * n_sel_ * cell_stride_, s);
+    payload_  = dalloc<float2>(static_cast<size_t>(n_sel_) * max_rows_, s);
+    rows_[0]  = dalloc<uint32_t>(max_rows_, s);
+    rows_[1]  = dalloc<uint32_t>(max_rows_, s);
+    scale_    = dalloc<float2>(1, s);
+    BB_CHECK(cudaMemsetAsync(scale_, 0, sizeof(float2), s));
+    pcr_      = dalloc<uint32_t>(max_front_ + 2, s);
+    nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
+    BB_CHECK(cudaStreamSynchronize(s));
+
+    // dynamic shared memory ceilings
+    size_t const cnt_smem  = k_warps_feat * cell_stride_ * sizeof(uint32_t);
+    size_t const bin_bytes = plane_.u8 ? 1 : 2;
+    size_t const sc_smem   = (k_build_rows * (4 + 8)) + cnt_smem +
+                           (k_warps_feat * k_build_rows * bin_bytes);
+    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
+    size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
+    if (sc_smem > 227 * 1024 || find_smem > 227 * 1024)
+    {
+        throw ConfigError("grower: bins per feature exceed the shared-memory budget");
+    }
+    if (plane_.u8)
+    {
+        BB_CHECK(cudaFuncSetAttribute(count_kernel<uint8_t>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(cnt_smem)));
+        BB_CHECK(cudaFuncSetAttribute(scatter_kernel<uint8_t>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sc_smem)));
+    }
+    else
+    {
+        BB_CHECK(cudaFuncSetAttribute(count_kernel<uint16_t>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(cnt_smem)));
+        BB_CHECK(cudaFuncSetAttribute(scatter_kernel<uint16_t>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sc_smem)));
+    }
+    BB_CHECK(cudaFuncSetAttribute(find_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(find_smem)));
+    BB_CHECK(cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(chain_smem)));
+}
+
+Grower::~Grower()
+{
+    void *ptrs[] = {sel_,     cell_off_, sel_nb_,  ctl_,     nodes_[0], nodes_[1],
+                    hist_[0], hist_[1],  cand_,    best_,    pchunks_,  pleft_,
+                    prbase_,  dst_,      build_,   bpair_,   brange_,   bchunks_,
+                    ccount_,  seg_,      payload_, rows_[0], rows_[1],  scale_,
+                    absmax_,  qgh_,     pcr_,     nleft_,   mono_};
+    for (void *p : ptrs)
+    {
+        if (p != nullptr)
+        {
+            cudaFreeAsync(p, stream_);
+        }
+    }
+    cudaStreamSynchronize(stream_);
+}
+
+void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
+{
+    cudaStream_t   s    = stream_;
+    size_t const   bin_bytes = plane_.u8 ? 1 : 2;
+    size_t const   cnt_smem  = k_warps_feat * cell_stride_ * sizeof(uint32_t);
+    size_t const   sc_smem   = (k_build_rows * (4 + 8)) + cnt_smem +
+                           (k_warps_feat * k_build_rows * bin_bytes);
+    dim3 const     gcs(max_bchunks_, ceil_div(nfb, k_warps_feat));
+    if (plane_.u8)
+    {
+        count_kernel<uint8_t><<<gcs, k_threads, cnt_smem, s>>>(
+            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
+            cell_stride_);
+    }
+    else
+    {
+        count_kernel<uint16_t><<<gcs, k_threads, cnt_smem, s>>>(
+            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
+            cell_stride_);
+    }
+    BB_LAUNCH("count_kernel");
+    offsets_kernel<<<dim3(max_front_, nfb), k_threads, 0, s>>>(
+        ctl_, brange_, ccount_, seg_, sel_nb_, nfb, cell_stride_, bchunks_);
+    BB_LAUNCH("offsets_kernel");
+    if (plane_.u8)
+    {
+        scatter_kernel<uint8_t><<<gcs, k_threads, sc_smem, s>>>(
+            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
+            ccount_, cell_stride_, payload_, max_rows_);
+    }
+    else
+    {
+        scatter_kernel<uint16_t><<<gcs, k_threads, sc_smem, s>>>(
+            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
+            ccount_, cell_stride_, payload_, max_rows_);
+    }
+    BB_LAUNCH("scatter_kernel");
+    size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
+    chain_kernel<<<dim3(max_front_, nfb, ceil_div(max_nb_, 32)), 32, chain_smem, s>>>(
+        ctl_, build_, bchunks_, brange_, seg_, payload_, max_rows_, sel_nb_, cell_off_, nfb,
+        cell_stride_, static_cast<float2 *>(hist_[dst]), total_cells_);
+    BB_LAUNCH("chain_kernel");
+}
+
+void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
+                   TreeOut const &t, uint32_t *leaf_id, float *scores, float lr)
+{
+    cudaStream_t s   = stream_;
+    int const    cur = static_cast<int>(L & 1);
+    int const    nxt = cur ^ 1;
+    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
+    find_kernel<<<dim3(max_front_, ceil_div(n_sel_, k_find_warps)), 32 * k_find_warps,
+                  find_smem, s>>>(ctl_, nodes_[cur], static_cast<float2 const *>(hist_[cur]),
+                                  total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_,
+                                  n_mono_, cfg_.tp, cand_, max_nb_);
+    BB_LAUNCH("find_kernel");
+    plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
+                                         plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_,
+                                         pcr_);
+    BB_LAUNCH("plan_kernel");
+    if (plane_.u8)
+    {
+        pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
+            ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
+            sel_nb_, pleft_);
+    }
+    else
+    {
+        pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
+            ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
+            sel_nb_, pleft_);
+    }
+    BB_LAUNCH("pcount_kernel");
+    plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
+                                          pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
+                                          build_, brange_, bchunks_, cfg_.tp, t);
+    BB_LAUNCH("plan2_kernel");
+    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
+                                                    t, leaf_id, scores, lr);
+    BB_LAUNCH("stamp_kernel");
+    if (plane_.u8)
+    {
+        pscatter_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
+            ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in,
+            rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_);
+    }
+    else
+    {
+        pscatter_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
+            ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in,
+            rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_);
+    }
+    BB_LAUNCH("pscatter_kernel");
+    bool const     last = (L + 1) == cfg_.tp.max_depth;
+    uint32_t const nfb  = last ? 1 : n_sel_;
+    build(rows_out, nfb, nxt);
+    uint32_t const n_cells = off_h_[nfb]; // the built features: a selection prefix
+    subtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+        ctl_, bpair_, static_cast<float2 const *>(hist_[cur]), static_cast<float2 *>(hist_[nxt]),
+        total_cells_, n_cells, nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_,
+        cfg_.tp);
+    BB_LAUNCH("subtract_totals_kernel");
+    advance_kernel<<<1, 1, 0, s>>>(ctl_);
+    BB_LAUNCH("advance_kernel");
+}
+
+void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
+                  TreeOut const &t, uint32_t *leaf_id, float *scores, float lr)
+{
+    if (n_root > max_rows_)
+    {
+        throw ConfigError("grower: more sampled rows than the grower was sized for");
+    }
+    cudaStream_t s = stream_;
+    gh_cur_        = gh;
+    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
+                                              build_, t);
+    BB_LAUNCH("root_setup_kernel");
+    build(root_rows, cfg_.tp.max_depth == 0 ? 1 : n_sel_, 0);
+    root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(hist_[0]),
+                                        sel_nb_);
+    BB_LAUNCH("root_totals_kernel");
+    uint32_t const *rows_in = root_rows;
+    for (uint32_t L = 0; L < cfg_.tp.max_depth; ++L)
+    {
+        uint32_t *rows_out = rows_[L & 1];
+        level(L, rows_in, rows_out, t, leaf_id, scores, lr);
+        rows_in = rows_out;
+    }
+    int const fin = static_cast<int>(cfg_.tp.max_depth & 1);
+    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t);
+    BB_LAUNCH("final_kernel");
+    final_stamp_kernel<<<ceil_div(max_rows_, k_threads), k_threads, 0, s>>>(
+        ctl_, nodes_[fin], rows_in, t, leaf_id, scores, lr);
+    BB_LAUNCH("final_stamp_kernel");
+    ++tree_no_;
+}
+
+} // namespace bb
+
+namespace bb
+{
+void Grower::set_monotone(std::vector<int8_t> const &m)
+{
+    if (mono_ != nullptr)
+    {
+        BB_CHECK(cudaFreeAsync(mono_, stream_));
+        mono_ = nullptr;
+    }
+    n_mono_ = static_cast<uint32_t>(m.size());
+    if (m.empty())
+    {
+        return;
+    }
+    BB_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&mono_), m.size(), stream_));
+    BB_CHECK(cudaMemcpyAsync(mono_, m.data(), m.size(), cudaMemcpyHostToDevice, stream_));
+    BB_CHECK(cudaStreamSynchronize(stream_));
+}
+} // namespace bb

@@ -1,0 +1,189 @@
+// Device-resident tree growth: the level plane of the reference's
+// CudaHistogramEngine (include/bonsai/cuda/histogram_engine.hpp:75-284,
+// driven by LevelStep<GPULevelEngine>, src/step/level.hpp:159-366), with the
+// control decisions of DepthwiseGrower::grow (src/grower_impl.hpp:465-577)
+// also taken on the device, so a whole tree is one stream of launches with
+// static shapes (capturable as a CUDA graph) and no host round trip.
+#pragma once
+
+#include "common.cuh"
+#include "ingest.cuh"
+
+#include <vector>
+
+namespace bb
+{
+
+// A frontier node: its row segment in the level's row buffer, its tree node
+// id, the reference's node totals (float, SplitInput::sums) and monotone
+// leaf-value bounds.
+struct Node
+{
+    uint32_t start;
+    uint32_t count;
+    uint32_t id;
+    uint32_t flags; // bit0 split, bit1 demoted
+    float    sum_g;
+    float    sum_h;
+    double   lo;
+    double   hi;
+};
+
+// SplitOutput (include/bonsai/split.hpp:62-69), one per (node, feature)
+// candidate and one per node after the feature reduce.
+struct Best
+{
+    double   gain;
+    uint32_t feature; // index into the selection (j), not the feature id
+    uint32_t bin;
+    uint32_t dl;
+    uint32_t valid;
+};
+
+// A node-aligned run of rows, the unit of partition and histogram work.
+struct Chunk
+{
+    uint32_t node;  // frontier slot (partition) or build index (histogram)
+    uint32_t begin; // first row position in the row buffer
+    uint32_t count;
+    uint32_t aux;
+};
+
+// Per-tree device control block.
+struct Ctl
+{
+    uint32_t n_cur;      // frontier size at the current level
+    uint32_t n_next;     // frontier size the level produced
+    uint32_t n_nodes;    // tree node count
+    uint32_t n_leaves;
+    uint32_t depth;
+    uint32_t n_pchunks;  // partition chunks at the current level
+    uint32_t n_bchunks;  // histogram-build chunks
+    uint32_t n_build;    // nodes whose histograms are built this level
+    uint32_t n_splits;   // surviving splits this level
+    uint32_t built_rows; // rows across the built nodes
+    uint32_t pad[6];
+};
+
+struct TreeOut
+{
+    uint32_t *feature;
+    float    *value;
+    uint32_t *left;
+    uint32_t *right;
+    uint8_t  *default_left;
+    float    *gain;
+    float    *cover;
+    uint32_t *split_bin;
+    uint32_t *meta; // n_nodes, depth, n_leaves
+};
+
+enum class HistMode : int32_t
+{
+    exact = 0,  // serial-order float cells, bit-identical to the CPU grower
+    quant8 = 1, // int8 gradients, exact integer histograms
+    quant16 = 2 // int16 gradients
+};
+
+struct GrowConfig
+{
+    TreeParams tp;
+    HistMode   mode = HistMode::exact;
+};
+
+// All device buffers one tree's growth needs, sized once for a dataset and
+// a selection, reused for every tree.
+class Grower
+{
+  public:
+    Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> selected,
+           uint32_t max_root_rows, cudaStream_t stream);
+    ~Grower();
+    Grower(Grower const &)            = delete;
+    Grower &operator=(Grower const &) = delete;
+
+    // Enqueues one tree on the stream. gh: float2 (g, h) per dataset row;
+    // root_rows: the sampled rows (ascending), n_root of them. out receives
+    // the tree; leaf_id (nullable) each sampled row's leaf; scores (nullable)
+    // gets scores[r] += lr * leaf value for every sampled row.
+    void grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
+              TreeOut const &out, uint32_t *leaf_id, float *scores, float lr);
+
+    uint32_t max_nodes() const
+    {
+        return max_nodes_;
+    }
+    uint32_t n_sel() const
+    {
+        return n_sel_;
+    }
+
+    // the quantisation scales of the last tree (g, h); 0 for the exact form
+    float2 const *quant_scale() const
+    {
+        return scale_;
+    }
+
+  private:
+    void level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
+               TreeOut const &out, uint32_t *leaf_id, float *scores, float lr);
+    void build(uint32_t const *rows, uint32_t n_feat_build, int dst);
+
+    Plane const          &plane_;
+    GrowConfig            cfg_;
+    std::vector<uint32_t> sel_h_;
+    cudaStream_t          stream_;
+    uint32_t              n_sel_       = 0;
+    uint32_t              total_cells_ = 0;
+    uint32_t              max_nb_      = 0;
+    uint32_t              max_front_   = 0;
+    uint32_t              max_nodes_   = 0;
+    uint32_t              max_rows_    = 0;
+    uint32_t              max_pchunks_ = 0;
+    uint32_t              max_bchunks_ = 0;
+    uint32_t              cell_stride_ = 0; // per-(chunk, feature) count stride
+
+    // device
+    uint32_t *sel_      = nullptr; // selected feature ids
+    uint32_t *cell_off_ = nullptr; // per selected feature, its first cell
+    uint32_t *sel_nb_   = nullptr; // per selected feature, its bin count
+    Ctl      *ctl_      = nullptr;
+    Node     *nodes_[2] = {nullptr, nullptr};
+    void     *hist_[2]  = {nullptr, nullptr}; // [front][total_cells] cells
+    Best     *cand_     = nullptr;             // [front][n_sel]
+    Best     *best_     = nullptr;             // [front]
+    Chunk    *pchunks_  = nullptr;
+    uint32_t *pleft_    = nullptr; // per partition chunk: left count, then base
+    uint32_t *prbase_   = nullptr;
+    uint32_t *dst_      = nullptr; // per frontier slot: child segment start
+    uint32_t *build_    = nullptr; // per build index: frontier slot in next
+    uint32_t *bpair_    = nullptr; // per split: (parent, small, large) slots
+    uint32_t *brange_   = nullptr; // per build index: chunk range [c0, c1)
+    Chunk    *bchunks_  = nullptr;
+    uint32_t *ccount_   = nullptr; // [bchunk][n_sel][cell_stride] counts/offsets
+    uint32_t *seg_      = nullptr; // [build][n_sel][cell_stride] bin segment starts
+    float2   *payload_  = nullptr; // [n_sel][max_rows] bin-sorted (g, h)
+    uint32_t *rows_[2]  = {nullptr, nullptr};
+    uint32_t *pcr_      = nullptr; // per frontier slot: partition chunk range
+    uint32_t *nleft_    = nullptr; // per frontier slot: rows routed left
+    int8_t   *mono_     = nullptr; // per feature monotone direction, or null
+    uint32_t  n_mono_   = 0;
+    float2 const *gh_cur_ = nullptr;
+    std::vector<uint32_t> off_h_;
+    // quantised form
+    int32_t  *qgh_      = nullptr; // per row, packed (g, h) integers
+    float2   *scale_    = nullptr;
+    uint32_t *absmax_   = nullptr;
+    uint64_t  seed_     = 0;
+    uint32_t  tree_no_  = 0;
+
+  public:
+    void set_seed(uint64_t s)
+    {
+        seed_ = s;
+    }
+    // per-feature monotone directions (+1 / -1 / 0), copied to the device
+    void set_monotone(std::vector<int8_t> const &m);
+};
+
+} // namespace bb

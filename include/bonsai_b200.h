@@ -1,0 +1,174 @@
+/* bonsai_b200 — C ABI of the B200-native CUDA growers.
+ *
+ * The drop-in boundary for the reference's CUDA grower surface
+ * (daniel-m-campos/bonsai). Plain pointers and sizes only. Every call returns
+ * 0 on success or a nonzero status; bb_last_error() then holds the message,
+ * "cuda: <what>: <detail>" for CUDA failures (the reference's check() text,
+ * src/cuda/detail/device_buffer.cuh:96-103) and the remedy text for capacity
+ * refusals (the reference's ConfigError, src/cuda/detail/device_context.cu:
+ * 60-87). Status BB_DECLINED means "not handled on the device": the caller
+ * falls back to its host path, as the reference's nullptr/false declines do
+ * (src/cuda/histogram_engine.cu:336-340, src/cuda/predict.cu:151-170).
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef BONSAI_B200_H
+#define BONSAI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+enum
+{
+    BB_OK          = 0,
+    BB_ERR_CUDA    = 1, /* a CUDA runtime failure */
+    BB_ERR_CONFIG  = 2, /* a capacity / configuration refusal */
+    BB_ERR_ARG     = 3, /* an invalid argument */
+    BB_DECLINED    = 4  /* not handled here; use the host path */
+};
+
+typedef struct bb_plane   bb_plane;   /* a device-resident binned dataset */
+typedef struct bb_booster bb_booster; /* a device-resident boosting fit */
+
+/* Last error message of the calling thread ("" when none). */
+char const *bb_last_error(void);
+
+/* 1 when a usable CUDA device is present.
+ * Replaces bonsai::cuda_available (include/bonsai/cuda/histogram_engine.hpp:22). */
+int bb_available(void);
+
+/* Select the device for the calling thread's later calls.
+ * Replaces bonsai::cuda_select_device (histogram_engine.hpp:31). */
+int bb_select_device(uint32_t device_id);
+
+/* ---- ingest: bin application -------------------------------------------
+ * Bins a row-major float32 matrix (n_rows x n_feats) against per-feature
+ * cuts (cuts[cut_off[f] .. cut_off[f+1]), strictly increasing, the last two
+ * FLT_MAX and +inf) into a device plane of feature-major u8 codes (u16 when
+ * any feature has more than 256 bins). x_on_device selects whether X is a
+ * device pointer (read, not retained) or host memory (streamed up in 64 MB
+ * chunks). Bin codes are bit-identical to BinMapper::transform.
+ * Replaces bonsai::cuda_ingest(features_view, BinMappers) and
+ * cuda_ingest_device(DeviceMatrix, BinMappers) (histogram_engine.hpp:41-68). */
+int bb_ingest(float const *X, uint64_t n_rows, uint32_t n_feats, int x_on_device,
+              float const *cuts, uint32_t const *cut_off, bb_plane **out);
+
+/* 1 when the plane stores u8 codes, 0 for u16. */
+int bb_plane_is_u8(bb_plane const *plane);
+
+/* Copies the plane's codes to host, feature-major, widened to u16
+ * (out[f * n_rows + r]). Replaces IngestPlane::materialize
+ * (include/bonsai/dataset.hpp:44-45). */
+int bb_plane_download(bb_plane const *plane, uint16_t *out);
+
+void bb_plane_destroy(bb_plane *plane);
+
+/* ---- training ------------------------------------------------------------ */
+
+/* The TreeConfig / BoosterConfig keys the device path reads
+ * (include/bonsai/config/tree_config.hpp:9-29, booster_config.hpp:8-24). */
+typedef struct
+{
+    int32_t        objective;  /* 0 mse, 1 logloss */
+    float          learning_rate;
+    float          min_child_hess;
+    float          min_gain_to_split;
+    float          lambda_l2;
+    float          lambda_l1;
+    uint32_t       max_depth;  /* <= 8 */
+    uint32_t       min_data_in_leaf;
+    int32_t        hist_mode;  /* 0 exact (plain), 1 int8 quantised, 2 int16 */
+    uint64_t       seed;       /* quantised stochastic-rounding seed */
+    int8_t const  *monotone;   /* per-feature +1/-1/0, or NULL */
+    uint32_t       n_monotone;
+    uint32_t const *selected;  /* ascending feature ids, or NULL for all */
+    uint32_t       n_selected;
+    int32_t        use_graph;  /* capture one boosting round as a CUDA graph */
+} bb_train_cfg;
+
+/* A device-resident boosting fit over the plane: labels (host, n_rows) and
+ * the scores stay on the device; every round derives (g, h) on the device,
+ * grows a depthwise tree and fuses scores += lr * leaf into the grow.
+ * init_scores (host, n_rows) may be NULL: the objective's init_score
+ * (src/objective.cpp:76-83, :124-131) is then used.
+ * Replaces Booster<Obj, DepthwiseGrower<CudaHistogramEngine>, AllRows> with
+ * the resident round armed (include/bonsai/booster.hpp:630-676) and the
+ * engine's resident_begin (histogram_engine.hpp:251-253). */
+int bb_booster_create(bb_plane const *plane, float const *labels,
+                      float const *init_scores, bb_train_cfg const *cfg,
+                      uint32_t max_trees, bb_booster **out);
+
+/* Runs n_iters more rounds (asynchronous; bb_booster_sync waits). */
+int bb_booster_update(bb_booster *b, uint32_t n_iters);
+int bb_booster_sync(bb_booster *b);
+
+int   bb_booster_n_trees(bb_booster const *b, uint32_t *n);
+float bb_booster_init_score(bb_booster const *b);
+/* Nodes per tree slot (2^(max_depth+1) - 1). */
+uint32_t bb_booster_tree_capacity(bb_booster const *b);
+
+/* Copies tree t in the reference's DenseTree layout (tree.hpp:38-45):
+ * feature == 0xFFFFFFFF marks a leaf holding value; internal nodes hold
+ * the threshold cuts[feature][split_bin]. Arrays hold capacity entries;
+ * meta = (n_nodes, depth, n_leaves). */
+int bb_booster_tree(bb_booster const *b, uint32_t t, uint32_t *feature, float *value,
+                    uint32_t *left, uint32_t *right, uint8_t *default_left,
+                    float *gain, float *cover, uint32_t *split_bin, uint32_t *meta);
+
+/* The training scores (host, n_rows). Replaces resident_end
+ * (histogram_engine.hpp:262). */
+int bb_booster_scores(bb_booster const *b, float *out);
+
+/* Per-row leaf node id of the last tree (host, n_rows). */
+int bb_booster_leaf_ids(bb_booster const *b, uint32_t *out);
+
+/* Device time of the last bb_booster_update, in milliseconds. */
+int bb_booster_last_ms(bb_booster const *b, float *ms);
+
+void bb_booster_destroy(bb_booster *b);
+
+/* One tree from caller-provided gradients: grad/hess (host, n_rows), the
+ * sampled rows (host, ascending, n_sel_rows of them; NULL = all). Returns
+ * the tree and every sampled row's leaf value and node id (values/leaf_ids
+ * host, n_rows; entries of unsampled rows are left untouched).
+ * Replaces one DepthwiseGrower<CudaHistogramEngine>::grow call
+ * (src/grower_impl.hpp:465-577) over the engine's level plane
+ * (begin_tree .. finalize_tree, histogram_engine.hpp:94-170). */
+int bb_grow_tree(bb_plane const *plane, bb_train_cfg const *cfg, float const *grad,
+                 float const *hess, uint32_t const *rows, uint64_t n_sel_rows,
+                 uint32_t *feature, float *value, uint32_t *left, uint32_t *right,
+                 uint8_t *default_left, float *gain, float *cover,
+                 uint32_t *split_bin, uint32_t *meta, float *values,
+                 uint32_t *leaf_ids);
+
+/* ---- inference ------------------------------------------------------------
+ * Ensemble predict over a plane: out[r] = init + lr * sum_t leaf_t(r), the
+ * leaves summed in tree order (bit-identical to predict_at_binned,
+ * include/bonsai/booster.hpp:831-845). Trees are concatenated node tables
+ * (n_nodes total), tree t starting at roots[t]; child ids are tree-local.
+ * out is host memory (n_rows).
+ * Replaces cuda_predict_plan + cuda_predict (include/bonsai/cuda/predict.hpp:
+ * 29-38). */
+int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+               uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
+               uint32_t const *left, uint32_t const *right,
+               uint8_t const *default_left, float const *value, float lr, float init,
+               float *out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -137,8 +137,10 @@ static void best_for_feature(float const *cells, uint32_t nb, uint32_t fid, floa
     float const  miss_g    = cells[2 * (nb - 1)];
     float const  miss_h    = cells[(2 * (nb - 1)) + 1];
     double const node_sc   = score(tot_g, tot_h, l1, l2);
-    double const real_grad = (double)tot_g - (double)miss_g;
-    double const real_hess = (double)tot_h - (double)miss_h;
+    /* HistCell fields are float: the reference subtracts in float, then
+     * widens (src/split.cpp:117-118) */
+    double const real_grad = (double)(float)(tot_g - miss_g);
+    double const real_hess = (double)(float)(tot_h - miss_h);
     int const    mc        = monotone_of(cfg, fid);
     int const    n_dirs    = (miss_g == 0.0F && miss_h == 0.0F) ? 1 : 2;
     double       lg = 0.0, lh = 0.0;

@@ -427,3 +427,30 @@ class Oracle:
                                   arr, C.c_size_t(len(bufs)), C.c_float(init),
                                   C.c_float(lr), _p(out, C.c_float))
         return out
+
+
+def orc_find_split(orc: "Oracle", hist, n_rows, tc: TreeCfg, tot=None, lo=-np.inf, hi=np.inf):
+    """orc_find_split on a [F, n_bins, 2] float32 histogram set sharing n_bins.
+    Node totals default to Histogram::totals of feature 0."""
+    hist = np.ascontiguousarray(hist, np.float32)
+    F, nb, _ = hist.shape
+    if tot is None:
+        tot = (np.float32(hist[0, :, 0].astype(np.float64).sum()),
+               np.float32(hist[0, :, 1].astype(np.float64).sum()))
+    rows = [np.ascontiguousarray(hist[f].reshape(-1)) for f in range(F)]
+    arr = (C.POINTER(C.c_float) * F)(*[_p(r, C.c_float) for r in rows])
+    nbins = np.full(F, nb, np.uint32)
+    present = np.ones(F, np.uint8)
+
+    class _Split(C.Structure):
+        _fields_ = [("gain", C.c_double), ("feature", C.c_uint32), ("bin", C.c_uint32),
+                    ("default_left", C.c_uint8), ("valid", C.c_uint8)]
+
+    orc.L.orc_find_split.restype = _Split
+    cfg = Oracle.cfg(tc)
+    s = orc.L.orc_find_split(arr, _p(nbins, C.c_uint32), _p(present, C.c_uint8),
+                             C.c_size_t(F), C.c_size_t(n_rows), C.c_float(tot[0]),
+                             C.c_float(tot[1]), C.c_double(lo), C.c_double(hi),
+                             C.byref(cfg))
+    return dict(gain=s.gain, feature=s.feature, bin=s.bin, default_left=s.default_left,
+                valid=s.valid)
