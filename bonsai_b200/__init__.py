@@ -26,7 +26,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "predict", "fit_cuts", "cuts_from_sample", "sample_rows",
+    "grow_tree", "populate", "predict", "fit_cuts", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
@@ -217,6 +217,12 @@ class Booster:
         check(lib().bb_booster_leaf_ids(self.h, ptr(out)))
         return out
 
+    def profile_round(self) -> dict:
+        """One boosting round timed phase by phase (bb_booster_profile_round)."""
+        p = _lib.Profile()
+        check(lib().bb_booster_profile_round(self.h, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in _lib.Profile._fields_}
+
     def close(self):
         if getattr(self, "h", None):
             lib().bb_booster_destroy(self.h)
@@ -244,6 +250,22 @@ def grow_tree(plane: Plane, params: TrainParams, grad, hess, rows=None):
                              *(ptr(a[k]) for k in _ORDER), ptr(meta), ptr(values),
                              ptr(ids)))
     return _finish(a, meta), values, ids
+
+
+def populate(plane: Plane, params: TrainParams, grad, hess, rows=None) -> np.ndarray:
+    """One node's histograms (bb_populate): [total_bins, 2] FP64 (g, h) cell
+    sums, features in selection order."""
+    grad = np.ascontiguousarray(grad, np.float32)
+    hess = np.ascontiguousarray(hess, np.float32)
+    sel = params.selected if params.selected is not None else range(plane.n_feats)
+    total = int(sum(int(plane.n_bins[f]) for f in sel))
+    out = np.empty((total, 2), np.float64)
+    r = None if rows is None else np.ascontiguousarray(rows, np.uint32)
+    cfg = params.c()
+    check(lib().bb_populate(plane.h, C.byref(cfg), ptr(grad), ptr(hess),
+                            None if r is None else ptr(r), 0 if r is None else len(r),
+                            ptr(out)))
+    return out
 
 
 def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:

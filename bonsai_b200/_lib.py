@@ -40,6 +40,14 @@ class TrainCfg(C.Structure):
     ]
 
 
+class Profile(C.Structure):
+    _fields_ = [
+        ("hist_ms", C.c_double), ("partition_ms", C.c_double), ("find_ms", C.c_double),
+        ("other_ms", C.c_double), ("total_ms", C.c_double), ("hist_bytes", C.c_double),
+        ("hist_rows", C.c_uint64), ("hist_builds", C.c_uint32), ("launches", C.c_uint32),
+    ]
+
+
 _lib = None
 
 
@@ -70,10 +78,12 @@ def lib() -> C.CDLL:
         L.bb_booster_leaf_ids.argtypes = [vp, vp]
         L.bb_booster_last_ms.argtypes = [vp, C.POINTER(C.c_float)]
         L.bb_booster_destroy.argtypes = [vp]
+        L.bb_booster_profile_round.argtypes = [vp, C.POINTER(Profile)]
         L.bb_grow_tree.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64] + [vp] * 11
         L.bb_predict.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 6 + [
             C.c_float, C.c_float, vp]
         L.bb_select_device.argtypes = [C.c_uint32]
+        L.bb_populate.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64, vp]
         _lib = L
     return _lib
 

@@ -310,7 +310,7 @@ struct bb_booster
         uint64_t const n = plane->n_rows;
         gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
         BB_LAUNCH("gradient_kernel");
-        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t, leaf_id, scores, lr);
+        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t, leaf_id, scores, lr, true);
         commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
         BB_LAUNCH("commit_tree_kernel");
     }
@@ -396,6 +396,7 @@ extern "C"
                 try
                 {
                     ingest(p, X, x_on_device != 0, s);
+                    build_mirror(p, s);
                     BB_CHECK(cudaStreamSynchronize(s));
                 }
                 catch (...)
@@ -453,6 +454,7 @@ extern "C"
         }
         Plane &p = plane->p;
         cudaFree(p.bins);
+        cudaFree(p.mirror);
         cudaFree(p.cuts);
         cudaFree(p.cut_off);
         cudaFree(p.n_bins);
@@ -473,10 +475,6 @@ extern "C"
                 need(cfg->objective == 0 || cfg->objective == 1,
                      "objective must be 0 (mse) or 1 (logloss)");
                 need(max_trees > 0, "max_trees must be positive");
-                if (cfg->hist_mode != 0)
-                {
-                    throw ConfigError("quantised histograms are not built in this library");
-                }
                 auto         b = std::make_unique<bb_booster>();
                 Plane const &p = plane->p;
                 uint64_t const n = p.n_rows;
@@ -516,6 +514,7 @@ extern "C"
                                                      selection(*cfg, p.n_feats),
                                                      static_cast<uint32_t>(n), b->stream);
                 b->grower->set_monotone(monotone(*cfg));
+                b->grower->set_seed(cfg->seed);
                 b->scratch.alloc(b->grower->max_nodes(), 1);
                 b->trees.alloc(b->grower->max_nodes(), max_trees);
                 b->use_graph = cfg->use_graph != 0;
@@ -632,6 +631,43 @@ extern "C"
             });
     }
 
+    int bb_booster_profile_round(bb_booster *b, bb_profile *out)
+    {
+        return guarded(
+            [&]
+            {
+                need(b->n_trees + 1 <= b->trees.n, "bb_booster_profile_round: tree capacity");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                Profile p;
+                b->grower->set_profile(&p);
+                BB_CHECK(cudaEventRecord(b->ev0, b->stream));
+                try
+                {
+                    b->round_body();
+                }
+                catch (...)
+                {
+                    b->grower->set_profile(nullptr);
+                    throw;
+                }
+                b->grower->set_profile(nullptr);
+                BB_CHECK(cudaEventRecord(b->ev1, b->stream));
+                BB_CHECK(cudaEventSynchronize(b->ev1));
+                float ms = 0.0F;
+                BB_CHECK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+                b->n_trees += 1;
+                out->hist_ms      = p.hist_ms;
+                out->partition_ms = p.partition_ms;
+                out->find_ms      = p.find_ms;
+                out->other_ms     = p.other_ms;
+                out->total_ms     = ms;
+                out->hist_bytes   = p.hist_bytes;
+                out->hist_rows    = p.hist_rows;
+                out->hist_builds  = p.hist_builds;
+                out->launches     = b->grower->launches_per_tree() + 2;
+            });
+    }
+
     void bb_booster_destroy(bb_booster *b)
     {
         if (b == nullptr)
@@ -668,10 +704,6 @@ extern "C"
             {
                 need(plane != nullptr && cfg != nullptr && grad != nullptr && hess != nullptr,
                      "bb_grow_tree: null argument");
-                if (cfg->hist_mode != 0)
-                {
-                    throw ConfigError("quantised histograms are not built in this library");
-                }
                 Plane const   &p = plane->p;
                 uint64_t const n = p.n_rows;
                 uint64_t const m = rows == nullptr ? n : n_sel_rows;
@@ -710,6 +742,7 @@ extern "C"
                     Grower g(p, grow_config(*cfg), selection(*cfg, p.n_feats),
                              static_cast<uint32_t>(std::max<uint64_t>(m, 1)), s);
                     g.set_monotone(monotone(*cfg));
+                    g.set_seed(cfg->seed);
                     ts.alloc(g.max_nodes(), 1);
                     g.grow(d_gh, d_rows, static_cast<uint32_t>(m), ts.t, d_leaf, d_val, 1.0F);
                     BB_CHECK(cudaStreamSynchronize(s));
@@ -741,6 +774,66 @@ extern "C"
                 cudaFree(d_rows);
                 cudaFree(d_leaf);
                 cudaFree(d_val);
+                BB_CHECK(cudaStreamDestroy(s));
+            });
+    }
+
+    int bb_populate(bb_plane const *plane, bb_train_cfg const *cfg, float const *grad,
+                    float const *hess, uint32_t const *rows, uint64_t n_sel_rows, double *out)
+    {
+        return guarded(
+            [&]
+            {
+                need(plane != nullptr && cfg != nullptr && grad != nullptr && hess != nullptr &&
+                         out != nullptr,
+                     "bb_populate: null argument");
+                Plane const   &p = plane->p;
+                uint64_t const n = p.n_rows;
+                uint64_t const m = rows == nullptr ? n : n_sel_rows;
+                need(m <= n, "bb_populate: more rows than the plane holds");
+                for (uint64_t k = 0; rows != nullptr && k < m; ++k)
+                {
+                    need(rows[k] < n && (k == 0 || rows[k] > rows[k - 1]),
+                         "bb_populate: rows must be ascending row ids below n_rows");
+                }
+                cudaStream_t s;
+                BB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                std::vector<float2> gh(n);
+                for (uint64_t i = 0; i < n; ++i)
+                {
+                    gh[i] = make_float2(grad[i], hess[i]);
+                }
+                float2   *d_gh   = dmalloc<float2>(n);
+                uint32_t *d_rows = dmalloc<uint32_t>(std::max<uint64_t>(m, 1));
+                try
+                {
+                    BB_CHECK(cudaMemcpyAsync(d_gh, gh.data(), n * 8, cudaMemcpyHostToDevice, s));
+                    if (rows == nullptr)
+                    {
+                        iota_kernel<<<blocks(n), 256, 0, s>>>(d_rows, n);
+                        BB_LAUNCH("iota_kernel");
+                    }
+                    else if (m > 0)
+                    {
+                        BB_CHECK(cudaMemcpyAsync(d_rows, rows, m * 4, cudaMemcpyHostToDevice, s));
+                    }
+                    GrowConfig gc = grow_config(*cfg);
+                    gc.tp.max_depth = 1;
+                    Grower g(p, gc, selection(*cfg, p.n_feats),
+                             static_cast<uint32_t>(std::max<uint64_t>(m, 1)), s);
+                    g.set_seed(cfg->seed);
+                    g.populate(d_gh, d_rows, static_cast<uint32_t>(m),
+                               reinterpret_cast<double2 *>(out));
+                }
+                catch (...)
+                {
+                    cudaFree(d_gh);
+                    cudaFree(d_rows);
+                    cudaStreamDestroy(s);
+                    throw;
+                }
+                cudaFree(d_gh);
+                cudaFree(d_rows);
                 BB_CHECK(cudaStreamDestroy(s));
             });
     }

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <type_traits>
 
 namespace bb
 {
@@ -30,7 +31,8 @@ namespace
 
 constexpr uint32_t k_threads    = 256;
 constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
-constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk
+constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk (exact)
+constexpr uint32_t k_qbuild_rows = 32768; // rows per histogram-build chunk (quantised)
 constexpr uint32_t k_warps_feat = 8;    // features per count/scatter CTA
 constexpr uint32_t k_find_warps = 4;    // features per find CTA
 constexpr uint32_t k_chain_stg  = 32;   // elements per lane per cp.async stage
@@ -120,9 +122,10 @@ __device__ __forceinline__ float leaf_value(Node const &nd, TreeParams const &tp
 // ---------------------------------------------------------------- root ----
 
 __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk *bchunks,
-                                  uint32_t *brange, uint32_t *build, TreeOut t)
+                                  uint32_t *brange, uint32_t *build, TreeOut t,
+                                  uint32_t crows)
 {
-    uint32_t const nch = (n_root + k_build_rows - 1) / k_build_rows;
+    uint32_t const nch = (n_root + crows - 1) / crows;
     if (threadIdx.x == 0)
     {
         Ctl c{};
@@ -148,8 +151,8 @@ __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk 
     }
     for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x)
     {
-        uint32_t const b = c * k_build_rows;
-        bchunks[c]       = {0, b, min(k_build_rows, n_root - b), 0};
+        uint32_t const b = c * crows;
+        bchunks[c]       = {0, b, min(crows, n_root - b), 0};
     }
 }
 
@@ -466,7 +469,8 @@ __global__ void __launch_bounds__(32)
 
 // The per-candidate core of update_best_for_feature_for_node
 // (src/split.cpp:55-82,101-162) for one (bin, default_left).
-__device__ __forceinline__ bool candidate_gain(double lg, double lh, float mg, float mh,
+template <typename M>
+__device__ __forceinline__ bool candidate_gain(double lg, double lh, M mg, M mh,
                                                double real_g, double real_h, bool dl,
                                                double node_score, TreeParams const &tp,
                                                int mc, double lo, double hi,
@@ -517,11 +521,12 @@ __device__ __forceinline__ void warp_best(double &gain, uint32_t &order)
 }
 
 // grid (frontier, ceil(n_sel / 4)), 4 warps: one warp per (node, feature).
+template <bool Q>
 __global__ void __launch_bounds__(32 * k_find_warps)
-    find_kernel(Ctl const *ctl, Node const *nodes, float2 const *hist,
+    find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
                 uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                 uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
-                TreeParams tp, Best *cand, uint32_t max_nb)
+                TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale)
 {
     extern __shared__ unsigned char smem_raw[];
     uint32_t const i = blockIdx.x;
@@ -551,36 +556,85 @@ __global__ void __launch_bounds__(32 * k_find_warps)
         }
         return;
     }
-    float2 const *src = hist + (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
-    for (uint32_t b = lane; b < nb; b += 32)
-    {
-        cell[b] = src[b];
-    }
-    __syncwarp();
     uint32_t const n_cut = nb - 2;
-    if (lane == 0)
+    using MissT          = typename std::conditional<Q, double, float>::type;
+    MissT          mg;
+    MissT          mh;
+    double         node_sc;
+    double         real_g;
+    double         real_h;
+    bool           miss_empty;
+    double const   l1 = tp.lambda_l1;
+    double const   l2 = tp.lambda_l2;
+    if constexpr (Q)
     {
-        double lg = 0.0;
-        double lh = 0.0;
-        for (uint32_t b = 0; b < n_cut; ++b)
+        // exact integer cells: an exact prefix, then one FP64 scaling
+        auto const *src = static_cast<unsigned long long const *>(hist_v) +
+                          (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
+        double2 const sc = *qscale;
+        auto *icell      = reinterpret_cast<unsigned long long *>(cell);
+        for (uint32_t b = lane; b < nb; b += 32)
         {
-            lg += cell[b].x;
-            lh += cell[b].y;
-            pref[b] = make_double2(lg, lh);
+            icell[b] = src[b];
         }
+        __syncwarp();
+        if (lane == 0)
+        {
+            int64_t pg = 0;
+            int64_t ph = 0;
+            for (uint32_t b = 0; b < n_cut; ++b)
+            {
+                unsigned long long const c = icell[b];
+                pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+                ph += static_cast<uint32_t>(c);
+                pref[b] = make_double2(static_cast<double>(pg) * sc.x,
+                                       static_cast<double>(ph) * sc.y);
+            }
+        }
+        __syncwarp();
+        unsigned long long const mc_ = icell[nb - 1];
+        int64_t const mqg = static_cast<int32_t>(static_cast<uint32_t>(mc_ >> 32));
+        int64_t const mqh = static_cast<uint32_t>(mc_);
+        mg         = static_cast<double>(mqg) * sc.x;
+        mh         = static_cast<double>(mqh) * sc.y;
+        node_sc    = split_score(static_cast<double>(nd.qg) * sc.x,
+                                 static_cast<double>(nd.qh) * sc.y, l1, l2);
+        real_g     = static_cast<double>(nd.qg - mqg) * sc.x;
+        real_h     = static_cast<double>(nd.qh - mqh) * sc.y;
+        miss_empty = mqg == 0 && mqh == 0;
     }
-    __syncwarp();
-    float const  mg      = cell[nb - 1].x;
-    float const  mh      = cell[nb - 1].y;
-    double const l1      = tp.lambda_l1;
-    double const l2      = tp.lambda_l2;
-    double const node_sc = split_score(nd.sum_g, nd.sum_h, l1, l2);
-    // float fields subtract in float, then widen (src/split.cpp:117-118)
-    double const real_g  = static_cast<double>(nd.sum_g - mg);
-    double const real_h  = static_cast<double>(nd.sum_h - mh);
+    else
+    {
+        float2 const *src = static_cast<float2 const *>(hist_v) +
+                            (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
+        for (uint32_t b = lane; b < nb; b += 32)
+        {
+            cell[b] = src[b];
+        }
+        __syncwarp();
+        if (lane == 0)
+        {
+            double lg = 0.0;
+            double lh = 0.0;
+            for (uint32_t b = 0; b < n_cut; ++b)
+            {
+                lg += cell[b].x;
+                lh += cell[b].y;
+                pref[b] = make_double2(lg, lh);
+            }
+        }
+        __syncwarp();
+        mg      = cell[nb - 1].x;
+        mh      = cell[nb - 1].y;
+        node_sc = split_score(nd.sum_g, nd.sum_h, l1, l2);
+        // float fields subtract in float, then widen (src/split.cpp:117-118)
+        real_g     = static_cast<double>(nd.sum_g - mg);
+        real_h     = static_cast<double>(nd.sum_h - mh);
+        miss_empty = mg == 0.0F && mh == 0.0F;
+    }
     uint32_t const f     = sel[j];
     int const      mc    = (mono != nullptr && f < n_mono) ? mono[f] : 0;
-    uint32_t const n_dir = (mg == 0.0F && mh == 0.0F) ? 1 : 2;
+    uint32_t const n_dir = miss_empty ? 1 : 2;
     double         best  = 0.0;
     uint32_t       order = 0xFFFFFFFFu;
     double const   min_gain = tp.min_gain_to_split;
@@ -590,7 +644,7 @@ __global__ void __launch_bounds__(32 * k_find_warps)
         for (uint32_t d = 0; d < n_dir; ++d)
         {
             double gain = 0.0;
-            if (candidate_gain(p.x, p.y, mg, mh, real_g, real_h, d == 0, node_sc, tp, mc,
+            if (candidate_gain<MissT>(p.x, p.y, mg, mh, real_g, real_h, d == 0, node_sc, tp, mc,
                                nd.lo, nd.hi, gain) &&
                 gain > best && gain >= min_gain)
             {
@@ -742,7 +796,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  Chunk const *pchunks, uint32_t const *pcr, uint32_t *pleft,
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
-                 TreeOut t)
+                 TreeOut t, uint32_t crows)
 {
     uint32_t const n_cur = ctl->n_cur;
     uint32_t const lane  = threadIdx.x & 31;
@@ -834,7 +888,7 @@ __global__ void __launch_bounds__(k_plan_thr)
         small_count         = left_sm ? nl : nr;
     }
     // histogram-build chunk table over the smaller children
-    uint32_t const nch   = surv ? (small_count + k_build_rows - 1) / k_build_rows : 0;
+    uint32_t const nch   = surv ? (small_count + crows - 1) / crows : 0;
     uint32_t       nch_t = 0;
     uint32_t const c0    = block_excl_scan<k_plan_thr>(nch, &nch_t);
     uint32_t       built = 0;
@@ -845,8 +899,8 @@ __global__ void __launch_bounds__(k_plan_thr)
         brange[k]          = c0;
         for (uint32_t c = 0; c < nch; ++c)
         {
-            uint32_t const b = c * k_build_rows;
-            bchunks[c0 + c]  = {k, sst + b, min(k_build_rows, small_count - b), pbase};
+            uint32_t const b = c * crows;
+            bchunks[c0 + c]  = {k, sst + b, min(crows, small_count - b), pbase};
         }
     }
     if (i == 0)
@@ -1017,65 +1071,415 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
-// The surviving frontier after the last level: leaves (end_tree).
+// The surviving frontier after the last level: leaves (end_tree). Marks
+// every node a leaf and lays out its partition-chunk table, so the stamp
+// (and, quantised, the leaf renewal) run chunk by chunk as on any level.
 __global__ void __launch_bounds__(k_plan_thr)
-    final_kernel(Ctl *ctl, Node const *nodes, TreeParams tp, TreeOut t)
+    final_kernel(Ctl *ctl, Node *nodes, TreeParams tp, TreeOut t, Chunk *pchunks,
+                 uint32_t *pcr)
 {
-    uint32_t const n = ctl->n_cur;
-    uint32_t const i = threadIdx.x;
-    uint32_t       c = 0;
-    if (i < n)
+    uint32_t const n    = ctl->n_cur;
+    uint32_t const i    = threadIdx.x;
+    bool const     live = i < n;
+    Node           nd   = live ? nodes[i] : Node{};
+    if (live)
     {
-        Node const nd = nodes[i];
         write_leaf_node(t, nd.id, leaf_value(nd, tp));
-        c = nd.count;
+        nd.flags = 0;
+        nodes[i] = nd;
     }
-    uint32_t total = 0;
-    block_excl_scan<k_plan_thr>(c, &total);
+    uint32_t const nch   = live ? (nd.count + k_part_rows - 1) / k_part_rows : 0;
+    uint32_t       total = 0;
+    uint32_t const c0    = block_excl_scan<k_plan_thr>(nch, &total);
+    if (live)
+    {
+        pcr[i] = c0;
+        for (uint32_t c = 0; c < nch; ++c)
+        {
+            uint32_t const b = c * k_part_rows;
+            pchunks[c0 + c]  = {i, nd.start + b, min(k_part_rows, nd.count - b), 0};
+        }
+    }
     if (i == 0)
     {
-        ctl->n_leaves += n;
-        ctl->built_rows = total;
+        pcr[n]          = total;
+        ctl->n_pchunks  = total;
+        ctl->n_leaves  += n;
         t.meta[0]       = ctl->n_nodes;
         t.meta[1]       = ctl->depth;
         t.meta[2]       = ctl->n_leaves;
     }
 }
 
-__global__ void __launch_bounds__(k_threads)
-    final_stamp_kernel(Ctl const *ctl, Node const *nodes, uint32_t const *rows,
-                       TreeOut t, uint32_t *leaf_id, float *scores, float lr)
+
+
+// ------------------------------------------------------ quantised form ----
+// Per tree: (g, h) scaled by FP64 scales max|g| / 127 and max h / 127 and
+// stochastically rounded to int8 with a counter-based generator, so the
+// histograms are exact integer sums (order-independent, deterministic). The
+// split gain is evaluated in FP64 from the integer sums; leaf values are
+// renewed in FP64 from the full-precision gradients of each leaf's rows
+// (the scheme of Shi et al., "Quantized Training of Gradient Boosting
+// Decision Trees", NeurIPS 2022).
+
+// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers:
+// as easy as 1, 2, 3", SC 2011): ten rounds of the Philox S-box with the
+// published multipliers and Weyl key increments.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 {
-    uint32_t const p = (blockIdx.x * k_threads) + threadIdx.x;
-    if (p >= ctl->built_rows)
+    constexpr uint32_t m0 = 0xD2511F53u;
+    constexpr uint32_t m1 = 0xCD9E8D57u;
+    constexpr uint32_t w0 = 0x9E3779B9u;
+    constexpr uint32_t w1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r)
+    {
+        uint32_t const hi0 = __umulhi(m0, c.x);
+        uint32_t const lo0 = m0 * c.x;
+        uint32_t const hi1 = __umulhi(m1, c.z);
+        uint32_t const lo1 = m1 * c.z;
+        c                  = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += w0;
+        k.y += w1;
+    }
+    return c;
+}
+
+__global__ void __launch_bounds__(k_threads)
+    absmax_kernel(float2 const *__restrict__ gh, uint32_t n, uint32_t *absmax)
+{
+    __shared__ float sg[k_threads / 32];
+    __shared__ float sh[k_threads / 32];
+    float            mg = 0.0F;
+    float            mh = 0.0F;
+    for (uint32_t i = (blockIdx.x * k_threads) + threadIdx.x; i < n;
+         i += gridDim.x * k_threads)
+    {
+        float2 const v = gh[i];
+        mg             = fmaxf(mg, fabsf(v.x));
+        mh             = fmaxf(mh, fmaxf(v.y, 0.0F));
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        mg = fmaxf(mg, __shfl_xor_sync(0xFFFFFFFFu, mg, o));
+        mh = fmaxf(mh, __shfl_xor_sync(0xFFFFFFFFu, mh, o));
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        sg[threadIdx.x >> 5] = mg;
+        sh[threadIdx.x >> 5] = mh;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (uint32_t w = 1; w < k_threads / 32; ++w)
+        {
+            mg = fmaxf(mg, sg[w]);
+            mh = fmaxf(mh, sh[w]);
+        }
+        // non-negative floats order as their bit patterns
+        atomicMax(&absmax[0], __float_as_uint(mg));
+        atomicMax(&absmax[1], __float_as_uint(mh));
+    }
+}
+
+__global__ void __launch_bounds__(k_threads)
+    quantise_kernel(float2 const *__restrict__ gh, uint32_t n,
+                    uint32_t const *__restrict__ absmax, uint2 key,
+                    uint32_t const *__restrict__ tree_no, uint16_t *__restrict__ q,
+                    double2 *__restrict__ scale)
+{
+    double const mg = __uint_as_float(absmax[0]);
+    double const mh = __uint_as_float(absmax[1]);
+    double const sg = mg > 0.0 ? mg / 127.0 : 1.0;
+    double const sh = mh > 0.0 ? mh / 127.0 : 1.0;
+    uint32_t const t = *tree_no;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        *scale = make_double2(sg, sh);
+    }
+    for (uint32_t i = (blockIdx.x * k_threads) + threadIdx.x; i < n;
+         i += gridDim.x * k_threads)
+    {
+        float2 const v  = gh[i];
+        uint4 const  r  = philox4x32_10(make_uint4(i, t, 0x5157u, 0u), key);
+        double const ug = static_cast<double>(r.x >> 8) * (1.0 / 16777216.0);
+        double const uh = static_cast<double>(r.y >> 8) * (1.0 / 16777216.0);
+        double const xg = static_cast<double>(v.x) / sg;
+        double const xh = static_cast<double>(fmaxf(v.y, 0.0F)) / sh;
+        int          qg = isnan(xg) ? 0 : static_cast<int>(floor(xg + ug));
+        int          qh = isnan(xh) ? 0 : static_cast<int>(floor(xh + uh));
+        qg              = max(-127, min(127, qg));
+        qh              = max(0, min(127, qh));
+        q[i] = static_cast<uint16_t>(static_cast<uint8_t>(static_cast<int8_t>(qg)) |
+                                     (static_cast<uint32_t>(qh) << 8));
+    }
+}
+
+// Zeroes the cells of the nodes about to be built.
+__global__ void __launch_bounds__(k_threads)
+    zero_build_kernel(Ctl const *ctl, uint32_t const *build, unsigned long long *hist,
+                      uint32_t total_cells, uint32_t n_cells)
+{
+    uint32_t const i = blockIdx.x;
+    if (i >= ctl->n_build)
     {
         return;
     }
-    uint32_t const n  = ctl->n_cur;
-    uint32_t       lo = 0;
-    uint32_t       hi = n;
-    while (hi - lo > 1)
+    unsigned long long *h = hist + (static_cast<uint64_t>(build[i]) * total_cells);
+    for (uint32_t x = threadIdx.x; x < n_cells; x += k_threads)
     {
-        uint32_t const mid = (lo + hi) >> 1;
-        if (nodes[mid].start <= p)
+        h[x] = 0ULL;
+    }
+}
+
+// Exact integer histogram of a chunk of a built node's rows over one mirror
+// tile: one gathered 32-byte sector per row, one packed 64-bit
+// shared-memory add per (row, feature) -- the gradient in the high word
+// (two's complement), the hessian in the low word -- then one global add
+// per touched cell. grid (chunks, tiles), 256 threads.
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    qhist_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
+                 uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                 uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
+                 int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
+                 uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
+{
+    constexpr uint32_t        per = k_mirror_bytes / sizeof(BinT);
+    extern __shared__ unsigned long long h_s[]; // [per][max_nb]
+    __shared__ int32_t        j_s[per];
+    uint32_t const            c = blockIdx.x;
+    if (c >= ctl->n_bchunks)
+    {
+        return;
+    }
+    uint32_t const tile = tile_ids[blockIdx.y];
+    if (threadIdx.x < per)
+    {
+        j_s[threadIdx.x] = tile_j[(blockIdx.y * per) + threadIdx.x];
+    }
+    for (uint32_t x = threadIdx.x; x < per * max_nb; x += k_threads)
+    {
+        h_s[x] = 0ULL;
+    }
+    __syncthreads();
+    Chunk const   ch  = bchunks[c];
+    uint4 const  *mt  = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        uint32_t const r = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
+        uint32_t const q = qgh[r];
+        unsigned long long const packed =
+            (static_cast<unsigned long long>(static_cast<uint32_t>(
+                 static_cast<int32_t>(static_cast<int8_t>(q & 0xFFu))))
+             << 32) |
+            static_cast<unsigned long long>(q >> 8);
+        uint4 const    a = mt[static_cast<uint64_t>(r) * 2];
+        uint4 const    b = mt[(static_cast<uint64_t>(r) * 2) + 1];
+        alignas(16) uint4 v[2] = {a, b};
+        BinT const    *bins = reinterpret_cast<BinT const *>(v);
+#pragma unroll
+        for (uint32_t i = 0; i < per; ++i)
         {
-            lo = mid;
+            if (j_s[i] >= 0)
+            {
+                atomicAdd(&h_s[(i * max_nb) + bins[i]], packed);
+            }
         }
-        else
+    }
+    __syncthreads();
+    unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells);
+    for (uint32_t x = threadIdx.x; x < per * max_nb; x += k_threads)
+    {
+        uint32_t const i  = x / max_nb;
+        uint32_t const bb = x % max_nb;
+        int32_t const  jj = j_s[i];
+        if (jj >= 0 && bb < sel_nb[jj])
         {
-            hi = mid;
+            unsigned long long const v = h_s[x];
+            if (v != 0ULL)
+            {
+                atomicAdd(&dst[cell_off[jj] + bb], v);
+            }
         }
     }
-    uint32_t const id = nodes[lo].id;
-    uint32_t const r  = rows[p];
-    if (leaf_id != nullptr)
+}
+
+__device__ __forceinline__ void qtotals_from_cells(unsigned long long const *cells,
+                                                   uint32_t nb, int64_t &g, int64_t &h)
+{
+    int64_t sg = 0;
+    int64_t sh = 0;
+    for (uint32_t b = 0; b < nb; ++b)
     {
-        leaf_id[r] = id;
+        unsigned long long const c = cells[b];
+        sg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+        sh += static_cast<uint32_t>(c);
     }
-    if (scores != nullptr)
+    g = sg;
+    h = sh;
+}
+
+__global__ void qroot_totals_kernel(Node *nodes, unsigned long long const *hist,
+                                    uint32_t const *sel_nb)
+{
+    if (threadIdx.x == 0)
     {
-        scores[r] = scores[r] + (lr * t.value[id]);
+        qtotals_from_cells(hist, sel_nb[0], nodes[0].qg, nodes[0].qh);
     }
+}
+
+// Larger child = parent - smaller child in exact integers (both packed
+// words subtract without borrow: a child's hessian sum never exceeds its
+// parent's); children's totals and monotone bounds from the integer sums.
+__global__ void __launch_bounds__(k_threads)
+    qsubtract_totals_kernel(Ctl const *ctl, uint32_t const *bpair,
+                            unsigned long long const *hist_cur, unsigned long long *hist_nxt,
+                            uint32_t total_cells, uint32_t n_cells, Node const *cur,
+                            Node *next, Best const *best, uint32_t const *sel,
+                            uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
+                            TreeParams tp, double2 const *qscale)
+{
+    uint32_t const k = blockIdx.x;
+    if (k >= ctl->n_splits)
+    {
+        return;
+    }
+    uint32_t const p  = bpair[3 * k];
+    uint32_t const s  = bpair[(3 * k) + 1];
+    uint32_t const l  = bpair[(3 * k) + 2];
+    auto const    *hp = hist_cur + (static_cast<uint64_t>(p) * total_cells);
+    auto const    *hs = hist_nxt + (static_cast<uint64_t>(s) * total_cells);
+    auto          *hl = hist_nxt + (static_cast<uint64_t>(l) * total_cells);
+    for (uint32_t x = threadIdx.x; x < n_cells; x += k_threads)
+    {
+        hl[x] = hp[x] - hs[x];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t const nb0 = sel_nb[0];
+        Node           L   = next[2 * k];
+        Node           R   = next[(2 * k) + 1];
+        qtotals_from_cells(hist_nxt + (static_cast<uint64_t>(2 * k) * total_cells), nb0,
+                           L.qg, L.qh);
+        qtotals_from_cells(hist_nxt + (static_cast<uint64_t>((2 * k) + 1) * total_cells),
+                           nb0, R.qg, R.qh);
+        Node const     par = cur[p];
+        uint32_t const f   = sel[best[p].feature];
+        int const      mc  = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+        if (mc != 0)
+        {
+            double2 const sc  = *qscale;
+            double const  l1  = tp.lambda_l1;
+            double const  l2  = tp.lambda_l2;
+            double const  wl  = bounded_leaf_weight(static_cast<double>(L.qg) * sc.x,
+                                                    static_cast<double>(L.qh) * sc.y, l1, l2,
+                                                    par.lo, par.hi);
+            double const  wr  = bounded_leaf_weight(static_cast<double>(R.qg) * sc.x,
+                                                    static_cast<double>(R.qh) * sc.y, l1, l2,
+                                                    par.lo, par.hi);
+            double const  mid = 0.5 * (wl + wr);
+            if (mc > 0)
+            {
+                L.hi = fmin(L.hi, mid);
+                R.lo = fmax(R.lo, mid);
+            }
+            else
+            {
+                L.lo = fmax(L.lo, mid);
+                R.hi = fmin(R.hi, mid);
+            }
+        }
+        next[2 * k]       = L;
+        next[(2 * k) + 1] = R;
+    }
+}
+
+// Leaf renewal, pass 1: per partition chunk of a leaf node, the FP64 sums of
+// the full-precision (g, h) of its rows, in a fixed reduction order.
+__global__ void __launch_bounds__(k_threads)
+    leafsum_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
+                   uint32_t const *rows, float2 const *__restrict__ gh, double2 *partial)
+{
+    __shared__ double sg_s[k_threads / 32];
+    __shared__ double sh_s[k_threads / 32];
+    uint32_t const    c = blockIdx.x;
+    if (c >= ctl->n_pchunks)
+    {
+        return;
+    }
+    Chunk const ch = pchunks[c];
+    Node const  nd = nodes[ch.node];
+    if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
+    {
+        return;
+    }
+    double g = 0.0;
+    double h = 0.0;
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        float2 const v = gh[rows[ch.begin + k]];
+        g += v.x;
+        h += v.y;
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        g += __shfl_xor_sync(0xFFFFFFFFu, g, o);
+        h += __shfl_xor_sync(0xFFFFFFFFu, h, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        sg_s[threadIdx.x >> 5] = g;
+        sh_s[threadIdx.x >> 5] = h;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double tg = 0.0;
+        double th = 0.0;
+        for (uint32_t w = 0; w < k_threads / 32; ++w)
+        {
+            tg += sg_s[w];
+            th += sh_s[w];
+        }
+        partial[c] = make_double2(tg, th);
+    }
+}
+
+// Leaf renewal, pass 2: per leaf node, its chunks' sums in chunk order and
+// the FP64 Newton value under the node's bounds.
+__global__ void __launch_bounds__(k_plan_thr)
+    leafval_kernel(Ctl const *ctl, Node const *nodes, uint32_t const *pcr,
+                   double2 const *partial, TreeParams tp, TreeOut t)
+{
+    uint32_t const i = threadIdx.x;
+    if (i >= ctl->n_cur)
+    {
+        return;
+    }
+    Node const nd = nodes[i];
+    if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
+    {
+        return;
+    }
+    double g = 0.0;
+    double h = 0.0;
+    for (uint32_t c = pcr[i]; c < pcr[i + 1]; ++c)
+    {
+        g += partial[c].x;
+        h += partial[c].y;
+    }
+    t.value[nd.id] = static_cast<float>(
+        bounded_leaf_weight(g, h, tp.lambda_l1, tp.lambda_l2, nd.lo, nd.hi));
+}
+
+__global__ void tree_counter_kernel(uint32_t *tree_no)
+{
+    *tree_no += 1;
 }
 
 __global__ void advance_kernel(Ctl *ctl)
@@ -1097,6 +1501,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     : plane_(plane), cfg_(cfg), sel_h_(std::move(selected)), stream_(stream)
 {
     n_sel_ = static_cast<uint32_t>(sel_h_.size());
+    quant_ = cfg_.mode != HistMode::exact;
     if (n_sel_ == 0)
     {
         throw ConfigError("grower: the feature selection is empty");
@@ -1105,6 +1510,10 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     {
         throw ConfigError("grower: max_depth above 8 exceeds the level plane's "
                           "512-node frontier; use a host grower");
+    }
+    if (cfg_.mode == HistMode::quant16)
+    {
+        throw ConfigError("grower: hist_mode int16 is not available; use int8 (1)");
     }
     std::vector<uint32_t> off(n_sel_ + 1, 0);
     std::vector<uint32_t> nb(n_sel_, 0);
@@ -1120,14 +1529,20 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         throw ConfigError("grower: a feature has more than 4096 bins; lower "
                           "bin_mapper.max_bin or use a host grower");
     }
+    if (quant_ && static_cast<uint64_t>(max_root_rows) * 127ULL >= (1ULL << 31))
+    {
+        throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per "
+                          "node; use hist_mode exact");
+    }
     total_cells_ = off[n_sel_];
     off_h_       = off;
     cell_stride_ = ((max_nb_ + 1 + 3) / 4) * 4;
     max_front_   = 1u << cfg_.tp.max_depth;
     max_nodes_   = (2u << cfg_.tp.max_depth) - 1;
-    max_rows_    = max_root_rows;
+    max_rows_    = std::max<uint32_t>(max_root_rows, 1);
+    crows_       = quant_ ? k_qbuild_rows : k_build_rows;
     max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
-    max_bchunks_ = ceil_div(max_rows_, k_build_rows) + max_front_;
+    max_bchunks_ = ceil_div(max_rows_, crows_) + max_front_;
 
     cudaStream_t s = stream_;
     sel_      = dalloc<uint32_t>(n_sel_, s);
@@ -1152,59 +1567,113 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     bpair_    = dalloc<uint32_t>(3 * max_front_, s);
     brange_   = dalloc<uint32_t>(max_front_ + 2, s);
     bchunks_  = dalloc<Chunk>(max_bchunks_, s);
-    ccount_   = dalloc<uint32_t>(static_cast<size_t>(max_bchunks_) * n_sel_ * cell_stride_, s);
-    seg_      = dalloc<uint32_t>(static_cast<size_t>(max_front_) * n_sel_ * cell_stride_, s);
-    payload_  = dalloc<float2>(static_cast<size_t>(n_sel_) * max_rows_, s);
     rows_[0]  = dalloc<uint32_t>(max_rows_, s);
     rows_[1]  = dalloc<uint32_t>(max_rows_, s);
-    scale_    = dalloc<float2>(1, s);
-    BB_CHECK(cudaMemsetAsync(scale_, 0, sizeof(float2), s));
     pcr_      = dalloc<uint32_t>(max_front_ + 2, s);
     nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
-    BB_CHECK(cudaStreamSynchronize(s));
-
-    // dynamic shared memory ceilings
-    size_t const cnt_smem  = k_warps_feat * cell_stride_ * sizeof(uint32_t);
-    size_t const bin_bytes = plane_.u8 ? 1 : 2;
-    size_t const sc_smem   = (k_build_rows * (4 + 8)) + cnt_smem +
-                           (k_warps_feat * k_build_rows * bin_bytes);
-    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
-    size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
-    if (sc_smem > 227 * 1024 || find_smem > 227 * 1024)
+    dtree_    = dalloc<uint32_t>(1, s);
+    BB_CHECK(cudaMemsetAsync(dtree_, 0, 4, s));
+    if (quant_)
     {
-        throw ConfigError("grower: bins per feature exceed the shared-memory budget");
-    }
-    if (plane_.u8)
-    {
-        BB_CHECK(cudaFuncSetAttribute(count_kernel<uint8_t>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(cnt_smem)));
-        BB_CHECK(cudaFuncSetAttribute(scatter_kernel<uint8_t>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sc_smem)));
+        absmax_  = dalloc<uint32_t>(2, s);
+        qscale_  = dalloc<double2>(1, s);
+        qgh8_    = dalloc<uint16_t>(max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows, s);
+        partial_ = dalloc<double2>(max_pchunks_, s);
+        // the mirror tiles holding the selection: all selected features, and
+        // the first one alone (the last level builds only its totals)
+        uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
+        for (int v = 0; v < 2; ++v)
+        {
+            std::vector<uint32_t> ids;
+            std::vector<int32_t>  js;
+            uint32_t const        nfb = v == 0 ? n_sel_ : 1;
+            for (uint32_t j = 0; j < nfb; ++j)
+            {
+                uint32_t const t = sel_h_[j] / per;
+                if (ids.empty() || ids.back() != t)
+                {
+                    ids.push_back(t);
+                    js.insert(js.end(), per, -1);
+                }
+                js[((ids.size() - 1) * per) + (sel_h_[j] % per)] = static_cast<int32_t>(j);
+            }
+            n_tiles_[v]  = static_cast<uint32_t>(ids.size());
+            tile_ids_[v] = dalloc<uint32_t>(ids.size(), s);
+            tile_j_[v]   = dalloc<int32_t>(js.size(), s);
+            BB_CHECK(cudaMemcpyAsync(tile_ids_[v], ids.data(), ids.size() * 4,
+                                     cudaMemcpyHostToDevice, s));
+            BB_CHECK(cudaMemcpyAsync(tile_j_[v], js.data(), js.size() * 4,
+                                     cudaMemcpyHostToDevice, s));
+            BB_CHECK(cudaStreamSynchronize(s));
+        }
+        size_t const qsmem = static_cast<size_t>(per) * max_nb_ * 8;
+        if (qsmem > 200 * 1024)
+        {
+            throw ConfigError("grower: quantised histograms of this many bins exceed "
+                              "shared memory; lower bin_mapper.max_bin");
+        }
+        auto qk = plane_.u8 ? reinterpret_cast<void const *>(&qhist_kernel<uint8_t>)
+                            : reinterpret_cast<void const *>(&qhist_kernel<uint16_t>);
+        BB_CHECK(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(qsmem)));
     }
     else
     {
-        BB_CHECK(cudaFuncSetAttribute(count_kernel<uint16_t>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(cnt_smem)));
-        BB_CHECK(cudaFuncSetAttribute(scatter_kernel<uint16_t>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(sc_smem)));
+        ccount_  = dalloc<uint32_t>(static_cast<size_t>(max_bchunks_) * n_sel_ * cell_stride_, s);
+        seg_     = dalloc<uint32_t>(static_cast<size_t>(max_front_) * n_sel_ * cell_stride_, s);
+        payload_ = dalloc<float2>(static_cast<size_t>(n_sel_) * max_rows_, s);
     }
-    BB_CHECK(cudaFuncSetAttribute(find_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    scale_ = dalloc<float2>(1, s);
+    BB_CHECK(cudaMemsetAsync(scale_, 0, sizeof(float2), s));
+    BB_CHECK(cudaStreamSynchronize(s));
+
+    // dynamic shared memory ceilings
+    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
+    if (find_smem > 227 * 1024)
+    {
+        throw ConfigError("grower: bins per feature exceed the shared-memory budget");
+    }
+    BB_CHECK(cudaFuncSetAttribute(find_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(find_smem)));
-    BB_CHECK(cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(chain_smem)));
+    BB_CHECK(cudaFuncSetAttribute(find_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(find_smem)));
+    if (!quant_)
+    {
+        size_t const cnt_smem   = k_warps_feat * cell_stride_ * sizeof(uint32_t);
+        size_t const bin_bytes  = plane_.u8 ? 1 : 2;
+        size_t const sc_smem    = (k_build_rows * (4 + 8)) + cnt_smem +
+                               (k_warps_feat * k_build_rows * bin_bytes);
+        size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
+        if (sc_smem > 227 * 1024)
+        {
+            throw ConfigError("grower: bins per feature exceed the shared-memory budget");
+        }
+        auto ck = plane_.u8 ? reinterpret_cast<void const *>(&count_kernel<uint8_t>)
+                            : reinterpret_cast<void const *>(&count_kernel<uint16_t>);
+        auto sk = plane_.u8 ? reinterpret_cast<void const *>(&scatter_kernel<uint8_t>)
+                            : reinterpret_cast<void const *>(&scatter_kernel<uint16_t>);
+        BB_CHECK(cudaFuncSetAttribute(ck, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(cnt_smem)));
+        BB_CHECK(cudaFuncSetAttribute(sk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(sc_smem)));
+        BB_CHECK(cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(chain_smem)));
+    }
+    BB_CHECK(cudaEventCreate(&pev_[0]));
+    BB_CHECK(cudaEventCreate(&pev_[1]));
 }
 
 Grower::~Grower()
 {
-    void *ptrs[] = {sel_,     cell_off_, sel_nb_,  ctl_,     nodes_[0], nodes_[1],
-                    hist_[0], hist_[1],  cand_,    best_,    pchunks_,  pleft_,
-                    prbase_,  dst_,      build_,   bpair_,   brange_,   bchunks_,
-                    ccount_,  seg_,      payload_, rows_[0], rows_[1],  scale_,
-                    absmax_,  qgh_,     pcr_,     nleft_,   mono_};
+    void *ptrs[] = {sel_,     cell_off_, sel_nb_,  ctl_,      nodes_[0],   nodes_[1],
+                    hist_[0], hist_[1],  cand_,    best_,     pchunks_,    pleft_,
+                    prbase_,  dst_,      build_,   bpair_,    brange_,     bchunks_,
+                    ccount_,  seg_,      payload_, rows_[0],  rows_[1],    scale_,
+                    absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
+                    qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
+                    tile_j_[1]};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -1213,50 +1682,149 @@ Grower::~Grower()
         }
     }
     cudaStreamSynchronize(stream_);
+    cudaEventDestroy(pev_[0]);
+    cudaEventDestroy(pev_[1]);
+}
+
+void Grower::phase_begin()
+{
+    if (prof_ != nullptr)
+    {
+        BB_CHECK(cudaEventRecord(pev_[0], stream_));
+    }
+}
+
+void Grower::phase_end(double &acc)
+{
+    if (prof_ != nullptr)
+    {
+        float ms = 0.0F;
+        BB_CHECK(cudaEventRecord(pev_[1], stream_));
+        BB_CHECK(cudaEventSynchronize(pev_[1]));
+        BB_CHECK(cudaEventElapsedTime(&ms, pev_[0], pev_[1]));
+        acc += ms;
+    }
+}
+
+void Grower::quantise(float2 const *gh, uint32_t n)
+{
+    cudaStream_t s = stream_;
+    BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
+    uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
+                                             148u * 8u);
+    absmax_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_);
+    BB_LAUNCH("absmax_kernel");
+    uint2 const key = make_uint2(static_cast<uint32_t>(seed_),
+                                 static_cast<uint32_t>(seed_ >> 32));
+    quantise_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_, qscale_);
+    BB_LAUNCH("quantise_kernel");
+    n_launch_ += 2;
 }
 
 void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
 {
-    cudaStream_t   s    = stream_;
-    size_t const   bin_bytes = plane_.u8 ? 1 : 2;
-    size_t const   cnt_smem  = k_warps_feat * cell_stride_ * sizeof(uint32_t);
-    size_t const   sc_smem   = (k_build_rows * (4 + 8)) + cnt_smem +
-                           (k_warps_feat * k_build_rows * bin_bytes);
-    dim3 const     gcs(max_bchunks_, ceil_div(nfb, k_warps_feat));
-    if (plane_.u8)
+    cudaStream_t s = stream_;
+    phase_begin();
+    if (quant_)
     {
-        count_kernel<uint8_t><<<gcs, k_threads, cnt_smem, s>>>(
-            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
-            cell_stride_);
+        int const v = nfb == n_sel_ ? 0 : 1;
+        zero_build_kernel<<<max_front_, k_threads, 0, s>>>(
+            ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_,
+            off_h_[nfb]);
+        BB_LAUNCH("zero_build_kernel");
+        uint32_t const per   = k_mirror_bytes / (plane_.u8 ? 1 : 2);
+        size_t const   qsmem = static_cast<size_t>(per) * max_nb_ * 8;
+        dim3 const     grid(max_bchunks_, n_tiles_[v]);
+        if (plane_.u8)
+        {
+            qhist_kernel<uint8_t><<<grid, k_threads, qsmem, s>>>(
+                ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+        }
+        else
+        {
+            qhist_kernel<uint16_t><<<grid, k_threads, qsmem, s>>>(
+                ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+        }
+        BB_LAUNCH("qhist_kernel");
+        n_launch_ += 2;
     }
     else
     {
-        count_kernel<uint16_t><<<gcs, k_threads, cnt_smem, s>>>(
-            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
-            cell_stride_);
+        size_t const bin_bytes = plane_.u8 ? 1 : 2;
+        size_t const cnt_smem  = k_warps_feat * cell_stride_ * sizeof(uint32_t);
+        size_t const sc_smem   = (k_build_rows * (4 + 8)) + cnt_smem +
+                               (k_warps_feat * k_build_rows * bin_bytes);
+        dim3 const   gcs(max_bchunks_, ceil_div(nfb, k_warps_feat));
+        uint32_t const *crow = rows != nullptr ? rows : root_rows_;
+        if (plane_.u8)
+        {
+            count_kernel<uint8_t><<<gcs, k_threads, cnt_smem, s>>>(
+                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
+                cell_stride_);
+        }
+        else
+        {
+            count_kernel<uint16_t><<<gcs, k_threads, cnt_smem, s>>>(
+                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
+                cell_stride_);
+        }
+        BB_LAUNCH("count_kernel");
+        offsets_kernel<<<dim3(max_front_, nfb), k_threads, 0, s>>>(
+            ctl_, brange_, ccount_, seg_, sel_nb_, nfb, cell_stride_, bchunks_);
+        BB_LAUNCH("offsets_kernel");
+        if (plane_.u8)
+        {
+            scatter_kernel<uint8_t><<<gcs, k_threads, sc_smem, s>>>(
+                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
+                ccount_, cell_stride_, payload_, max_rows_);
+        }
+        else
+        {
+            scatter_kernel<uint16_t><<<gcs, k_threads, sc_smem, s>>>(
+                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
+                ccount_, cell_stride_, payload_, max_rows_);
+        }
+        BB_LAUNCH("scatter_kernel");
+        size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
+        chain_kernel<<<dim3(max_front_, nfb, ceil_div(max_nb_, 32)), 32, chain_smem, s>>>(
+            ctl_, build_, bchunks_, brange_, seg_, payload_, max_rows_, sel_nb_, cell_off_,
+            nfb, cell_stride_, static_cast<float2 *>(hist_[dst]), total_cells_);
+        BB_LAUNCH("chain_kernel");
+        n_launch_ += 4;
     }
-    BB_LAUNCH("count_kernel");
-    offsets_kernel<<<dim3(max_front_, nfb), k_threads, 0, s>>>(
-        ctl_, brange_, ccount_, seg_, sel_nb_, nfb, cell_stride_, bchunks_);
-    BB_LAUNCH("offsets_kernel");
-    if (plane_.u8)
+    if (prof_ != nullptr)
     {
-        scatter_kernel<uint8_t><<<gcs, k_threads, sc_smem, s>>>(
-            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
-            ccount_, cell_stride_, payload_, max_rows_);
+        phase_end(prof_->hist_ms);
+        Ctl c{};
+        BB_CHECK(cudaMemcpy(&c, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        double const bin_bytes = plane_.u8 ? 1.0 : 2.0;
+        // per built row: the codes read, the gradient pair, the row id
+        double const per_row = quant_ ? ((nfb * bin_bytes) + 2.0 + 4.0)
+                                      : ((nfb * bin_bytes) + 8.0 + 4.0);
+        prof_->hist_rows += c.built_rows;
+        prof_->hist_bytes += (static_cast<double>(c.built_rows) * per_row) +
+                             (static_cast<double>(c.n_build) * off_h_[nfb] * 8.0);
+        prof_->hist_builds += 1;
     }
-    else
+}
+
+void Grower::leaf_values(TreeOut const &t, bool)
+{
+    if (!quant_)
     {
-        scatter_kernel<uint16_t><<<gcs, k_threads, sc_smem, s>>>(
-            ctl_, bchunks_, rows, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
-            ccount_, cell_stride_, payload_, max_rows_);
+        return;
     }
-    BB_LAUNCH("scatter_kernel");
-    size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
-    chain_kernel<<<dim3(max_front_, nfb, ceil_div(max_nb_, 32)), 32, chain_smem, s>>>(
-        ctl_, build_, bchunks_, brange_, seg_, payload_, max_rows_, sel_nb_, cell_off_, nfb,
-        cell_stride_, static_cast<float2 *>(hist_[dst]), total_cells_);
-    BB_LAUNCH("chain_kernel");
+    cudaStream_t s = stream_;
+    leafsum_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_cur_, rows_cur_,
+                                                      gh_cur_, partial_);
+    BB_LAUNCH("leafsum_kernel");
+    leafval_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_cur_, pcr_, partial_, cfg_.tp, t);
+    BB_LAUNCH("leafval_kernel");
+    n_launch_ += 2;
 }
 
 void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
@@ -1266,15 +1834,30 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     int const    cur = static_cast<int>(L & 1);
     int const    nxt = cur ^ 1;
     size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
-    find_kernel<<<dim3(max_front_, ceil_div(n_sel_, k_find_warps)), 32 * k_find_warps,
-                  find_smem, s>>>(ctl_, nodes_[cur], static_cast<float2 const *>(hist_[cur]),
-                                  total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_,
-                                  n_mono_, cfg_.tp, cand_, max_nb_);
+    phase_begin();
+    dim3 const fgrid(max_front_, ceil_div(n_sel_, k_find_warps));
+    if (quant_)
+    {
+        find_kernel<true><<<fgrid, 32 * k_find_warps, find_smem, s>>>(
+            ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
+    }
+    else
+    {
+        find_kernel<false><<<fgrid, 32 * k_find_warps, find_smem, s>>>(
+            ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
+    }
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
                                          plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_,
                                          pcr_);
     BB_LAUNCH("plan_kernel");
+    if (prof_ != nullptr)
+    {
+        phase_end(prof_->find_ms);
+    }
+    phase_begin();
     if (plane_.u8)
     {
         pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
@@ -1290,8 +1873,11 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     BB_LAUNCH("pcount_kernel");
     plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
                                           pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
-                                          build_, brange_, bchunks_, cfg_.tp, t);
+                                          build_, brange_, bchunks_, cfg_.tp, t, crows_);
     BB_LAUNCH("plan2_kernel");
+    nodes_cur_ = nodes_[cur];
+    rows_cur_  = rows_in;
+    leaf_values(t, false);
     stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
                                                     t, leaf_id, scores, lr);
     BB_LAUNCH("stamp_kernel");
@@ -1308,21 +1894,44 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_);
     }
     BB_LAUNCH("pscatter_kernel");
-    bool const     last = (L + 1) == cfg_.tp.max_depth;
-    uint32_t const nfb  = last ? 1 : n_sel_;
+    if (prof_ != nullptr)
+    {
+        phase_end(prof_->partition_ms);
+    }
+    n_launch_ += 6;
+    bool const     last    = (L + 1) == cfg_.tp.max_depth;
+    uint32_t const nfb     = last ? 1 : n_sel_;
     build(rows_out, nfb, nxt);
     uint32_t const n_cells = off_h_[nfb]; // the built features: a selection prefix
-    subtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
-        ctl_, bpair_, static_cast<float2 const *>(hist_[cur]), static_cast<float2 *>(hist_[nxt]),
-        total_cells_, n_cells, nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_,
-        cfg_.tp);
-    BB_LAUNCH("subtract_totals_kernel");
+    phase_begin();
+    if (quant_)
+    {
+        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
+            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells,
+            nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_);
+        BB_LAUNCH("qsubtract_totals_kernel");
+    }
+    else
+    {
+        subtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+            ctl_, bpair_, static_cast<float2 const *>(hist_[cur]),
+            static_cast<float2 *>(hist_[nxt]), total_cells_, n_cells, nodes_[cur],
+            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp);
+        BB_LAUNCH("subtract_totals_kernel");
+    }
     advance_kernel<<<1, 1, 0, s>>>(ctl_);
     BB_LAUNCH("advance_kernel");
+    n_launch_ += 2;
+    if (prof_ != nullptr)
+    {
+        phase_end(prof_->other_ms);
+    }
 }
 
 void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
-                  TreeOut const &t, uint32_t *leaf_id, float *scores, float lr)
+                  TreeOut const &t, uint32_t *leaf_id, float *scores, float lr,
+                  bool identity_root)
 {
     if (n_root > max_rows_)
     {
@@ -1330,13 +1939,42 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     }
     cudaStream_t s = stream_;
     gh_cur_        = gh;
+    root_rows_     = root_rows;
+    n_launch_      = 0;
+    if (quant_)
+    {
+        phase_begin();
+        quantise(gh, static_cast<uint32_t>(plane_.n_rows));
+        if (prof_ != nullptr)
+        {
+            phase_end(prof_->other_ms);
+        }
+    }
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t);
+                                              build_, t, crows_);
     BB_LAUNCH("root_setup_kernel");
-    build(root_rows, cfg_.tp.max_depth == 0 ? 1 : n_sel_, 0);
-    root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(hist_[0]),
-                                        sel_nb_);
-    BB_LAUNCH("root_totals_kernel");
+    n_launch_ += 1;
+    // the root's rows: the quantised build reads an identity list implicitly
+    build(quant_ && identity_root ? nullptr : root_rows,
+          cfg_.tp.max_depth == 0 ? 1 : n_sel_, 0);
+    phase_begin();
+    if (quant_)
+    {
+        qroot_totals_kernel<<<1, 32, 0, s>>>(
+            nodes_[0], static_cast<unsigned long long const *>(hist_[0]), sel_nb_);
+        BB_LAUNCH("qroot_totals_kernel");
+    }
+    else
+    {
+        root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(hist_[0]),
+                                            sel_nb_);
+        BB_LAUNCH("root_totals_kernel");
+    }
+    n_launch_ += 1;
+    if (prof_ != nullptr)
+    {
+        phase_end(prof_->other_ms);
+    }
     uint32_t const *rows_in = root_rows;
     for (uint32_t L = 0; L < cfg_.tp.max_depth; ++L)
     {
@@ -1344,19 +1982,76 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         level(L, rows_in, rows_out, t, leaf_id, scores, lr);
         rows_in = rows_out;
     }
+    phase_begin();
     int const fin = static_cast<int>(cfg_.tp.max_depth & 1);
-    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t);
+    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_);
     BB_LAUNCH("final_kernel");
-    final_stamp_kernel<<<ceil_div(max_rows_, k_threads), k_threads, 0, s>>>(
-        ctl_, nodes_[fin], rows_in, t, leaf_id, scores, lr);
-    BB_LAUNCH("final_stamp_kernel");
+    nodes_cur_ = nodes_[fin];
+    rows_cur_  = rows_in;
+    leaf_values(t, true);
+    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in, t,
+                                                    leaf_id, scores, lr);
+    BB_LAUNCH("stamp_kernel");
+    tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
+    BB_LAUNCH("tree_counter_kernel");
+    n_launch_ += 3;
+    if (prof_ != nullptr)
+    {
+        phase_end(prof_->other_ms);
+    }
+    launches_ = n_launch_;
     ++tree_no_;
 }
 
-} // namespace bb
-
-namespace bb
+void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double2 *out)
 {
+    cudaStream_t s = stream_;
+    gh_cur_        = gh;
+    root_rows_     = rows;
+    TreeOut t{};
+    std::vector<uint32_t> meta_dummy(3);
+    // a tree output the setup kernel may write node 0 into
+    uint32_t *scratch = dalloc<uint32_t>(64, s);
+    t.feature = t.left = t.right = t.split_bin = t.meta = scratch;
+    t.value = t.gain = t.cover = reinterpret_cast<float *>(scratch + 16);
+    t.default_left = reinterpret_cast<uint8_t *>(scratch + 32);
+    if (quant_)
+    {
+        quantise(gh, static_cast<uint32_t>(plane_.n_rows));
+    }
+    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n, bchunks_, brange_, build_,
+                                              t, crows_);
+    BB_LAUNCH("root_setup_kernel");
+    build(rows, n_sel_, 0);
+    std::vector<double2> cells(total_cells_);
+    if (quant_)
+    {
+        std::vector<unsigned long long> q(total_cells_);
+        double2                         sc{};
+        BB_CHECK(cudaMemcpyAsync(q.data(), hist_[0], total_cells_ * 8ULL, cudaMemcpyDeviceToHost, s));
+        BB_CHECK(cudaMemcpyAsync(&sc, qscale_, sizeof(double2), cudaMemcpyDeviceToHost, s));
+        BB_CHECK(cudaStreamSynchronize(s));
+        for (uint32_t x = 0; x < total_cells_; ++x)
+        {
+            out[x] = make_double2(static_cast<double>(static_cast<int32_t>(
+                                      static_cast<uint32_t>(q[x] >> 32))) * sc.x,
+                                  static_cast<double>(static_cast<uint32_t>(q[x])) * sc.y);
+        }
+    }
+    else
+    {
+        std::vector<float2> f(total_cells_);
+        BB_CHECK(cudaMemcpyAsync(f.data(), hist_[0], total_cells_ * 8ULL, cudaMemcpyDeviceToHost, s));
+        BB_CHECK(cudaStreamSynchronize(s));
+        for (uint32_t x = 0; x < total_cells_; ++x)
+        {
+            out[x] = make_double2(f[x].x, f[x].y);
+        }
+    }
+    BB_CHECK(cudaFreeAsync(scratch, s));
+    BB_CHECK(cudaStreamSynchronize(s));
+}
+
 void Grower::set_monotone(std::vector<int8_t> const &m)
 {
     if (mono_ != nullptr)
@@ -1373,4 +2068,5 @@ void Grower::set_monotone(std::vector<int8_t> const &m)
     BB_CHECK(cudaMemcpyAsync(mono_, m.data(), m.size(), cudaMemcpyHostToDevice, stream_));
     BB_CHECK(cudaStreamSynchronize(stream_));
 }
+
 } // namespace bb

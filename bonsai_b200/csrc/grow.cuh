@@ -27,6 +27,8 @@ struct Node
     float    sum_h;
     double   lo;
     double   hi;
+    int64_t  qg; // quantised form: exact integer totals
+    int64_t  qh;
 };
 
 // SplitOutput (include/bonsai/split.hpp:62-69), one per (node, feature)
@@ -85,6 +87,21 @@ enum class HistMode : int32_t
     quant16 = 2 // int16 gradients
 };
 
+// Per-phase device time of profiled trees (CUDA events on the grower's
+// stream) and the histogram build's algorithmic bytes: per built node,
+// rows x (features x bin bytes + 8 B gradient pair + 4 B row id) read plus
+// its cells written.
+struct Profile
+{
+    double   hist_ms      = 0.0;
+    double   partition_ms = 0.0;
+    double   find_ms      = 0.0;
+    double   other_ms     = 0.0;
+    double   hist_bytes   = 0.0;
+    uint64_t hist_rows    = 0;
+    uint32_t hist_builds  = 0;
+};
+
 struct GrowConfig
 {
     TreeParams tp;
@@ -107,7 +124,19 @@ class Grower
     // the tree; leaf_id (nullable) each sampled row's leaf; scores (nullable)
     // gets scores[r] += lr * leaf value for every sampled row.
     void grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
-              TreeOut const &out, uint32_t *leaf_id, float *scores, float lr);
+              TreeOut const &out, uint32_t *leaf_id, float *scores, float lr,
+              bool identity_root = false);
+
+    // One node's histograms (HistogramEngine::populate): quantises (when
+    // quantised) and builds every selected feature over the given rows;
+    // out receives total_cells (g, h) pairs as FP64 cell sums, scaled back
+    // from integers in the quantised form.
+    void populate(float2 const *gh, uint32_t const *rows, uint32_t n, double2 *out_host);
+
+    uint32_t total_cells() const
+    {
+        return total_cells_;
+    }
 
     uint32_t max_nodes() const
     {
@@ -173,7 +202,21 @@ class Grower
     // quantised form
     int32_t  *qgh_      = nullptr; // per row, packed (g, h) integers
     float2   *scale_    = nullptr;
-    uint32_t *absmax_   = nullptr;
+    uint32_t *absmax_   = nullptr; // max |g| and max h, as float bits
+    double2  *qscale_   = nullptr; // (scale_g, scale_h) in FP64
+    uint16_t *qgh8_     = nullptr; // per row: int8 g | uint8 h << 8
+    double2  *partial_  = nullptr; // per partition chunk: leaf (G, H) in FP64
+    uint32_t  crows_    = 0;       // rows per histogram-build chunk
+    bool      quant_    = false;
+    uint32_t *dtree_    = nullptr; // device tree counter (the rounding stream)
+    uint32_t *tile_ids_[2] = {nullptr, nullptr};
+    int32_t  *tile_j_[2]   = {nullptr, nullptr};
+    uint32_t  n_tiles_[2]  = {0, 0};
+    Node const     *nodes_cur_ = nullptr;
+    uint32_t const *rows_cur_  = nullptr;
+    uint32_t const *root_rows_ = nullptr;
+    void      quantise(float2 const *gh, uint32_t n);
+    void      leaf_values(TreeOut const &t, bool final_level);
     uint64_t  seed_     = 0;
     uint32_t  tree_no_  = 0;
 
@@ -184,6 +227,24 @@ class Grower
     }
     // per-feature monotone directions (+1 / -1 / 0), copied to the device
     void set_monotone(std::vector<int8_t> const &m);
+    // non-null: the next grow() calls time their phases into *p (synchronous)
+    void set_profile(Profile *p)
+    {
+        prof_ = p;
+    }
+    // kernel launches one grow() enqueues
+    uint32_t launches_per_tree() const
+    {
+        return launches_;
+    }
+
+  private:
+    Profile    *prof_     = nullptr;
+    uint32_t    launches_ = 0;
+    uint32_t    n_launch_ = 0;
+    cudaEvent_t pev_[2]   = {nullptr, nullptr};
+    void        phase_begin();
+    void        phase_end(double &acc);
 };
 
 } // namespace bb

@@ -124,7 +124,57 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// One thread per (row, tile): gathers the tile's codes from the
+// feature-major columns (coalesced across the warp's consecutive rows) and
+// writes the row's 32-byte tile as two 16-byte stores.
+template <typename BinT>
+__global__ void __launch_bounds__(k_threads)
+    mirror_kernel(BinT const *__restrict__ bins, uint64_t n_rows, uint64_t n_pad,
+                  uint32_t F, uint4 *__restrict__ mirror)
+{
+    constexpr uint32_t per = k_mirror_bytes / sizeof(BinT);
+    uint64_t const     r   = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
+    uint32_t const     t   = blockIdx.y;
+    if (r >= n_rows)
+    {
+        return;
+    }
+    alignas(16) BinT v[per];
+#pragma unroll
+    for (uint32_t k = 0; k < per; ++k)
+    {
+        uint32_t const f = (t * per) + k;
+        v[k]             = f < F ? bins[(static_cast<uint64_t>(f) * n_pad) + r] : BinT{0};
+    }
+    uint4 const   *src = reinterpret_cast<uint4 const *>(v);
+    uint64_t const o   = ((static_cast<uint64_t>(t) * n_rows) + r) * 2;
+    mirror[o]          = src[0];
+    mirror[o + 1]      = src[1];
+}
+
 } // namespace
+
+void build_mirror(Plane &p, cudaStream_t stream)
+{
+    uint32_t const per = k_mirror_bytes / (p.u8 ? 1 : 2);
+    p.n_tiles          = (p.n_feats + per - 1) / per;
+    size_t const bytes = static_cast<size_t>(p.n_tiles) * p.n_rows * k_mirror_bytes;
+    BB_CHECK(cudaMalloc(&p.mirror, bytes));
+    dim3 const grid(ceil_div(p.n_rows, k_threads), p.n_tiles);
+    if (p.u8)
+    {
+        mirror_kernel<uint8_t><<<grid, k_threads, 0, stream>>>(
+            static_cast<uint8_t const *>(p.bins), p.n_rows, p.n_pad, p.n_feats,
+            static_cast<uint4 *>(p.mirror));
+    }
+    else
+    {
+        mirror_kernel<uint16_t><<<grid, k_threads, 0, stream>>>(
+            static_cast<uint16_t const *>(p.bins), p.n_rows, p.n_pad, p.n_feats,
+            static_cast<uint4 *>(p.mirror));
+    }
+    BB_LAUNCH("mirror_kernel");
+}
 
 void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream)
 {

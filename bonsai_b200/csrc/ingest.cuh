@@ -24,6 +24,11 @@ struct Plane
     uint32_t  n_feats  = 0;
     bool      u8       = true;
     void     *bins     = nullptr; // uint8_t or uint16_t
+    // Row-major mirror for gathered reads: features in tiles of 32 bytes
+    // (32 u8 or 16 u16 codes), tile t of row r at mirror[(t * n_rows + r) * 32],
+    // so one gathered row costs one 32-byte DRAM sector per tile.
+    void     *mirror   = nullptr;
+    uint32_t  n_tiles  = 0;
     float    *cuts     = nullptr; // flattened cuts, device
     uint32_t *cut_off  = nullptr; // F + 1 offsets, device
     uint32_t *n_bins   = nullptr; // per feature, device
@@ -34,5 +39,10 @@ struct Plane
 };
 
 void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream);
+
+// Fills p.mirror from the feature-major codes (allocating it).
+void build_mirror(Plane &p, cudaStream_t stream);
+
+constexpr uint32_t k_mirror_bytes = 32;
 
 } // namespace bb

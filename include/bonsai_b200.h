@@ -133,6 +133,27 @@ int bb_booster_leaf_ids(bb_booster const *b, uint32_t *out);
 /* Device time of the last bb_booster_update, in milliseconds. */
 int bb_booster_last_ms(bb_booster const *b, float *ms);
 
+/* Per-phase device time of one profiled boosting round (the reference's
+ * BONSAI_CUDA_PROFILE counters, src/cuda/detail/profile.cuh:20-122): the
+ * round runs like any other (its tree is kept) but synchronises between
+ * phases to time them with CUDA events. hist_bytes are the histogram
+ * build's algorithmic bytes: per built node rows x (features x bin bytes +
+ * 8 B gradient pair + 4 B row id) plus the cells written. */
+typedef struct
+{
+    double   hist_ms;
+    double   partition_ms;
+    double   find_ms;
+    double   other_ms;
+    double   total_ms;
+    double   hist_bytes;
+    uint64_t hist_rows;
+    uint32_t hist_builds;
+    uint32_t launches; /* this library's kernel launches per round */
+} bb_profile;
+
+int bb_booster_profile_round(bb_booster *b, bb_profile *out);
+
 void bb_booster_destroy(bb_booster *b);
 
 /* One tree from caller-provided gradients: grad/hess (host, n_rows), the
@@ -148,6 +169,18 @@ int bb_grow_tree(bb_plane const *plane, bb_train_cfg const *cfg, float const *gr
                  uint8_t *default_left, float *gain, float *cover,
                  uint32_t *split_bin, uint32_t *meta, float *values,
                  uint32_t *leaf_ids);
+
+/* One node's histograms: every selected feature's cells over the given rows
+ * (host, ascending; NULL = all rows) from grad/hess (host, n_rows), written
+ * to out as (sum_g, sum_h) doubles per cell, features in selection order,
+ * n_bins(f) cells each (out holds the selection's total bins x 2). The
+ * plain form's cells are the serial-order float sums; the quantised form's
+ * are its exact integer sums times the round's FP64 scales.
+ * Replaces HistogramEngine::populate (include/bonsai/grower.hpp:78-84,
+ * CudaHistogramEngine::populate, histogram_engine.hpp:92-93). */
+int bb_populate(bb_plane const *plane, bb_train_cfg const *cfg, float const *grad,
+                float const *hess, uint32_t const *rows, uint64_t n_sel_rows,
+                double *out);
 
 /* ---- inference ------------------------------------------------------------
  * Ensemble predict over a plane: out[r] = init + lr * sum_t leaf_t(r), the

@@ -454,3 +454,21 @@ def orc_find_split(orc: "Oracle", hist, n_rows, tc: TreeCfg, tot=None, lo=-np.in
                              C.byref(cfg))
     return dict(gain=s.gain, feature=s.feature, bin=s.bin, default_left=s.default_left,
                 valid=s.valid)
+
+
+def orc_fill(orc: "Oracle", bins, n_bins, grad, hess, rows=None, selected=None):
+    """orc_fill: one node's serial-order float histograms, [total_bins, 2]."""
+    F, n = bins.shape
+    bins = np.ascontiguousarray(bins, np.uint16)
+    rows = np.arange(n, dtype=np.uint32) if rows is None else np.ascontiguousarray(rows, np.uint32)
+    selected = np.arange(F, dtype=np.uint32) if selected is None else np.ascontiguousarray(selected, np.uint32)
+    nb = np.ascontiguousarray(n_bins, np.uint32)
+    total = int(nb[selected].sum())
+    out = np.zeros((total, 2), np.float32)
+    grad = np.ascontiguousarray(grad, np.float32)
+    hess = np.ascontiguousarray(hess, np.float32)
+    orc.L.orc_fill(_p(bins, C.c_uint16), C.c_size_t(n), _p(selected, C.c_uint32),
+                   C.c_size_t(len(selected)), _p(nb, C.c_uint32), _p(grad, C.c_float),
+                   _p(hess, C.c_float), _p(rows, C.c_uint32), C.c_size_t(len(rows)),
+                   _p(out, C.c_float))
+    return out

@@ -1,0 +1,135 @@
+"""GPU tests of the quantised form: int8 stochastic-rounded gradients with
+exact integer histograms, FP64 gain and FP64 leaf renewal. Histogram error
+is stated against FP64 sums, model quality against the plain form."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import orc_fill
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(seed, n, F=10):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    X[rng.random((n, F)) < 0.05] = np.nan
+    g = rng.normal(0, 1, n).astype(np.float32)
+    h = rng.uniform(0.05, 0.25, n).astype(np.float32)
+    return X, g, h
+
+
+def test_populate_exact_is_the_serial_fill(bb, orc):
+    X, g, h = _data(1, 20000)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    rows = np.flatnonzero(np.random.Generator(np.random.PCG64(2)).random(len(g)) < 0.4)
+    got = bb.populate(plane, bb.TrainParams(), g, h, rows=rows)
+    want = orc_fill(orc, plane.bins(), np.diff(off), g, h, rows=rows)
+    assert np.array_equal(got.astype(np.float32), want)
+
+
+def _fp64_hist(bins, n_bins, g, h):
+    cells = []
+    for f in range(bins.shape[0]):
+        G = np.zeros(n_bins[f]); H = np.zeros(n_bins[f])
+        np.add.at(G, bins[f], g.astype(np.float64))
+        np.add.at(H, bins[f], h.astype(np.float64))
+        cells.append(np.stack([G, H], 1))
+    return np.concatenate(cells)
+
+
+def test_quantised_histogram_error_vs_fp64(bb):
+    X, g, h = _data(3, 400_000)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    nb = np.diff(off)
+    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=7), g, h)
+    ref = _fp64_hist(plane.bins(), nb, g, h)
+    sg = np.abs(g).max() / 127.0
+    sh = h.max() / 127.0
+    counts = np.concatenate([np.bincount(plane.bins()[f], minlength=nb[f]) for f in range(len(nb))])
+    # stochastic rounding: unbiased, per-row error below one scale step
+    err_g = np.abs(q[:, 0] - ref[:, 0])
+    err_h = np.abs(q[:, 1] - ref[:, 1])
+    assert np.all(err_g <= 6 * sg * np.sqrt(counts) + sg)
+    assert np.all(err_h <= 6 * sh * np.sqrt(counts) + sh)
+    # every feature sees the same rows: the integer totals agree exactly
+    # (cells are integer sums times the FP64 scale: recover the integers)
+    scale = np.array([np.abs(g).max() / 127.0, h.max() / 127.0])
+    ints = np.rint(q / scale)
+    tot = [ints[off[f]:off[f + 1]].sum(0) for f in range(len(nb))]
+    assert all(np.array_equal(tot[0], t) for t in tot)
+    tot = [q[off[0]:off[1]].sum(0)]
+    rel = abs(tot[0][0] - g.astype(np.float64).sum()) / np.abs(g).sum()
+    assert rel < 1e-3
+
+
+def test_quantised_seeded_and_deterministic(bb):
+    X, g, h = _data(4, 100_000)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    y = (g > 0).astype(np.float32)
+    def fit(seed, graph):
+        b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=6,
+                                                 hist_mode="int8", seed=seed,
+                                                 use_graph=graph), max_trees=8)
+        b.update(8)
+        return b.scores(), [b.tree(i) for i in range(8)]
+    s1, t1 = fit(11, False)
+    s2, t2 = fit(11, True)
+    s3, _ = fit(12, False)
+    assert np.array_equal(s1, s2)
+    for a, c in zip(t1, t2):
+        assert np.array_equal(a.feature, c.feature) and np.array_equal(a.value, c.value)
+    assert not np.array_equal(s1, s3)
+
+
+def _auc(y, p):
+    order = np.argsort(p, kind="stable")
+    ranks = np.empty(len(p)); ranks[order] = np.arange(1, len(p) + 1)
+    pos = y > 0.5
+    n1, n0 = pos.sum(), (~pos).sum()
+    return (ranks[pos].sum() - n1 * (n1 + 1) / 2) / (n1 * n0)
+
+
+def test_quantised_auc_matches_plain_on_tall_binary_subset(bb):
+    """HIGGS-shaped 1M-row subset, depth 8, 100 rounds: the quantised fit's
+    validation AUC within 1e-3 of the plain form's."""
+    from bonsai_b200 import synth
+    X, y = synth.tall_binary(n=1_200_000)
+    Xt, yt, Xv, yv = X[:1_000_000], y[:1_000_000], X[1_000_000:], y[1_000_000:]
+    cuts, off = bb.fit_cuts(Xt)
+    pt = bb.Plane(Xt, cuts, off)
+    pv = bb.Plane(Xv, cuts, off)
+    aucs = {}
+    for mode in ("exact", "int8"):
+        b = bb.Booster(pt, yt, bb.TrainParams(objective="logloss", max_depth=8,
+                                               learning_rate=0.1, hist_mode=mode, seed=1,
+                                               use_graph=True), max_trees=100)
+        b.update(100)
+        aucs[mode] = _auc(yv, bb.predict(pv, b.trees(), b.init_score, 0.1))
+    assert aucs["exact"] > 0.7
+    assert abs(aucs["int8"] - aucs["exact"]) <= 1e-3, aucs
+
+
+def test_quantised_large_invariants(bb):
+    rng = np.random.Generator(np.random.PCG64(5))
+    n, F = 2_000_000, 28
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    y = (X[:, 0] + X[:, 1] * X[:, 2] > 0).astype(np.float32)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=8,
+                                             hist_mode="int8"), max_trees=3)
+    b.update(3)
+    trees = b.trees()
+    for t in trees:
+        for i in np.flatnonzero(t.feature != bb.LEAF):
+            assert t.covers[t.left[i]] + t.covers[t.right[i]] == t.covers[i]
+    s = np.full(n, np.float32(b.init_score), np.float32)
+    for t in trees:
+        s = (s + np.float32(0.1) * bb.predict(plane, [t], 0.0, 1.0)).astype(np.float32)
+    np.testing.assert_array_equal(b.scores(), s)
