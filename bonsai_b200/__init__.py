@@ -56,6 +56,7 @@ class TrainParams:
     monotone: list = field(default_factory=list)
     selected: list | None = None
     use_graph: bool = False
+    record_leaf_ids: bool = False
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -70,6 +71,7 @@ class TrainParams:
         c.hist_mode = HIST_MODES[self.hist_mode]
         c.seed = self.seed
         c.use_graph = 1 if self.use_graph else 0
+        c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:
             c._mono = np.ascontiguousarray(self.monotone, dtype=np.int8)
             c.monotone = c._mono.ctypes.data_as(C.POINTER(C.c_int8))

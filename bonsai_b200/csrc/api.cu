@@ -301,6 +301,7 @@ struct bb_booster
     bb::TreeStore               trees;
     uint32_t                    n_trees = 0;
     bool                        use_graph = false;
+    bool                        record_leaf_ids = false;
     cudaGraphExec_t             graph     = nullptr;
     cudaEvent_t                 ev0{}, ev1{};
     float                       last_ms = 0.0F;
@@ -310,7 +311,8 @@ struct bb_booster
         uint64_t const n = plane->n_rows;
         gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
         BB_LAUNCH("gradient_kernel");
-        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t, leaf_id, scores, lr, true);
+        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
+                     record_leaf_ids ? leaf_id : nullptr, scores, lr, true);
         commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
         BB_LAUNCH("commit_tree_kernel");
     }
@@ -517,7 +519,8 @@ extern "C"
                 b->grower->set_seed(cfg->seed);
                 b->scratch.alloc(b->grower->max_nodes(), 1);
                 b->trees.alloc(b->grower->max_nodes(), max_trees);
-                b->use_graph = cfg->use_graph != 0;
+                b->use_graph       = cfg->use_graph != 0;
+                b->record_leaf_ids = cfg->record_leaf_ids != 0;
                 BB_CHECK(cudaEventCreate(&b->ev0));
                 BB_CHECK(cudaEventCreate(&b->ev1));
                 BB_CHECK(cudaStreamSynchronize(b->stream));
@@ -626,6 +629,7 @@ extern "C"
         return guarded(
             [&]
             {
+                need(b->record_leaf_ids, "bb_booster_leaf_ids: create with record_leaf_ids");
                 BB_CHECK(cudaStreamSynchronize(b->stream));
                 BB_CHECK(cudaMemcpy(out, b->leaf_id, b->plane->n_rows * 4, cudaMemcpyDeviceToHost));
             });

@@ -32,7 +32,9 @@ namespace
 constexpr uint32_t k_threads    = 256;
 constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
 constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk (exact)
-constexpr uint32_t k_qbuild_rows = 32768; // rows per histogram-build chunk (quantised)
+constexpr uint32_t k_qbuild_rows = 8192;  // rows per histogram-build chunk (quantised)
+constexpr uint32_t k_qthreads    = 512;   // threads per quantised-histogram CTA
+constexpr uint32_t k_tthreads    = 512;   // threads per conflict-free (u8) histogram CTA
 constexpr uint32_t k_warps_feat = 8;    // features per count/scatter CTA
 constexpr uint32_t k_find_warps = 4;    // features per find CTA
 constexpr uint32_t k_chain_stg  = 32;   // elements per lane per cp.async stage
@@ -667,6 +669,41 @@ __global__ void __launch_bounds__(32 * k_find_warps)
     }
 }
 
+
+// Cuts n row segments into chunks of `rows` rows with the whole block:
+// segment i owns chunks [range[i], range[i + 1]); chunk c finds its segment
+// by binary search (range is in global memory, written before a barrier).
+// seg(i, start, count, aux) describes segment i.
+template <typename Seg>
+__device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *range,
+                                                 uint32_t total, uint32_t rows, Seg seg,
+                                                 Chunk *out)
+{
+    for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
+    {
+        uint32_t lo = 0;
+        uint32_t hi = n;
+        while (hi - lo > 1)
+        {
+            uint32_t const mid = (lo + hi) >> 1;
+            if (range[mid] <= c)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid;
+            }
+        }
+        uint32_t start = 0;
+        uint32_t count = 0;
+        uint32_t aux   = 0;
+        seg(lo, start, count, aux);
+        uint32_t const b = (c - range[lo]) * rows;
+        out[c]           = {lo, start + b, min(rows, count - b), aux};
+    }
+}
+
 // ------------------------------------------------------------- planning ----
 
 __global__ void __launch_bounds__(k_plan_thr)
@@ -742,11 +779,6 @@ __global__ void __launch_bounds__(k_plan_thr)
     if (live)
     {
         pcr[i] = c0;
-        for (uint32_t c = 0; c < nch; ++c)
-        {
-            uint32_t const b = c * k_part_rows;
-            pchunks[c0 + c]  = {i, nd.start + b, min(k_part_rows, nd.count - b), 0};
-        }
     }
     if (i == 0)
     {
@@ -755,16 +787,34 @@ __global__ void __launch_bounds__(k_plan_thr)
         ctl->n_nodes    = n_nodes0 + (2 * n_split_total);
         ctl->n_leaves  += n_cur - n_split_total;
     }
+    __syncthreads();
+    fill_chunk_table(
+        n_cur, pcr, total, k_part_rows,
+        [&](uint32_t x, uint32_t &st, uint32_t &cnt, uint32_t &aux)
+        {
+            Node const nx = nodes[x];
+            st            = nx.start;
+            cnt           = nx.count;
+            aux           = 0;
+        },
+        pchunks);
 }
+
+// Partition pass 1: each warp routes a contiguous run of the chunk's rows
+// (lanes = consecutive rows, coalesced), keeps the directions as a bitmask
+// (one word per 32 rows) so pass 2 never re-reads the bins, and the block
+// sums the left counts.
+constexpr uint32_t k_warp_rows = k_part_rows / (k_threads / 32); // 512
 
 template <typename BinT>
 __global__ void __launch_bounds__(k_threads)
     pcount_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
                   Best const *best, uint32_t const *rows, void const *bins,
                   uint64_t n_pad, uint32_t const *sel, uint32_t const *sel_nb,
-                  uint32_t *pleft)
+                  uint32_t *pleft, uint32_t *dirs)
 {
-    uint32_t const c = blockIdx.x;
+    __shared__ uint32_t wsum[k_threads / 32];
+    uint32_t const      c = blockIdx.x;
     if (c >= ctl->n_pchunks)
     {
         return;
@@ -772,22 +822,49 @@ __global__ void __launch_bounds__(k_threads)
     Chunk const ch = pchunks[c];
     if ((nodes[ch.node].flags & 1) == 0)
     {
+        if (threadIdx.x == 0)
+        {
+            pleft[c] = 0; // a leaf's chunk routes nothing
+        }
         return;
     }
     Best const     bs   = best[ch.node];
     uint32_t const f    = sel[bs.feature];
     uint32_t const last = sel_nb[bs.feature] - 1;
+    BinT const    *col  = static_cast<BinT const *>(bins) + (static_cast<uint64_t>(f) * n_pad);
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t      *dw   = dirs + (static_cast<uint64_t>(c) * (k_part_rows / 32));
     uint32_t       n    = 0;
-    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+#pragma unroll 4
+    for (uint32_t s = 0; s < k_warp_rows; s += 32)
     {
-        uint32_t const b = bin_at<BinT>(bins, n_pad, f, rows[ch.begin + k]);
-        n += routes_left(b, last, bs.bin, bs.dl != 0) ? 1 : 0;
+        uint32_t const k  = (w * k_warp_rows) + s + lane;
+        bool           lf = false;
+        if (k < ch.count)
+        {
+            lf = routes_left(col[rows[ch.begin + k]], last, bs.bin, bs.dl != 0);
+        }
+        uint32_t const m = __ballot_sync(0xFFFFFFFFu, lf);
+        if (lane == 0)
+        {
+            dw[((w * k_warp_rows) + s) / 32] = m;
+        }
+        n += __popc(m);
     }
-    uint32_t total = 0;
-    block_excl_scan<k_threads>(n, &total);
+    if (lane == 0)
+    {
+        wsum[w] = n;
+    }
+    __syncthreads();
     if (threadIdx.x == 0)
     {
-        pleft[c] = total;
+        uint32_t t = 0;
+        for (uint32_t x = 0; x < k_threads / 32; ++x)
+        {
+            t += wsum[x];
+        }
+        pleft[c] = t;
     }
 }
 
@@ -796,58 +873,48 @@ __global__ void __launch_bounds__(k_plan_thr)
                  Chunk const *pchunks, uint32_t const *pcr, uint32_t *pleft,
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
-                 TreeOut t, uint32_t crows)
+                 TreeOut t, uint32_t crows, uint32_t *bbase)
 {
-    uint32_t const n_cur = ctl->n_cur;
-    uint32_t const lane  = threadIdx.x & 31;
-    uint32_t const w     = threadIdx.x >> 5;
-    // per split node: left count and each chunk's left/right write base
-    for (uint32_t i = w; i < n_cur; i += k_plan_thr / 32)
+    __shared__ uint32_t grand_s;
+    uint32_t const      n_cur = ctl->n_cur;
+    uint32_t const      n_ch  = ctl->n_pchunks;
+    // A. exclusive prefix of the chunks' left counts over the whole level
+    //    (leaf chunks count zero), each thread a contiguous run of chunks
+    uint32_t const per = (n_ch + k_plan_thr - 1) / k_plan_thr;
+    uint32_t const c_a = min(n_ch, threadIdx.x * per);
+    uint32_t const c_b = min(n_ch, c_a + per);
+    uint32_t       sum = 0;
+    for (uint32_t c = c_a; c < c_b; ++c)
     {
-        Node const nd = nodes[i];
-        if ((nd.flags & 1) == 0)
-        {
-            continue;
-        }
-        uint32_t const c0  = pcr[i];
-        uint32_t const c1  = pcr[i + 1];
-        uint32_t       run = 0;
-        for (uint32_t cb = c0; cb < c1; cb += 32)
-        {
-            uint32_t const c = cb + lane;
-            uint32_t const v = c < c1 ? pleft[c] : 0;
-            uint32_t       x = v;
-#pragma unroll
-            for (uint32_t o = 1; o < 32; o <<= 1)
-            {
-                uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if (lane >= o)
-                {
-                    x += y;
-                }
-            }
-            uint32_t const ex = run + x - v;
-            if (c < c1)
-            {
-                pleft[c]  = ex;
-                prbase[c] = (pchunks[c].begin - nd.start) - ex;
-            }
-            run += __shfl_sync(0xFFFFFFFFu, x, 31);
-        }
-        if (lane == 0)
-        {
-            nleft[i] = run;
-        }
+        sum += pleft[c];
+    }
+    uint32_t       grand = 0;
+    uint32_t const base  = block_excl_scan<k_plan_thr>(sum, &grand);
+    for (uint32_t c = c_a, run = base; c < c_b; ++c)
+    {
+        uint32_t const v = pleft[c];
+        pleft[c]         = run;
+        run += v;
+    }
+    if (threadIdx.x == 0)
+    {
+        grand_s = grand;
     }
     __syncthreads();
+    // B. per split node: its left count, or demotion when a side is empty
     uint32_t const i    = threadIdx.x;
     bool const     live = i < n_cur;
     Node           nd   = live ? nodes[i] : Node{};
     bool           surv = false;
     uint32_t       nl   = 0;
+    uint32_t       p0   = 0;
     if (live && (nd.flags & 1) != 0)
     {
-        nl = nleft[i];
+        uint32_t const c0 = pcr[i];
+        uint32_t const c1 = pcr[i + 1];
+        p0                = pleft[c0];
+        nl                = (c1 < n_ch ? pleft[c1] : grand_s) - p0;
+        nleft[i]          = nl;
         if (nl == 0 || nl == nd.count)
         {
             // demote_empty_splits: the parent is a leaf after all
@@ -861,12 +928,30 @@ __global__ void __launch_bounds__(k_plan_thr)
             surv = true;
         }
     }
-    uint32_t       n_surv = 0;
-    uint32_t const k      = block_excl_scan<k_plan_thr>(surv ? 1 : 0, &n_surv);
+    if (live)
+    {
+        dst[i] = p0; // the node's prefix origin, consumed by C below
+    }
+    __syncthreads();
+    // C. per chunk of a split node: its left and right write bases
+    for (uint32_t c = threadIdx.x; c < n_ch; c += k_plan_thr)
+    {
+        Chunk const ch = pchunks[c];
+        Node const  nx = nodes[ch.node];
+        if ((nx.flags & 1) != 0 && (nx.flags & 2) == 0)
+        {
+            uint32_t const lb = pleft[c] - dst[ch.node];
+            pleft[c]          = lb;
+            prbase[c]         = (ch.begin - nx.start) - lb;
+        }
+    }
+    __syncthreads();
+    // D. survivors: their children in the next frontier, and the chunk table
+    //    of the smaller children whose histograms are built
+    uint32_t       n_surv     = 0;
+    uint32_t const k          = block_excl_scan<k_plan_thr>(surv ? 1 : 0, &n_surv);
     uint32_t       rows_total = 0;
     uint32_t const start = block_excl_scan<k_plan_thr>(surv ? nd.count : 0, &rows_total);
-    uint32_t const n_demoted_before = 0;
-    (void)n_demoted_before;
     uint32_t small_count = 0;
     if (surv)
     {
@@ -874,8 +959,8 @@ __global__ void __launch_bounds__(k_plan_thr)
         uint32_t const nr   = nd.count - nl;
         uint32_t const lid  = t.left[nd.id];
         uint32_t const rid  = t.right[nd.id];
-        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi};
-        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi};
+        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0};
+        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0};
         next[2 * k]         = L;
         next[(2 * k) + 1]   = R;
         t.cover[lid]        = static_cast<float>(nl);
@@ -887,7 +972,6 @@ __global__ void __launch_bounds__(k_plan_thr)
         build[k]            = (2 * k) + (left_sm ? 0 : 1);
         small_count         = left_sm ? nl : nr;
     }
-    // histogram-build chunk table over the smaller children
     uint32_t const nch   = surv ? (small_count + crows - 1) / crows : 0;
     uint32_t       nch_t = 0;
     uint32_t const c0    = block_excl_scan<k_plan_thr>(nch, &nch_t);
@@ -895,21 +979,13 @@ __global__ void __launch_bounds__(k_plan_thr)
     uint32_t const pbase = block_excl_scan<k_plan_thr>(small_count, &built);
     if (surv)
     {
-        uint32_t const sst = (nl <= nd.count - nl) ? start : start + nl;
-        brange[k]          = c0;
-        for (uint32_t c = 0; c < nch; ++c)
-        {
-            uint32_t const b = c * crows;
-            bchunks[c0 + c]  = {k, sst + b, min(crows, small_count - b), pbase};
-        }
+        brange[k] = c0;
+        bbase[k]  = pbase; // the built node's payload base
     }
+    uint32_t n_dem = 0;
+    block_excl_scan<k_plan_thr>((live && (nd.flags & 2) != 0) ? 1 : 0, &n_dem);
     if (i == 0)
     {
-        uint32_t n_dem = 0;
-        for (uint32_t x = 0; x < n_cur; ++x)
-        {
-            n_dem += (nodes[x].flags & 2) != 0 ? 1 : 0;
-        }
         brange[n_surv]  = nch_t;
         ctl->n_leaves  += n_dem;
         ctl->n_next     = 2 * n_surv;
@@ -922,6 +998,17 @@ __global__ void __launch_bounds__(k_plan_thr)
             ctl->depth += 1;
         }
     }
+    __syncthreads();
+    fill_chunk_table(
+        n_surv, brange, nch_t, crows,
+        [&](uint32_t x, uint32_t &st, uint32_t &cnt, uint32_t &aux)
+        {
+            Node const sm = next[build[x]];
+            st            = sm.start;
+            cnt           = sm.count;
+            aux           = bbase[x];
+        },
+        bchunks);
 }
 
 // Rows of this level's leaves (never split, or demoted): their leaf id and
@@ -957,17 +1044,18 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
-// Stable scatter of a split node's chunk: lefts keep their order at
-// dst + left base, rights at dst + n_left + right base.
-template <typename BinT>
+// Partition pass 2, the stable scatter: lefts keep their order at
+// dst + left base, rights at dst + n_left + right base. Each warp takes the
+// same run of rows as pass 1, its base from the bitmask's popcounts (one
+// block barrier), its in-warp ranks from the bitmask words.
 __global__ void __launch_bounds__(k_threads)
     pscatter_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
                     Best const *best, uint32_t const *pleft, uint32_t const *prbase,
                     uint32_t const *nleft, uint32_t const *dst, uint32_t const *rows,
-                    uint32_t *rows_out, void const *bins, uint64_t n_pad,
-                    uint32_t const *sel, uint32_t const *sel_nb)
+                    uint32_t *rows_out, uint32_t const *dirs)
 {
-    uint32_t const c = blockIdx.x;
+    __shared__ uint32_t wsum[k_threads / 32];
+    uint32_t const      c = blockIdx.x;
     if (c >= ctl->n_pchunks)
     {
         return;
@@ -978,34 +1066,57 @@ __global__ void __launch_bounds__(k_threads)
     {
         return;
     }
-    Best const     bs   = best[ch.node];
-    uint32_t const f    = sel[bs.feature];
-    uint32_t const last = sel_nb[bs.feature] - 1;
-    uint32_t const d0   = dst[ch.node];
-    uint32_t const nl   = nleft[ch.node];
-    uint32_t       lb   = d0 + pleft[c];
-    uint32_t       rb   = d0 + nl + prbase[c];
-    for (uint32_t k0 = 0; k0 < ch.count; k0 += k_threads)
+    uint32_t const  lane = threadIdx.x & 31;
+    uint32_t const  w    = threadIdx.x >> 5;
+    uint32_t const *dw   = dirs + (static_cast<uint64_t>(c) * (k_part_rows / 32)) +
+                         ((w * k_warp_rows) / 32);
+    // this warp's left count
+    uint32_t mine = 0;
+    if (lane < k_warp_rows / 32)
     {
-        uint32_t const k     = k0 + threadIdx.x;
-        bool const     valid = k < ch.count;
-        uint32_t       r     = 0;
-        bool           left  = false;
-        if (valid)
+        mine = __popc(dw[lane]);
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        mine += __shfl_xor_sync(0xFFFFFFFFu, mine, o);
+    }
+    if (lane == 0)
+    {
+        wsum[w] = mine;
+    }
+    __syncthreads();
+    uint32_t lb = 0;
+    for (uint32_t x = 0; x < w; ++x)
+    {
+        lb += wsum[x];
+    }
+    uint32_t const w0  = w * k_warp_rows;
+    uint32_t const d0  = dst[ch.node];
+    uint32_t       lo  = d0 + pleft[c] + lb;                                   // next left
+    uint32_t       ro  = d0 + nleft[ch.node] + prbase[c] + (min(w0, ch.count) - lb); // next right
+    uint32_t const ltm = (1u << lane) - 1u;
+    for (uint32_t s = 0; s < k_warp_rows && w0 + s < ch.count; s += 32)
+    {
+        uint32_t const k = w0 + s + lane;
+        uint32_t const m = dw[s / 32];
+        uint32_t const nvalid = min(32u, ch.count - (w0 + s));
+        uint32_t const vm     = nvalid == 32 ? 0xFFFFFFFFu : ((1u << nvalid) - 1u);
+        uint32_t const lm     = m & vm;
+        if (k < ch.count)
         {
-            r    = rows[ch.begin + k];
-            left = routes_left(bin_at<BinT>(bins, n_pad, f, r), last, bs.bin, bs.dl != 0);
+            uint32_t const r = rows[ch.begin + k];
+            if ((m >> lane) & 1u)
+            {
+                rows_out[lo + __popc(lm & ltm)] = r;
+            }
+            else
+            {
+                rows_out[ro + __popc(~lm & vm & ltm)] = r;
+            }
         }
-        uint32_t       n_l = 0;
-        uint32_t const lr  = block_excl_scan<k_threads>(left ? 1 : 0, &n_l);
-        if (valid)
-        {
-            uint32_t const rr = threadIdx.x - lr;
-            rows_out[left ? lb + lr : rb + rr] = r;
-        }
-        uint32_t const tile = min(k_threads, ch.count - k0);
-        lb += n_l;
-        rb += tile - n_l;
+        lo += __popc(lm);
+        ro += nvalid - __popc(lm);
     }
 }
 
@@ -1094,11 +1205,6 @@ __global__ void __launch_bounds__(k_plan_thr)
     if (live)
     {
         pcr[i] = c0;
-        for (uint32_t c = 0; c < nch; ++c)
-        {
-            uint32_t const b = c * k_part_rows;
-            pchunks[c0 + c]  = {i, nd.start + b, min(k_part_rows, nd.count - b), 0};
-        }
     }
     if (i == 0)
     {
@@ -1109,6 +1215,17 @@ __global__ void __launch_bounds__(k_plan_thr)
         t.meta[1]       = ctl->depth;
         t.meta[2]       = ctl->n_leaves;
     }
+    __syncthreads();
+    fill_chunk_table(
+        n, pcr, total, k_part_rows,
+        [&](uint32_t x, uint32_t &st, uint32_t &cnt, uint32_t &aux)
+        {
+            Node const nx = nodes[x];
+            st            = nx.start;
+            cnt           = nx.count;
+            aux           = 0;
+        },
+        pchunks);
 }
 
 
@@ -1235,73 +1352,208 @@ __global__ void __launch_bounds__(k_threads)
 }
 
 // Exact integer histogram of a chunk of a built node's rows over one mirror
-// tile: one gathered 32-byte sector per row, one packed 64-bit
-// shared-memory add per (row, feature) -- the gradient in the high word
-// (two's complement), the hessian in the low word -- then one global add
-// per touched cell. grid (chunks, tiles), 256 threads.
+// tile: one gathered 32-byte sector per row, two native 32-bit
+// shared-memory adds per (row, feature) -- the gradient word signed, the
+// hessian word unsigned; a chunk's sums stay below 2^31 since a chunk holds
+// at most 32,768 rows of |q| <= 127 -- then one packed 64-bit global add per
+// touched cell (gradient in the high word, two's complement; hessian in the
+// low word). grid (chunks, tiles), 256 threads.
 template <typename BinT>
-__global__ void __launch_bounds__(k_threads)
+__global__ void __launch_bounds__(k_qthreads, 3)
     qhist_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
                  uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
                  uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
                  int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
                  uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
-    constexpr uint32_t        per = k_mirror_bytes / sizeof(BinT);
-    extern __shared__ unsigned long long h_s[]; // [per][max_nb]
+    constexpr uint32_t per = k_mirror_bytes / sizeof(BinT);
+    constexpr uint32_t U   = 2; // rows in flight per thread
+    extern __shared__ int32_t hq_s[]; // [per][max_nb] gradient words, then hessian words
     __shared__ int32_t        j_s[per];
     uint32_t const            c = blockIdx.x;
     if (c >= ctl->n_bchunks)
     {
         return;
     }
-    uint32_t const tile = tile_ids[blockIdx.y];
+    uint32_t const tile  = tile_ids[blockIdx.y];
+    uint32_t const cells = per * max_nb;
+    int32_t       *hg_s  = hq_s;
+    uint32_t      *hh_s  = reinterpret_cast<uint32_t *>(hq_s + cells);
     if (threadIdx.x < per)
     {
         j_s[threadIdx.x] = tile_j[(blockIdx.y * per) + threadIdx.x];
     }
-    for (uint32_t x = threadIdx.x; x < per * max_nb; x += k_threads)
+    for (uint32_t x = threadIdx.x; x < 2 * cells; x += k_qthreads)
     {
-        h_s[x] = 0ULL;
+        hq_s[x] = 0;
     }
     __syncthreads();
-    Chunk const   ch  = bchunks[c];
-    uint4 const  *mt  = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
-    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    Chunk const  ch = bchunks[c];
+    uint4 const *mt = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
+    for (uint32_t k0 = threadIdx.x; k0 < ch.count; k0 += k_qthreads * U)
     {
-        uint32_t const r = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
-        uint32_t const q = qgh[r];
-        unsigned long long const packed =
-            (static_cast<unsigned long long>(static_cast<uint32_t>(
-                 static_cast<int32_t>(static_cast<int8_t>(q & 0xFFu))))
-             << 32) |
-            static_cast<unsigned long long>(q >> 8);
-        uint4 const    a = mt[static_cast<uint64_t>(r) * 2];
-        uint4 const    b = mt[(static_cast<uint64_t>(r) * 2) + 1];
-        alignas(16) uint4 v[2] = {a, b};
-        BinT const    *bins = reinterpret_cast<BinT const *>(v);
+        uint32_t r[U];
+        bool     ok[U];
 #pragma unroll
-        for (uint32_t i = 0; i < per; ++i)
+        for (uint32_t u = 0; u < U; ++u)
         {
-            if (j_s[i] >= 0)
+            uint32_t const k = k0 + (u * k_qthreads);
+            ok[u]            = k < ch.count;
+            r[u]             = ok[u] ? (rows != nullptr ? rows[ch.begin + k] : ch.begin + k) : 0;
+        }
+        uint4    va[U];
+        uint4    vb[U];
+        uint32_t q[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u)
+        {
+            if (ok[u])
             {
-                atomicAdd(&h_s[(i * max_nb) + bins[i]], packed);
+                q[u]  = qgh[r[u]];
+                va[u] = mt[static_cast<uint64_t>(r[u]) * 2];
+                vb[u] = mt[(static_cast<uint64_t>(r[u]) * 2) + 1];
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u)
+        {
+            if (!ok[u])
+            {
+                continue;
+            }
+            int32_t const  qg   = static_cast<int8_t>(q[u] & 0xFFu);
+            uint32_t const qh   = q[u] >> 8;
+            uint32_t const w[8] = {va[u].x, va[u].y, va[u].z, va[u].w,
+                                   vb[u].x, vb[u].y, vb[u].z, vb[u].w};
+#pragma unroll
+            for (uint32_t i = 0; i < per; ++i)
+            {
+                if (j_s[i] >= 0)
+                {
+                    uint32_t const bin =
+                        sizeof(BinT) == 1 ? (w[i >> 2] >> ((i & 3) * 8)) & 0xFFu
+                                          : (w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+                    uint32_t const x = (i * max_nb) + bin;
+                    atomicAdd(&hg_s[x], qg);
+                    atomicAdd(&hh_s[x], qh);
+                }
             }
         }
     }
     __syncthreads();
     unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells);
-    for (uint32_t x = threadIdx.x; x < per * max_nb; x += k_threads)
+    for (uint32_t x = threadIdx.x; x < cells; x += k_qthreads)
     {
         uint32_t const i  = x / max_nb;
         uint32_t const bb = x % max_nb;
         int32_t const  jj = j_s[i];
         if (jj >= 0 && bb < sel_nb[jj])
         {
-            unsigned long long const v = h_s[x];
+            unsigned long long const v =
+                (static_cast<unsigned long long>(static_cast<uint32_t>(hg_s[x])) << 32) +
+                static_cast<unsigned long long>(hh_s[x]);
             if (v != 0ULL)
             {
                 atomicAdd(&dst[cell_off[jj] + bb], v);
+            }
+        }
+    }
+}
+
+
+// The u8 form of the quantised histogram, bank-conflict free: a warp stages
+// 32 rows' 32-byte tiles in shared memory, then walks them row by row with
+// lane l adding feature l. Cells are laid out [bin][32 features], so lane l
+// always lands in bank l whatever the bins. Same cells, same integer sums
+// as qhist_kernel. grid (chunks, tiles), k_tthreads threads.
+__global__ void __launch_bounds__(k_tthreads, 2)
+    qhist_t_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
+                   uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                   uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
+                   int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
+                   uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
+{
+    extern __shared__ uint4 t_smem[];
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_bchunks)
+    {
+        return;
+    }
+    uint32_t const lane   = threadIdx.x & 31;
+    uint32_t const w      = threadIdx.x >> 5;
+    uint32_t const cells  = 32 * max_nb;
+    auto          *hg_s   = reinterpret_cast<int32_t *>(t_smem);        // [bin][32]
+    auto          *hh_s   = reinterpret_cast<uint32_t *>(hg_s + cells); // [bin][32]
+    auto          *stage  = reinterpret_cast<uint4 *>(hh_s + cells) + (w * 64); // 32 rows x 32 B
+    auto const    *st_b   = reinterpret_cast<uint8_t const *>(stage);
+    uint32_t const tile   = tile_ids[blockIdx.y];
+    int32_t const  jj     = tile_j[(blockIdx.y * 32) + lane];
+    for (uint32_t x = threadIdx.x; x < 2 * cells; x += k_tthreads)
+    {
+        hg_s[x] = 0;
+    }
+    __syncthreads();
+    Chunk const  ch = bchunks[c];
+    uint4 const *mt = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
+    for (uint32_t k0 = w * 32; k0 < ch.count; k0 += k_tthreads)
+    {
+        uint32_t const k  = k0 + lane;
+        uint32_t const nr = min(32u, ch.count - k0);
+        uint32_t       q  = 0;
+        if (k < ch.count)
+        {
+            uint32_t const r = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
+            q                = qgh[r];
+            stage[2 * lane]       = mt[static_cast<uint64_t>(r) * 2];
+            stage[(2 * lane) + 1] = mt[(static_cast<uint64_t>(r) * 2) + 1];
+        }
+        __syncwarp();
+        if (nr == 32)
+        {
+#pragma unroll 8
+            for (uint32_t j = 0; j < 32; ++j)
+            {
+                uint32_t const qj  = __shfl_sync(0xFFFFFFFFu, q, j);
+                uint32_t const bin = st_b[(j * 32) + lane];
+                if (jj >= 0)
+                {
+                    atomicAdd(&hg_s[(bin * 32) + lane],
+                              static_cast<int32_t>(static_cast<int8_t>(qj & 0xFFu)));
+                    atomicAdd(&hh_s[(bin * 32) + lane], qj >> 8);
+                }
+            }
+        }
+        else
+        {
+            for (uint32_t j = 0; j < nr; ++j)
+            {
+                uint32_t const qj  = __shfl_sync(0xFFFFFFFFu, q, j);
+                uint32_t const bin = st_b[(j * 32) + lane];
+                if (jj >= 0)
+                {
+                    atomicAdd(&hg_s[(bin * 32) + lane],
+                              static_cast<int32_t>(static_cast<int8_t>(qj & 0xFFu)));
+                    atomicAdd(&hh_s[(bin * 32) + lane], qj >> 8);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells);
+    for (uint32_t x = threadIdx.x; x < cells; x += k_tthreads)
+    {
+        uint32_t const f  = x & 31;
+        uint32_t const bb = x >> 5;
+        int32_t const  j2 = tile_j[(blockIdx.y * 32) + f];
+        if (j2 >= 0 && bb < sel_nb[j2])
+        {
+            unsigned long long const v =
+                (static_cast<unsigned long long>(static_cast<uint32_t>(hg_s[x])) << 32) +
+                static_cast<unsigned long long>(hh_s[x]);
+            if (v != 0ULL)
+            {
+                atomicAdd(&dst[cell_off[j2] + bb], v);
             }
         }
     }
@@ -1561,10 +1813,12 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     best_     = dalloc<Best>(max_front_, s);
     pchunks_  = dalloc<Chunk>(max_pchunks_, s);
     pleft_    = dalloc<uint32_t>(max_pchunks_, s);
+    dirs_     = dalloc<uint32_t>(static_cast<size_t>(max_pchunks_) * (k_part_rows / 32), s);
     prbase_   = dalloc<uint32_t>(max_pchunks_, s);
     dst_      = dalloc<uint32_t>(max_front_ + 1, s);
     build_    = dalloc<uint32_t>(max_front_ * 2 + 2, s);
     bpair_    = dalloc<uint32_t>(3 * max_front_, s);
+    bbase_    = dalloc<uint32_t>(max_front_ + 1, s);
     brange_   = dalloc<uint32_t>(max_front_ + 2, s);
     bchunks_  = dalloc<Chunk>(max_bchunks_, s);
     rows_[0]  = dalloc<uint32_t>(max_rows_, s);
@@ -1612,10 +1866,14 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
             throw ConfigError("grower: quantised histograms of this many bins exceed "
                               "shared memory; lower bin_mapper.max_bin");
         }
-        auto qk = plane_.u8 ? reinterpret_cast<void const *>(&qhist_kernel<uint8_t>)
-                            : reinterpret_cast<void const *>(&qhist_kernel<uint16_t>);
-        BB_CHECK(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
+        size_t const tsmem = (static_cast<size_t>(32) * max_nb_ * 8) +
+                             ((k_tthreads / 32) * 32 * 32);
+        BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(tsmem)));
     }
     else
     {
@@ -1673,7 +1931,7 @@ Grower::~Grower()
                     ccount_,  seg_,      payload_, rows_[0],  rows_[1],    scale_,
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
-                    tile_j_[1]};
+                    tile_j_[1], bbase_,   dirs_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -1737,14 +1995,16 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
         if (plane_.u8)
         {
-            qhist_kernel<uint8_t><<<grid, k_threads, qsmem, s>>>(
+            size_t const tsmem = (static_cast<size_t>(32) * max_nb_ * 8) +
+                                 ((k_tthreads / 32) * 32 * 32);
+            qhist_t_kernel<<<grid, k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);
         }
         else
         {
-            qhist_kernel<uint16_t><<<grid, k_threads, qsmem, s>>>(
+            qhist_kernel<uint16_t><<<grid, k_qthreads, qsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);
@@ -1862,18 +2122,19 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     {
         pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
             ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
-            sel_nb_, pleft_);
+            sel_nb_, pleft_, dirs_);
     }
     else
     {
         pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
             ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
-            sel_nb_, pleft_);
+            sel_nb_, pleft_, dirs_);
     }
     BB_LAUNCH("pcount_kernel");
     plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
                                           pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
-                                          build_, brange_, bchunks_, cfg_.tp, t, crows_);
+                                          build_, brange_, bchunks_, cfg_.tp, t, crows_,
+                                          bbase_);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -1881,18 +2142,9 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
                                                     t, leaf_id, scores, lr);
     BB_LAUNCH("stamp_kernel");
-    if (plane_.u8)
-    {
-        pscatter_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
-            ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in,
-            rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_);
-    }
-    else
-    {
-        pscatter_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
-            ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in,
-            rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_);
-    }
+    pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
+        ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
+        dirs_);
     BB_LAUNCH("pscatter_kernel");
     if (prof_ != nullptr)
     {

@@ -184,9 +184,11 @@ class Grower
     Chunk    *pchunks_  = nullptr;
     uint32_t *pleft_    = nullptr; // per partition chunk: left count, then base
     uint32_t *prbase_   = nullptr;
+    uint32_t *dirs_     = nullptr; // per partition chunk: one direction bit per row
     uint32_t *dst_      = nullptr; // per frontier slot: child segment start
     uint32_t *build_    = nullptr; // per build index: frontier slot in next
     uint32_t *bpair_    = nullptr; // per split: (parent, small, large) slots
+    uint32_t *bbase_    = nullptr; // per build index: its payload base
     uint32_t *brange_   = nullptr; // per build index: chunk range [c0, c1)
     Chunk    *bchunks_  = nullptr;
     uint32_t *ccount_   = nullptr; // [bchunk][n_sel][cell_stride] counts/offsets

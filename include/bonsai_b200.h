@@ -92,6 +92,7 @@ typedef struct
     uint32_t const *selected;  /* ascending feature ids, or NULL for all */
     uint32_t       n_selected;
     int32_t        use_graph;  /* capture one boosting round as a CUDA graph */
+    int32_t        record_leaf_ids; /* keep each row's leaf id of the last tree */
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
@@ -127,7 +128,8 @@ int bb_booster_tree(bb_booster const *b, uint32_t t, uint32_t *feature, float *v
  * (histogram_engine.hpp:262). */
 int bb_booster_scores(bb_booster const *b, float *out);
 
-/* Per-row leaf node id of the last tree (host, n_rows). */
+/* Per-row leaf node id of the last tree (host, n_rows); needs
+ * record_leaf_ids set at creation. */
 int bb_booster_leaf_ids(bb_booster const *b, uint32_t *out);
 
 /* Device time of the last bb_booster_update, in milliseconds. */

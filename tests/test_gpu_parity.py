@@ -192,7 +192,8 @@ def test_large_tree_structural_invariants(bb):
     y = (X[:, 0] + X[:, 1] * X[:, 2] > 0).astype(np.float32)
     cuts, off = bb.fit_cuts(X)
     plane = bb.Plane(X, cuts, off)
-    b = bb.Booster(plane, y, _params(bb, objective="logloss", max_depth=8), max_trees=3)
+    b = bb.Booster(plane, y, _params(bb, objective="logloss", max_depth=8,
+                                     record_leaf_ids=True), max_trees=3)
     b.update(3)
     trees = b.trees()
     for t in trees:
