@@ -32,7 +32,9 @@ namespace
 constexpr uint32_t k_threads    = 256;
 constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
 constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk (exact)
-constexpr uint32_t k_qbuild_rows = 8192;  // rows per histogram-build chunk (quantised)
+constexpr uint32_t k_qbuild_rows = 2048;  // rows per histogram-build chunk (quantised)
+constexpr uint32_t k_qflush_chunks = 8;  // chunks a quantised shared histogram holds
+constexpr uint32_t k_qctas = 2 * 148;    // persistent quantised-histogram CTAs per tile
 constexpr uint32_t k_qthreads    = 512;   // threads per quantised-histogram CTA
 constexpr uint32_t k_tthreads    = 512;   // threads per conflict-free (u8) histogram CTA
 constexpr uint32_t k_warps_feat = 8;    // features per count/scatter CTA
@@ -1461,11 +1463,46 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 }
 
 
-// The u8 form of the quantised histogram, bank-conflict free: a warp stages
-// 32 rows' 32-byte tiles in shared memory, then walks them row by row with
-// lane l adding feature l. Cells are laid out [bin][32 features], so lane l
-// always lands in bank l whatever the bins. Same cells, same integer sums
-// as qhist_kernel. grid (chunks, tiles), k_tthreads threads.
+// The u8 form of the quantised histogram, bank-conflict free without any
+// staging: lane = row. Each lane rotates its row's 32-byte tile right by
+// `lane` bytes, so at (unrolled) step i it reads byte i -- a compile-time
+// position -- which is feature (i + lane) mod 32 of its row. The 32 lanes
+// thus touch 32 different features at every step, and with cells laid out
+// [bin][32 features] each lane lands in its own bank whatever the bins.
+// Two native 32-bit shared adds per (row, feature): the gradient word
+// signed, the hessian word unsigned.
+//
+// Persistent: a grid of k_qctas CTAs per tile, each walking a contiguous
+// range of the level's chunks (node-ordered), so no wave tail; the shared
+// histogram flushes -- one packed 64-bit global add per touched cell,
+// gradient in the high word (two's complement), hessian in the low word --
+// only when the node changes. A flush covers at most 16,384 rows (8 chunks
+// of 2,048) of |q| <= 127, so the 32-bit words never overflow: the range is
+// also flushed every 8 chunks.
+__device__ __forceinline__ void qflush_t(int32_t *hg_s, uint32_t *hh_s, uint32_t cells,
+                                         int32_t const *j_s, uint32_t const *sel_nb,
+                                         uint32_t const *cell_off, unsigned long long *dst)
+{
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < cells; x += k_tthreads)
+    {
+        uint32_t const f  = x & 31;
+        uint32_t const bb = x >> 5;
+        int32_t const  j2 = j_s[f];
+        int32_t const  g  = hg_s[x];
+        uint32_t const h  = hh_s[x];
+        if (j2 >= 0 && bb < sel_nb[j2] && (g != 0 || h != 0))
+        {
+            atomicAdd(&dst[cell_off[j2] + bb],
+                      (static_cast<unsigned long long>(static_cast<uint32_t>(g)) << 32) +
+                          static_cast<unsigned long long>(h));
+        }
+        hg_s[x] = 0;
+        hh_s[x] = 0;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(k_tthreads, 2)
     qhist_t_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
                    uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
@@ -1474,89 +1511,99 @@ __global__ void __launch_bounds__(k_tthreads, 2)
                    uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
     extern __shared__ uint4 t_smem[];
-    uint32_t const c = blockIdx.x;
-    if (c >= ctl->n_bchunks)
+    __shared__ int32_t      j_s[32];
+    uint32_t const          total = ctl->n_bchunks;
+    uint32_t const          c_a   = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x) * total) / gridDim.x);
+    uint32_t const          c_b   = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x + 1) * total) / gridDim.x);
+    if (c_a >= c_b)
     {
         return;
     }
-    uint32_t const lane   = threadIdx.x & 31;
-    uint32_t const w      = threadIdx.x >> 5;
-    uint32_t const cells  = 32 * max_nb;
-    auto          *hg_s   = reinterpret_cast<int32_t *>(t_smem);        // [bin][32]
-    auto          *hh_s   = reinterpret_cast<uint32_t *>(hg_s + cells); // [bin][32]
-    auto          *stage  = reinterpret_cast<uint4 *>(hh_s + cells) + (w * 64); // 32 rows x 32 B
-    auto const    *st_b   = reinterpret_cast<uint8_t const *>(stage);
-    uint32_t const tile   = tile_ids[blockIdx.y];
-    int32_t const  jj     = tile_j[(blockIdx.y * 32) + lane];
+    uint32_t const lane  = threadIdx.x & 31;
+    uint32_t const cells = 32 * max_nb;
+    auto          *hg_s  = reinterpret_cast<int32_t *>(t_smem);        // [bin][32]
+    auto          *hh_s  = reinterpret_cast<uint32_t *>(hg_s + cells); // [bin][32]
+    uint32_t const tile  = tile_ids[blockIdx.y];
+    if (threadIdx.x < 32)
+    {
+        j_s[threadIdx.x] = tile_j[(blockIdx.y * 32) + threadIdx.x];
+    }
     for (uint32_t x = threadIdx.x; x < 2 * cells; x += k_tthreads)
     {
         hg_s[x] = 0;
     }
     __syncthreads();
-    Chunk const  ch = bchunks[c];
-    uint4 const *mt = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
-    for (uint32_t k0 = w * 32; k0 < ch.count; k0 += k_tthreads)
+    // active features of the tile, rotated like the bytes: bit i <-> feature
+    // (i + lane) mod 32
+    uint32_t amask = 0;
+    for (uint32_t f = 0; f < 32; ++f)
     {
-        uint32_t const k  = k0 + lane;
-        uint32_t const nr = min(32u, ch.count - k0);
-        uint32_t       q  = 0;
-        if (k < ch.count)
+        amask |= j_s[f] >= 0 ? (1u << f) : 0u;
+    }
+    uint32_t const rmask = __funnelshift_r(amask, amask, lane);
+    uint4 const   *mt    = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
+    uint32_t       node  = bchunks[c_a].node;
+    uint32_t       held  = 0; // chunks accumulated since the last flush
+    for (uint32_t c = c_a; c < c_b; ++c)
+    {
+        Chunk const ch = bchunks[c];
+        if (ch.node != node || held == k_qflush_chunks)
         {
-            uint32_t const r = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
-            q                = qgh[r];
-            stage[2 * lane]       = mt[static_cast<uint64_t>(r) * 2];
-            stage[(2 * lane) + 1] = mt[(static_cast<uint64_t>(r) * 2) + 1];
+            qflush_t(hg_s, hh_s, cells, j_s, sel_nb, cell_off,
+                     hist + (static_cast<uint64_t>(build[node]) * total_cells));
+            node = ch.node;
+            held = 0;
         }
-        __syncwarp();
-        if (nr == 32)
+        ++held;
+        for (uint32_t k = threadIdx.x; k < ch.count; k += k_tthreads)
         {
-#pragma unroll 8
-            for (uint32_t j = 0; j < 32; ++j)
+            uint32_t const r  = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
+            uint32_t const q  = qgh[r];
+            uint4 const    va = mt[static_cast<uint64_t>(r) * 2];
+            uint4 const    vb = mt[(static_cast<uint64_t>(r) * 2) + 1];
+            int32_t const  qg = static_cast<int8_t>(q & 0xFFu);
+            uint32_t const qh = q >> 8;
+            // rotate the 8 words by lane / 4 words, then by lane % 4 bytes
+            uint32_t       w[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+            uint32_t const wk   = lane >> 2;
+#pragma unroll
+            for (uint32_t st = 1; st < 8; st <<= 1)
             {
-                uint32_t const qj  = __shfl_sync(0xFFFFFFFFu, q, j);
-                uint32_t const bin = st_b[(j * 32) + lane];
-                if (jj >= 0)
+                bool const take = (wk & st) != 0;
+                uint32_t   t[8];
+#pragma unroll
+                for (uint32_t i = 0; i < 8; ++i)
                 {
-                    atomicAdd(&hg_s[(bin * 32) + lane],
-                              static_cast<int32_t>(static_cast<int8_t>(qj & 0xFFu)));
-                    atomicAdd(&hh_s[(bin * 32) + lane], qj >> 8);
+                    t[i] = take ? w[(i + st) & 7] : w[i];
+                }
+#pragma unroll
+                for (uint32_t i = 0; i < 8; ++i)
+                {
+                    w[i] = t[i];
+                }
+            }
+            uint32_t const bs = (lane & 3) * 8;
+            uint32_t       rw[8];
+#pragma unroll
+            for (uint32_t i = 0; i < 8; ++i)
+            {
+                rw[i] = __funnelshift_r(w[i], w[(i + 1) & 7], bs);
+            }
+#pragma unroll
+            for (uint32_t i = 0; i < 32; ++i)
+            {
+                if ((rmask >> i) & 1u)
+                {
+                    uint32_t const bin = (rw[i >> 2] >> ((i & 3) * 8)) & 0xFFu;
+                    uint32_t const x   = (bin * 32) + ((lane + i) & 31);
+                    atomicAdd(&hg_s[x], qg);
+                    atomicAdd(&hh_s[x], qh);
                 }
             }
         }
-        else
-        {
-            for (uint32_t j = 0; j < nr; ++j)
-            {
-                uint32_t const qj  = __shfl_sync(0xFFFFFFFFu, q, j);
-                uint32_t const bin = st_b[(j * 32) + lane];
-                if (jj >= 0)
-                {
-                    atomicAdd(&hg_s[(bin * 32) + lane],
-                              static_cast<int32_t>(static_cast<int8_t>(qj & 0xFFu)));
-                    atomicAdd(&hh_s[(bin * 32) + lane], qj >> 8);
-                }
-            }
-        }
-        __syncwarp();
     }
-    __syncthreads();
-    unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells);
-    for (uint32_t x = threadIdx.x; x < cells; x += k_tthreads)
-    {
-        uint32_t const f  = x & 31;
-        uint32_t const bb = x >> 5;
-        int32_t const  j2 = tile_j[(blockIdx.y * 32) + f];
-        if (j2 >= 0 && bb < sel_nb[j2])
-        {
-            unsigned long long const v =
-                (static_cast<unsigned long long>(static_cast<uint32_t>(hg_s[x])) << 32) +
-                static_cast<unsigned long long>(hh_s[x]);
-            if (v != 0ULL)
-            {
-                atomicAdd(&dst[cell_off[j2] + bb], v);
-            }
-        }
-    }
+    qflush_t(hg_s, hh_s, cells, j_s, sel_nb, cell_off,
+             hist + (static_cast<uint64_t>(build[node]) * total_cells));
 }
 
 __device__ __forceinline__ void qtotals_from_cells(unsigned long long const *cells,
@@ -1869,8 +1916,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
-        size_t const tsmem = (static_cast<size_t>(32) * max_nb_ * 8) +
-                             ((k_tthreads / 32) * 32 * 32);
+        size_t const tsmem = static_cast<size_t>(32) * max_nb_ * 8;
         BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(tsmem)));
@@ -1995,9 +2041,8 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
         if (plane_.u8)
         {
-            size_t const tsmem = (static_cast<size_t>(32) * max_nb_ * 8) +
-                                 ((k_tthreads / 32) * 32 * 32);
-            qhist_t_kernel<<<grid, k_tthreads, tsmem, s>>>(
+            size_t const tsmem = static_cast<size_t>(32) * max_nb_ * 8;
+            qhist_t_kernel<<<dim3(k_qctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);

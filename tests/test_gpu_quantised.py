@@ -133,3 +133,22 @@ def test_quantised_large_invariants(bb):
     for t in trees:
         s = (s + np.float32(0.1) * bb.predict(plane, [t], 0.0, 1.0)).astype(np.float32)
     np.testing.assert_array_equal(b.scores(), s)
+
+
+def test_quantised_u16_bins_histogram_and_fit(bb):
+    """u16 codes (more than 256 bins) take the generic quantised kernel."""
+    X, g, h = _data(8, 150_000, F=6)
+    cuts, off = bb.fit_cuts(X, max_bin=700)
+    plane = bb.Plane(X, cuts, off)
+    assert not plane.u8
+    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=3), g, h)
+    ref = _fp64_hist(plane.bins(), np.diff(off), g, h)
+    sg = np.abs(g).max() / 127.0
+    counts = np.concatenate([np.bincount(plane.bins()[f], minlength=np.diff(off)[f])
+                             for f in range(6)])
+    assert np.all(np.abs(q[:, 0] - ref[:, 0]) <= 6 * sg * np.sqrt(counts) + sg)
+    y = (X[:, 0] + np.nan_to_num(X[:, 1]) > 0).astype(np.float32)
+    b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=6,
+                                             hist_mode="int8"), max_trees=10)
+    b.update(10)
+    assert b.n_trees == 10 and np.isfinite(b.scores()).all()
