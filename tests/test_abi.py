@@ -1,0 +1,81 @@
+"""CPU checks of the C ABI boundary: the library loads without a GPU and
+exports every entry point include/*.h declares; host-side logic (cut
+fitting) matches the reference."""
+
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+from conftest import ROOT, load_golden
+
+
+def _declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(bb_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from bonsai_b200.build import LIB, build_library
+    build_library()
+    lib = C.CDLL(LIB)
+    declared = _declared()
+    assert len(declared) >= 15
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_reports_no_device_without_raising():
+    import bonsai_b200 as bb
+    assert bb.available() in (True, False)
+
+
+def test_error_text_of_a_refused_call():
+    """A device call with a null plane fails with a status, not a crash,
+    and sets the thread's error text."""
+    import bonsai_b200 as bb
+    from bonsai_b200._lib import lib
+    rc = lib().bb_ingest(None, 0, 0, 0, None, None, C.byref(C.c_void_p()))
+    assert rc != 0
+    assert lib().bb_last_error().decode()
+
+
+def test_fit_cuts_matches_golden():
+    import bonsai_b200 as bb
+    from bonsai_b200 import synth
+    d = load_golden("small_regression.npz")
+    X, _ = synth.regression_small()
+    cuts, off = bb.fit_cuts(X)
+    assert np.array_equal(off, d["cut_off"])
+    assert np.array_equal(cuts.view(np.uint32), d["cuts"].view(np.uint32))
+    m = load_golden("missing_values.npz")
+    cuts, off = bb.fit_cuts(m["X"])
+    assert np.array_equal(off, m["cut_off"])
+    assert np.array_equal(cuts.view(np.uint32), m["cuts"].view(np.uint32))
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fit_cuts_matches_reference_live(ref, seed):
+    import bonsai_b200 as bb
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = 5000
+    X = np.stack([
+        rng.standard_normal(n),                                   # quantile stride
+        rng.integers(0, 12, n),                                   # distinct values
+        np.where(rng.random(n) < 0.8, 0.0, rng.standard_normal(n)),  # heavy value: greedy
+        np.round(rng.lognormal(0, 1, n), 1),                      # duplicates
+    ], 1).astype(np.float32)
+    X[rng.random((n, 4)) < 0.1] = np.nan
+    for max_bin in (16, 63, 255):
+        rc, ro = ref.fit_cuts(X, max_bin=max_bin)
+        cuts, off = bb.fit_cuts(X, max_bin=max_bin)
+        assert np.array_equal(off, ro), max_bin
+        assert np.array_equal(cuts.view(np.uint32), rc.view(np.uint32)), max_bin
