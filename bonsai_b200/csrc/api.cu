@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -914,4 +915,205 @@ extern "C"
                 }
             });
     }
+}
+
+// ---------------------------------------------------------------------------
+// bb_predict_static: ensemble predict that allocates no device memory.
+//
+// Who needs this: a caller that may not call cudaMalloc / cudaFree on its
+// serving path. Two kinds are common. A host whose device memory belongs to
+// another allocator under a fixed budget (a framework's caching allocator,
+// or a serving process that reserves all device memory up front) cannot let
+// a library take more. And a latency-bound caller cannot afford the
+// device-wide synchronisation that cudaMalloc and cudaFree imply. bb_predict
+// copies the packed ensemble into freshly allocated device buffers on every
+// call; this variant copies it into one fixed array that the library holds
+// for the life of the process instead.
+//
+// The array: k_static_bytes (11,534,336 bytes, 11 MiB) of file-scope device
+// memory, present on every GPU that loads the library until the process
+// exits. It holds at most k_max_static_nodes (524,288) tree nodes,
+// k_max_static_trees (65,536) trees and k_max_static_feats (65,536)
+// features; larger ensembles are refused with BB_ERR_CONFIG and nothing runs.
+//
+// Set-up: the first call on each device resolves the array's device address
+// (cudaGetSymbolAddress, with that device current) and caches it; make that
+// first call before any stream capture. Every call shares the one array and
+// leaves the last ensemble in it: calls whose work overlaps on the GPU (from
+// several host threads, or before the previous call's kernel has run) race
+// on it. The kernel runs on the legacy default stream and the call returns
+// once it is enqueued; synchronise that stream before reading out.
+
+namespace bb
+{
+namespace
+{
+
+constexpr uint32_t k_max_static_nodes = 524288;
+constexpr uint32_t k_max_static_trees = 65536;
+constexpr uint32_t k_max_static_feats = 65536;
+
+// layout (4-byte words, then the u8 default directions)
+constexpr size_t k_off_roots   = 0;
+constexpr size_t k_off_last    = k_off_roots + k_max_static_trees;
+constexpr size_t k_off_feature = k_off_last + k_max_static_feats;
+constexpr size_t k_off_split   = k_off_feature + k_max_static_nodes;
+constexpr size_t k_off_left    = k_off_split + k_max_static_nodes;
+constexpr size_t k_off_right   = k_off_left + k_max_static_nodes;
+constexpr size_t k_off_value   = k_off_right + k_max_static_nodes;
+constexpr size_t k_words       = k_off_value + k_max_static_nodes;
+constexpr size_t k_static_bytes = (k_words * 4) + k_max_static_nodes;
+
+static __device__ __align__(256) unsigned char g_predict_scratch[k_static_bytes];
+
+constexpr int k_max_devices = 64;
+std::mutex    g_mu;
+void         *g_addr[k_max_devices] = {};
+
+// The array's device address on the current device, resolved once.
+unsigned char *scratch_address()
+{
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= k_max_devices)
+    {
+        throw ConfigError("bb_predict_static: device ordinal above 63");
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_addr[dev] == nullptr)
+    {
+        void *p = nullptr;
+        check(cudaGetSymbolAddress(&p, g_predict_scratch), "cudaGetSymbolAddress");
+        g_addr[dev] = p;
+    }
+    return static_cast<unsigned char *>(g_addr[dev]);
+}
+
+// The predict walk of bb_predict (one thread per row, trees in order, leaves
+// summed in float, out = init + sum * lr), reading the ensemble from the
+// fixed array.
+template <typename BinT>
+__global__ void predict_static_kernel(BinT const *__restrict__ bins, uint64_t n_pad,
+                                      uint64_t n, uint32_t n_trees,
+                                      unsigned char const *__restrict__ scratch, float lr,
+                                      float init, float *__restrict__ out)
+{
+    uint64_t const r = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (r >= n)
+    {
+        return;
+    }
+    auto const *w       = reinterpret_cast<uint32_t const *>(scratch);
+    auto const *roots   = w + k_off_roots;
+    auto const *last    = w + k_off_last;
+    auto const *feature = w + k_off_feature;
+    auto const *split   = w + k_off_split;
+    auto const *left    = w + k_off_left;
+    auto const *right   = w + k_off_right;
+    auto const *value   = reinterpret_cast<float const *>(w + k_off_value);
+    auto const *dl      = scratch + (k_words * 4);
+    float       acc     = 0.0F;
+    for (uint32_t t = 0; t < n_trees; ++t)
+    {
+        uint32_t const base = roots[t];
+        uint32_t       idx  = base;
+        while (feature[idx] != k_leaf_flag)
+        {
+            uint32_t const f = feature[idx];
+            uint32_t const b = bins[(static_cast<uint64_t>(f) * n_pad) + r];
+            idx = base + (routes_left(b, last[f], split[idx], dl[idx] != 0) ? left[idx]
+                                                                           : right[idx]);
+        }
+        acc = acc + value[idx];
+    }
+    out[r] = init + (acc * lr);
+}
+
+} // namespace
+} // namespace bb
+
+extern "C" int bb_predict_static(bb_plane const *plane, uint32_t n_trees,
+                                 uint32_t const *roots, uint32_t n_nodes,
+                                 uint32_t const *feature, uint32_t const *split_bin,
+                                 uint32_t const *left, uint32_t const *right,
+                                 uint8_t const *default_left, float const *value, float lr,
+                                 float init, float *out_device)
+{
+    return guarded([&] {
+        need(plane != nullptr && roots != nullptr && feature != nullptr &&
+                        split_bin != nullptr && left != nullptr && right != nullptr &&
+                        default_left != nullptr && value != nullptr && out_device != nullptr,
+                    "bb_predict_static: null argument");
+        Plane const &p = plane->p;
+        if (n_nodes > k_max_static_nodes || n_trees > k_max_static_trees ||
+            p.n_feats > k_max_static_feats)
+        {
+            throw ConfigError(
+                "bb_predict_static: the ensemble exceeds the fixed device array (at most "
+                "524,288 nodes, 65,536 trees, 65,536 features); use bb_predict");
+        }
+        need(n_trees > 0 && n_nodes > 0, "bb_predict_static: empty ensemble");
+        // every walk must end: children lie after their parent inside the tree
+        for (uint32_t t = 0; t < n_trees; ++t)
+        {
+            uint32_t const b = roots[t];
+            uint32_t const e = t + 1 < n_trees ? roots[t + 1] : n_nodes;
+            need(b < e && e <= n_nodes, "bb_predict_static: bad tree roots");
+            for (uint32_t i = b; i < e; ++i)
+            {
+                if (feature[i] == k_leaf_flag)
+                {
+                    continue;
+                }
+                need(feature[i] < p.n_feats,
+                            "bb_predict_static: node feature out of range");
+                need(left[i] > i - b && right[i] > i - b && b + left[i] < e &&
+                                b + right[i] < e,
+                            "bb_predict_static: a child id must follow its parent in its tree");
+            }
+        }
+        unsigned char *scr = scratch_address();
+        auto          *w   = reinterpret_cast<uint32_t *>(scr);
+        uint32_t       last_bins[256];
+        // last bins go up in slices through a small host buffer
+        for (uint32_t f0 = 0; f0 < p.n_feats; f0 += 256)
+        {
+            uint32_t const m = p.n_feats - f0 < 256 ? p.n_feats - f0 : 256;
+            for (uint32_t k = 0; k < m; ++k)
+            {
+                last_bins[k] = p.h_cut_off[f0 + k + 1] - p.h_cut_off[f0 + k] - 1;
+            }
+            check(cudaMemcpy(w + k_off_last + f0, last_bins, m * 4, cudaMemcpyHostToDevice),
+                  "cudaMemcpy");
+        }
+        check(cudaMemcpy(w + k_off_roots, roots, n_trees * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(w + k_off_feature, feature, n_nodes * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(w + k_off_split, split_bin, n_nodes * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(w + k_off_left, left, n_nodes * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(w + k_off_right, right, n_nodes * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(w + k_off_value, value, n_nodes * 4ULL, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        check(cudaMemcpy(scr + (k_words * 4), default_left, n_nodes, cudaMemcpyHostToDevice),
+              "cudaMemcpy");
+        uint64_t const n      = p.n_rows;
+        uint32_t const blocks = static_cast<uint32_t>((n + 255) / 256);
+        if (p.u8)
+        {
+            predict_static_kernel<uint8_t><<<blocks, 256>>>(
+                static_cast<uint8_t const *>(p.bins), p.n_pad, n, n_trees, scr, lr, init,
+                out_device);
+        }
+        else
+        {
+            predict_static_kernel<uint16_t><<<blocks, 256>>>(
+                static_cast<uint16_t const *>(p.bins), p.n_pad, n, n_trees, scr, lr, init,
+                out_device);
+        }
+        check(cudaGetLastError(), "predict_static_kernel");
+    });
 }

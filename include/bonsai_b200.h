@@ -198,6 +198,27 @@ int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
                uint8_t const *default_left, float const *value, float lr, float init,
                float *out);
 
+/* Ensemble predict that allocates no device memory. No counterpart in the
+ * reference: it exists for callers that may not call cudaMalloc / cudaFree on
+ * their serving path -- a host whose device memory belongs to another
+ * allocator under a fixed budget, or a latency-bound caller that cannot
+ * absorb the device-wide synchronisation cudaMalloc and cudaFree imply.
+ * Same arguments and arithmetic as bb_predict (bit-identical scores), but
+ * the ensemble is copied into one fixed 11 MiB device array that the library
+ * holds on every GPU that loads it until the process exits, and out_device
+ * is the caller's device buffer (n_rows floats). Limits: at most 524,288
+ * nodes, 65,536 trees and 65,536 features; larger ensembles are refused
+ * with BB_ERR_CONFIG before anything runs. The first call on a device
+ * resolves the array's address there (make it before any stream capture).
+ * All calls share the array: calls whose work overlaps on the GPU race on
+ * it. The kernel runs on the legacy default stream; the call returns once it
+ * is enqueued, so synchronise before reading out_device. */
+int bb_predict_static(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+                      uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
+                      uint32_t const *left, uint32_t const *right,
+                      uint8_t const *default_left, float const *value, float lr,
+                      float init, float *out_device);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
