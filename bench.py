@@ -303,7 +303,9 @@ def main():
                 "h2d_bytes_per_step": (X.nbytes + y.nbytes) / N_ROUNDS,
                 "d2h_bytes_per_step": tree_bytes + scores.nbytes / N_ROUNDS,
                 "setup_s": t_setup, "download_s_per_500": t_down},
-        "roofline": {"bound": "hbm", "kernel": "histogram build (count+offsets+scatter+chain)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("histogram build (qhist_t_kernel per level)" if args.mode != "exact"
+                                else "histogram build (count+offsets+scatter+chain)"),
                      "achieved": hist_gbs, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": hist_gbs / peak, "traffic": traffic,
                      "algorithmic_bytes_per_tree": prof["hist_bytes"],
