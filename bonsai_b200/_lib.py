@@ -64,6 +64,8 @@ def lib() -> C.CDLL:
         vp = C.c_void_p
         L.bb_ingest.argtypes = [vp, C.c_uint64, C.c_uint32, C.c_int, vp, vp, C.POINTER(vp)]
         L.bb_plane_is_u8.argtypes = [vp]
+        L.bb_plane_from_bins.argtypes = [vp, C.c_int, C.c_uint64, C.c_uint32, vp, vp,
+                                         C.POINTER(vp)]
         L.bb_plane_download.argtypes = [vp, vp]
         L.bb_plane_destroy.argtypes = [vp]
         L.bb_booster_create.argtypes = [vp, vp, vp, C.POINTER(TrainCfg), C.c_uint32,

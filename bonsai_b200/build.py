@@ -77,6 +77,10 @@ def build_oracle() -> None:
     """Compiles the oracle checkers (test infrastructure): the C restatement
     always, the reference's own CPU grower when its sources are present."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
+    if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver.o")):
+        # the drop-in check links the product library: build it after
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin"],
+                       check=True)
 
 
 if __name__ == "__main__":

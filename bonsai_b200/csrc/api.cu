@@ -412,6 +412,84 @@ extern "C"
             });
     }
 
+    int bb_plane_from_bins(void const *bins, int is_u8, uint64_t n_rows, uint32_t n_feats,
+                           float const *cuts, uint32_t const *cut_off, bb_plane **out)
+    {
+        return guarded(
+            [&]
+            {
+                need(out != nullptr && bins != nullptr && cuts != nullptr && cut_off != nullptr,
+                     "bb_plane_from_bins: null argument");
+                need(n_rows > 0 && n_feats > 0, "bb_plane_from_bins: empty matrix");
+                need(n_rows < (1ull << 32), "bb_plane_from_bins: more than 2^32 - 1 rows");
+                uint32_t max_nb = 0;
+                for (uint32_t f = 0; f < n_feats; ++f)
+                {
+                    need(cut_off[f + 1] > cut_off[f] + 1,
+                         "bb_plane_from_bins: a feature needs >= 2 bins");
+                    max_nb = std::max(max_nb, cut_off[f + 1] - cut_off[f]);
+                }
+                need(is_u8 == 0 || max_nb <= 256, "bb_plane_from_bins: u8 codes need <= 256 bins");
+                need(max_nb <= 65535, "bb_plane_from_bins: more than 65535 bins");
+                // every code indexes a histogram cell: check them all
+                for (uint32_t f = 0; f < n_feats; ++f)
+                {
+                    uint32_t const nb = cut_off[f + 1] - cut_off[f];
+                    for (uint64_t r = 0; r < n_rows; ++r)
+                    {
+                        uint32_t const b =
+                            is_u8 != 0 ? static_cast<uint8_t const *>(bins)[(f * n_rows) + r]
+                                       : static_cast<uint16_t const *>(bins)[(f * n_rows) + r];
+                        need(b < nb, "bb_plane_from_bins: a code is not below its bin count");
+                    }
+                }
+                auto   pl = std::make_unique<bb_plane>();
+                Plane &p  = pl->p;
+                p.n_rows  = n_rows;
+                p.n_pad   = ((n_rows + 63) / 64) * 64;
+                p.n_feats = n_feats;
+                p.u8      = is_u8 != 0;
+                BB_CHECK(cudaGetDevice(&p.device));
+                uint32_t const n_cuts = cut_off[n_feats];
+                p.h_cuts              = new float[n_cuts];
+                p.h_cut_off           = new uint32_t[n_feats + 1];
+                std::memcpy(p.h_cuts, cuts, n_cuts * sizeof(float));
+                std::memcpy(p.h_cut_off, cut_off, (n_feats + 1) * sizeof(uint32_t));
+                std::vector<uint32_t> nb(n_feats);
+                for (uint32_t f = 0; f < n_feats; ++f)
+                {
+                    nb[f] = cut_off[f + 1] - cut_off[f];
+                }
+                p.cuts    = dmalloc<float>(n_cuts);
+                p.cut_off = dmalloc<uint32_t>(n_feats + 1);
+                p.n_bins  = dmalloc<uint32_t>(n_feats);
+                BB_CHECK(cudaMemcpy(p.cuts, cuts, n_cuts * 4, cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(p.cut_off, cut_off, (n_feats + 1) * 4,
+                                    cudaMemcpyHostToDevice));
+                BB_CHECK(cudaMemcpy(p.n_bins, nb.data(), n_feats * 4, cudaMemcpyHostToDevice));
+                size_t const el    = p.u8 ? 1 : 2;
+                size_t const bytes = static_cast<size_t>(n_feats) * p.n_pad * el;
+                BB_CHECK(cudaMalloc(&p.bins, bytes));
+                BB_CHECK(cudaMemset(p.bins, 0, bytes));
+                BB_CHECK(cudaMemcpy2D(p.bins, p.n_pad * el, bins, n_rows * el, n_rows * el,
+                                      n_feats, cudaMemcpyHostToDevice));
+                cudaStream_t s;
+                BB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                try
+                {
+                    build_mirror(p, s);
+                    BB_CHECK(cudaStreamSynchronize(s));
+                }
+                catch (...)
+                {
+                    cudaStreamDestroy(s);
+                    throw;
+                }
+                BB_CHECK(cudaStreamDestroy(s));
+                *out = pl.release();
+            });
+    }
+
     int bb_plane_is_u8(bb_plane const *plane)
     {
         return plane->p.u8 ? 1 : 0;

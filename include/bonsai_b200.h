@@ -61,6 +61,14 @@ int bb_select_device(uint32_t device_id);
 int bb_ingest(float const *X, uint64_t n_rows, uint32_t n_feats, int x_on_device,
               float const *cuts, uint32_t const *cut_off, bb_plane **out);
 
+/* A plane from codes already binned on the host: feature-major codes
+ * (bins[f * n_rows + r], u8 when is_u8 else u16), each below its feature's bin
+ * count (checked), and the cuts they were binned with. Replaces the engine
+ * adopting a host Dataset's columns (CudaDeviceContext's ensure_dataset,
+ * src/cuda/detail/device_context.cuh:55-62, device_context.cu:499-520). */
+int bb_plane_from_bins(void const *bins, int is_u8, uint64_t n_rows, uint32_t n_feats,
+                       float const *cuts, uint32_t const *cut_off, bb_plane **out);
+
 /* 1 when the plane stores u8 codes, 0 for u16. */
 int bb_plane_is_u8(bb_plane const *plane);
 

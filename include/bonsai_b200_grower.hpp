@@ -1,0 +1,271 @@
+// B200DepthwiseGrower: the reference-side binding of the B200 growers.
+//
+// A C++ grower satisfying bonsai's TreeGrower concept
+// (include/bonsai/grower.hpp:54-62) and the booster's grower seams
+// (recycle, resident_begin/end, eval_begin/accumulate; booster.hpp:562-676,
+// 1008-1021), implemented entirely through the C ABI in bonsai_b200.h. It
+// compiles against bonsai's own headers, so a maintainer drops it into
+// include/bonsai/cuda/ and registers it beside CudaDepthwiseGrower
+// (include/bonsai/registry/typelists.hpp:19-22). One grow() call is one
+// DepthwiseGrower<CudaHistogramEngine>::grow (src/grower_impl.hpp:465-577):
+// the same feature draw (std::sample over the ids with a mt19937 seeded by
+// feature_seed, as sample_features does, grower_impl.hpp:165-180), the same
+// DenseTree node table, the same per-row values and leaf ids, rows outside
+// the sample routed through the finished tree in bin space
+// (route_unsampled, grower_impl.hpp:438-461).
+//
+// Status codes rethrow as the reference does: BB_ERR_CONFIG as
+// bonsai::ConfigError, everything else as std::runtime_error.
+#pragma once
+
+#include "bonsai/config/errors.hpp"
+#include "bonsai/dataset.hpp"
+#include "bonsai/grower.hpp"
+#include "bonsai/tree.hpp"
+#include "bonsai_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <iterator>
+#include <numeric>
+#include <optional>
+#include <random>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace bonsai
+{
+
+inline void b200_rethrow(int rc)
+{
+    if (rc == BB_OK)
+    {
+        return;
+    }
+    std::string const msg = bb_last_error();
+    if (rc == BB_ERR_CONFIG)
+    {
+        throw ConfigError(msg);
+    }
+    throw std::runtime_error(msg);
+}
+
+class B200DepthwiseGrower
+{
+  public:
+    using Tree = DenseTree;
+
+    explicit B200DepthwiseGrower(TreeConfig const &cfg)
+        : config_(cfg), feature_rng_(cfg.feature_seed)
+    {
+        if (!cfg.interaction_constraints.empty())
+        {
+            throw ConfigError("interaction_constraints are not supported by the B200 "
+                              "grower; use the host depthwise grower");
+        }
+    }
+    B200DepthwiseGrower(B200DepthwiseGrower const &)            = delete;
+    B200DepthwiseGrower &operator=(B200DepthwiseGrower const &) = delete;
+    ~B200DepthwiseGrower()
+    {
+        if (plane_ != nullptr)
+        {
+            bb_plane_destroy(plane_);
+        }
+    }
+
+    GrowResult<Tree> grow(Dataset const &ds, floats_view grad, floats_view hess,
+                          row_index_view rows)
+    {
+        bind(ds);
+        std::vector<uint32_t> const selected = sample_features(ds.n_features());
+        std::vector<int8_t>         mono(config_.monotone_constraints.begin(),
+                                         config_.monotone_constraints.end());
+        bb_train_cfg c{};
+        c.objective         = 0;
+        c.learning_rate     = 1.0F;
+        c.min_child_hess    = config_.min_child_hess;
+        c.min_gain_to_split = config_.min_gain_to_split;
+        c.lambda_l2         = config_.lambda_l2;
+        c.lambda_l1         = config_.lambda_l1;
+        c.max_depth         = config_.max_depth;
+        c.min_data_in_leaf  = config_.min_data_in_leaf;
+        c.hist_mode         = 0;
+        c.monotone          = mono.empty() ? nullptr : mono.data();
+        c.n_monotone        = static_cast<uint32_t>(mono.size());
+        c.selected          = selected.data();
+        c.n_selected        = static_cast<uint32_t>(selected.size());
+        size_t const cap    = (size_t{2} << config_.max_depth) - 1;
+        std::vector<uint32_t> feat(cap), left(cap), right(cap), split_bin(cap), meta(3);
+        std::vector<float>    value(cap), gain(cap), cover(cap);
+        std::vector<uint8_t>  dl(cap);
+        size_t const          n = ds.n_rows();
+        train_leaf_values     values(n, 0.0F);
+        std::vector<node_id_t> leaf_ids(n, 0);
+        bool const all = rows.size() == n;
+        b200_rethrow(bb_grow_tree(plane_, &c, grad.data(), hess.data(),
+                                  all ? nullptr : rows.data(), rows.size(), feat.data(),
+                                  value.data(), left.data(), right.data(), dl.data(),
+                                  gain.data(), cover.data(), split_bin.data(), meta.data(),
+                                  values.data(), leaf_ids.data()));
+        size_t const n_nodes = meta[0];
+        Tree::Nodes  nodes(n_nodes);
+        for (size_t i = 0; i < n_nodes; ++i)
+        {
+            nodes[i] = feat[i] == DenseTree::k_leaf_flag
+                           ? DenseTree::leaf(value[i])
+                           : DenseTree::internal(feat[i], value[i], left[i], right[i],
+                                                 dl[i] != 0);
+        }
+        if (!all)
+        {
+            route_unsampled(ds, nodes, split_bin, rows, values, leaf_ids);
+        }
+        return {.tree     = Tree(std::move(nodes), {.depth = meta[1], .n_leaves = meta[2]},
+                                 std::vector<float>(gain.begin(), gain.begin() + n_nodes),
+                                 std::vector<float>(cover.begin(), cover.begin() + n_nodes)),
+                .values   = std::move(values),
+                .leaf_ids = std::move(leaf_ids)};
+    }
+
+    // The booster's seams. The per-row buffers are rebuilt every grow, so
+    // recycling is a no-op; the resident and device-validation seams decline,
+    // so the booster keeps its host objective and host eval walk.
+    void recycle(train_leaf_values, std::vector<node_id_t>) {}
+    bool resident_begin(Dataset const &, DeviceObjectiveKind, std::span<float const>, float)
+    {
+        return false;
+    }
+    void resident_end(std::span<float>) {}
+    bool resident() const
+    {
+        return false;
+    }
+    bool eval_begin(Dataset const &, DeviceObjectiveKind, std::span<float const>)
+    {
+        return false;
+    }
+    bool eval_accumulate(Tree const &, Dataset const &, float, std::span<float>,
+                         std::optional<float> &)
+    {
+        return false;
+    }
+
+  private:
+    // The device plane for ds, built once per Dataset from its host columns.
+    void bind(Dataset const &ds)
+    {
+        if (plane_ != nullptr && bound_ == &ds && bound_rows_ == ds.n_rows())
+        {
+            return;
+        }
+        if (plane_ != nullptr)
+        {
+            bb_plane_destroy(plane_);
+            plane_ = nullptr;
+        }
+        size_t const          n = ds.n_rows();
+        size_t const          F = ds.n_features();
+        std::vector<float>    cuts;
+        std::vector<uint32_t> off(F + 1, 0);
+        for (size_t f = 0; f < F; ++f)
+        {
+            auto const c = ds.cuts(static_cast<feature_id_t>(f));
+            cuts.insert(cuts.end(), c.begin(), c.end());
+            off[f + 1] = static_cast<uint32_t>(cuts.size());
+        }
+        bool const            u8 = ds.bins_are_u8();
+        std::vector<uint8_t>  b8;
+        std::vector<uint16_t> b16;
+        if (u8)
+        {
+            b8.resize(n * F);
+        }
+        else
+        {
+            b16.resize(n * F);
+        }
+        for (size_t f = 0; f < F; ++f)
+        {
+            ds.visit_bins(f,
+                          [&](auto bins)
+                          {
+                              for (size_t r = 0; r < n; ++r)
+                              {
+                                  if (u8)
+                                  {
+                                      b8[(f * n) + r] = static_cast<uint8_t>(bins[r]);
+                                  }
+                                  else
+                                  {
+                                      b16[(f * n) + r] = static_cast<uint16_t>(bins[r]);
+                                  }
+                              }
+                          });
+        }
+        b200_rethrow(bb_plane_from_bins(u8 ? static_cast<void const *>(b8.data())
+                                           : static_cast<void const *>(b16.data()),
+                                        u8 ? 1 : 0, n, static_cast<uint32_t>(F), cuts.data(),
+                                        off.data(), &plane_));
+        bound_      = &ds;
+        bound_rows_ = n;
+    }
+
+    std::vector<uint32_t> sample_features(size_t n_features)
+    {
+        std::vector<uint32_t> all(n_features);
+        std::iota(all.begin(), all.end(), uint32_t{0});
+        float const fraction = config_.feature_fraction;
+        if (fraction >= 1.0F || n_features <= 1)
+        {
+            return all;
+        }
+        auto const k = std::max<size_t>(
+            1, static_cast<size_t>(std::ceil(fraction * static_cast<float>(n_features))));
+        std::vector<uint32_t> selected;
+        selected.reserve(k);
+        std::sample(all.begin(), all.end(), std::back_inserter(selected), k, feature_rng_);
+        return selected;
+    }
+
+    static void route_unsampled(Dataset const &ds, Tree::Nodes const &nodes,
+                                std::vector<uint32_t> const &split_bin, row_index_view rows,
+                                train_leaf_values &values, std::vector<node_id_t> &leaf_ids)
+    {
+        size_t j = 0;
+        for (size_t r = 0; r < ds.n_rows(); ++r)
+        {
+            if (j < rows.size() && rows[j] == r)
+            {
+                ++j;
+                continue;
+            }
+            node_id_t idx = 0;
+            while (!DenseTree::is_leaf(nodes[idx]))
+            {
+                auto const &nd   = nodes[idx];
+                auto const  last = static_cast<bin_id_t>(ds.n_bins(nd.feature_id) - 1);
+                bin_id_t const b = ds.bin_at(nd.feature_id, r);
+                idx = routes_left(b, last, static_cast<bin_id_t>(split_bin[idx]),
+                                  nd.default_left)
+                          ? nd.left
+                          : nd.right;
+            }
+            values[r]   = nodes[idx].threshold_or_value;
+            leaf_ids[r] = idx;
+        }
+    }
+
+    TreeConfig     config_;
+    std::mt19937   feature_rng_;
+    bb_plane      *plane_      = nullptr;
+    Dataset const *bound_      = nullptr;
+    size_t         bound_rows_ = 0;
+};
+
+static_assert(TreeGrower<B200DepthwiseGrower>);
+
+} // namespace bonsai

@@ -21,6 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libbonsai_ref.so")
 ORACLE_SO = os.path.join(HERE, "_ref", "liboracle.so")
+# the reference's Booster over bonsai_b200's grower shim (the drop-in check)
+REF_B200_SO = os.path.join(HERE, "_ref", "libbonsai_ref_b200.so")
 LEAF = 0xFFFFFFFF
 
 
@@ -164,6 +166,17 @@ class RefLib:
     def train(self, ds, cfg: TreeCfg):
         rc = cfg.ref()
         h = self.L.ref_train(C.c_void_p(ds.h), C.byref(rc))
+        if not h:
+            raise RuntimeError(self.err())
+        return RefModel(self, h)
+
+    def train_b200(self, ds, cfg: TreeCfg):
+        """The reference's Booster with B200DepthwiseGrower (needs REF_B200_SO)."""
+        f = self.L.ref_b200_train
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_void_p, C.POINTER(RefCfg)]
+        rc = cfg.ref()
+        h = f(C.c_void_p(ds.h), C.byref(rc))
         if not h:
             raise RuntimeError(self.err())
         return RefModel(self, h)

@@ -656,3 +656,42 @@ extern "C"
             });
     }
 }
+
+#ifdef BONSAI_B200_DROPIN
+// The drop-in check: the reference's own Booster and boosting loop
+// (include/bonsai/booster.hpp:484-592) with bonsai_b200's grower shim in
+// place of DepthwiseGrower<CudaHistogramEngine>. Trains cfg.n_iters rounds
+// on ds; the model handle reads back like ref_train's.
+#include "bonsai_b200_grower.hpp"
+
+extern "C" void *ref_b200_train(void const *dsp, ref_cfg const *c)
+{
+    RefModel *m  = nullptr;
+    int const rc = guarded(
+        [&]
+        {
+            auto const &ds  = *static_cast<Dataset const *>(dsp);
+            Config      cfg = make_config(*c);
+            parallel::set_n_threads(c->n_threads);
+            auto mm         = std::make_unique<RefModel>();
+            mm->grower      = 0;
+            mm->booster     = make_for_sampler<B200DepthwiseGrower>(*c, cfg);
+            for (uint32_t i = 0; i < c->n_iters; ++i)
+            {
+                mm->booster->update_one_iter(ds);
+            }
+            harvest<B200DepthwiseGrower>(*mm, *c);
+            auto *raw = mm->booster.get();
+            read_init(*mm, dynamic_cast<Booster<MSEObjective, B200DepthwiseGrower,
+                                                AllRowsSampler> const *>(raw));
+            read_init(*mm, dynamic_cast<Booster<LogLossObjective, B200DepthwiseGrower,
+                                                AllRowsSampler> const *>(raw));
+            read_init(*mm, dynamic_cast<Booster<MSEObjective, B200DepthwiseGrower,
+                                                BernoulliSampler> const *>(raw));
+            read_init(*mm, dynamic_cast<Booster<LogLossObjective, B200DepthwiseGrower,
+                                                BernoulliSampler> const *>(raw));
+            m = mm.release();
+        });
+    return rc == 0 ? m : nullptr;
+}
+#endif

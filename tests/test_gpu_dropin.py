@@ -1,0 +1,66 @@
+"""The drop-in check: the reference's own Booster (include/bonsai/booster.hpp:
+484-592) trained with bonsai_b200's grower shim (include/bonsai_b200_grower.hpp)
+in place of its CPU DepthwiseGrower must produce the same model -- the same
+trees, node for node and bit for bit -- as the reference's CPU grower under
+the same booster, sampler and feature draw."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+from conftest import assert_trees_equal
+
+from oracle import REF_B200_SO, RefLib, TreeCfg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dref(bb):
+    if not os.path.exists(REF_B200_SO):
+        pytest.skip("the drop-in harness is not built (make -C oracle dropin)")
+    return RefLib(REF_B200_SO)
+
+
+def _data(seed=5, n=12_000, F=7):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    X[rng.random((n, F)) < 0.08] = np.nan
+    X[:, 3] = np.round(X[:, 3] * 3)
+    y = (np.sin(2 * np.nan_to_num(X[:, 0])) + np.nan_to_num(X[:, 1]) * np.nan_to_num(X[:, 3])
+         + rng.normal(0, 0.1, n)).astype(np.float32)
+    return X, y
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(max_depth=6, n_iters=30, learning_rate=0.1),
+    dict(max_depth=5, n_iters=20, feature_fraction=0.5, lambda_l1=0.3),
+    dict(max_depth=6, n_iters=20, subsample=0.8, min_data_in_leaf=5),
+    dict(max_depth=4, n_iters=15, monotone=[1, 0, 0, -1, 0, 0, 0]),
+])
+def test_reference_booster_over_b200_grower_matches_cpu(dref, cfg):
+    X, y = _data()
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(**cfg)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    assert cpu.n_trees() == gpu.n_trees() == tc.n_iters
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+    assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
+
+
+def test_reference_booster_over_b200_grower_logloss(dref):
+    X, y = _data(seed=9)
+    yb = (y > np.median(y)).astype(np.float32)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, yb, cuts, off)
+    tc = TreeCfg(objective="logloss", max_depth=6, n_iters=20)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    # host objective on both sides: the same gradients, the same trees
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
