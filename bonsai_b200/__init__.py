@@ -26,7 +26,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "fit_cuts", "cuts_from_sample", "sample_rows",
+    "grow_tree", "populate", "predict", "pred_contribs", "fit_cuts", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
@@ -270,19 +270,37 @@ def populate(plane: Plane, params: TrainParams, grad, hess, rows=None) -> np.nda
     return out
 
 
-def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
-    """Ensemble predict in bin space (bb_predict)."""
+def _concat(trees: list, keys):
     roots = np.zeros(len(trees), np.uint32)
-    parts = {k: [] for k in ("feature", "split_bin", "left", "right", "default_left", "value")}
+    parts = {k: [] for k in keys}
     base = 0
     for i, t in enumerate(trees):
         roots[i] = base
         for k in parts:
             parts[k].append(getattr(t, k))
         base += len(t.feature)
-    cat = {k: np.ascontiguousarray(np.concatenate(v)) for k, v in parts.items()}
+    return roots, base, {k: np.ascontiguousarray(np.concatenate(v)) for k, v in parts.items()}
+
+
+def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
+    """Ensemble predict in bin space (bb_predict)."""
+    roots, base, cat = _concat(trees, ("feature", "split_bin", "left", "right",
+                                       "default_left", "value"))
     out = np.empty(plane.n_rows, np.float32)
     check(lib().bb_predict(plane.h, len(trees), ptr(roots), base, ptr(cat["feature"]),
                            ptr(cat["split_bin"]), ptr(cat["left"]), ptr(cat["right"]),
                            ptr(cat["default_left"]), ptr(cat["value"]), lr, init, ptr(out)))
+    return out
+
+
+def pred_contribs(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
+    """TreeSHAP contributions in bin space (bb_pred_contribs): [n_rows,
+    n_feats + 1] FP64, the last column the bias; rows sum to the margin."""
+    roots, base, cat = _concat(trees, ("feature", "split_bin", "left", "right",
+                                       "default_left", "value", "covers"))
+    out = np.empty((plane.n_rows, plane.n_feats + 1), np.float64)
+    check(lib().bb_pred_contribs(plane.h, len(trees), ptr(roots), base, ptr(cat["feature"]),
+                                 ptr(cat["split_bin"]), ptr(cat["left"]), ptr(cat["right"]),
+                                 ptr(cat["default_left"]), ptr(cat["value"]),
+                                 ptr(cat["covers"]), lr, init, ptr(out)))
     return out

@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
         L.bb_select_device.argtypes = [C.c_uint32]
         L.bb_predict_static.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 6 + [
             C.c_float, C.c_float, vp]
+        L.bb_pred_contribs.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 7 + [
+            C.c_float, C.c_float, vp]
         L.bb_populate.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64, vp]
         _lib = L
     return _lib

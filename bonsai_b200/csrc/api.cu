@@ -25,6 +25,16 @@ namespace
 
 thread_local std::string g_err;
 
+} // namespace
+
+void set_last_error(char const *msg)
+{
+    g_err = msg;
+}
+
+namespace
+{
+
 template <typename F> int guarded(F &&f)
 {
     try

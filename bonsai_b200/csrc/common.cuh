@@ -38,6 +38,9 @@ inline void check(cudaError_t e, char const *what)
     }
 }
 
+// Sets the calling thread's bb_last_error() text (defined with the C ABI).
+void set_last_error(char const *msg);
+
 #define BB_CHECK(call) ::bb::check((call), #call)
 #define BB_LAUNCH(what) ::bb::check(cudaGetLastError(), what)
 

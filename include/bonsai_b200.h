@@ -206,6 +206,24 @@ int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
                uint8_t const *default_left, float const *value, float lr, float init,
                float *out);
 
+/* TreeSHAP contributions over a plane, FP64: out is host memory, n_rows x
+ * (n_feats + 1) row-major, the last column the bias. Same tree layout as
+ * bb_predict plus per-node covers (the hessian sums the booster recorded).
+ * The values are the reference's: per tree, Lundberg's path-dependent
+ * TreeSHAP with a repeated feature's conditions merged, zero-cover branches
+ * carrying nothing, the bias its cover-weighted expected value; then every
+ * column x lr and init added to the bias (contribs_impl,
+ * include/bonsai/booster.hpp:901-924). At most 128 features and 32 distinct
+ * features on one root-to-leaf path (BB_ERR_CONFIG otherwise).
+ * Replaces cuda_shap_plan + cuda_pred_contribs
+ * (include/bonsai/cuda/shap.hpp:31-43) and the host pred_contribs_binned
+ * (include/bonsai/booster.hpp:887-899). */
+int bb_pred_contribs(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+                     uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
+                     uint32_t const *left, uint32_t const *right,
+                     uint8_t const *default_left, float const *value, float const *cover,
+                     float lr, float init, double *out);
+
 /* Ensemble predict that allocates no device memory. No counterpart in the
  * reference: it exists for callers that may not call cudaMalloc / cudaFree on
  * their serving path -- a host whose device memory belongs to another

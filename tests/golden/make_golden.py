@@ -6,11 +6,14 @@ inputs and stores inputs and outputs as .npz:
 
   small_regression.npz   20,640 x 8 regression: cuts, bin codes, 100 MSE
                          depthwise trees (depth 6, lr 0.1), training-set
-                         predictions, tree 0's per-row leaf ids
+                         predictions, tree 0's per-row leaf ids, the
+                         reference's binned TreeSHAP contributions of the
+                         first 1,024 rows
   missing_values.npz     4,096 x 6 with NaN columns and duplicate-heavy
                          values (the reference's test_cuda_grower scenario
                          shape): cuts, bins, one tree from fixed gradients
                          with its per-row values/leaf ids, 20 logloss trees
+                         and their binned TreeSHAP contributions
   split_cases.npz        hand-built histograms and the reference finder's
                          chosen split for each (the test_split_node cases)
 
@@ -125,6 +128,7 @@ def main():
     m = ref.train(ds, tc)
     trees = m.trees()
     pred = m.predict_binned(ds)
+    contribs = m.contribs_binned(ds)[:1024]
     g = np.zeros(len(y), np.float32)
     h = np.ones(len(y), np.float32)
     init = m.init_score()
@@ -132,7 +136,8 @@ def main():
     _, v0, ids0 = ref.grow_tree(ds, TreeCfg(max_depth=6), g, h)[:3]
     np.savez_compressed(os.path.join(HERE, "small_regression.npz"), cuts=cuts, cut_off=off,
                         bins=bins.astype(np.uint8), init=np.float32(init), pred=pred,
-                        tree0_values=v0, tree0_leaf_ids=ids0, **pack_trees(trees))
+                        tree0_values=v0, tree0_leaf_ids=ids0, contribs=contribs,
+                        **pack_trees(trees))
     # --- missing values
     X, y = missing_values_data()
     cuts, off = ref.fit_cuts(X)
@@ -148,6 +153,7 @@ def main():
                         cuts=cuts, cut_off=off, bins=ds.bins(), grad=g, hess=hh,
                         values=vals, leaf_ids=ids, logloss_init=np.float32(mb.init_score()),
                         logloss_pred=mb.predict_binned(dsb),
+                        ll_contribs=mb.contribs_binned(dsb),
                         **{"one_" + k: v for k, v in pack_trees([t]).items()},
                         **{"ll_" + k: v for k, v in pack_trees(mb.trees()).items()})
     # --- split finder cases
