@@ -85,17 +85,7 @@ __global__ void gradient_kernel(int objective, float const *__restrict__ scores,
     {
         return;
     }
-    float const s = scores[i];
-    float const y = labels[i];
-    if (objective == 0)
-    {
-        gh[i] = make_float2(s - y, 1.0F);
-    }
-    else
-    {
-        float const p = 1.0F / (1.0F + expf(-s));
-        gh[i]         = make_float2(p - y, p * (1.0F - p));
-    }
+    gh[i] = objective_gradient(objective, scores[i], labels[i]);
 }
 
 __global__ void iota_kernel(uint32_t *rows, uint64_t n)
@@ -317,13 +307,14 @@ struct bb_booster
     cudaEvent_t                 ev0{}, ev1{};
     float                       last_ms = 0.0F;
 
+    // gh always holds the gradients of the current scores: computed once at
+    // creation, then by each round's final walk for the next round
     void round_body()
     {
-        uint64_t const n = plane->n_rows;
-        gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
-        BB_LAUNCH("gradient_kernel");
+        uint64_t const      n = plane->n_rows;
+        bb::NextRound const next{objective, labels, gh};
         grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
-                     record_leaf_ids ? leaf_id : nullptr, scores, lr, true);
+                     record_leaf_ids ? leaf_id : nullptr, scores, lr, true, &next);
         commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
         BB_LAUNCH("commit_tree_kernel");
     }
@@ -610,6 +601,10 @@ extern "C"
                 b->trees.alloc(b->grower->max_nodes(), max_trees);
                 b->use_graph       = cfg->use_graph != 0;
                 b->record_leaf_ids = cfg->record_leaf_ids != 0;
+                gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores,
+                                                                  b->labels, b->gh, n);
+                BB_LAUNCH("gradient_kernel");
+                b->grower->seed_absmax(b->gh);
                 BB_CHECK(cudaEventCreate(&b->ev0));
                 BB_CHECK(cudaEventCreate(&b->ev1));
                 BB_CHECK(cudaStreamSynchronize(b->stream));

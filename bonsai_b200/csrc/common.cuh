@@ -83,6 +83,18 @@ __host__ __device__ inline bool routes_left(uint32_t b, uint32_t last, uint32_t 
     return b == last ? dl : b <= split;
 }
 
+// The resident objectives' gradient pair at score s and label y
+// (src/objective.cpp:44-58 squared error, 86-101 logistic loss).
+__device__ __forceinline__ float2 objective_gradient(int objective, float s, float y)
+{
+    if (objective == 0)
+    {
+        return make_float2(s - y, 1.0F);
+    }
+    float const p = 1.0F / (1.0F + expf(-s));
+    return make_float2(p - y, p * (1.0F - p));
+}
+
 // Tree-level knobs the device reads (TreeConfig, include/bonsai/config/
 // tree_config.hpp:9-29). Floats stay float: the reference widens them to
 // double at each use, and so does every kernel here.

@@ -33,7 +33,6 @@ constexpr uint32_t k_threads    = 256;
 constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
 constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk (exact)
 constexpr uint32_t k_qbuild_rows = 2048;  // rows per histogram-build chunk (quantised)
-constexpr uint32_t k_qflush_chunks = 8;  // chunks a quantised shared histogram holds
 constexpr uint32_t k_qctas = 2 * 148;    // persistent quantised-histogram CTAs per tile
 constexpr uint32_t k_qthreads    = 512;   // threads per quantised-histogram CTA
 constexpr uint32_t k_tthreads    = 512;   // threads per conflict-free (u8) histogram CTA
@@ -811,9 +810,10 @@ constexpr uint32_t k_warp_rows = k_part_rows / (k_threads / 32); // 512
 template <typename BinT>
 __global__ void __launch_bounds__(k_threads)
     pcount_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
-                  Best const *best, uint32_t const *rows, void const *bins,
-                  uint64_t n_pad, uint32_t const *sel, uint32_t const *sel_nb,
-                  uint32_t *pleft, uint32_t *dirs)
+                  Best const *best, uint32_t const *__restrict__ rows,
+                  void const *__restrict__ bins, uint64_t n_pad, uint32_t const *sel,
+                  uint32_t const *sel_nb, uint32_t *__restrict__ pleft,
+                  uint32_t *__restrict__ dirs)
 {
     __shared__ uint32_t wsum[k_threads / 32];
     uint32_t const      c = blockIdx.x;
@@ -837,20 +837,32 @@ __global__ void __launch_bounds__(k_threads)
     uint32_t const lane = threadIdx.x & 31;
     uint32_t const w    = threadIdx.x >> 5;
     uint32_t      *dw   = dirs + (static_cast<uint64_t>(c) * (k_part_rows / 32));
-    uint32_t       n    = 0;
-#pragma unroll 4
-    for (uint32_t s = 0; s < k_warp_rows; s += 32)
+    uint32_t const k0   = (w * k_warp_rows) + lane;
+    // every row id of the warp's run, then every code, then the ballots:
+    // all loads in flight together
+    constexpr uint32_t steps = k_warp_rows / 32;
+    uint32_t           r[steps];
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
     {
-        uint32_t const k  = (w * k_warp_rows) + s + lane;
-        bool           lf = false;
-        if (k < ch.count)
+        uint32_t const k = k0 + (32 * i);
+        r[i]             = k < ch.count ? rows[ch.begin + k] : k_leaf_flag;
+    }
+    uint32_t b[steps];
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        b[i] = r[i] != k_leaf_flag ? static_cast<uint32_t>(col[r[i]]) : 0u;
+    }
+    uint32_t n = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        bool const     lf = r[i] != k_leaf_flag && routes_left(b[i], last, bs.bin, bs.dl != 0);
+        uint32_t const m  = __ballot_sync(0xFFFFFFFFu, lf);
+        if (lane == i)
         {
-            lf = routes_left(col[rows[ch.begin + k]], last, bs.bin, bs.dl != 0);
-        }
-        uint32_t const m = __ballot_sync(0xFFFFFFFFu, lf);
-        if (lane == 0)
-        {
-            dw[((w * k_warp_rows) + s) / 32] = m;
+            dw[(w * steps) + i] = m;
         }
         n += __popc(m);
     }
@@ -1046,6 +1058,151 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// The final walk, for trees grown over every row: each row (one thread,
+// rows in order) walks the finished tree through its 32-byte mirror tiles
+// with the partition's own rule (routes_left on the split bin, the last bin
+// following default_left), so it reaches the leaf whose segment held it.
+// It then takes scores[r] = scores[r] + lr * value -- the stamp's arithmetic,
+// now coalesced -- its leaf id, and, for a resident booster, the next round's
+// gradient pair and a block maximum of |g| and h for the next quantisation.
+constexpr uint32_t k_walk_nodes = 512; // a depth-8 tree has at most 511
+
+struct WalkArgs
+{
+    float        *scores;
+    uint32_t     *leaf_id;
+    float         lr;
+    int           objective;
+    float const  *labels;
+    float2       *gh;
+    uint32_t     *absmax;
+};
+
+__device__ __forceinline__ uint32_t pick_word(uint32_t const w[8], uint32_t i)
+{
+    uint32_t const a = (i & 1) != 0 ? w[1] : w[0];
+    uint32_t const b = (i & 1) != 0 ? w[3] : w[2];
+    uint32_t const c = (i & 1) != 0 ? w[5] : w[4];
+    uint32_t const d = (i & 1) != 0 ? w[7] : w[6];
+    uint32_t const e = (i & 2) != 0 ? b : a;
+    uint32_t const f = (i & 2) != 0 ? d : c;
+    return (i & 4) != 0 ? f : e;
+}
+
+__global__ void __launch_bounds__(k_threads)
+    walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                uint32_t const *cut_off, uint32_t per, bool u8, WalkArgs a)
+{
+    // per node: x = tile << 8 | position (or the leaf flag), y = split bin |
+    // missing bin << 16, z = left | right << 12 | default_left << 24, w = value
+    __shared__ uint4 node_s[k_walk_nodes];
+    __shared__ float mg_s[k_threads / 32];
+    __shared__ float mh_s[k_threads / 32];
+    uint32_t const   n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        uint32_t const f = t.feature[i];
+        uint4          e;
+        e.w = __float_as_uint(t.value[i]);
+        if (f == k_leaf_flag)
+        {
+            e.x = k_leaf_flag;
+            e.y = 0;
+            e.z = 0;
+        }
+        else
+        {
+            e.x = ((f / per) << 8) | (f % per);
+            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
+            e.z = t.left[i] | (t.right[i] << 12) |
+                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
+        }
+        node_s[i] = e;
+    }
+    __syncthreads();
+    uint4 const    root   = node_s[0];
+    uint32_t const tile0  = root.x == k_leaf_flag ? 0u : root.x >> 8;
+    float *__restrict__ scores = a.scores;
+    float mg = 0.0F;
+    float mh = 0.0F;
+    uint64_t const stride = static_cast<uint64_t>(gridDim.x) * k_threads;
+    for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x; r < n_rows;
+         r += stride)
+    {
+        // independent loads first: the root's tile, the score, the label
+        uint4 const *src = mirror + (((static_cast<uint64_t>(tile0) * n_rows) + r) * 2);
+        uint4 const  va  = src[0];
+        uint4 const  vb  = src[1];
+        float const  s0  = scores != nullptr ? scores[r] : 0.0F;
+        float const  y   = a.gh != nullptr ? a.labels[r] : 0.0F;
+        uint32_t     w[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+        uint32_t     held = tile0;
+        uint32_t     node = 0;
+        uint4        e    = root;
+        for (uint32_t d = 0; d < 16 && e.x != k_leaf_flag; ++d)
+        {
+            uint32_t const tile = e.x >> 8;
+            uint32_t const pos  = e.x & 0xFFu;
+            if (tile != held)
+            {
+                uint4 const *s2 = mirror + (((static_cast<uint64_t>(tile) * n_rows) + r) * 2);
+                uint4 const  xa = s2[0];
+                uint4 const  xb = s2[1];
+                w[0] = xa.x; w[1] = xa.y; w[2] = xa.z; w[3] = xa.w;
+                w[4] = xb.x; w[5] = xb.y; w[6] = xb.z; w[7] = xb.w;
+                held = tile;
+            }
+            uint32_t const b = u8 ? (pick_word(w, pos >> 2) >> ((pos & 3) * 8)) & 0xFFu
+                                  : (pick_word(w, pos >> 1) >> ((pos & 1) * 16)) & 0xFFFFu;
+            bool const left = routes_left(b, e.y >> 16, e.y & 0xFFFFu, ((e.z >> 24) & 1u) != 0);
+            node            = left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
+            e               = node_s[node];
+        }
+        if (a.leaf_id != nullptr)
+        {
+            a.leaf_id[r] = node;
+        }
+        if (scores != nullptr)
+        {
+            float const sc = s0 + (a.lr * __uint_as_float(e.w));
+            scores[r]      = sc;
+            if (a.gh != nullptr)
+            {
+                float2 const g = objective_gradient(a.objective, sc, y);
+                a.gh[r]        = g;
+                mg             = fmaxf(mg, fabsf(g.x));
+                mh             = fmaxf(mh, fmaxf(g.y, 0.0F));
+            }
+        }
+    }
+    if (a.absmax == nullptr)
+    {
+        return;
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        mg = fmaxf(mg, __shfl_xor_sync(0xFFFFFFFFu, mg, o));
+        mh = fmaxf(mh, __shfl_xor_sync(0xFFFFFFFFu, mh, o));
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        mg_s[threadIdx.x >> 5] = mg;
+        mh_s[threadIdx.x >> 5] = mh;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (uint32_t w = 1; w < k_threads / 32; ++w)
+        {
+            mg = fmaxf(mg, mg_s[w]);
+            mh = fmaxf(mh, mh_s[w]);
+        }
+        atomicMax(&a.absmax[0], __float_as_uint(mg));
+        atomicMax(&a.absmax[1], __float_as_uint(mh));
+    }
+}
+
 // Partition pass 2, the stable scatter: lefts keep their order at
 // dst + left base, rights at dst + n_left + right base. Each warp takes the
 // same run of rows as pass 1, its base from the bitmask's popcounts (one
@@ -1053,8 +1210,9 @@ __global__ void __launch_bounds__(k_threads)
 __global__ void __launch_bounds__(k_threads)
     pscatter_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
                     Best const *best, uint32_t const *pleft, uint32_t const *prbase,
-                    uint32_t const *nleft, uint32_t const *dst, uint32_t const *rows,
-                    uint32_t *rows_out, uint32_t const *dirs)
+                    uint32_t const *nleft, uint32_t const *dst,
+                    uint32_t const *__restrict__ rows, uint32_t *__restrict__ rows_out,
+                    uint32_t const *__restrict__ dirs)
 {
     __shared__ uint32_t wsum[k_threads / 32];
     uint32_t const      c = blockIdx.x;
@@ -1068,16 +1226,23 @@ __global__ void __launch_bounds__(k_threads)
     {
         return;
     }
-    uint32_t const  lane = threadIdx.x & 31;
-    uint32_t const  w    = threadIdx.x >> 5;
-    uint32_t const *dw   = dirs + (static_cast<uint64_t>(c) * (k_part_rows / 32)) +
-                         ((w * k_warp_rows) / 32);
-    // this warp's left count
-    uint32_t mine = 0;
-    if (lane < k_warp_rows / 32)
+    constexpr uint32_t steps = k_warp_rows / 32;
+    uint32_t const     lane  = threadIdx.x & 31;
+    uint32_t const     w     = threadIdx.x >> 5;
+    uint32_t const     w0    = w * k_warp_rows;
+    // the warp's direction words (lane i holds step i's) and row ids
+    uint32_t const mword = lane < steps ? dirs[(static_cast<uint64_t>(c) * (k_part_rows / 32)) +
+                                               (w * steps) + lane]
+                                        : 0u;
+    uint32_t r[steps];
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
     {
-        mine = __popc(dw[lane]);
+        uint32_t const k = w0 + (32 * i) + lane;
+        r[i]             = k < ch.count ? rows[ch.begin + k] : 0u;
     }
+    // this warp's left count
+    uint32_t mine = __popc(mword);
 #pragma unroll
     for (uint32_t o = 16; o > 0; o >>= 1)
     {
@@ -1093,28 +1258,31 @@ __global__ void __launch_bounds__(k_threads)
     {
         lb += wsum[x];
     }
-    uint32_t const w0  = w * k_warp_rows;
     uint32_t const d0  = dst[ch.node];
     uint32_t       lo  = d0 + pleft[c] + lb;                                   // next left
     uint32_t       ro  = d0 + nleft[ch.node] + prbase[c] + (min(w0, ch.count) - lb); // next right
     uint32_t const ltm = (1u << lane) - 1u;
-    for (uint32_t s = 0; s < k_warp_rows && w0 + s < ch.count; s += 32)
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
     {
-        uint32_t const k = w0 + s + lane;
-        uint32_t const m = dw[s / 32];
-        uint32_t const nvalid = min(32u, ch.count - (w0 + s));
+        uint32_t const base = w0 + (32 * i);
+        if (base >= ch.count)
+        {
+            break;
+        }
+        uint32_t const m      = __shfl_sync(0xFFFFFFFFu, mword, i);
+        uint32_t const nvalid = min(32u, ch.count - base);
         uint32_t const vm     = nvalid == 32 ? 0xFFFFFFFFu : ((1u << nvalid) - 1u);
         uint32_t const lm     = m & vm;
-        if (k < ch.count)
+        if (lane < nvalid)
         {
-            uint32_t const r = rows[ch.begin + k];
             if ((m >> lane) & 1u)
             {
-                rows_out[lo + __popc(lm & ltm)] = r;
+                rows_out[lo + __popc(lm & ltm)] = r[i];
             }
             else
             {
-                rows_out[ro + __popc(~lm & vm & ltm)] = r;
+                rows_out[ro + __popc(~lm & vm & ltm)] = r[i];
             }
         }
         lo += __popc(lm);
@@ -1313,6 +1481,8 @@ __global__ void __launch_bounds__(k_threads)
     double const mh = __uint_as_float(absmax[1]);
     double const sg = mg > 0.0 ? mg / 127.0 : 1.0;
     double const sh = mh > 0.0 ? mh / 127.0 : 1.0;
+    double const ig = 1.0 / sg; // one division per thread, a multiply per row
+    double const ih = 1.0 / sh;
     uint32_t const t = *tree_no;
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
@@ -1325,8 +1495,8 @@ __global__ void __launch_bounds__(k_threads)
         uint4 const  r  = philox4x32_10(make_uint4(i, t, 0x5157u, 0u), key);
         double const ug = static_cast<double>(r.x >> 8) * (1.0 / 16777216.0);
         double const uh = static_cast<double>(r.y >> 8) * (1.0 / 16777216.0);
-        double const xg = static_cast<double>(v.x) / sg;
-        double const xh = static_cast<double>(fmaxf(v.y, 0.0F)) / sh;
+        double const xg = static_cast<double>(v.x) * ig;
+        double const xh = static_cast<double>(fmaxf(v.y, 0.0F)) * ih;
         int          qg = isnan(xg) ? 0 : static_cast<int>(floor(xg + ug));
         int          qh = isnan(xh) ? 0 : static_cast<int>(floor(xh + uh));
         qg              = max(-127, min(127, qg));
@@ -1464,43 +1634,94 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 
 
 // The u8 form of the quantised histogram, bank-conflict free without any
-// staging: lane = row. Each lane rotates its row's 32-byte tile right by
-// `lane` bytes, so at (unrolled) step i it reads byte i -- a compile-time
-// position -- which is feature (i + lane) mod 32 of its row. The 32 lanes
-// thus touch 32 different features at every step, and with cells laid out
-// [bin][32 features] each lane lands in its own bank whatever the bins.
-// Two native 32-bit shared adds per (row, feature): the gradient word
-// signed, the hessian word unsigned.
+// staging: lane = row. At (unrolled) step i every lane handles feature
+// i ^ lane of its row, so the 32 lanes touch 32 different features at every
+// step. The shared table is [bin][g: 32 features][h: 32 features], 256 bytes
+// per bin, so cell (b, f) sits in bank f whatever the bins, and its address
+// is (b << 8) | (f << 2): one byte permute puts the row's code of feature
+// i ^ lane at bits 8..15, one three-input logic op ORs in ((4 i) ^ (4 lane)),
+// and two 32-bit shared reductions (gradient word signed, hessian word
+// unsigned, at +0 and +128) complete the (row, feature). The 32-byte tile is
+// brought into that order once per row by a word permutation (j -> j ^ lane/4,
+// three select stages); the byte within a word is chosen by the permute's
+// per-lane selector. Slots of unselected features accumulate into columns
+// that are never flushed.
 //
 // Persistent: a grid of k_qctas CTAs per tile, each walking a contiguous
 // range of the level's chunks (node-ordered), so no wave tail; the shared
 // histogram flushes -- one packed 64-bit global add per touched cell,
 // gradient in the high word (two's complement), hessian in the low word --
-// only when the node changes. A flush covers at most 16,384 rows (8 chunks
-// of 2,048) of |q| <= 127, so the 32-bit words never overflow: the range is
-// also flushed every 8 chunks.
-__device__ __forceinline__ void qflush_t(int32_t *hg_s, uint32_t *hh_s, uint32_t cells,
-                                         int32_t const *j_s, uint32_t const *sel_nb,
-                                         uint32_t const *cell_off, unsigned long long *dst)
+// only when the node changes. The 32-bit words cannot overflow in between:
+// the quantised forms take fewer than 16,909,320 rows and both codes are at
+// most 127 in magnitude, so no cell's sum leaves the int32 range.
+constexpr uint32_t k_ttable_bytes = 256 * 256; // 256 bins x (32 g + 32 h) x 4 B
+
+__device__ __forceinline__ void red_shared_u32(uint32_t addr, uint32_t v)
+{
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void red_shared_u32_hi(uint32_t addr, uint32_t v)
+{
+    asm volatile("red.shared.add.u32 [%0+128], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void qflush_t(uint32_t *tbl, uint32_t max_nb, int32_t const *j_s,
+                                         uint32_t const *sel_nb, uint32_t const *cell_off,
+                                         unsigned long long *dst)
 {
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < cells; x += k_tthreads)
+    for (uint32_t x = threadIdx.x; x < 256 * 32; x += k_tthreads)
     {
         uint32_t const f  = x & 31;
         uint32_t const bb = x >> 5;
+        uint32_t const gi = (bb * 64) + f;
+        uint32_t const g  = tbl[gi];
+        uint32_t const h  = tbl[gi + 32];
         int32_t const  j2 = j_s[f];
-        int32_t const  g  = hg_s[x];
-        uint32_t const h  = hh_s[x];
-        if (j2 >= 0 && bb < sel_nb[j2] && (g != 0 || h != 0))
+        if (bb < max_nb && j2 >= 0 && bb < sel_nb[j2] && (g != 0 || h != 0))
         {
             atomicAdd(&dst[cell_off[j2] + bb],
-                      (static_cast<unsigned long long>(static_cast<uint32_t>(g)) << 32) +
+                      (static_cast<unsigned long long>(g) << 32) +
                           static_cast<unsigned long long>(h));
         }
-        hg_s[x] = 0;
-        hh_s[x] = 0;
+        tbl[gi]      = 0;
+        tbl[gi + 32] = 0;
     }
     __syncthreads();
+}
+
+// One row's 32 (feature, bin) cells: w is the row's 32-byte tile.
+__device__ __forceinline__ void qrow_t(uint32_t base, uint32_t lane4, uint32_t wsel,
+                                       uint32_t const sel[4], uint4 va, uint4 vb, uint32_t q)
+{
+    uint32_t const qg = static_cast<uint32_t>(static_cast<int32_t>(static_cast<int8_t>(q & 0xFFu)));
+    uint32_t const qh = q >> 8;
+    uint32_t       w[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+#pragma unroll
+    for (uint32_t st = 1; st < 8; st <<= 1)
+    {
+        bool const take = (wsel & st) != 0;
+        uint32_t   t[8];
+#pragma unroll
+        for (uint32_t i = 0; i < 8; ++i)
+        {
+            t[i] = take ? w[i ^ st] : w[i];
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < 8; ++i)
+        {
+            w[i] = t[i];
+        }
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < 32; ++i)
+    {
+        uint32_t const off  = __byte_perm(w[i >> 2], 0u, sel[i & 3]) | ((4u * i) ^ lane4);
+        uint32_t const addr = base + off;
+        red_shared_u32(addr, qg);
+        red_shared_u32_hi(addr, qh);
+    }
 }
 
 __global__ void __launch_bounds__(k_tthreads, 2)
@@ -1519,90 +1740,61 @@ __global__ void __launch_bounds__(k_tthreads, 2)
     {
         return;
     }
-    uint32_t const lane  = threadIdx.x & 31;
-    uint32_t const cells = 32 * max_nb;
-    auto          *hg_s  = reinterpret_cast<int32_t *>(t_smem);        // [bin][32]
-    auto          *hh_s  = reinterpret_cast<uint32_t *>(hg_s + cells); // [bin][32]
-    uint32_t const tile  = tile_ids[blockIdx.y];
+    uint32_t const lane = threadIdx.x & 31;
+    auto          *tbl  = reinterpret_cast<uint32_t *>(t_smem);
+    uint32_t const base = static_cast<uint32_t>(__cvta_generic_to_shared(tbl));
+    uint32_t const tile = tile_ids[blockIdx.y];
     if (threadIdx.x < 32)
     {
         j_s[threadIdx.x] = tile_j[(blockIdx.y * 32) + threadIdx.x];
     }
-    for (uint32_t x = threadIdx.x; x < 2 * cells; x += k_tthreads)
+    for (uint32_t x = threadIdx.x; x < k_ttable_bytes / 4; x += k_tthreads)
     {
-        hg_s[x] = 0;
+        tbl[x] = 0;
     }
     __syncthreads();
-    // active features of the tile, rotated like the bytes: bit i <-> feature
-    // (i + lane) mod 32
-    uint32_t amask = 0;
-    for (uint32_t f = 0; f < 32; ++f)
+    // byte k ^ (lane % 4) of a word to bits 8..15, zeros elsewhere
+    uint32_t sel[4];
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k)
     {
-        amask |= j_s[f] >= 0 ? (1u << f) : 0u;
+        sel[k] = 0x4404u | (((k ^ lane) & 3u) << 4);
     }
-    uint32_t const rmask = __funnelshift_r(amask, amask, lane);
+    uint32_t const lane4 = lane * 4;
+    uint32_t const wsel  = lane >> 2;
     uint4 const   *mt    = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
     uint32_t       node  = bchunks[c_a].node;
-    uint32_t       held  = 0; // chunks accumulated since the last flush
     for (uint32_t c = c_a; c < c_b; ++c)
     {
         Chunk const ch = bchunks[c];
-        if (ch.node != node || held == k_qflush_chunks)
+        if (ch.node != node)
         {
-            qflush_t(hg_s, hh_s, cells, j_s, sel_nb, cell_off,
+            qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
                      hist + (static_cast<uint64_t>(build[node]) * total_cells));
             node = ch.node;
-            held = 0;
         }
-        ++held;
-        for (uint32_t k = threadIdx.x; k < ch.count; k += k_tthreads)
+        // two rows per thread per pass, both loaded before either is added
+        for (uint32_t k = threadIdx.x; k < ch.count; k += 2 * k_tthreads)
         {
-            uint32_t const r  = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
-            uint32_t const q  = qgh[r];
-            uint4 const    va = mt[static_cast<uint64_t>(r) * 2];
-            uint4 const    vb = mt[(static_cast<uint64_t>(r) * 2) + 1];
-            int32_t const  qg = static_cast<int8_t>(q & 0xFFu);
-            uint32_t const qh = q >> 8;
-            // rotate the 8 words by lane / 4 words, then by lane % 4 bytes
-            uint32_t       w[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
-            uint32_t const wk   = lane >> 2;
-#pragma unroll
-            for (uint32_t st = 1; st < 8; st <<= 1)
+            bool const     two = k + k_tthreads < ch.count;
+            uint32_t const r0  = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
+            uint32_t const r1  = !two ? r0
+                                      : (rows != nullptr ? rows[ch.begin + k + k_tthreads]
+                                                         : ch.begin + k + k_tthreads);
+            uint32_t const q0  = qgh[r0];
+            uint4 const    a0  = mt[static_cast<uint64_t>(r0) * 2];
+            uint4 const    b0  = mt[(static_cast<uint64_t>(r0) * 2) + 1];
+            uint32_t const q1  = qgh[r1];
+            uint4 const    a1  = mt[static_cast<uint64_t>(r1) * 2];
+            uint4 const    b1  = mt[(static_cast<uint64_t>(r1) * 2) + 1];
+            qrow_t(base, lane4, wsel, sel, a0, b0, q0);
+            if (two)
             {
-                bool const take = (wk & st) != 0;
-                uint32_t   t[8];
-#pragma unroll
-                for (uint32_t i = 0; i < 8; ++i)
-                {
-                    t[i] = take ? w[(i + st) & 7] : w[i];
-                }
-#pragma unroll
-                for (uint32_t i = 0; i < 8; ++i)
-                {
-                    w[i] = t[i];
-                }
-            }
-            uint32_t const bs = (lane & 3) * 8;
-            uint32_t       rw[8];
-#pragma unroll
-            for (uint32_t i = 0; i < 8; ++i)
-            {
-                rw[i] = __funnelshift_r(w[i], w[(i + 1) & 7], bs);
-            }
-#pragma unroll
-            for (uint32_t i = 0; i < 32; ++i)
-            {
-                if ((rmask >> i) & 1u)
-                {
-                    uint32_t const bin = (rw[i >> 2] >> ((i & 3) * 8)) & 0xFFu;
-                    uint32_t const x   = (bin * 32) + ((lane + i) & 31);
-                    atomicAdd(&hg_s[x], qg);
-                    atomicAdd(&hh_s[x], qh);
-                }
+                qrow_t(base, lane4, wsel, sel, a1, b1, q1);
             }
         }
     }
-    qflush_t(hg_s, hh_s, cells, j_s, sel_nb, cell_off,
+    qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
              hist + (static_cast<uint64_t>(build[node]) * total_cells));
 }
 
@@ -1639,7 +1831,7 @@ __global__ void __launch_bounds__(k_threads)
                             uint32_t total_cells, uint32_t n_cells, Node const *cur,
                             Node *next, Best const *best, uint32_t const *sel,
                             uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
-                            TreeParams tp, double2 const *qscale)
+                            TreeParams tp, double2 const *qscale, int64_t const *btot)
 {
     uint32_t const k = blockIdx.x;
     if (k >= ctl->n_splits)
@@ -1656,19 +1848,51 @@ __global__ void __launch_bounds__(k_threads)
     {
         hl[x] = hp[x] - hs[x];
     }
-    __syncthreads();
+    if (threadIdx.x >= 32)
+    {
+        return;
+    }
+    // the smaller child's exact totals: its first feature's cells (every row
+    // lands in one of them), or the per-build sums when no cells were built;
+    // the larger child's are the parent's minus them
+    int64_t sg = 0;
+    int64_t sh = 0;
+    if (btot != nullptr)
+    {
+        if (threadIdx.x == 0)
+        {
+            sg = btot[2 * k];
+            sh = btot[(2 * k) + 1];
+        }
+    }
+    else
+    {
+        for (uint32_t b = threadIdx.x; b < sel_nb[0]; b += 32)
+        {
+            unsigned long long const c = hs[b];
+            sg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+            sh += static_cast<uint32_t>(c);
+        }
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        sg += __shfl_xor_sync(0xFFFFFFFFu, sg, o);
+        sh += __shfl_xor_sync(0xFFFFFFFFu, sh, o);
+    }
     if (threadIdx.x == 0)
     {
-        uint32_t const nb0 = sel_nb[0];
-        Node           L   = next[2 * k];
-        Node           R   = next[(2 * k) + 1];
-        qtotals_from_cells(hist_nxt + (static_cast<uint64_t>(2 * k) * total_cells), nb0,
-                           L.qg, L.qh);
-        qtotals_from_cells(hist_nxt + (static_cast<uint64_t>((2 * k) + 1) * total_cells),
-                           nb0, R.qg, R.qh);
-        Node const     par = cur[p];
-        uint32_t const f   = sel[best[p].feature];
-        int const      mc  = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+        Node const par = cur[p];
+        Node       S   = next[s];
+        Node       G   = next[l];
+        S.qg           = sg;
+        S.qh           = sh;
+        G.qg           = par.qg - sg;
+        G.qh           = par.qh - sh;
+        Node          &L  = s == 2 * k ? S : G;
+        Node          &R  = s == 2 * k ? G : S;
+        uint32_t const f  = sel[best[p].feature];
+        int const      mc = (mono != nullptr && f < n_mono) ? mono[f] : 0;
         if (mc != 0)
         {
             double2 const sc  = *qscale;
@@ -1697,11 +1921,48 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// Exact integer totals of the smaller children when no histogram is built
+// for them (the last level): per build chunk, the sums of its rows' codes,
+// added into the chunk's build slot.
+__global__ void __launch_bounds__(k_threads)
+    qbuilt_totals_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *rows,
+                         uint16_t const *__restrict__ qgh, int64_t *btot)
+{
+    uint32_t const c = blockIdx.x;
+    if (c >= ctl->n_bchunks)
+    {
+        return;
+    }
+    Chunk const ch = bchunks[c];
+    int64_t     g  = 0;
+    int64_t     h  = 0;
+    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+    {
+        uint32_t const q = qgh[rows[ch.begin + k]];
+        g += static_cast<int8_t>(q & 0xFFu);
+        h += q >> 8;
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        g += __shfl_xor_sync(0xFFFFFFFFu, g, o);
+        h += __shfl_xor_sync(0xFFFFFFFFu, h, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicAdd(reinterpret_cast<unsigned long long *>(&btot[2 * ch.node]),
+                  static_cast<unsigned long long>(g));
+        atomicAdd(reinterpret_cast<unsigned long long *>(&btot[(2 * ch.node) + 1]),
+                  static_cast<unsigned long long>(h));
+    }
+}
+
 // Leaf renewal, pass 1: per partition chunk of a leaf node, the FP64 sums of
 // the full-precision (g, h) of its rows, in a fixed reduction order.
 __global__ void __launch_bounds__(k_threads)
     leafsum_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
-                   uint32_t const *rows, float2 const *__restrict__ gh, double2 *partial)
+                   uint32_t const *__restrict__ rows, float2 const *__restrict__ gh,
+                   double2 *__restrict__ partial)
 {
     __shared__ double sg_s[k_threads / 32];
     __shared__ double sh_s[k_threads / 32];
@@ -1718,6 +1979,7 @@ __global__ void __launch_bounds__(k_threads)
     }
     double g = 0.0;
     double h = 0.0;
+#pragma unroll 8
     for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
     {
         float2 const v = gh[rows[ch.begin + k]];
@@ -1880,6 +2142,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         qscale_  = dalloc<double2>(1, s);
         qgh8_    = dalloc<uint16_t>(max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows, s);
         partial_ = dalloc<double2>(max_pchunks_, s);
+        btot_    = dalloc<int64_t>(2 * static_cast<size_t>(max_front_), s);
         // the mirror tiles holding the selection: all selected features, and
         // the first one alone (the last level builds only its totals)
         uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
@@ -1916,7 +2179,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
-        size_t const tsmem = static_cast<size_t>(32) * max_nb_ * 8;
+        size_t const tsmem = k_ttable_bytes;
         BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(tsmem)));
@@ -1977,7 +2240,7 @@ Grower::~Grower()
                     ccount_,  seg_,      payload_, rows_[0],  rows_[1],    scale_,
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
-                    tile_j_[1], bbase_,   dirs_};
+                    tile_j_[1], bbase_,   dirs_,    btot_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -2010,19 +2273,38 @@ void Grower::phase_end(double &acc)
     }
 }
 
-void Grower::quantise(float2 const *gh, uint32_t n)
+void Grower::seed_absmax(float2 const *gh)
 {
-    cudaStream_t s = stream_;
-    BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
+    if (!quant_)
+    {
+        return;
+    }
+    cudaStream_t   s    = stream_;
+    uint32_t const n    = static_cast<uint32_t>(plane_.n_rows);
     uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
                                              148u * 8u);
+    BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
     absmax_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_);
     BB_LAUNCH("absmax_kernel");
+}
+
+void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
+{
+    cudaStream_t s = stream_;
+    uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
+                                             148u * 8u);
+    if (!have_absmax)
+    {
+        BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
+        absmax_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_);
+        BB_LAUNCH("absmax_kernel");
+        n_launch_ += 1;
+    }
     uint2 const key = make_uint2(static_cast<uint32_t>(seed_),
                                  static_cast<uint32_t>(seed_ >> 32));
     quantise_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_, qscale_);
     BB_LAUNCH("quantise_kernel");
-    n_launch_ += 2;
+    n_launch_ += 1;
 }
 
 void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
@@ -2041,7 +2323,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
         if (plane_.u8)
         {
-            size_t const tsmem = static_cast<size_t>(32) * max_nb_ * 8;
+            size_t const tsmem = k_ttable_bytes;
             qhist_t_kernel<<<dim3(k_qctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
@@ -2184,9 +2466,13 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
     leaf_values(t, false);
-    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
-                                                    t, leaf_id, scores, lr);
-    BB_LAUNCH("stamp_kernel");
+    if (!walk_)
+    {
+        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
+                                                        t, leaf_id, scores, lr);
+        BB_LAUNCH("stamp_kernel");
+        n_launch_ += 1;
+    }
     pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
         ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
         dirs_);
@@ -2195,8 +2481,31 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     {
         phase_end(prof_->partition_ms);
     }
-    n_launch_ += 6;
-    bool const     last    = (L + 1) == cfg_.tp.max_depth;
+    n_launch_ += 5;
+    bool const last = (L + 1) == cfg_.tp.max_depth;
+    if (quant_ && last)
+    {
+        // the last level's nodes are leaves: the quantised form needs their
+        // exact totals only (monotone bounds), not their histograms
+        phase_begin();
+        BB_CHECK(cudaMemsetAsync(btot_, 0, sizeof(int64_t) * 2 * max_front_, s));
+        qbuilt_totals_kernel<<<max_bchunks_, k_threads, 0, s>>>(ctl_, bchunks_, rows_out,
+                                                                 qgh8_, btot_);
+        BB_LAUNCH("qbuilt_totals_kernel");
+        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
+            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
+            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_);
+        BB_LAUNCH("qsubtract_totals_kernel");
+        advance_kernel<<<1, 1, 0, s>>>(ctl_);
+        BB_LAUNCH("advance_kernel");
+        n_launch_ += 3;
+        if (prof_ != nullptr)
+        {
+            phase_end(prof_->other_ms);
+        }
+        return;
+    }
     uint32_t const nfb     = last ? 1 : n_sel_;
     build(rows_out, nfb, nxt);
     uint32_t const n_cells = off_h_[nfb]; // the built features: a selection prefix
@@ -2206,7 +2515,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
             ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells,
-            nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_);
+            nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_,
+            nullptr);
         BB_LAUNCH("qsubtract_totals_kernel");
     }
     else
@@ -2228,7 +2538,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
 
 void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
                   TreeOut const &t, uint32_t *leaf_id, float *scores, float lr,
-                  bool identity_root)
+                  bool identity_root, NextRound const *next)
 {
     if (n_root > max_rows_)
     {
@@ -2238,10 +2548,16 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     gh_cur_        = gh;
     root_rows_     = root_rows;
     n_launch_      = 0;
+    walk_          = identity_root && n_root == plane_.n_rows &&
+            (leaf_id != nullptr || scores != nullptr || next != nullptr);
+    if (next != nullptr && !walk_)
+    {
+        throw ConfigError("grower: a fused next round needs every row as the root");
+    }
     if (quant_)
     {
         phase_begin();
-        quantise(gh, static_cast<uint32_t>(plane_.n_rows));
+        quantise(gh, static_cast<uint32_t>(plane_.n_rows), next != nullptr);
         if (prof_ != nullptr)
         {
             phase_end(prof_->other_ms);
@@ -2286,9 +2602,35 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     nodes_cur_ = nodes_[fin];
     rows_cur_  = rows_in;
     leaf_values(t, true);
-    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in, t,
-                                                    leaf_id, scores, lr);
-    BB_LAUNCH("stamp_kernel");
+    if (walk_)
+    {
+        if (next != nullptr && quant_)
+        {
+            BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
+        }
+        uint32_t const n    = static_cast<uint32_t>(plane_.n_rows);
+        uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
+                                                 148u * 8u);
+        WalkArgs a{};
+        a.scores    = scores;
+        a.leaf_id   = leaf_id;
+        a.lr        = lr;
+        a.objective = next != nullptr ? next->objective : 0;
+        a.labels    = next != nullptr ? next->labels : nullptr;
+        a.gh        = next != nullptr ? next->gh : nullptr;
+        a.absmax    = next != nullptr && quant_ ? absmax_ : nullptr;
+        walk_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, static_cast<uint4 const *>(plane_.mirror),
+                                               plane_.n_rows, plane_.cut_off,
+                                               k_mirror_bytes / (plane_.u8 ? 1u : 2u),
+                                               plane_.u8, a);
+        BB_LAUNCH("walk_kernel");
+    }
+    else
+    {
+        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in,
+                                                        t, leaf_id, scores, lr);
+        BB_LAUNCH("stamp_kernel");
+    }
     tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
     BB_LAUNCH("tree_counter_kernel");
     n_launch_ += 3;
@@ -2314,8 +2656,9 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     t.default_left = reinterpret_cast<uint8_t *>(scratch + 32);
     if (quant_)
     {
-        quantise(gh, static_cast<uint32_t>(plane_.n_rows));
+        quantise(gh, static_cast<uint32_t>(plane_.n_rows), false);
     }
+    walk_ = false;
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n, bchunks_, brange_, build_,
                                               t, crows_);
     BB_LAUNCH("root_setup_kernel");

@@ -102,6 +102,16 @@ struct Profile
     uint32_t hist_builds  = 0;
 };
 
+// A resident booster's next round, computed by the final walk over every
+// row once the tree is complete: gh[r] from the updated score and the label,
+// and (quantised form) the maxima the next quantisation scales come from.
+struct NextRound
+{
+    int          objective = 0;
+    float const *labels    = nullptr;
+    float2      *gh        = nullptr;
+};
+
 struct GrowConfig
 {
     TreeParams tp;
@@ -123,9 +133,18 @@ class Grower
     // root_rows: the sampled rows (ascending), n_root of them. out receives
     // the tree; leaf_id (nullable) each sampled row's leaf; scores (nullable)
     // gets scores[r] += lr * leaf value for every sampled row.
+    //
+    // With identity_root (every dataset row, in order) the rows take their
+    // leaf ids and score updates from one walk of the finished tree in row
+    // order, and next (nullable) also has the walk write the next round's
+    // gradient pairs; the quantised form then reads their maxima from that
+    // walk, so the first such round must follow seed_absmax.
     void grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
               TreeOut const &out, uint32_t *leaf_id, float *scores, float lr,
-              bool identity_root = false);
+              bool identity_root = false, NextRound const *next = nullptr);
+    // The quantised form's gradient maxima of gh (every dataset row), for a
+    // first grow() whose next round is fused.
+    void seed_absmax(float2 const *gh);
 
     // One node's histograms (HistogramEngine::populate): quantises (when
     // quantised) and builds every selected feature over the given rows;
@@ -208,6 +227,7 @@ class Grower
     double2  *qscale_   = nullptr; // (scale_g, scale_h) in FP64
     uint16_t *qgh8_     = nullptr; // per row: int8 g | uint8 h << 8
     double2  *partial_  = nullptr; // per partition chunk: leaf (G, H) in FP64
+    int64_t  *btot_     = nullptr; // per build index: exact (G, H) of the last level
     uint32_t  crows_    = 0;       // rows per histogram-build chunk
     bool      quant_    = false;
     uint32_t *dtree_    = nullptr; // device tree counter (the rounding stream)
@@ -217,7 +237,8 @@ class Grower
     Node const     *nodes_cur_ = nullptr;
     uint32_t const *rows_cur_  = nullptr;
     uint32_t const *root_rows_ = nullptr;
-    void      quantise(float2 const *gh, uint32_t n);
+    void      quantise(float2 const *gh, uint32_t n, bool have_absmax);
+    bool      walk_ = false; // this tree's rows are stamped by the final walk
     void      leaf_values(TreeOut const &t, bool final_level);
     uint64_t  seed_     = 0;
     uint32_t  tree_no_  = 0;
