@@ -33,11 +33,11 @@ constexpr uint32_t k_threads    = 256;
 constexpr uint32_t k_part_rows  = 4096; // rows per partition chunk
 constexpr uint32_t k_build_rows = 4096; // rows per histogram-build chunk (exact)
 constexpr uint32_t k_qbuild_rows = 2048;  // rows per histogram-build chunk (quantised)
-constexpr uint32_t k_qctas = 2 * 148;    // persistent quantised-histogram CTAs per tile
+constexpr uint32_t k_qctas = 148;        // persistent quantised-histogram CTAs per tile (one per SM)
 constexpr uint32_t k_qthreads    = 512;   // threads per quantised-histogram CTA
-constexpr uint32_t k_tthreads    = 512;   // threads per conflict-free (u8) histogram CTA
+constexpr uint32_t k_tthreads    = 1024;  // threads per conflict-free (u8) histogram CTA
 constexpr uint32_t k_warps_feat = 8;    // features per count/scatter CTA
-constexpr uint32_t k_find_warps = 4;    // features per find CTA
+constexpr uint32_t k_find_thr   = 128;  // threads per (node, feature) find CTA
 constexpr uint32_t k_chain_stg  = 32;   // elements per lane per cp.async stage
 constexpr uint32_t k_chain_nst  = 4;    // cp.async stages per lane
 constexpr uint32_t k_max_bins   = 4096; // per feature, this engine's ceiling
@@ -523,79 +523,111 @@ __device__ __forceinline__ void warp_best(double &gain, uint32_t &order)
     }
 }
 
-// grid (frontier, ceil(n_sel / 4)), 4 warps: one warp per (node, feature).
+// grid (frontier, n_sel): one CTA of k_find_thr threads per (node,
+// feature), each thread a few candidates. The exact form's prefix is one
+// serial FP64 chain (the reference's summation order); the quantised form's
+// is an exact integer block scan.
 template <bool Q>
-__global__ void __launch_bounds__(32 * k_find_warps)
+__global__ void __launch_bounds__(k_find_thr)
     find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
                 uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                 uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
                 TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale)
 {
     extern __shared__ unsigned char smem_raw[];
-    uint32_t const i = blockIdx.x;
+    __shared__ double   bg_s[k_find_thr / 32];
+    __shared__ uint32_t bo_s[k_find_thr / 32];
+    __shared__ int64_t  wg_s[k_find_thr / 32];
+    __shared__ int64_t  wh_s[k_find_thr / 32];
+    uint32_t const      i = blockIdx.x;
     if (i >= ctl->n_cur)
     {
         return;
     }
-    uint32_t const lane = threadIdx.x & 31;
-    uint32_t const w    = threadIdx.x >> 5;
-    uint32_t const j    = (blockIdx.y * k_find_warps) + w;
-    if (j >= n_sel)
-    {
-        return;
-    }
-    auto *pref = reinterpret_cast<double2 *>(smem_raw) + (w * max_nb);
-    auto *cell = reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(smem_raw) +
-                                            (k_find_warps * max_nb)) +
-                 (w * max_nb);
-    Node const     nd  = nodes[i];
-    uint32_t const nb  = sel_nb[j];
-    Best           out = {0.0, j, 0, 1, 0};
+    uint32_t const tid  = threadIdx.x;
+    uint32_t const lane = tid & 31;
+    uint32_t const w    = tid >> 5;
+    uint32_t const j    = blockIdx.y;
+    auto          *pref = reinterpret_cast<double2 *>(smem_raw);                  // [max_nb]
+    auto          *raw  = reinterpret_cast<unsigned long long *>(pref + max_nb); // [max_nb]
+    Node const     nd   = nodes[i];
+    uint32_t const nb   = sel_nb[j];
+    Best           out  = {0.0, j, 0, 1, 0};
     if (nd.count < 2 * tp.min_data_in_leaf || nb < 2)
     {
-        if (lane == 0)
+        if (tid == 0)
         {
             cand[(i * n_sel) + j] = out;
         }
         return;
     }
     uint32_t const n_cut = nb - 2;
-    using MissT          = typename std::conditional<Q, double, float>::type;
-    MissT          mg;
-    MissT          mh;
-    double         node_sc;
-    double         real_g;
-    double         real_h;
-    bool           miss_empty;
-    double const   l1 = tp.lambda_l1;
-    double const   l2 = tp.lambda_l2;
+    // the cells, 8 bytes each (packed integers or a float2)
+    auto const *src = static_cast<unsigned long long const *>(hist_v) +
+                      (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
+    for (uint32_t b = tid; b < nb; b += k_find_thr)
+    {
+        raw[b] = src[b];
+    }
+    __syncthreads();
+    using MissT = typename std::conditional<Q, double, float>::type;
+    MissT        mg;
+    MissT        mh;
+    double       node_sc;
+    double       real_g;
+    double       real_h;
+    bool         miss_empty;
+    double const l1 = tp.lambda_l1;
+    double const l2 = tp.lambda_l2;
     if constexpr (Q)
     {
-        // exact integer cells: an exact prefix, then one FP64 scaling
-        auto const *src = static_cast<unsigned long long const *>(hist_v) +
-                          (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
-        double2 const sc = *qscale;
-        auto *icell      = reinterpret_cast<unsigned long long *>(cell);
-        for (uint32_t b = lane; b < nb; b += 32)
+        double2 const  sc  = *qscale;
+        uint32_t const run = (n_cut + k_find_thr - 1) / k_find_thr;
+        uint32_t const b0  = min(n_cut, tid * run);
+        uint32_t const b1  = min(n_cut, b0 + run);
+        int64_t        tg  = 0;
+        int64_t        th  = 0;
+        for (uint32_t b = b0; b < b1; ++b)
         {
-            icell[b] = src[b];
+            unsigned long long const c = raw[b];
+            tg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+            th += static_cast<uint32_t>(c);
         }
-        __syncwarp();
-        if (lane == 0)
+        int64_t eg = tg;
+        int64_t eh = th;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1)
         {
-            int64_t pg = 0;
-            int64_t ph = 0;
-            for (uint32_t b = 0; b < n_cut; ++b)
+            int64_t const ug = __shfl_up_sync(0xFFFFFFFFu, eg, o);
+            int64_t const uh = __shfl_up_sync(0xFFFFFFFFu, eh, o);
+            if (lane >= o)
             {
-                unsigned long long const c = icell[b];
-                pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-                ph += static_cast<uint32_t>(c);
-                pref[b] = make_double2(static_cast<double>(pg) * sc.x,
-                                       static_cast<double>(ph) * sc.y);
+                eg += ug;
+                eh += uh;
             }
         }
-        __syncwarp();
-        unsigned long long const mc_ = icell[nb - 1];
+        if (lane == 31)
+        {
+            wg_s[w] = eg;
+            wh_s[w] = eh;
+        }
+        __syncthreads();
+        int64_t pg = eg - tg;
+        int64_t ph = eh - th;
+        for (uint32_t x = 0; x < w; ++x)
+        {
+            pg += wg_s[x];
+            ph += wh_s[x];
+        }
+        for (uint32_t b = b0; b < b1; ++b)
+        {
+            unsigned long long const c = raw[b];
+            pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+            ph += static_cast<uint32_t>(c);
+            pref[b] = make_double2(static_cast<double>(pg) * sc.x,
+                                   static_cast<double>(ph) * sc.y);
+        }
+        unsigned long long const mc_ = raw[nb - 1];
         int64_t const mqg = static_cast<int32_t>(static_cast<uint32_t>(mc_ >> 32));
         int64_t const mqh = static_cast<uint32_t>(mc_);
         mg         = static_cast<double>(mqg) * sc.x;
@@ -608,14 +640,8 @@ __global__ void __launch_bounds__(32 * k_find_warps)
     }
     else
     {
-        float2 const *src = static_cast<float2 const *>(hist_v) +
-                            (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
-        for (uint32_t b = lane; b < nb; b += 32)
-        {
-            cell[b] = src[b];
-        }
-        __syncwarp();
-        if (lane == 0)
+        auto const *cell = reinterpret_cast<float2 const *>(raw);
+        if (tid == 0)
         {
             double lg = 0.0;
             double lh = 0.0;
@@ -626,7 +652,6 @@ __global__ void __launch_bounds__(32 * k_find_warps)
                 pref[b] = make_double2(lg, lh);
             }
         }
-        __syncwarp();
         mg      = cell[nb - 1].x;
         mh      = cell[nb - 1].y;
         node_sc = split_score(nd.sum_g, nd.sum_h, l1, l2);
@@ -635,20 +660,21 @@ __global__ void __launch_bounds__(32 * k_find_warps)
         real_h     = static_cast<double>(nd.sum_h - mh);
         miss_empty = mg == 0.0F && mh == 0.0F;
     }
-    uint32_t const f     = sel[j];
-    int const      mc    = (mono != nullptr && f < n_mono) ? mono[f] : 0;
-    uint32_t const n_dir = miss_empty ? 1 : 2;
-    double         best  = 0.0;
-    uint32_t       order = 0xFFFFFFFFu;
+    __syncthreads();
+    uint32_t const f        = sel[j];
+    int const      mc       = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+    uint32_t const n_dir    = miss_empty ? 1 : 2;
+    double         best     = 0.0;
+    uint32_t       order    = 0xFFFFFFFFu;
     double const   min_gain = tp.min_gain_to_split;
-    for (uint32_t b = lane; b < n_cut; b += 32)
+    for (uint32_t b = tid; b < n_cut; b += k_find_thr)
     {
         double2 const p = pref[b];
         for (uint32_t d = 0; d < n_dir; ++d)
         {
             double gain = 0.0;
-            if (candidate_gain<MissT>(p.x, p.y, mg, mh, real_g, real_h, d == 0, node_sc, tp, mc,
-                               nd.lo, nd.hi, gain) &&
+            if (candidate_gain<MissT>(p.x, p.y, mg, mh, real_g, real_h, d == 0, node_sc, tp,
+                                      mc, nd.lo, nd.hi, gain) &&
                 gain > best && gain >= min_gain)
             {
                 best  = gain;
@@ -659,6 +685,20 @@ __global__ void __launch_bounds__(32 * k_find_warps)
     warp_best(best, order);
     if (lane == 0)
     {
+        bg_s[w] = best;
+        bo_s[w] = order;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        for (uint32_t x = 1; x < k_find_thr / 32; ++x)
+        {
+            if (bg_s[x] > best || (bg_s[x] == best && bo_s[x] < order))
+            {
+                best  = bg_s[x];
+                order = bo_s[x];
+            }
+        }
         if (order != 0xFFFFFFFFu)
         {
             out.gain  = best;
@@ -1089,15 +1129,44 @@ __device__ __forceinline__ uint32_t pick_word(uint32_t const w[8], uint32_t i)
     return (i & 4) != 0 ? f : e;
 }
 
+// Block maxima of |g| and h into the quantiser's two words.
+__device__ __forceinline__ void block_absmax(float mg, float mh, uint32_t *absmax)
+{
+    __shared__ float mg_s[k_threads / 32];
+    __shared__ float mh_s[k_threads / 32];
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        mg = fmaxf(mg, __shfl_xor_sync(0xFFFFFFFFu, mg, o));
+        mh = fmaxf(mh, __shfl_xor_sync(0xFFFFFFFFu, mh, o));
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        mg_s[threadIdx.x >> 5] = mg;
+        mh_s[threadIdx.x >> 5] = mh;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (uint32_t w = 1; w < k_threads / 32; ++w)
+        {
+            mg = fmaxf(mg, mg_s[w]);
+            mh = fmaxf(mh, mh_s[w]);
+        }
+        atomicMax(&absmax[0], __float_as_uint(mg));
+        atomicMax(&absmax[1], __float_as_uint(mh));
+    }
+}
+
+// The general walk: features over several mirror tiles.
 __global__ void __launch_bounds__(k_threads)
-    walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
-                uint32_t const *cut_off, uint32_t per, bool u8, WalkArgs a)
+    walk_tiles_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror,
+                      uint64_t n_rows, uint32_t const *cut_off, uint32_t per, bool u8,
+                      WalkArgs a)
 {
     // per node: x = tile << 8 | position (or the leaf flag), y = split bin |
     // missing bin << 16, z = left | right << 12 | default_left << 24, w = value
     __shared__ uint4 node_s[k_walk_nodes];
-    __shared__ float mg_s[k_threads / 32];
-    __shared__ float mh_s[k_threads / 32];
     uint32_t const   n_nodes = min(ctl->n_nodes, k_walk_nodes);
     for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
     {
@@ -1175,31 +1244,136 @@ __global__ void __launch_bounds__(k_threads)
             }
         }
     }
-    if (a.absmax == nullptr)
+    if (a.absmax != nullptr)
     {
-        return;
+        block_absmax(mg, mh, a.absmax);
     }
-#pragma unroll
-    for (uint32_t o = 16; o > 0; o >>= 1)
+}
+
+// The walk when every feature sits in the first mirror tile: a fixed
+// number of steps (leaves loop to themselves: missing bin 0xFFFF never
+// matches, split bin 0xFFFF takes every code left, and both children are the
+// leaf), fully unrolled, two rows per thread so their chains interleave.
+template <bool U8>
+__device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
+{
+    if constexpr (U8)
     {
-        mg = fmaxf(mg, __shfl_xor_sync(0xFFFFFFFFu, mg, o));
-        mh = fmaxf(mh, __shfl_xor_sync(0xFFFFFFFFu, mh, o));
+        return __byte_perm(pick_word(w, pos >> 2), 0u, 0x4440u | (pos & 3u));
     }
-    if ((threadIdx.x & 31) == 0)
+    else
     {
-        mg_s[threadIdx.x >> 5] = mg;
-        mh_s[threadIdx.x >> 5] = mh;
+        return __byte_perm(pick_word(w, pos >> 1), 0u, 0x4410u | ((pos & 1u) * 0x22u));
+    }
+}
+
+__device__ __forceinline__ uint32_t walk_step(uint4 const e, uint32_t code)
+{
+    bool const left = code == (e.y >> 16) ? ((e.z >> 24) & 1u) != 0 : code <= (e.y & 0xFFFFu);
+    return left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
+}
+
+template <bool U8>
+__global__ void __launch_bounds__(k_threads)
+    walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                uint32_t const *cut_off, uint32_t depth, WalkArgs a)
+{
+    constexpr uint32_t per = U8 ? 32 : 16;
+    __shared__ uint4   node_s[k_walk_nodes];
+    uint32_t const     n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        uint32_t const f = t.feature[i];
+        uint4          e;
+        e.w = __float_as_uint(t.value[i]);
+        if (f == k_leaf_flag)
+        {
+            e.x = 0;
+            e.y = 0xFFFFFFFFu;
+            e.z = i | (i << 12);
+        }
+        else
+        {
+            e.x = f % per;
+            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
+            e.z = t.left[i] | (t.right[i] << 12) |
+                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
+        }
+        node_s[i] = e;
     }
     __syncthreads();
-    if (threadIdx.x == 0)
+    float *__restrict__ scores = a.scores;
+    float           mg     = 0.0F;
+    float           mh     = 0.0F;
+    uint64_t const  stride = static_cast<uint64_t>(gridDim.x) * k_threads;
+    for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
+         r0 < n_rows; r0 += 2 * stride)
     {
-        for (uint32_t w = 1; w < k_threads / 32; ++w)
+        uint64_t const r1  = r0 + stride;
+        bool const     two = r1 < n_rows;
+        uint64_t const rb  = two ? r1 : r0;
+        // independent loads first: both tiles, scores and labels
+        uint4 const a0 = mirror[r0 * 2];
+        uint4 const b0 = mirror[(r0 * 2) + 1];
+        uint4 const a1 = mirror[rb * 2];
+        uint4 const b1 = mirror[(rb * 2) + 1];
+        float const s0 = scores != nullptr ? scores[r0] : 0.0F;
+        float const s1 = scores != nullptr ? scores[rb] : 0.0F;
+        float const y0 = a.gh != nullptr ? a.labels[r0] : 0.0F;
+        float const y1 = a.gh != nullptr ? a.labels[rb] : 0.0F;
+        uint32_t const w0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+        uint32_t const w1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t       n0    = 0;
+        uint32_t       n1    = 0;
+#pragma unroll
+        for (uint32_t d = 0; d < 8; ++d)
         {
-            mg = fmaxf(mg, mg_s[w]);
-            mh = fmaxf(mh, mh_s[w]);
+            if (d < depth)
+            {
+                uint4 const e0 = node_s[n0];
+                uint4 const e1 = node_s[n1];
+                n0             = walk_step(e0, tile_code<U8>(w0, e0.x));
+                n1             = walk_step(e1, tile_code<U8>(w1, e1.x));
+            }
         }
-        atomicMax(&a.absmax[0], __float_as_uint(mg));
-        atomicMax(&a.absmax[1], __float_as_uint(mh));
+        float const v0 = __uint_as_float(node_s[n0].w);
+        float const v1 = __uint_as_float(node_s[n1].w);
+        if (a.leaf_id != nullptr)
+        {
+            a.leaf_id[r0] = n0;
+            if (two)
+            {
+                a.leaf_id[r1] = n1;
+            }
+        }
+        if (scores != nullptr)
+        {
+            float const c0 = s0 + (a.lr * v0);
+            float const c1 = s1 + (a.lr * v1);
+            scores[r0]     = c0;
+            if (two)
+            {
+                scores[r1] = c1;
+            }
+            if (a.gh != nullptr)
+            {
+                float2 const g0 = objective_gradient(a.objective, c0, y0);
+                a.gh[r0]        = g0;
+                mg              = fmaxf(mg, fabsf(g0.x));
+                mh              = fmaxf(mh, fmaxf(g0.y, 0.0F));
+                if (two)
+                {
+                    float2 const g1 = objective_gradient(a.objective, c1, y1);
+                    a.gh[r1]        = g1;
+                    mg              = fmaxf(mg, fabsf(g1.x));
+                    mh              = fmaxf(mh, fmaxf(g1.y, 0.0F));
+                }
+            }
+        }
+    }
+    if (a.absmax != nullptr)
+    {
+        block_absmax(mg, mh, a.absmax);
     }
 }
 
@@ -1647,8 +1821,13 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 // per-lane selector. Slots of unselected features accumulate into columns
 // that are never flushed.
 //
-// Persistent: a grid of k_qctas CTAs per tile, each walking a contiguous
-// range of the level's chunks (node-ordered), so no wave tail; the shared
+// Persistent: a grid of k_qctas CTAs per tile (one per SM), each walking a
+// contiguous range of the level's chunks (node-ordered), so no wave tail.
+// The gathers are software-pipelined: while a chunk's rows are added, every
+// thread's cp.async copies of the next chunk's 32-byte tiles are in flight
+// into its own slots of a double-buffered staging area (so no barrier guards
+// them), with the next chunk's gradient codes and the row ids two chunks
+// ahead loaded into registers. The shared
 // histogram flushes -- one packed 64-bit global add per touched cell,
 // gradient in the high word (two's complement), hessian in the low word --
 // only when the node changes. The 32-bit words cannot overflow in between:
@@ -1724,10 +1903,20 @@ __device__ __forceinline__ void qrow_t(uint32_t base, uint32_t lane4, uint32_t w
     }
 }
 
-__global__ void __launch_bounds__(k_tthreads, 2)
+constexpr uint32_t k_tper   = k_qbuild_rows / k_tthreads; // rows per thread per chunk
+constexpr uint32_t k_tstage = 2 * 2 * k_qbuild_rows * 16; // 2 buffers x 2 halves x rows x 16 B
+constexpr uint32_t k_tsmem  = k_ttable_bytes + k_tstage;
+constexpr uint32_t k_no_row = 0xFFFFFFFFu;
+
+__device__ __forceinline__ void cp_async16(uint32_t smem_addr, void const *gsrc)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr), "l"(gsrc));
+}
+
+__global__ void __launch_bounds__(k_tthreads, 1)
     qhist_t_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
-                   uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
-                   uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
+                   uint32_t const *__restrict__ rows, uint4 const *__restrict__ mirror,
+                   uint64_t n_rows, uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
                    int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
                    uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
@@ -1740,20 +1929,25 @@ __global__ void __launch_bounds__(k_tthreads, 2)
     {
         return;
     }
-    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const tid  = threadIdx.x;
+    uint32_t const lane = tid & 31;
     auto          *tbl  = reinterpret_cast<uint32_t *>(t_smem);
     uint32_t const base = static_cast<uint32_t>(__cvta_generic_to_shared(tbl));
+    // staging after the table: [buffer][half][row slot] x 16 B; a thread
+    // uses only its own slots
+    uint32_t const stg   = base + k_ttable_bytes;
+    auto const    *stg_p = reinterpret_cast<uint4 const *>(
+        reinterpret_cast<unsigned char const *>(t_smem) + k_ttable_bytes);
     uint32_t const tile = tile_ids[blockIdx.y];
-    if (threadIdx.x < 32)
+    if (tid < 32)
     {
-        j_s[threadIdx.x] = tile_j[(blockIdx.y * 32) + threadIdx.x];
+        j_s[tid] = tile_j[(blockIdx.y * 32) + tid];
     }
-    for (uint32_t x = threadIdx.x; x < k_ttable_bytes / 4; x += k_tthreads)
+    for (uint32_t x = tid; x < k_ttable_bytes / 4; x += k_tthreads)
     {
         tbl[x] = 0;
     }
     __syncthreads();
-    // byte k ^ (lane % 4) of a word to bits 8..15, zeros elsewhere
     uint32_t sel[4];
 #pragma unroll
     for (uint32_t k = 0; k < 4; ++k)
@@ -1763,37 +1957,87 @@ __global__ void __launch_bounds__(k_tthreads, 2)
     uint32_t const lane4 = lane * 4;
     uint32_t const wsel  = lane >> 2;
     uint4 const   *mt    = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
-    uint32_t       node  = bchunks[c_a].node;
+    // the thread's row ids of chunk c (k_no_row past the chunk's end)
+    auto ids_of = [&](uint32_t c, uint32_t (&out)[k_tper])
+    {
+        Chunk const ch = c < c_b ? bchunks[c] : Chunk{0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t m = 0; m < k_tper; ++m)
+        {
+            uint32_t const k = (m * k_tthreads) + tid;
+            out[m] = k < ch.count ? (rows != nullptr ? rows[ch.begin + k] : ch.begin + k)
+                                  : k_no_row;
+        }
+    };
+    // the copies of those rows' tiles into buffer buf, as one group
+    auto issue = [&](uint32_t const (&id)[k_tper], uint32_t buf)
+    {
+#pragma unroll
+        for (uint32_t m = 0; m < k_tper; ++m)
+        {
+            if (id[m] != k_no_row)
+            {
+                uint32_t const slot = (m * k_tthreads) + tid;
+                uint4 const   *src  = mt + (static_cast<uint64_t>(id[m]) * 2);
+                cp_async16(stg + ((((buf * 2) + 0) * k_qbuild_rows) + slot) * 16, src);
+                cp_async16(stg + ((((buf * 2) + 1) * k_qbuild_rows) + slot) * 16, src + 1);
+            }
+        }
+        cp_async_commit();
+    };
+    auto codes_of = [&](uint32_t const (&id)[k_tper], uint32_t (&q)[k_tper])
+    {
+#pragma unroll
+        for (uint32_t m = 0; m < k_tper; ++m)
+        {
+            q[m] = id[m] != k_no_row ? static_cast<uint32_t>(qgh[id[m]]) : 0u;
+        }
+    };
+    uint32_t id_c[k_tper];
+    uint32_t id_n[k_tper];
+    uint32_t id_nn[k_tper];
+    uint32_t q_c[k_tper];
+    uint32_t q_n[k_tper];
+    ids_of(c_a, id_c);
+    issue(id_c, 0);
+    codes_of(id_c, q_c);
+    ids_of(c_a + 1, id_n);
+    uint32_t node = bchunks[c_a].node;
     for (uint32_t c = c_a; c < c_b; ++c)
     {
-        Chunk const ch = bchunks[c];
-        if (ch.node != node)
+        uint32_t const buf = (c - c_a) & 1;
+        // next chunk's copies and codes, the ids after it
+        issue(id_n, buf ^ 1);
+        codes_of(id_n, q_n);
+        ids_of(c + 2, id_nn);
+        uint32_t const cnode = bchunks[c].node;
+        if (cnode != node)
         {
             qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
                      hist + (static_cast<uint64_t>(build[node]) * total_cells));
-            node = ch.node;
+            node = cnode;
         }
-        // two rows per thread per pass, both loaded before either is added
-        for (uint32_t k = threadIdx.x; k < ch.count; k += 2 * k_tthreads)
+        cp_async_wait<1>(); // this thread's copies of chunk c have landed
+#pragma unroll
+        for (uint32_t m = 0; m < k_tper; ++m)
         {
-            bool const     two = k + k_tthreads < ch.count;
-            uint32_t const r0  = rows != nullptr ? rows[ch.begin + k] : ch.begin + k;
-            uint32_t const r1  = !two ? r0
-                                      : (rows != nullptr ? rows[ch.begin + k + k_tthreads]
-                                                         : ch.begin + k + k_tthreads);
-            uint32_t const q0  = qgh[r0];
-            uint4 const    a0  = mt[static_cast<uint64_t>(r0) * 2];
-            uint4 const    b0  = mt[(static_cast<uint64_t>(r0) * 2) + 1];
-            uint32_t const q1  = qgh[r1];
-            uint4 const    a1  = mt[static_cast<uint64_t>(r1) * 2];
-            uint4 const    b1  = mt[(static_cast<uint64_t>(r1) * 2) + 1];
-            qrow_t(base, lane4, wsel, sel, a0, b0, q0);
-            if (two)
+            if (id_c[m] != k_no_row)
             {
-                qrow_t(base, lane4, wsel, sel, a1, b1, q1);
+                uint32_t const slot = (m * k_tthreads) + tid;
+                uint4 const    va   = stg_p[((buf * 2) * k_qbuild_rows) + slot];
+                uint4 const    vb   = stg_p[(((buf * 2) + 1) * k_qbuild_rows) + slot];
+                qrow_t(base, lane4, wsel, sel, va, vb, q_c[m]);
             }
         }
+#pragma unroll
+        for (uint32_t m = 0; m < k_tper; ++m)
+        {
+            id_c[m] = id_n[m];
+            id_n[m] = id_nn[m];
+            q_c[m]  = q_n[m];
+        }
     }
+    cp_async_wait<0>();
     qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
              hist + (static_cast<uint64_t>(build[node]) * total_cells));
 }
@@ -1822,6 +2066,8 @@ __global__ void qroot_totals_kernel(Node *nodes, unsigned long long const *hist,
     }
 }
 
+constexpr uint32_t k_sub_cells = 1024; // cells per subtraction CTA
+
 // Larger child = parent - smaller child in exact integers (both packed
 // words subtract without borrow: a child's hessian sum never exceeds its
 // parent's); children's totals and monotone bounds from the integer sums.
@@ -1844,11 +2090,15 @@ __global__ void __launch_bounds__(k_threads)
     auto const    *hp = hist_cur + (static_cast<uint64_t>(p) * total_cells);
     auto const    *hs = hist_nxt + (static_cast<uint64_t>(s) * total_cells);
     auto          *hl = hist_nxt + (static_cast<uint64_t>(l) * total_cells);
-    for (uint32_t x = threadIdx.x; x < n_cells; x += k_threads)
+    // blockIdx.y takes cells [y * k_sub_cells, (y + 1) * k_sub_cells)
+    uint32_t const x0 = blockIdx.y * k_sub_cells;
+    uint32_t const x1 = min(n_cells, x0 + k_sub_cells);
+#pragma unroll 4
+    for (uint32_t x = x0 + threadIdx.x; x < x1; x += k_threads)
     {
         hl[x] = hp[x] - hs[x];
     }
-    if (threadIdx.x >= 32)
+    if (blockIdx.y != 0 || threadIdx.x >= 32)
     {
         return;
     }
@@ -2140,7 +2390,8 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     {
         absmax_  = dalloc<uint32_t>(2, s);
         qscale_  = dalloc<double2>(1, s);
-        qgh8_    = dalloc<uint16_t>(max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows, s);
+        // +2: the histogram copies whole 4-byte words of codes
+        qgh8_    = dalloc<uint16_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 2, s);
         partial_ = dalloc<double2>(max_pchunks_, s);
         btot_    = dalloc<int64_t>(2 * static_cast<size_t>(max_front_), s);
         // the mirror tiles holding the selection: all selected features, and
@@ -2179,7 +2430,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
-        size_t const tsmem = k_ttable_bytes;
+        size_t const tsmem = k_tsmem;
         BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(tsmem)));
@@ -2195,7 +2446,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     BB_CHECK(cudaStreamSynchronize(s));
 
     // dynamic shared memory ceilings
-    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
+    size_t const find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
     if (find_smem > 227 * 1024)
     {
         throw ConfigError("grower: bins per feature exceed the shared-memory budget");
@@ -2323,7 +2574,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
         if (plane_.u8)
         {
-            size_t const tsmem = k_ttable_bytes;
+            size_t const tsmem = k_tsmem;
             qhist_t_kernel<<<dim3(k_qctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
@@ -2420,18 +2671,18 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     cudaStream_t s   = stream_;
     int const    cur = static_cast<int>(L & 1);
     int const    nxt = cur ^ 1;
-    size_t const find_smem = k_find_warps * max_nb_ * (sizeof(double2) + sizeof(float2));
+    size_t const find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
     phase_begin();
-    dim3 const fgrid(max_front_, ceil_div(n_sel_, k_find_warps));
+    dim3 const fgrid(max_front_, n_sel_);
     if (quant_)
     {
-        find_kernel<true><<<fgrid, 32 * k_find_warps, find_smem, s>>>(
+        find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
             mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
     }
     else
     {
-        find_kernel<false><<<fgrid, 32 * k_find_warps, find_smem, s>>>(
+        find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
             mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
     }
@@ -2512,7 +2763,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     phase_begin();
     if (quant_)
     {
-        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+        qsubtract_totals_kernel<<<dim3(max_front_, std::max(1u, ceil_div(n_cells, k_sub_cells))),
+                                  k_threads, 0, s>>>(
             ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells,
             nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_,
@@ -2619,10 +2871,23 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         a.labels    = next != nullptr ? next->labels : nullptr;
         a.gh        = next != nullptr ? next->gh : nullptr;
         a.absmax    = next != nullptr && quant_ ? absmax_ : nullptr;
-        walk_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, static_cast<uint4 const *>(plane_.mirror),
-                                               plane_.n_rows, plane_.cut_off,
-                                               k_mirror_bytes / (plane_.u8 ? 1u : 2u),
-                                               plane_.u8, a);
+        uint32_t const per  = k_mirror_bytes / (plane_.u8 ? 1u : 2u);
+        auto const    *mir  = static_cast<uint4 const *>(plane_.mirror);
+        if (plane_.n_feats > per)
+        {
+            walk_tiles_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
+                                                         plane_.cut_off, per, plane_.u8, a);
+        }
+        else if (plane_.u8)
+        {
+            walk_kernel<true><<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
+                                                         plane_.cut_off, cfg_.tp.max_depth, a);
+        }
+        else
+        {
+            walk_kernel<false><<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
+                                                          plane_.cut_off, cfg_.tp.max_depth, a);
+        }
         BB_LAUNCH("walk_kernel");
     }
     else
