@@ -750,7 +750,7 @@ __device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *ran
 __global__ void __launch_bounds__(k_plan_thr)
     plan_kernel(Ctl *ctl, Node *nodes, Best const *cand, Best *best, uint32_t n_sel,
                 uint32_t const *sel, float const *cuts, uint32_t const *cut_off,
-                TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr)
+                TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound)
 {
     uint32_t const n_cur = ctl->n_cur;
     uint32_t const lane  = threadIdx.x & 31;
@@ -786,6 +786,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     Node           nd       = live ? nodes[i] : Node{};
     if (live)
     {
+        nbound[nd.id] = make_double2(nd.lo, nd.hi); // for a later leaf renewal
         if (split)
         {
             uint32_t const f     = sel[bs.feature];
@@ -1101,11 +1102,22 @@ __global__ void __launch_bounds__(k_threads)
 // The final walk, for trees grown over every row: each row (one thread,
 // rows in order) walks the finished tree through its 32-byte mirror tiles
 // with the partition's own rule (routes_left on the split bin, the last bin
-// following default_left), so it reaches the leaf whose segment held it.
-// It then takes scores[r] = scores[r] + lr * value -- the stamp's arithmetic,
-// now coalesced -- its leaf id, and, for a resident booster, the next round's
-// gradient pair and a block maximum of |g| and h for the next quantisation.
-constexpr uint32_t k_walk_nodes = 512; // a depth-8 tree has at most 511
+// following default_left), so it reaches the leaf whose segment held it --
+// and rows read in order are coalesced, where the partitioned rows are a
+// gather. The walk takes a fixed number of steps: leaves loop to themselves
+// (missing bin 0xFFFF never matches, split bin 0xFFFF sends every code left,
+// both children are the leaf). One pass (exact form) updates
+// scores[r] = scores[r] + lr * value -- the stamp's arithmetic -- and the
+// leaf ids and, for a resident booster, writes the next round's gradient
+// pairs and their maxima. The quantised form renews its leaves from
+// full-precision gradients first: pass A walks and sums each leaf's
+// (g, h) as exact fixed-point integers (2^38 / max |g| and 2^38 / max h per
+// unit, so at most 2^62 over 2^24 rows; integer sums are order-free, hence
+// deterministic), a one-CTA kernel turns them into FP64 Newton values, and
+// pass B applies them from the leaf id pass A recorded.
+constexpr uint32_t k_walk_nodes = 512;     // a depth-8 tree has at most 511
+constexpr uint32_t k_no_tile    = 0xFFFFFFu;
+constexpr double   k_fix_unit   = 274877906944.0; // 2^38
 
 struct WalkArgs
 {
@@ -1127,6 +1139,91 @@ __device__ __forceinline__ uint32_t pick_word(uint32_t const w[8], uint32_t i)
     uint32_t const e = (i & 2) != 0 ? b : a;
     uint32_t const f = (i & 2) != 0 ? d : c;
     return (i & 4) != 0 ? f : e;
+}
+
+template <bool U8>
+__device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
+{
+    if constexpr (U8)
+    {
+        return __byte_perm(pick_word(w, pos >> 2), 0u, 0x4440u | (pos & 3u));
+    }
+    else
+    {
+        return __byte_perm(pick_word(w, pos >> 1), 0u, 0x4410u | ((pos & 1u) * 0x22u));
+    }
+}
+
+__device__ __forceinline__ uint32_t walk_step(uint4 const e, uint32_t code)
+{
+    bool const left = code == (e.y >> 16) ? ((e.z >> 24) & 1u) != 0 : code <= (e.y & 0xFFFFu);
+    return left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
+}
+
+// The tree as one 16-byte entry per node: x = tile << 8 | position (a leaf:
+// no tile), y = split bin | missing bin << 16, z = left | right << 12 |
+// default_left << 24, w = value bits.
+__device__ __forceinline__ uint32_t load_node_table(uint4 *node_s, Ctl const *ctl,
+                                                    TreeOut const &t, uint32_t const *cut_off,
+                                                    uint32_t per)
+{
+    uint32_t const n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        uint32_t const f = t.feature[i];
+        uint4          e;
+        e.w = __float_as_uint(t.value[i]);
+        if (f == k_leaf_flag)
+        {
+            e.x = k_no_tile << 8;
+            e.y = 0xFFFFFFFFu;
+            e.z = i | (i << 12);
+        }
+        else
+        {
+            e.x = ((f / per) << 8) | (f % per);
+            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
+            e.z = t.left[i] | (t.right[i] << 12) |
+                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
+        }
+        node_s[i] = e;
+    }
+    __syncthreads();
+    return n_nodes;
+}
+
+// Row r's leaf: its tile of the root's feature is passed in; with MULTI the
+// walk fetches another tile when a node's feature lives there.
+template <bool U8, bool MULTI>
+__device__ __forceinline__ uint32_t walk_row(uint4 const *node_s, uint4 const *__restrict__ mirror,
+                                             uint64_t n_rows, uint64_t r, uint32_t depth,
+                                             uint4 ta, uint4 tb, uint32_t held)
+{
+    uint32_t w[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+    uint32_t n    = 0;
+#pragma unroll
+    for (uint32_t d = 0; d < 8; ++d)
+    {
+        if (d < depth)
+        {
+            uint4 const e = node_s[n];
+            if constexpr (MULTI)
+            {
+                uint32_t const tile = e.x >> 8;
+                if (tile != held && tile != k_no_tile)
+                {
+                    uint4 const *src = mirror + (((static_cast<uint64_t>(tile) * n_rows) + r) * 2);
+                    uint4 const  xa  = src[0];
+                    uint4 const  xb  = src[1];
+                    w[0] = xa.x; w[1] = xa.y; w[2] = xa.z; w[3] = xa.w;
+                    w[4] = xb.x; w[5] = xb.y; w[6] = xb.z; w[7] = xb.w;
+                    held = tile;
+                }
+            }
+            n = walk_step(e, tile_code<U8>(w, e.x & 0xFFu));
+        }
+    }
+    return n;
 }
 
 // Block maxima of |g| and h into the quantiser's two words.
@@ -1158,90 +1255,64 @@ __device__ __forceinline__ void block_absmax(float mg, float mh, uint32_t *absma
     }
 }
 
-// The general walk: features over several mirror tiles.
-__global__ void __launch_bounds__(k_threads)
-    walk_tiles_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror,
-                      uint64_t n_rows, uint32_t const *cut_off, uint32_t per, bool u8,
-                      WalkArgs a)
+// A row's score update and, for a resident booster, its next gradient pair.
+__device__ __forceinline__ void apply_leaf(WalkArgs const &a, uint64_t r, uint32_t leaf,
+                                           float s_old, float y, float v, float &mg, float &mh)
 {
-    // per node: x = tile << 8 | position (or the leaf flag), y = split bin |
-    // missing bin << 16, z = left | right << 12 | default_left << 24, w = value
-    __shared__ uint4 node_s[k_walk_nodes];
-    uint32_t const   n_nodes = min(ctl->n_nodes, k_walk_nodes);
-    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    if (a.leaf_id != nullptr)
     {
-        uint32_t const f = t.feature[i];
-        uint4          e;
-        e.w = __float_as_uint(t.value[i]);
-        if (f == k_leaf_flag)
-        {
-            e.x = k_leaf_flag;
-            e.y = 0;
-            e.z = 0;
-        }
-        else
-        {
-            e.x = ((f / per) << 8) | (f % per);
-            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
-            e.z = t.left[i] | (t.right[i] << 12) |
-                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
-        }
-        node_s[i] = e;
+        a.leaf_id[r] = leaf;
     }
-    __syncthreads();
-    uint4 const    root   = node_s[0];
-    uint32_t const tile0  = root.x == k_leaf_flag ? 0u : root.x >> 8;
-    float *__restrict__ scores = a.scores;
-    float mg = 0.0F;
-    float mh = 0.0F;
-    uint64_t const stride = static_cast<uint64_t>(gridDim.x) * k_threads;
-    for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x; r < n_rows;
-         r += stride)
+    if (a.scores == nullptr)
     {
-        // independent loads first: the root's tile, the score, the label
-        uint4 const *src = mirror + (((static_cast<uint64_t>(tile0) * n_rows) + r) * 2);
-        uint4 const  va  = src[0];
-        uint4 const  vb  = src[1];
-        float const  s0  = scores != nullptr ? scores[r] : 0.0F;
-        float const  y   = a.gh != nullptr ? a.labels[r] : 0.0F;
-        uint32_t     w[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
-        uint32_t     held = tile0;
-        uint32_t     node = 0;
-        uint4        e    = root;
-        for (uint32_t d = 0; d < 16 && e.x != k_leaf_flag; ++d)
+        return;
+    }
+    float const s = s_old + (a.lr * v);
+    a.scores[r]   = s;
+    if (a.gh != nullptr)
+    {
+        float2 const g = objective_gradient(a.objective, s, y);
+        a.gh[r]        = g;
+        mg             = fmaxf(mg, fabsf(g.x));
+        mh             = fmaxf(mh, fmaxf(g.y, 0.0F));
+    }
+}
+
+// One pass: walk and apply (exact form), two rows per thread so their
+// chains interleave.
+template <bool U8, bool MULTI>
+__global__ void __launch_bounds__(k_threads)
+    walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                uint32_t const *cut_off, uint32_t depth, WalkArgs a)
+{
+    constexpr uint32_t per = U8 ? 32 : 16;
+    __shared__ uint4   node_s[k_walk_nodes];
+    load_node_table(node_s, ctl, t, cut_off, per);
+    uint32_t const root_tile = (node_s[0].x >> 8) == k_no_tile ? 0u : node_s[0].x >> 8;
+    uint4 const   *mt        = mirror + (static_cast<uint64_t>(root_tile) * n_rows * 2);
+    float          mg        = 0.0F;
+    float          mh        = 0.0F;
+    uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
+    for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
+         r0 < n_rows; r0 += 2 * stride)
+    {
+        uint64_t const r1  = r0 + stride;
+        bool const     two = r1 < n_rows;
+        uint64_t const rb  = two ? r1 : r0;
+        uint4 const    a0  = mt[r0 * 2];
+        uint4 const    b0  = mt[(r0 * 2) + 1];
+        uint4 const    a1  = mt[rb * 2];
+        uint4 const    b1  = mt[(rb * 2) + 1];
+        float const    s0  = a.scores != nullptr ? a.scores[r0] : 0.0F;
+        float const    s1  = a.scores != nullptr ? a.scores[rb] : 0.0F;
+        float const    y0  = a.gh != nullptr ? a.labels[r0] : 0.0F;
+        float const    y1  = a.gh != nullptr ? a.labels[rb] : 0.0F;
+        uint32_t const n0 = walk_row<U8, MULTI>(node_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
+        uint32_t const n1 = walk_row<U8, MULTI>(node_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
+        apply_leaf(a, r0, n0, s0, y0, __uint_as_float(node_s[n0].w), mg, mh);
+        if (two)
         {
-            uint32_t const tile = e.x >> 8;
-            uint32_t const pos  = e.x & 0xFFu;
-            if (tile != held)
-            {
-                uint4 const *s2 = mirror + (((static_cast<uint64_t>(tile) * n_rows) + r) * 2);
-                uint4 const  xa = s2[0];
-                uint4 const  xb = s2[1];
-                w[0] = xa.x; w[1] = xa.y; w[2] = xa.z; w[3] = xa.w;
-                w[4] = xb.x; w[5] = xb.y; w[6] = xb.z; w[7] = xb.w;
-                held = tile;
-            }
-            uint32_t const b = u8 ? (pick_word(w, pos >> 2) >> ((pos & 3) * 8)) & 0xFFu
-                                  : (pick_word(w, pos >> 1) >> ((pos & 1) * 16)) & 0xFFFFu;
-            bool const left = routes_left(b, e.y >> 16, e.y & 0xFFFFu, ((e.z >> 24) & 1u) != 0);
-            node            = left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
-            e               = node_s[node];
-        }
-        if (a.leaf_id != nullptr)
-        {
-            a.leaf_id[r] = node;
-        }
-        if (scores != nullptr)
-        {
-            float const sc = s0 + (a.lr * __uint_as_float(e.w));
-            scores[r]      = sc;
-            if (a.gh != nullptr)
-            {
-                float2 const g = objective_gradient(a.objective, sc, y);
-                a.gh[r]        = g;
-                mg             = fmaxf(mg, fabsf(g.x));
-                mh             = fmaxf(mh, fmaxf(g.y, 0.0F));
-            }
+            apply_leaf(a, r1, n1, s1, y1, __uint_as_float(node_s[n1].w), mg, mh);
         }
     }
     if (a.absmax != nullptr)
@@ -1250,126 +1321,117 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
-// The walk when every feature sits in the first mirror tile: a fixed
-// number of steps (leaves loop to themselves: missing bin 0xFFFF never
-// matches, split bin 0xFFFF takes every code left, and both children are the
-// leaf), fully unrolled, two rows per thread so their chains interleave.
-template <bool U8>
-__device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
-{
-    if constexpr (U8)
-    {
-        return __byte_perm(pick_word(w, pos >> 2), 0u, 0x4440u | (pos & 3u));
-    }
-    else
-    {
-        return __byte_perm(pick_word(w, pos >> 1), 0u, 0x4410u | ((pos & 1u) * 0x22u));
-    }
-}
-
-__device__ __forceinline__ uint32_t walk_step(uint4 const e, uint32_t code)
-{
-    bool const left = code == (e.y >> 16) ? ((e.z >> 24) & 1u) != 0 : code <= (e.y & 0xFFFFu);
-    return left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
-}
-
-template <bool U8>
+// Pass A of the quantised form: each row's leaf (as 16 bits) and every
+// leaf's exact fixed-point (g, h) sums -- shared-memory 64-bit integer adds,
+// then one global add per touched leaf and CTA.
+template <bool U8, bool MULTI>
 __global__ void __launch_bounds__(k_threads)
-    walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
-                uint32_t const *cut_off, uint32_t depth, WalkArgs a)
+    walk_sum_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror,
+                    uint64_t n_rows, uint32_t const *cut_off, uint32_t depth,
+                    float2 const *__restrict__ gh, uint32_t const *absmax,
+                    uint16_t *__restrict__ leaf16, unsigned long long *acc)
 {
-    constexpr uint32_t per = U8 ? 32 : 16;
-    __shared__ uint4   node_s[k_walk_nodes];
-    uint32_t const     n_nodes = min(ctl->n_nodes, k_walk_nodes);
-    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    constexpr uint32_t  per = U8 ? 32 : 16;
+    __shared__ uint4    node_s[k_walk_nodes];
+    __shared__ unsigned long long acc_s[2 * k_walk_nodes];
+    for (uint32_t i = threadIdx.x; i < 2 * k_walk_nodes; i += k_threads)
     {
-        uint32_t const f = t.feature[i];
-        uint4          e;
-        e.w = __float_as_uint(t.value[i]);
-        if (f == k_leaf_flag)
-        {
-            e.x = 0;
-            e.y = 0xFFFFFFFFu;
-            e.z = i | (i << 12);
-        }
-        else
-        {
-            e.x = f % per;
-            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
-            e.z = t.left[i] | (t.right[i] << 12) |
-                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
-        }
-        node_s[i] = e;
+        acc_s[i] = 0ULL;
     }
-    __syncthreads();
-    float *__restrict__ scores = a.scores;
-    float           mg     = 0.0F;
-    float           mh     = 0.0F;
-    uint64_t const  stride = static_cast<uint64_t>(gridDim.x) * k_threads;
+    uint32_t const n_nodes   = load_node_table(node_s, ctl, t, cut_off, per);
+    uint32_t const root_tile = (node_s[0].x >> 8) == k_no_tile ? 0u : node_s[0].x >> 8;
+    uint4 const   *mt        = mirror + (static_cast<uint64_t>(root_tile) * n_rows * 2);
+    float const    mgx       = __uint_as_float(absmax[0]);
+    float const    mhx       = __uint_as_float(absmax[1]);
+    double const   fg        = mgx > 0.0F ? k_fix_unit / static_cast<double>(mgx) : 1.0;
+    double const   fh        = mhx > 0.0F ? k_fix_unit / static_cast<double>(mhx) : 1.0;
+    uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
     for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
          r0 < n_rows; r0 += 2 * stride)
     {
         uint64_t const r1  = r0 + stride;
         bool const     two = r1 < n_rows;
         uint64_t const rb  = two ? r1 : r0;
-        // independent loads first: both tiles, scores and labels
-        uint4 const a0 = mirror[r0 * 2];
-        uint4 const b0 = mirror[(r0 * 2) + 1];
-        uint4 const a1 = mirror[rb * 2];
-        uint4 const b1 = mirror[(rb * 2) + 1];
-        float const s0 = scores != nullptr ? scores[r0] : 0.0F;
-        float const s1 = scores != nullptr ? scores[rb] : 0.0F;
-        float const y0 = a.gh != nullptr ? a.labels[r0] : 0.0F;
-        float const y1 = a.gh != nullptr ? a.labels[rb] : 0.0F;
-        uint32_t const w0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
-        uint32_t const w1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
-        uint32_t       n0    = 0;
-        uint32_t       n1    = 0;
-#pragma unroll
-        for (uint32_t d = 0; d < 8; ++d)
+        uint4 const    a0  = mt[r0 * 2];
+        uint4 const    b0  = mt[(r0 * 2) + 1];
+        uint4 const    a1  = mt[rb * 2];
+        uint4 const    b1  = mt[(rb * 2) + 1];
+        float2 const   g0  = gh[r0];
+        float2 const   g1  = gh[rb];
+        uint32_t const n0 = walk_row<U8, MULTI>(node_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
+        uint32_t const n1 = walk_row<U8, MULTI>(node_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
+        leaf16[r0] = static_cast<uint16_t>(n0);
+        atomicAdd(&acc_s[2 * n0], static_cast<unsigned long long>(
+                                      llrint(static_cast<double>(g0.x) * fg)));
+        atomicAdd(&acc_s[(2 * n0) + 1], static_cast<unsigned long long>(
+                                            llrint(static_cast<double>(fmaxf(g0.y, 0.0F)) * fh)));
+        if (two)
         {
-            if (d < depth)
-            {
-                uint4 const e0 = node_s[n0];
-                uint4 const e1 = node_s[n1];
-                n0             = walk_step(e0, tile_code<U8>(w0, e0.x));
-                n1             = walk_step(e1, tile_code<U8>(w1, e1.x));
-            }
+            leaf16[r1] = static_cast<uint16_t>(n1);
+            atomicAdd(&acc_s[2 * n1], static_cast<unsigned long long>(
+                                          llrint(static_cast<double>(g1.x) * fg)));
+            atomicAdd(&acc_s[(2 * n1) + 1],
+                      static_cast<unsigned long long>(
+                          llrint(static_cast<double>(fmaxf(g1.y, 0.0F)) * fh)));
         }
-        float const v0 = __uint_as_float(node_s[n0].w);
-        float const v1 = __uint_as_float(node_s[n1].w);
-        if (a.leaf_id != nullptr)
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 2 * n_nodes; i += k_threads)
+    {
+        if (acc_s[i] != 0ULL)
         {
-            a.leaf_id[r0] = n0;
-            if (two)
-            {
-                a.leaf_id[r1] = n1;
-            }
+            atomicAdd(&acc[i], acc_s[i]);
         }
-        if (scores != nullptr)
+    }
+}
+
+// The quantised form's leaf values from pass A's sums: FP64 Newton values
+// under each leaf's monotone bounds.
+__global__ void __launch_bounds__(k_threads)
+    leaf_fix_kernel(Ctl const *ctl, TreeOut t, unsigned long long const *acc,
+                    double2 const *nbound, uint32_t const *absmax, TreeParams tp)
+{
+    float const  mgx = __uint_as_float(absmax[0]);
+    float const  mhx = __uint_as_float(absmax[1]);
+    double const fg  = mgx > 0.0F ? k_fix_unit / static_cast<double>(mgx) : 1.0;
+    double const fh  = mhx > 0.0F ? k_fix_unit / static_cast<double>(mhx) : 1.0;
+    uint32_t const n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        if (t.feature[i] != k_leaf_flag)
         {
-            float const c0 = s0 + (a.lr * v0);
-            float const c1 = s1 + (a.lr * v1);
-            scores[r0]     = c0;
-            if (two)
-            {
-                scores[r1] = c1;
-            }
-            if (a.gh != nullptr)
-            {
-                float2 const g0 = objective_gradient(a.objective, c0, y0);
-                a.gh[r0]        = g0;
-                mg              = fmaxf(mg, fabsf(g0.x));
-                mh              = fmaxf(mh, fmaxf(g0.y, 0.0F));
-                if (two)
-                {
-                    float2 const g1 = objective_gradient(a.objective, c1, y1);
-                    a.gh[r1]        = g1;
-                    mg              = fmaxf(mg, fabsf(g1.x));
-                    mh              = fmaxf(mh, fmaxf(g1.y, 0.0F));
-                }
-            }
+            continue;
         }
+        double const g = static_cast<double>(static_cast<int64_t>(acc[2 * i])) / fg;
+        double const h = static_cast<double>(static_cast<int64_t>(acc[(2 * i) + 1])) / fh;
+        double2 const b = nbound[i];
+        t.value[i] = static_cast<float>(
+            bounded_leaf_weight(g, h, tp.lambda_l1, tp.lambda_l2, b.x, b.y));
+    }
+}
+
+// Pass B of the quantised form: apply the renewed values by pass A's leaf ids.
+__global__ void __launch_bounds__(k_threads)
+    walk_apply_kernel(Ctl const *ctl, TreeOut t, uint64_t n_rows,
+                      uint16_t const *__restrict__ leaf16, WalkArgs a)
+{
+    __shared__ float val_s[k_walk_nodes];
+    uint32_t const   n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        val_s[i] = t.value[i];
+    }
+    __syncthreads();
+    float          mg     = 0.0F;
+    float          mh     = 0.0F;
+    uint64_t const stride = static_cast<uint64_t>(gridDim.x) * k_threads;
+    for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x; r < n_rows;
+         r += stride)
+    {
+        uint32_t const n = leaf16[r];
+        float const    s = a.scores != nullptr ? a.scores[r] : 0.0F;
+        float const    y = a.gh != nullptr ? a.labels[r] : 0.0F;
+        apply_leaf(a, r, n, s, y, val_s[n], mg, mh);
     }
     if (a.absmax != nullptr)
     {
@@ -1386,10 +1448,20 @@ __global__ void __launch_bounds__(k_threads)
                     Best const *best, uint32_t const *pleft, uint32_t const *prbase,
                     uint32_t const *nleft, uint32_t const *dst,
                     uint32_t const *__restrict__ rows, uint32_t *__restrict__ rows_out,
-                    uint32_t const *__restrict__ dirs)
+                    uint32_t const *__restrict__ dirs, unsigned long long *zhist,
+                    uint32_t const *build, uint32_t total_cells, uint32_t n_zcells)
 {
     __shared__ uint32_t wsum[k_threads / 32];
     uint32_t const      c = blockIdx.x;
+    // the quantised build that follows adds into zeroed cells: every CTA
+    // clears a share of the built slots' first n_zcells cells
+    uint64_t const nz = static_cast<uint64_t>(ctl->n_build) * n_zcells;
+    for (uint64_t x = (static_cast<uint64_t>(c) * k_threads) + threadIdx.x; x < nz;
+         x += static_cast<uint64_t>(gridDim.x) * k_threads)
+    {
+        uint64_t const i = x / n_zcells;
+        zhist[(static_cast<uint64_t>(build[i]) * total_cells) + (x - (i * n_zcells))] = 0ULL;
+    }
     if (c >= ctl->n_pchunks)
     {
         return;
@@ -1467,13 +1539,17 @@ __global__ void __launch_bounds__(k_threads)
 // Larger child = parent - smaller child, cell by cell in float
 // (finish_split); then both children's totals and monotone bounds.
 __global__ void __launch_bounds__(k_threads)
-    subtract_totals_kernel(Ctl const *ctl, uint32_t const *bpair, float2 const *hist_cur,
+    subtract_totals_kernel(Ctl *ctl, uint32_t const *bpair, float2 const *hist_cur,
                            float2 *hist_nxt, uint32_t total_cells, uint32_t n_cells,
                            Node const *cur, Node *next, Best const *best,
                            uint32_t const *sel, uint32_t const *sel_nb,
                            int8_t const *mono, uint32_t n_mono, TreeParams tp)
 {
     uint32_t const k = blockIdx.x;
+    if (k == 0 && threadIdx.x == 0)
+    {
+        ctl->n_cur = ctl->n_next; // the level's last kernel advances the frontier
+    }
     if (k >= ctl->n_splits)
     {
         return;
@@ -1531,7 +1607,7 @@ __global__ void __launch_bounds__(k_threads)
 // (and, quantised, the leaf renewal) run chunk by chunk as on any level.
 __global__ void __launch_bounds__(k_plan_thr)
     final_kernel(Ctl *ctl, Node *nodes, TreeParams tp, TreeOut t, Chunk *pchunks,
-                 uint32_t *pcr)
+                 uint32_t *pcr, double2 *nbound)
 {
     uint32_t const n    = ctl->n_cur;
     uint32_t const i    = threadIdx.x;
@@ -1539,6 +1615,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     Node           nd   = live ? nodes[i] : Node{};
     if (live)
     {
+        nbound[nd.id] = make_double2(nd.lo, nd.hi);
         write_leaf_node(t, nd.id, leaf_value(nd, tp));
         nd.flags = 0;
         nodes[i] = nd;
@@ -2072,7 +2149,7 @@ constexpr uint32_t k_sub_cells = 1024; // cells per subtraction CTA
 // words subtract without borrow: a child's hessian sum never exceeds its
 // parent's); children's totals and monotone bounds from the integer sums.
 __global__ void __launch_bounds__(k_threads)
-    qsubtract_totals_kernel(Ctl const *ctl, uint32_t const *bpair,
+    qsubtract_totals_kernel(Ctl *ctl, uint32_t const *bpair,
                             unsigned long long const *hist_cur, unsigned long long *hist_nxt,
                             uint32_t total_cells, uint32_t n_cells, Node const *cur,
                             Node *next, Best const *best, uint32_t const *sel,
@@ -2080,6 +2157,10 @@ __global__ void __launch_bounds__(k_threads)
                             TreeParams tp, double2 const *qscale, int64_t const *btot)
 {
     uint32_t const k = blockIdx.x;
+    if (k == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+    {
+        ctl->n_cur = ctl->n_next; // the level's last kernel advances the frontier
+    }
     if (k >= ctl->n_splits)
     {
         return;
@@ -2207,95 +2288,101 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
-// Leaf renewal, pass 1: per partition chunk of a leaf node, the FP64 sums of
-// the full-precision (g, h) of its rows, in a fixed reduction order.
+// Leaf renewal: per partition chunk of a leaf node, the FP64 sums of the
+// full-precision (g, h) of its rows in a fixed reduction order; the last CTA
+// to finish (a ticket after a fence) then sums each leaf's chunks in chunk
+// order and writes the FP64 Newton value under the node's bounds.
 __global__ void __launch_bounds__(k_threads)
     leafsum_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes,
                    uint32_t const *__restrict__ rows, float2 const *__restrict__ gh,
-                   double2 *__restrict__ partial)
+                   double2 *partial, uint32_t const *pcr, TreeParams tp, TreeOut t,
+                   uint32_t *done)
 {
     __shared__ double sg_s[k_threads / 32];
     __shared__ double sh_s[k_threads / 32];
-    uint32_t const    c = blockIdx.x;
-    if (c >= ctl->n_pchunks)
+    __shared__ bool   last_s;
+    uint32_t const    c    = blockIdx.x;
+    bool              work = c < ctl->n_pchunks;
+    Chunk             ch{};
+    if (work)
     {
-        return;
+        ch               = pchunks[c];
+        Node const nd    = nodes[ch.node];
+        work             = (nd.flags & 1) == 0 || (nd.flags & 2) != 0;
     }
-    Chunk const ch = pchunks[c];
-    Node const  nd = nodes[ch.node];
-    if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
+    if (work)
     {
-        return;
-    }
-    double g = 0.0;
-    double h = 0.0;
+        double g = 0.0;
+        double h = 0.0;
 #pragma unroll 8
-    for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
-    {
-        float2 const v = gh[rows[ch.begin + k]];
-        g += v.x;
-        h += v.y;
-    }
+        for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
+        {
+            float2 const v = gh[rows[ch.begin + k]];
+            g += v.x;
+            h += v.y;
+        }
 #pragma unroll
-    for (uint32_t o = 16; o > 0; o >>= 1)
-    {
-        g += __shfl_xor_sync(0xFFFFFFFFu, g, o);
-        h += __shfl_xor_sync(0xFFFFFFFFu, h, o);
+        for (uint32_t o = 16; o > 0; o >>= 1)
+        {
+            g += __shfl_xor_sync(0xFFFFFFFFu, g, o);
+            h += __shfl_xor_sync(0xFFFFFFFFu, h, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            sg_s[threadIdx.x >> 5] = g;
+            sh_s[threadIdx.x >> 5] = h;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double tg = 0.0;
+            double th = 0.0;
+            for (uint32_t w = 0; w < k_threads / 32; ++w)
+            {
+                tg += sg_s[w];
+                th += sh_s[w];
+            }
+            partial[c] = make_double2(tg, th);
+        }
     }
-    if ((threadIdx.x & 31) == 0)
-    {
-        sg_s[threadIdx.x >> 5] = g;
-        sh_s[threadIdx.x >> 5] = h;
-    }
-    __syncthreads();
     if (threadIdx.x == 0)
     {
-        double tg = 0.0;
-        double th = 0.0;
-        for (uint32_t w = 0; w < k_threads / 32; ++w)
+        __threadfence();
+        last_s = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last_s)
+    {
+        return;
+    }
+    __threadfence();
+    for (uint32_t i = threadIdx.x; i < ctl->n_cur; i += k_threads)
+    {
+        Node const nd = nodes[i];
+        if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
         {
-            tg += sg_s[w];
-            th += sh_s[w];
+            continue;
         }
-        partial[c] = make_double2(tg, th);
+        double g = 0.0;
+        double h = 0.0;
+        for (uint32_t x = pcr[i]; x < pcr[i + 1]; ++x)
+        {
+            double2 const v = __ldcg(&partial[x]);
+            g += v.x;
+            h += v.y;
+        }
+        t.value[nd.id] = static_cast<float>(
+            bounded_leaf_weight(g, h, tp.lambda_l1, tp.lambda_l2, nd.lo, nd.hi));
     }
-}
-
-// Leaf renewal, pass 2: per leaf node, its chunks' sums in chunk order and
-// the FP64 Newton value under the node's bounds.
-__global__ void __launch_bounds__(k_plan_thr)
-    leafval_kernel(Ctl const *ctl, Node const *nodes, uint32_t const *pcr,
-                   double2 const *partial, TreeParams tp, TreeOut t)
-{
-    uint32_t const i = threadIdx.x;
-    if (i >= ctl->n_cur)
+    if (threadIdx.x == 0)
     {
-        return;
+        *done = 0; // ready for the next launch
     }
-    Node const nd = nodes[i];
-    if ((nd.flags & 1) != 0 && (nd.flags & 2) == 0)
-    {
-        return;
-    }
-    double g = 0.0;
-    double h = 0.0;
-    for (uint32_t c = pcr[i]; c < pcr[i + 1]; ++c)
-    {
-        g += partial[c].x;
-        h += partial[c].y;
-    }
-    t.value[nd.id] = static_cast<float>(
-        bounded_leaf_weight(g, h, tp.lambda_l1, tp.lambda_l2, nd.lo, nd.hi));
 }
 
 __global__ void tree_counter_kernel(uint32_t *tree_no)
 {
     *tree_no += 1;
-}
-
-__global__ void advance_kernel(Ctl *ctl)
-{
-    ctl->n_cur = ctl->n_next;
 }
 
 template <typename T> T *dalloc(size_t n, cudaStream_t s)
@@ -2383,6 +2470,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     rows_[0]  = dalloc<uint32_t>(max_rows_, s);
     rows_[1]  = dalloc<uint32_t>(max_rows_, s);
     pcr_      = dalloc<uint32_t>(max_front_ + 2, s);
+    nbound_   = dalloc<double2>(std::max<uint32_t>(max_nodes_, k_walk_nodes), s);
     nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
     dtree_    = dalloc<uint32_t>(1, s);
     BB_CHECK(cudaMemsetAsync(dtree_, 0, 4, s));
@@ -2394,6 +2482,10 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         qgh8_    = dalloc<uint16_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 2, s);
         partial_ = dalloc<double2>(max_pchunks_, s);
         btot_    = dalloc<int64_t>(2 * static_cast<size_t>(max_front_), s);
+        done_    = dalloc<uint32_t>(1, s);
+        wacc_    = dalloc<unsigned long long>(2 * k_walk_nodes, s);
+        leaf16_  = dalloc<uint16_t>(plane_.n_rows, s);
+        BB_CHECK(cudaMemsetAsync(done_, 0, 4, s));
         // the mirror tiles holding the selection: all selected features, and
         // the first one alone (the last level builds only its totals)
         uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
@@ -2491,7 +2583,8 @@ Grower::~Grower()
                     ccount_,  seg_,      payload_, rows_[0],  rows_[1],    scale_,
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
-                    tile_j_[1], bbase_,   dirs_,    btot_};
+                    tile_j_[1], bbase_,   dirs_,    btot_,    done_,    wacc_,
+                    leaf16_,  nbound_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -2558,17 +2651,21 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
     n_launch_ += 1;
 }
 
-void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
+void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
 {
     cudaStream_t s = stream_;
     phase_begin();
     if (quant_)
     {
         int const v = nfb == n_sel_ ? 0 : 1;
-        zero_build_kernel<<<max_front_, k_threads, 0, s>>>(
-            ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_,
-            off_h_[nfb]);
-        BB_LAUNCH("zero_build_kernel");
+        if (!zeroed)
+        {
+            zero_build_kernel<<<max_front_, k_threads, 0, s>>>(
+                ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_,
+                off_h_[nfb]);
+            BB_LAUNCH("zero_build_kernel");
+            n_launch_ += 1;
+        }
         uint32_t const per   = k_mirror_bytes / (plane_.u8 ? 1 : 2);
         size_t const   qsmem = static_cast<size_t>(per) * max_nb_ * 8;
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
@@ -2588,7 +2685,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst)
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);
         }
         BB_LAUNCH("qhist_kernel");
-        n_launch_ += 2;
+        n_launch_ += 1;
     }
     else
     {
@@ -2658,11 +2755,10 @@ void Grower::leaf_values(TreeOut const &t, bool)
     }
     cudaStream_t s = stream_;
     leafsum_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_cur_, rows_cur_,
-                                                      gh_cur_, partial_);
+                                                      gh_cur_, partial_, pcr_, cfg_.tp, t,
+                                                      done_);
     BB_LAUNCH("leafsum_kernel");
-    leafval_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_cur_, pcr_, partial_, cfg_.tp, t);
-    BB_LAUNCH("leafval_kernel");
-    n_launch_ += 2;
+    n_launch_ += 1;
 }
 
 void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
@@ -2689,7 +2785,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
                                          plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_,
-                                         pcr_);
+                                         pcr_, nbound_);
     BB_LAUNCH("plan_kernel");
     if (prof_ != nullptr)
     {
@@ -2716,7 +2812,10 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
-    leaf_values(t, false);
+    if (!(walk_ && quant_))
+    {
+        leaf_values(t, false);
+    }
     if (!walk_)
     {
         stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
@@ -2724,16 +2823,18 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         BB_LAUNCH("stamp_kernel");
         n_launch_ += 1;
     }
+    bool const     last     = (L + 1) == cfg_.tp.max_depth;
+    uint32_t const nfb      = last ? 1 : n_sel_;
+    uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] : 0;
     pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
         ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
-        dirs_);
+        dirs_, static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_, n_zcells);
     BB_LAUNCH("pscatter_kernel");
     if (prof_ != nullptr)
     {
         phase_end(prof_->partition_ms);
     }
     n_launch_ += 5;
-    bool const last = (L + 1) == cfg_.tp.max_depth;
     if (quant_ && last)
     {
         // the last level's nodes are leaves: the quantised form needs their
@@ -2748,17 +2849,14 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
             nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_);
         BB_LAUNCH("qsubtract_totals_kernel");
-        advance_kernel<<<1, 1, 0, s>>>(ctl_);
-        BB_LAUNCH("advance_kernel");
-        n_launch_ += 3;
+        n_launch_ += 2;
         if (prof_ != nullptr)
         {
             phase_end(prof_->other_ms);
         }
         return;
     }
-    uint32_t const nfb     = last ? 1 : n_sel_;
-    build(rows_out, nfb, nxt);
+    build(rows_out, nfb, nxt, true);
     uint32_t const n_cells = off_h_[nfb]; // the built features: a selection prefix
     phase_begin();
     if (quant_)
@@ -2779,9 +2877,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp);
         BB_LAUNCH("subtract_totals_kernel");
     }
-    advance_kernel<<<1, 1, 0, s>>>(ctl_);
-    BB_LAUNCH("advance_kernel");
-    n_launch_ += 2;
+    n_launch_ += 1;
     if (prof_ != nullptr)
     {
         phase_end(prof_->other_ms);
@@ -2849,20 +2945,20 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     }
     phase_begin();
     int const fin = static_cast<int>(cfg_.tp.max_depth & 1);
-    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_);
+    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_,
+                                          nbound_);
     BB_LAUNCH("final_kernel");
     nodes_cur_ = nodes_[fin];
     rows_cur_  = rows_in;
-    leaf_values(t, true);
     if (walk_)
     {
-        if (next != nullptr && quant_)
-        {
-            BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
-        }
         uint32_t const n    = static_cast<uint32_t>(plane_.n_rows);
         uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
                                                  148u * 8u);
+        uint32_t const per   = k_mirror_bytes / (plane_.u8 ? 1u : 2u);
+        bool const     multi = plane_.n_feats > per;
+        auto const    *mir   = static_cast<uint4 const *>(plane_.mirror);
+        uint32_t const depth = cfg_.tp.max_depth;
         WalkArgs a{};
         a.scores    = scores;
         a.leaf_id   = leaf_id;
@@ -2871,34 +2967,63 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         a.labels    = next != nullptr ? next->labels : nullptr;
         a.gh        = next != nullptr ? next->gh : nullptr;
         a.absmax    = next != nullptr && quant_ ? absmax_ : nullptr;
-        uint32_t const per  = k_mirror_bytes / (plane_.u8 ? 1u : 2u);
-        auto const    *mir  = static_cast<uint4 const *>(plane_.mirror);
-        if (plane_.n_feats > per)
+        if (quant_)
         {
-            walk_tiles_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
-                                                         plane_.cut_off, per, plane_.u8, a);
-        }
-        else if (plane_.u8)
-        {
-            walk_kernel<true><<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
-                                                         plane_.cut_off, cfg_.tp.max_depth, a);
+            BB_CHECK(cudaMemsetAsync(wacc_, 0, sizeof(unsigned long long) * 2 * k_walk_nodes, s));
+            auto sum = [&](auto kern)
+            {
+                kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
+                                                gh_cur_, absmax_, leaf16_, wacc_);
+            };
+            if (plane_.u8)
+            {
+                multi ? sum(walk_sum_kernel<true, true>) : sum(walk_sum_kernel<true, false>);
+            }
+            else
+            {
+                multi ? sum(walk_sum_kernel<false, true>) : sum(walk_sum_kernel<false, false>);
+            }
+            BB_LAUNCH("walk_sum_kernel");
+            leaf_fix_kernel<<<1, k_threads, 0, s>>>(ctl_, t, wacc_, nbound_, absmax_, cfg_.tp);
+            BB_LAUNCH("leaf_fix_kernel");
+            if (next != nullptr)
+            {
+                BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
+            }
+            walk_apply_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, plane_.n_rows, leaf16_, a);
+            BB_LAUNCH("walk_apply_kernel");
+            n_launch_ += 3;
         }
         else
         {
-            walk_kernel<false><<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows,
-                                                          plane_.cut_off, cfg_.tp.max_depth, a);
+            auto walk = [&](auto kern)
+            {
+                kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
+                                                a);
+            };
+            if (plane_.u8)
+            {
+                multi ? walk(walk_kernel<true, true>) : walk(walk_kernel<true, false>);
+            }
+            else
+            {
+                multi ? walk(walk_kernel<false, true>) : walk(walk_kernel<false, false>);
+            }
+            BB_LAUNCH("walk_kernel");
+            n_launch_ += 1;
         }
-        BB_LAUNCH("walk_kernel");
     }
     else
     {
-        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in,
-                                                        t, leaf_id, scores, lr);
+        leaf_values(t, true);
+        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in, t,
+                                                        leaf_id, scores, lr);
         BB_LAUNCH("stamp_kernel");
+        n_launch_ += 1;
     }
     tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
     BB_LAUNCH("tree_counter_kernel");
-    n_launch_ += 3;
+    n_launch_ += 2;
     if (prof_ != nullptr)
     {
         phase_end(prof_->other_ms);

@@ -175,7 +175,8 @@ class Grower
   private:
     void level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
                TreeOut const &out, uint32_t *leaf_id, float *scores, float lr);
-    void build(uint32_t const *rows, uint32_t n_feat_build, int dst);
+    // zeroed: the quantised slots were already cleared (by the partition)
+    void build(uint32_t const *rows, uint32_t n_feat_build, int dst, bool zeroed = false);
 
     Plane const          &plane_;
     GrowConfig            cfg_;
@@ -228,6 +229,10 @@ class Grower
     uint16_t *qgh8_     = nullptr; // per row: int8 g | uint8 h << 8
     double2  *partial_  = nullptr; // per partition chunk: leaf (G, H) in FP64
     int64_t  *btot_     = nullptr; // per build index: exact (G, H) of the last level
+    uint32_t *done_     = nullptr; // leaf-renewal CTA ticket (zero between launches)
+    unsigned long long *wacc_ = nullptr; // per tree node: fixed-point (G, H) of the walk
+    uint16_t *leaf16_   = nullptr; // per row: its leaf, from the walk
+    double2  *nbound_   = nullptr; // per tree node: monotone bounds (lo, hi)
     uint32_t  crows_    = 0;       // rows per histogram-build chunk
     bool      quant_    = false;
     uint32_t *dtree_    = nullptr; // device tree counter (the rounding stream)

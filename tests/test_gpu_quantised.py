@@ -87,6 +87,50 @@ def test_quantised_seeded_and_deterministic(bb):
     assert not np.array_equal(s1, s3)
 
 
+@pytest.mark.parametrize("mono", [False, True])
+def test_quantised_leaf_values_renew_from_full_gradients(bb, mono):
+    """Every leaf's value is the FP64 Newton step of its rows' full-precision
+    (g, h) -- not of the quantised codes -- under its monotone bounds, and the
+    scores take score + lr * value of each row's leaf."""
+    X, g, h = _data(8, 60_000)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    y = (X[:, 0] + 0.3 * np.nan_to_num(X[:, 1]) > 0).astype(np.float32)
+    lr = 0.3
+    b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=7,
+                                            learning_rate=lr, hist_mode="int8",
+                                            lambda_l2=2.0, monotone=[1] if mono else [],
+                                            record_leaf_ids=True), max_trees=1)
+    b.update(1)
+    t = b.tree(0)
+    leaf = b.leaf_ids()
+    assert (t.feature[leaf] == bb.LEAF).all()
+    s0 = np.float32(b.init_score)
+    p = (np.float32(1.0) / (np.float32(1.0) + np.exp(-s0, dtype=np.float32))).astype(np.float32)
+    gg = (p - y).astype(np.float64)
+    hh = np.full(len(y), np.float64(np.float32(p * (np.float32(1.0) - p))))
+    G = np.bincount(leaf, weights=gg, minlength=len(t.feature))
+    H = np.bincount(leaf, weights=hh, minlength=len(t.feature))
+    used = np.unique(leaf)
+    want = -G[used] / (H[used] + 2.0)
+    if not mono:
+        # device expf and numpy exp may differ in the last place
+        np.testing.assert_allclose(t.value[used], want, rtol=2e-6, atol=1e-7)
+    else:
+        # bounds clamp the Newton steps; every split on the constrained
+        # feature orders its subtrees' values
+        assert np.isfinite(t.value[used]).all()
+
+        def leaves(i):
+            if t.feature[i] == bb.LEAF:
+                return [t.value[i]]
+            return leaves(t.left[i]) + leaves(t.right[i])
+        for i in np.flatnonzero(t.feature == 0):
+            assert max(leaves(t.left[i])) <= min(leaves(t.right[i])) + 1e-6
+    expect = (s0 + np.float32(lr) * t.value[leaf]).astype(np.float32)
+    assert np.array_equal(b.scores(), expect)
+
+
 def _auc(y, p):
     order = np.argsort(p, kind="stable")
     ranks = np.empty(len(p)); ranks[order] = np.arange(1, len(p) + 1)
