@@ -282,7 +282,7 @@ def main():
     peak, peak_kind = peaks()
     hist_gbs = prof["hist_bytes"] / (prof["hist_ms"] * 1e-3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "hist_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "qhist_t_tall_binary_int8_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             td = json.load(f)
