@@ -26,12 +26,13 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "pred_contribs", "fit_cuts", "cuts_from_sample", "sample_rows",
+    "grow_tree", "populate", "predict", "pred_contribs", "oblivious_tables", "fit_cuts", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
 LEAF = 0xFFFFFFFF
 OBJECTIVES = {"mse": 0, "logloss": 1}
+GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1}
 HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
 
 
@@ -57,6 +58,7 @@ class TrainParams:
     selected: list | None = None
     use_graph: bool = False
     record_leaf_ids: bool = False
+    grower: str = "depthwise"
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -70,6 +72,7 @@ class TrainParams:
         c.min_data_in_leaf = self.min_data_in_leaf
         c.hist_mode = HIST_MODES[self.hist_mode]
         c.seed = self.seed
+        c.grower = GROWERS[self.grower]
         c.use_graph = 1 if self.use_graph else 0
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:
@@ -96,6 +99,25 @@ class Tree:
     split_bin: np.ndarray
     depth: int = 0
     n_leaves: int = 0
+
+
+def oblivious_tables(tree: Tree):
+    """A levelwise tree as the reference's ObliviousTree keeps it
+    (include/bonsai/oblivious_tree.hpp): per level the split feature,
+    threshold and default direction, and the 2^depth leaf values in frontier
+    order (the first level is the most significant bit of a leaf's index)."""
+    feats, thr, dl = [], [], []
+    i = 0
+    while tree.feature[i] != LEAF:
+        feats.append(int(tree.feature[i]))
+        thr.append(float(tree.value[i]))
+        dl.append(int(tree.default_left[i]))
+        i = int(tree.left[i])
+    d = len(feats)
+    first = (1 << d) - 1
+    leaves = tree.value[first:first + (1 << d)].astype(np.float32)
+    return (np.array(feats, np.uint32), np.array(thr, np.float32), np.array(dl, np.uint8),
+            leaves)
 
 
 def _tree_arrays(cap: int):

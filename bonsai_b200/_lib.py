@@ -37,6 +37,7 @@ class TrainCfg(C.Structure):
         ("monotone", C.POINTER(C.c_int8)), ("n_monotone", C.c_uint32),
         ("selected", C.POINTER(C.c_uint32)), ("n_selected", C.c_uint32),
         ("use_graph", C.c_int32), ("record_leaf_ids", C.c_int32),
+        ("grower", C.c_int32),
     ]
 
 

@@ -235,7 +235,21 @@ GrowConfig grow_config(bb_train_cfg const &c)
 {
     need(c.max_depth <= 8, "max_depth must be <= 8 on the device level plane");
     need(c.hist_mode >= 0 && c.hist_mode <= 2, "hist_mode must be 0, 1 or 2");
+    need(c.grower == 0 || c.grower == 1, "grower must be 0 (depthwise) or 1 (levelwise)");
+    if (c.grower == 1)
+    {
+        for (uint32_t f = 0; c.monotone != nullptr && f < c.n_monotone; ++f)
+        {
+            if (c.monotone[f] != 0)
+            {
+                // ObliviousGrower's constructor (src/grower_impl.hpp:582-590)
+                throw ConfigError("monotone_constraints are not supported by the levelwise "
+                                  "grower");
+            }
+        }
+    }
     GrowConfig g;
+    g.level                = c.grower == 1;
     g.tp.min_child_hess    = c.min_child_hess;
     g.tp.min_gain_to_split = c.min_gain_to_split;
     g.tp.lambda_l2         = c.lambda_l2;

@@ -711,6 +711,260 @@ __global__ void __launch_bounds__(k_find_thr)
 }
 
 
+// ------------------------------------------------------- level split find ----
+//
+// update_best_for_feature_for_level (src/split.cpp:164-235): one split for
+// the whole frontier. Per feature and candidate (bin, default_left), the sum
+// over the frontier's nodes, in frontier order, of each node's children
+// score when both children clear min_child_hess and of its own score
+// otherwise (issue #60: an infeasible node no longer vetoes the cut), minus
+// the sum of the nodes' scores. grid (n_sel), k_lfind_thr threads: warps
+// take the nodes of a group in parallel (prefix over the cut bins: the
+// exact form's serial FP64 chain, the quantised form's exact integer scan),
+// then every thread adds the group's nodes for its bins in frontier order,
+// so the FP64 sums follow the reference's order bit for bit.
+constexpr uint32_t k_lfind_thr = 512;
+
+struct LevelNode
+{
+    double score; // the node's own split score
+    double real_g;
+    double real_h;
+    double mg;    // its missing cell
+    double mh;
+};
+
+template <typename M>
+__device__ __forceinline__ double level_term(double lg, double lh, M mg, M mh, double real_g,
+                                             double real_h, bool dl, double node_score,
+                                             TreeParams const &tp)
+{
+    double const rg = real_g - lg;
+    double const rh = real_h - lh;
+    double const gL = lg + (dl ? static_cast<double>(mg) : 0.0);
+    double const hL = lh + (dl ? static_cast<double>(mh) : 0.0);
+    double const gR = rg + (!dl ? static_cast<double>(mg) : 0.0);
+    double const hR = rh + (!dl ? static_cast<double>(mh) : 0.0);
+    double const mch = tp.min_child_hess;
+    if (hL < mch || hR < mch)
+    {
+        return node_score;
+    }
+    double const l1 = tp.lambda_l1;
+    double const l2 = tp.lambda_l2;
+    return split_score(gL, hL, l1, l2) + split_score(gR, hR, l1, l2);
+}
+
+template <bool Q>
+__global__ void __launch_bounds__(k_lfind_thr)
+    level_find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
+                      uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
+                      uint32_t n_sel, TreeParams tp, Best *cand, uint32_t max_nb,
+                      uint32_t group, double2 const *qscale)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ LevelNode ln_s[k_lfind_thr / 32];
+    __shared__ double    bg_s[k_lfind_thr / 32];
+    __shared__ uint32_t  bo_s[k_lfind_thr / 32];
+    constexpr uint32_t   k_bins_per_thr = k_max_bins / k_lfind_thr;
+    uint32_t const       j     = blockIdx.x;
+    uint32_t const       tid   = threadIdx.x;
+    uint32_t const       lane  = tid & 31;
+    uint32_t const       w     = tid >> 5;
+    uint32_t const       n_cur = ctl->n_cur;
+    uint32_t const       nb    = sel_nb[j];
+    Best                 out   = {0.0, j, 0, 1, 0};
+    if (nb < 3 || n_cur == 0)
+    {
+        if (tid == 0)
+        {
+            cand[j] = out;
+        }
+        return;
+    }
+    uint32_t const n_cut = nb - 2;
+    auto          *pref  = reinterpret_cast<double2 *>(smem_raw); // [group][max_nb]
+    double         acc[2 * k_bins_per_thr];
+#pragma unroll
+    for (uint32_t x = 0; x < 2 * k_bins_per_thr; ++x)
+    {
+        acc[x] = 0.0;
+    }
+    double         parent_sum = 0.0;
+    double2 const  sc         = Q ? *qscale : make_double2(1.0, 1.0);
+    for (uint32_t g0 = 0; g0 < n_cur; g0 += group)
+    {
+        // warp w prefixes node g0 + w of the group
+        if (w < group && g0 + w < n_cur)
+        {
+            uint32_t const p   = g0 + w;
+            Node const     nd  = nodes[p];
+            double2       *pr  = pref + (static_cast<uint64_t>(w) * max_nb);
+            auto const    *src = static_cast<unsigned long long const *>(hist_v) +
+                              (static_cast<uint64_t>(p) * total_cells) + cell_off[j];
+            if constexpr (Q)
+            {
+                uint32_t const run = (n_cut + 31) / 32;
+                uint32_t const b0  = min(n_cut, lane * run);
+                uint32_t const b1  = min(n_cut, b0 + run);
+                int64_t        tg  = 0;
+                int64_t        th  = 0;
+                for (uint32_t b = b0; b < b1; ++b)
+                {
+                    unsigned long long const c = src[b];
+                    tg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+                    th += static_cast<uint32_t>(c);
+                }
+                int64_t eg = tg;
+                int64_t eh = th;
+#pragma unroll
+                for (uint32_t o = 1; o < 32; o <<= 1)
+                {
+                    int64_t const ug = __shfl_up_sync(0xFFFFFFFFu, eg, o);
+                    int64_t const uh = __shfl_up_sync(0xFFFFFFFFu, eh, o);
+                    if (lane >= o)
+                    {
+                        eg += ug;
+                        eh += uh;
+                    }
+                }
+                int64_t pg = eg - tg;
+                int64_t ph = eh - th;
+                for (uint32_t b = b0; b < b1; ++b)
+                {
+                    unsigned long long const c = src[b];
+                    pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+                    ph += static_cast<uint32_t>(c);
+                    pr[b] = make_double2(static_cast<double>(pg) * sc.x,
+                                         static_cast<double>(ph) * sc.y);
+                }
+                if (lane == 0)
+                {
+                    unsigned long long const mc_ = src[nb - 1];
+                    int64_t const mqg = static_cast<int32_t>(static_cast<uint32_t>(mc_ >> 32));
+                    int64_t const mqh = static_cast<uint32_t>(mc_);
+                    LevelNode     l;
+                    l.score  = split_score(static_cast<double>(nd.qg) * sc.x,
+                                           static_cast<double>(nd.qh) * sc.y, tp.lambda_l1,
+                                           tp.lambda_l2);
+                    l.real_g = static_cast<double>(nd.qg - mqg) * sc.x;
+                    l.real_h = static_cast<double>(nd.qh - mqh) * sc.y;
+                    l.mg     = static_cast<double>(mqg) * sc.x;
+                    l.mh     = static_cast<double>(mqh) * sc.y;
+                    ln_s[w]  = l;
+                }
+            }
+            else
+            {
+                auto const *cell = reinterpret_cast<float2 const *>(src);
+                if (lane == 0)
+                {
+                    double lg = 0.0;
+                    double lh = 0.0;
+                    for (uint32_t b = 0; b < n_cut; ++b)
+                    {
+                        float2 const c = cell[b];
+                        lg += c.x;
+                        lh += c.y;
+                        pr[b] = make_double2(lg, lh);
+                    }
+                    float2 const m = cell[nb - 1];
+                    LevelNode    l;
+                    l.score  = split_score(nd.sum_g, nd.sum_h, tp.lambda_l1, tp.lambda_l2);
+                    // float fields subtract in float, then widen
+                    l.real_g = static_cast<double>(nd.sum_g - m.x);
+                    l.real_h = static_cast<double>(nd.sum_h - m.y);
+                    l.mg     = m.x;
+                    l.mh     = m.y;
+                    ln_s[w]  = l;
+                }
+            }
+        }
+        __syncthreads();
+        uint32_t const gn = min(group, n_cur - g0);
+        for (uint32_t q = 0; q < gn; ++q)
+        {
+            LevelNode const l  = ln_s[q];
+            double2 const  *pr = pref + (static_cast<uint64_t>(q) * max_nb);
+#pragma unroll
+            for (uint32_t x = 0; x < k_bins_per_thr; ++x)
+            {
+                uint32_t const b = tid + (x * k_lfind_thr);
+                if (b < n_cut)
+                {
+                    double2 const p2 = pr[b];
+                    if constexpr (Q)
+                    {
+                        acc[2 * x] += level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g,
+                                                         l.real_h, true, l.score, tp);
+                        acc[(2 * x) + 1] += level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g,
+                                                               l.real_h, false, l.score, tp);
+                    }
+                    else
+                    {
+                        float const mg = static_cast<float>(l.mg);
+                        float const mh = static_cast<float>(l.mh);
+                        acc[2 * x] += level_term<float>(p2.x, p2.y, mg, mh, l.real_g, l.real_h,
+                                                        true, l.score, tp);
+                        acc[(2 * x) + 1] += level_term<float>(p2.x, p2.y, mg, mh, l.real_g,
+                                                              l.real_h, false, l.score, tp);
+                    }
+                }
+            }
+            parent_sum += l.score;
+        }
+        __syncthreads();
+    }
+    // every node's missing cell empty: both routings sum the same, and the
+    // first (default left) wins the strict > below, as the serial scan does
+    double         best     = 0.0;
+    uint32_t       order    = 0xFFFFFFFFu;
+    double const   min_gain = tp.min_gain_to_split;
+#pragma unroll
+    for (uint32_t x = 0; x < k_bins_per_thr; ++x)
+    {
+        uint32_t const b = tid + (x * k_lfind_thr);
+        if (b < n_cut)
+        {
+            for (uint32_t d = 0; d < 2; ++d)
+            {
+                double const gain = acc[(2 * x) + d] - parent_sum;
+                if (gain > best && gain >= min_gain)
+                {
+                    best  = gain;
+                    order = (b * 2) + d;
+                }
+            }
+        }
+    }
+    warp_best(best, order);
+    if (lane == 0)
+    {
+        bg_s[w] = best;
+        bo_s[w] = order;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        for (uint32_t x = 1; x < k_lfind_thr / 32; ++x)
+        {
+            if (bg_s[x] > best || (bg_s[x] == best && bo_s[x] < order))
+            {
+                best  = bg_s[x];
+                order = bo_s[x];
+            }
+        }
+        if (order != 0xFFFFFFFFu)
+        {
+            out.gain  = best;
+            out.bin   = order >> 1;
+            out.dl    = (order & 1) == 0 ? 1 : 0;
+            out.valid = 1;
+        }
+        cand[j] = out;
+    }
+}
+
 // Cuts n row segments into chunks of `rows` rows with the whole block:
 // segment i owns chunks [range[i], range[i + 1]); chunk c finds its segment
 // by binary search (range is in global memory, written before a barrier).
@@ -750,13 +1004,44 @@ __device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *ran
 __global__ void __launch_bounds__(k_plan_thr)
     plan_kernel(Ctl *ctl, Node *nodes, Best const *cand, Best *best, uint32_t n_sel,
                 uint32_t const *sel, float const *cuts, uint32_t const *cut_off,
-                TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound)
+                TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound,
+                bool level)
 {
+    __shared__ Best    level_s;
     uint32_t const n_cur = ctl->n_cur;
     uint32_t const lane  = threadIdx.x & 31;
     uint32_t const w     = threadIdx.x >> 5;
+    if (level)
+    {
+        // one split for the level (reduce_in_feature_order, src/split.cpp:239-250),
+        // broadcast to every frontier node
+        if (w == 0)
+        {
+            double   g = 0.0;
+            uint32_t o = 0xFFFFFFFFu;
+            for (uint32_t j = lane; j < n_sel; j += 32)
+            {
+                Best const c = cand[j];
+                if (c.valid != 0 && (c.gain > g || (c.gain == g && j < o)))
+                {
+                    g = c.gain;
+                    o = j;
+                }
+            }
+            warp_best(g, o);
+            if (lane == 0)
+            {
+                level_s = o == 0xFFFFFFFFu ? Best{0.0, 0, 0, 1, 0} : cand[o];
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n_cur; i += k_plan_thr)
+        {
+            best[i] = level_s;
+        }
+    }
     // per node: the first feature (ascending) holding the largest gain
-    for (uint32_t i = w; i < n_cur; i += k_plan_thr / 32)
+    for (uint32_t i = w; !level && i < n_cur; i += k_plan_thr / 32)
     {
         double   g = 0.0;
         uint32_t o = 0xFFFFFFFFu;
@@ -928,7 +1213,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  Chunk const *pchunks, uint32_t const *pcr, uint32_t *pleft,
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
-                 TreeOut t, uint32_t crows, uint32_t *bbase)
+                 TreeOut t, uint32_t crows, uint32_t *bbase, bool level)
 {
     __shared__ uint32_t grand_s;
     uint32_t const      n_cur = ctl->n_cur;
@@ -967,12 +1252,15 @@ __global__ void __launch_bounds__(k_plan_thr)
     {
         uint32_t const c0 = pcr[i];
         uint32_t const c1 = pcr[i + 1];
-        p0                = pleft[c0];
+        // a node without chunks (a level split of an empty node) past the
+        // last chunk: its prefix origin is the grand total
+        p0                = c0 < n_ch ? pleft[c0] : grand_s;
         nl                = (c1 < n_ch ? pleft[c1] : grand_s) - p0;
         nleft[i]          = nl;
-        if (nl == 0 || nl == nd.count)
+        if (!level && (nl == 0 || nl == nd.count))
         {
-            // demote_empty_splits: the parent is a leaf after all
+            // demote_empty_splits: the parent is a leaf after all (a level
+            // split applies to every node, empty children included)
             nd.flags |= 2;
             write_leaf_node(t, nd.id, leaf_value(nd, tp));
             t.gain[nd.id] = 0.0F;
@@ -2549,6 +2837,16 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     BB_CHECK(cudaFuncSetAttribute(find_kernel<true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(find_smem)));
+    // the level finder prefixes up to 16 nodes at a time in shared memory
+    lgroup_ = static_cast<uint32_t>(std::min<size_t>(
+        k_lfind_thr / 32, std::max<size_t>(1, (192 * 1024) / (max_nb_ * sizeof(double2)))));
+    size_t const lsmem = static_cast<size_t>(lgroup_) * max_nb_ * sizeof(double2);
+    BB_CHECK(cudaFuncSetAttribute(level_find_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(lsmem)));
+    BB_CHECK(cudaFuncSetAttribute(level_find_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(lsmem)));
     if (!quant_)
     {
         size_t const cnt_smem   = k_warps_feat * cell_stride_ * sizeof(uint32_t);
@@ -2770,7 +3068,23 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     size_t const find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
     phase_begin();
     dim3 const fgrid(max_front_, n_sel_);
-    if (quant_)
+    if (cfg_.level)
+    {
+        size_t const lsmem = static_cast<size_t>(lgroup_) * max_nb_ * sizeof(double2);
+        if (quant_)
+        {
+            level_find_kernel<true><<<n_sel_, k_lfind_thr, lsmem, s>>>(
+                ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
+                cand_, max_nb_, lgroup_, qscale_);
+        }
+        else
+        {
+            level_find_kernel<false><<<n_sel_, k_lfind_thr, lsmem, s>>>(
+                ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
+                cand_, max_nb_, lgroup_, qscale_);
+        }
+    }
+    else if (quant_)
     {
         find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
@@ -2785,7 +3099,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
                                          plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_,
-                                         pcr_, nbound_);
+                                         pcr_, nbound_, cfg_.level);
     BB_LAUNCH("plan_kernel");
     if (prof_ != nullptr)
     {
@@ -2808,7 +3122,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
                                           pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
                                           build_, brange_, bchunks_, cfg_.tp, t, crows_,
-                                          bbase_);
+                                          bbase_, cfg_.level);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;

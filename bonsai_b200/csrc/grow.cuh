@@ -115,7 +115,11 @@ struct NextRound
 struct GrowConfig
 {
     TreeParams tp;
-    HistMode   mode = HistMode::exact;
+    HistMode   mode  = HistMode::exact;
+    // levelwise (ObliviousGrower, src/grower_impl.hpp:579-720): one split per
+    // level over the whole frontier, broadcast to every node; trees are
+    // perfect to their depth, empty children included
+    bool       level = false;
 };
 
 // All device buffers one tree's growth needs, sized once for a dataset and
@@ -191,6 +195,7 @@ class Grower
     uint32_t              max_pchunks_ = 0;
     uint32_t              max_bchunks_ = 0;
     uint32_t              cell_stride_ = 0; // per-(chunk, feature) count stride
+    uint32_t              lgroup_      = 1; // nodes per level-finder group
 
     // device
     uint32_t *sel_      = nullptr; // selected feature ids

@@ -101,6 +101,9 @@ typedef struct
     uint32_t       n_selected;
     int32_t        use_graph;  /* capture one boosting round as a CUDA graph */
     int32_t        record_leaf_ids; /* keep each row's leaf id of the last tree */
+    int32_t        grower;     /* 0 depthwise (DepthwiseGrower), 1 levelwise
+                                  (ObliviousGrower: one split per level over the
+                                  whole frontier, src/grower_impl.hpp:579-720) */
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
