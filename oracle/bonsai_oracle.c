@@ -286,6 +286,106 @@ static orc_split find_node(gctx const *c, onode const *nd)
     return s;
 }
 
+/* The levelwise grower's split finder: update_best_for_feature_for_level
+ * (src/split.cpp:164-235) per selected feature, then reduce_in_feature_order
+ * (:239-250). Per candidate (bin, default_left) the frontier's nodes are
+ * summed in frontier order: a node's children score when both children clear
+ * min_child_hess, else its own score (issue #60); the gain is that sum minus
+ * the sum of the nodes' scores. No min_data_in_leaf gate, no monotone
+ * bounds (the levelwise grower rejects them). */
+static orc_split find_level(gctx const *c, onode const *cur, size_t n_cur)
+{
+    orc_tree_cfg const *cfg  = c->cfg;
+    double const        l1   = cfg->lambda_l1;
+    double const        l2   = cfg->lambda_l2;
+    orc_split           best = {0.0, 0, 0, 1, 0};
+    if (n_cur == 0)
+    {
+        return best;
+    }
+    double *pscore = (double *)malloc(sizeof(double) * n_cur);
+    double *rg     = (double *)malloc(sizeof(double) * n_cur);
+    double *rh     = (double *)malloc(sizeof(double) * n_cur);
+    float  *mg     = (float *)malloc(sizeof(float) * n_cur);
+    float  *mh     = (float *)malloc(sizeof(float) * n_cur);
+    for (size_t j = 0; j < c->n_sel; ++j)
+    {
+        uint32_t const f     = c->selected[j];
+        uint32_t const nb    = c->n_bins[f];
+        uint32_t const n_cut = nb >= 2 ? nb - 2 : 0;
+        if (n_cut == 0)
+        {
+            continue;
+        }
+        double *pref       = (double *)malloc(sizeof(double) * 2 * n_cur * n_cut);
+        double  sum_parent = 0.0;
+        int     all_empty  = 1;
+        for (size_t p = 0; p < n_cur; ++p)
+        {
+            float const *cells = cur[p].hist + (2 * c->off[j]);
+            mg[p]              = cells[2 * (nb - 1)];
+            mh[p]              = cells[(2 * (nb - 1)) + 1];
+            /* Histogram::fill_prefix (include/bonsai/histogram.hpp:139-160) */
+            double lg = 0.0, lh = 0.0;
+            for (uint32_t b = 0; b < n_cut; ++b)
+            {
+                lg += cells[2 * b];
+                lh += cells[(2 * b) + 1];
+                pref[2 * ((p * n_cut) + b)]       = lg;
+                pref[(2 * ((p * n_cut) + b)) + 1] = lh;
+            }
+            pscore[p] = score(cur[p].sum_g, cur[p].sum_h, l1, l2);
+            sum_parent += pscore[p];
+            rg[p]     = (double)(float)(cur[p].sum_g - mg[p]);
+            rh[p]     = (double)(float)(cur[p].sum_h - mh[p]);
+            all_empty = all_empty && mg[p] == 0.0F && mh[p] == 0.0F;
+        }
+        int const n_dirs = all_empty ? 1 : 2;
+        orc_split cand   = {0.0, 0, 0, 1, 0};
+        for (uint32_t b = 0; b < n_cut; ++b)
+        {
+            for (int d = 0; d < n_dirs; ++d)
+            {
+                int const dl       = d == 0;
+                double    children = 0.0;
+                for (size_t p = 0; p < n_cur; ++p)
+                {
+                    double const lg = pref[2 * ((p * n_cut) + b)];
+                    double const lh = pref[(2 * ((p * n_cut) + b)) + 1];
+                    double const gL = lg + (dl ? (double)mg[p] : 0.0);
+                    double const hL = lh + (dl ? (double)mh[p] : 0.0);
+                    double const gR = (rg[p] - lg) + (!dl ? (double)mg[p] : 0.0);
+                    double const hR = (rh[p] - lh) + (!dl ? (double)mh[p] : 0.0);
+                    int const    ok = !(hL < (double)cfg->min_child_hess ||
+                                     hR < (double)cfg->min_child_hess);
+                    children += ok ? score(gL, hL, l1, l2) + score(gR, hR, l1, l2)
+                                   : pscore[p];
+                }
+                double const gain = children - sum_parent;
+                if (gain > cand.gain && gain >= (double)cfg->min_gain_to_split)
+                {
+                    cand.gain         = gain;
+                    cand.feature      = f;
+                    cand.bin          = b;
+                    cand.default_left = (uint8_t)dl;
+                    cand.valid        = 1;
+                }
+            }
+        }
+        free(pref);
+        if (cand.valid && cand.gain > best.gain)
+        {
+            best = cand;
+        }
+    }
+    free(pscore);
+    free(rg);
+    free(rh);
+    free(mg);
+    free(mh);
+    return best;
+}
+
 /* write_leaf + stamping (src/step/primitives.hpp:42-69). */
 static void finalize_leaf(gctx *c, onode const *nd, uint32_t const *order,
                           float *values, uint32_t *leaf_ids)
@@ -354,10 +454,23 @@ int orc_grow_depthwise(uint16_t const *bins, size_t n, size_t F, uint32_t const 
     while (depth < cfg->max_depth)
     {
         /* open_level: one split per frontier node (src/step/level.hpp:55-80) */
-        orc_split *sp = (orc_split *)malloc(sizeof(orc_split) * n_cur);
-        for (size_t i = 0; i < n_cur; ++i)
+        orc_split *sp = (orc_split *)malloc(sizeof(orc_split) * (n_cur + 1));
+        if (cfg->grower == 1)
         {
-            sp[i] = find_node(&c, &cur[i]);
+            /* ObliviousGrower::grow (src/grower_impl.hpp:599-720): one split
+             * broadcast to every frontier node, or none and the tree ends */
+            orc_split const lv = find_level(&c, cur, n_cur);
+            for (size_t i = 0; i < n_cur; ++i)
+            {
+                sp[i] = lv;
+            }
+        }
+        else
+        {
+            for (size_t i = 0; i < n_cur; ++i)
+            {
+                sp[i] = find_node(&c, &cur[i]);
+            }
         }
         /* plan_level (src/grower_impl.hpp:212-255) + host_partition
          * (src/step/primitives.hpp:262-374) + demote_empty_splits (:262-298)
@@ -436,7 +549,7 @@ int orc_grow_depthwise(uint16_t const *bins, size_t n, size_t F, uint32_t const 
             }
             uint32_t const lid = t->left[nd->id];
             uint32_t const rid = t->right[nd->id];
-            if (nl == 0 || nr == 0)
+            if (cfg->grower != 1 && (nl == 0 || nr == 0))
             {
                 /* demote_empty_splits: the survivor's rows return to the
                  * parent, which becomes a leaf with its own sums */

@@ -33,6 +33,7 @@ typedef struct
     uint32_t       max_leaves; /* leafwise only */
     int32_t const *monotone;   /* per-feature +1/-1/0; may be NULL */
     uint32_t       n_monotone;
+    int32_t        grower;     /* 0 depthwise, 1 levelwise (oblivious) */
 } orc_tree_cfg;
 
 /* One grown tree in the reference's DenseTree layout (tree.hpp:38-45):

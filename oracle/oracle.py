@@ -306,7 +306,7 @@ class OrcTreeCfg(C.Structure):
         ("lambda_l2", C.c_float), ("lambda_l1", C.c_float),
         ("max_depth", C.c_uint32), ("min_data_in_leaf", C.c_uint32),
         ("max_leaves", C.c_uint32), ("monotone", C.POINTER(C.c_int32)),
-        ("n_monotone", C.c_uint32),
+        ("n_monotone", C.c_uint32), ("grower", C.c_int32),
     ]
 
 
@@ -358,6 +358,7 @@ class Oracle:
         c.max_depth = tc.max_depth
         c.min_data_in_leaf = tc.min_data_in_leaf
         c.max_leaves = tc.max_leaves
+        c.grower = GROWERS[tc.grower]
         if tc.monotone:
             c._mono = np.asarray(tc.monotone, dtype=np.int32)
             c.monotone = _p(c._mono, C.c_int32)
@@ -381,7 +382,7 @@ class Oracle:
         rows = np.arange(n, dtype=np.uint32) if rows is None else np.ascontiguousarray(rows, np.uint32)
         selected = np.arange(F, dtype=np.uint32) if selected is None else np.ascontiguousarray(selected, np.uint32)
         nb = np.ascontiguousarray(n_bins, np.uint32)
-        cap = 4 << tc.max_depth if tc.grower == "depthwise" else 4 * max(tc.max_leaves, 2)
+        cap = 4 << tc.max_depth if tc.grower != "leafwise" else 4 * max(tc.max_leaves, 2)
         tb = _TreeBuf(cap)
         values = np.empty(n, np.float32)
         ids = np.empty(n, np.uint32)

@@ -16,6 +16,13 @@ inputs and stores inputs and outputs as .npz:
                          and their binned TreeSHAP contributions
   split_cases.npz        hand-built histograms and the reference finder's
                          chosen split for each (the test_split_node cases)
+  levelwise.npz          the levelwise (oblivious) grower: one depth-7 tree
+                         from fixed gradients over the missing-values data
+                         (min_child_hess 5: infeasible nodes) with its per-row
+                         values, and 20 MSE rounds at depth 6 on the small
+                         regression data with their training predictions;
+                         trees as level tables (features, thresholds,
+                         default directions, leaf values)
 
     python tests/golden/make_golden.py
 """
@@ -166,6 +173,31 @@ def main():
         out[f"split{i}"] = np.array([s["gain"], s["feature"], s["bin"], s["default_left"],
                                      s["valid"]], np.float64)
     np.savez_compressed(os.path.join(HERE, "split_cases.npz"), n=len(split_cases()), **out)
+    # --- levelwise
+    X, y = missing_values_data()
+    cuts, off = ref.fit_cuts(X)
+    ds = ref.dataset(X, y, cuts, off)
+    rng = np.random.Generator(np.random.PCG64(5))
+    g = rng.normal(0, 1, len(y)).astype(np.float32)
+    hh = rng.uniform(0.2, 1.0, len(y)).astype(np.float32)
+    _, lv_vals, _, m1 = ref.grow_tree(ds, TreeCfg(grower="levelwise", max_depth=7,
+                                                  min_child_hess=5.0), g, hh)
+    f1, t1, d1, l1 = m1.oblivious(0)
+    Xs, ys = synth.regression_small()
+    cs, os_ = ref.fit_cuts(Xs)
+    dss = ref.dataset(Xs, ys, cs, os_)
+    mb = ref.train(dss, TreeCfg(grower="levelwise", max_depth=6, n_iters=20))
+    lv = {}
+    for i in range(20):
+        f, t, d, lf = mb.oblivious(i)
+        lv[f"boost{i}_features"] = f
+        lv[f"boost{i}_thresholds"] = t
+        lv[f"boost{i}_default_left"] = d
+        lv[f"boost{i}_leaves"] = lf
+    np.savez_compressed(os.path.join(HERE, "levelwise.npz"), grad=g, hess=hh,
+                        one_values=lv_vals, one_features=f1, one_thresholds=t1,
+                        one_default_left=d1, one_leaves=l1, boost_init=np.float32(mb.init_score()),
+                        boost_pred=mb.predict_binned(dss), **lv)
     print("golden fixtures written")
 
 

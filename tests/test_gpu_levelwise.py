@@ -118,3 +118,36 @@ def test_levelwise_quantised_close_to_plain(bb):
         pos = y > 0.5
         return (r[pos].sum() - pos.sum() * (pos.sum() + 1) / 2) / (pos.sum() * (~pos).sum())
     assert abs(auc(out["exact"]) - auc(out["int8"])) < 2e-3
+
+
+def test_levelwise_tree_matches_golden(bb):
+    from conftest import load_golden
+    d = load_golden("missing_values.npz")
+    lv = load_golden("levelwise.npz")
+    plane = bb.Plane(d["X"], d["cuts"], d["cut_off"])
+    t, vals, _ = bb.grow_tree(plane, bb.TrainParams(grower="levelwise", max_depth=7,
+                                                    min_child_hess=5.0),
+                              lv["grad"], lv["hess"])
+    for a, b in zip(bb.oblivious_tables(t), (lv["one_features"], lv["one_thresholds"],
+                                             lv["one_default_left"], lv["one_leaves"])):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert np.array_equal(vals.view(np.uint32), lv["one_values"].view(np.uint32))
+
+
+def test_levelwise_booster_matches_golden(bb):
+    from conftest import load_golden
+    from bonsai_b200 import synth
+    d = load_golden("small_regression.npz")
+    lv = load_golden("levelwise.npz")
+    X, y = synth.regression_small()
+    plane = bb.Plane(X, d["cuts"], d["cut_off"])
+    b = bb.Booster(plane, y, bb.TrainParams(grower="levelwise", max_depth=6, use_graph=True),
+                   max_trees=20)
+    b.update(20)
+    assert np.float32(b.init_score) == lv["boost_init"]
+    for i in range(20):
+        want = (lv[f"boost{i}_features"], lv[f"boost{i}_thresholds"],
+                lv[f"boost{i}_default_left"], lv[f"boost{i}_leaves"])
+        for a, c in zip(bb.oblivious_tables(b.tree(i)), want):
+            assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(c).view(np.uint8)), i
+    assert np.array_equal(bb.predict(plane, b.trees(), b.init_score, 0.1), lv["boost_pred"])

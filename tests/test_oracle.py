@@ -108,3 +108,64 @@ def test_live_sampled_rows_match_reference(orc: Oracle, ref):
     assert_trees_equal(ot, rt)
     assert np.array_equal(ov, rv)
     assert np.array_equal(oids, rids)
+
+
+# ---- levelwise (ObliviousGrower) ------------------------------------------------
+
+def _tables_equal(mine, theirs, where=""):
+    for a, b, what in zip(mine, theirs, ("features", "thresholds", "default_left", "leaves")):
+        a, b = np.asarray(a), np.asarray(b)
+        assert a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8)), (
+            f"{where} {what}")
+
+
+def test_levelwise_tree_matches_golden(orc: Oracle):
+    from bonsai_b200 import oblivious_tables
+    d = load_golden("missing_values.npz")
+    lv = load_golden("levelwise.npz")
+    nb = np.diff(d["cut_off"])
+    t, vals, _ = orc.grow(d["bins"], nb, d["cuts"], d["cut_off"], lv["grad"], lv["hess"],
+                          TreeCfg(grower="levelwise", max_depth=7, min_child_hess=5.0))
+    _tables_equal(oblivious_tables(t), (lv["one_features"], lv["one_thresholds"],
+                                        lv["one_default_left"], lv["one_leaves"]))
+    assert np.array_equal(vals.view(np.uint32), lv["one_values"].view(np.uint32))
+
+
+def test_levelwise_boosting_matches_golden(orc: Oracle):
+    from bonsai_b200 import oblivious_tables, synth
+    d = load_golden("small_regression.npz")
+    lv = load_golden("levelwise.npz")
+    _, y = synth.regression_small()
+    bins = d["bins"].astype(np.uint16)
+    nb = np.diff(d["cut_off"])
+    trees, init, _ = orc.train(bins, nb, d["cuts"], d["cut_off"], y,
+                               TreeCfg(grower="levelwise", max_depth=6, n_iters=20))
+    assert np.float32(init) == lv["boost_init"]
+    for i, t in enumerate(trees):
+        _tables_equal(oblivious_tables(t), (lv[f"boost{i}_features"], lv[f"boost{i}_thresholds"],
+                                            lv[f"boost{i}_default_left"], lv[f"boost{i}_leaves"]),
+                      f"tree {i}")
+    assert np.array_equal(orc.predict_binned(bins, nb, trees, init, 0.1), lv["boost_pred"])
+
+
+@pytest.mark.parametrize("seed,cfg", [
+    (11, dict(max_depth=8)),
+    (12, dict(max_depth=8, min_child_hess=4.0, lambda_l2=0.0)),
+    (13, dict(max_depth=4, lambda_l1=0.7, min_gain_to_split=0.3)),
+])
+def test_levelwise_live_matches_reference(orc: Oracle, ref, seed, cfg):
+    from bonsai_b200 import oblivious_tables
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n, F = 3000, 5
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    X[rng.random(n) < 0.15, 1] = np.nan
+    X[:, 2] = np.round(X[:, 2])
+    g = rng.normal(0, 1, n).astype(np.float32)
+    h = rng.uniform(0.05, 1.0, n).astype(np.float32)
+    cuts, off = ref.fit_cuts(X)
+    ds = ref.dataset(X, np.zeros(n, np.float32), cuts, off)
+    tc = TreeCfg(grower="levelwise", **cfg)
+    _, rvals, _, m = ref.grow_tree(ds, tc, g, h)
+    t, vals, _ = orc.grow(ds.bins(), np.diff(off), cuts, off, g, h, tc)
+    _tables_equal(oblivious_tables(t), m.oblivious(0))
+    assert np.array_equal(vals.view(np.uint32), rvals.view(np.uint32))
