@@ -26,7 +26,8 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "pred_contribs", "oblivious_tables", "fit_cuts", "cuts_from_sample", "sample_rows",
+    "grow_tree", "populate", "predict", "pred_contribs", "oblivious_tables", "fit_cuts",
+    "Comm", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
@@ -181,20 +182,109 @@ class Plane:
         self.close()
 
 
+COMM_ID_BYTES = 128
+
+
+class Comm:
+    """A row-shard reducer (bb_comm): NCCL across processes, or one member
+    of an in-process group of shards."""
+
+    def __init__(self, h):
+        self.h = h
+
+    @staticmethod
+    def unique_id() -> bytes:
+        buf = (C.c_uint8 * COMM_ID_BYTES)()
+        check(lib().bb_comm_unique_id(C.cast(buf, C.c_void_p)))
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, uid: bytes, n_ranks: int, rank: int) -> "Comm":
+        buf = (C.c_uint8 * COMM_ID_BYTES).from_buffer_copy(uid)
+        h = C.c_void_p()
+        check(lib().bb_comm_create(C.cast(buf, C.c_void_p), n_ranks, rank, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def group(cls, n_shards: int) -> list:
+        arr = (C.c_void_p * n_shards)()
+        check(lib().bb_comm_group(n_shards, C.cast(arr, C.c_void_p)))
+        return [cls(arr[i]) for i in range(n_shards)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_comm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def shard_range(n_rows: int, n_shards: int, shard: int) -> tuple:
+    """Rows [begin, end) of shard `shard`: contiguous, sizes differing by one."""
+    return (n_rows * shard) // n_shards, (n_rows * (shard + 1)) // n_shards
+
+
+def label_sum(labels, start: float = 0.0) -> np.float32:
+    """std::accumulate over float labels: a float serial sum, continued from
+    `start` (so shards can chain it in row order)."""
+    s = np.float32(start)
+    for v in np.asarray(labels, np.float32):
+        s = np.float32(s + v)
+    return s
+
+
+_logf = None
+
+
+def init_score_from_sum(total: float, n_rows: int, objective: str) -> np.float32:
+    """The objective's initial score from the fit's float label sum: the
+    mean, or its log-odds through the C library's logf as the booster does."""
+    global _logf
+    m = np.float32(np.float32(total) / np.float32(n_rows))
+    if OBJECTIVES[objective] == 0:
+        return m
+    if _logf is None:
+        libm = C.CDLL("libm.so.6")
+        libm.logf.restype = C.c_float
+        libm.logf.argtypes = [C.c_float]
+        _logf = libm.logf
+    return np.float32(_logf(float(np.float32(m / np.float32(np.float32(1.0) - m)))))
+
+
+def init_score(labels, objective: str) -> np.float32:
+    """bb_booster_create's initial score over all of `labels`."""
+    return init_score_from_sum(label_sum(labels), len(labels), objective)
+
+
 class Booster:
-    """Device-resident boosting (bb_booster_*)."""
+    """Device-resident boosting (bb_booster_*). With comm, one row shard of a
+    fit: the plane and labels hold the fit's rows [row_offset, row_offset +
+    plane rows) of total_rows, and init_score is the fit's."""
 
     def __init__(self, plane: Plane, labels, params: TrainParams, max_trees: int = 1000,
-                 init_scores=None):
+                 init_scores=None, comm: Comm | None = None, row_offset: int = 0,
+                 total_rows: int | None = None, init_score: float | None = None):
         self.plane = plane
         self.params = params
         self._labels = np.ascontiguousarray(labels, dtype=np.float32)
         init = None if init_scores is None else np.ascontiguousarray(init_scores, np.float32)
         h = C.c_void_p()
         self._cfg = params.c()
-        check(lib().bb_booster_create(plane.h, ptr(self._labels),
-                                      None if init is None else ptr(init),
-                                      C.byref(self._cfg), max_trees, C.byref(h)))
+        if comm is None:
+            check(lib().bb_booster_create(plane.h, ptr(self._labels),
+                                          None if init is None else ptr(init),
+                                          C.byref(self._cfg), max_trees, C.byref(h)))
+        else:
+            self._comm = comm
+            check(lib().bb_booster_create_sharded(
+                plane.h, ptr(self._labels), None if init is None else ptr(init),
+                C.byref(self._cfg), max_trees, comm.h, row_offset,
+                plane.n_rows if total_rows is None else total_rows,
+                float(init_score), C.byref(h)))
         self.h = h.value
 
     def update(self, n_iters: int = 1, sync: bool = True):

@@ -90,6 +90,14 @@ def lib() -> C.CDLL:
             C.c_float, C.c_float, vp]
         L.bb_pred_contribs.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 7 + [
             C.c_float, C.c_float, vp]
+        L.bb_comm_unique_id.argtypes = [vp]
+        L.bb_comm_create.argtypes = [vp, C.c_uint32, C.c_uint32, C.POINTER(vp)]
+        L.bb_comm_group.argtypes = [C.c_uint32, vp]
+        L.bb_comm_destroy.argtypes = [vp]
+        L.bb_comm_destroy.restype = None
+        L.bb_booster_create_sharded.argtypes = [vp, vp, vp, C.POINTER(TrainCfg), C.c_uint32,
+                                                vp, C.c_uint64, C.c_uint64, C.c_float,
+                                                C.POINTER(vp)]
         L.bb_populate.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64, vp]
         _lib = L
     return _lib

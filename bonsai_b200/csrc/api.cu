@@ -1,6 +1,7 @@
 // The C ABI (include/bonsai_b200.h): planes, the device-resident booster,
 // single-tree growth and ensemble predict.
 #include "bonsai_b200.h"
+#include "shard.cuh"
 #include "grow.cuh"
 #include "ingest.cuh"
 
@@ -334,6 +335,86 @@ struct bb_booster
     }
 };
 
+namespace
+{
+
+// bb_booster_create's body; a sharded fit also passes its reducer, the
+// shard's first row in the fit, the fit's row count and the fit's init score
+// (the mean over every shard's labels, which no shard can form alone).
+bb_booster *create_booster(bb_plane const *plane, float const *labels, float const *init_scores,
+                           bb_train_cfg const *cfg, uint32_t max_trees, bb::Reducer *red,
+                           uint64_t row_offset, uint64_t total_rows, float const *init_score)
+{
+    need(plane != nullptr && labels != nullptr && cfg != nullptr,
+         "bb_booster_create: null argument");
+    need(cfg->objective == 0 || cfg->objective == 1, "objective must be 0 (mse) or 1 (logloss)");
+    need(max_trees > 0, "max_trees must be positive");
+    auto           b = std::make_unique<bb_booster>();
+    Plane const   &p = plane->p;
+    uint64_t const n = p.n_rows;
+    b->plane         = &p;
+    b->objective     = cfg->objective;
+    b->lr            = cfg->learning_rate;
+    BB_CHECK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    if (init_score != nullptr)
+    {
+        b->init = *init_score;
+    }
+    else
+    {
+        // init_score: a float serial sum, as std::accumulate does
+        float sum = 0.0F;
+        for (uint64_t i = 0; i < n; ++i)
+        {
+            sum += labels[i];
+        }
+        float const nn = static_cast<float>(n);
+        b->init = cfg->objective == 0 ? sum / nn : std::log((sum / nn) / (1.0F - (sum / nn)));
+    }
+    b->labels  = dmalloc<float>(n);
+    b->scores  = dmalloc<float>(n);
+    b->gh      = dmalloc<float2>(n);
+    b->rows    = dmalloc<uint32_t>(n);
+    b->leaf_id = dmalloc<uint32_t>(n);
+    b->round   = dmalloc<uint32_t>(1);
+    BB_CHECK(cudaMemcpyAsync(b->labels, labels, n * 4, cudaMemcpyHostToDevice, b->stream));
+    if (init_scores != nullptr)
+    {
+        BB_CHECK(cudaMemcpyAsync(b->scores, init_scores, n * 4, cudaMemcpyHostToDevice,
+                                 b->stream));
+    }
+    else
+    {
+        fill_kernel<<<blocks(n), 256, 0, b->stream>>>(b->scores, b->init, n);
+        BB_LAUNCH("fill_kernel");
+    }
+    iota_kernel<<<blocks(n), 256, 0, b->stream>>>(b->rows, n);
+    BB_LAUNCH("iota_kernel");
+    BB_CHECK(cudaMemsetAsync(b->round, 0, 4, b->stream));
+    b->grower = std::make_unique<Grower>(p, grow_config(*cfg), selection(*cfg, p.n_feats),
+                                         static_cast<uint32_t>(n), b->stream);
+    b->grower->set_monotone(monotone(*cfg));
+    b->grower->set_seed(cfg->seed);
+    if (red != nullptr)
+    {
+        b->grower->set_shard(red, row_offset, total_rows);
+    }
+    b->scratch.alloc(b->grower->max_nodes(), 1);
+    b->trees.alloc(b->grower->max_nodes(), max_trees);
+    b->use_graph       = cfg->use_graph != 0;
+    b->record_leaf_ids = cfg->record_leaf_ids != 0;
+    gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores, b->labels, b->gh,
+                                                      n);
+    BB_LAUNCH("gradient_kernel");
+    b->grower->seed_absmax(b->gh);
+    BB_CHECK(cudaEventCreate(&b->ev0));
+    BB_CHECK(cudaEventCreate(&b->ev1));
+    BB_CHECK(cudaStreamSynchronize(b->stream));
+    return b.release();
+}
+
+} // namespace
+
 extern "C"
 {
 
@@ -563,66 +644,29 @@ extern "C"
                           float const *init_scores, bb_train_cfg const *cfg,
                           uint32_t max_trees, bb_booster **out)
     {
+        return guarded([&] { *out = create_booster(plane, labels, init_scores, cfg, max_trees,
+                                                   nullptr, 0, 0, nullptr); });
+    }
+
+    int bb_booster_create_sharded(bb_plane const *plane, float const *labels,
+                                  float const *init_scores, bb_train_cfg const *cfg,
+                                  uint32_t max_trees, bb_comm *comm, uint64_t row_offset,
+                                  uint64_t total_rows, float init_score, bb_booster **out)
+    {
         return guarded(
             [&]
             {
-                need(plane != nullptr && labels != nullptr && cfg != nullptr && out != nullptr,
-                     "bb_booster_create: null argument");
-                need(cfg->objective == 0 || cfg->objective == 1,
-                     "objective must be 0 (mse) or 1 (logloss)");
-                need(max_trees > 0, "max_trees must be positive");
-                auto         b = std::make_unique<bb_booster>();
-                Plane const &p = plane->p;
-                uint64_t const n = p.n_rows;
-                b->plane         = &p;
-                b->objective     = cfg->objective;
-                b->lr            = cfg->learning_rate;
-                BB_CHECK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-                // init_score: a float serial sum, as std::accumulate does
-                float sum = 0.0F;
-                for (uint64_t i = 0; i < n; ++i)
+                need(comm != nullptr, "bb_booster_create_sharded: null comm");
+                need(plane != nullptr && row_offset + plane->p.n_rows <= total_rows,
+                     "bb_booster_create_sharded: the shard lies outside the fit's rows");
+                if (comm->member && cfg != nullptr && cfg->use_graph != 0)
                 {
-                    sum += labels[i];
+                    throw ConfigError("bb_booster_create_sharded: an in-process shard group "
+                                      "orders its shards by host threads; use_graph needs a "
+                                      "process per shard");
                 }
-                float const nn = static_cast<float>(n);
-                b->init        = cfg->objective == 0 ? sum / nn : std::log((sum / nn) / (1.0F - (sum / nn)));
-                b->labels      = dmalloc<float>(n);
-                b->scores      = dmalloc<float>(n);
-                b->gh          = dmalloc<float2>(n);
-                b->rows        = dmalloc<uint32_t>(n);
-                b->leaf_id     = dmalloc<uint32_t>(n);
-                b->round       = dmalloc<uint32_t>(1);
-                BB_CHECK(cudaMemcpyAsync(b->labels, labels, n * 4, cudaMemcpyHostToDevice, b->stream));
-                if (init_scores != nullptr)
-                {
-                    BB_CHECK(cudaMemcpyAsync(b->scores, init_scores, n * 4, cudaMemcpyHostToDevice,
-                                             b->stream));
-                }
-                else
-                {
-                    fill_kernel<<<blocks(n), 256, 0, b->stream>>>(b->scores, b->init, n);
-                    BB_LAUNCH("fill_kernel");
-                }
-                iota_kernel<<<blocks(n), 256, 0, b->stream>>>(b->rows, n);
-                BB_LAUNCH("iota_kernel");
-                BB_CHECK(cudaMemsetAsync(b->round, 0, 4, b->stream));
-                b->grower = std::make_unique<Grower>(p, grow_config(*cfg),
-                                                     selection(*cfg, p.n_feats),
-                                                     static_cast<uint32_t>(n), b->stream);
-                b->grower->set_monotone(monotone(*cfg));
-                b->grower->set_seed(cfg->seed);
-                b->scratch.alloc(b->grower->max_nodes(), 1);
-                b->trees.alloc(b->grower->max_nodes(), max_trees);
-                b->use_graph       = cfg->use_graph != 0;
-                b->record_leaf_ids = cfg->record_leaf_ids != 0;
-                gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores,
-                                                                  b->labels, b->gh, n);
-                BB_LAUNCH("gradient_kernel");
-                b->grower->seed_absmax(b->gh);
-                BB_CHECK(cudaEventCreate(&b->ev0));
-                BB_CHECK(cudaEventCreate(&b->ev1));
-                BB_CHECK(cudaStreamSynchronize(b->stream));
-                *out = b.release();
+                *out = create_booster(plane, labels, init_scores, cfg, max_trees,
+                                      comm->reducer(), row_offset, total_rows, &init_score);
             });
     }
 

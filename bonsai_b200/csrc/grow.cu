@@ -126,7 +126,7 @@ __device__ __forceinline__ float leaf_value(Node const &nd, TreeParams const &tp
 
 __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk *bchunks,
                                   uint32_t *brange, uint32_t *build, TreeOut t,
-                                  uint32_t crows)
+                                  uint32_t crows, uint32_t g_root)
 {
     uint32_t const nch = (n_root + crows - 1) / crows;
     if (threadIdx.x == 0)
@@ -141,6 +141,7 @@ __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk 
         Node nd{};
         nd.start  = 0;
         nd.count  = n_root;
+        nd.gcount = g_root;
         nd.id     = 0;
         nd.lo     = -INFINITY;
         nd.hi     = INFINITY;
@@ -150,7 +151,7 @@ __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk 
         brange[1] = nch;
         write_leaf_node(t, 0, 0.0F);
         t.gain[0]  = 0.0F;
-        t.cover[0] = static_cast<float>(n_root);
+        t.cover[0] = static_cast<float>(g_root);
     }
     for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x)
     {
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(k_find_thr)
     Node const     nd   = nodes[i];
     uint32_t const nb   = sel_nb[j];
     Best           out  = {0.0, j, 0, 1, 0};
-    if (nd.count < 2 * tp.min_data_in_leaf || nb < 2)
+    if (nd.gcount < 2 * tp.min_data_in_leaf || nb < 2)
     {
         if (tid == 0)
         {
@@ -1208,12 +1209,34 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// A sharded level's per-node left counts before they are combined across
+// shards: the sum of the node's chunks' counts from partition pass 1.
+__global__ void __launch_bounds__(k_plan_thr)
+    node_left_kernel(Ctl const *ctl, uint32_t const *pcr, uint32_t const *pleft,
+                     uint64_t *gleft, uint32_t n_slots)
+{
+    uint32_t const n_cur = ctl->n_cur;
+    for (uint32_t i = threadIdx.x; i < n_slots; i += k_plan_thr)
+    {
+        uint64_t nl = 0;
+        if (i < n_cur)
+        {
+            for (uint32_t c = pcr[i]; c < pcr[i + 1]; ++c)
+            {
+                nl += pleft[c];
+            }
+        }
+        gleft[i] = nl;
+    }
+}
+
 __global__ void __launch_bounds__(k_plan_thr)
     plan2_kernel(Ctl *ctl, Node *nodes, Node *next, Best const *best,
                  Chunk const *pchunks, uint32_t const *pcr, uint32_t *pleft,
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
-                 TreeOut t, uint32_t crows, uint32_t *bbase, bool level)
+                 TreeOut t, uint32_t crows, uint32_t *bbase, bool level,
+                 uint64_t const *gleft)
 {
     __shared__ uint32_t grand_s;
     uint32_t const      n_cur = ctl->n_cur;
@@ -1247,6 +1270,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     Node           nd   = live ? nodes[i] : Node{};
     bool           surv = false;
     uint32_t       nl   = 0;
+    uint32_t       gnl  = 0; // rows routed left over every shard
     uint32_t       p0   = 0;
     if (live && (nd.flags & 1) != 0)
     {
@@ -1257,7 +1281,8 @@ __global__ void __launch_bounds__(k_plan_thr)
         p0                = c0 < n_ch ? pleft[c0] : grand_s;
         nl                = (c1 < n_ch ? pleft[c1] : grand_s) - p0;
         nleft[i]          = nl;
-        if (!level && (nl == 0 || nl == nd.count))
+        gnl               = gleft != nullptr ? static_cast<uint32_t>(gleft[i]) : nl;
+        if (!level && (gnl == 0 || gnl == nd.gcount))
         {
             // demote_empty_splits: the parent is a leaf after all (a level
             // split applies to every node, empty children included)
@@ -1300,15 +1325,17 @@ __global__ void __launch_bounds__(k_plan_thr)
     {
         dst[i]              = start;
         uint32_t const nr   = nd.count - nl;
+        uint32_t const gnr  = nd.gcount - gnl;
         uint32_t const lid  = t.left[nd.id];
         uint32_t const rid  = t.right[nd.id];
-        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0};
-        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0};
+        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0};
+        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0};
         next[2 * k]         = L;
         next[(2 * k) + 1]   = R;
-        t.cover[lid]        = static_cast<float>(nl);
-        t.cover[rid]        = static_cast<float>(nr);
-        bool const left_sm  = nl <= nr;
+        t.cover[lid]        = static_cast<float>(gnl);
+        t.cover[rid]        = static_cast<float>(gnr);
+        // the smaller child over the whole fit: every shard builds the same one
+        bool const left_sm  = gnl <= gnr;
         bpair[(3 * k) + 0]  = i;
         bpair[(3 * k) + 1]  = (2 * k) + (left_sm ? 0 : 1);
         bpair[(3 * k) + 2]  = (2 * k) + (left_sm ? 1 : 0);
@@ -2014,7 +2041,7 @@ __global__ void __launch_bounds__(k_threads)
     quantise_kernel(float2 const *__restrict__ gh, uint32_t n,
                     uint32_t const *__restrict__ absmax, uint2 key,
                     uint32_t const *__restrict__ tree_no, uint16_t *__restrict__ q,
-                    double2 *__restrict__ scale)
+                    double2 *__restrict__ scale, uint64_t row_off)
 {
     double const mg = __uint_as_float(absmax[0]);
     double const mh = __uint_as_float(absmax[1]);
@@ -2031,7 +2058,11 @@ __global__ void __launch_bounds__(k_threads)
          i += gridDim.x * k_threads)
     {
         float2 const v  = gh[i];
-        uint4 const  r  = philox4x32_10(make_uint4(i, t, 0x5157u, 0u), key);
+        // counter: the row's index in the whole fit, so shards round alike
+        uint64_t const gi = row_off + i;
+        uint4 const  r  = philox4x32_10(make_uint4(static_cast<uint32_t>(gi), t, 0x5157u,
+                                                   static_cast<uint32_t>(gi >> 32)),
+                                        key);
         double const ug = static_cast<double>(r.x >> 8) * (1.0 / 16777216.0);
         double const uh = static_cast<double>(r.y >> 8) * (1.0 / 16777216.0);
         double const xg = static_cast<double>(v.x) * ig;
@@ -2882,7 +2913,7 @@ Grower::~Grower()
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
                     tile_j_[1], bbase_,   dirs_,    btot_,    done_,    wacc_,
-                    leaf16_,  nbound_};
+                    leaf16_,  nbound_,  gleft_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -2915,6 +2946,27 @@ void Grower::phase_end(double &acc)
     }
 }
 
+void Grower::set_shard(Reducer *r, uint64_t row_offset, uint64_t total_rows)
+{
+    if (r != nullptr && !quant_)
+    {
+        throw ConfigError("grower: a sharded fit needs the quantised form (integer "
+                          "histograms combine exactly; float cells would not)");
+    }
+    if (r != nullptr && total_rows * 127ULL >= (1ULL << 31))
+    {
+        throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per fit");
+    }
+    red_        = r;
+    row_off_    = row_offset;
+    total_rows_ = total_rows;
+    if (gleft_ == nullptr)
+    {
+        gleft_ = dalloc<uint64_t>(max_front_, stream_);
+        BB_CHECK(cudaStreamSynchronize(stream_));
+    }
+}
+
 void Grower::seed_absmax(float2 const *gh)
 {
     if (!quant_)
@@ -2942,9 +2994,14 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
         BB_LAUNCH("absmax_kernel");
         n_launch_ += 1;
     }
+    if (red_ != nullptr)
+    {
+        red_->max_u32(absmax_, 2, s); // the fit's maxima: one scale for every shard
+    }
     uint2 const key = make_uint2(static_cast<uint32_t>(seed_),
                                  static_cast<uint32_t>(seed_ >> 32));
-    quantise_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_, qscale_);
+    quantise_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_, qscale_,
+                                               row_off_);
     BB_LAUNCH("quantise_kernel");
     n_launch_ += 1;
 }
@@ -3119,10 +3176,17 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             sel_nb_, pleft_, dirs_);
     }
     BB_LAUNCH("pcount_kernel");
+    if (red_ != nullptr)
+    {
+        node_left_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pcr_, pleft_, gleft_, max_front_);
+        BB_LAUNCH("node_left_kernel");
+        red_->sum_u64(gleft_, max_front_, s);
+        n_launch_ += 1;
+    }
     plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
                                           pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
                                           build_, brange_, bchunks_, cfg_.tp, t, crows_,
-                                          bbase_, cfg_.level);
+                                          bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -3158,6 +3222,10 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         qbuilt_totals_kernel<<<max_bchunks_, k_threads, 0, s>>>(ctl_, bchunks_, rows_out,
                                                                  qgh8_, btot_);
         BB_LAUNCH("qbuilt_totals_kernel");
+        if (red_ != nullptr)
+        {
+            red_->sum_u64(btot_, 2 * static_cast<size_t>(max_front_), s);
+        }
         qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
             ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
@@ -3172,6 +3240,13 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     build(rows_out, nfb, nxt, true);
     uint32_t const n_cells = off_h_[nfb]; // the built features: a selection prefix
+    if (red_ != nullptr)
+    {
+        // the next frontier's slots (at most 2^(L+1)): the built ones carry
+        // this shard's partial cells, the rest are rewritten by the subtraction
+        size_t const slots = std::min<size_t>(size_t{2} << L, max_front_);
+        red_->sum_u64(hist_[nxt], slots * total_cells_, s);
+    }
     phase_begin();
     if (quant_)
     {
@@ -3216,6 +3291,11 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     {
         throw ConfigError("grower: a fused next round needs every row as the root");
     }
+    if (red_ != nullptr && (!quant_ || !walk_))
+    {
+        throw ConfigError("grower: a sharded fit needs the quantised form and every row as "
+                          "the root");
+    }
     if (quant_)
     {
         phase_begin();
@@ -3225,13 +3305,18 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             phase_end(prof_->other_ms);
         }
     }
+    uint32_t const g_root = red_ != nullptr ? static_cast<uint32_t>(total_rows_) : n_root;
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t, crows_);
+                                              build_, t, crows_, g_root);
     BB_LAUNCH("root_setup_kernel");
     n_launch_ += 1;
     // the root's rows: the quantised build reads an identity list implicitly
     build(quant_ && identity_root ? nullptr : root_rows,
           cfg_.tp.max_depth == 0 ? 1 : n_sel_, 0);
+    if (red_ != nullptr)
+    {
+        red_->sum_u64(hist_[0], total_cells_, s);
+    }
     phase_begin();
     if (quant_)
     {
@@ -3298,6 +3383,10 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
                 multi ? sum(walk_sum_kernel<false, true>) : sum(walk_sum_kernel<false, false>);
             }
             BB_LAUNCH("walk_sum_kernel");
+            if (red_ != nullptr)
+            {
+                red_->sum_u64(wacc_, 2 * static_cast<size_t>(k_walk_nodes), s);
+            }
             leaf_fix_kernel<<<1, k_threads, 0, s>>>(ctl_, t, wacc_, nbound_, absmax_, cfg_.tp);
             BB_LAUNCH("leaf_fix_kernel");
             if (next != nullptr)
@@ -3364,7 +3453,7 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     }
     walk_ = false;
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n, bchunks_, brange_, build_,
-                                              t, crows_);
+                                              t, crows_, n);
     BB_LAUNCH("root_setup_kernel");
     build(rows, n_sel_, 0);
     std::vector<double2> cells(total_cells_);

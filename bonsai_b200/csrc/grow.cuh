@@ -29,6 +29,8 @@ struct Node
     double   hi;
     int64_t  qg; // quantised form: exact integer totals
     int64_t  qh;
+    uint32_t gcount; // rows over every shard of the fit (count when unsharded)
+    uint32_t pad_;
 };
 
 // SplitOutput (include/bonsai/split.hpp:62-69), one per (node, feature)
@@ -102,6 +104,20 @@ struct Profile
     uint32_t hist_builds  = 0;
 };
 
+// Combines a device buffer across the row shards of one fit, in stream
+// order and in place: sums of 64-bit two's-complement integers, or maxima of
+// 32-bit unsigned words. Every shard makes the same calls in the same order.
+// The shard-parallel design of the reference's parked multi-GPU plan
+// (docs/architecture/19-multi-gpu.md:20-35): rows stay where they are, only
+// integer histograms and a few counts cross between shards.
+class Reducer
+{
+  public:
+    virtual ~Reducer()                                            = default;
+    virtual void sum_u64(void *buf, size_t n, cudaStream_t s) = 0;
+    virtual void max_u32(void *buf, size_t n, cudaStream_t s) = 0;
+};
+
 // A resident booster's next round, computed by the final walk over every
 // row once the tree is complete: gh[r] from the updated score and the label,
 // and (quantised form) the maxima the next quantisation scales come from.
@@ -149,6 +165,12 @@ class Grower
     // The quantised form's gradient maxima of gh (every dataset row), for a
     // first grow() whose next round is fused.
     void seed_absmax(float2 const *gh);
+    // Makes this grower one row shard of a fit: its plane holds the fit's
+    // rows [row_offset, row_offset + n_rows) of total_rows, and r combines the
+    // shards' integer partial sums so every shard takes the same decisions.
+    // Quantised form with every row as the root only; the trees equal an
+    // unsharded fit's bit for bit.
+    void set_shard(Reducer *r, uint64_t row_offset, uint64_t total_rows);
 
     // One node's histograms (HistogramEngine::populate): quantises (when
     // quantised) and builds every selected feature over the given rows;
@@ -249,6 +271,10 @@ class Grower
     uint32_t const *root_rows_ = nullptr;
     void      quantise(float2 const *gh, uint32_t n, bool have_absmax);
     bool      walk_ = false; // this tree's rows are stamped by the final walk
+    Reducer  *red_        = nullptr; // shard reducer, or none
+    uint64_t  row_off_    = 0;       // the shard's first row in the fit
+    uint64_t  total_rows_ = 0;       // rows of the whole fit
+    uint64_t *gleft_      = nullptr; // per frontier node: rows routed left, all shards
     void      leaf_values(TreeOut const &t, bool final_level);
     uint64_t  seed_     = 0;
     uint32_t  tree_no_  = 0;

@@ -195,6 +195,43 @@ int bb_populate(bb_plane const *plane, bb_train_cfg const *cfg, float const *gra
                 float const *hess, uint32_t const *rows, uint64_t n_sel_rows,
                 double *out);
 
+/* ---- row shards: one fit over several GPUs ----------------------------------
+ * No counterpart in the reference's code: its multi-GPU plan is parked
+ * (docs/architecture/19-multi-gpu.md, "The algorithm maps onto bonsai's
+ * control flow"). Each shard holds a contiguous range of the fit's rows in its
+ * own plane; per level the shards combine their integer partial histograms,
+ * per-node row counts, the quantisation maxima and the leaves' fixed-point
+ * sums (in place, every shard the same calls), so every shard takes the same
+ * decisions and the trees equal a one-GPU fit's bit for bit. Rows never move.
+ * The quantised form only (float cells would not combine exactly). */
+typedef struct bb_comm bb_comm;
+
+#define BB_COMM_ID_BYTES 128
+
+/* A fresh NCCL unique id (rank 0 makes it and shares it with the others). */
+int bb_comm_unique_id(uint8_t *out /* BB_COMM_ID_BYTES */);
+
+/* One process's member of an NCCL communicator over n_ranks processes (one
+ * GPU each, the calling thread's current device); collectives run in place
+ * on the booster's stream and are captured into its CUDA graph. */
+int bb_comm_create(uint8_t const *id, uint32_t n_ranks, uint32_t rank, bb_comm **out);
+
+/* n_shards (<= 16) members of an in-process group: shards of one fit driven
+ * from one host thread each (boosters created without use_graph, updated
+ * concurrently); they order through CUDA events on the boosters' streams. */
+int bb_comm_group(uint32_t n_shards, bb_comm **members);
+
+void bb_comm_destroy(bb_comm *comm);
+
+/* bb_booster_create for one shard: plane and labels hold the fit's rows
+ * [row_offset, row_offset + plane rows) of total_rows; init_score is the
+ * fit's (the objective's initial score over every shard's labels). hist_mode
+ * must be quantised. */
+int bb_booster_create_sharded(bb_plane const *plane, float const *labels,
+                              float const *init_scores, bb_train_cfg const *cfg,
+                              uint32_t max_trees, bb_comm *comm, uint64_t row_offset,
+                              uint64_t total_rows, float init_score, bb_booster **out);
+
 /* ---- inference ------------------------------------------------------------
  * Ensemble predict over a plane: out[r] = init + lr * sum_t leaf_t(r), the
  * leaves summed in tree order (bit-identical to predict_at_binned,
