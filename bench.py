@@ -229,7 +229,22 @@ def main():
     barrier(world)
     bb.lib().bb_select_device(local)
     X, y, cuts, off = make_data(args.rows)
-    n, F = X.shape
+    n_fit, F = X.shape
+    # N > 1: the quantised fit is row-sharded -- each rank holds a contiguous
+    # slice of the same 10M rows and the ranks combine integer histograms over
+    # NCCL (strong scaling; trees equal the one-GPU fit's); the exact form's
+    # float cells do not combine exactly, so it runs one replica per GPU
+    sharded = world > 1 and args.mode != "exact"
+    comm = None
+    row0 = 0
+    if sharded:
+        from bonsai_b200 import dist as bdist
+        row0, row1 = bdist.shard_range(n_fit, world, rank)
+        X = np.ascontiguousarray(X[row0:row1])
+        y = np.ascontiguousarray(y[row0:row1])
+        init = bdist.sharded_init_score(y, n_fit, "logloss", world, rank)
+        comm = bdist.open_comm(world, rank)
+    n = X.shape[0]
 
     # ---- end to end through the C ABI with host buffers: ingest (H2D of the
     # raw matrix + bin application), labels up, rounds, model + scores down
@@ -243,7 +258,11 @@ def main():
     barrier(world)
     t0 = time.perf_counter()
     plane = bb.Plane(Xp, cuts, off)
-    b = bb.Booster(plane, yp, params, max_trees=W + K + 4)
+    if sharded:
+        b = bb.Booster(plane, yp, params, max_trees=W + K + 4, comm=comm, row_offset=row0,
+                       total_rows=n_fit, init_score=init)
+    else:
+        b = bb.Booster(plane, yp, params, max_trees=W + K + 4)
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
 
@@ -264,10 +283,12 @@ def main():
 
     prof = b.profile_round()
     b.close()
+    if comm is not None:
+        comm.close()
 
     # the plain (exact) form on the same plane, for the headline ratio
     plain = None
-    if args.mode != "exact" and args.compare_steps > 0:
+    if args.mode != "exact" and args.compare_steps > 0 and not sharded:
         pp = bb.TrainParams(objective="logloss", max_depth=8, learning_rate=0.1,
                             min_data_in_leaf=20, hist_mode="exact", use_graph=True)
         bp = bb.Booster(plane, yp, pp, max_trees=W + args.compare_steps + 1)
@@ -292,12 +313,16 @@ def main():
     e2e = t_setup + value + t_down
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": K,
-        "warmup": W, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "warmup": W, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f32" if args.mode == "exact" else args.mode,
         "data": "synthetic (seeded HIGGS-shaped stand-in)",
-        "config": {"workload": WORKLOAD, "rows": n, "features": F, "rounds": N_ROUNDS,
+        "config": {"workload": WORKLOAD, "rows": n_fit, "features": F, "rounds": N_ROUNDS,
                    "hist_mode": args.mode, "graph": True,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "parallelism": (f"row shards x{world} (NCCL all-reduce of integer "
+                                   "histograms)" if sharded else
+                                   f"replicas x{world}" if world > 1 else "single"),
+                   "rows_per_gpu": n,
                    "l2": "inputs larger than L2 (bins 280 MB, gh 80 MB)"},
         "e2e": {"value": e2e, "unit": "s",
                 "h2d_bytes_per_step": (X.nbytes + y.nbytes) / N_ROUNDS,

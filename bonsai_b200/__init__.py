@@ -193,13 +193,24 @@ class Comm:
         self.h = h
 
     @staticmethod
+    def _load_nccl():
+        # the process's NCCL is PyTorch's when PyTorch is present: load it
+        # before the library resolves libnccl.so.2
+        try:
+            import torch  # noqa: F401
+        except ImportError:
+            pass
+
+    @staticmethod
     def unique_id() -> bytes:
+        Comm._load_nccl()
         buf = (C.c_uint8 * COMM_ID_BYTES)()
         check(lib().bb_comm_unique_id(C.cast(buf, C.c_void_p)))
         return bytes(buf)
 
     @classmethod
     def nccl(cls, uid: bytes, n_ranks: int, rank: int) -> "Comm":
+        cls._load_nccl()
         buf = (C.c_uint8 * COMM_ID_BYTES).from_buffer_copy(uid)
         h = C.c_void_p()
         check(lib().bb_comm_create(C.cast(buf, C.c_void_p), n_ranks, rank, C.byref(h)))

@@ -4,8 +4,8 @@
 // NCCL: one process per GPU, an in-place ncclAllReduce on the grower's
 // stream (sums as uint64, maxima as uint32), so it orders with the kernels
 // around it and is captured into the round's CUDA graph. libnccl.so.2 is
-// opened at run time (the copy a process already loaded, e.g. PyTorch's, is
-// the one found), so the library itself needs no NCCL at link time.
+// opened at run time -- the copy the process already loaded (e.g.
+// PyTorch's) when there is one -- so the library needs no NCCL at link time.
 //
 // Group: several shards in one process (one host thread per shard, each with
 // its own stream). At each reduction every member records an event on its
@@ -53,7 +53,13 @@ NcclApi const &nccl()
     {
         return api;
     }
-    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    // the process's own NCCL when one is loaded (e.g. PyTorch's): loading a
+    // second copy first would take the soname from the one it links against
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (h == nullptr)
+    {
+        h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+    }
     if (h == nullptr)
     {
         throw ConfigError(std::string("bb_comm: libnccl.so.2 not found: ") + dlerror());

@@ -213,7 +213,9 @@ int bb_comm_unique_id(uint8_t *out /* BB_COMM_ID_BYTES */);
 
 /* One process's member of an NCCL communicator over n_ranks processes (one
  * GPU each, the calling thread's current device); collectives run in place
- * on the booster's stream and are captured into its CUDA graph. */
+ * on the booster's stream and are captured into its CUDA graph. NCCL is
+ * resolved at the first bb_comm call: the libnccl.so.2 the process already
+ * loaded if any (load the framework's NCCL first), else the system's. */
 int bb_comm_create(uint8_t const *id, uint32_t n_ranks, uint32_t rank, bb_comm **out);
 
 /* n_shards (<= 16) members of an in-process group: shards of one fit driven
