@@ -33,7 +33,7 @@ __all__ = [
 
 LEAF = 0xFFFFFFFF
 OBJECTIVES = {"mse": 0, "logloss": 1}
-GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1}
+GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1, "leafwise": 2}
 HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
 
 
@@ -60,6 +60,7 @@ class TrainParams:
     use_graph: bool = False
     record_leaf_ids: bool = False
     grower: str = "depthwise"
+    max_leaves: int = 31
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -74,6 +75,7 @@ class TrainParams:
         c.hist_mode = HIST_MODES[self.hist_mode]
         c.seed = self.seed
         c.grower = GROWERS[self.grower]
+        c.max_leaves = self.max_leaves
         c.use_graph = 1 if self.use_graph else 0
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:
@@ -358,18 +360,18 @@ class Booster:
 
 
 def grow_tree(plane: Plane, params: TrainParams, grad, hess, rows=None):
-    """One depthwise tree from given gradients (bb_grow_tree): returns
+    """One tree from given gradients (bb_grow_tree): returns
     (tree, values, leaf_ids) over every row (unsampled rows: NaN / max)."""
     n = plane.n_rows
     grad = np.ascontiguousarray(grad, np.float32)
     hess = np.ascontiguousarray(hess, np.float32)
-    cap = (2 << params.max_depth) - 1
+    cfg = params.c()
+    cap = int(lib().bb_tree_capacity(C.byref(cfg)))
     a = _tree_arrays(cap)
     meta = np.zeros(3, np.uint32)
     values = np.full(n, np.nan, np.float32)
     ids = np.full(n, LEAF, np.uint32)
     r = None if rows is None else np.ascontiguousarray(rows, np.uint32)
-    cfg = params.c()
     check(lib().bb_grow_tree(plane.h, C.byref(cfg), ptr(grad), ptr(hess),
                              None if r is None else ptr(r), 0 if r is None else len(r),
                              *(ptr(a[k]) for k in _ORDER), ptr(meta), ptr(values),

@@ -234,9 +234,11 @@ struct TreeStore
 
 GrowConfig grow_config(bb_train_cfg const &c)
 {
-    need(c.max_depth <= 8, "max_depth must be <= 8 on the device level plane");
+    need(c.grower >= 0 && c.grower <= 2,
+         "grower must be 0 (depthwise), 1 (levelwise) or 2 (leafwise)");
+    need(c.grower == 2 ? c.max_depth <= 255 : c.max_depth <= 8,
+         "max_depth must be <= 8 on the device level plane (leafwise: <= 255)");
     need(c.hist_mode >= 0 && c.hist_mode <= 2, "hist_mode must be 0, 1 or 2");
-    need(c.grower == 0 || c.grower == 1, "grower must be 0 (depthwise) or 1 (levelwise)");
     if (c.grower == 1)
     {
         for (uint32_t f = 0; c.monotone != nullptr && f < c.n_monotone; ++f)
@@ -251,13 +253,14 @@ GrowConfig grow_config(bb_train_cfg const &c)
     }
     GrowConfig g;
     g.level                = c.grower == 1;
+    g.leaf                 = c.grower == 2;
     g.tp.min_child_hess    = c.min_child_hess;
     g.tp.min_gain_to_split = c.min_gain_to_split;
     g.tp.lambda_l2         = c.lambda_l2;
     g.tp.lambda_l1         = c.lambda_l1;
     g.tp.max_depth         = c.max_depth;
     g.tp.min_data_in_leaf  = c.min_data_in_leaf;
-    g.tp.max_leaves        = 0;
+    g.tp.max_leaves        = c.grower == 2 ? c.max_leaves : 0;
     g.mode                 = static_cast<HistMode>(c.hist_mode);
     return g;
 }
@@ -326,7 +329,19 @@ struct bb_booster
     // creation, then by each round's final walk for the next round
     void round_body()
     {
-        uint64_t const      n = plane->n_rows;
+        uint64_t const n = plane->n_rows;
+        if (!grower->fuses_next())
+        {
+            // the leafwise plane stamps from its leaves' segments: gradients
+            // of the current scores come from their own pass
+            gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
+            BB_LAUNCH("gradient_kernel");
+            grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
+                         record_leaf_ids ? leaf_id : nullptr, scores, lr, true, nullptr);
+            commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
+            BB_LAUNCH("commit_tree_kernel");
+            return;
+        }
         bb::NextRound const next{objective, labels, gh};
         grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
                      record_leaf_ids ? leaf_id : nullptr, scores, lr, true, &next);
@@ -401,7 +416,8 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     }
     b->scratch.alloc(b->grower->max_nodes(), 1);
     b->trees.alloc(b->grower->max_nodes(), max_trees);
-    b->use_graph       = cfg->use_graph != 0;
+    // a leafwise round reads every pop back to the host: it runs eagerly
+    b->use_graph       = cfg->use_graph != 0 && b->grower->fuses_next();
     b->record_leaf_ids = cfg->record_leaf_ids != 0;
     gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores, b->labels, b->gh,
                                                       n);
@@ -421,6 +437,22 @@ extern "C"
     char const *bb_last_error(void)
     {
         return g_err.c_str();
+    }
+
+    uint32_t bb_tree_capacity(bb_train_cfg const *cfg)
+    {
+        if (cfg == nullptr)
+        {
+            return 0;
+        }
+        if (cfg->grower == 2)
+        {
+            uint32_t const l = cfg->max_leaves == 0 && cfg->max_depth <= 9
+                                   ? 1u << cfg->max_depth
+                                   : cfg->max_leaves;
+            return 4 * std::max<uint32_t>(l, 1);
+        }
+        return cfg->max_depth <= 8 ? (2u << cfg->max_depth) - 1 : 0;
     }
 
     int bb_available(void)
@@ -894,14 +926,14 @@ extern "C"
                     BB_CHECK(cudaStreamSynchronize(s));
                     ts.download(0, feature, value, left, right, default_left, gain, cover,
                                 split_bin, meta);
-                    std::vector<float>    v(n);
                     std::vector<uint32_t> ids(n);
-                    BB_CHECK(cudaMemcpy(v.data(), d_val, n * 4, cudaMemcpyDeviceToHost));
                     BB_CHECK(cudaMemcpy(ids.data(), d_leaf, n * 4, cudaMemcpyDeviceToHost));
+                    // each row takes its leaf's value itself (a stamped 0 + v
+                    // would turn a -0.0 leaf into +0.0)
                     for (uint64_t k = 0; k < m; ++k)
                     {
                         uint64_t const r = rows == nullptr ? k : rows[k];
-                        values[r]        = v[r];
+                        values[r]        = value[ids[r]];
                         leaf_ids[r]      = ids[r];
                     }
                 }

@@ -533,7 +533,8 @@ __global__ void __launch_bounds__(k_find_thr)
     find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
                 uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                 uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
-                TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale)
+                TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale,
+                uint32_t const *slot_of)
 {
     extern __shared__ unsigned char smem_raw[];
     __shared__ double   bg_s[k_find_thr / 32];
@@ -563,9 +564,11 @@ __global__ void __launch_bounds__(k_find_thr)
         return;
     }
     uint32_t const n_cut = nb - 2;
-    // the cells, 8 bytes each (packed integers or a float2)
+    // the cells, 8 bytes each (packed integers or a float2); a node's slot
+    // is its frontier index unless slot_of names it (the leafwise pool)
+    uint32_t const slot = slot_of != nullptr ? slot_of[i] : i;
     auto const *src = static_cast<unsigned long long const *>(hist_v) +
-                      (static_cast<uint64_t>(i) * total_cells) + cell_off[j];
+                      (static_cast<uint64_t>(slot) * total_cells) + cell_off[j];
     for (uint32_t b = tid; b < nb; b += k_find_thr)
     {
         raw[b] = src[b];
@@ -2699,6 +2702,292 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// ----------------------------------------------------------------- leafwise ----
+//
+// One heap pop of the leafwise grower (LeafwiseGrower::grow,
+// src/grower_impl.hpp:744-850; split_node, src/step/primitives.hpp:381-430) on
+// the device data plane. The host keeps the gain heap and the tree (pop order,
+// child ids, demotions, the leaf budget); the device partitions the popped
+// node's segment of the row buffer with the two partition passes (stable),
+// builds its smaller child's histograms into a free slot of a histogram pool,
+// subtracts the larger child in place in the parent's slot (finish_split),
+// and finds both children's best splits with the node finder.
+
+struct LeafPop
+{
+    Node     node; // the popped node: its segment of the row buffer, totals, bounds
+    Best     best; // its split
+    uint32_t left_id;
+    uint32_t right_id;
+    uint32_t parent_slot;
+    uint32_t small_slot;
+};
+
+// What the host reads back after a pop (or after the root).
+struct LeafOut
+{
+    Node     child[2];
+    Best     best[2];
+    uint32_t split; // 0: the partition emptied a side (the split is demoted)
+    uint32_t small_left;
+    uint32_t pad[2];
+};
+
+__global__ void __launch_bounds__(k_plan_thr)
+    leaf_setup_kernel(Ctl *ctl, Node *nodes, Best *best, Chunk *pchunks, uint32_t *pcr,
+                      LeafPop p)
+{
+    uint32_t const nch = (p.node.count + k_part_rows - 1) / k_part_rows;
+    if (threadIdx.x == 0)
+    {
+        ctl->n_cur     = 1;
+        ctl->n_pchunks = nch;
+        Node nd        = p.node;
+        nd.flags       = 1;
+        nodes[0]       = nd;
+        best[0]        = p.best;
+        pcr[0]         = 0;
+        pcr[1]         = nch;
+    }
+    for (uint32_t c = threadIdx.x; c < nch; c += k_plan_thr)
+    {
+        uint32_t const b = c * k_part_rows;
+        pchunks[c]       = {0, p.node.start + b, min(k_part_rows, p.node.count - b), 0};
+    }
+}
+
+// After partition pass 1: the chunks' left bases, the node's left count, and
+// either the demotion (a side came out empty) or the two children, the
+// smaller child's build chunks (in the scatter's output, which starts at 0)
+// and the pool slots each child's histograms will sit in.
+__global__ void __launch_bounds__(k_plan_thr)
+    leaf_plan_kernel(Ctl *ctl, Chunk const *pchunks, uint32_t *pleft, uint32_t *prbase,
+                     uint32_t *nleft, uint32_t *dst, uint32_t *build, uint32_t *brange,
+                     uint32_t *bbase, Chunk *bchunks, uint32_t *bpair, Node *nodes, Node *next,
+                     uint32_t *slot_of, LeafOut *out, uint32_t crows, LeafPop p)
+{
+    uint32_t const n_ch = ctl->n_pchunks;
+    uint32_t const per  = (n_ch + k_plan_thr - 1) / k_plan_thr;
+    uint32_t const c_a  = min(n_ch, threadIdx.x * per);
+    uint32_t const c_b  = min(n_ch, c_a + per);
+    uint32_t       sum  = 0;
+    for (uint32_t c = c_a; c < c_b; ++c)
+    {
+        sum += pleft[c];
+    }
+    uint32_t       nl   = 0;
+    uint32_t const base = block_excl_scan<k_plan_thr>(sum, &nl);
+    for (uint32_t c = c_a, run = base; c < c_b; ++c)
+    {
+        uint32_t const v = pleft[c];
+        pleft[c]         = run;
+        prbase[c]        = (pchunks[c].begin - p.node.start) - run;
+        run += v;
+    }
+    uint32_t const count = p.node.count;
+    uint32_t const nr    = count - nl;
+    bool const     split = nl != 0 && nl != count;
+    bool const     sl    = nl <= nr; // the left child wins a size tie
+    uint32_t const sc    = sl ? nl : nr;
+    uint32_t const sb    = sl ? 0 : nl;
+    uint32_t const nchb  = split ? (sc + crows - 1) / crows : 0;
+    if (threadIdx.x == 0)
+    {
+        nleft[0]        = nl;
+        dst[0]          = 0;
+        out->split      = split ? 1 : 0;
+        out->small_left = sl ? 1 : 0;
+        ctl->n_build    = split ? 1 : 0;
+        ctl->n_bchunks  = nchb;
+        ctl->n_splits   = split ? 1 : 0;
+        ctl->built_rows = split ? sc : 0;
+        if (!split)
+        {
+            nodes[0].flags |= 2; // the scatter leaves a demoted node's rows alone
+        }
+        else
+        {
+            Node L    = p.node;
+            L.count   = nl;
+            L.gcount  = nl;
+            L.id      = p.left_id;
+            L.flags   = 0;
+            Node R    = p.node;
+            R.start   = p.node.start + nl;
+            R.count   = nr;
+            R.gcount  = nr;
+            R.id      = p.right_id;
+            R.flags   = 0;
+            next[0]   = L;
+            next[1]   = R;
+            build[0]  = p.small_slot;
+            brange[0] = 0;
+            brange[1] = nchb;
+            bbase[0]  = 0;
+            slot_of[0] = sl ? p.small_slot : p.parent_slot;
+            slot_of[1] = sl ? p.parent_slot : p.small_slot;
+            bpair[0]   = p.parent_slot;
+            bpair[1]   = p.small_slot;
+            bpair[2]   = p.parent_slot;
+        }
+    }
+    for (uint32_t c = threadIdx.x; c < nchb; c += k_plan_thr)
+    {
+        uint32_t const b = c * crows;
+        bchunks[c]       = {0, sb + b, min(crows, sc - b), 0};
+    }
+}
+
+// The partitioned segment back into the row buffer.
+__global__ void leaf_copyback_kernel(LeafOut const *out, uint32_t const *__restrict__ tmp,
+                                     uint32_t *__restrict__ rows, uint32_t start, uint32_t count)
+{
+    if (out->split == 0)
+    {
+        return;
+    }
+    for (uint32_t k = (blockIdx.x * blockDim.x) + threadIdx.x; k < count;
+         k += gridDim.x * blockDim.x)
+    {
+        rows[start + k] = tmp[k];
+    }
+}
+
+// Larger child = parent - smaller, in place in the parent's slot (float
+// cells in float, finish_split; packed integers without borrow).
+template <bool Q>
+__global__ void leaf_sub_kernel(LeafOut const *out, uint32_t const *bpair, void *pool,
+                                uint32_t total_cells, uint32_t n_cells)
+{
+    if (out->split == 0)
+    {
+        return;
+    }
+    uint64_t const hp = static_cast<uint64_t>(bpair[0]) * total_cells;
+    uint64_t const hs = static_cast<uint64_t>(bpair[1]) * total_cells;
+    for (uint32_t x = (blockIdx.x * blockDim.x) + threadIdx.x; x < n_cells;
+         x += gridDim.x * blockDim.x)
+    {
+        if constexpr (Q)
+        {
+            auto *h = static_cast<unsigned long long *>(pool);
+            h[hp + x] -= h[hs + x];
+        }
+        else
+        {
+            auto        *h = static_cast<float2 *>(pool);
+            float2 const a = h[hp + x];
+            float2 const b = h[hs + x];
+            h[hp + x]      = make_float2(a.x - b.x, a.y - b.y);
+        }
+    }
+}
+
+// The children's totals from their cells (Histogram::totals) and their
+// monotone bounds (propagate_monotone_bounds, src/grower_impl.hpp:52-80).
+template <bool Q>
+__global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
+                                   uint32_t const *slot_of, void const *pool,
+                                   uint32_t total_cells, uint32_t const *sel,
+                                   uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
+                                   TreeParams tp, double2 const *qscale, LeafPop p)
+{
+    if (threadIdx.x != 0)
+    {
+        return;
+    }
+    if (out->split == 0)
+    {
+        ctl->n_cur = 0;
+        return;
+    }
+    Node L = next[0];
+    Node R = next[1];
+    double gl, hl, gr, hr;
+    if constexpr (Q)
+    {
+        auto const *h = static_cast<unsigned long long const *>(pool);
+        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells), sel_nb[0],
+                           L.qg, L.qh);
+        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells), sel_nb[0],
+                           R.qg, R.qh);
+        double2 const sc = *qscale;
+        gl = static_cast<double>(L.qg) * sc.x;
+        hl = static_cast<double>(L.qh) * sc.y;
+        gr = static_cast<double>(R.qg) * sc.x;
+        hr = static_cast<double>(R.qh) * sc.y;
+    }
+    else
+    {
+        auto const *h = static_cast<float2 const *>(pool);
+        totals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells), sel_nb[0],
+                          L.sum_g, L.sum_h);
+        totals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells), sel_nb[0],
+                          R.sum_g, R.sum_h);
+        gl = L.sum_g;
+        hl = L.sum_h;
+        gr = R.sum_g;
+        hr = R.sum_h;
+    }
+    uint32_t const f  = sel[p.best.feature];
+    int const      mc = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+    if (mc != 0)
+    {
+        double const wl  = bounded_leaf_weight(gl, hl, tp.lambda_l1, tp.lambda_l2, p.node.lo,
+                                               p.node.hi);
+        double const wr  = bounded_leaf_weight(gr, hr, tp.lambda_l1, tp.lambda_l2, p.node.lo,
+                                               p.node.hi);
+        double const mid = 0.5 * (wl + wr);
+        if (mc > 0)
+        {
+            L.hi = fmin(L.hi, mid);
+            R.lo = fmax(R.lo, mid);
+        }
+        else
+        {
+            L.lo = fmax(L.lo, mid);
+            R.hi = fmin(R.hi, mid);
+        }
+    }
+    next[0]    = L;
+    next[1]    = R;
+    ctl->n_cur = 2;
+}
+
+// Each node's best split over the features (the lowest feature wins a gain
+// tie), no split past the depth cap; the nodes and splits go to the host.
+__global__ void leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_sel,
+                                 Node const *nodes, LeafOut *out, uint32_t may_split)
+{
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t const lane = threadIdx.x & 31;
+    if (w >= 2)
+    {
+        return;
+    }
+    bool const live = w < ctl->n_cur;
+    double     g    = 0.0;
+    uint32_t   o    = 0xFFFFFFFFu;
+    for (uint32_t j = lane; live && may_split != 0 && j < n_sel; j += 32)
+    {
+        Best const c = cand[(w * n_sel) + j];
+        if (c.valid != 0 && (c.gain > g || (c.gain == g && j < o)))
+        {
+            g = c.gain;
+            o = j;
+        }
+    }
+    warp_best(g, o);
+    if (lane == 0)
+    {
+        out->best[w] = o == 0xFFFFFFFFu ? Best{0.0, 0, 0, 1, 0} : cand[(w * n_sel) + o];
+        if (live)
+        {
+            out->child[w] = nodes[w];
+        }
+    }
+}
+
 __global__ void tree_counter_kernel(uint32_t *tree_no)
 {
     *tree_no += 1;
@@ -2723,7 +3012,19 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     {
         throw ConfigError("grower: the feature selection is empty");
     }
-    if (cfg_.tp.max_depth > 8)
+    if (cfg_.leaf)
+    {
+        if (cfg_.tp.max_leaves == 0 && cfg_.tp.max_depth <= 9)
+        {
+            cfg_.tp.max_leaves = 1u << cfg_.tp.max_depth; // unbounded: the depth's cap
+        }
+        if (cfg_.tp.max_leaves < 1 || cfg_.tp.max_leaves > 512 || cfg_.tp.max_depth > 255)
+        {
+            throw ConfigError("grower: leafwise needs 1 <= max_leaves <= 512 and "
+                              "max_depth <= 255");
+        }
+    }
+    else if (cfg_.tp.max_depth > 8)
     {
         throw ConfigError("grower: max_depth above 8 exceeds the level plane's "
                           "512-node frontier; use a host grower");
@@ -2754,8 +3055,10 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     total_cells_ = off[n_sel_];
     off_h_       = off;
     cell_stride_ = ((max_nb_ + 1 + 3) / 4) * 4;
-    max_front_   = 1u << cfg_.tp.max_depth;
-    max_nodes_   = (2u << cfg_.tp.max_depth) - 1;
+    // leafwise: a pool slot per live leaf plus the one being built; a pop
+    // consumes a heap entry (at most 2 per split + the root), two nodes each
+    max_front_   = cfg_.leaf ? cfg_.tp.max_leaves + 1 : 1u << cfg_.tp.max_depth;
+    max_nodes_   = cfg_.leaf ? 4 * cfg_.tp.max_leaves : (2u << cfg_.tp.max_depth) - 1;
     max_rows_    = std::max<uint32_t>(max_root_rows, 1);
     crows_       = quant_ ? k_qbuild_rows : k_build_rows;
     max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
@@ -2773,7 +3076,8 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     nodes_[0] = dalloc<Node>(max_front_, s);
     nodes_[1] = dalloc<Node>(max_front_, s);
     hist_[0]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_, s);
-    hist_[1]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_, s);
+    // (leafwise uses the first buffer as its slot pool)
+    hist_[1]  = dalloc<float2>(static_cast<size_t>(cfg_.leaf ? 1 : max_front_) * total_cells_, s);
     cand_     = dalloc<Best>(static_cast<size_t>(max_front_) * n_sel_, s);
     best_     = dalloc<Best>(max_front_, s);
     pchunks_  = dalloc<Chunk>(max_pchunks_, s);
@@ -2790,6 +3094,12 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     rows_[1]  = dalloc<uint32_t>(max_rows_, s);
     pcr_      = dalloc<uint32_t>(max_front_ + 2, s);
     nbound_   = dalloc<double2>(std::max<uint32_t>(max_nodes_, k_walk_nodes), s);
+    if (cfg_.leaf)
+    {
+        lout_    = dalloc<LeafOut>(1, s);
+        slot_of_ = dalloc<uint32_t>(2, s);
+        BB_CHECK(cudaMallocHost(&lout_h_, sizeof(LeafOut)));
+    }
     nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
     dtree_    = dalloc<uint32_t>(1, s);
     BB_CHECK(cudaMemsetAsync(dtree_, 0, 4, s));
@@ -2921,7 +3231,16 @@ Grower::~Grower()
             cudaFreeAsync(p, stream_);
         }
     }
+    if (lout_ != nullptr)
+    {
+        cudaFreeAsync(lout_, stream_);
+        cudaFreeAsync(slot_of_, stream_);
+    }
     cudaStreamSynchronize(stream_);
+    if (lout_h_ != nullptr)
+    {
+        cudaFreeHost(lout_h_);
+    }
     cudaEventDestroy(pev_[0]);
     cudaEventDestroy(pev_[1]);
 }
@@ -3145,13 +3464,13 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     {
         find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr);
     }
     else
     {
         find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr);
     }
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
@@ -3285,6 +3604,21 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     gh_cur_        = gh;
     root_rows_     = root_rows;
     n_launch_      = 0;
+    if (cfg_.leaf)
+    {
+        if (next != nullptr || red_ != nullptr)
+        {
+            throw ConfigError("grower: the leafwise plane takes neither a fused next round "
+                              "nor row shards");
+        }
+        walk_ = false;
+        if (quant_)
+        {
+            quantise(gh, static_cast<uint32_t>(plane_.n_rows), false);
+        }
+        grow_leafwise(root_rows, n_root, t, leaf_id, scores, lr);
+        return;
+    }
     walk_          = identity_root && n_root == plane_.n_rows &&
             (leaf_id != nullptr || scores != nullptr || next != nullptr);
     if (next != nullptr && !walk_)
@@ -3432,6 +3766,283 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         phase_end(prof_->other_ms);
     }
     launches_ = n_launch_;
+    ++tree_no_;
+}
+
+namespace
+{
+
+// A leaf awaiting expansion (Candidate, src/step/primitives.hpp:440-450): its
+// node, its best split, its depth and the pool slot holding its histograms.
+struct HeapEntry
+{
+    Node     node;
+    Best     best;
+    uint32_t depth;
+    uint32_t slot;
+};
+
+__global__ void leaf_final_ctl_kernel(Ctl *ctl, uint32_t n_leaves, uint32_t n_nodes,
+                                      uint32_t depth)
+{
+    ctl->n_cur    = n_leaves;
+    ctl->n_nodes  = n_nodes;
+    ctl->depth    = depth;
+    ctl->n_leaves = 0;
+}
+
+} // namespace
+
+// LeafwiseGrower::grow with the host as the control plane: the same gain
+// heap (max gain, the lower node id on a tie), child ids allocated at the
+// pop, demotion when the partition empties a side (its two children stay as
+// zero leaf placeholders), no children's split at the depth cap, the leaf
+// budget; every pop's data plane on the device, one read-back per pop.
+void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut const &t,
+                           uint32_t *leaf_id, float *scores, float lr)
+{
+    cudaStream_t      s         = stream_;
+    TreeParams const &tp        = cfg_.tp;
+    size_t const      find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
+    auto             *lout      = static_cast<LeafOut *>(lout_);
+    auto             *lh        = static_cast<LeafOut *>(lout_h_);
+    void             *pool      = hist_[0];
+    BB_CHECK(cudaMemcpyAsync(rows_[0], root_rows, size_t{n_root} * 4, cudaMemcpyDeviceToDevice,
+                             s));
+    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
+                                              build_, t, crows_, n_root);
+    BB_LAUNCH("root_setup_kernel");
+    build(rows_[0], n_sel_, 0);
+    if (quant_)
+    {
+        qroot_totals_kernel<<<1, 32, 0, s>>>(
+            nodes_[0], static_cast<unsigned long long const *>(pool), sel_nb_);
+    }
+    else
+    {
+        root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(pool),
+                                            sel_nb_);
+    }
+    BB_LAUNCH("root_totals_kernel");
+    auto find = [&](Node const *nodes, uint32_t const *slot_of, bool may_split)
+    {
+        dim3 const fgrid(2, n_sel_);
+        if (quant_)
+        {
+            find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
+                ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
+                tp, cand_, max_nb_, qscale_, slot_of);
+        }
+        else
+        {
+            find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
+                ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
+                tp, cand_, max_nb_, qscale_, slot_of);
+        }
+        BB_LAUNCH("find_kernel");
+        leaf_best_kernel<<<1, 64, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split ? 1 : 0);
+        BB_LAUNCH("leaf_best_kernel");
+        BB_CHECK(cudaMemcpyAsync(lh, lout, sizeof(LeafOut), cudaMemcpyDeviceToHost, s));
+        BB_CHECK(cudaStreamSynchronize(s));
+    };
+    find(nodes_[0], nullptr, tp.max_depth > 0);
+
+    // the tree as the host assembles it (DenseTree nodes, gains, covers)
+    std::vector<uint32_t> feat{k_leaf_flag};
+    std::vector<uint32_t> left{0};
+    std::vector<uint32_t> right{0};
+    std::vector<uint32_t> sbin{0};
+    std::vector<float>    value{0.0F};
+    std::vector<float>    gain{0.0F};
+    std::vector<float>    cover{static_cast<float>(n_root)};
+    std::vector<uint8_t>  dl{0};
+    auto                  push_leaf = [&]
+    {
+        feat.push_back(k_leaf_flag);
+        left.push_back(0);
+        right.push_back(0);
+        sbin.push_back(0);
+        value.push_back(0.0F);
+        gain.push_back(0.0F);
+        cover.push_back(0.0F);
+        dl.push_back(0);
+    };
+    std::vector<uint32_t> free_slots;
+    for (uint32_t k = max_front_; k-- > 1;)
+    {
+        free_slots.push_back(k); // slot 0 holds the root
+    }
+    auto gain_less = [](HeapEntry const &a, HeapEntry const &b)
+    {
+        if (a.best.gain != b.best.gain)
+        {
+            return a.best.gain < b.best.gain;
+        }
+        return a.node.id > b.node.id;
+    };
+    std::vector<HeapEntry> heap;
+    std::vector<HeapEntry> pending;
+    std::vector<Node>      leaves; // demoted splits, as they happen
+    HeapEntry const        root{lh->child[0], lh->best[0], 0, 0};
+    if (root.best.valid != 0 && tp.max_depth > 0)
+    {
+        heap.push_back(root);
+    }
+    else
+    {
+        pending.push_back(root);
+    }
+    uint32_t live  = 1;
+    uint32_t depth = 0;
+    while (!heap.empty() && (tp.max_leaves == 0 || live < tp.max_leaves))
+    {
+        std::pop_heap(heap.begin(), heap.end(), gain_less);
+        HeapEntry const c = heap.back();
+        heap.pop_back();
+        // commit_split_node (src/grower_impl.hpp:189-206)
+        uint32_t const id  = c.node.id;
+        uint32_t const lid = static_cast<uint32_t>(feat.size());
+        uint32_t const rid = lid + 1;
+        if (rid >= max_nodes_)
+        {
+            throw ConfigError("grower: leafwise tree outgrew its node table");
+        }
+        push_leaf();
+        push_leaf();
+        uint32_t const f = sel_h_[c.best.feature];
+        feat[id]         = f;
+        value[id]        = plane_.h_cuts[plane_.h_cut_off[f] + c.best.bin];
+        left[id]         = lid;
+        right[id]        = rid;
+        dl[id]           = static_cast<uint8_t>(c.best.dl);
+        gain[id]         = static_cast<float>(c.best.gain);
+        sbin[id]         = c.best.bin;
+        if (free_slots.empty())
+        {
+            throw ConfigError("grower: leafwise histogram pool exhausted");
+        }
+        uint32_t const small = free_slots.back();
+        free_slots.pop_back();
+        LeafPop const p{c.node, c.best, lid, rid, c.slot, small};
+        leaf_setup_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], best_, pchunks_, pcr_, p);
+        BB_LAUNCH("leaf_setup_kernel");
+        if (plane_.u8)
+        {
+            pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
+                ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                sel_nb_, pleft_, dirs_);
+        }
+        else
+        {
+            pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
+                ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                sel_nb_, pleft_, dirs_);
+        }
+        BB_LAUNCH("pcount_kernel");
+        leaf_plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pchunks_, pleft_, prbase_, nleft_, dst_,
+                                                  build_, brange_, bbase_, bchunks_, bpair_,
+                                                  nodes_[0], nodes_[1], slot_of_, lout, crows_,
+                                                  p);
+        BB_LAUNCH("leaf_plan_kernel");
+        pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
+            ctl_, pchunks_, nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0], rows_[1],
+            dirs_, static_cast<unsigned long long *>(pool), build_, total_cells_,
+            quant_ ? total_cells_ : 0);
+        BB_LAUNCH("pscatter_kernel");
+        build(rows_[1], n_sel_, 0, true);
+        uint32_t const cgrid = std::max(1u, std::min(ceil_div(c.node.count, 256), 148u * 8u));
+        leaf_copyback_kernel<<<cgrid, 256, 0, s>>>(lout, rows_[1], rows_[0], c.node.start,
+                                                   c.node.count);
+        BB_LAUNCH("leaf_copyback_kernel");
+        uint32_t const sgrid = std::max(1u, std::min(ceil_div(total_cells_, 256), 148u * 8u));
+        if (quant_)
+        {
+            leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
+                                                        total_cells_);
+            leaf_totals_kernel<true><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
+                                                      total_cells_, sel_, sel_nb_, mono_, n_mono_,
+                                                      tp, qscale_, p);
+        }
+        else
+        {
+            leaf_sub_kernel<false><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
+                                                         total_cells_);
+            leaf_totals_kernel<false><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
+                                                       total_cells_, sel_, sel_nb_, mono_,
+                                                       n_mono_, tp, qscale_, p);
+        }
+        BB_LAUNCH("leaf_totals_kernel");
+        find(nodes_[1], slot_of_, c.depth + 1 < tp.max_depth);
+        if (lh->split == 0)
+        {
+            // commit_pop's demotion: the survivor holds the parent's rows and
+            // takes its id and bounds; the two children stay placeholders
+            gain[id] = 0.0F;
+            leaves.push_back(c.node);
+            free_slots.push_back(small);
+            free_slots.push_back(c.slot);
+            continue;
+        }
+        Node const     L  = lh->child[0];
+        Node const     R  = lh->child[1];
+        bool const     sl = lh->small_left != 0;
+        cover[lid]        = static_cast<float>(L.gcount);
+        cover[rid]        = static_cast<float>(R.gcount);
+        ++live;
+        depth = std::max(depth, c.depth + 1);
+        HeapEntry const kids[2] = {{L, lh->best[0], c.depth + 1, sl ? small : c.slot},
+                                   {R, lh->best[1], c.depth + 1, sl ? c.slot : small}};
+        for (HeapEntry const &k : kids)
+        {
+            // queue_children (src/grower_impl.hpp:405-425)
+            if (k.best.valid != 0)
+            {
+                heap.push_back(k);
+                std::push_heap(heap.begin(), heap.end(), gain_less);
+            }
+            else
+            {
+                pending.push_back(k);
+                free_slots.push_back(k.slot);
+            }
+        }
+    }
+    // the tree epilogue: every remaining candidate and pending node is a leaf
+    for (HeapEntry const &h : heap)
+    {
+        leaves.push_back(h.node);
+    }
+    for (HeapEntry const &h : pending)
+    {
+        leaves.push_back(h.node);
+    }
+    uint32_t const n_nodes = static_cast<uint32_t>(feat.size());
+    BB_CHECK(cudaMemcpyAsync(t.feature, feat.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.value, value.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.left, left.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.right, right.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.default_left, dl.data(), n_nodes, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.gain, gain.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.cover, cover.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(t.split_bin, sbin.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(nodes_[0], leaves.data(), leaves.size() * sizeof(Node),
+                             cudaMemcpyHostToDevice, s));
+    leaf_final_ctl_kernel<<<1, 1, 0, s>>>(ctl_, static_cast<uint32_t>(leaves.size()), n_nodes,
+                                          depth);
+    BB_LAUNCH("leaf_final_ctl_kernel");
+    // write_leaf for every leaf, then (quantised) the FP64 renewal, then the
+    // rows' leaf ids and score updates from the leaves' segments
+    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], tp, t, pchunks_, pcr_, nbound_);
+    BB_LAUNCH("final_kernel");
+    nodes_cur_ = nodes_[0];
+    rows_cur_  = rows_[0];
+    leaf_values(t, true);
+    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[0], rows_[0], t,
+                                                    leaf_id, scores, lr);
+    BB_LAUNCH("stamp_kernel");
+    tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
+    BB_LAUNCH("tree_counter_kernel");
+    BB_CHECK(cudaStreamSynchronize(s)); // the host tables above are read until here
     ++tree_no_;
 }
 

@@ -136,6 +136,10 @@ struct GrowConfig
     // level over the whole frontier, broadcast to every node; trees are
     // perfect to their depth, empty children included
     bool       level = false;
+    // leafwise (LeafwiseGrower, src/grower_impl.hpp:744-850): best-first, one
+    // node per heap pop, at most tp.max_leaves leaves (<= 512), tp.max_depth
+    // caps the depth (<= 255)
+    bool       leaf  = false;
 };
 
 // All device buffers one tree's growth needs, sized once for a dataset and
@@ -201,6 +205,9 @@ class Grower
   private:
     void level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
                TreeOut const &out, uint32_t *leaf_id, float *scores, float lr);
+    void grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut const &out,
+                       uint32_t *leaf_id, float *scores, float lr);
+    void find_nodes(void const *hist, uint32_t n_nodes, uint32_t const *slot_of);
     // zeroed: the quantised slots were already cleared (by the partition)
     void build(uint32_t const *rows, uint32_t n_feat_build, int dst, bool zeroed = false);
 
@@ -260,6 +267,10 @@ class Grower
     unsigned long long *wacc_ = nullptr; // per tree node: fixed-point (G, H) of the walk
     uint16_t *leaf16_   = nullptr; // per row: its leaf, from the walk
     double2  *nbound_   = nullptr; // per tree node: monotone bounds (lo, hi)
+    // leafwise
+    void     *lout_     = nullptr; // the pop's results (device)
+    void     *lout_h_   = nullptr; // ... read back (pinned host)
+    uint32_t *slot_of_  = nullptr; // the children's pool slots
     uint32_t  crows_    = 0;       // rows per histogram-build chunk
     bool      quant_    = false;
     uint32_t *dtree_    = nullptr; // device tree counter (the rounding stream)
@@ -290,6 +301,12 @@ class Grower
     void set_profile(Profile *p)
     {
         prof_ = p;
+    }
+    // whether grow() can take a fused next round (and be graph-captured):
+    // not on the leafwise plane, whose host reads each pop back
+    bool fuses_next() const
+    {
+        return !cfg_.leaf;
     }
     // kernel launches one grow() enqueues
     uint32_t launches_per_tree() const

@@ -103,7 +103,12 @@ typedef struct
     int32_t        record_leaf_ids; /* keep each row's leaf id of the last tree */
     int32_t        grower;     /* 0 depthwise (DepthwiseGrower), 1 levelwise
                                   (ObliviousGrower: one split per level over the
-                                  whole frontier, src/grower_impl.hpp:579-720) */
+                                  whole frontier, src/grower_impl.hpp:579-720),
+                                  2 leafwise (LeafwiseGrower: best-first, one
+                                  node per heap pop, :744-850; the host keeps the
+                                  heap, so its rounds are not graph-captured) */
+    uint32_t       max_leaves; /* leafwise: 1..512 (0: 2^max_depth, depth <= 9);
+                                  max_depth <= 255 caps its depth */
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
@@ -169,13 +174,21 @@ int bb_booster_profile_round(bb_booster *b, bb_profile *out);
 
 void bb_booster_destroy(bb_booster *b);
 
+/* Node-table entries one tree of this configuration may need: 2^(max_depth+1)
+ * - 1 for the depthwise and levelwise growers, 4 x max_leaves for leafwise
+ * (each heap pop allocates two nodes, demoted ones included). */
+uint32_t bb_tree_capacity(bb_train_cfg const *cfg);
+
 /* One tree from caller-provided gradients: grad/hess (host, n_rows), the
  * sampled rows (host, ascending, n_sel_rows of them; NULL = all). Returns
- * the tree and every sampled row's leaf value and node id (values/leaf_ids
- * host, n_rows; entries of unsampled rows are left untouched).
+ * the tree (node arrays of bb_tree_capacity(cfg) entries) and every sampled
+ * row's leaf value and node id (values/leaf_ids host, n_rows; entries of
+ * unsampled rows are left untouched).
  * Replaces one DepthwiseGrower<CudaHistogramEngine>::grow call
  * (src/grower_impl.hpp:465-577) over the engine's level plane
- * (begin_tree .. finalize_tree, histogram_engine.hpp:94-170). */
+ * (begin_tree .. finalize_tree, histogram_engine.hpp:94-170), or with
+ * cfg->grower an ObliviousGrower / LeafwiseGrower one (the latter over the
+ * leaf plane, LeafStep<GPULeafEngine>, src/step/leaf.hpp:124-269). */
 int bb_grow_tree(bb_plane const *plane, bb_train_cfg const *cfg, float const *grad,
                  float const *hess, uint32_t const *rows, uint64_t n_sel_rows,
                  uint32_t *feature, float *value, uint32_t *left, uint32_t *right,
