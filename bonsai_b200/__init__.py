@@ -26,13 +26,13 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "pred_contribs", "oblivious_tables", "fit_cuts",
+    "grow_tree", "populate", "predict", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
     "Comm", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
 LEAF = 0xFFFFFFFF
-OBJECTIVES = {"mse": 0, "logloss": 1}
+OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2}
 GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1, "leafwise": 2}
 HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
 
@@ -61,6 +61,7 @@ class TrainParams:
     record_leaf_ids: bool = False
     grower: str = "depthwise"
     max_leaves: int = 31
+    n_classes: int = 0
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -76,6 +77,7 @@ class TrainParams:
         c.seed = self.seed
         c.grower = GROWERS[self.grower]
         c.max_leaves = self.max_leaves
+        c.n_classes = self.n_classes
         c.use_graph = 1 if self.use_graph else 0
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:
@@ -334,8 +336,21 @@ class Booster:
     def trees(self) -> list:
         return [self.tree(t) for t in range(self.n_trees)]
 
+    @property
+    def n_classes(self) -> int:
+        return int(lib().bb_booster_n_classes(self.h))
+
+    @property
+    def init_scores(self) -> np.ndarray:
+        """One init score per class (softmax), else the one."""
+        out = np.empty(max(1, self.n_classes), np.float32)
+        check(lib().bb_booster_init_scores(self.h, ptr(out)))
+        return out
+
     def scores(self) -> np.ndarray:
-        out = np.empty(self.plane.n_rows, np.float32)
+        """Training scores: n_rows, or n_rows x n_classes (softmax)."""
+        K = self.n_classes
+        out = np.empty((self.plane.n_rows, K) if K > 1 else self.plane.n_rows, np.float32)
         check(lib().bb_booster_scores(self.h, ptr(out)))
         return out
 
@@ -416,6 +431,14 @@ def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
                            ptr(cat["split_bin"]), ptr(cat["left"]), ptr(cat["right"]),
                            ptr(cat["default_left"]), ptr(cat["value"]), lr, init, ptr(out)))
     return out
+
+
+def predict_classes(plane: Plane, trees: list, init_scores, lr: float) -> np.ndarray:
+    """Raw per-class scores (n_rows x K) of a softmax ensemble whose trees are
+    round-major (tree r * K + k is class k's): each class through predict."""
+    K = len(init_scores)
+    return np.stack([predict(plane, trees[k::K], float(init_scores[k]), lr)
+                     for k in range(K)], axis=1)
 
 
 def pred_contribs(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:

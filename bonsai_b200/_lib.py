@@ -37,7 +37,7 @@ class TrainCfg(C.Structure):
         ("monotone", C.POINTER(C.c_int8)), ("n_monotone", C.c_uint32),
         ("selected", C.POINTER(C.c_uint32)), ("n_selected", C.c_uint32),
         ("use_graph", C.c_int32), ("record_leaf_ids", C.c_int32),
-        ("grower", C.c_int32), ("max_leaves", C.c_uint32),
+        ("grower", C.c_int32), ("max_leaves", C.c_uint32), ("n_classes", C.c_uint32),
     ]
 
 
@@ -90,6 +90,9 @@ def lib() -> C.CDLL:
             C.c_float, C.c_float, vp]
         L.bb_pred_contribs.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 7 + [
             C.c_float, C.c_float, vp]
+        L.bb_booster_n_classes.argtypes = [vp]
+        L.bb_booster_n_classes.restype = C.c_uint32
+        L.bb_booster_init_scores.argtypes = [vp, vp]
         L.bb_tree_capacity.argtypes = [C.POINTER(TrainCfg)]
         L.bb_tree_capacity.restype = C.c_uint32
         L.bb_comm_unique_id.argtypes = [vp]

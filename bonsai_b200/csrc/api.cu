@@ -89,6 +89,45 @@ __global__ void gradient_kernel(int objective, float const *__restrict__ scores,
     gh[i] = objective_gradient(objective, scores[i], labels[i]);
 }
 
+// Softmax gradients for K classes (MulticlassBooster::update_one_iter,
+// include/bonsai/multiclass_booster.hpp:105-140, row_softmax_exp :525-541):
+// per row the double max of its class scores, e_k = exp(s_k - max) in
+// double, summed in class order; p_k = float(e_k) / float(sum); g = p - 1[y
+// == k], h = max(p (1 - p), 1e-6). Scores and pairs are class-major (k * n + i).
+constexpr uint32_t k_max_classes = 16;
+
+__global__ void softmax_gradient_kernel(float const *__restrict__ scores,
+                                        float const *__restrict__ labels,
+                                        float2 *__restrict__ gh, uint64_t n, uint32_t K)
+{
+    uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
+    if (i >= n)
+    {
+        return;
+    }
+    double maxv = scores[i];
+    for (uint32_t k = 1; k < K; ++k)
+    {
+        maxv = fmax(maxv, static_cast<double>(scores[(k * n) + i]));
+    }
+    double e[k_max_classes];
+    double sum = 0.0;
+    for (uint32_t k = 0; k < K; ++k)
+    {
+        e[k] = exp(static_cast<double>(scores[(k * n) + i]) - maxv);
+        sum += e[k];
+    }
+    long const    lab = lround(labels[i]);
+    uint32_t const c  = lab >= 0 && static_cast<uint64_t>(lab) < K ? static_cast<uint32_t>(lab) : 0;
+    float const   fs  = static_cast<float>(sum);
+    for (uint32_t k = 0; k < K; ++k)
+    {
+        float const p = static_cast<float>(e[k]) / fs;
+        float const y = c == k ? 1.0F : 0.0F;
+        gh[(k * n) + i] = make_float2(p - y, fmaxf(p * (1.0F - p), 1e-6F));
+    }
+}
+
 __global__ void iota_kernel(uint32_t *rows, uint64_t n)
 {
     uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
@@ -321,6 +360,8 @@ struct bb_booster
     uint32_t                    n_trees = 0;
     bool                        use_graph = false;
     bool                        record_leaf_ids = false;
+    uint32_t                    n_classes = 1;  // softmax: K score and gradient columns
+    std::vector<float>          init_k;         // softmax: per-class log priors
     cudaGraphExec_t             graph     = nullptr;
     cudaEvent_t                 ev0{}, ev1{};
     float                       last_ms = 0.0F;
@@ -330,6 +371,23 @@ struct bb_booster
     void round_body()
     {
         uint64_t const n = plane->n_rows;
+        if (objective == 2)
+        {
+            // one round: the softmax pairs of the round's scores, then one
+            // tree per class, each adding lr x leaf to its class's scores
+            softmax_gradient_kernel<<<blocks(n), 256, 0, stream>>>(scores, labels, gh, n,
+                                                                    n_classes);
+            BB_LAUNCH("softmax_gradient_kernel");
+            for (uint32_t k = 0; k < n_classes; ++k)
+            {
+                grower->grow(gh + (k * n), rows, static_cast<uint32_t>(n), scratch.t,
+                             record_leaf_ids ? leaf_id : nullptr, scores + (k * n), lr, true,
+                             nullptr);
+                commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
+                BB_LAUNCH("commit_tree_kernel");
+            }
+            return;
+        }
         if (!grower->fuses_next())
         {
             // the leafwise plane stamps from its leaves' segments: gradients
@@ -362,7 +420,11 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
 {
     need(plane != nullptr && labels != nullptr && cfg != nullptr,
          "bb_booster_create: null argument");
-    need(cfg->objective == 0 || cfg->objective == 1, "objective must be 0 (mse) or 1 (logloss)");
+    need(cfg->objective >= 0 && cfg->objective <= 2,
+         "objective must be 0 (mse), 1 (logloss) or 2 (softmax)");
+    need(cfg->objective != 2 || (cfg->n_classes >= 2 && cfg->n_classes <= k_max_classes),
+         "softmax needs 2 <= n_classes <= 16");
+    need(cfg->objective != 2 || red == nullptr, "softmax fits do not shard");
     need(max_trees > 0, "max_trees must be positive");
     auto           b = std::make_unique<bb_booster>();
     Plane const   &p = plane->p;
@@ -371,7 +433,25 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     b->objective     = cfg->objective;
     b->lr            = cfg->learning_rate;
     BB_CHECK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    if (init_score != nullptr)
+    uint32_t const K = cfg->objective == 2 ? cfg->n_classes : 1;
+    b->n_classes     = K;
+    if (cfg->objective == 2)
+    {
+        // log class priors (multiclass_booster.hpp:60-77)
+        std::vector<double> counts(K, 0.0);
+        for (uint64_t i = 0; i < n; ++i)
+        {
+            long const c = std::lround(labels[i]);
+            counts[c >= 0 && static_cast<uint64_t>(c) < K ? c : 0] += 1.0;
+        }
+        for (uint32_t k = 0; k < K; ++k)
+        {
+            b->init_k.push_back(static_cast<float>(
+                std::log(std::max(counts[k], 1.0) / static_cast<double>(n))));
+        }
+        b->init = b->init_k[0];
+    }
+    else if (init_score != nullptr)
     {
         b->init = *init_score;
     }
@@ -387,8 +467,8 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
         b->init = cfg->objective == 0 ? sum / nn : std::log((sum / nn) / (1.0F - (sum / nn)));
     }
     b->labels  = dmalloc<float>(n);
-    b->scores  = dmalloc<float>(n);
-    b->gh      = dmalloc<float2>(n);
+    b->scores  = dmalloc<float>(n * K);
+    b->gh      = dmalloc<float2>(n * K);
     b->rows    = dmalloc<uint32_t>(n);
     b->leaf_id = dmalloc<uint32_t>(n);
     b->round   = dmalloc<uint32_t>(1);
@@ -400,8 +480,12 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     }
     else
     {
-        fill_kernel<<<blocks(n), 256, 0, b->stream>>>(b->scores, b->init, n);
-        BB_LAUNCH("fill_kernel");
+        for (uint32_t k = 0; k < K; ++k)
+        {
+            fill_kernel<<<blocks(n), 256, 0, b->stream>>>(b->scores + (k * n),
+                                                          K > 1 ? b->init_k[k] : b->init, n);
+            BB_LAUNCH("fill_kernel");
+        }
     }
     iota_kernel<<<blocks(n), 256, 0, b->stream>>>(b->rows, n);
     BB_LAUNCH("iota_kernel");
@@ -415,14 +499,17 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
         b->grower->set_shard(red, row_offset, total_rows);
     }
     b->scratch.alloc(b->grower->max_nodes(), 1);
-    b->trees.alloc(b->grower->max_nodes(), max_trees);
+    b->trees.alloc(b->grower->max_nodes(), max_trees * K); // round-major: r * K + k
     // a leafwise round reads every pop back to the host: it runs eagerly
     b->use_graph       = cfg->use_graph != 0 && b->grower->fuses_next();
     b->record_leaf_ids = cfg->record_leaf_ids != 0;
-    gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores, b->labels, b->gh,
-                                                      n);
-    BB_LAUNCH("gradient_kernel");
-    b->grower->seed_absmax(b->gh);
+    if (K == 1)
+    {
+        gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores, b->labels,
+                                                          b->gh, n);
+        BB_LAUNCH("gradient_kernel");
+        b->grower->seed_absmax(b->gh);
+    }
     BB_CHECK(cudaEventCreate(&b->ev0));
     BB_CHECK(cudaEventCreate(&b->ev1));
     BB_CHECK(cudaStreamSynchronize(b->stream));
@@ -707,7 +794,8 @@ extern "C"
         return guarded(
             [&]
             {
-                need(b->n_trees + n_iters <= b->trees.n, "bb_booster_update: tree capacity");
+                need(b->n_trees + (n_iters * b->n_classes) <= b->trees.n,
+                     "bb_booster_update: tree capacity");
                 if (b->use_graph && b->graph == nullptr)
                 {
                     cudaGraph_t g;
@@ -738,7 +826,7 @@ extern "C"
                     }
                 }
                 BB_CHECK(cudaEventRecord(b->ev1, b->stream));
-                b->n_trees += n_iters;
+                b->n_trees += n_iters * b->n_classes;
             });
     }
 
@@ -794,7 +882,43 @@ extern "C"
             [&]
             {
                 BB_CHECK(cudaStreamSynchronize(b->stream));
-                BB_CHECK(cudaMemcpy(out, b->scores, b->plane->n_rows * 4, cudaMemcpyDeviceToHost));
+                uint64_t const n = b->plane->n_rows;
+                uint32_t const K = b->n_classes;
+                if (K == 1)
+                {
+                    BB_CHECK(cudaMemcpy(out, b->scores, n * 4, cudaMemcpyDeviceToHost));
+                    return;
+                }
+                // class-major on the device, row-major (n x K) for the caller
+                std::vector<float> cm(n * K);
+                BB_CHECK(cudaMemcpy(cm.data(), b->scores, n * K * 4, cudaMemcpyDeviceToHost));
+                for (uint64_t i = 0; i < n; ++i)
+                {
+                    for (uint32_t k = 0; k < K; ++k)
+                    {
+                        out[(i * K) + k] = cm[(k * n) + i];
+                    }
+                }
+            });
+    }
+
+    uint32_t bb_booster_n_classes(bb_booster const *b)
+    {
+        return b->n_classes;
+    }
+
+    int bb_booster_init_scores(bb_booster const *b, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                need(out != nullptr, "bb_booster_init_scores: null argument");
+                if (b->n_classes == 1)
+                {
+                    out[0] = b->init;
+                    return;
+                }
+                std::copy(b->init_k.begin(), b->init_k.end(), out);
             });
     }
 
@@ -814,7 +938,8 @@ extern "C"
         return guarded(
             [&]
             {
-                need(b->n_trees + 1 <= b->trees.n, "bb_booster_profile_round: tree capacity");
+                need(b->n_trees + b->n_classes <= b->trees.n,
+                     "bb_booster_profile_round: tree capacity");
                 BB_CHECK(cudaStreamSynchronize(b->stream));
                 Profile p;
                 b->grower->set_profile(&p);

@@ -85,7 +85,8 @@ void bb_plane_destroy(bb_plane *plane);
  * (include/bonsai/config/tree_config.hpp:9-29, booster_config.hpp:8-24). */
 typedef struct
 {
-    int32_t        objective;  /* 0 mse, 1 logloss */
+    int32_t        objective;  /* 0 mse, 1 logloss, 2 softmax (MulticlassBooster:
+                                  n_classes trees per round, round-major) */
     float          learning_rate;
     float          min_child_hess;
     float          min_gain_to_split;
@@ -109,6 +110,7 @@ typedef struct
                                   heap, so its rounds are not graph-captured) */
     uint32_t       max_leaves; /* leafwise: 1..512 (0: 2^max_depth, depth <= 9);
                                   max_depth <= 255 caps its depth */
+    uint32_t       n_classes;  /* objective 2 (softmax): 2..16 */
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
@@ -171,6 +173,14 @@ typedef struct
 } bb_profile;
 
 int bb_booster_profile_round(bb_booster *b, bb_profile *out);
+
+/* Softmax: the class count (1 otherwise) and the per-class log-prior init
+ * scores (out holds n_classes floats; the one init score otherwise).
+ * bb_booster_scores then writes n_rows x n_classes, row-major, and tree t of
+ * bb_booster_tree is round t / n_classes, class t % n_classes
+ * (include/bonsai/multiclass_booster.hpp:28-33). */
+uint32_t bb_booster_n_classes(bb_booster const *b);
+int      bb_booster_init_scores(bb_booster const *b, float *out);
 
 void bb_booster_destroy(bb_booster *b);
 

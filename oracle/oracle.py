@@ -287,6 +287,14 @@ class RefModel:
             raise RuntimeError(self.lib.err())
         return out
 
+    def init_scores(self):
+        out = np.zeros(64, np.float32)
+        L = self.lib.L
+        L.ref_model_init_scores.restype = C.c_size_t
+        L.ref_model_init_scores.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        n = L.ref_model_init_scores(C.c_void_p(self.h), out.ctypes.data, 64)
+        return out[:n].copy()
+
     def contribs_binned(self, ds):
         out = np.empty((ds.n, ds.F + 1), np.float64)
         if self.lib.L.ref_model_contribs_binned(C.c_void_p(self.h), C.c_void_p(ds.h),

@@ -280,6 +280,16 @@ namespace
             m.init_scores = {b->init_score()};
         }
     }
+
+    // MulticlassBooster keeps one log-prior per class.
+    template <typename G> void read_init_multi(RefModel &m, void const *raw)
+    {
+        if (auto const *b = dynamic_cast<MulticlassBooster<G, AllRowsSampler> const *>(
+                static_cast<IBooster const *>(raw)))
+        {
+            m.init_scores = b->init_scores();
+        }
+    }
 } // namespace
 
 
@@ -468,6 +478,9 @@ extern "C"
                                                     BernoulliSampler> const *>(raw));
                 read_init(*mm, dynamic_cast<Booster<MSEObjective, LeafwiseGrower<>,
                                                     BernoulliSampler> const *>(raw));
+                read_init_multi<DepthwiseGrower<>>(*mm, raw);
+                read_init_multi<ObliviousGrower<>>(*mm, raw);
+                read_init_multi<LeafwiseGrower<>>(*mm, raw);
                 m = mm.release();
             });
         return rc == 0 ? m : nullptr;
@@ -487,6 +500,15 @@ extern "C"
     {
         auto const *m = static_cast<RefModel const *>(mp);
         return m->init_scores.empty() ? 0.0F : m->init_scores[0];
+    }
+
+    // Every init score (one per class for softmax); returns how many.
+    size_t ref_model_init_scores(void const *mp, float *out, size_t cap)
+    {
+        auto const  *m = static_cast<RefModel const *>(mp);
+        size_t const n = std::min(cap, m->init_scores.size());
+        std::memcpy(out, m->init_scores.data(), n * 4);
+        return m->init_scores.size();
     }
 
     size_t ref_model_tree_size(void const *mp, size_t t)
