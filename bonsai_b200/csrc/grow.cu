@@ -2220,7 +2220,8 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 // per-lane selector. Slots of unselected features accumulate into columns
 // that are never flushed.
 //
-// Persistent: a grid of k_qctas CTAs per tile (one per SM), each walking a
+// Persistent: a grid of up to k_qctas CTAs per tile (one per SM; fewer for a
+// small dataset, so several fits share the GPU), each walking a
 // contiguous range of the level's chunks (node-ordered), so no wave tail.
 // The gathers are software-pipelined: while a chunk's rows are added, every
 // thread's cp.async copies of the next chunk's 32-byte tiles are in flight
@@ -3061,6 +3062,9 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     max_nodes_   = cfg_.leaf ? 4 * cfg_.tp.max_leaves : (2u << cfg_.tp.max_depth) - 1;
     max_rows_    = std::max<uint32_t>(max_root_rows, 1);
     crows_       = quant_ ? k_qbuild_rows : k_build_rows;
+    // the histogram grid: one CTA per SM for a large fit, about one per four
+    // 2,048-row chunks of the root for a small one
+    qctas_       = std::max(1u, std::min(k_qctas, ceil_div(max_rows_, 4 * k_qbuild_rows)));
     max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
     max_bchunks_ = ceil_div(max_rows_, crows_) + max_front_;
 
@@ -3346,7 +3350,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         if (plane_.u8)
         {
             size_t const tsmem = k_tsmem;
-            qhist_t_kernel<<<dim3(k_qctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
+            qhist_t_kernel<<<dim3(qctas_, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);

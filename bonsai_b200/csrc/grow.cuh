@@ -225,6 +225,7 @@ class Grower
     uint32_t              max_bchunks_ = 0;
     uint32_t              cell_stride_ = 0; // per-(chunk, feature) count stride
     uint32_t              lgroup_      = 1; // nodes per level-finder group
+    uint32_t              qctas_       = 1; // u8 quantised histogram CTAs per tile
 
     // device
     uint32_t *sel_      = nullptr; // selected feature ids
