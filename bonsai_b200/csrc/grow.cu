@@ -469,6 +469,26 @@ __global__ void __launch_bounds__(32)
     }
 }
 
+// A quantised cell: with cw == 1 (int8 codes) one packed word -- the int32
+// gradient sum in the high half (two's complement), the uint32 hessian sum in
+// the low half; with cw == 2 (int16 codes, whose sums outgrow 32 bits) two
+// words, the int64 gradient sum then the uint64 hessian sum. x counts cells.
+__device__ __forceinline__ void qcell(unsigned long long const *h, uint64_t x, uint32_t cw,
+                                      int64_t &g, int64_t &hs)
+{
+    if (cw == 2)
+    {
+        g  = static_cast<int64_t>(h[2 * x]);
+        hs = static_cast<int64_t>(h[(2 * x) + 1]);
+    }
+    else
+    {
+        unsigned long long const c = h[x];
+        g  = static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
+        hs = static_cast<uint32_t>(c);
+    }
+}
+
 // ------------------------------------------------------------ split find ----
 
 // The per-candidate core of update_best_for_feature_for_node
@@ -534,7 +554,7 @@ __global__ void __launch_bounds__(k_find_thr)
                 uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                 uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
                 TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale,
-                uint32_t const *slot_of)
+                uint32_t const *slot_of, uint32_t cw)
 {
     extern __shared__ unsigned char smem_raw[];
     __shared__ double   bg_s[k_find_thr / 32];
@@ -568,8 +588,8 @@ __global__ void __launch_bounds__(k_find_thr)
     // is its frontier index unless slot_of names it (the leafwise pool)
     uint32_t const slot = slot_of != nullptr ? slot_of[i] : i;
     auto const *src = static_cast<unsigned long long const *>(hist_v) +
-                      (static_cast<uint64_t>(slot) * total_cells) + cell_off[j];
-    for (uint32_t b = tid; b < nb; b += k_find_thr)
+                      (((static_cast<uint64_t>(slot) * total_cells) + cell_off[j]) * cw);
+    for (uint32_t b = tid; b < nb * cw; b += k_find_thr)
     {
         raw[b] = src[b];
     }
@@ -593,9 +613,10 @@ __global__ void __launch_bounds__(k_find_thr)
         int64_t        th  = 0;
         for (uint32_t b = b0; b < b1; ++b)
         {
-            unsigned long long const c = raw[b];
-            tg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-            th += static_cast<uint32_t>(c);
+            int64_t cg, ch;
+            qcell(raw, b, cw, cg, ch);
+            tg += cg;
+            th += ch;
         }
         int64_t eg = tg;
         int64_t eh = th;
@@ -625,15 +646,15 @@ __global__ void __launch_bounds__(k_find_thr)
         }
         for (uint32_t b = b0; b < b1; ++b)
         {
-            unsigned long long const c = raw[b];
-            pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-            ph += static_cast<uint32_t>(c);
+            int64_t cg, ch;
+            qcell(raw, b, cw, cg, ch);
+            pg += cg;
+            ph += ch;
             pref[b] = make_double2(static_cast<double>(pg) * sc.x,
                                    static_cast<double>(ph) * sc.y);
         }
-        unsigned long long const mc_ = raw[nb - 1];
-        int64_t const mqg = static_cast<int32_t>(static_cast<uint32_t>(mc_ >> 32));
-        int64_t const mqh = static_cast<uint32_t>(mc_);
+        int64_t mqg, mqh;
+        qcell(raw, nb - 1, cw, mqg, mqh);
         mg         = static_cast<double>(mqg) * sc.x;
         mh         = static_cast<double>(mqh) * sc.y;
         node_sc    = split_score(static_cast<double>(nd.qg) * sc.x,
@@ -764,7 +785,7 @@ __global__ void __launch_bounds__(k_lfind_thr)
     level_find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
                       uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                       uint32_t n_sel, TreeParams tp, Best *cand, uint32_t max_nb,
-                      uint32_t group, double2 const *qscale)
+                      uint32_t group, double2 const *qscale, uint32_t cw)
 {
     extern __shared__ unsigned char smem_raw[];
     __shared__ LevelNode ln_s[k_lfind_thr / 32];
@@ -805,7 +826,7 @@ __global__ void __launch_bounds__(k_lfind_thr)
             Node const     nd  = nodes[p];
             double2       *pr  = pref + (static_cast<uint64_t>(w) * max_nb);
             auto const    *src = static_cast<unsigned long long const *>(hist_v) +
-                              (static_cast<uint64_t>(p) * total_cells) + cell_off[j];
+                              (((static_cast<uint64_t>(p) * total_cells) + cell_off[j]) * cw);
             if constexpr (Q)
             {
                 uint32_t const run = (n_cut + 31) / 32;
@@ -815,9 +836,10 @@ __global__ void __launch_bounds__(k_lfind_thr)
                 int64_t        th  = 0;
                 for (uint32_t b = b0; b < b1; ++b)
                 {
-                    unsigned long long const c = src[b];
-                    tg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-                    th += static_cast<uint32_t>(c);
+                    int64_t cg, ch;
+                    qcell(src, b, cw, cg, ch);
+                    tg += cg;
+                    th += ch;
                 }
                 int64_t eg = tg;
                 int64_t eh = th;
@@ -836,17 +858,17 @@ __global__ void __launch_bounds__(k_lfind_thr)
                 int64_t ph = eh - th;
                 for (uint32_t b = b0; b < b1; ++b)
                 {
-                    unsigned long long const c = src[b];
-                    pg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-                    ph += static_cast<uint32_t>(c);
+                    int64_t cg, ch;
+                    qcell(src, b, cw, cg, ch);
+                    pg += cg;
+                    ph += ch;
                     pr[b] = make_double2(static_cast<double>(pg) * sc.x,
                                          static_cast<double>(ph) * sc.y);
                 }
                 if (lane == 0)
                 {
-                    unsigned long long const mc_ = src[nb - 1];
-                    int64_t const mqg = static_cast<int32_t>(static_cast<uint32_t>(mc_ >> 32));
-                    int64_t const mqh = static_cast<uint32_t>(mc_);
+                    int64_t mqg, mqh;
+                    qcell(src, nb - 1, cw, mqg, mqh);
                     LevelNode     l;
                     l.score  = split_score(static_cast<double>(nd.qg) * sc.x,
                                            static_cast<double>(nd.qh) * sc.y, tp.lambda_l1,
@@ -2040,16 +2062,21 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+// W16: int16 codes (scales max / 32767, g in the low half of a 32-bit word,
+// h in the high half) instead of int8 (max / 127, a 16-bit word).
+template <bool W16>
 __global__ void __launch_bounds__(k_threads)
     quantise_kernel(float2 const *__restrict__ gh, uint32_t n,
                     uint32_t const *__restrict__ absmax, uint2 key,
-                    uint32_t const *__restrict__ tree_no, uint16_t *__restrict__ q,
+                    uint32_t const *__restrict__ tree_no, void *__restrict__ qout,
                     double2 *__restrict__ scale, uint64_t row_off)
 {
+    constexpr double qmax = W16 ? 32767.0 : 127.0;
+    constexpr int    imax = W16 ? 32767 : 127;
     double const mg = __uint_as_float(absmax[0]);
     double const mh = __uint_as_float(absmax[1]);
-    double const sg = mg > 0.0 ? mg / 127.0 : 1.0;
-    double const sh = mh > 0.0 ? mh / 127.0 : 1.0;
+    double const sg = mg > 0.0 ? mg / qmax : 1.0;
+    double const sh = mh > 0.0 ? mh / qmax : 1.0;
     double const ig = 1.0 / sg; // one division per thread, a multiply per row
     double const ih = 1.0 / sh;
     uint32_t const t = *tree_no;
@@ -2072,10 +2099,19 @@ __global__ void __launch_bounds__(k_threads)
         double const xh = static_cast<double>(fmaxf(v.y, 0.0F)) * ih;
         int          qg = isnan(xg) ? 0 : static_cast<int>(floor(xg + ug));
         int          qh = isnan(xh) ? 0 : static_cast<int>(floor(xh + uh));
-        qg              = max(-127, min(127, qg));
-        qh              = max(0, min(127, qh));
-        q[i] = static_cast<uint16_t>(static_cast<uint8_t>(static_cast<int8_t>(qg)) |
-                                     (static_cast<uint32_t>(qh) << 8));
+        qg              = max(-imax, min(imax, qg));
+        qh              = max(0, min(imax, qh));
+        if constexpr (W16)
+        {
+            static_cast<uint32_t *>(qout)[i] =
+                static_cast<uint32_t>(static_cast<uint16_t>(static_cast<int16_t>(qg))) |
+                (static_cast<uint32_t>(qh) << 16);
+        }
+        else
+        {
+            static_cast<uint16_t *>(qout)[i] = static_cast<uint16_t>(
+                static_cast<uint8_t>(static_cast<int8_t>(qg)) | (static_cast<uint32_t>(qh) << 8));
+        }
     }
 }
 
@@ -2103,11 +2139,14 @@ __global__ void __launch_bounds__(k_threads)
 // at most 32,768 rows of |q| <= 127 -- then one packed 64-bit global add per
 // touched cell (gradient in the high word, two's complement; hessian in the
 // low word). grid (chunks, tiles), 256 threads.
-template <typename BinT>
+// W16: int16 codes (a 32-bit word per row) into two-word cells (int64
+// gradient, uint64 hessian sums); a 2,048-row chunk's sums of |q| <= 32767
+// still fit the 32-bit shared words.
+template <typename BinT, bool W16 = false>
 __global__ void __launch_bounds__(k_qthreads, 3)
     qhist_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
                  uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
-                 uint16_t const *__restrict__ qgh, uint32_t const *tile_ids,
+                 void const *__restrict__ qgh, uint32_t const *tile_ids,
                  int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
                  uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
@@ -2154,7 +2193,8 @@ __global__ void __launch_bounds__(k_qthreads, 3)
         {
             if (ok[u])
             {
-                q[u]  = qgh[r[u]];
+                q[u]  = W16 ? static_cast<uint32_t const *>(qgh)[r[u]]
+                            : static_cast<uint32_t>(static_cast<uint16_t const *>(qgh)[r[u]]);
                 va[u] = mt[static_cast<uint64_t>(r[u]) * 2];
                 vb[u] = mt[(static_cast<uint64_t>(r[u]) * 2) + 1];
             }
@@ -2166,8 +2206,9 @@ __global__ void __launch_bounds__(k_qthreads, 3)
             {
                 continue;
             }
-            int32_t const  qg   = static_cast<int8_t>(q[u] & 0xFFu);
-            uint32_t const qh   = q[u] >> 8;
+            int32_t const  qg   = W16 ? static_cast<int16_t>(q[u] & 0xFFFFu)
+                                      : static_cast<int8_t>(q[u] & 0xFFu);
+            uint32_t const qh   = W16 ? q[u] >> 16 : q[u] >> 8;
             uint32_t const w[8] = {va[u].x, va[u].y, va[u].z, va[u].w,
                                    vb[u].x, vb[u].y, vb[u].z, vb[u].w};
 #pragma unroll
@@ -2186,20 +2227,27 @@ __global__ void __launch_bounds__(k_qthreads, 3)
         }
     }
     __syncthreads();
-    unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells);
+    constexpr uint32_t  cw  = W16 ? 2 : 1;
+    unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells * cw);
     for (uint32_t x = threadIdx.x; x < cells; x += k_qthreads)
     {
         uint32_t const i  = x / max_nb;
         uint32_t const bb = x % max_nb;
         int32_t const  jj = j_s[i];
-        if (jj >= 0 && bb < sel_nb[jj])
+        if (jj >= 0 && bb < sel_nb[jj] && (hg_s[x] != 0 || hh_s[x] != 0))
         {
-            unsigned long long const v =
-                (static_cast<unsigned long long>(static_cast<uint32_t>(hg_s[x])) << 32) +
-                static_cast<unsigned long long>(hh_s[x]);
-            if (v != 0ULL)
+            uint64_t const cell = cell_off[jj] + bb;
+            if constexpr (W16)
             {
-                atomicAdd(&dst[cell_off[jj] + bb], v);
+                atomicAdd(&dst[2 * cell],
+                          static_cast<unsigned long long>(static_cast<int64_t>(hg_s[x])));
+                atomicAdd(&dst[(2 * cell) + 1], static_cast<unsigned long long>(hh_s[x]));
+            }
+            else
+            {
+                atomicAdd(&dst[cell],
+                          (static_cast<unsigned long long>(static_cast<uint32_t>(hg_s[x])) << 32) +
+                              static_cast<unsigned long long>(hh_s[x]));
             }
         }
     }
@@ -2443,26 +2491,28 @@ __global__ void __launch_bounds__(k_tthreads, 1)
 }
 
 __device__ __forceinline__ void qtotals_from_cells(unsigned long long const *cells,
-                                                   uint32_t nb, int64_t &g, int64_t &h)
+                                                   uint32_t nb, uint32_t cw, int64_t &g,
+                                                   int64_t &h)
 {
     int64_t sg = 0;
     int64_t sh = 0;
     for (uint32_t b = 0; b < nb; ++b)
     {
-        unsigned long long const c = cells[b];
-        sg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-        sh += static_cast<uint32_t>(c);
+        int64_t cg, ch;
+        qcell(cells, b, cw, cg, ch);
+        sg += cg;
+        sh += ch;
     }
     g = sg;
     h = sh;
 }
 
 __global__ void qroot_totals_kernel(Node *nodes, unsigned long long const *hist,
-                                    uint32_t const *sel_nb)
+                                    uint32_t const *sel_nb, uint32_t cw)
 {
     if (threadIdx.x == 0)
     {
-        qtotals_from_cells(hist, sel_nb[0], nodes[0].qg, nodes[0].qh);
+        qtotals_from_cells(hist, sel_nb[0], cw, nodes[0].qg, nodes[0].qh);
     }
 }
 
@@ -2477,7 +2527,8 @@ __global__ void __launch_bounds__(k_threads)
                             uint32_t total_cells, uint32_t n_cells, Node const *cur,
                             Node *next, Best const *best, uint32_t const *sel,
                             uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
-                            TreeParams tp, double2 const *qscale, int64_t const *btot)
+                            TreeParams tp, double2 const *qscale, int64_t const *btot,
+                            uint32_t cw)
 {
     uint32_t const k = blockIdx.x;
     if (k == 0 && blockIdx.y == 0 && threadIdx.x == 0)
@@ -2491,12 +2542,13 @@ __global__ void __launch_bounds__(k_threads)
     uint32_t const p  = bpair[3 * k];
     uint32_t const s  = bpair[(3 * k) + 1];
     uint32_t const l  = bpair[(3 * k) + 2];
-    auto const    *hp = hist_cur + (static_cast<uint64_t>(p) * total_cells);
-    auto const    *hs = hist_nxt + (static_cast<uint64_t>(s) * total_cells);
-    auto          *hl = hist_nxt + (static_cast<uint64_t>(l) * total_cells);
-    // blockIdx.y takes cells [y * k_sub_cells, (y + 1) * k_sub_cells)
+    // words: cw per cell (two for int16 codes); the subtraction is word-wise
+    auto const    *hp = hist_cur + (static_cast<uint64_t>(p) * total_cells * cw);
+    auto const    *hs = hist_nxt + (static_cast<uint64_t>(s) * total_cells * cw);
+    auto          *hl = hist_nxt + (static_cast<uint64_t>(l) * total_cells * cw);
+    // blockIdx.y takes words [y * k_sub_cells, (y + 1) * k_sub_cells)
     uint32_t const x0 = blockIdx.y * k_sub_cells;
-    uint32_t const x1 = min(n_cells, x0 + k_sub_cells);
+    uint32_t const x1 = min(n_cells * cw, x0 + k_sub_cells);
 #pragma unroll 4
     for (uint32_t x = x0 + threadIdx.x; x < x1; x += k_threads)
     {
@@ -2523,9 +2575,10 @@ __global__ void __launch_bounds__(k_threads)
     {
         for (uint32_t b = threadIdx.x; b < sel_nb[0]; b += 32)
         {
-            unsigned long long const c = hs[b];
-            sg += static_cast<int32_t>(static_cast<uint32_t>(c >> 32));
-            sh += static_cast<uint32_t>(c);
+            int64_t cg, ch;
+            qcell(hs, b, cw, cg, ch);
+            sg += cg;
+            sh += ch;
         }
     }
 #pragma unroll
@@ -2580,7 +2633,8 @@ __global__ void __launch_bounds__(k_threads)
 // added into the chunk's build slot.
 __global__ void __launch_bounds__(k_threads)
     qbuilt_totals_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *rows,
-                         uint16_t const *__restrict__ qgh, int64_t *btot)
+                         uint16_t const *__restrict__ qgh, uint32_t const *__restrict__ qgh16,
+                         int64_t *btot)
 {
     uint32_t const c = blockIdx.x;
     if (c >= ctl->n_bchunks)
@@ -2592,9 +2646,19 @@ __global__ void __launch_bounds__(k_threads)
     int64_t     h  = 0;
     for (uint32_t k = threadIdx.x; k < ch.count; k += k_threads)
     {
-        uint32_t const q = qgh[rows[ch.begin + k]];
-        g += static_cast<int8_t>(q & 0xFFu);
-        h += q >> 8;
+        uint32_t const r = rows[ch.begin + k];
+        if (qgh16 != nullptr)
+        {
+            uint32_t const q = qgh16[r];
+            g += static_cast<int16_t>(q & 0xFFFFu);
+            h += q >> 16;
+        }
+        else
+        {
+            uint32_t const q = qgh[r];
+            g += static_cast<int8_t>(q & 0xFFu);
+            h += q >> 8;
+        }
     }
 #pragma unroll
     for (uint32_t o = 16; o > 0; o >>= 1)
@@ -2860,6 +2924,7 @@ template <bool Q>
 __global__ void leaf_sub_kernel(LeafOut const *out, uint32_t const *bpair, void *pool,
                                 uint32_t total_cells, uint32_t n_cells)
 {
+    // quantised: total_cells and n_cells count words (cw per cell)
     if (out->split == 0)
     {
         return;
@@ -2891,7 +2956,7 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
                                    uint32_t const *slot_of, void const *pool,
                                    uint32_t total_cells, uint32_t const *sel,
                                    uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
-                                   TreeParams tp, double2 const *qscale, LeafPop p)
+                                   TreeParams tp, double2 const *qscale, LeafPop p, uint32_t cw)
 {
     if (threadIdx.x != 0)
     {
@@ -2908,10 +2973,10 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
     if constexpr (Q)
     {
         auto const *h = static_cast<unsigned long long const *>(pool);
-        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells), sel_nb[0],
-                           L.qg, L.qh);
-        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells), sel_nb[0],
-                           R.qg, R.qh);
+        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells * cw),
+                           sel_nb[0], cw, L.qg, L.qh);
+        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells * cw),
+                           sel_nb[0], cw, R.qg, R.qh);
         double2 const sc = *qscale;
         gl = static_cast<double>(L.qg) * sc.x;
         hl = static_cast<double>(L.qh) * sc.y;
@@ -3030,10 +3095,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         throw ConfigError("grower: max_depth above 8 exceeds the level plane's "
                           "512-node frontier; use a host grower");
     }
-    if (cfg_.mode == HistMode::quant16)
-    {
-        throw ConfigError("grower: hist_mode int16 is not available; use int8 (1)");
-    }
+    cw_ = cfg_.mode == HistMode::quant16 ? 2 : 1; // int16 sums take two-word cells
     std::vector<uint32_t> off(n_sel_ + 1, 0);
     std::vector<uint32_t> nb(n_sel_, 0);
     for (uint32_t j = 0; j < n_sel_; ++j)
@@ -3048,7 +3110,8 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         throw ConfigError("grower: a feature has more than 4096 bins; lower "
                           "bin_mapper.max_bin or use a host grower");
     }
-    if (quant_ && static_cast<uint64_t>(max_root_rows) * 127ULL >= (1ULL << 31))
+    if (cfg_.mode == HistMode::quant8 &&
+        static_cast<uint64_t>(max_root_rows) * 127ULL >= (1ULL << 31))
     {
         throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per "
                           "node; use hist_mode exact");
@@ -3079,9 +3142,10 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     ctl_      = dalloc<Ctl>(1, s);
     nodes_[0] = dalloc<Node>(max_front_, s);
     nodes_[1] = dalloc<Node>(max_front_, s);
-    hist_[0]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_, s);
+    hist_[0]  = dalloc<float2>(static_cast<size_t>(max_front_) * total_cells_ * cw_, s);
     // (leafwise uses the first buffer as its slot pool)
-    hist_[1]  = dalloc<float2>(static_cast<size_t>(cfg_.leaf ? 1 : max_front_) * total_cells_, s);
+    hist_[1]  = dalloc<float2>(static_cast<size_t>(cfg_.leaf ? 1 : max_front_) * total_cells_ * cw_,
+                               s);
     cand_     = dalloc<Best>(static_cast<size_t>(max_front_) * n_sel_, s);
     best_     = dalloc<Best>(max_front_, s);
     pchunks_  = dalloc<Chunk>(max_pchunks_, s);
@@ -3113,6 +3177,11 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         qscale_  = dalloc<double2>(1, s);
         // +2: the histogram copies whole 4-byte words of codes
         qgh8_    = dalloc<uint16_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 2, s);
+        if (cw_ == 2)
+        {
+            qgh16_ = dalloc<uint32_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 1,
+                                      s);
+        }
         partial_ = dalloc<double2>(max_pchunks_, s);
         btot_    = dalloc<int64_t>(2 * static_cast<size_t>(max_front_), s);
         done_    = dalloc<uint32_t>(1, s);
@@ -3155,6 +3224,12 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
+        BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(qsmem)));
+        BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint8_t, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(static_cast<size_t>(32) * max_nb_ * 8)));
         size_t const tsmem = k_tsmem;
         BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3171,7 +3246,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     BB_CHECK(cudaStreamSynchronize(s));
 
     // dynamic shared memory ceilings
-    size_t const find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
+    size_t const find_smem = max_nb_ * (sizeof(double2) + (sizeof(unsigned long long) * cw_));
     if (find_smem > 227 * 1024)
     {
         throw ConfigError("grower: bins per feature exceed the shared-memory budget");
@@ -3227,7 +3302,7 @@ Grower::~Grower()
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
                     tile_j_[1], bbase_,   dirs_,    btot_,    done_,    wacc_,
-                    leaf16_,  nbound_,  gleft_};
+                    leaf16_,  nbound_,  gleft_,   qgh16_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -3276,7 +3351,7 @@ void Grower::set_shard(Reducer *r, uint64_t row_offset, uint64_t total_rows)
         throw ConfigError("grower: a sharded fit needs the quantised form (integer "
                           "histograms combine exactly; float cells would not)");
     }
-    if (r != nullptr && total_rows * 127ULL >= (1ULL << 31))
+    if (r != nullptr && cfg_.mode == HistMode::quant8 && total_rows * 127ULL >= (1ULL << 31))
     {
         throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per fit");
     }
@@ -3323,8 +3398,16 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
     }
     uint2 const key = make_uint2(static_cast<uint32_t>(seed_),
                                  static_cast<uint32_t>(seed_ >> 32));
-    quantise_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_, qscale_,
-                                               row_off_);
+    if (cw_ == 2)
+    {
+        quantise_kernel<true><<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh16_,
+                                                         qscale_, row_off_);
+    }
+    else
+    {
+        quantise_kernel<false><<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_,
+                                                          qscale_, row_off_);
+    }
     BB_LAUNCH("quantise_kernel");
     n_launch_ += 1;
 }
@@ -3339,15 +3422,33 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         if (!zeroed)
         {
             zero_build_kernel<<<max_front_, k_threads, 0, s>>>(
-                ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_,
-                off_h_[nfb]);
+                ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_ * cw_,
+                off_h_[nfb] * cw_);
             BB_LAUNCH("zero_build_kernel");
             n_launch_ += 1;
         }
         uint32_t const per   = k_mirror_bytes / (plane_.u8 ? 1 : 2);
         size_t const   qsmem = static_cast<size_t>(per) * max_nb_ * 8;
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
-        if (plane_.u8)
+        if (cw_ == 2)
+        {
+            // int16 codes: the per-chunk kernel with two-word cells
+            if (plane_.u8)
+            {
+                qhist_kernel<uint8_t, true><<<grid, k_qthreads, qsmem, s>>>(
+                    ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                    plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                    static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+            }
+            else
+            {
+                qhist_kernel<uint16_t, true><<<grid, k_qthreads, qsmem, s>>>(
+                    ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                    plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                    static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+            }
+        }
+        else if (plane_.u8)
         {
             size_t const tsmem = k_tsmem;
             qhist_t_kernel<<<dim3(qctas_, n_tiles_[v]), k_tthreads, tsmem, s>>>(
@@ -3445,7 +3546,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     cudaStream_t s   = stream_;
     int const    cur = static_cast<int>(L & 1);
     int const    nxt = cur ^ 1;
-    size_t const find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
+    size_t const find_smem = max_nb_ * (sizeof(double2) + (sizeof(unsigned long long) * cw_));
     phase_begin();
     dim3 const fgrid(max_front_, n_sel_);
     if (cfg_.level)
@@ -3455,26 +3556,26 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         {
             level_find_kernel<true><<<n_sel_, k_lfind_thr, lsmem, s>>>(
                 ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
-                cand_, max_nb_, lgroup_, qscale_);
+                cand_, max_nb_, lgroup_, qscale_, cw_);
         }
         else
         {
             level_find_kernel<false><<<n_sel_, k_lfind_thr, lsmem, s>>>(
                 ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
-                cand_, max_nb_, lgroup_, qscale_);
+                cand_, max_nb_, lgroup_, qscale_, cw_);
         }
     }
     else if (quant_)
     {
         find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_);
     }
     else
     {
         find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_);
     }
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
@@ -3526,10 +3627,10 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     bool const     last     = (L + 1) == cfg_.tp.max_depth;
     uint32_t const nfb      = last ? 1 : n_sel_;
-    uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] : 0;
+    uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] * cw_ : 0;
     pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
         ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
-        dirs_, static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_, n_zcells);
+        dirs_, static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_, n_zcells);
     BB_LAUNCH("pscatter_kernel");
     if (prof_ != nullptr)
     {
@@ -3543,7 +3644,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         phase_begin();
         BB_CHECK(cudaMemsetAsync(btot_, 0, sizeof(int64_t) * 2 * max_front_, s));
         qbuilt_totals_kernel<<<max_bchunks_, k_threads, 0, s>>>(ctl_, bchunks_, rows_out,
-                                                                 qgh8_, btot_);
+                                                                 qgh8_, qgh16_, btot_);
         BB_LAUNCH("qbuilt_totals_kernel");
         if (red_ != nullptr)
         {
@@ -3552,7 +3653,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
             ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
-            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_);
+            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
         BB_LAUNCH("qsubtract_totals_kernel");
         n_launch_ += 2;
         if (prof_ != nullptr)
@@ -3568,17 +3669,18 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         // the next frontier's slots (at most 2^(L+1)): the built ones carry
         // this shard's partial cells, the rest are rewritten by the subtraction
         size_t const slots = std::min<size_t>(size_t{2} << L, max_front_);
-        red_->sum_u64(hist_[nxt], slots * total_cells_, s);
+        red_->sum_u64(hist_[nxt], slots * total_cells_ * cw_, s);
     }
     phase_begin();
     if (quant_)
     {
-        qsubtract_totals_kernel<<<dim3(max_front_, std::max(1u, ceil_div(n_cells, k_sub_cells))),
+        qsubtract_totals_kernel<<<dim3(max_front_,
+                                       std::max(1u, ceil_div(n_cells * cw_, k_sub_cells))),
                                   k_threads, 0, s>>>(
             ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
             static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells,
             nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_,
-            nullptr);
+            nullptr, cw_);
         BB_LAUNCH("qsubtract_totals_kernel");
     }
     else
@@ -3653,13 +3755,13 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
           cfg_.tp.max_depth == 0 ? 1 : n_sel_, 0);
     if (red_ != nullptr)
     {
-        red_->sum_u64(hist_[0], total_cells_, s);
+        red_->sum_u64(hist_[0], total_cells_ * cw_, s);
     }
     phase_begin();
     if (quant_)
     {
         qroot_totals_kernel<<<1, 32, 0, s>>>(
-            nodes_[0], static_cast<unsigned long long const *>(hist_[0]), sel_nb_);
+            nodes_[0], static_cast<unsigned long long const *>(hist_[0]), sel_nb_, cw_);
         BB_LAUNCH("qroot_totals_kernel");
     }
     else
@@ -3807,7 +3909,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
 {
     cudaStream_t      s         = stream_;
     TreeParams const &tp        = cfg_.tp;
-    size_t const      find_smem = max_nb_ * (sizeof(double2) + sizeof(unsigned long long));
+    size_t const      find_smem = max_nb_ * (sizeof(double2) + (sizeof(unsigned long long) * cw_));
     auto             *lout      = static_cast<LeafOut *>(lout_);
     auto             *lh        = static_cast<LeafOut *>(lout_h_);
     void             *pool      = hist_[0];
@@ -3820,7 +3922,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     if (quant_)
     {
         qroot_totals_kernel<<<1, 32, 0, s>>>(
-            nodes_[0], static_cast<unsigned long long const *>(pool), sel_nb_);
+            nodes_[0], static_cast<unsigned long long const *>(pool), sel_nb_, cw_);
     }
     else
     {
@@ -3835,13 +3937,13 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         {
             find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
                 ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of);
+                tp, cand_, max_nb_, qscale_, slot_of, cw_);
         }
         else
         {
             find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
                 ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of);
+                tp, cand_, max_nb_, qscale_, slot_of, cw_);
         }
         BB_LAUNCH("find_kernel");
         leaf_best_kernel<<<1, 64, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split ? 1 : 0);
@@ -3950,22 +4052,23 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         BB_LAUNCH("leaf_plan_kernel");
         pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
             ctl_, pchunks_, nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0], rows_[1],
-            dirs_, static_cast<unsigned long long *>(pool), build_, total_cells_,
-            quant_ ? total_cells_ : 0);
+            dirs_, static_cast<unsigned long long *>(pool), build_, total_cells_ * cw_,
+            quant_ ? total_cells_ * cw_ : 0);
         BB_LAUNCH("pscatter_kernel");
         build(rows_[1], n_sel_, 0, true);
         uint32_t const cgrid = std::max(1u, std::min(ceil_div(c.node.count, 256), 148u * 8u));
         leaf_copyback_kernel<<<cgrid, 256, 0, s>>>(lout, rows_[1], rows_[0], c.node.start,
                                                    c.node.count);
         BB_LAUNCH("leaf_copyback_kernel");
-        uint32_t const sgrid = std::max(1u, std::min(ceil_div(total_cells_, 256), 148u * 8u));
+        uint32_t const sgrid =
+            std::max(1u, std::min(ceil_div(total_cells_ * cw_, 256), 148u * 8u));
         if (quant_)
         {
-            leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
-                                                        total_cells_);
+            leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_ * cw_,
+                                                        total_cells_ * cw_);
             leaf_totals_kernel<true><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                       total_cells_, sel_, sel_nb_, mono_, n_mono_,
-                                                      tp, qscale_, p);
+                                                      tp, qscale_, p, cw_);
         }
         else
         {
@@ -3973,7 +4076,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                                          total_cells_);
             leaf_totals_kernel<false><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                        total_cells_, sel_, sel_nb_, mono_,
-                                                       n_mono_, tp, qscale_, p);
+                                                       n_mono_, tp, qscale_, p, 1);
         }
         BB_LAUNCH("leaf_totals_kernel");
         find(nodes_[1], slot_of_, c.depth + 1 < tp.max_depth);
@@ -4074,16 +4177,18 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     std::vector<double2> cells(total_cells_);
     if (quant_)
     {
-        std::vector<unsigned long long> q(total_cells_);
+        std::vector<unsigned long long> q(static_cast<size_t>(total_cells_) * cw_);
         double2                         sc{};
-        BB_CHECK(cudaMemcpyAsync(q.data(), hist_[0], total_cells_ * 8ULL, cudaMemcpyDeviceToHost, s));
+        BB_CHECK(cudaMemcpyAsync(q.data(), hist_[0], q.size() * 8ULL, cudaMemcpyDeviceToHost, s));
         BB_CHECK(cudaMemcpyAsync(&sc, qscale_, sizeof(double2), cudaMemcpyDeviceToHost, s));
         BB_CHECK(cudaStreamSynchronize(s));
         for (uint32_t x = 0; x < total_cells_; ++x)
         {
-            out[x] = make_double2(static_cast<double>(static_cast<int32_t>(
-                                      static_cast<uint32_t>(q[x] >> 32))) * sc.x,
-                                  static_cast<double>(static_cast<uint32_t>(q[x])) * sc.y);
+            int64_t const g = cw_ == 2 ? static_cast<int64_t>(q[2 * x])
+                                       : static_cast<int32_t>(static_cast<uint32_t>(q[x] >> 32));
+            int64_t const h = cw_ == 2 ? static_cast<int64_t>(q[(2 * x) + 1])
+                                       : static_cast<int64_t>(static_cast<uint32_t>(q[x]));
+            out[x] = make_double2(static_cast<double>(g) * sc.x, static_cast<double>(h) * sc.y);
         }
     }
     else

@@ -226,6 +226,7 @@ class Grower
     uint32_t              cell_stride_ = 0; // per-(chunk, feature) count stride
     uint32_t              lgroup_      = 1; // nodes per level-finder group
     uint32_t              qctas_       = 1; // u8 quantised histogram CTAs per tile
+    uint32_t              cw_          = 1; // words per quantised cell (2: int16 codes)
 
     // device
     uint32_t *sel_      = nullptr; // selected feature ids
@@ -262,6 +263,7 @@ class Grower
     uint32_t *absmax_   = nullptr; // max |g| and max h, as float bits
     double2  *qscale_   = nullptr; // (scale_g, scale_h) in FP64
     uint16_t *qgh8_     = nullptr; // per row: int8 g | uint8 h << 8
+    uint32_t *qgh16_    = nullptr; // per row (int16 codes): int16 g | uint16 h << 16
     double2  *partial_  = nullptr; // per partition chunk: leaf (G, H) in FP64
     int64_t  *btot_     = nullptr; // per build index: exact (G, H) of the last level
     uint32_t *done_     = nullptr; // leaf-renewal CTA ticket (zero between launches)

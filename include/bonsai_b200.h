@@ -94,7 +94,8 @@ typedef struct
     float          lambda_l1;
     uint32_t       max_depth;  /* <= 8 */
     uint32_t       min_data_in_leaf;
-    int32_t        hist_mode;  /* 0 exact (plain), 1 int8 quantised, 2 int16 */
+    int32_t        hist_mode;  /* 0 exact (plain), 1 int8 quantised, 2 int16 quantised
+                                  (two-word cells; finer, slower) */
     uint64_t       seed;       /* quantised stochastic-rounding seed */
     int8_t const  *monotone;   /* per-feature +1/-1/0, or NULL */
     uint32_t       n_monotone;

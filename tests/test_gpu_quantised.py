@@ -41,15 +41,16 @@ def _fp64_hist(bins, n_bins, g, h):
     return np.concatenate(cells)
 
 
-def test_quantised_histogram_error_vs_fp64(bb):
+@pytest.mark.parametrize("mode,qmax", [("int8", 127.0), ("int16", 32767.0)])
+def test_quantised_histogram_error_vs_fp64(bb, mode, qmax):
     X, g, h = _data(3, 400_000)
     cuts, off = bb.fit_cuts(X)
     plane = bb.Plane(X, cuts, off)
     nb = np.diff(off)
-    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=7), g, h)
+    q = bb.populate(plane, bb.TrainParams(hist_mode=mode, seed=7), g, h)
     ref = _fp64_hist(plane.bins(), nb, g, h)
-    sg = np.abs(g).max() / 127.0
-    sh = h.max() / 127.0
+    sg = np.abs(g).max() / qmax
+    sh = h.max() / qmax
     counts = np.concatenate([np.bincount(plane.bins()[f], minlength=nb[f]) for f in range(len(nb))])
     # stochastic rounding: unbiased, per-row error below one scale step
     err_g = np.abs(q[:, 0] - ref[:, 0])
@@ -58,7 +59,7 @@ def test_quantised_histogram_error_vs_fp64(bb):
     assert np.all(err_h <= 6 * sh * np.sqrt(counts) + sh)
     # every feature sees the same rows: the integer totals agree exactly
     # (cells are integer sums times the FP64 scale: recover the integers)
-    scale = np.array([np.abs(g).max() / 127.0, h.max() / 127.0])
+    scale = np.array([np.abs(g).max() / qmax, h.max() / qmax])
     ints = np.rint(q / scale)
     tot = [ints[off[f]:off[f + 1]].sum(0) for f in range(len(nb))]
     assert all(np.array_equal(tot[0], t) for t in tot)
@@ -196,3 +197,60 @@ def test_quantised_u16_bins_histogram_and_fit(bb):
                                              hist_mode="int8"), max_trees=10)
     b.update(10)
     assert b.n_trees == 10 and np.isfinite(b.scores()).all()
+
+
+def test_int16_u16_bins_levelwise_leafwise_and_shards(bb):
+    """int16 codes (two-word cells) through the generic kernel on both bin
+    widths, the three growers, and a two-shard fit equal to the unsharded one."""
+    import threading
+    X, g, h = _data(13, 120_000, F=7)
+    y = (X[:, 0] + np.nan_to_num(X[:, 1]) * X[:, 2] > 0).astype(np.float32)
+    for max_bin in (255, 700):
+        cuts, off = bb.fit_cuts(X, max_bin=max_bin)
+        plane = bb.Plane(X, cuts, off)
+        q = bb.populate(plane, bb.TrainParams(hist_mode="int16", seed=3), g, h)
+        ref = _fp64_hist(plane.bins(), np.diff(off), g, h)
+        counts = np.concatenate([np.bincount(plane.bins()[f], minlength=np.diff(off)[f])
+                                 for f in range(7)])
+        sg = np.abs(g).max() / 32767.0
+        assert np.all(np.abs(q[:, 0] - ref[:, 0]) <= 6 * sg * np.sqrt(counts) + sg)
+        for grower in ("depthwise", "levelwise", "leafwise"):
+            b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", grower=grower,
+                                                     max_depth=6, max_leaves=40,
+                                                     hist_mode="int16"), max_trees=5)
+            b.update(5)
+            assert b.n_trees == 5 and np.isfinite(b.scores()).all(), (max_bin, grower)
+    cuts, off = bb.fit_cuts(X)
+    params = bb.TrainParams(objective="logloss", max_depth=6, hist_mode="int16", seed=4)
+    full = bb.Booster(bb.Plane(X, cuts, off), y, params, max_trees=4)
+    full.update(4)
+    comms = bb.Comm.group(2)
+    shards = []
+    for s in range(2):
+        a, e = bb.shard_range(len(X), 2, s)
+        shards.append(bb.Booster(bb.Plane(X[a:e], cuts, off), y[a:e], params, max_trees=4,
+                                 comm=comms[s], row_offset=a, total_rows=len(X),
+                                 init_score=full.init_score))
+    ts = [threading.Thread(target=lambda b=b: b.update(4)) for b in shards]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert np.array_equal(np.concatenate([b.scores() for b in shards]), full.scores())
+
+
+def test_int16_closer_to_plain_than_int8(bb):
+    """Finer codes: the int16 fit's scores sit nearer the plain fit's."""
+    X, g, h = _data(17, 200_000, F=8)
+    y = (X[:, 0] + np.nan_to_num(X[:, 1]) * X[:, 2] + 0.3 * g > 0).astype(np.float32)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    out = {}
+    for mode in ("exact", "int8", "int16"):
+        b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=6,
+                                                hist_mode=mode, seed=2), max_trees=20)
+        b.update(20)
+        out[mode] = b.scores()
+    d8 = np.abs(out["int8"] - out["exact"]).mean()
+    d16 = np.abs(out["int16"] - out["exact"]).mean()
+    assert d16 < d8
