@@ -11,6 +11,15 @@ per-row state exceed the 126 MB L2, so no flush is needed between rounds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode exact|int8|int16]
   python bench.py --impl reference      # the reference's CPU grower, timed
+  python bench.py --workload serve [--impl reference]
+
+The serving workload fits a 1,000-tree depth-8 ensemble (squared error, 255
+bins, lr 0.1) on 20,000 rows x 28 of the ragged-many family, then scores
+request batches of 1 to 1,000,000 rows x 28: predict rows/s through a
+predict plan (device time per launch, L2 flushed between launches, and end
+to end from pinned host rows through ingest to host scores) and TreeSHAP
+rows/s with the additivity error against an FP64 recomputation of the
+margin.
 
 Multi-GPU (torchrun): every rank fits its own replica of the workload (one
 fit per GPU, no collective in the data path); value is the time for all
@@ -188,6 +197,190 @@ def make_data(rows):
     return X, y, cuts, off
 
 
+SERVE_METRIC = ("1,000-tree depth-8 ensemble predict rows/s at a 1,000,000-row batch; "
+                "TreeSHAP rows/s and additivity error vs FP64")
+SERVE_WORKLOAD = ("serving: 1,000 depth-8 trees (mse, 255 bins, lr 0.1) fit on 20,000x28; "
+                  "request batches of 1 to 1,000,000 rows x 28 float32")
+SERVE_FIT_ROWS = 20_000
+SERVE_TREES = 1000
+SERVE_BATCHES = (1, 100, 10_000, 1_000_000)
+SHAP_BATCHES = (1, 100, 2_000)
+LEAF = 0xFFFFFFFF
+
+
+def margin64(codes, n_bins, trees, init, lr):
+    """init + lr * sum of leaves in FP64 (the bin-space walk of routes_left,
+    vectorised over rows)."""
+    F, n = codes.shape
+    last = np.asarray(n_bins, np.int64) - 1
+    acc = np.zeros(n, np.float64)
+    rows = np.arange(n)
+    for t in trees:
+        idx = np.zeros(n, np.int64)
+        feat = t.feature.astype(np.int64)
+        while True:
+            f = feat[idx]
+            live = f != LEAF
+            if not live.any():
+                break
+            fl = np.where(live, f, 0)
+            b = codes[fl, rows].astype(np.int64)
+            left = np.where(b == last[fl], t.default_left[idx] != 0, b <= t.split_bin[idx])
+            nxt = np.where(left, t.left[idx], t.right[idx]).astype(np.int64)
+            idx = np.where(live, nxt, idx)
+        acc += t.value[idx].astype(np.float64)
+    # the booster's own float init and learning rate, widened
+    return float(np.float32(init)) + float(np.float32(lr)) * acc
+
+
+def serve_data():
+    from bonsai_b200 import synth
+    from bonsai_b200.binning import fit_cuts
+    X, y, Xr = synth.serving(n_fit=SERVE_FIT_ROWS, n_requests=max(SERVE_BATCHES))
+    cuts, off = fit_cuts(X, max_bin=255)
+    return X, y, Xr, cuts, off
+
+
+def serve_reference(args):
+    """The reference's own CPU path (oracle/_ref, all host threads): the same
+    fit through its depthwise Booster, then predict_at_binned and
+    pred_contribs_binned over bounded samples of each request batch."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    X, y, Xr, cuts, off = serve_data()
+    threads = len(os.sched_getaffinity(0))
+    ref = O.RefLib()
+    tc = O.TreeCfg(objective="mse", max_depth=8, learning_rate=0.1, n_iters=SERVE_TREES,
+                   n_threads=threads)
+    model = ref.train(ref.dataset(X, y, cuts, off), tc)
+    out = {}
+    for B in SERVE_BATCHES:
+        m = min(B, 50_000)
+        ds = ref.dataset(Xr[:m], np.zeros(m, np.float32), cuts, off)
+        model.predict_binned(ds)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            model.predict_binned(ds)
+        out[B] = m * args.steps / (time.perf_counter() - t0)
+    shap = {}
+    for B in SHAP_BATCHES:
+        m = min(B, 64)
+        ds = ref.dataset(Xr[:m], np.zeros(m, np.float32), cuts, off)
+        t0 = time.perf_counter()
+        model.contribs_binned(ds)
+        shap[B] = m / (time.perf_counter() - t0)
+    big = max(SERVE_BATCHES)
+    cb = {"value": out[big], "unit": "rows/s", "cores": threads, "kind": "reference",
+          "sample": f"predict_at_binned over min(batch, 50,000) rows x {args.steps} calls; "
+                    "pred_contribs_binned over min(batch, 64) rows"}
+    line = {"metric": SERVE_METRIC, "value": out[big], "unit": "rows/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": big / out[big] * 1000.0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "host_threads": threads},
+            "predict_rows_per_s": {str(k): v for k, v in out.items()},
+            "shap_rows_per_s": {str(k): v for k, v in shap.items()},
+            "cpu_baseline": cb,
+            "e2e": {"value": out[big], "unit": "rows/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def serve_ours(args, local):
+    import torch
+
+    import bonsai_b200 as bb
+    X, y, Xr, cuts, off = serve_data()
+    plane = bb.Plane(X, cuts, off)
+    b = bb.Booster(plane, y, bb.TrainParams(objective="mse", max_depth=8, learning_rate=0.1,
+                                            min_data_in_leaf=20, hist_mode="exact",
+                                            use_graph=True), max_trees=SERVE_TREES)
+    b.update(SERVE_TREES)
+    trees, init = b.trees(), b.init_score
+    b.close()
+    plane.close()
+    n_max = max(SERVE_BATCHES)
+    Xp = torch.empty((n_max, Xr.shape[1]), dtype=torch.float32, pin_memory=True).numpy()
+    Xp[...] = Xr
+    big = bb.Plane(Xp, cuts, off)
+    plan = bb.PredictPlan(big, trees, init, 0.1)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    W, K = max(3, args.warmup), max(1, args.steps)
+    dev, e2e, launches = {}, {}, {}
+    with Clocks(local) as clk:
+        for B in SERVE_BATCHES:
+            pb = bb.Plane(Xp[:B], cuts, off)
+            out = torch.empty(B, dtype=torch.float32, device="cuda")
+            for _ in range(W):
+                plan.launch(pb, out.data_ptr(), stream.cuda_stream)
+            ms, k = 0.0, 0
+            for _ in range(K):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                k += plan.launch(pb, out.data_ptr(), stream.cuda_stream)
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+            dev[B] = B * K / (ms * 1e-3)
+            launches[B] = k / K
+            pb.close()
+            # end to end: pinned host rows -> ingest -> plan -> host scores
+            for _ in range(W):
+                q = bb.Plane(Xp[:B], cuts, off)
+                plan.run(q)
+                q.close()
+            t0 = time.perf_counter()
+            for _ in range(K):
+                q = bb.Plane(Xp[:B], cuts, off)
+                plan.run(q)
+                q.close()
+            e2e[B] = B * K / (time.perf_counter() - t0)
+    shap, additivity = {}, {}
+    for B in SHAP_BATCHES:
+        pb = bb.Plane(Xp[:B], cuts, off)
+        bb.pred_contribs(pb, trees, init, 0.1)
+        t0 = time.perf_counter()
+        phi = bb.pred_contribs(pb, trees, init, 0.1)
+        shap[B] = B / (time.perf_counter() - t0)
+        m64 = margin64(pb.bins(), pb.n_bins, trees, init, 0.1)
+        additivity[B] = float(np.max(np.abs(phi.sum(axis=1) - m64)))
+        pb.close()
+    # the CPU baseline: the oracle's bin-space walk (C, one thread) on a sample
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    orc = O.Oracle()
+    m = 20_000
+    codes = big.bins()[:, :m]
+    t0 = time.perf_counter()
+    orc.predict_binned(codes, big.n_bins, trees, init, 0.1)
+    cpu = m / (time.perf_counter() - t0)
+    big.close()
+    plan.close()
+    depth = max(t.depth for t in trees)
+    line = {
+        "metric": SERVE_METRIC, "value": dev[n_max], "unit": "rows/s", "n_gpus": 1,
+        "steps": K, "warmup": W, "ms_per_step": n_max / dev[n_max] * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ragged-many family)",
+        "config": {"workload": SERVE_WORKLOAD, "trees": len(trees), "max_depth": depth,
+                   "l2": "256 MB flush written between timed launches"},
+        "predict_rows_per_s": {str(k): v for k, v in dev.items()},
+        "predict_e2e_rows_per_s": {str(k): v for k, v in e2e.items()},
+        "shap_rows_per_s": {str(k): v for k, v in shap.items()},
+        "shap_additivity_max_abs": {str(k): v for k, v in additivity.items()},
+        "e2e": {"value": e2e[n_max], "unit": "rows/s", "h2d_bytes_per_step": n_max * 28 * 4,
+                "d2h_bytes_per_step": n_max * 4},
+        "gpu_launches": int(launches[n_max] * K),
+        "clocks": clk.summary(),
+        "cpu_baseline": {"value": cpu, "unit": "rows/s", "cores": 1, "kind": "port",
+                         "sample": f"oracle bin-space walk over the first {m:,} request rows"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -200,11 +393,31 @@ def main():
                          "(0 skips it)")
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="fit", choices=["fit", "serve"])
     args = ap.parse_args()
     W = max(3, args.warmup)
     K = max(1, args.steps)
 
     world, rank, local = dist_init(args.gpus)
+    if args.workload == "serve":
+        # one replica per GPU; rank 0 reports
+        if args.impl == "reference":
+            if rank == 0:
+                serve_reference(args)
+            return
+        import bonsai_b200 as bb
+        from bonsai_b200.build import build_library
+        if rank == 0:
+            build_library()
+        barrier(world)
+        bb.lib().bb_select_device(local)
+        if rank == 0:
+            serve_ours(args, local)
+        barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         if rank != 0:
             return

@@ -26,7 +26,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
+    "grow_tree", "populate", "predict", "PredictPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
     "Comm", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
@@ -168,6 +168,29 @@ class Plane:
         self.h = h.value
         self._keep = None
 
+    @classmethod
+    def from_bins(cls, bins, cuts, cut_off) -> "Plane":
+        """A plane over codes binned elsewhere (bb_plane_from_bins): bins is
+        [n_feats, n_rows], uint8 (every feature <= 256 bins) or uint16, each
+        code below its feature's bin count cut_off[f + 1] - cut_off[f]."""
+        bins = np.ascontiguousarray(bins)
+        if bins.dtype not in (np.uint8, np.uint16) or bins.ndim != 2:
+            raise ValueError("bins must be a 2-D uint8 or uint16 array [n_feats, n_rows]")
+        self = cls.__new__(cls)
+        self.cuts = np.ascontiguousarray(cuts, dtype=np.float32)
+        self.cut_off = np.ascontiguousarray(cut_off, dtype=np.uint32)
+        F, n = bins.shape
+        if len(self.cut_off) != F + 1:
+            raise ValueError("cut_off must hold n_features + 1 offsets")
+        self.n_rows, self.n_feats = int(n), int(F)
+        self.n_bins = np.diff(self.cut_off).astype(np.uint32)
+        self._keep = None
+        h = C.c_void_p()
+        check(lib().bb_plane_from_bins(ptr(bins), 1 if bins.dtype == np.uint8 else 0, n, F,
+                                       ptr(self.cuts), ptr(self.cut_off), C.byref(h)))
+        self.h = h.value
+        return self
+
     @property
     def u8(self) -> bool:
         return bool(lib().bb_plane_is_u8(self.h))
@@ -183,7 +206,10 @@ class Plane:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:
+            pass  # interpreter shutdown: the library may be gone already
 
 
 COMM_ID_BYTES = 128
@@ -371,7 +397,10 @@ class Booster:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:
+            pass  # interpreter shutdown: the library may be gone already
 
 
 def grow_tree(plane: Plane, params: TrainParams, grad, hess, rows=None):
@@ -431,6 +460,55 @@ def predict(plane: Plane, trees: list, init: float, lr: float) -> np.ndarray:
                            ptr(cat["split_bin"]), ptr(cat["left"]), ptr(cat["right"]),
                            ptr(cat["default_left"]), ptr(cat["value"]), lr, init, ptr(out)))
     return out
+
+
+class PredictPlan:
+    """An ensemble packed for the device once (bb_predict_plan_*): `run`
+    scores any plane with the features and bin counts of the one it was
+    packed against, bit-identical to `predict`."""
+
+    def __init__(self, plane: Plane, trees: list, init: float, lr: float):
+        roots, base, cat = _concat(trees, ("feature", "split_bin", "left", "right",
+                                           "default_left", "value"))
+        self.n_trees = len(trees)
+        h = C.c_void_p()
+        check(lib().bb_predict_plan_create(plane.h, len(trees), ptr(roots), base,
+                                           ptr(cat["feature"]), ptr(cat["split_bin"]),
+                                           ptr(cat["left"]), ptr(cat["right"]),
+                                           ptr(cat["default_left"]), ptr(cat["value"]), lr,
+                                           init, C.byref(h)))
+        self.h = h
+
+    @property
+    def depth(self) -> int:
+        """The padded heap depth, or 0 for the node-table form."""
+        d = C.c_uint32()
+        check(lib().bb_predict_plan_depth(self.h, C.byref(d)))
+        return d.value
+
+    def run(self, plane: Plane, n_trees: int = 0) -> np.ndarray:
+        out = np.empty(plane.n_rows, np.float32)
+        check(lib().bb_predict_plan_run(self.h, plane.h, n_trees, ptr(out)))
+        return out
+
+    def launch(self, plane: Plane, out_ptr: int, stream_ptr: int = 0, n_trees: int = 0) -> int:
+        """Enqueues the scores into device memory at out_ptr on a stream
+        (a cudaStream_t as an int); returns the kernels launched."""
+        k = C.c_uint32()
+        check(lib().bb_predict_plan_launch(self.h, plane.h, n_trees, C.c_void_p(out_ptr),
+                                           C.c_void_p(stream_ptr), C.byref(k)))
+        return k.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_predict_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def predict_classes(plane: Plane, trees: list, init_scores, lr: float) -> np.ndarray:

@@ -104,6 +104,14 @@ def lib() -> C.CDLL:
                                                 vp, C.c_uint64, C.c_uint64, C.c_float,
                                                 C.POINTER(vp)]
         L.bb_populate.argtypes = [vp, C.POINTER(TrainCfg), vp, vp, vp, C.c_uint64, vp]
+        L.bb_predict_plan_create.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 6 + [
+            C.c_float, C.c_float, C.POINTER(vp)]
+        L.bb_predict_plan_run.argtypes = [vp, vp, C.c_uint32, vp]
+        L.bb_predict_plan_launch.argtypes = [vp, vp, C.c_uint32, vp, vp,
+                                             C.POINTER(C.c_uint32)]
+        L.bb_predict_plan_depth.argtypes = [vp, C.POINTER(C.c_uint32)]
+        L.bb_predict_plan_destroy.argtypes = [vp]
+        L.bb_predict_plan_destroy.restype = None
         _lib = L
     return _lib
 

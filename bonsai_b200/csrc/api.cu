@@ -175,44 +175,6 @@ __global__ void commit_tree_kernel(TreeOut scratch, TreeOut slots, uint32_t cap,
     }
 }
 
-// One thread per row, every tree in order: the bin-space walk of
-// routes_left, leaves summed in float in tree order, then init + sum * lr
-// with no contraction (booster.hpp:831-845, detail/bin_walk.hpp).
-template <typename BinT>
-__global__ void predict_kernel(BinT const *__restrict__ bins, uint64_t n_pad, uint64_t n,
-                               uint32_t const *__restrict__ last_bin, uint32_t n_trees,
-                               uint32_t const *__restrict__ roots,
-                               uint32_t const *__restrict__ feature,
-                               uint32_t const *__restrict__ split_bin,
-                               uint32_t const *__restrict__ left,
-                               uint32_t const *__restrict__ right,
-                               uint8_t const *__restrict__ dl,
-                               float const *__restrict__ value, float lr, float init,
-                               float *__restrict__ out)
-{
-    uint64_t const r = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
-    if (r >= n)
-    {
-        return;
-    }
-    float acc = 0.0F;
-    for (uint32_t t = 0; t < n_trees; ++t)
-    {
-        uint32_t const base = roots[t];
-        uint32_t       idx  = base;
-        while (feature[idx] != k_leaf_flag)
-        {
-            uint32_t const f = feature[idx];
-            uint32_t const b = bins[(static_cast<uint64_t>(f) * n_pad) + r];
-            idx = base + (routes_left(b, last_bin[f], split_bin[idx], dl[idx] != 0)
-                              ? left[idx]
-                              : right[idx]);
-        }
-        acc = acc + value[idx];
-    }
-    out[r] = init + (acc * lr);
-}
-
 template <typename T> T *dmalloc(size_t n)
 {
     void *p = nullptr;
@@ -1138,79 +1100,6 @@ extern "C"
                 cudaFree(d_gh);
                 cudaFree(d_rows);
                 BB_CHECK(cudaStreamDestroy(s));
-            });
-    }
-
-    int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
-                   uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
-                   uint32_t const *left, uint32_t const *right, uint8_t const *default_left,
-                   float const *value, float lr, float init, float *out)
-    {
-        return guarded(
-            [&]
-            {
-                Plane const   &p = plane->p;
-                uint64_t const n = p.n_rows;
-                std::vector<uint32_t> last(p.n_feats);
-                for (uint32_t f = 0; f < p.n_feats; ++f)
-                {
-                    last[f] = p.h_cut_off[f + 1] - p.h_cut_off[f] - 1;
-                }
-                // every walk must end: children lie after their parent inside
-                // the tree, and split features exist
-                for (uint32_t t = 0; t < n_trees; ++t)
-                {
-                    uint32_t const b = roots[t];
-                    uint32_t const e = t + 1 < n_trees ? roots[t + 1] : n_nodes;
-                    need(b < e && e <= n_nodes, "bb_predict: bad tree roots");
-                    for (uint32_t i = b; i < e; ++i)
-                    {
-                        if (feature[i] == k_leaf_flag)
-                        {
-                            continue;
-                        }
-                        need(feature[i] < p.n_feats, "bb_predict: node feature out of range");
-                        need(left[i] > i - b && right[i] > i - b && b + left[i] < e &&
-                                 b + right[i] < e,
-                             "bb_predict: a child id must follow its parent in its tree");
-                    }
-                }
-                uint32_t *d_last  = dmalloc<uint32_t>(p.n_feats);
-                uint32_t *d_roots = dmalloc<uint32_t>(n_trees);
-                uint32_t *d_feat  = dmalloc<uint32_t>(n_nodes);
-                uint32_t *d_sb    = dmalloc<uint32_t>(n_nodes);
-                uint32_t *d_l     = dmalloc<uint32_t>(n_nodes);
-                uint32_t *d_r     = dmalloc<uint32_t>(n_nodes);
-                uint8_t  *d_dl    = dmalloc<uint8_t>(n_nodes);
-                float    *d_v     = dmalloc<float>(n_nodes);
-                float    *d_out   = dmalloc<float>(n);
-                BB_CHECK(cudaMemcpy(d_last, last.data(), p.n_feats * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_roots, roots, n_trees * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_feat, feature, n_nodes * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_sb, split_bin, n_nodes * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_l, left, n_nodes * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_r, right, n_nodes * 4, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_dl, default_left, n_nodes, cudaMemcpyHostToDevice));
-                BB_CHECK(cudaMemcpy(d_v, value, n_nodes * 4, cudaMemcpyHostToDevice));
-                if (p.u8)
-                {
-                    predict_kernel<uint8_t><<<blocks(n), 256>>>(
-                        static_cast<uint8_t const *>(p.bins), p.n_pad, n, d_last, n_trees,
-                        d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, lr, init, d_out);
-                }
-                else
-                {
-                    predict_kernel<uint16_t><<<blocks(n), 256>>>(
-                        static_cast<uint16_t const *>(p.bins), p.n_pad, n, d_last, n_trees,
-                        d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, lr, init, d_out);
-                }
-                BB_LAUNCH("predict_kernel");
-                BB_CHECK(cudaMemcpy(out, d_out, n * 4, cudaMemcpyDeviceToHost));
-                void *ps[] = {d_last, d_roots, d_feat, d_sb, d_l, d_r, d_dl, d_v, d_out};
-                for (void *q : ps)
-                {
-                    cudaFree(q);
-                }
             });
     }
 }

@@ -20,6 +20,9 @@ matrix is float32, C-contiguous, row-major (n_rows x n_features).
   ragged_many       64 regression datasets, rows log-uniform in
                     [1e3, 2e5], 28 N(0,1) features, y = sum of 8 random
                     depth-4 step trees + N(0, 0.1^2).
+  serving           one dataset of the ragged_many family (the same 8 step
+                    trees) to fit an ensemble on, and a matrix of request
+                    rows (28 N(0,1) features) to score.
 """
 
 from __future__ import annotations
@@ -33,6 +36,7 @@ __all__ = [
     "wide_sparse",
     "multiclass_onehot",
     "ragged_many",
+    "serving",
 ]
 
 
@@ -146,3 +150,15 @@ def ragged_many(n_sets: int = 64, seed: int = 64, F: int = 28,
         y = sum(_eval_step_tree(X, t) for t in trees) + rng.normal(0.0, 0.1, n)
         out.append((X, y.astype(np.float32)))
     return out
+
+
+def serving(n_fit: int = 100_000, n_requests: int = 1_000_000, seed: int = 64, F: int = 28):
+    """(X_fit, y_fit, X_requests): the fit set drawn like one ragged_many
+    dataset (same step trees), the request rows from their own stream."""
+    rng = _rng(seed)
+    trees = [_step_tree(rng, F) for _ in range(8)]
+    fr = _rng(seed + 1)
+    X = fr.standard_normal((n_fit, F), dtype=np.float32)
+    y = sum(_eval_step_tree(X, t) for t in trees) + fr.normal(0.0, 0.1, n_fit)
+    Xr = _rng(seed + 2).standard_normal((n_requests, F), dtype=np.float32)
+    return X, y.astype(np.float32), Xr

@@ -272,6 +272,42 @@ int bb_predict(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
                uint8_t const *default_left, float const *value, float lr, float init,
                float *out);
 
+/* The ensemble packed for the device once, walked over any plane with the
+ * same features and bin counts: bb_predict split into its two halves.
+ * Arguments as bb_predict; the plan copies what it needs (the caller's
+ * arrays may be freed after the call). Runs through one plan serialise.
+ * Replaces cuda_predict_plan (include/bonsai/cuda/predict.hpp:29-31). */
+typedef struct bb_predict_plan bb_predict_plan;
+int bb_predict_plan_create(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+                           uint32_t n_nodes, uint32_t const *feature,
+                           uint32_t const *split_bin, uint32_t const *left,
+                           uint32_t const *right, uint8_t const *default_left,
+                           float const *value, float lr, float init, bb_predict_plan **out);
+
+/* Scores of the plan's first n_trees trees (every tree when 0) for every row
+ * of plane into host out (n_rows floats), bit-identical to bb_predict over
+ * those trees. A plane whose features or bin counts differ from the plan's
+ * is refused with BB_ERR_ARG. Replaces cuda_predict (include/bonsai/cuda/
+ * predict.hpp:33-38). */
+int bb_predict_plan_run(bb_predict_plan *plan, bb_plane const *plane, uint32_t n_trees,
+                        float *out);
+
+/* bb_predict_plan_run enqueued on a caller's stream (a cudaStream_t; NULL is
+ * the legacy default stream) into device out_device, without waiting.
+ * *launches (if not NULL) receives the kernels enqueued. Small batches use a
+ * workspace the plan owns: one launch per plan in flight at a time, and the
+ * first launch of a new largest small batch allocates it (not inside a
+ * stream capture). */
+int bb_predict_plan_launch(bb_predict_plan *plan, bb_plane const *plane, uint32_t n_trees,
+                           float *out_device, void *stream, uint32_t *launches);
+
+/* The depth the plan padded its trees to (1..10), or 0 when it kept the
+ * reference's node tables (deeper ensembles, planes over 256 u8 or 128 u16
+ * features). */
+int bb_predict_plan_depth(bb_predict_plan const *plan, uint32_t *depth);
+
+void bb_predict_plan_destroy(bb_predict_plan *plan);
+
 /* TreeSHAP contributions over a plane, FP64: out is host memory, n_rows x
  * (n_feats + 1) row-major, the last column the bias. Same tree layout as
  * bb_predict plus per-node covers (the hessian sums the booster recorded).
