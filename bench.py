@@ -204,7 +204,7 @@ SERVE_WORKLOAD = ("serving: 1,000 depth-8 trees (mse, 255 bins, lr 0.1) fit on 2
 SERVE_FIT_ROWS = 20_000
 SERVE_TREES = 1000
 SERVE_BATCHES = (1, 100, 10_000, 1_000_000)
-SHAP_BATCHES = (1, 100, 2_000)
+SHAP_BATCHES = (1, 100, 10_000, 100_000)
 LEAF = 0xFFFFFFFF
 
 
@@ -338,16 +338,34 @@ def serve_ours(args, local):
                 plan.run(q)
                 q.close()
             e2e[B] = B * K / (time.perf_counter() - t0)
-    shap, additivity = {}, {}
+    # TreeSHAP through a plan: device time per launch, then the additivity of
+    # (up to) the first 2,000 rows against an FP64 recomputation
+    splan = bb.ShapPlan(big, trees, init, 0.1)
+    shap, shap_e2e, additivity = {}, {}, {}
     for B in SHAP_BATCHES:
         pb = bb.Plane(Xp[:B], cuts, off)
-        bb.pred_contribs(pb, trees, init, 0.1)
+        phi_d = torch.empty((B, Xr.shape[1] + 1), dtype=torch.float64, device="cuda")
+        splan.launch(pb, phi_d.data_ptr(), stream.cuda_stream)
+        ms = 0.0
+        ks = max(1, min(K, 3))
+        for _ in range(ks):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            splan.launch(pb, phi_d.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        shap[B] = B * ks / (ms * 1e-3)
         t0 = time.perf_counter()
-        phi = bb.pred_contribs(pb, trees, init, 0.1)
-        shap[B] = B / (time.perf_counter() - t0)
-        m64 = margin64(pb.bins(), pb.n_bins, trees, init, 0.1)
-        additivity[B] = float(np.max(np.abs(phi.sum(axis=1) - m64)))
+        phi = splan.run(pb)
+        shap_e2e[B] = B / (time.perf_counter() - t0)
+        m = min(B, 2_000)
+        m64 = margin64(pb.bins()[:, :m], pb.n_bins, trees, init, 0.1)
+        additivity[B] = float(np.max(np.abs(phi[:m].sum(axis=1) - m64)))
         pb.close()
+    splan.close()
     # the CPU baseline: the oracle's bin-space walk (C, one thread) on a sample
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -370,6 +388,7 @@ def serve_ours(args, local):
         "predict_rows_per_s": {str(k): v for k, v in dev.items()},
         "predict_e2e_rows_per_s": {str(k): v for k, v in e2e.items()},
         "shap_rows_per_s": {str(k): v for k, v in shap.items()},
+        "shap_e2e_rows_per_s": {str(k): v for k, v in shap_e2e.items()},
         "shap_additivity_max_abs": {str(k): v for k, v in additivity.items()},
         "e2e": {"value": e2e[n_max], "unit": "rows/s", "h2d_bytes_per_step": n_max * 28 * 4,
                 "d2h_bytes_per_step": n_max * 4},

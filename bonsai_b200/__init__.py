@@ -26,7 +26,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "PredictPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
+    "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
     "Comm", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
@@ -530,3 +530,44 @@ def pred_contribs(plane: Plane, trees: list, init: float, lr: float) -> np.ndarr
                                  ptr(cat["default_left"]), ptr(cat["value"]),
                                  ptr(cat["covers"]), lr, init, ptr(out)))
     return out
+
+
+class ShapPlan:
+    """An ensemble's TreeSHAP paths packed for the device once
+    (bb_shap_plan_*): `run` returns [n_rows, n_feats + 1] FP64 contributions
+    for any plane with the features and bin counts it was packed against."""
+
+    def __init__(self, plane: Plane, trees: list, init: float, lr: float):
+        roots, base, cat = _concat(trees, ("feature", "split_bin", "left", "right",
+                                           "default_left", "value", "covers"))
+        h = C.c_void_p()
+        check(lib().bb_shap_plan_create(plane.h, len(trees), ptr(roots), base,
+                                        ptr(cat["feature"]), ptr(cat["split_bin"]),
+                                        ptr(cat["left"]), ptr(cat["right"]),
+                                        ptr(cat["default_left"]), ptr(cat["value"]),
+                                        ptr(cat["covers"]), lr, init, C.byref(h)))
+        self.h = h
+
+    def run(self, plane: Plane) -> np.ndarray:
+        out = np.empty((plane.n_rows, plane.n_feats + 1), np.float64)
+        check(lib().bb_shap_plan_run(self.h, plane.h, ptr(out)))
+        return out
+
+    def launch(self, plane: Plane, out_ptr: int, stream_ptr: int = 0) -> int:
+        """Enqueues the contributions into device memory at out_ptr
+        (n_rows x (n_feats + 1) doubles); returns the kernels launched."""
+        k = C.c_uint32()
+        check(lib().bb_shap_plan_launch(self.h, plane.h, C.c_void_p(out_ptr),
+                                        C.c_void_p(stream_ptr), C.byref(k)))
+        return k.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_shap_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

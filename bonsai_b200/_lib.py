@@ -112,6 +112,12 @@ def lib() -> C.CDLL:
         L.bb_predict_plan_depth.argtypes = [vp, C.POINTER(C.c_uint32)]
         L.bb_predict_plan_destroy.argtypes = [vp]
         L.bb_predict_plan_destroy.restype = None
+        L.bb_shap_plan_create.argtypes = [vp, C.c_uint32, vp, C.c_uint32] + [vp] * 7 + [
+            C.c_float, C.c_float, C.POINTER(vp)]
+        L.bb_shap_plan_run.argtypes = [vp, vp, vp]
+        L.bb_shap_plan_launch.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_uint32)]
+        L.bb_shap_plan_destroy.argtypes = [vp]
+        L.bb_shap_plan_destroy.restype = None
         _lib = L
     return _lib
 

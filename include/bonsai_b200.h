@@ -326,6 +326,35 @@ int bb_pred_contribs(bb_plane const *plane, uint32_t n_trees, uint32_t const *ro
                      uint8_t const *default_left, float const *value, float const *cover,
                      float lr, float init, double *out);
 
+/* The TreeSHAP paths of an ensemble packed for the device once, evaluated
+ * over any plane with the same features and bin counts: bb_pred_contribs
+ * split into its two halves. Arguments and limits as bb_pred_contribs; the
+ * plan copies what it needs. Results are bit-identical run to run; runs
+ * through one plan serialise. Replaces cuda_shap_plan + cuda_pred_contribs
+ * (include/bonsai/cuda/shap.hpp:31-43). */
+typedef struct bb_shap_plan bb_shap_plan;
+int bb_shap_plan_create(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
+                        uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
+                        uint32_t const *left, uint32_t const *right,
+                        uint8_t const *default_left, float const *value, float const *cover,
+                        float lr, float init, bb_shap_plan **out);
+
+/* Contributions for every row of plane into host out (n_rows x (n_feats + 1)
+ * doubles, bias last). A plane whose features or bin counts differ from the
+ * plan's is refused with BB_ERR_ARG. */
+int bb_shap_plan_run(bb_shap_plan *plan, bb_plane const *plane, double *out);
+
+/* bb_shap_plan_run enqueued on a caller's stream (a cudaStream_t; NULL is
+ * the legacy default stream) into device out_device, without waiting.
+ * *launches (if not NULL) receives the kernels enqueued. Small batches use a
+ * workspace the plan owns: one launch per plan in flight at a time, and the
+ * first launch of a new largest small batch allocates it (not inside a
+ * stream capture). */
+int bb_shap_plan_launch(bb_shap_plan *plan, bb_plane const *plane, double *out_device,
+                        void *stream, uint32_t *launches);
+
+void bb_shap_plan_destroy(bb_shap_plan *plan);
+
 /* Ensemble predict that allocates no device memory. No counterpart in the
  * reference: it exists for callers that may not call cudaMalloc / cudaFree on
  * their serving path -- a host whose device memory belongs to another

@@ -203,3 +203,87 @@ def test_device_contribs_refuses_wide_plane(bb):
                            rng.normal(0, 1, 64).astype(np.float32), np.ones(64, np.float32))
     with pytest.raises(bb.ConfigError):
         bb.pred_contribs(plane, [t], 0.0, 1.0)
+
+
+@pytest.mark.gpu
+def test_shap_plan_over_batches(bb):
+    """A plan packed once scores planes of 1 to 20,640 rows: the same
+    contributions as the full-plane call (row tiles, path lanes and path
+    splits change with the batch, so agreement is to FP64 rounding), the
+    same bits on a repeated run, and a plane of another shape is refused."""
+    from bonsai_b200 import synth
+    d = load_golden("small_regression.npz")
+    X, y = synth.regression_small()
+    plane = bb.Plane(X, d["cuts"], d["cut_off"])
+    b = bb.Booster(plane, y, bb.TrainParams(max_depth=6, learning_rate=0.1), max_trees=100)
+    b.update(100)
+    trees = b.trees()
+    full = bb.pred_contribs(plane, trees, b.init_score, 0.1)
+    np.testing.assert_allclose(full[:1024], d["contribs"], rtol=RTOL, atol=ATOL)
+    plan = bb.ShapPlan(plane, trees, b.init_score, 0.1)
+    for n in (1, 37, 500, 5_000, len(X)):
+        p = bb.Plane(X[:n], d["cuts"], d["cut_off"])
+        phi = plan.run(p)
+        np.testing.assert_allclose(phi, full[:n], rtol=RTOL, atol=ATOL)
+        assert np.array_equal(phi, plan.run(p))
+    other = bb.Plane(X[:, :7], d["cuts"][:d["cut_off"][7]], d["cut_off"][:8])
+    with pytest.raises(bb.BonsaiError):
+        plan.run(other)
+
+
+def chain_tree(rng, n_bins, depth):
+    """A tree whose main path splits on `depth` distinct features (each
+    right child a leaf), covers splitting each parent's at random."""
+    from bonsai_b200 import Tree
+    feats = rng.permutation(len(n_bins))[:depth]
+    feature, split, left, right, dl, value, cover = [], [], [], [], [], [], []
+
+    def node(c):
+        feature.append(LEAF)
+        split.append(0)
+        left.append(0)
+        right.append(0)
+        dl.append(0)
+        value.append(float(np.float32(rng.standard_normal())))
+        cover.append(c)
+        return len(feature) - 1
+
+    cur = node(1000.0)
+    for f in feats:
+        f = int(f)
+        c = cover[cur]
+        u = rng.uniform(0.2, 0.8)
+        feature[cur] = f
+        split[cur] = int(rng.integers(max(int(n_bins[f]) - 1, 1)))
+        dl[cur] = int(rng.random() < 0.5)
+        a = node(c * u)
+        b = node(c - c * u)
+        left[cur], right[cur] = (a, b) if rng.random() < 0.5 else (b, a)
+        cur = a
+    n = len(feature)
+    return Tree(feature=np.array(feature, np.uint32), value=np.array(value, np.float32),
+                left=np.array(left, np.uint32), right=np.array(right, np.uint32),
+                default_left=np.array(dl, np.uint8), gains=np.zeros(n, np.float32),
+                covers=np.array(cover, np.float32), split_bin=np.array(split, np.uint32),
+                depth=depth)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("depth,n", [(12, 3), (12, 2_000), (24, 3), (24, 2_000)])
+def test_shap_plan_long_paths(bb, depth, n):
+    """Paths of 12 and 24 distinct features (16- and 32-element records)
+    against the numpy path form, over codes with missing values."""
+    rng = np.random.Generator(np.random.PCG64(91 + depth + n))
+    F = 30
+    nb = rng.integers(3, 200, F).astype(np.uint32)
+    codes = np.empty((F, n), np.uint8)
+    for f in range(F):
+        c = rng.integers(0, nb[f] - 1, n)
+        c[rng.random(n) < 0.1] = nb[f] - 1
+        codes[f] = c
+    off = np.concatenate([[0], np.cumsum(nb)]).astype(np.uint32)
+    plane = bb.Plane.from_bins(codes, np.arange(off[-1], dtype=np.float32), off)
+    trees = [chain_tree(rng, nb, depth) for _ in range(5)]
+    phi = bb.ShapPlan(plane, trees, 0.25, 0.2).run(plane)
+    ref = shap_numpy(codes.T.astype(np.int64), nb.astype(np.int64) - 1, trees, 0.25, 0.2)
+    np.testing.assert_allclose(phi, ref, rtol=RTOL, atol=1e-11)
