@@ -56,7 +56,7 @@ constexpr uint32_t k_max_path       = 32; // merged elements per path
 constexpr uint32_t k_max_gauss      = 16;
 constexpr uint32_t k_max_shap_feats = 128;
 constexpr uint32_t k_sms            = 148;
-constexpr size_t   k_chunk_budget   = 24576;
+constexpr size_t   k_chunk_budget   = 16384;
 constexpr size_t   k_max_ws_bytes   = size_t{256} << 20;
 
 // One merged path element: the feature and whether the missing (last) bin
@@ -107,23 +107,28 @@ __global__ void __launch_bounds__(128)
     uint32_t const lane = t & (PL - 1u);
     auto *const    phi_s   = reinterpret_cast<double *>(smem);             // [F + 1][T]
     auto *const    heads_s = reinterpret_cast<PathHead *>(phi_s + ((F + 1) * T));
-    auto *const    elems_s = reinterpret_cast<PathElem *>(heads_s + chunk); // [chunk][K]
-    auto *const    codes_s = reinterpret_cast<uint16_t *>(elems_s + (chunk * K)); // [F][rpb]
-    auto *const    last_s  = reinterpret_cast<uint32_t *>(codes_s + (((F * rpb) + 1) & ~1u));
+    // path j's elements at elems_s[j * (K + 1)]: the odd stride puts the
+    // paths of different lanes on different banks
+    auto *const    elems_s = reinterpret_cast<PathElem *>(heads_s + chunk);
+    // row rl's code of feature f at codes_s[f * (rpb + 1) + rl]: lanes of one
+    // row reading different features land on different banks
+    auto *const    codes_s = reinterpret_cast<uint16_t *>(elems_s + (chunk * (K + 1)));
+    auto *const    last_s  = reinterpret_cast<uint32_t *>(codes_s + (((F * (rpb + 1)) + 1) & ~1u));
     uint64_t const row0 = static_cast<uint64_t>(blockIdx.x) * rpb;
     uint64_t const row  = row0 + rl;
 
     for (uint32_t i = t; i < F * rpb; i += T)
     {
-        uint32_t const f = i / rpb;
-        uint64_t const r = row0 + (i - (f * rpb));
+        uint32_t const f  = i / rpb;
+        uint32_t const rr = i - (f * rpb);
+        uint64_t const r  = row0 + rr;
         uint32_t       c = 0;
         if (r < n_rows)
         {
             c = bins8 != nullptr ? bins8[(static_cast<uint64_t>(f) * n_pad) + r]
                                  : bins16[(static_cast<uint64_t>(f) * n_pad) + r];
         }
-        codes_s[i] = static_cast<uint16_t>(c);
+        codes_s[(f * (rpb + 1)) + rr] = static_cast<uint16_t>(c);
     }
     __shared__ double gx_s[k_max_gauss];
     __shared__ double gw_s[k_max_gauss];
@@ -158,7 +163,8 @@ __global__ void __launch_bounds__(128)
             uint32_t const ne = nc * K;
             for (uint32_t i = t; i < ne; i += T)
             {
-                ed[i] = es[i];
+                uint32_t const j = i / K;
+                ed[i + j]        = es[i];
             }
         }
         __syncthreads();
@@ -169,7 +175,7 @@ __global__ void __launch_bounds__(128)
         for (uint32_t j = lane; j < nc; j += PL)
         {
             PathHead const  h = heads_s[j];
-            PathElem const *e = elems_s + (j * K);
+            PathElem const *e = elems_s + (j * (K + 1));
             uint32_t const  n = h.count;
             double          z[K];
             double          d[K];
@@ -186,7 +192,7 @@ __global__ void __launch_bounds__(128)
                 {
                     PathElem const x  = e[i];
                     uint32_t const f  = x.fm & 0x7FFFFFFFu;
-                    uint32_t const bn = codes_s[(f * rpb) + rl];
+                    uint32_t const bn = codes_s[(f * (rpb + 1)) + rl];
                     bool const     on = bn == last_s[f] ? (x.fm >> 31) != 0
                                                         : (bn >= (x.lohi & 0xFFFFu) &&
                                                            bn <= (x.lohi >> 16));
@@ -614,75 +620,79 @@ void shap_check_plane(bb_shap_plan const &pl, Plane const &p)
     }
 }
 
-template <uint32_t K> void launch_tile(dim3 grid, uint32_t T, size_t smem, cudaStream_t s,
-                                        Plane const &p, bb_shap_plan const &pl, uint32_t pps,
-                                        uint32_t chunk, uint32_t lane_shift, double *out,
-                                        double *ws)
+using TileFn = void (*)(uint8_t const *, uint16_t const *, uint64_t, uint64_t, uint32_t const *,
+                        uint32_t, PathHead const *, PathElem const *, uint32_t, uint32_t,
+                        uint32_t, uint32_t, Gauss, double, double, double, double *, double *);
+
+TileFn tile_fn(uint32_t K)
 {
-    check(cudaFuncSetAttribute(shap_tile_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)),
-          "cudaFuncSetAttribute");
-    shap_tile_kernel<K><<<grid, T, smem, s>>>(
-        p.u8 ? static_cast<uint8_t const *>(p.bins) : nullptr,
-        p.u8 ? nullptr : static_cast<uint16_t const *>(p.bins), p.n_pad, p.n_rows,
-        pl.last.as<uint32_t>(), pl.n_feats, pl.heads.as<PathHead>(), pl.elems.as<PathElem>(),
-        pl.n_paths, pps, chunk, lane_shift, pl.gauss, pl.lr, pl.bias, pl.init, out, ws);
+    return K == 8 ? shap_tile_kernel<8> : (K == 16 ? shap_tile_kernel<16> : shap_tile_kernel<32>);
 }
 
 // Enqueues the contributions of every row of p into out (device,
 // n_rows x (F + 1)); returns the kernels launched.
 uint32_t shap_launch(bb_shap_plan &pl, Plane const &p, double *out, cudaStream_t s)
 {
-    uint64_t const n = p.n_rows;
-    uint32_t const F = pl.n_feats;
+    uint64_t const n  = p.n_rows;
+    uint32_t const F  = pl.n_feats;
+    TileFn const   fn = tile_fn(pl.K);
     // 128 threads while their FP64 slices fit 100 KB, else 64
-    uint32_t const T = (static_cast<size_t>(F) + 1) * 128 * 8 <= 102400 ? 128u : 64u;
-    // path lanes per row: enough row tiles for two CTAs per SM, or one row
+    uint32_t const T   = (static_cast<size_t>(F) + 1) * 128 * 8 <= 102400 ? 128u : 64u;
+    size_t const   rec = sizeof(PathHead) + ((pl.K + 1ull) * sizeof(PathElem));
+    auto const chunk_of = [&](uint32_t PL)
+    { return PL * std::max<uint32_t>(1, static_cast<uint32_t>(k_chunk_budget / (rec * PL))); };
+    auto const smem_of = [&](uint32_t PL)
+    {
+        return ((static_cast<size_t>(F) + 1) * T * sizeof(double)) + (chunk_of(PL) * rec) +
+               ((((static_cast<size_t>(F) * ((T / PL) + 1)) + 1) & ~size_t{1}) * 2) + (F * 4ull);
+    };
+    // one wave of resident CTAs is the target
+    int occ = 0;
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem_of(1))),
+          "cudaFuncSetAttribute");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, static_cast<int>(T), smem_of(1)),
+          "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    uint32_t const target = static_cast<uint32_t>(std::max(occ, 1)) * k_sms;
+    // path lanes per row: raised until the row tiles fill the wave, or one row
     uint32_t lane_shift = 0;
-    while ((1u << lane_shift) < T && ceil_div(n, T >> lane_shift) < 2 * k_sms)
+    while ((1u << lane_shift) < T && ceil_div(n, T >> lane_shift) < target)
     {
         ++lane_shift;
     }
     uint32_t const PL       = 1u << lane_shift;
     uint32_t const rpb      = T >> lane_shift;
     uint32_t const row_blks = ceil_div(n, rpb);
-    size_t const   rec      = sizeof(PathHead) + (static_cast<size_t>(pl.K) * sizeof(PathElem));
-    uint32_t const chunk =
-        PL * std::max<uint32_t>(1, static_cast<uint32_t>(k_chunk_budget / (rec * PL)));
-    // split the paths when the row tiles leave SMs idle, each lane keeping
-    // at least eight paths per split
+    uint32_t const chunk    = chunk_of(PL);
+    // split the paths when the row tiles still leave the wave short, each
+    // lane keeping at least eight paths per split
     uint32_t splits = 1;
-    if (row_blks < 2 * k_sms)
+    if (row_blks < target)
     {
         uint32_t const most = std::max<uint32_t>(1, pl.n_paths / (8 * PL));
-        splits              = std::min(ceil_div(2 * k_sms, row_blks), most);
+        splits              = std::min(ceil_div(target, row_blks), most);
         size_t const per    = n * (static_cast<size_t>(F) + 1) * sizeof(double);
-        splits = static_cast<uint32_t>(std::min<size_t>(splits, std::max<size_t>(1, k_max_ws_bytes / per)));
+        splits = static_cast<uint32_t>(
+            std::min<size_t>(splits, std::max<size_t>(1, k_max_ws_bytes / per)));
     }
     uint32_t const pps = ceil_div(ceil_div(pl.n_paths, splits), chunk) * chunk;
     splits             = ceil_div(pl.n_paths, pps);
-    size_t const smem  = ((static_cast<size_t>(F) + 1) * T * sizeof(double)) + (chunk * rec) +
-                        ((((static_cast<size_t>(F) * rpb) + 1) & ~size_t{1}) * 2) + (F * 4ull);
-    double *ws = nullptr;
+    size_t const smem  = smem_of(PL);
+    double      *ws    = nullptr;
     if (splits > 1)
     {
         pl.ws.grow(static_cast<size_t>(splits) * n * (F + 1) * sizeof(double), pl.ws_cap);
         ws = pl.ws.as<double>();
     }
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)),
+          "cudaFuncSetAttribute");
     dim3 const grid(row_blks, splits);
-    double    *tile_out = splits > 1 ? nullptr : out;
-    if (pl.K == 8)
-    {
-        launch_tile<8>(grid, T, smem, s, p, pl, pps, chunk, lane_shift, tile_out, ws);
-    }
-    else if (pl.K == 16)
-    {
-        launch_tile<16>(grid, T, smem, s, p, pl, pps, chunk, lane_shift, tile_out, ws);
-    }
-    else
-    {
-        launch_tile<32>(grid, T, smem, s, p, pl, pps, chunk, lane_shift, tile_out, ws);
-    }
+    fn<<<grid, T, smem, s>>>(p.u8 ? static_cast<uint8_t const *>(p.bins) : nullptr,
+                             p.u8 ? nullptr : static_cast<uint16_t const *>(p.bins), p.n_pad,
+                             n, pl.last.as<uint32_t>(), F, pl.heads.as<PathHead>(),
+                             pl.elems.as<PathElem>(), pl.n_paths, pps, chunk, lane_shift,
+                             pl.gauss, pl.lr, pl.bias, pl.init, splits > 1 ? nullptr : out, ws);
     check(cudaGetLastError(), "shap_tile_kernel");
     if (splits == 1)
     {
