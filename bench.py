@@ -415,6 +415,8 @@ def main():
                          "(0 skips it)")
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eval-rows", type=int, default=1_000_000,
+                    help="fit: validation rows for the device validation plane's cost (0 skips)")
     ap.add_argument("--workload", default="fit", choices=["fit", "serve"])
     ap.add_argument("--batches", default=",".join(map(str, SERVE_BATCHES)),
                     help="serve: predict request batch sizes")
@@ -539,6 +541,25 @@ def main():
         plain = {"value": pms * N_ROUNDS / 1000.0, "unit": "s", "ms_per_step": pms,
                  "steps": args.compare_steps,
                  "quantised_speedup": pms / ms}
+    # the device validation plane: the same fit with a validation set of the
+    # workload's generator (seed 10,000,001) armed, every round recording its
+    # validation logloss on the device inside the round's graph
+    vplane = None
+    if args.eval_rows > 0 and not sharded:
+        from bonsai_b200 import synth
+        Xv, yv = synth.tall_binary(n=args.eval_rows, seed=10_000_001)
+        pv = bb.Plane(Xv, cuts, off)
+        be = bb.Booster(plane, yp, params, max_trees=W + K + 4)
+        be.eval_arm(pv, yv)
+        be.update(W)
+        barrier(world)
+        be.update(K)
+        ems = be.last_ms / K
+        losses = be.eval_losses()
+        be.close()
+        pv.close()
+        vplane = {"rows": args.eval_rows, "ms_per_step": ems, "overhead_ms_per_step": ems - ms,
+                  "rounds_recorded": int(len(losses)), "last_logloss": float(losses[-1])}
     peak, peak_kind = peaks()
     hist_gbs = prof["hist_bytes"] / (prof["hist_ms"] * 1e-3) / 1e9
     traffic = None
@@ -577,6 +598,7 @@ def main():
         "phases_ms": {k: prof[k] for k in ("hist_ms", "partition_ms", "find_ms", "other_ms",
                                            "total_ms")},
         "plain_form": plain,
+        "validation_plane": vplane,
         "gpu_launches": int(prof["launches"]) * K,
         "clocks": clk.summary(),
     }

@@ -27,7 +27,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
     "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
-    "Comm", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
+    "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
     "available", "LEAF",
 ]
 
@@ -380,6 +380,46 @@ class Booster:
         check(lib().bb_booster_scores(self.h, ptr(out)))
         return out
 
+    def eval_arm(self, valid: Plane, labels, init_scores=None):
+        """Arms the device validation plane (bb_booster_eval_arm): every later
+        round records its validation loss on the device. `valid` must be
+        binned with the training plane's cuts and outlive the booster."""
+        y = np.ascontiguousarray(labels, np.float32)
+        if len(y) != valid.n_rows:
+            raise ValueError("labels must hold one value per validation row")
+        init = None
+        if init_scores is not None:
+            init = np.ascontiguousarray(init_scores, np.float32)
+            if init.size != valid.n_rows * self.n_classes:
+                raise ValueError("init_scores must hold n_valid x n_classes values")
+            # the device keeps one column per class
+            if self.n_classes > 1:
+                init = np.ascontiguousarray(init.reshape(valid.n_rows, self.n_classes).T)
+        check(lib().bb_booster_eval_arm(self.h, valid.h, ptr(y),
+                                        None if init is None else ptr(init)))
+        self.valid = valid
+
+    def eval_losses(self) -> np.ndarray:
+        """The validation loss of every round since eval_arm."""
+        n = C.c_uint32()
+        check(lib().bb_booster_eval_losses(self.h, None, 0, C.byref(n)))
+        out = np.empty(n.value, np.float32)
+        if n.value:
+            check(lib().bb_booster_eval_losses(self.h, ptr(out), n.value, C.byref(n)))
+        return out
+
+    def eval_scores(self) -> np.ndarray:
+        """The validation raw scores: n_valid, or n_valid x n_classes."""
+        K = self.n_classes
+        n = self.valid.n_rows
+        out = np.empty((n, K) if K > 1 else n, np.float32)
+        check(lib().bb_booster_eval_scores(self.h, ptr(out)))
+        return out
+
+    def truncate(self, n_rounds: int):
+        """Keeps the first n_rounds rounds (bb_booster_truncate)."""
+        check(lib().bb_booster_truncate(self.h, n_rounds))
+
     def leaf_ids(self) -> np.ndarray:
         out = np.empty(self.plane.n_rows, np.uint32)
         check(lib().bb_booster_leaf_ids(self.h, ptr(out)))
@@ -401,6 +441,42 @@ class Booster:
             self.close()
         except Exception:
             pass  # interpreter shutdown: the library may be gone already
+
+
+def early_stop_round(losses, patience: int):
+    """The reference's early-stopping rule over a loss record
+    (src/cli/pipeline.cpp:452-462): the best round is the first with the
+    lowest loss so far; the fit stops at the first round `patience` rounds
+    past the best. Returns (rounds to keep, stopped)."""
+    best, best_i = 0.0, 0
+    for i, loss in enumerate(losses):
+        if i == 0 or loss < best:
+            best, best_i = float(loss), i
+        elif i - best_i >= patience:
+            return best_i + 1, True
+    return len(losses), False
+
+
+def fit_early_stopping(booster: "Booster", valid: Plane, labels, n_iters: int, patience: int,
+                       check_every: int = 16) -> int:
+    """Boosts up to n_iters rounds with the validation loss recorded on the
+    device, reading the record every `check_every` rounds, and keeps the
+    rounds the reference's early-stopping rule keeps (bb_booster_truncate).
+    Rounds run past the stopping point only cost time: the kept model is the
+    one the per-round rule keeps. Returns the rounds kept."""
+    if patience <= 0:
+        raise ValueError("patience must be positive")
+    booster.eval_arm(valid, labels)
+    done = 0
+    while done < n_iters:
+        step = min(check_every, n_iters - done)
+        booster.update(step)
+        done += step
+        keep, stopped = early_stop_round(booster.eval_losses(), patience)
+        if stopped:
+            booster.truncate(keep)
+            return keep
+    return done
 
 
 def grow_tree(plane: Plane, params: TrainParams, grad, hess, rows=None):

@@ -118,6 +118,10 @@ def lib() -> C.CDLL:
         L.bb_shap_plan_launch.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_uint32)]
         L.bb_shap_plan_destroy.argtypes = [vp]
         L.bb_shap_plan_destroy.restype = None
+        L.bb_booster_eval_arm.argtypes = [vp, vp, vp, vp]
+        L.bb_booster_eval_losses.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.bb_booster_eval_scores.argtypes = [vp, vp]
+        L.bb_booster_truncate.argtypes = [vp, C.c_uint32]
         _lib = L
     return _lib
 

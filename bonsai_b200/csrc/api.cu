@@ -128,6 +128,120 @@ __global__ void softmax_gradient_kernel(float const *__restrict__ scores,
     }
 }
 
+// ---- the validation plane ------------------------------------------------
+// CudaDeviceContext::eval_begin / eval_accumulate (src/cuda/detail/
+// device_context.cu:1666-1760): each round walks its new tree(s) over the
+// validation rows, adds lr x leaf to their scores (scores[i] += lr * value,
+// accumulate_last_round, include/bonsai/booster.hpp:995-1006) and records the
+// round's loss -- without leaving the device, so it runs inside the round's
+// CUDA graph. The loss terms are the reference's device forms
+// (eval_loss_pass1_kernel, src/cuda/detail/kernels.cuh:1062-1103: squared
+// error in FP64, logloss in float), and softmax cross-entropy from the
+// double max and exp of logloss_from_scores (include/bonsai/
+// multiclass_booster.hpp:545-559); per-row terms summed in FP64 in a fixed
+// order (grid-stride per thread, a fixed tree per block, blocks in order).
+
+constexpr uint32_t k_eval_threads = 256;
+constexpr uint32_t k_eval_blocks  = 1024;
+
+template <typename BinT>
+__global__ void __launch_bounds__(k_eval_threads)
+    eval_walk_kernel(BinT const *__restrict__ bins, uint64_t n_pad, uint64_t n,
+                     uint32_t const *__restrict__ n_bins, TreeOut slots, uint32_t cap,
+                     uint32_t const *round, uint32_t K, float lr, int objective,
+                     float const *__restrict__ labels, float *__restrict__ vs,
+                     double *__restrict__ partial)
+{
+    __shared__ double red[k_eval_threads];
+    uint32_t const    t_end = *round; // this round's trees are [t_end - K, t_end)
+    double            acc   = 0.0;
+    for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x; r < n;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    {
+        for (uint32_t k = 0; k < K; ++k)
+        {
+            uint64_t const off = static_cast<uint64_t>(t_end - K + k) * cap;
+            uint32_t       idx = 0;
+            for (uint32_t step = 0; step < cap && slots.feature[off + idx] != k_leaf_flag; ++step)
+            {
+                uint32_t const f = slots.feature[off + idx];
+                uint32_t const b = bins[(static_cast<uint64_t>(f) * n_pad) + r];
+                idx = routes_left(b, n_bins[f] - 1, slots.split_bin[off + idx],
+                                  slots.default_left[off + idx] != 0)
+                          ? slots.left[off + idx]
+                          : slots.right[off + idx];
+            }
+            float *sk = vs + (static_cast<uint64_t>(k) * n) + r;
+            *sk       = *sk + (lr * slots.value[off + idx]);
+        }
+        float const y = labels[r];
+        if (objective == 0)
+        {
+            double const d = static_cast<double>(vs[r]) - static_cast<double>(y);
+            acc += d * d;
+        }
+        else if (objective == 1)
+        {
+            float const s  = vs[r];
+            float const ax = fabsf(s);
+            acc += fmaxf(0.0F, s) + log1pf(expf(-ax)) - (y * s);
+        }
+        else
+        {
+            double maxv = vs[r];
+            for (uint32_t k = 1; k < K; ++k)
+            {
+                maxv = fmax(maxv, static_cast<double>(vs[(static_cast<uint64_t>(k) * n) + r]));
+            }
+            double sum = 0.0;
+            for (uint32_t k = 0; k < K; ++k)
+            {
+                sum += exp(static_cast<double>(vs[(static_cast<uint64_t>(k) * n) + r]) - maxv);
+            }
+            long const     lab = lround(y);
+            uint32_t const c =
+                lab >= 0 && static_cast<uint64_t>(lab) < K ? static_cast<uint32_t>(lab) : 0;
+            acc -= (static_cast<double>(vs[(static_cast<uint64_t>(c) * n) + r]) - maxv) - log(sum);
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (uint32_t w = k_eval_threads / 2; w > 0; w >>= 1)
+    {
+        if (threadIdx.x < w)
+        {
+            red[threadIdx.x] += red[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        partial[blockIdx.x] = red[0];
+    }
+}
+
+// The round's loss: the block partials in block order, / n, as float, into
+// losses[*count] (count advances; rounds past cap are not recorded).
+__global__ void eval_finish_kernel(double const *partial, uint32_t n_blocks, uint64_t n,
+                                   float *losses, uint32_t *count, uint32_t cap)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+    {
+        return;
+    }
+    double total = 0.0;
+    for (uint32_t b = 0; b < n_blocks; ++b)
+    {
+        total += partial[b];
+    }
+    uint32_t const c = *count;
+    if (c < cap)
+    {
+        losses[c] = static_cast<float>(total / static_cast<double>(n));
+    }
+    *count = c + 1;
+}
+
 __global__ void iota_kernel(uint32_t *rows, uint64_t n)
 {
     uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
@@ -327,10 +441,68 @@ struct bb_booster
     cudaGraphExec_t             graph     = nullptr;
     cudaEvent_t                 ev0{}, ev1{};
     float                       last_ms = 0.0F;
+    bool                        truncated = false;
+    bool                        sharded   = false;
+    // the validation plane (armed by bb_booster_eval_arm)
+    bb::Plane const            *vplane   = nullptr;
+    float                      *vlabels  = nullptr;
+    float                      *vscores  = nullptr; // K columns, class-major
+    float                      *vlosses  = nullptr; // one per round since arming
+    uint32_t                   *vcount   = nullptr;
+    double                     *vpartial = nullptr;
+    uint32_t                    vcap     = 0;
+
+    void round_body()
+    {
+        grow_round();
+        if (vplane != nullptr)
+        {
+            eval_round();
+        }
+    }
+
+    void eval_round()
+    {
+        uint64_t const n    = vplane->n_rows;
+        uint32_t const grid = static_cast<uint32_t>(
+            std::min<uint64_t>(k_eval_blocks, std::max<uint64_t>(1, (n + 255) / 256)));
+        if (vplane->u8)
+        {
+            eval_walk_kernel<uint8_t><<<grid, k_eval_threads, 0, stream>>>(
+                static_cast<uint8_t const *>(vplane->bins), vplane->n_pad, n, vplane->n_bins,
+                trees.t, trees.cap, round, n_classes, lr, objective, vlabels, vscores,
+                vpartial);
+        }
+        else
+        {
+            eval_walk_kernel<uint16_t><<<grid, k_eval_threads, 0, stream>>>(
+                static_cast<uint16_t const *>(vplane->bins), vplane->n_pad, n, vplane->n_bins,
+                trees.t, trees.cap, round, n_classes, lr, objective, vlabels, vscores,
+                vpartial);
+        }
+        BB_LAUNCH("eval_walk_kernel");
+        eval_finish_kernel<<<1, 32, 0, stream>>>(vpartial, grid, n, vlosses, vcount, vcap);
+        BB_LAUNCH("eval_finish_kernel");
+    }
+
+    void release_eval()
+    {
+        void *ps[] = {vlabels, vscores, vlosses, vcount, vpartial};
+        for (void *q : ps)
+        {
+            cudaFree(q);
+        }
+        vlabels  = nullptr;
+        vscores  = nullptr;
+        vlosses  = nullptr;
+        vcount   = nullptr;
+        vpartial = nullptr;
+        vplane   = nullptr;
+    }
 
     // gh always holds the gradients of the current scores: computed once at
     // creation, then by each round's final walk for the next round
-    void round_body()
+    void grow_round()
     {
         uint64_t const n = plane->n_rows;
         if (objective == 2)
@@ -459,6 +631,7 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     if (red != nullptr)
     {
         b->grower->set_shard(red, row_offset, total_rows);
+        b->sharded = true;
     }
     b->scratch.alloc(b->grower->max_nodes(), 1);
     b->trees.alloc(b->grower->max_nodes(), max_trees * K); // round-major: r * K + k
@@ -758,6 +931,7 @@ extern "C"
             {
                 need(b->n_trees + (n_iters * b->n_classes) <= b->trees.n,
                      "bb_booster_update: tree capacity");
+                need(!b->truncated, "bb_booster_update: the booster was truncated");
                 if (b->use_graph && b->graph == nullptr)
                 {
                     cudaGraph_t g;
@@ -933,6 +1107,121 @@ extern "C"
             });
     }
 
+    int bb_booster_eval_arm(bb_booster *b, bb_plane const *valid, float const *labels,
+                            float const *init_scores)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr && valid != nullptr && labels != nullptr,
+                     "bb_booster_eval_arm: null argument");
+                if (b->sharded)
+                {
+                    throw ConfigError("bb_booster_eval_arm: a row-sharded fit has no "
+                                      "validation plane; score the model with a predict plan");
+                }
+                Plane const &v = valid->p;
+                Plane const &t = *b->plane;
+                need(v.n_feats == t.n_feats && v.u8 == t.u8 &&
+                         std::equal(t.h_cut_off, t.h_cut_off + t.n_feats + 1, v.h_cut_off) &&
+                         std::equal(t.h_cuts, t.h_cuts + t.h_cut_off[t.n_feats], v.h_cuts),
+                     "bb_booster_eval_arm: the validation plane was not binned with the "
+                     "training plane's cuts");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                b->release_eval();
+                uint64_t const n = v.n_rows;
+                uint32_t const K = b->n_classes;
+                b->vcap          = b->trees.n / K;
+                b->vlabels       = dmalloc<float>(n);
+                b->vscores       = dmalloc<float>(n * K);
+                b->vlosses       = dmalloc<float>(b->vcap);
+                b->vcount        = dmalloc<uint32_t>(1);
+                b->vpartial      = dmalloc<double>(k_eval_blocks);
+                BB_CHECK(cudaMemcpyAsync(b->vlabels, labels, n * 4, cudaMemcpyHostToDevice,
+                                         b->stream));
+                if (init_scores != nullptr)
+                {
+                    BB_CHECK(cudaMemcpyAsync(b->vscores, init_scores, n * K * 4,
+                                             cudaMemcpyHostToDevice, b->stream));
+                }
+                else
+                {
+                    for (uint32_t k = 0; k < K; ++k)
+                    {
+                        fill_kernel<<<blocks(n), 256, 0, b->stream>>>(
+                            b->vscores + (k * n), K > 1 ? b->init_k[k] : b->init, n);
+                        BB_LAUNCH("fill_kernel");
+                    }
+                }
+                BB_CHECK(cudaMemsetAsync(b->vcount, 0, 4, b->stream));
+                b->vplane = &v;
+                // a captured round without the eval step is stale
+                if (b->graph != nullptr)
+                {
+                    BB_CHECK(cudaGraphExecDestroy(b->graph));
+                    b->graph = nullptr;
+                }
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+            });
+    }
+
+    int bb_booster_eval_losses(bb_booster const *b, float *out, uint32_t cap, uint32_t *n)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr && n != nullptr && (out != nullptr || cap == 0),
+                     "bb_booster_eval_losses: null argument");
+                need(b->vplane != nullptr, "bb_booster_eval_losses: no validation plane armed");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                uint32_t c = 0;
+                BB_CHECK(cudaMemcpy(&c, b->vcount, 4, cudaMemcpyDeviceToHost));
+                c  = std::min(c, b->vcap);
+                *n = c;
+                uint32_t const m = std::min(c, cap);
+                if (m > 0)
+                {
+                    BB_CHECK(cudaMemcpy(out, b->vlosses, m * 4ull, cudaMemcpyDeviceToHost));
+                }
+            });
+    }
+
+    int bb_booster_eval_scores(bb_booster const *b, float *out)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr && out != nullptr, "bb_booster_eval_scores: null argument");
+                need(b->vplane != nullptr, "bb_booster_eval_scores: no validation plane armed");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                uint64_t const n = b->vplane->n_rows;
+                uint32_t const K = b->n_classes;
+                std::vector<float> cm(n * K);
+                BB_CHECK(cudaMemcpy(cm.data(), b->vscores, n * K * 4, cudaMemcpyDeviceToHost));
+                for (uint64_t i = 0; i < n; ++i)
+                {
+                    for (uint32_t k = 0; k < K; ++k)
+                    {
+                        out[(i * K) + k] = cm[(k * n) + i];
+                    }
+                }
+            });
+    }
+
+    int bb_booster_truncate(bb_booster *b, uint32_t n_rounds)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr, "bb_booster_truncate: null argument");
+                need(n_rounds * b->n_classes <= b->n_trees,
+                     "bb_booster_truncate: more rounds than the booster ran");
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                b->n_trees   = n_rounds * b->n_classes;
+                b->truncated = true;
+            });
+    }
+
     void bb_booster_destroy(bb_booster *b)
     {
         if (b == nullptr)
@@ -944,6 +1233,7 @@ extern "C"
         {
             cudaGraphExecDestroy(b->graph);
         }
+        b->release_eval();
         b->grower.reset();
         b->scratch.release();
         b->trees.release();

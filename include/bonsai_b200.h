@@ -154,6 +154,33 @@ int bb_booster_leaf_ids(bb_booster const *b, uint32_t *out);
 /* Device time of the last bb_booster_update, in milliseconds. */
 int bb_booster_last_ms(bb_booster const *b, float *ms);
 
+/* Arms the booster's validation plane: valid is a plane binned with the
+ * training plane's cuts (it must outlive the booster), labels its host labels
+ * (class ids for softmax), init_scores its starting raw scores (host,
+ * n_valid x K row-major) or NULL for the booster's initial scores. From the
+ * next round on, every round walks its new tree(s) over the plane, adds
+ * lr x leaf to the validation scores and records the round's loss on the
+ * device -- mean squared error, logloss, or softmax cross-entropy, by the
+ * booster's objective -- inside the round's CUDA graph, with no host round
+ * trip. Re-arming starts a new loss record. A row-sharded booster refuses
+ * (BB_ERR_CONFIG). Replaces the eval plane (CudaDeviceContext::eval_begin /
+ * eval_accumulate, src/cuda/detail/device_context.cu:1666-1760) behind
+ * Booster::begin_resident_validation / accumulate_last_round_resident
+ * (include/bonsai/booster.hpp:1008-1021). */
+int bb_booster_eval_arm(bb_booster *b, bb_plane const *valid, float const *labels,
+                        float const *init_scores);
+
+/* The validation losses recorded since arming, one per round, into host out
+ * (the first min(cap, *n)); *n receives how many rounds were recorded. */
+int bb_booster_eval_losses(bb_booster const *b, float *out, uint32_t cap, uint32_t *n);
+
+/* The current validation raw scores (host, n_valid x K row-major). */
+int bb_booster_eval_scores(bb_booster const *b, float *out);
+
+/* Keeps the first n_rounds rounds' trees (early stopping's truncate,
+ * src/cli/pipeline.cpp:458-461); a truncated booster runs no more rounds. */
+int bb_booster_truncate(bb_booster *b, uint32_t n_rounds);
+
 /* Per-phase device time of one profiled boosting round (the reference's
  * BONSAI_CUDA_PROFILE counters, src/cuda/detail/profile.cuh:20-122): the
  * round runs like any other (its tree is kept) but synchronises between
