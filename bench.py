@@ -403,6 +403,117 @@ def serve_ours(args, local):
     print(json.dumps(line), flush=True)
 
 
+CONFIGS = {
+    # name: (workload text, rounds, rows)
+    "wide": ("wide sparse regression 1,000,000x2,000 (90% missing), leafwise 255 leaves, "
+             "256 bins, lr 0.1, all rows each round", 200, 1_000_000),
+    "multiclass": ("multiclass 581,012x54 (one-hot blocks), 7-class softmax, levelwise depth 8, "
+                   "255 bins, lr 0.1", 300, 581_012),
+}
+
+
+def config_data(name, rows):
+    from bonsai_b200 import synth
+    from bonsai_b200.binning import fit_cuts
+    if name == "wide":
+        X, y = synth.wide_sparse(n=rows)
+        cuts, off = fit_cuts(X, max_bin=256)
+        return X, y, cuts, off
+    X, y = synth.multiclass_onehot(n=rows)
+    cuts, off = fit_cuts(X, max_bin=255)
+    return X, y, cuts, off
+
+
+def config_tc(name, mod):
+    """The fit's knobs for the booster (mod = bonsai_b200) or the oracle's
+    TreeCfg (mod = oracle)."""
+    if name == "wide":
+        kw = dict(objective="mse", grower="leafwise", max_leaves=255, max_depth=255,
+                  learning_rate=0.1)
+    else:
+        kw = dict(objective="softmax", n_classes=7, grower="levelwise", max_depth=8,
+                  learning_rate=0.1)
+    return kw
+
+
+def config_main(args, name):
+    """Device time per round of the configuration's fit (K timed rounds after W
+    warm-up rounds, CUDA events on the booster's stream), x its rounds; the
+    reference's CPU booster timed on a bounded row sample beside it."""
+    import bonsai_b200 as bb
+    from bonsai_b200.build import build_library
+    text, rounds, rows = CONFIGS[name]
+    rows = args.rows if args.rows != 10_000_000 else rows
+    W, K = max(3, args.warmup), max(1, args.steps)
+    X, y, cuts, off = config_data(name, rows)
+    if args.impl == "reference":
+        cb = config_reference(name, X, y, cuts, off, rounds)
+        print(json.dumps({"metric": f"{name} fit s/{rounds} iters", "value": cb["value"],
+                          "unit": "s", "impl": "reference", "n_gpus": 1, "steps": K,
+                          "warmup": W, "ms_per_step": cb["value"] / rounds * 1000.0,
+                          "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": text, "rows": rows}, "cpu_baseline": cb,
+                          "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    build_library()
+    import torch
+    Xp = torch.empty(X.shape, dtype=torch.float32, pin_memory=True).numpy()
+    Xp[...] = X
+    t0 = time.perf_counter()
+    plane = bb.Plane(Xp, cuts, off)
+    params = bb.TrainParams(hist_mode=args.mode, use_graph=True, **config_tc(name, bb))
+    b = bb.Booster(plane, y, params, max_trees=W + K + 2)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    b.update(W)
+    with Clocks(0) as clk:
+        b.update(K)
+    ms = b.last_ms / K
+    prof = b.profile_round()
+    b.close()
+    value = ms * rounds / 1000.0
+    line = {"metric": f"{name} fit s/{rounds} iters", "value": value, "unit": "s", "n_gpus": 1,
+            "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.mode == "exact" else args.mode,
+            "data": "synthetic (seeded stand-in)",
+            "config": {"workload": text, "rows": rows, "features": X.shape[1],
+                       "rounds": rounds, "hist_mode": args.mode,
+                       "graph": name != "wide"},
+            "e2e": {"value": t_setup + value, "unit": "s",
+                    "h2d_bytes_per_step": X.nbytes / rounds, "d2h_bytes_per_step": 0,
+                    "setup_s": t_setup},
+            "phases_ms": {k: prof[k] for k in ("hist_ms", "partition_ms", "find_ms",
+                                               "other_ms", "total_ms")},
+            "gpu_launches": int(prof["launches"]) * K, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = config_reference(name, X, y, cuts, off, rounds)
+    print(json.dumps(line), flush=True)
+    plane.close()
+
+
+def config_reference(name, X, y, cuts, off, rounds, sample_rows=100_000, steps=2):
+    """The reference's own CPU booster (oracle/_ref, all host threads) for
+    `steps` rounds on the first sample_rows rows, per-round time scaled by
+    rows and rounds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m = min(sample_rows, len(y))
+    threads = len(os.sched_getaffinity(0))
+    ref = O.RefLib()
+    ds = ref.dataset(X[:m], y[:m], cuts, off)
+    tc = O.TreeCfg(n_iters=steps, n_threads=threads, **config_tc(name, O))
+    t0 = time.perf_counter()
+    ref.train(ds, tc)
+    per_round = (time.perf_counter() - t0) / steps
+    value = per_round * (len(y) / m) * rounds
+    return {"value": value, "unit": "s", "cores": threads, "kind": "reference",
+            "sample": f"first {m:,} rows, {steps} rounds, per-round time x "
+                      f"{len(y) / m:g} (rows) x {rounds} (rounds)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,7 +528,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
                     help="fit: validation rows for the device validation plane's cost (0 skips)")
-    ap.add_argument("--workload", default="fit", choices=["fit", "serve"])
+    ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass"])
     ap.add_argument("--batches", default=",".join(map(str, SERVE_BATCHES)),
                     help="serve: predict request batch sizes")
     ap.add_argument("--shap-batches", default=",".join(map(str, SHAP_BATCHES)),
@@ -427,6 +538,12 @@ def main():
     K = max(1, args.steps)
 
     world, rank, local = dist_init(args.gpus)
+    if args.workload in CONFIGS:
+        # one GPU; other ranks (if any) idle
+        if rank == 0:
+            config_main(args, args.workload)
+        barrier(world)
+        return
     if args.workload == "serve":
         # one replica per GPU; rank 0 reports
         if args.impl == "reference":

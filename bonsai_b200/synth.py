@@ -89,18 +89,29 @@ def tall_binary(n: int = 10_000_000, seed: int = 10_000_000, chunk: int = 1 << 2
 
 
 def wide_sparse(n: int = 1_000_000, F: int = 2_000, seed: int = 2_000,
-                missing: float = 0.9):
+                missing: float = 0.9, chunk: int = 16_384):
+    """Generated in row chunks (the 20 product terms drawn first), so the
+    float64 temporaries stay small at 1M x 2,000."""
     rng = _rng(seed)
-    X = rng.lognormal(0.0, 1.0, (n, F)).astype(np.float32)
-    X[rng.random((n, F)) < missing] = np.nan
-    Z = np.nan_to_num(X, nan=0.0).astype(np.float64)
-    y = np.zeros(n)
+    terms = []
     for _ in range(20):
         k = int(rng.integers(2, 4))
-        cols = rng.choice(F, size=k, replace=False)
-        y += np.prod(Z[:, cols], axis=1)
-    y += rng.normal(0.0, 0.1, n)
-    return X, y.astype(np.float32)
+        terms.append(rng.choice(F, size=k, replace=False))
+    X = np.empty((n, F), dtype=np.float32)
+    y = np.empty(n, dtype=np.float32)
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        m = e - s
+        Xc = rng.lognormal(0.0, 1.0, (m, F)).astype(np.float32)
+        Xc[rng.random((m, F)) < missing] = np.nan
+        Z = np.nan_to_num(Xc, nan=0.0).astype(np.float64)
+        yc = np.zeros(m)
+        for cols in terms:
+            yc += np.prod(Z[:, cols], axis=1)
+        yc += rng.normal(0.0, 0.1, m)
+        X[s:e] = Xc
+        y[s:e] = yc
+    return X, y
 
 
 def multiclass_onehot(n: int = 581_012, seed: int = 581_012, n_classes: int = 7):
