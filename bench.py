@@ -514,6 +514,108 @@ def config_reference(name, X, y, cuts, off, rounds, sample_rows=100_000, steps=2
                       f"{len(y) / m:g} (rows) x {rounds} (rounds)"}
 
 
+MANY_WORKLOAD = ("64 regression datasets of 1,000-200,000 rows x 28 (ragged-many family), "
+                 "mse, depthwise depth 6, 255 bins, lr 0.1, 100 rounds each, all in flight")
+MANY_ROUNDS = 100
+
+
+def many_main(args):
+    """The many-datasets batch: every dataset's booster on its own stream, a
+    round one CUDA graph; all boosters' rounds are launched before any is
+    waited on. Wall time of the whole batch (synchronize on both sides: the
+    fits run on 64 streams), beside the same fits run one after another."""
+    import bonsai_b200 as bb
+    from bonsai_b200 import synth
+    from bonsai_b200.build import build_library
+    sets = synth.ragged_many()
+    cuts = [bb.fit_cuts(X) for X, _ in sets]
+    if args.impl == "reference":
+        cb = many_reference(sets, cuts)
+        print(json.dumps({"metric": "64-dataset batch fit s/100 iters", "value": cb["value"],
+                          "unit": "s", "impl": "reference", "n_gpus": 1, "steps": MANY_ROUNDS,
+                          "warmup": 0, "ms_per_step": cb["value"] / MANY_ROUNDS * 1000.0,
+                          "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": MANY_WORKLOAD}, "cpu_baseline": cb,
+                          "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    build_library()
+    import torch
+    params = bb.TrainParams(max_depth=6, learning_rate=0.1, hist_mode=args.mode, use_graph=True)
+    W = max(3, args.warmup)
+
+    def fits():
+        planes = [bb.Plane(X, c, o) for (X, _), (c, o) in zip(sets, cuts)]
+        boosters = [bb.Booster(p, y, params, max_trees=W + MANY_ROUNDS + 1)
+                    for p, (_, y) in zip(planes, sets)]
+        for b in boosters:
+            b.update(W, sync=False)
+        for b in boosters:
+            b.sync()
+        return planes, boosters
+
+    planes, boosters = fits()
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        for b in boosters:
+            b.update(MANY_ROUNDS, sync=False)
+        for b in boosters:
+            b.sync()
+        torch.cuda.synchronize()
+        batch = time.perf_counter() - t0
+    launches = sum(int(b.profile_round()["launches"]) for b in boosters) * MANY_ROUNDS
+    for b in boosters:
+        b.close()
+    planes, boosters = fits()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for b in boosters:
+        b.update(MANY_ROUNDS)
+    torch.cuda.synchronize()
+    serial = time.perf_counter() - t0
+    rows = sum(len(y) for _, y in sets)
+    line = {"metric": "64-dataset batch fit s/100 iters", "value": batch, "unit": "s",
+            "n_gpus": 1, "steps": MANY_ROUNDS, "warmup": W,
+            "ms_per_step": batch / MANY_ROUNDS * 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.mode == "exact" else args.mode,
+            "data": "synthetic (seeded ragged-many family)",
+            "config": {"workload": MANY_WORKLOAD, "datasets": len(sets), "rows": rows,
+                       "hist_mode": args.mode, "timing": "wall clock, synchronized"},
+            "one_at_a_time_s": serial, "concurrency_speedup": serial / batch,
+            "e2e": {"value": batch, "unit": "s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = many_reference(sets, cuts)
+    print(json.dumps(line), flush=True)
+
+
+def many_reference(sets, cuts, every=8, steps=3):
+    """The reference's CPU booster (oracle/_ref, all host threads) on every
+    8th dataset for `steps` rounds; per-round time summed and scaled to all
+    64 datasets (by rows) and 100 rounds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.RefLib()
+    threads = len(os.sched_getaffinity(0))
+    tc = O.TreeCfg(max_depth=6, learning_rate=0.1, n_iters=steps, n_threads=threads)
+    t, r = 0.0, 0
+    for (X, y), (c, o) in list(zip(sets, cuts))[::every]:
+        ds = ref.dataset(X, y, c, o)
+        t0 = time.perf_counter()
+        ref.train(ds, tc)
+        t += (time.perf_counter() - t0) / steps
+        r += len(y)
+    total = sum(len(y) for _, y in sets)
+    value = t * (total / r) * MANY_ROUNDS
+    return {"value": value, "unit": "s", "cores": threads, "kind": "reference",
+            "sample": f"every {every}th dataset ({r:,} rows), {steps} rounds, per-round time "
+                      f"x {total / r:.3g} (rows) x {MANY_ROUNDS} (rounds)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -528,7 +630,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
                     help="fit: validation rows for the device validation plane's cost (0 skips)")
-    ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass"])
+    ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass", "many"])
     ap.add_argument("--batches", default=",".join(map(str, SERVE_BATCHES)),
                     help="serve: predict request batch sizes")
     ap.add_argument("--shap-batches", default=",".join(map(str, SHAP_BATCHES)),
@@ -538,6 +640,11 @@ def main():
     K = max(1, args.steps)
 
     world, rank, local = dist_init(args.gpus)
+    if args.workload == "many":
+        if rank == 0:
+            many_main(args)
+        barrier(world)
+        return
     if args.workload in CONFIGS:
         # one GPU; other ranks (if any) idle
         if rank == 0:

@@ -1094,7 +1094,7 @@ extern "C"
                 BB_CHECK(cudaEventSynchronize(b->ev1));
                 float ms = 0.0F;
                 BB_CHECK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
-                b->n_trees += 1;
+                b->n_trees += b->n_classes;
                 out->hist_ms      = p.hist_ms;
                 out->partition_ms = p.partition_ms;
                 out->find_ms      = p.find_ms;
