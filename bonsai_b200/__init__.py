@@ -191,6 +191,34 @@ class Plane:
         self.h = h.value
         return self
 
+    @classmethod
+    def like(cls, plane: "Plane", max_rows: int) -> "Plane":
+        """A request plane (bb_plane_create_like): `plane`'s mappers and room
+        for max_rows rows, allocated once; `refill` bins each batch into it."""
+        self = cls.__new__(cls)
+        self.cuts, self.cut_off, self.n_bins = plane.cuts, plane.cut_off, plane.n_bins
+        self.n_feats, self.n_rows, self.max_rows = plane.n_feats, 0, int(max_rows)
+        self._keep = None
+        h = C.c_void_p()
+        check(lib().bb_plane_create_like(plane.h, max_rows, C.byref(h)))
+        self.h = h.value
+        return self
+
+    def refill(self, X, x_on_device: bool = False) -> "Plane":
+        """Bins a new batch into this request plane (bb_plane_refill)."""
+        if x_on_device:
+            n, F = X.shape
+            xp = X.data_ptr()
+        else:
+            X = np.ascontiguousarray(X, dtype=np.float32)
+            n, F = X.shape
+            xp = ptr(X)
+        if F != self.n_feats:
+            raise ValueError("the batch has another feature count")
+        check(lib().bb_plane_refill(self.h, xp, n, 1 if x_on_device else 0))
+        self.n_rows = int(n)
+        return self
+
     @property
     def u8(self) -> bool:
         return bool(lib().bb_plane_is_u8(self.h))

@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
         L.bb_booster_eval_losses.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
         L.bb_booster_eval_scores.argtypes = [vp, vp]
         L.bb_booster_truncate.argtypes = [vp, C.c_uint32]
+        L.bb_plane_create_like.argtypes = [vp, C.c_uint64, C.POINTER(vp)]
+        L.bb_plane_refill.argtypes = [vp, vp, C.c_uint64, C.c_int]
         _lib = L
     return _lib
 

@@ -877,6 +877,76 @@ extern "C"
             });
     }
 
+    int bb_plane_create_like(bb_plane const *like, uint64_t max_rows, bb_plane **out)
+    {
+        return guarded(
+            [&]
+            {
+                need(like != nullptr && out != nullptr, "bb_plane_create_like: null argument");
+                need(max_rows > 0 && max_rows < (1ull << 32),
+                     "bb_plane_create_like: max_rows must be in [1, 2^32 - 1]");
+                Plane const &q  = like->p;
+                auto         pl = std::make_unique<bb_plane>();
+                Plane       &p  = pl->p;
+                // an empty plane until the first refill; sized for max_rows
+                p.n_rows   = 0;
+                p.n_pad    = 0;
+                p.n_feats  = q.n_feats;
+                p.u8       = q.u8;
+                p.cap_rows = max_rows;
+                BB_CHECK(cudaGetDevice(&p.device));
+                uint32_t const F      = q.n_feats;
+                uint32_t const n_cuts = q.h_cut_off[F];
+                p.h_cuts              = new float[n_cuts];
+                p.h_cut_off           = new uint32_t[F + 1];
+                std::memcpy(p.h_cuts, q.h_cuts, n_cuts * sizeof(float));
+                std::memcpy(p.h_cut_off, q.h_cut_off, (F + 1) * sizeof(uint32_t));
+                p.cuts    = dmalloc<float>(n_cuts);
+                p.cut_off = dmalloc<uint32_t>(F + 1);
+                p.n_bins  = dmalloc<uint32_t>(F);
+                BB_CHECK(cudaMemcpy(p.cuts, q.cuts, n_cuts * 4, cudaMemcpyDeviceToDevice));
+                BB_CHECK(cudaMemcpy(p.cut_off, q.cut_off, (F + 1) * 4, cudaMemcpyDeviceToDevice));
+                BB_CHECK(cudaMemcpy(p.n_bins, q.n_bins, F * 4, cudaMemcpyDeviceToDevice));
+                uint64_t const cap_pad = ((max_rows + 63) / 64) * 64;
+                size_t const   el      = p.u8 ? 1 : 2;
+                BB_CHECK(cudaMalloc(&p.bins, static_cast<size_t>(F) * cap_pad * el));
+                BB_CHECK(cudaMemset(p.bins, 0, static_cast<size_t>(F) * cap_pad * el));
+                uint32_t const per = k_mirror_bytes / (p.u8 ? 1 : 2);
+                p.n_tiles          = (F + per - 1) / per;
+                BB_CHECK(cudaMalloc(&p.mirror,
+                                    static_cast<size_t>(p.n_tiles) * max_rows * k_mirror_bytes));
+                // host rows go up through a staging buffer of at most 64 MB
+                uint64_t const row_bytes = static_cast<uint64_t>(F) * sizeof(float);
+                p.stage_rows             = stage_rows_for(F, max_rows);
+                BB_CHECK(cudaMalloc(&p.stage, p.stage_rows * row_bytes));
+                BB_CHECK(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+                *out = pl.release();
+            });
+    }
+
+    int bb_plane_refill(bb_plane *plane, float const *X, uint64_t n_rows, int x_on_device)
+    {
+        return guarded(
+            [&]
+            {
+                need(plane != nullptr && X != nullptr, "bb_plane_refill: null argument");
+                Plane &p = plane->p;
+                need(p.cap_rows > 0, "bb_plane_refill: not a request plane "
+                                     "(make one with bb_plane_create_like)");
+                if (n_rows == 0 || n_rows > p.cap_rows)
+                {
+                    throw ConfigError("bb_plane_refill: " + std::to_string(n_rows) +
+                                      " rows; the plane holds 1 to " +
+                                      std::to_string(p.cap_rows));
+                }
+                p.n_rows = n_rows;
+                p.n_pad  = ((n_rows + 63) / 64) * 64;
+                ingest(p, X, x_on_device != 0, p.stream, p.stage, p.stage_rows);
+                fill_mirror(p, p.stream);
+                BB_CHECK(cudaStreamSynchronize(p.stream));
+            });
+    }
+
     void bb_plane_destroy(bb_plane *plane)
     {
         if (plane == nullptr)
@@ -884,6 +954,12 @@ extern "C"
             return;
         }
         Plane &p = plane->p;
+        if (p.stream != nullptr)
+        {
+            cudaStreamSynchronize(p.stream);
+            cudaStreamDestroy(p.stream);
+        }
+        cudaFree(p.stage);
         cudaFree(p.bins);
         cudaFree(p.mirror);
         cudaFree(p.cuts);

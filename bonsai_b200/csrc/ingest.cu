@@ -160,6 +160,11 @@ void build_mirror(Plane &p, cudaStream_t stream)
     p.n_tiles          = (p.n_feats + per - 1) / per;
     size_t const bytes = static_cast<size_t>(p.n_tiles) * p.n_rows * k_mirror_bytes;
     BB_CHECK(cudaMalloc(&p.mirror, bytes));
+    fill_mirror(p, stream);
+}
+
+void fill_mirror(Plane &p, cudaStream_t stream)
+{
     dim3 const grid(ceil_div(p.n_rows, k_threads), p.n_tiles);
     if (p.u8)
     {
@@ -176,7 +181,22 @@ void build_mirror(Plane &p, cudaStream_t stream)
     BB_LAUNCH("mirror_kernel");
 }
 
-void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream)
+uint64_t stage_rows_for(uint32_t n_feats, uint64_t max_rows)
+{
+    // at most 64 MB; when a batch can take more than one chunk, every chunk
+    // starts on a tile boundary (the kernel's 16-byte code stores need the
+    // chunk's first row aligned)
+    uint64_t const row_bytes = static_cast<uint64_t>(n_feats) * sizeof(float);
+    uint64_t       rows      = std::min<uint64_t>(max_rows, (64ull << 20) / row_bytes);
+    if (rows < max_rows)
+    {
+        rows = std::max<uint64_t>(k_tile_rows, rows - (rows % k_tile_rows));
+    }
+    return std::max<uint64_t>(rows, 1);
+}
+
+void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream, float *owned_stage,
+            uint64_t owned_rows)
 {
     uint32_t const F = p.n_feats;
     // the largest per-tile cut table
@@ -221,6 +241,24 @@ void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream)
     if (x_on_device)
     {
         launch(X, p.n_rows, 0);
+        return;
+    }
+    if (owned_stage != nullptr)
+    {
+        if (owned_rows < p.n_rows && owned_rows % k_tile_rows != 0)
+        {
+            throw std::logic_error("ingest: a staging buffer that chunks must hold whole tiles");
+        }
+        // a request plane: one staging buffer the plane owns, copy then bin
+        // chunk by chunk on the one stream (no allocation)
+        uint64_t const row_bytes = static_cast<uint64_t>(F) * sizeof(float);
+        for (uint64_t r0 = 0; r0 < p.n_rows; r0 += owned_rows)
+        {
+            uint64_t const rows = std::min(owned_rows, p.n_rows - r0);
+            BB_CHECK(cudaMemcpyAsync(owned_stage, X + (r0 * F), rows * row_bytes,
+                                     cudaMemcpyHostToDevice, stream));
+            launch(owned_stage, rows, r0);
+        }
         return;
     }
     // Host input: stream it through two device staging buffers of <= 64 MB

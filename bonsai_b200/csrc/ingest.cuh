@@ -36,12 +36,31 @@ struct Plane
     // host copies of the mapper tables
     float    *h_cuts    = nullptr;
     uint32_t *h_cut_off = nullptr;
+    // a request plane (bb_plane_create_like): rows it was sized for, its
+    // staging buffer and stream; 0 / null for planes made from one matrix
+    uint64_t     cap_rows   = 0;
+    float       *stage      = nullptr;
+    uint64_t     stage_rows = 0;
+    cudaStream_t stream     = nullptr;
 };
 
-void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream);
+// owned_stage (optional): a device staging buffer of owned_rows rows the
+// caller keeps (a request plane's): host X then goes up through it with no
+// allocation, chunk after chunk on `stream`, without waiting.
+void ingest(Plane &p, float const *X, bool x_on_device, cudaStream_t stream,
+            float *owned_stage = nullptr, uint64_t owned_rows = 0);
 
 // Fills p.mirror from the feature-major codes (allocating it).
 void build_mirror(Plane &p, cudaStream_t stream);
+
+// Rows of a request plane's staging buffer for batches of up to max_rows:
+// at most 64 MB, and a whole number of bin-application tiles whenever a batch
+// can take more than one chunk.
+uint64_t stage_rows_for(uint32_t n_feats, uint64_t max_rows);
+
+// Rewrites p.mirror (already allocated for at least p.n_rows rows) from the
+// feature-major codes.
+void fill_mirror(Plane &p, cudaStream_t stream);
 
 constexpr uint32_t k_mirror_bytes = 32;
 

@@ -612,6 +612,10 @@ uint32_t plan_launch(bb_predict_plan &pl, Plane const &p, uint32_t n_trees, floa
                      cudaStream_t s)
 {
     uint64_t const n = p.n_rows;
+    if (n == 0)
+    {
+        return 0; // an empty request plane: nothing to score
+    }
     if (pl.depth == 0)
     {
         if (p.u8)
@@ -798,6 +802,10 @@ void plan_run_host(bb_predict_plan &pl, Plane const &p, uint32_t n_trees, float 
 {
     std::lock_guard<std::mutex> lock(pl.mu);
     size_t const bytes = p.n_rows * sizeof(float);
+    if (bytes == 0)
+    {
+        return;
+    }
     if (pl.out_cap < bytes)
     {
         if (pl.out != nullptr)

@@ -634,6 +634,10 @@ TileFn tile_fn(uint32_t K)
 uint32_t shap_launch(bb_shap_plan &pl, Plane const &p, double *out, cudaStream_t s)
 {
     uint64_t const n  = p.n_rows;
+    if (n == 0)
+    {
+        return 0; // an empty request plane: nothing to explain
+    }
     uint32_t const F  = pl.n_feats;
     TileFn const   fn = tile_fn(pl.K);
     // 128 threads while their FP64 slices fit 100 KB, else 64
@@ -709,6 +713,10 @@ void shap_run_host(bb_shap_plan &pl, Plane const &p, double *out)
 {
     std::lock_guard<std::mutex> lock(pl.mu);
     size_t const bytes = p.n_rows * (pl.n_feats + 1ull) * sizeof(double);
+    if (bytes == 0)
+    {
+        return;
+    }
     pl.out.grow(bytes, pl.out_cap);
     shap_launch(pl, p, pl.out.as<double>(), pl.stream);
     check(cudaMemcpyAsync(out, pl.out.p, bytes, cudaMemcpyDeviceToHost, pl.stream),

@@ -79,6 +79,20 @@ int bb_plane_download(bb_plane const *plane, uint16_t *out);
 
 void bb_plane_destroy(bb_plane *plane);
 
+/* A request plane for serving: the mappers of `like` (its cuts, bin counts
+ * and code width) and device room for up to max_rows rows, allocated once.
+ * It holds no rows until bb_plane_refill. No counterpart in the reference,
+ * whose serving path ingests a fresh device plane per request (cuda_ingest,
+ * include/bonsai/cuda/histogram_engine.hpp:41-68). */
+int bb_plane_create_like(bb_plane const *like, uint64_t max_rows, bb_plane **out);
+
+/* Bins a new batch of n_rows (1..max_rows) row-major float32 rows into a
+ * request plane, replacing its rows, with no device allocation: host X goes
+ * up through the plane's own staging buffer. Returns when the plane is
+ * ready. Predict and SHAP plans made against `like` score it directly.
+ * More rows than the plane was made for: BB_ERR_CONFIG. */
+int bb_plane_refill(bb_plane *plane, float const *X, uint64_t n_rows, int x_on_device);
+
 /* ---- training ------------------------------------------------------------ */
 
 /* The TreeConfig / BoosterConfig keys the device path reads
