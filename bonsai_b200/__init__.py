@@ -27,7 +27,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
     "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
-    "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows",
+    "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows", "fit_cuts_device",
     "available", "LEAF",
 ]
 
@@ -35,6 +35,28 @@ LEAF = 0xFFFFFFFF
 OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2}
 GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1, "leafwise": 2}
 HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
+
+
+def fit_cuts_device(X, max_bin: int = 255, n_samples: int = 200_000, seed: int = 0):
+    """fit_cuts on the device (bb_fit_cuts): the same row sample as the host
+    fit (sample_rows), the same cuts. X is a host array or a CUDA tensor."""
+    on_device = hasattr(X, "data_ptr") and getattr(X, "is_cuda", False)
+    n, F = X.shape
+    rows = sample_rows(n, n_samples, seed)
+    if on_device:
+        import torch
+        S = X if rows is None else X[torch.as_tensor(rows, device=X.device)]
+        S = S.float().contiguous()
+        sp = S.data_ptr()
+    else:
+        X = np.asarray(X, dtype=np.float32)
+        S = np.ascontiguousarray(X if rows is None else X[rows])
+        sp = ptr(S)
+    cuts = np.empty(F * max_bin, np.float32)
+    off = np.empty(F + 1, np.uint32)
+    check(lib().bb_fit_cuts(sp, S.shape[0], F, 1 if on_device else 0, max_bin, ptr(cuts),
+                            len(cuts), ptr(off)))
+    return cuts[: off[-1]].copy(), off
 
 
 def available() -> bool:

@@ -124,6 +124,8 @@ def lib() -> C.CDLL:
         L.bb_booster_truncate.argtypes = [vp, C.c_uint32]
         L.bb_plane_create_like.argtypes = [vp, C.c_uint64, C.POINTER(vp)]
         L.bb_plane_refill.argtypes = [vp, vp, C.c_uint64, C.c_int]
+        L.bb_fit_cuts.argtypes = [vp, C.c_uint64, C.c_uint32, C.c_int, C.c_uint32, vp,
+                                  C.c_uint32, vp]
         _lib = L
     return _lib
 

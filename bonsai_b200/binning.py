@@ -56,7 +56,17 @@ def cuts_from_sample(sample: np.ndarray, max_bin: int = 255) -> np.ndarray:
     working set."""
     assert max_bin > 2
     budget = max_bin - 2
-    s = np.sort(np.asarray(sample, dtype=np.float32), kind="stable")
+    s = np.asarray(sample, dtype=np.float32)
+    if s.size >= 2048:
+        # the reference's radix order (sort_floats, src/bin_mapper.cpp:115-157):
+        # order-preserving keys, so a run of zeros starts with -0.0 if any
+        b = s.view(np.uint32)
+        key = np.where((b >> 31) != 0, ~b, b ^ np.uint32(0x80000000)).astype(np.uint32)
+        key.sort()
+        s = np.where((key >> 31) != 0, key ^ np.uint32(0x80000000), ~key).astype(
+            np.uint32).view(np.float32)
+    else:
+        s = np.sort(s, kind="stable")
     if s.size:
         # run-length encode under operator<: -0.0 and +0.0 are one value
         new = np.empty(s.size, dtype=bool)

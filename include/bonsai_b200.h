@@ -61,6 +61,21 @@ int bb_select_device(uint32_t device_id);
 int bb_ingest(float const *X, uint64_t n_rows, uint32_t n_feats, int x_on_device,
               float const *cuts, uint32_t const *cut_off, bb_plane **out);
 
+/* Per-feature cuts fitted on the device from a working set S (n_rows x n_feats
+ * row-major float32, NaN allowed; host memory, or device memory when
+ * s_on_device): each column's NaN-free values sorted, run-length encoded,
+ * and cut by the reference's rules for max_bin (every distinct value within
+ * the budget of max_bin - 2 cuts, the count-weighted greedy walk when a
+ * value is at least a mean bin, else the quantile stride), closed by FLT_MAX
+ * and +inf -- the cuts BinMapper::from_sample gives the same working set
+ * (src/bin_mapper.cpp:159-252). Outputs to host: cuts (cuts_cap >=
+ * n_feats x max_bin suffices) and cut_off (n_feats + 1). The row sample for
+ * tall data is the caller's (the reference draws one shared sample,
+ * src/bin_mappers.cpp:31-44). Replaces the host fit behind cuda_ingest's
+ * mappers (the reference's ingest_fit phase). */
+int bb_fit_cuts(float const *S, uint64_t n_rows, uint32_t n_feats, int s_on_device,
+                uint32_t max_bin, float *cuts, uint32_t cuts_cap, uint32_t *cut_off);
+
 /* A plane from codes already binned on the host: feature-major codes
  * (bins[f * n_rows + r], u8 when is_u8 else u16), each below its feature's bin
  * count (checked), and the cuts they were binned with. Replaces the engine

@@ -79,3 +79,20 @@ def test_fit_cuts_matches_reference_live(ref, seed):
         cuts, off = bb.fit_cuts(X, max_bin=max_bin)
         assert np.array_equal(off, ro), max_bin
         assert np.array_equal(cuts.view(np.uint32), rc.view(np.uint32)), max_bin
+
+
+def test_fit_cuts_signed_zeros_match_reference(ref):
+    """Runs of zeros of both signs: the reference sorts samples of 2,048 or
+    more values by radix key, so the run's representative is -0.0 whenever
+    one is present; the restatement sorts the same way."""
+    import bonsai_b200 as bb
+    rng = np.random.Generator(np.random.PCG64(3))
+    n = 3000
+    X = np.stack([np.array([0.0, -0.0, 1.0] * 1000),
+                  rng.choice([-0.0, 0.0, 2.5], n),
+                  np.where(rng.random(n) < 0.5, -0.0, rng.standard_normal(n))], 1)
+    X = X.astype(np.float32)
+    rc, ro = ref.fit_cuts(X)
+    cuts, off = bb.fit_cuts(X)
+    assert np.array_equal(off, ro)
+    assert np.array_equal(cuts.view(np.uint32), rc.view(np.uint32))
