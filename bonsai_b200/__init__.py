@@ -84,6 +84,9 @@ class TrainParams:
     grower: str = "depthwise"
     max_leaves: int = 31
     n_classes: int = 0
+    # TreeConfig::interaction_constraints: feature groups, each a list of ids
+    # or the reference's string form ("0,1" or "0+1")
+    interaction_constraints: list = field(default_factory=list)
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -106,6 +109,20 @@ class TrainParams:
             c._mono = np.ascontiguousarray(self.monotone, dtype=np.int8)
             c.monotone = c._mono.ctypes.data_as(C.POINTER(C.c_int8))
             c.n_monotone = len(self.monotone)
+        if self.interaction_constraints:
+            groups = []
+            for g in self.interaction_constraints:
+                if isinstance(g, str):
+                    g = [int(x) for x in g.replace("+", ",").split(",") if x.strip()]
+                groups.append(sorted(int(x) for x in g))
+            c._ifeat = np.ascontiguousarray(
+                np.concatenate([np.asarray(g, np.uint32) for g in groups]) if groups
+                else np.zeros(0, np.uint32), dtype=np.uint32)
+            c._ioff = np.ascontiguousarray(
+                np.concatenate([[0], np.cumsum([len(g) for g in groups])]), dtype=np.uint32)
+            c.interaction_features = c._ifeat.ctypes.data_as(C.POINTER(C.c_uint32))
+            c.interaction_offsets = c._ioff.ctypes.data_as(C.POINTER(C.c_uint32))
+            c.n_interaction_groups = len(groups)
         if self.selected is not None:
             c._sel = np.ascontiguousarray(self.selected, dtype=np.uint32)
             c.selected = c._sel.ctypes.data_as(C.POINTER(C.c_uint32))

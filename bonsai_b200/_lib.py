@@ -38,6 +38,8 @@ class TrainCfg(C.Structure):
         ("selected", C.POINTER(C.c_uint32)), ("n_selected", C.c_uint32),
         ("use_graph", C.c_int32), ("record_leaf_ids", C.c_int32),
         ("grower", C.c_int32), ("max_leaves", C.c_uint32), ("n_classes", C.c_uint32),
+        ("interaction_features", C.POINTER(C.c_uint32)),
+        ("interaction_offsets", C.POINTER(C.c_uint32)), ("n_interaction_groups", C.c_uint32),
     ]
 
 

@@ -407,6 +407,50 @@ std::vector<int8_t> monotone(bb_train_cfg const &c)
     return {c.monotone, c.monotone + c.n_monotone};
 }
 
+// Interaction constraints (TreeConfig::interaction_constraints, parsed by
+// parse_interaction_groups, src/grower_impl.hpp:83-109): group g holds
+// features[offsets[g] .. offsets[g + 1]); per feature, the bit mask of the
+// groups containing it. Empty groups are dropped, as the reference drops them.
+std::vector<uint64_t> interaction(bb_train_cfg const &c, uint32_t n_feats)
+{
+    if (c.n_interaction_groups == 0)
+    {
+        return {};
+    }
+    need(c.interaction_offsets != nullptr, "interaction constraints: null offset array");
+    need(c.interaction_offsets[c.n_interaction_groups] == c.interaction_offsets[0] ||
+             c.interaction_features != nullptr,
+         "interaction constraints: null feature array");
+    std::vector<uint64_t> masks(n_feats, 0);
+    uint32_t              g = 0;
+    for (uint32_t k = 0; k < c.n_interaction_groups; ++k)
+    {
+        uint32_t const b = c.interaction_offsets[k];
+        uint32_t const e = c.interaction_offsets[k + 1];
+        need(b <= e, "interaction constraints: offsets must not decrease");
+        if (b == e)
+        {
+            continue;
+        }
+        if (g >= 64)
+        {
+            throw ConfigError("interaction constraints: at most 64 non-empty groups");
+        }
+        for (uint32_t x = b; x < e; ++x)
+        {
+            need(c.interaction_features[x] < n_feats,
+                 "interaction constraints: feature id out of range");
+            masks[c.interaction_features[x]] |= uint64_t{1} << g;
+        }
+        ++g;
+    }
+    if (g == 0)
+    {
+        return {};
+    }
+    return masks;
+}
+
 uint32_t blocks(uint64_t n, uint32_t t = 256)
 {
     return ceil_div(std::max<uint64_t>(n, 1), t);
@@ -627,6 +671,7 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     b->grower = std::make_unique<Grower>(p, grow_config(*cfg), selection(*cfg, p.n_feats),
                                          static_cast<uint32_t>(n), b->stream);
     b->grower->set_monotone(monotone(*cfg));
+    b->grower->set_interaction(interaction(*cfg, p.n_feats));
     b->grower->set_seed(cfg->seed);
     if (red != nullptr)
     {
@@ -1373,6 +1418,7 @@ extern "C"
                     Grower g(p, grow_config(*cfg), selection(*cfg, p.n_feats),
                              static_cast<uint32_t>(std::max<uint64_t>(m, 1)), s);
                     g.set_monotone(monotone(*cfg));
+                    g.set_interaction(interaction(*cfg, p.n_feats));
                     g.set_seed(cfg->seed);
                     ts.alloc(g.max_nodes(), 1);
                     g.grow(d_gh, d_rows, static_cast<uint32_t>(m), ts.t, d_leaf, d_val, 1.0F);

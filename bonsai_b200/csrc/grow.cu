@@ -548,13 +548,53 @@ __device__ __forceinline__ void warp_best(double &gain, uint32_t &order)
 // feature), each thread a few candidates. The exact form's prefix is one
 // serial FP64 chain (the reference's summation order); the quantised form's
 // is an exact integer block scan.
+// Interaction constraints (allowed_features / propagate_interaction_state,
+// src/grower_impl.hpp:114-160). fgroups[f]: the groups containing feature f
+// as a bit mask (at most 64 groups). A node may split on f when its path is
+// empty, when a group containing its whole path contains f, or when f is the
+// path's only feature.
+__device__ __forceinline__ bool interaction_allows(Node const &nd, uint64_t const *fgroups,
+                                                   uint32_t f)
+{
+    uint32_t const plen = nd.ipath & 3u;
+    return fgroups == nullptr || plen == 0 || (fgroups[f] & nd.icover) != 0 ||
+           (plen == 1 && (nd.ipath >> 2) == f);
+}
+
+// Both children's path state after the parent splits on f.
+__device__ __forceinline__ void interaction_children(Node const &par, uint64_t const *fgroups,
+                                                     uint32_t f, Node &L, Node &R)
+{
+    if (fgroups == nullptr)
+    {
+        return;
+    }
+    uint32_t const plen = par.ipath & 3u;
+    uint64_t       cover;
+    uint32_t       path;
+    if (plen == 0)
+    {
+        cover = fgroups[f];
+        path  = 1u | (f << 2);
+    }
+    else
+    {
+        cover = par.icover & fgroups[f];
+        path  = (plen == 1 && (par.ipath >> 2) == f) ? par.ipath : 2u;
+    }
+    L.icover = cover;
+    R.icover = cover;
+    L.ipath  = path;
+    R.ipath  = path;
+}
+
 template <bool Q>
 __global__ void __launch_bounds__(k_find_thr)
     find_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
                 uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
                 uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
                 TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale,
-                uint32_t const *slot_of, uint32_t cw)
+                uint32_t const *slot_of, uint32_t cw, uint64_t const *fgroups)
 {
     extern __shared__ unsigned char smem_raw[];
     __shared__ double   bg_s[k_find_thr / 32];
@@ -575,7 +615,8 @@ __global__ void __launch_bounds__(k_find_thr)
     Node const     nd   = nodes[i];
     uint32_t const nb   = sel_nb[j];
     Best           out  = {0.0, j, 0, 1, 0};
-    if (nd.gcount < 2 * tp.min_data_in_leaf || nb < 2)
+    if (nd.gcount < 2 * tp.min_data_in_leaf || nb < 2 ||
+        !interaction_allows(nd, fgroups, sel[j]))
     {
         if (tid == 0)
         {
@@ -1261,7 +1302,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
                  TreeOut t, uint32_t crows, uint32_t *bbase, bool level,
-                 uint64_t const *gleft)
+                 uint64_t const *gleft, uint64_t const *fgroups)
 {
     __shared__ uint32_t grand_s;
     uint32_t const      n_cur = ctl->n_cur;
@@ -1353,8 +1394,9 @@ __global__ void __launch_bounds__(k_plan_thr)
         uint32_t const gnr  = nd.gcount - gnl;
         uint32_t const lid  = t.left[nd.id];
         uint32_t const rid  = t.right[nd.id];
-        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0};
-        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0};
+        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0, 0};
+        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0, 0};
+        interaction_children(nd, fgroups, t.feature[nd.id], L, R);
         next[2 * k]         = L;
         next[(2 * k) + 1]   = R;
         t.cover[lid]        = static_cast<float>(gnl);
@@ -2956,7 +2998,8 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
                                    uint32_t const *slot_of, void const *pool,
                                    uint32_t total_cells, uint32_t const *sel,
                                    uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
-                                   TreeParams tp, double2 const *qscale, LeafPop p, uint32_t cw)
+                                   TreeParams tp, double2 const *qscale, LeafPop p, uint32_t cw,
+                                   uint64_t const *fgroups)
 {
     if (threadIdx.x != 0)
     {
@@ -2997,6 +3040,7 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
     }
     uint32_t const f  = sel[p.best.feature];
     int const      mc = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+    interaction_children(p.node, fgroups, f, L, R);
     if (mc != 0)
     {
         double const wl  = bounded_leaf_weight(gl, hl, tp.lambda_l1, tp.lambda_l2, p.node.lo,
@@ -3302,7 +3346,7 @@ Grower::~Grower()
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
                     tile_j_[1], bbase_,   dirs_,    btot_,    done_,    wacc_,
-                    leaf16_,  nbound_,  gleft_,   qgh16_};
+                    leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -3569,13 +3613,13 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     {
         find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_, fgroups_);
     }
     else
     {
         find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_);
+            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_, fgroups_);
     }
     BB_LAUNCH("find_kernel");
     plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
@@ -3610,7 +3654,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
                                           pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
                                           build_, brange_, bchunks_, cfg_.tp, t, crows_,
-                                          bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr);
+                                          bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr,
+                                          fgroups_);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -3937,13 +3982,13 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         {
             find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
                 ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of, cw_);
+                tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
         }
         else
         {
             find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
                 ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of, cw_);
+                tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
         }
         BB_LAUNCH("find_kernel");
         leaf_best_kernel<<<1, 64, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split ? 1 : 0);
@@ -4068,7 +4113,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                                         total_cells_ * cw_);
             leaf_totals_kernel<true><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                       total_cells_, sel_, sel_nb_, mono_, n_mono_,
-                                                      tp, qscale_, p, cw_);
+                                                      tp, qscale_, p, cw_, fgroups_);
         }
         else
         {
@@ -4076,7 +4121,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                                          total_cells_);
             leaf_totals_kernel<false><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                        total_cells_, sel_, sel_nb_, mono_,
-                                                       n_mono_, tp, qscale_, p, 1);
+                                                       n_mono_, tp, qscale_, p, 1, fgroups_);
         }
         BB_LAUNCH("leaf_totals_kernel");
         find(nodes_[1], slot_of_, c.depth + 1 < tp.max_depth);
@@ -4203,6 +4248,32 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     }
     BB_CHECK(cudaFreeAsync(scratch, s));
     BB_CHECK(cudaStreamSynchronize(s));
+}
+
+void Grower::set_interaction(std::vector<uint64_t> const &fgroups)
+{
+    if (fgroups_ != nullptr)
+    {
+        BB_CHECK(cudaFreeAsync(fgroups_, stream_));
+        fgroups_ = nullptr;
+    }
+    if (fgroups.empty())
+    {
+        return;
+    }
+    if (cfg_.level)
+    {
+        // ObliviousGrower refuses them (src/grower_impl.hpp:591-595)
+        throw ConfigError("interaction_constraints are not supported by the levelwise grower");
+    }
+    if (fgroups.size() != plane_.n_feats)
+    {
+        throw std::invalid_argument("grower: one interaction mask per feature");
+    }
+    BB_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&fgroups_), fgroups.size() * 8, stream_));
+    BB_CHECK(cudaMemcpyAsync(fgroups_, fgroups.data(), fgroups.size() * 8, cudaMemcpyHostToDevice,
+                             stream_));
+    BB_CHECK(cudaStreamSynchronize(stream_));
 }
 
 void Grower::set_monotone(std::vector<int8_t> const &m)

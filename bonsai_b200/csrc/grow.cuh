@@ -30,7 +30,11 @@ struct Node
     int64_t  qg; // quantised form: exact integer totals
     int64_t  qh;
     uint32_t gcount; // rows over every shard of the fit (count when unsharded)
-    uint32_t pad_;
+    // interaction constraints (the node's path state): the number of
+    // distinct features on its path (0, 1 or 2 for two or more) | the one
+    // feature when it is 1, << 2; and the groups that contain the whole path
+    uint32_t ipath;
+    uint64_t icover;
 };
 
 // SplitOutput (include/bonsai/split.hpp:62-69), one per (node, feature)
@@ -254,6 +258,7 @@ class Grower
     uint32_t *pcr_      = nullptr; // per frontier slot: partition chunk range
     uint32_t *nleft_    = nullptr; // per frontier slot: rows routed left
     int8_t   *mono_     = nullptr; // per feature monotone direction, or null
+    uint64_t *fgroups_  = nullptr; // per feature interaction-group mask, or null
     uint32_t  n_mono_   = 0;
     float2 const *gh_cur_ = nullptr;
     std::vector<uint32_t> off_h_;
@@ -300,6 +305,9 @@ class Grower
     }
     // per-feature monotone directions (+1 / -1 / 0), copied to the device
     void set_monotone(std::vector<int8_t> const &m);
+    // Interaction constraints: per feature, the groups containing it as a
+    // bit mask (empty: unconstrained).
+    void set_interaction(std::vector<uint64_t> const &fgroups);
     // non-null: the next grow() calls time their phases into *p (synchronous)
     void set_profile(Profile *p)
     {

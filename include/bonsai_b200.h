@@ -141,6 +141,15 @@ typedef struct
     uint32_t       max_leaves; /* leafwise: 1..512 (0: 2^max_depth, depth <= 9);
                                   max_depth <= 255 caps its depth */
     uint32_t       n_classes;  /* objective 2 (softmax): 2..16 */
+    /* interaction constraints (TreeConfig::interaction_constraints): group g
+     * holds interaction_features[interaction_offsets[g] ..
+     * interaction_offsets[g + 1]); a node splits only on features of a group
+     * containing every feature on its path, or on its path's only feature
+     * (src/grower_impl.hpp:114-160). At most 64 non-empty groups;
+     * n_interaction_groups 0: unconstrained. Depthwise and leafwise only. */
+    uint32_t const *interaction_features;
+    uint32_t const *interaction_offsets; /* n_interaction_groups + 1 */
+    uint32_t       n_interaction_groups;
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and

@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <iterator>
 #include <numeric>
+#include <string>
 #include <optional>
 #include <random>
 #include <span>
@@ -61,11 +62,6 @@ class B200DepthwiseGrower
     explicit B200DepthwiseGrower(TreeConfig const &cfg)
         : config_(cfg), feature_rng_(cfg.feature_seed)
     {
-        if (!cfg.interaction_constraints.empty())
-        {
-            throw ConfigError("interaction_constraints are not supported by the B200 "
-                              "grower; use the host depthwise grower");
-        }
     }
     B200DepthwiseGrower(B200DepthwiseGrower const &)            = delete;
     B200DepthwiseGrower &operator=(B200DepthwiseGrower const &) = delete;
@@ -98,6 +94,28 @@ class B200DepthwiseGrower
         c.n_monotone        = static_cast<uint32_t>(mono.size());
         c.selected          = selected.data();
         c.n_selected        = static_cast<uint32_t>(selected.size());
+        // interaction_constraints as the reference parses them ("0,1" or
+        // "0+1" per group): features in groups, group g's at [off[g], off[g+1])
+        std::vector<uint32_t> ifeat;
+        std::vector<uint32_t> ioff{0};
+        for (auto const &entry : config_.interaction_constraints)
+        {
+            size_t start = 0;
+            while (start < entry.size())
+            {
+                size_t const sep = std::min(entry.find(',', start), entry.find('+', start));
+                size_t const end = sep == std::string::npos ? entry.size() : sep;
+                if (end > start)
+                {
+                    ifeat.push_back(static_cast<uint32_t>(std::stoul(entry.substr(start, end - start))));
+                }
+                start = end + 1;
+            }
+            ioff.push_back(static_cast<uint32_t>(ifeat.size()));
+        }
+        c.interaction_features = ifeat.empty() ? nullptr : ifeat.data();
+        c.interaction_offsets  = ioff.data();
+        c.n_interaction_groups = static_cast<uint32_t>(ioff.size() - 1);
         size_t const cap    = (size_t{2} << config_.max_depth) - 1;
         std::vector<uint32_t> feat(cap), left(cap), right(cap), split_bin(cap), meta(3);
         std::vector<float>    value(cap), gain(cap), cover(cap);

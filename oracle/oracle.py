@@ -41,6 +41,7 @@ class RefCfg(C.Structure):
         ("subsample", C.c_float), ("random_seed", C.c_uint32),
         ("n_threads", C.c_uint32), ("n_classes", C.c_uint32),
         ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
+        ("interaction", C.c_char_p),
     ]
 
 
@@ -70,6 +71,7 @@ class TreeCfg:
     n_threads: int = 1
     n_classes: int = 3
     monotone: list = field(default_factory=list)
+    interaction_constraints: list = field(default_factory=list)  # TOML strings, "0,1"
 
     def ref(self):
         c = RefCfg()
@@ -84,6 +86,9 @@ class TreeCfg:
             self._mono = np.asarray(self.monotone, dtype=np.int32)
             c.monotone = _p(self._mono, C.c_int32)
             c.n_monotone = len(self.monotone)
+        if self.interaction_constraints:
+            self._inter = ";".join(self.interaction_constraints).encode()
+            c.interaction = self._inter
         return c
 
 

@@ -151,6 +151,7 @@ struct ref_cfg
         uint32_t n_classes;
         int32_t const *monotone;
         uint32_t       n_monotone;
+        char const    *interaction; // groups as the TOML strings, ';'-separated, or null
     };
 
     struct RefModel
@@ -182,6 +183,20 @@ namespace
         {
             cfg.tree_config.monotone_constraints.assign(c.monotone,
                                                         c.monotone + c.n_monotone);
+        }
+        if (c.interaction != nullptr)
+        {
+            std::string const all(c.interaction);
+            size_t            at = 0;
+            while (at <= all.size())
+            {
+                size_t const e = std::min(all.find(';', at), all.size());
+                if (e > at)
+                {
+                    cfg.tree_config.interaction_constraints.push_back(all.substr(at, e - at));
+                }
+                at = e + 1;
+            }
         }
         cfg.booster_config.n_iters       = c.n_iters;
         cfg.booster_config.learning_rate = c.learning_rate;

@@ -39,6 +39,7 @@ def _data(seed=5, n=12_000, F=7):
     dict(max_depth=5, n_iters=20, feature_fraction=0.5, lambda_l1=0.3),
     dict(max_depth=6, n_iters=20, subsample=0.8, min_data_in_leaf=5),
     dict(max_depth=4, n_iters=15, monotone=[1, 0, 0, -1, 0, 0, 0]),
+    dict(max_depth=5, n_iters=10, interaction_constraints=["0,1", "1+3", "2"]),
 ])
 def test_reference_booster_over_b200_grower_matches_cpu(dref, cfg):
     X, y = _data()
