@@ -32,7 +32,7 @@ __all__ = [
 ]
 
 LEAF = 0xFFFFFFFF
-OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2}
+OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2, "poisson": 3}
 GROWERS = {"depthwise": 0, "levelwise": 1, "oblivious": 1, "leafwise": 2}
 HIST_MODES = {"exact": 0, "plain": 0, "int8": 1, "quant8": 1, "int16": 2, "quant16": 2}
 
@@ -365,6 +365,14 @@ def init_score_from_sum(total: float, n_rows: int, objective: str) -> np.float32
 
 def init_score(labels, objective: str) -> np.float32:
     """bb_booster_create's initial score over all of `labels`."""
+    if objective == "poisson":
+        # PoissonObjective::init_score: an FP64 sum, the log of the mean
+        y = np.asarray(labels, np.float32)
+        if (y < 0).any() or np.isnan(y).any():
+            raise ValueError("poisson objective requires non-negative labels")
+        total = float(np.cumsum(y.astype(np.float64))[-1]) if len(y) else 0.0  # in row order
+        mean = total / max(len(y), 1)
+        return np.float32(np.log(max(mean, 1e-9)))
     return init_score_from_sum(label_sum(labels), len(labels), objective)
 
 

@@ -186,6 +186,12 @@ __global__ void __launch_bounds__(k_eval_threads)
             float const ax = fabsf(s);
             acc += fmaxf(0.0F, s) + log1pf(expf(-ax)) - (y * s);
         }
+        else if (objective == 3)
+        {
+            // Poisson NLL up to a label-only constant, the raw score clamped
+            float const f = fminf(fmaxf(vs[r], -k_poisson_max_log), k_poisson_max_log);
+            acc += static_cast<double>(expf(f)) - (static_cast<double>(y) * static_cast<double>(f));
+        }
         else
         {
             double maxv = vs[r];
@@ -598,8 +604,8 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
 {
     need(plane != nullptr && labels != nullptr && cfg != nullptr,
          "bb_booster_create: null argument");
-    need(cfg->objective >= 0 && cfg->objective <= 2,
-         "objective must be 0 (mse), 1 (logloss) or 2 (softmax)");
+    need(cfg->objective >= 0 && cfg->objective <= 3,
+         "objective must be 0 (mse), 1 (logloss), 2 (softmax) or 3 (poisson)");
     need(cfg->objective != 2 || (cfg->n_classes >= 2 && cfg->n_classes <= k_max_classes),
          "softmax needs 2 <= n_classes <= 16");
     need(cfg->objective != 2 || red == nullptr, "softmax fits do not shard");
@@ -632,6 +638,20 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     else if (init_score != nullptr)
     {
         b->init = *init_score;
+    }
+    else if (cfg->objective == 3)
+    {
+        // PoissonObjective::init_score (src/objective.cpp:293-308): the log of
+        // the mean label (an FP64 sum), floored at 1e-9
+        double sum = 0.0;
+        for (uint64_t i = 0; i < n; ++i)
+        {
+            need(labels[i] >= 0.0F && !std::isnan(labels[i]),
+                 "poisson objective requires non-negative labels");
+            sum += labels[i];
+        }
+        double const mean = sum / static_cast<double>(std::max<uint64_t>(n, 1));
+        b->init           = static_cast<float>(std::log(std::max(mean, 1e-9)));
     }
     else
     {

@@ -83,13 +83,24 @@ __host__ __device__ inline bool routes_left(uint32_t b, uint32_t last, uint32_t 
     return b == last ? dl : b <= split;
 }
 
+// Raw scores clamp to +-30 before the Poisson exp (k_poisson_max_log,
+// include/bonsai/objective.hpp:47).
+constexpr float k_poisson_max_log = 30.0F;
+
 // The resident objectives' gradient pair at score s and label y
-// (src/objective.cpp:44-58 squared error, 86-101 logistic loss).
+// (src/objective.cpp:44-58 squared error, 86-101 logistic loss, 267-278
+// Poisson with a log link: g = exp(s) - y, h = exp(s), s clamped). Objective
+// codes: 0 mse, 1 logloss, 3 poisson (2, softmax, has its own pass).
 __device__ __forceinline__ float2 objective_gradient(int objective, float s, float y)
 {
     if (objective == 0)
     {
         return make_float2(s - y, 1.0F);
+    }
+    if (objective == 3)
+    {
+        float const rate = expf(fminf(fmaxf(s, -k_poisson_max_log), k_poisson_max_log));
+        return make_float2(rate - y, rate);
     }
     float const p = 1.0F / (1.0F + expf(-s));
     return make_float2(p - y, p * (1.0F - p));

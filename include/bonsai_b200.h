@@ -115,7 +115,8 @@ int bb_plane_refill(bb_plane *plane, float const *X, uint64_t n_rows, int x_on_d
 typedef struct
 {
     int32_t        objective;  /* 0 mse, 1 logloss, 2 softmax (MulticlassBooster:
-                                  n_classes trees per round, round-major) */
+                                  n_classes trees per round, round-major), 3 poisson
+                                  (log link, raw scores clamped to +-30) */
     float          learning_rate;
     float          min_child_hess;
     float          min_gain_to_split;
@@ -156,7 +157,7 @@ typedef struct
  * the scores stay on the device; every round derives (g, h) on the device,
  * grows a depthwise tree and fuses scores += lr * leaf into the grow.
  * init_scores (host, n_rows) may be NULL: the objective's init_score
- * (src/objective.cpp:76-83, :124-131) is then used.
+ * (src/objective.cpp:76-83, :124-131, :293-308) is then used.
  * Replaces Booster<Obj, DepthwiseGrower<CudaHistogramEngine>, AllRows> with
  * the resident round armed (include/bonsai/booster.hpp:630-676) and the
  * engine's resident_begin (histogram_engine.hpp:251-253). */

@@ -46,7 +46,7 @@ class RefCfg(C.Structure):
 
 
 GROWERS = {"depthwise": 0, "levelwise": 1, "leafwise": 2}
-OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2}
+OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2, "poisson": 3}
 
 
 @dataclass

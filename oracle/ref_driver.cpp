@@ -217,6 +217,8 @@ namespace
             return std::make_unique<Booster<LogLossObjective, Gr, Sa>>(cfg);
         case 2:
             return std::make_unique<MulticlassBooster<Gr, Sa>>(cfg);
+        case 3:
+            return std::make_unique<Booster<PoissonObjective, Gr, Sa>>(cfg);
         default:
             throw std::runtime_error("unknown objective");
         }
@@ -274,12 +276,14 @@ namespace
         {
             ok = go(dynamic_cast<Booster<MSEObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<LogLossObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<PoissonObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<MulticlassBooster<Gr, BernoulliSampler> *>(raw));
         }
         else
         {
             ok = go(dynamic_cast<Booster<MSEObjective, Gr, AllRowsSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<LogLossObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<PoissonObjective, Gr, AllRowsSampler> *>(raw)) ||
                  go(dynamic_cast<MulticlassBooster<Gr, AllRowsSampler> *>(raw));
         }
         if (!ok)
@@ -478,6 +482,12 @@ extern "C"
                 }
                 auto *raw = mm->booster.get();
                 read_init(*mm, dynamic_cast<Booster<MSEObjective, DepthwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<PoissonObjective, DepthwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<PoissonObjective, LeafwiseGrower<>,
+                                                    AllRowsSampler> const *>(raw));
+                read_init(*mm, dynamic_cast<Booster<PoissonObjective, ObliviousGrower<>,
                                                     AllRowsSampler> const *>(raw));
                 read_init(*mm, dynamic_cast<Booster<LogLossObjective, DepthwiseGrower<>,
                                                     AllRowsSampler> const *>(raw));
