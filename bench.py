@@ -408,7 +408,7 @@ def serve_ours(args, local):
 CONFIGS = {
     # name: (workload text, rounds, rows)
     "wide": ("wide sparse regression 1,000,000x2,000 (90% missing), leafwise 255 leaves, "
-             "256 bins, lr 0.1, all rows each round", 200, 1_000_000),
+             "256 bins, lr 0.1, Bernoulli row subsample 0.8 (seed 42)", 200, 1_000_000),
     "multiclass": ("multiclass 581,012x54 (one-hot blocks), 7-class softmax, levelwise depth 8, "
                    "255 bins, lr 0.1", 300, 581_012),
 }
@@ -431,7 +431,7 @@ def config_tc(name, mod):
     TreeCfg (mod = oracle)."""
     if name == "wide":
         kw = dict(objective="mse", grower="leafwise", max_leaves=255, max_depth=255,
-                  learning_rate=0.1)
+                  learning_rate=0.1, subsample=0.8, random_seed=42)
     else:
         kw = dict(objective="softmax", n_classes=7, grower="levelwise", max_depth=8,
                   learning_rate=0.1)

@@ -87,6 +87,11 @@ class TrainParams:
     # TreeConfig::interaction_constraints: feature groups, each a list of ids
     # or the reference's string form ("0,1" or "0+1")
     interaction_constraints: list = field(default_factory=list)
+    # sampler.subsample and booster_config.random_seed: a resident booster
+    # with subsample < 1 grows each tree over a Bernoulli row sample
+    # (BernoulliSampler, src/sampler.cpp:36-55)
+    subsample: float = 1.0
+    random_seed: int = 42
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -103,6 +108,8 @@ class TrainParams:
         c.grower = GROWERS[self.grower]
         c.max_leaves = self.max_leaves
         c.n_classes = self.n_classes
+        c.subsample = self.subsample
+        c.random_seed = self.random_seed
         c.use_graph = 1 if self.use_graph else 0
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:

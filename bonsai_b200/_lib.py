@@ -40,6 +40,7 @@ class TrainCfg(C.Structure):
         ("grower", C.c_int32), ("max_leaves", C.c_uint32), ("n_classes", C.c_uint32),
         ("interaction_features", C.POINTER(C.c_uint32)),
         ("interaction_offsets", C.POINTER(C.c_uint32)), ("n_interaction_groups", C.c_uint32),
+        ("subsample", C.c_float), ("random_seed", C.c_uint32),
     ]
 
 

@@ -8,9 +8,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -462,6 +464,265 @@ uint32_t blocks(uint64_t n, uint32_t t = 256)
     return ceil_div(std::max<uint64_t>(n, 1), t);
 }
 
+// ---- the row sample ---------------------------------------------------------
+// BernoulliSampler::sample (src/sampler.cpp:36-55) keeps row i when
+// std::bernoulli_distribution(p) says so, drawing row by row from the
+// booster's std::mt19937 (seeded with booster_config.random_seed,
+// include/bonsai/booster.hpp:496), one draw per tree (per class tree in a
+// softmax round, include/bonsai/multiclass_booster.hpp:138). The draw stays on
+// the host in exactly those library calls -- one sequential generator stream
+// -- and runs a round ahead on a worker thread; the device receives one bit
+// per row and compacts the bits into the ascending row list the grower's root
+// takes.
+
+constexpr uint32_t k_smp_threads = 256;
+constexpr uint32_t k_smp_words   = 4;                              // mask words per thread
+constexpr uint32_t k_smp_block   = k_smp_threads * k_smp_words;     // mask words per block
+constexpr uint32_t k_scan_threads = 1024;
+
+// Exclusive prefix sum of v over the block; total receives the block's sum.
+template <uint32_t T> __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t &total)
+{
+    __shared__ uint32_t warp_s[T / 32];
+    uint32_t const      lane = threadIdx.x & 31;
+    uint32_t const      wid  = threadIdx.x >> 5;
+    uint32_t            x    = v;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1)
+    {
+        uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        x += lane >= o ? y : 0u;
+    }
+    if (lane == 31)
+    {
+        warp_s[wid] = x;
+    }
+    __syncthreads();
+    uint32_t base = 0;
+    total         = 0;
+    for (uint32_t w = 0; w < T / 32; ++w)
+    {
+        uint32_t const c = warp_s[w];
+        base += w < wid ? c : 0u;
+        total += c;
+    }
+    __syncthreads();
+    return base + x - v;
+}
+
+__device__ __forceinline__ uint32_t thread_words(uint32_t const *bits, uint64_t n_words,
+                                                 uint64_t w0, uint32_t w[k_smp_words])
+{
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < k_smp_words; ++j)
+    {
+        w[j] = w0 + j < n_words ? bits[w0 + j] : 0u;
+        c += __popc(w[j]);
+    }
+    return c;
+}
+
+// Pass 1: each block's kept rows.
+__global__ void __launch_bounds__(k_smp_threads)
+    sample_count_kernel(uint32_t const *__restrict__ bits, uint64_t n_words,
+                        uint32_t *__restrict__ bsum)
+{
+    uint32_t       w[k_smp_words];
+    uint64_t const w0 = (static_cast<uint64_t>(blockIdx.x) * k_smp_block) +
+                        (static_cast<uint64_t>(threadIdx.x) * k_smp_words);
+    uint32_t       total = 0;
+    block_scan<k_smp_threads>(thread_words(bits, n_words, w0, w), total);
+    if (threadIdx.x == 0)
+    {
+        bsum[blockIdx.x] = total;
+    }
+}
+
+// Pass 2 (one block): the blocks' offsets in place, and the sample's size.
+__global__ void __launch_bounds__(k_scan_threads)
+    sample_scan_kernel(uint32_t *bsum, uint32_t n_blocks, uint32_t *count)
+{
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < n_blocks; b0 += k_scan_threads)
+    {
+        uint32_t const i     = b0 + threadIdx.x;
+        uint32_t const v     = i < n_blocks ? bsum[i] : 0u;
+        uint32_t       total = 0;
+        uint32_t const ex    = block_scan<k_scan_threads>(v, total);
+        if (i < n_blocks)
+        {
+            bsum[i] = carry + ex;
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0)
+    {
+        *count = carry;
+    }
+}
+
+// Pass 3: every kept row's id at its rank, so the list is ascending.
+__global__ void __launch_bounds__(k_smp_threads)
+    sample_list_kernel(uint32_t const *__restrict__ bits, uint64_t n_words,
+                       uint32_t const *__restrict__ boff, uint32_t *__restrict__ rows)
+{
+    uint32_t       w[k_smp_words];
+    uint64_t const w0 = (static_cast<uint64_t>(blockIdx.x) * k_smp_block) +
+                        (static_cast<uint64_t>(threadIdx.x) * k_smp_words);
+    uint32_t       total = 0;
+    uint32_t       pos   = boff[blockIdx.x] +
+                   block_scan<k_smp_threads>(thread_words(bits, n_words, w0, w), total);
+#pragma unroll
+    for (uint32_t j = 0; j < k_smp_words; ++j)
+    {
+        uint32_t x = w[j];
+        while (x != 0u)
+        {
+            uint32_t const b = __ffs(static_cast<int>(x)) - 1;
+            rows[pos++]      = static_cast<uint32_t>(((w0 + j) << 5) + b);
+            x &= x - 1u;
+        }
+    }
+}
+
+// The leafwise plane stamps the sampled rows from its leaves' segments; the
+// rest walk the finished tree (route_unsampled, src/grower_impl.hpp:438-461:
+// routes_left on the split bin, the last bin following default_left) over the
+// feature-major codes and take the same update, scores[r] + lr x value.
+template <typename BinT>
+__global__ void __launch_bounds__(256)
+    route_unsampled_kernel(BinT const *__restrict__ bins, uint64_t n_pad, uint64_t n,
+                           uint32_t const *__restrict__ n_bins, TreeOut t, uint32_t cap,
+                           uint32_t const *__restrict__ sbits, float *__restrict__ scores,
+                           uint32_t *__restrict__ leaf_id, float lr)
+{
+    for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x; r < n;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    {
+        if (((sbits[r >> 5] >> (r & 31)) & 1u) != 0)
+        {
+            continue;
+        }
+        uint32_t idx = 0;
+        for (uint32_t step = 0; step < cap && t.feature[idx] != k_leaf_flag; ++step)
+        {
+            uint32_t const f = t.feature[idx];
+            uint32_t const b = bins[(static_cast<uint64_t>(f) * n_pad) + r];
+            idx = routes_left(b, n_bins[f] - 1, t.split_bin[idx], t.default_left[idx] != 0)
+                      ? t.left[idx]
+                      : t.right[idx];
+        }
+        scores[r] = scores[r] + (lr * t.value[idx]);
+        if (leaf_id != nullptr)
+        {
+            leaf_id[r] = idx;
+        }
+    }
+}
+
+// The host side of the sample: two pinned slots of one round's masks (K trees
+// x words, tree-major). upload() sends the next round's masks and starts
+// drawing the round after into the other slot, once that slot's previous
+// copy has left it.
+class RowSampler
+{
+  public:
+    RowSampler(float p, uint32_t seed, uint64_t n, uint32_t trees, int device)
+        : p_(p), rng_(seed), n_(n), trees_(trees), words_((n + 31) / 32), device_(device)
+    {
+        for (int j = 0; j < 2; ++j)
+        {
+            BB_CHECK(cudaMallocHost(&slot_[j], bytes()));
+            BB_CHECK(cudaEventCreateWithFlags(&copied_[j], cudaEventDisableTiming));
+            counts_[j].assign(trees_, 0);
+        }
+    }
+    ~RowSampler()
+    {
+        if (pending_.valid())
+        {
+            pending_.wait();
+        }
+        for (int j = 0; j < 2; ++j)
+        {
+            cudaFreeHost(slot_[j]);
+            cudaEventDestroy(copied_[j]);
+        }
+    }
+    RowSampler(RowSampler const &)            = delete;
+    RowSampler &operator=(RowSampler const &) = delete;
+
+    uint64_t words() const
+    {
+        return words_;
+    }
+    size_t bytes() const
+    {
+        return static_cast<size_t>(words_) * trees_ * 4;
+    }
+
+    // The next round's masks into dev (on s); returns each tree's row count.
+    std::vector<uint32_t> const &upload(uint32_t *dev, cudaStream_t s)
+    {
+        if (pending_.valid())
+        {
+            pending_.get();
+        }
+        else
+        {
+            draw(cur_);
+        }
+        int const done = cur_;
+        BB_CHECK(cudaMemcpyAsync(dev, slot_[done], bytes(), cudaMemcpyHostToDevice, s));
+        BB_CHECK(cudaEventRecord(copied_[done], s));
+        int const next = done ^ 1;
+        cur_           = next;
+        pending_       = std::async(std::launch::async,
+                                    [this, next]
+                                    {
+                                  BB_CHECK(cudaSetDevice(device_));
+                                  BB_CHECK(cudaEventSynchronize(copied_[next]));
+                                  draw(next);
+                              });
+        return counts_[done];
+    }
+
+  private:
+    void draw(int j)
+    {
+        uint32_t *m = slot_[j];
+        std::memset(m, 0, bytes());
+        std::bernoulli_distribution keep(p_);
+        for (uint32_t k = 0; k < trees_; ++k)
+        {
+            uint32_t *w = m + (static_cast<size_t>(k) * words_);
+            uint32_t  c = 0;
+            for (uint64_t i = 0; i < n_; ++i)
+            {
+                if (keep(rng_))
+                {
+                    w[i >> 5] |= 1u << (i & 31);
+                    ++c;
+                }
+            }
+            counts_[j][k] = c;
+        }
+    }
+
+    float                 p_;
+    std::mt19937          rng_;
+    uint64_t              n_;
+    uint32_t              trees_;
+    uint64_t              words_;
+    int                   device_;
+    uint32_t             *slot_[2]{};
+    cudaEvent_t           copied_[2]{};
+    std::vector<uint32_t> counts_[2];
+    int                   cur_ = 0;
+    std::future<void>     pending_;
+};
+
 } // namespace
 } // namespace bb
 
@@ -501,6 +762,67 @@ struct bb_booster
     uint32_t                   *vcount   = nullptr;
     double                     *vpartial = nullptr;
     uint32_t                    vcap     = 0;
+    // the row sample (subsample < 1): a round's masks, one tree's rows
+    std::unique_ptr<RowSampler> sampler;
+    uint32_t                   *sbits  = nullptr; // K x words, tree-major
+    uint32_t                   *srows  = nullptr; // the tree's kept rows, ascending
+    uint32_t                   *scount = nullptr; // their number
+    uint32_t                   *sbsum  = nullptr; // per mask block: counts, then offsets
+    std::vector<uint32_t>       host_counts;      // this round's, per tree
+
+    // Sends the next round's masks (before its graph or its eager body).
+    void upload_sample()
+    {
+        if (sampler)
+        {
+            host_counts = sampler->upload(sbits, stream);
+        }
+    }
+
+    // Tree k's kept rows into srows / scount.
+    RootSample sample_tree(uint32_t k)
+    {
+        uint64_t const  words = sampler->words();
+        uint32_t const *bits  = sbits + (static_cast<uint64_t>(k) * words);
+        uint32_t const  nb    = static_cast<uint32_t>(ceil_div(words, k_smp_block));
+        sample_count_kernel<<<nb, k_smp_threads, 0, stream>>>(bits, words, sbsum);
+        BB_LAUNCH("sample_count_kernel");
+        sample_scan_kernel<<<1, k_scan_threads, 0, stream>>>(sbsum, nb, scount);
+        BB_LAUNCH("sample_scan_kernel");
+        sample_list_kernel<<<nb, k_smp_threads, 0, stream>>>(bits, words, sbsum, srows);
+        BB_LAUNCH("sample_list_kernel");
+        return RootSample{scount, bits};
+    }
+
+    // One tree over tree k's sample: the depthwise and levelwise planes walk
+    // every row; the leafwise plane stamps its rows and routes the rest.
+    void grow_sampled(uint32_t k, float2 const *g, float *sc, NextRound const *next)
+    {
+        RootSample const rs = sample_tree(k);
+        uint64_t const   n  = plane->n_rows;
+        uint32_t *const  li = record_leaf_ids ? leaf_id : nullptr;
+        if (grower->fuses_next())
+        {
+            grower->grow(g, srows, static_cast<uint32_t>(n), scratch.t, li, sc, lr, false, next,
+                         &rs);
+            return;
+        }
+        grower->grow(g, srows, host_counts[k], scratch.t, li, sc, lr, false, nullptr);
+        uint32_t const grid = std::min<uint32_t>(blocks(n), 148u * 16u);
+        if (plane->u8)
+        {
+            route_unsampled_kernel<uint8_t><<<grid, 256, 0, stream>>>(
+                static_cast<uint8_t const *>(plane->bins), plane->n_pad, n, plane->n_bins,
+                scratch.t, scratch.cap, rs.bits, sc, li, lr);
+        }
+        else
+        {
+            route_unsampled_kernel<uint16_t><<<grid, 256, 0, stream>>>(
+                static_cast<uint16_t const *>(plane->bins), plane->n_pad, n, plane->n_bins,
+                scratch.t, scratch.cap, rs.bits, sc, li, lr);
+        }
+        BB_LAUNCH("route_unsampled_kernel");
+    }
 
     void round_body()
     {
@@ -564,9 +886,16 @@ struct bb_booster
             BB_LAUNCH("softmax_gradient_kernel");
             for (uint32_t k = 0; k < n_classes; ++k)
             {
-                grower->grow(gh + (k * n), rows, static_cast<uint32_t>(n), scratch.t,
-                             record_leaf_ids ? leaf_id : nullptr, scores + (k * n), lr, true,
-                             nullptr);
+                if (sampler)
+                {
+                    grow_sampled(k, gh + (k * n), scores + (k * n), nullptr);
+                }
+                else
+                {
+                    grower->grow(gh + (k * n), rows, static_cast<uint32_t>(n), scratch.t,
+                                 record_leaf_ids ? leaf_id : nullptr, scores + (k * n), lr,
+                                 true, nullptr);
+                }
                 commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
                 BB_LAUNCH("commit_tree_kernel");
             }
@@ -578,15 +907,29 @@ struct bb_booster
             // of the current scores come from their own pass
             gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
             BB_LAUNCH("gradient_kernel");
-            grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
-                         record_leaf_ids ? leaf_id : nullptr, scores, lr, true, nullptr);
+            if (sampler)
+            {
+                grow_sampled(0, gh, scores, nullptr);
+            }
+            else
+            {
+                grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
+                             record_leaf_ids ? leaf_id : nullptr, scores, lr, true, nullptr);
+            }
             commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
             BB_LAUNCH("commit_tree_kernel");
             return;
         }
         bb::NextRound const next{objective, labels, gh};
-        grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
-                     record_leaf_ids ? leaf_id : nullptr, scores, lr, true, &next);
+        if (sampler)
+        {
+            grow_sampled(0, gh, scores, &next);
+        }
+        else
+        {
+            grower->grow(gh, rows, static_cast<uint32_t>(n), scratch.t,
+                         record_leaf_ids ? leaf_id : nullptr, scores, lr, true, &next);
+        }
         commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
         BB_LAUNCH("commit_tree_kernel");
     }
@@ -610,6 +953,12 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
          "softmax needs 2 <= n_classes <= 16");
     need(cfg->objective != 2 || red == nullptr, "softmax fits do not shard");
     need(max_trees > 0, "max_trees must be positive");
+    // sampler.subsample (src/sampler.cpp:27-34): 0 (a zeroed config) and
+    // values >= 1 keep every row
+    need(!(cfg->subsample < 0.0F) && !std::isnan(cfg->subsample),
+         "sampler.subsample must be > 0");
+    bool const sampled = cfg->subsample > 0.0F && cfg->subsample < 1.0F;
+    need(!sampled || red == nullptr, "a sharded fit keeps every row (subsample 1)");
     auto           b = std::make_unique<bb_booster>();
     Plane const   &p = plane->p;
     uint64_t const n = p.n_rows;
@@ -697,6 +1046,17 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     {
         b->grower->set_shard(red, row_offset, total_rows);
         b->sharded = true;
+    }
+    if (sampled)
+    {
+        int dev = 0;
+        BB_CHECK(cudaGetDevice(&dev));
+        b->sampler = std::make_unique<RowSampler>(cfg->subsample, cfg->random_seed, n, K, dev);
+        uint64_t const words = b->sampler->words();
+        b->sbits  = dmalloc<uint32_t>(words * K);
+        b->srows  = dmalloc<uint32_t>(n);
+        b->scount = dmalloc<uint32_t>(1);
+        b->sbsum  = dmalloc<uint32_t>(ceil_div(words, k_smp_block));
     }
     b->scratch.alloc(b->grower->max_nodes(), 1);
     b->trees.alloc(b->grower->max_nodes(), max_trees * K); // round-major: r * K + k
@@ -1076,6 +1436,8 @@ extern "C"
                 if (b->use_graph && b->graph == nullptr)
                 {
                     cudaGraph_t g;
+                    // the capture records the round; the first round's masks
+                    // (if sampled) go up before it runs
                     BB_CHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
                     try
                     {
@@ -1093,6 +1455,7 @@ extern "C"
                 BB_CHECK(cudaEventRecord(b->ev0, b->stream));
                 for (uint32_t i = 0; i < n_iters; ++i)
                 {
+                    b->upload_sample();
                     if (b->graph != nullptr)
                     {
                         BB_CHECK(cudaGraphLaunch(b->graph, b->stream));
@@ -1220,6 +1583,7 @@ extern "C"
                 BB_CHECK(cudaStreamSynchronize(b->stream));
                 Profile p;
                 b->grower->set_profile(&p);
+                b->upload_sample();
                 BB_CHECK(cudaEventRecord(b->ev0, b->stream));
                 try
                 {
@@ -1375,10 +1739,12 @@ extern "C"
             cudaGraphExecDestroy(b->graph);
         }
         b->release_eval();
+        b->sampler.reset();
         b->grower.reset();
         b->scratch.release();
         b->trees.release();
-        void *ps[] = {b->labels, b->scores, b->gh, b->rows, b->leaf_id, b->round};
+        void *ps[] = {b->labels, b->scores, b->gh,    b->rows,  b->leaf_id,
+                      b->round,  b->sbits,  b->srows, b->scount, b->sbsum};
         for (void *p : ps)
         {
             cudaFree(p);

@@ -124,10 +124,18 @@ __device__ __forceinline__ float leaf_value(Node const &nd, TreeParams const &tp
 
 // ---------------------------------------------------------------- root ----
 
+// n_root_dev (nullable): the root's row count lives on the device (a row
+// sample drawn for this tree); an unsharded root's global count is then the
+// same number.
 __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk *bchunks,
                                   uint32_t *brange, uint32_t *build, TreeOut t,
-                                  uint32_t crows, uint32_t g_root)
+                                  uint32_t crows, uint32_t g_root, uint32_t const *n_root_dev)
 {
+    if (n_root_dev != nullptr)
+    {
+        n_root = *n_root_dev;
+        g_root = n_root;
+    }
     uint32_t const nch = (n_root + crows - 1) / crows;
     if (threadIdx.x == 0)
     {
@@ -1703,6 +1711,11 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+__device__ __forceinline__ bool in_sample(uint32_t const *bits, uint64_t r)
+{
+    return bits == nullptr || ((bits[r >> 5] >> (r & 31)) & 1u) != 0;
+}
+
 // Pass A of the quantised form: each row's leaf (as 16 bits) and every
 // leaf's exact fixed-point (g, h) sums -- shared-memory 64-bit integer adds,
 // then one global add per touched leaf and CTA.
@@ -1711,7 +1724,8 @@ __global__ void __launch_bounds__(k_threads)
     walk_sum_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror,
                     uint64_t n_rows, uint32_t const *cut_off, uint32_t depth,
                     float2 const *__restrict__ gh, uint32_t const *absmax,
-                    uint16_t *__restrict__ leaf16, unsigned long long *acc)
+                    uint16_t *__restrict__ leaf16, unsigned long long *acc,
+                    uint32_t const *__restrict__ bits)
 {
     constexpr uint32_t  per = U8 ? 32 : 16;
     __shared__ uint4    node_s[k_walk_nodes];
@@ -1738,8 +1752,9 @@ __global__ void __launch_bounds__(k_threads)
         uint4 const    b0  = mt[(r0 * 2) + 1];
         uint4 const    a1  = mt[rb * 2];
         uint4 const    b1  = mt[(rb * 2) + 1];
-        float2 const   g0  = gh[r0];
-        float2 const   g1  = gh[rb];
+        // a row outside this tree's sample takes its leaf but adds nothing
+        float2 const   g0  = in_sample(bits, r0) ? gh[r0] : make_float2(0.0F, 0.0F);
+        float2 const   g1  = in_sample(bits, rb) ? gh[rb] : make_float2(0.0F, 0.0F);
         uint32_t const n0 = walk_row<U8, MULTI>(node_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
         uint32_t const n1 = walk_row<U8, MULTI>(node_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
         leaf16[r0] = static_cast<uint16_t>(n0);
@@ -3745,7 +3760,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
 
 void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
                   TreeOut const &t, uint32_t *leaf_id, float *scores, float lr,
-                  bool identity_root, NextRound const *next)
+                  bool identity_root, NextRound const *next, RootSample const *sample)
 {
     if (n_root > max_rows_)
     {
@@ -3757,7 +3772,7 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     n_launch_      = 0;
     if (cfg_.leaf)
     {
-        if (next != nullptr || red_ != nullptr)
+        if (next != nullptr || red_ != nullptr || sample != nullptr)
         {
             throw ConfigError("grower: the leafwise plane takes neither a fused next round "
                               "nor row shards");
@@ -3770,7 +3785,12 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         grow_leafwise(root_rows, n_root, t, leaf_id, scores, lr);
         return;
     }
-    walk_          = identity_root && n_root == plane_.n_rows &&
+    if (sample != nullptr && (identity_root || red_ != nullptr))
+    {
+        throw ConfigError("grower: a device row sample is neither the identity root nor a "
+                          "row shard");
+    }
+    walk_ = (sample != nullptr || (identity_root && n_root == plane_.n_rows)) &&
             (leaf_id != nullptr || scores != nullptr || next != nullptr);
     if (next != nullptr && !walk_)
     {
@@ -3792,7 +3812,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     }
     uint32_t const g_root = red_ != nullptr ? static_cast<uint32_t>(total_rows_) : n_root;
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t, crows_, g_root);
+                                              build_, t, crows_, g_root,
+                                              sample != nullptr ? sample->count : nullptr);
     BB_LAUNCH("root_setup_kernel");
     n_launch_ += 1;
     // the root's rows: the quantised build reads an identity list implicitly
@@ -3857,7 +3878,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             auto sum = [&](auto kern)
             {
                 kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
-                                                gh_cur_, absmax_, leaf16_, wacc_);
+                                                gh_cur_, absmax_, leaf16_, wacc_,
+                                                sample != nullptr ? sample->bits : nullptr);
             };
             if (plane_.u8)
             {
@@ -3961,7 +3983,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     BB_CHECK(cudaMemcpyAsync(rows_[0], root_rows, size_t{n_root} * 4, cudaMemcpyDeviceToDevice,
                              s));
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t, crows_, n_root);
+                                              build_, t, crows_, n_root, nullptr);
     BB_LAUNCH("root_setup_kernel");
     build(rows_[0], n_sel_, 0);
     if (quant_)
@@ -4216,7 +4238,7 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     }
     walk_ = false;
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n, bchunks_, brange_, build_,
-                                              t, crows_, n);
+                                              t, crows_, n, nullptr);
     BB_LAUNCH("root_setup_kernel");
     build(rows, n_sel_, 0);
     std::vector<double2> cells(total_cells_);

@@ -73,6 +73,14 @@ struct Ctl
     uint32_t pad[6];
 };
 
+// A row sample on the device: its size and one bit per dataset row (bit r of
+// word r / 32).
+struct RootSample
+{
+    uint32_t const *count;
+    uint32_t const *bits;
+};
+
 struct TreeOut
 {
     uint32_t *feature;
@@ -167,9 +175,17 @@ class Grower
     // order, and next (nullable) also has the walk write the next round's
     // gradient pairs; the quantised form then reads their maxima from that
     // walk, so the first such round must follow seed_absmax.
+    //
+    // With sample (depthwise and levelwise) the root is a row sample built on
+    // the device: root_rows holds sample->count[0] ascending rows (n_root is
+    // only their bound), and every dataset row still takes the walk -- the
+    // unsampled ones routed through the finished tree as the sampled ones
+    // are -- while the quantised form renews its leaves from the sampled
+    // rows alone (sample->bits, one bit per row).
     void grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
               TreeOut const &out, uint32_t *leaf_id, float *scores, float lr,
-              bool identity_root = false, NextRound const *next = nullptr);
+              bool identity_root = false, NextRound const *next = nullptr,
+              RootSample const *sample = nullptr);
     // The quantised form's gradient maxima of gh (every dataset row), for a
     // first grow() whose next round is fused.
     void seed_absmax(float2 const *gh);

@@ -151,6 +151,16 @@ typedef struct
     uint32_t const *interaction_features;
     uint32_t const *interaction_offsets; /* n_interaction_groups + 1 */
     uint32_t       n_interaction_groups;
+    /* sampler.subsample (BernoulliSampler, src/sampler.cpp:27-55) and
+     * booster_config.random_seed (booster_config.hpp:12, the reference's
+     * default is 42): a resident booster with 0 < subsample < 1 grows each
+     * tree over the rows std::bernoulli_distribution(subsample) keeps,
+     * drawn from std::mt19937(random_seed) row by row and tree by tree as
+     * the reference's booster draws them; every row's score still takes the
+     * tree. 0 (a zeroed config) or >= 1 keeps every row; negative values are
+     * refused. bb_grow_tree ignores both: its caller passes the rows. */
+    float          subsample;
+    uint32_t       random_seed;
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and

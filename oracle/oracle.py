@@ -499,3 +499,26 @@ def orc_fill(orc: "Oracle", bins, n_bins, grad, hess, rows=None, selected=None):
                    _p(hess, C.c_float), _p(rows, C.c_uint32), C.c_size_t(len(rows)),
                    _p(out, C.c_float))
     return out
+
+
+def bernoulli_keep(n: int, p: float, seed: int, trees: int) -> list:
+    """BernoulliSampler::sample (src/sampler.cpp:36-55) restated in numpy:
+    the booster's std::mt19937 seeded with booster_config.random_seed
+    (include/bonsai/booster.hpp:496) feeds std::bernoulli_distribution(p) row
+    by row, tree by tree. libstdc++ draws the uniform with
+    generate_canonical<double, 53>: two 32-bit outputs x0, x1 make
+    (x0 + x1 * 2^32) rounded to double, / 2^64, and a 1.0 becomes the
+    largest double below 1; the row is kept when that is below p (the float
+    p widened). numpy's MT19937 with its legacy seeding is the same
+    generator as std::mt19937(seed). Returns one boolean mask per tree."""
+    bg = np.random.MT19937(0)
+    bg._legacy_seeding(int(seed))
+    pd = np.float64(np.float32(p))
+    out = []
+    for _ in range(trees):
+        raw = bg.random_raw(2 * n)
+        u = (raw[0::2].astype(np.float64) + raw[1::2].astype(np.float64) * 4294967296.0)
+        u = u / 18446744073709551616.0
+        u = np.where(u >= 1.0, np.nextafter(1.0, 0.0), u)
+        out.append(u < pd)
+    return out
