@@ -390,7 +390,8 @@ class Booster:
 
     def __init__(self, plane: Plane, labels, params: TrainParams, max_trees: int = 1000,
                  init_scores=None, comm: Comm | None = None, row_offset: int = 0,
-                 total_rows: int | None = None, init_score: float | None = None):
+                 total_rows: int | None = None, init_score: float | None = None,
+                 weights=None):
         self.plane = plane
         self.params = params
         self._labels = np.ascontiguousarray(labels, dtype=np.float32)
@@ -409,6 +410,20 @@ class Booster:
                 plane.n_rows if total_rows is None else total_rows,
                 float(init_score), C.byref(h)))
         self.h = h.value
+        if weights is not None:
+            self.set_weights(weights)
+
+    def set_weights(self, weights):
+        """Per-row sample weights scaling every round's (g, h) (bb_booster_set_weights);
+        None returns to the unweighted fit. Before the first round only."""
+        if weights is None:
+            check(lib().bb_booster_set_weights(self.h, None))
+            self._weights = None
+            return
+        self._weights = np.ascontiguousarray(weights, dtype=np.float32)
+        if self._weights.shape != (self.plane.n_rows,):
+            raise ValueError("weights: one per plane row")
+        check(lib().bb_booster_set_weights(self.h, ptr(self._weights)))
 
     def update(self, n_iters: int = 1, sync: bool = True):
         check(lib().bb_booster_update(self.h, n_iters))

@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
                                         C.POINTER(vp)]
         L.bb_booster_update.argtypes = [vp, C.c_uint32]
         L.bb_booster_sync.argtypes = [vp]
+        L.bb_booster_set_weights.argtypes = [vp, vp]
         L.bb_booster_n_trees.argtypes = [vp, C.POINTER(C.c_uint32)]
         L.bb_booster_init_score.argtypes = [vp]
         L.bb_booster_tree_capacity.argtypes = [vp]

@@ -81,14 +81,14 @@ void need(bool ok, char const *what)
 // g = p - y, h = p(1-p) (src/objective.cpp:86-101).
 __global__ void gradient_kernel(int objective, float const *__restrict__ scores,
                                 float const *__restrict__ labels, float2 *__restrict__ gh,
-                                uint64_t n)
+                                uint64_t n, float const *__restrict__ weights)
 {
     uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
     if (i >= n)
     {
         return;
     }
-    gh[i] = objective_gradient(objective, scores[i], labels[i]);
+    gh[i] = weighted(objective_gradient(objective, scores[i], labels[i]), weights, i);
 }
 
 // Softmax gradients for K classes (MulticlassBooster::update_one_iter,
@@ -100,7 +100,8 @@ constexpr uint32_t k_max_classes = 16;
 
 __global__ void softmax_gradient_kernel(float const *__restrict__ scores,
                                         float const *__restrict__ labels,
-                                        float2 *__restrict__ gh, uint64_t n, uint32_t K)
+                                        float2 *__restrict__ gh, uint64_t n, uint32_t K,
+                                        float const *__restrict__ weights)
 {
     uint64_t const i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x) + threadIdx.x;
     if (i >= n)
@@ -126,7 +127,7 @@ __global__ void softmax_gradient_kernel(float const *__restrict__ scores,
     {
         float const p = static_cast<float>(e[k]) / fs;
         float const y = c == k ? 1.0F : 0.0F;
-        gh[(k * n) + i] = make_float2(p - y, fmaxf(p * (1.0F - p), 1e-6F));
+        gh[(k * n) + i] = weighted(make_float2(p - y, fmaxf(p * (1.0F - p), 1e-6F)), weights, i);
     }
 }
 
@@ -736,6 +737,7 @@ struct bb_booster
     float                       lr        = 0.1F;
     float                       init      = 0.0F;
     float                      *labels    = nullptr;
+    float                      *weights   = nullptr; // per row, or nullptr (unweighted)
     float                      *scores    = nullptr;
     float2                     *gh        = nullptr;
     uint32_t                   *rows      = nullptr;
@@ -882,7 +884,7 @@ struct bb_booster
             // one round: the softmax pairs of the round's scores, then one
             // tree per class, each adding lr x leaf to its class's scores
             softmax_gradient_kernel<<<blocks(n), 256, 0, stream>>>(scores, labels, gh, n,
-                                                                    n_classes);
+                                                                    n_classes, weights);
             BB_LAUNCH("softmax_gradient_kernel");
             for (uint32_t k = 0; k < n_classes; ++k)
             {
@@ -905,7 +907,8 @@ struct bb_booster
         {
             // the leafwise plane stamps from its leaves' segments: gradients
             // of the current scores come from their own pass
-            gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n);
+            gradient_kernel<<<blocks(n), 256, 0, stream>>>(objective, scores, labels, gh, n,
+                                                           weights);
             BB_LAUNCH("gradient_kernel");
             if (sampler)
             {
@@ -920,7 +923,7 @@ struct bb_booster
             BB_LAUNCH("commit_tree_kernel");
             return;
         }
-        bb::NextRound const next{objective, labels, gh};
+        bb::NextRound const next{objective, labels, gh, weights};
         if (sampler)
         {
             grow_sampled(0, gh, scores, &next);
@@ -1066,7 +1069,7 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     if (K == 1)
     {
         gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(b->objective, b->scores, b->labels,
-                                                          b->gh, n);
+                                                          b->gh, n, nullptr);
         BB_LAUNCH("gradient_kernel");
         b->grower->seed_absmax(b->gh);
     }
@@ -1470,6 +1473,41 @@ extern "C"
             });
     }
 
+    int bb_booster_set_weights(bb_booster *b, float const *weights)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr, "bb_booster_set_weights: null booster");
+                need(b->n_trees == 0, "bb_booster_set_weights: set weights before the first round");
+                uint64_t const n = b->plane->n_rows;
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                if (weights == nullptr)
+                {
+                    cudaFree(b->weights);
+                    b->weights = nullptr;
+                }
+                else
+                {
+                    if (b->weights == nullptr)
+                    {
+                        b->weights = dmalloc<float>(n);
+                    }
+                    BB_CHECK(cudaMemcpyAsync(b->weights, weights, n * 4, cudaMemcpyHostToDevice,
+                                             b->stream));
+                }
+                if (b->n_classes == 1)
+                {
+                    // the first round's pairs (a softmax round forms its own)
+                    gradient_kernel<<<blocks(n), 256, 0, b->stream>>>(
+                        b->objective, b->scores, b->labels, b->gh, n, b->weights);
+                    BB_LAUNCH("gradient_kernel");
+                    b->grower->seed_absmax(b->gh);
+                }
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+            });
+    }
+
     int bb_booster_sync(bb_booster *b)
     {
         return guarded(
@@ -1743,8 +1781,8 @@ extern "C"
         b->grower.reset();
         b->scratch.release();
         b->trees.release();
-        void *ps[] = {b->labels, b->scores, b->gh,    b->rows,  b->leaf_id,
-                      b->round,  b->sbits,  b->srows, b->scount, b->sbsum};
+        void *ps[] = {b->labels, b->scores, b->gh,     b->rows,   b->leaf_id, b->round,
+                      b->sbits,  b->srows,  b->scount, b->sbsum, b->weights};
         for (void *p : ps)
         {
             cudaFree(p);

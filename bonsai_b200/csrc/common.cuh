@@ -106,6 +106,20 @@ __device__ __forceinline__ float2 objective_gradient(int objective, float s, flo
     return make_float2(p - y, p * (1.0F - p));
 }
 
+// A weighted row scales both halves of its pair by its weight, one float
+// multiply each (Booster::update_one_iter, include/bonsai/booster.hpp:546-555;
+// the device form, src/cuda/detail/kernels.cuh:1001-1006); w == nullptr is
+// the unweighted fit.
+__device__ __forceinline__ float2 weighted(float2 g, float const *w, uint64_t r)
+{
+    if (w == nullptr)
+    {
+        return g;
+    }
+    float const x = w[r];
+    return make_float2(g.x * x, g.y * x);
+}
+
 // Tree-level knobs the device reads (TreeConfig, include/bonsai/config/
 // tree_config.hpp:9-29). Floats stay float: the reference widens them to
 // double at each use, and so does every kernel here.

@@ -1518,6 +1518,7 @@ struct WalkArgs
     float const  *labels;
     float2       *gh;
     uint32_t     *absmax;
+    float const  *weights;
 };
 
 __device__ __forceinline__ uint32_t pick_word(uint32_t const w[8], uint32_t i)
@@ -1661,7 +1662,7 @@ __device__ __forceinline__ void apply_leaf(WalkArgs const &a, uint64_t r, uint32
     a.scores[r]   = s;
     if (a.gh != nullptr)
     {
-        float2 const g = objective_gradient(a.objective, s, y);
+        float2 const g = weighted(objective_gradient(a.objective, s, y), a.weights, r);
         a.gh[r]        = g;
         mg             = fmaxf(mg, fabsf(g.x));
         mh             = fmaxf(mh, fmaxf(g.y, 0.0F));
@@ -3869,6 +3870,7 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         a.leaf_id   = leaf_id;
         a.lr        = lr;
         a.objective = next != nullptr ? next->objective : 0;
+        a.weights   = next != nullptr ? next->weights : nullptr;
         a.labels    = next != nullptr ? next->labels : nullptr;
         a.gh        = next != nullptr ? next->gh : nullptr;
         a.absmax    = next != nullptr && quant_ ? absmax_ : nullptr;

@@ -138,6 +138,7 @@ struct NextRound
     int          objective = 0;
     float const *labels    = nullptr;
     float2      *gh        = nullptr;
+    float const *weights   = nullptr; // per row, or nullptr (unweighted)
 };
 
 struct GrowConfig

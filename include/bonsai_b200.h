@@ -175,6 +175,16 @@ int bb_booster_create(bb_plane const *plane, float const *labels,
                       float const *init_scores, bb_train_cfg const *cfg,
                       uint32_t max_trees, bb_booster **out);
 
+/* Per-row sample weights for the fit (Dataset::weights, include/bonsai/
+ * dataset.hpp:73,86): weights (host, n_rows) scale every round's gradient
+ * and hessian, each by one float multiply, as Booster::update_one_iter
+ * (include/bonsai/booster.hpp:546-555) and the reference's device gradient
+ * kernel (src/cuda/detail/kernels.cuh:1001-1006) do; the initial scores stay
+ * unweighted, as the reference's are. NULL returns to the unweighted fit.
+ * Before the first round only (BB_ERR_ARG after). A sharded fit sets each
+ * shard's weights on its own rank. */
+int bb_booster_set_weights(bb_booster *b, float const *weights);
+
 /* Runs n_iters more rounds (asynchronous; bb_booster_sync waits). */
 int bb_booster_update(bb_booster *b, uint32_t n_iters);
 int bb_booster_sync(bb_booster *b);

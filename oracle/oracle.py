@@ -165,8 +165,8 @@ class RefLib:
             raise RuntimeError(self.err())
         return cuts[: off[-1]].copy(), off
 
-    def dataset(self, X, y, cuts, off):
-        return RefDataset(self, X, y, cuts, off)
+    def dataset(self, X, y, cuts, off, weights=None):
+        return RefDataset(self, X, y, cuts, off, weights)
 
     def train(self, ds, cfg: TreeCfg):
         rc = cfg.ref()
@@ -223,16 +223,26 @@ class RefLib:
 
 
 class RefDataset:
-    def __init__(self, lib, X, y, cuts, off):
+    def __init__(self, lib, X, y, cuts, off, weights=None):
         self.lib = lib
         X = np.ascontiguousarray(X, np.float32)
         y = np.ascontiguousarray(y, np.float32)
         self.n, self.F = X.shape
         self.cuts = np.ascontiguousarray(cuts, np.float32)
         self.off = np.ascontiguousarray(off, np.uint32)
-        lib.L.ref_dataset_create.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p]
-        self.h = lib.L.ref_dataset_create(X.ctypes.data, y.ctypes.data, self.n, self.F,
-                                          self.cuts.ctypes.data, self.off.ctypes.data)
+        if weights is None:
+            lib.L.ref_dataset_create.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t,
+                                                 C.c_void_p, C.c_void_p]
+            self.h = lib.L.ref_dataset_create(X.ctypes.data, y.ctypes.data, self.n, self.F,
+                                              self.cuts.ctypes.data, self.off.ctypes.data)
+        else:
+            w = np.ascontiguousarray(weights, np.float32)
+            f = lib.L.ref_dataset_create_weighted
+            f.restype = C.c_void_p
+            f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t,
+                          C.c_void_p, C.c_void_p]
+            self.h = f(X.ctypes.data, y.ctypes.data, w.ctypes.data, self.n, self.F,
+                       self.cuts.ctypes.data, self.off.ctypes.data)
         if not self.h:
             raise RuntimeError(lib.err())
 

@@ -410,6 +410,24 @@ extern "C"
         return rc == 0 ? out : nullptr;
     }
 
+    // The same with per-row sample weights (Dataset::bin's weights argument).
+    void *ref_dataset_create_weighted(float const *X, float const *y, float const *w, size_t n,
+                                      size_t F, float const *cuts, uint32_t const *cut_off)
+    {
+        Dataset *out = nullptr;
+        int const rc = guarded(
+            [&]
+            {
+                BinMappers const   mappers = mappers_from_cuts(cuts, cut_off, F);
+                features_view      Xv(X, n, F);
+                std::vector<float> labels(y, y + n);
+                std::vector<float> weights(w, w + n);
+                out = new Dataset(
+                    Dataset::bin(Xv, labels, mappers, DataConfig{}, nullptr, weights));
+            });
+        return rc == 0 ? out : nullptr;
+    }
+
     void ref_dataset_destroy(void *ds)
     {
         delete static_cast<Dataset *>(ds);
