@@ -934,6 +934,8 @@ __global__ void __launch_bounds__(k_lfind_thr)
                 auto const *cell = reinterpret_cast<float2 const *>(src);
                 if (lane == 0)
                 {
+                    // Histogram::fill_prefix (include/bonsai/histogram.hpp:139-160):
+                    // double running sums, each entry stored as a float cell
                     double lg = 0.0;
                     double lh = 0.0;
                     for (uint32_t b = 0; b < n_cut; ++b)
@@ -941,7 +943,7 @@ __global__ void __launch_bounds__(k_lfind_thr)
                         float2 const c = cell[b];
                         lg += c.x;
                         lh += c.y;
-                        pr[b] = make_double2(lg, lh);
+                        pr[b] = make_double2(static_cast<float>(lg), static_cast<float>(lh));
                     }
                     float2 const m = cell[nb - 1];
                     LevelNode    l;

@@ -325,14 +325,15 @@ static orc_split find_level(gctx const *c, onode const *cur, size_t n_cur)
             float const *cells = cur[p].hist + (2 * c->off[j]);
             mg[p]              = cells[2 * (nb - 1)];
             mh[p]              = cells[(2 * (nb - 1)) + 1];
-            /* Histogram::fill_prefix (include/bonsai/histogram.hpp:139-160) */
+            /* Histogram::fill_prefix (include/bonsai/histogram.hpp:139-160):
+               double running sums, each entry stored as a float cell */
             double lg = 0.0, lh = 0.0;
             for (uint32_t b = 0; b < n_cut; ++b)
             {
                 lg += cells[2 * b];
                 lh += cells[(2 * b) + 1];
-                pref[2 * ((p * n_cut) + b)]       = lg;
-                pref[(2 * ((p * n_cut) + b)) + 1] = lh;
+                pref[2 * ((p * n_cut) + b)]       = (double)(float)lg;
+                pref[(2 * ((p * n_cut) + b)) + 1] = (double)(float)lh;
             }
             pscore[p] = score(cur[p].sum_g, cur[p].sum_h, l1, l2);
             sum_parent += pscore[p];

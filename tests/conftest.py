@@ -66,6 +66,18 @@ def unpack_trees(d, prefix=""):
 TREE_FIELDS = ("feature", "value", "left", "right", "default_left", "gains", "covers")
 
 
+def level_gains(t):
+    """An oblivious tree's per-level gains, read along its left spine (the perfect
+    level-order tree a levelwise fit returns, or the reference's preorder
+    dense_equivalent, src/tree.cpp:64-117, which puts each level's gain on every node of
+    the level)."""
+    out, i = [], 0
+    while t.feature[i] != 0xFFFFFFFF:
+        out.append(t.gains[i])
+        i = int(t.left[i])
+    return np.asarray(out, np.float32)
+
+
 def assert_trees_equal(a, b, where=""):
     for k in TREE_FIELDS:
         x, y = getattr(a, k), getattr(b, k)

@@ -3,12 +3,14 @@ against the reference's own CPU implementation: one split per level chosen over 
 whole frontier (update_best_for_feature_for_level, src/split.cpp:164-235, infeasible
 nodes contributing their parent score), broadcast to every node, empty children kept.
 Trees are compared as the reference's ObliviousTree tables (level features,
-thresholds, default directions, leaf values) and per-row leaf values, bit for bit."""
+thresholds, default directions, leaf values, level gains) and per-row leaf values, bit
+for bit."""
 
 from __future__ import annotations
 
 import numpy as np
 import pytest
+from conftest import level_gains
 
 from oracle import TreeCfg
 
@@ -51,6 +53,7 @@ def test_levelwise_tree_matches_reference(bb, ref, seed, cfg):
     theirs = _ref_tables(m)
     for a, b, what in zip(mine, theirs, ("features", "thresholds", "default_left", "leaves")):
         assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8)), what
+    assert np.array_equal(level_gains(t).view(np.uint32), level_gains(m.tree(0)).view(np.uint32))
     assert np.array_equal(vals.view(np.uint32), rvals.view(np.uint32))
 
 
@@ -85,6 +88,8 @@ def test_levelwise_booster_matches_reference(bb, ref, use_graph):
         theirs = m.oblivious(i)
         for a, c in zip(mine, theirs):
             assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(c).view(np.uint8)), i
+        assert np.array_equal(level_gains(b.tree(i)).view(np.uint32),
+                              level_gains(m.tree(i)).view(np.uint32)), i
     pred = bb.predict(plane, b.trees(), b.init_score, 0.1)
     assert np.array_equal(pred, m.predict_binned(ds))
 

@@ -6,7 +6,7 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
-from conftest import assert_trees_equal, load_golden, unpack_trees
+from conftest import assert_trees_equal, level_gains, load_golden, unpack_trees
 
 from oracle import Oracle, TreeCfg, orc_find_split
 
@@ -168,4 +168,5 @@ def test_levelwise_live_matches_reference(orc: Oracle, ref, seed, cfg):
     _, rvals, _, m = ref.grow_tree(ds, tc, g, h)
     t, vals, _ = orc.grow(ds.bins(), np.diff(off), cuts, off, g, h, tc)
     _tables_equal(oblivious_tables(t), m.oblivious(0))
+    assert np.array_equal(level_gains(t).view(np.uint32), level_gains(m.tree(0)).view(np.uint32))
     assert np.array_equal(vals.view(np.uint32), rvals.view(np.uint32))
