@@ -215,6 +215,35 @@ class Plane:
         self._keep = None
 
     @classmethod
+    def from_device(cls, X, cuts, cut_off) -> "Plane":
+        """Zero-copy ingest of a device-resident n x F float32 row-major matrix
+        (cuda_ingest_device, include/bonsai/cuda/histogram_engine.hpp:41-50): a torch
+        CUDA tensor, any producer of DLPack (__dlpack__) or of the CUDA array interface
+        (CuPy, Numba, JAX ...). The bin kernel reads the matrix where it lies; the
+        producer's pending writes are ordered before it (DLPack and the array interface
+        hand their stream to torch's current stream, which is synchronised), and the
+        matrix is not retained: it may be freed once this returns."""
+        import torch
+        if isinstance(X, torch.Tensor):
+            t = X
+        elif hasattr(X, "__dlpack__"):
+            t = torch.from_dlpack(X)
+        elif hasattr(X, "__cuda_array_interface__"):
+            t = torch.as_tensor(X, device="cuda")
+        else:
+            raise TypeError("from_device: expected a CUDA tensor, a DLPack producer or an "
+                            "object with __cuda_array_interface__")
+        if not t.is_cuda:
+            raise ValueError("from_device: the matrix is not in CUDA device memory")
+        if t.dtype != torch.float32 or t.dim() != 2:
+            raise ValueError("from_device: expected a 2-D float32 matrix")
+        if not t.is_contiguous():
+            raise ValueError("from_device: the matrix must be row-major contiguous")
+        with torch.cuda.device(t.device):
+            torch.cuda.current_stream(t.device).synchronize()
+            return cls(t, cuts, cut_off, x_on_device=True)
+
+    @classmethod
     def from_bins(cls, bins, cuts, cut_off) -> "Plane":
         """A plane over codes binned elsewhere (bb_plane_from_bins): bins is
         [n_feats, n_rows], uint8 (every feature <= 256 bins) or uint16, each

@@ -169,17 +169,25 @@ __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk 
 }
 
 // Node totals from the first selected feature's cells: double sums over
-// every cell in bin order, rounded to float once (Histogram::totals).
-__device__ __forceinline__ void totals_from_cells(float2 const *cells, uint32_t nb,
-                                                  float &g, float &h)
+// every cell in bin order, rounded to float once (Histogram::totals), with
+// one warp: lanes load 32 cells at a time and every lane adds them in bin
+// order from the shuffles, so each lane holds the serial FP64 sums (one
+// dependent add per bin, no dependent global load).
+__device__ __forceinline__ void warp_totals(float2 const *cells, uint32_t nb, float &g,
+                                            float &h)
 {
-    double sg = 0.0;
-    double sh = 0.0;
-    for (uint32_t b = 0; b < nb; ++b)
+    uint32_t const lane = threadIdx.x & 31;
+    double         sg   = 0.0;
+    double         sh   = 0.0;
+    for (uint32_t b0 = 0; b0 < nb; b0 += 32)
     {
-        float2 const c = cells[b];
-        sg += c.x;
-        sh += c.y;
+        float2 const   c = b0 + lane < nb ? cells[b0 + lane] : make_float2(0.0F, 0.0F);
+        uint32_t const m = min(32u, nb - b0);
+        for (uint32_t i = 0; i < m; ++i)
+        {
+            sg += __shfl_sync(0xFFFFFFFFu, c.x, i);
+            sh += __shfl_sync(0xFFFFFFFFu, c.y, i);
+        }
     }
     g = static_cast<float>(sg);
     h = static_cast<float>(sh);
@@ -187,9 +195,12 @@ __device__ __forceinline__ void totals_from_cells(float2 const *cells, uint32_t 
 
 __global__ void root_totals_kernel(Node *nodes, float2 const *hist, uint32_t const *sel_nb)
 {
+    float g, h;
+    warp_totals(hist, sel_nb[0], g, h);
     if (threadIdx.x == 0)
     {
-        totals_from_cells(hist, sel_nb[0], nodes[0].sum_g, nodes[0].sum_h);
+        nodes[0].sum_g = g;
+        nodes[0].sum_h = h;
     }
 }
 
@@ -1967,15 +1978,29 @@ __global__ void __launch_bounds__(k_threads)
         hl[x]          = make_float2(a.x - b.x, a.y - b.y);
     }
     __syncthreads();
+    // the children's totals: warp c sums child c's first feature
+    __shared__ float tot_s[4];
+    uint32_t const   wc = threadIdx.x >> 5;
+    if (wc < 2)
+    {
+        float g, h;
+        warp_totals(hist_nxt + (static_cast<uint64_t>((2 * k) + wc) * total_cells), sel_nb[0],
+                    g, h);
+        if ((threadIdx.x & 31) == 0)
+        {
+            tot_s[2 * wc]       = g;
+            tot_s[(2 * wc) + 1] = h;
+        }
+    }
+    __syncthreads();
     if (threadIdx.x == 0)
     {
-        uint32_t const nb0 = sel_nb[0];
-        Node           L   = next[2 * k];
-        Node           R   = next[(2 * k) + 1];
-        totals_from_cells(hist_nxt + (static_cast<uint64_t>(2 * k) * total_cells), nb0,
-                          L.sum_g, L.sum_h);
-        totals_from_cells(hist_nxt + (static_cast<uint64_t>((2 * k) + 1) * total_cells),
-                          nb0, R.sum_g, R.sum_h);
+        Node L  = next[2 * k];
+        Node R  = next[(2 * k) + 1];
+        L.sum_g = tot_s[0];
+        L.sum_h = tot_s[1];
+        R.sum_g = tot_s[2];
+        R.sum_h = tot_s[3];
         Node const     par = cur[p];
         uint32_t const f   = sel[best[p].feature];
         int const      mc  = (mono != nullptr && f < n_mono) ? mono[f] : 0;
@@ -2550,18 +2575,25 @@ __global__ void __launch_bounds__(k_tthreads, 1)
              hist + (static_cast<uint64_t>(build[node]) * total_cells));
 }
 
-__device__ __forceinline__ void qtotals_from_cells(unsigned long long const *cells,
-                                                   uint32_t nb, uint32_t cw, int64_t &g,
-                                                   int64_t &h)
+// The quantised form's node totals: exact integer sums of the first selected
+// feature's cells with one warp (order-free), every lane holding them.
+__device__ __forceinline__ void warp_qtotals(unsigned long long const *cells, uint32_t nb,
+                                             uint32_t cw, int64_t &g, int64_t &h)
 {
     int64_t sg = 0;
     int64_t sh = 0;
-    for (uint32_t b = 0; b < nb; ++b)
+    for (uint32_t b = threadIdx.x & 31; b < nb; b += 32)
     {
         int64_t cg, ch;
         qcell(cells, b, cw, cg, ch);
         sg += cg;
         sh += ch;
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        sg += __shfl_xor_sync(0xFFFFFFFFu, sg, o);
+        sh += __shfl_xor_sync(0xFFFFFFFFu, sh, o);
     }
     g = sg;
     h = sh;
@@ -2570,9 +2602,12 @@ __device__ __forceinline__ void qtotals_from_cells(unsigned long long const *cel
 __global__ void qroot_totals_kernel(Node *nodes, unsigned long long const *hist,
                                     uint32_t const *sel_nb, uint32_t cw)
 {
+    int64_t g, h;
+    warp_qtotals(hist, sel_nb[0], cw, g, h);
     if (threadIdx.x == 0)
     {
-        qtotals_from_cells(hist, sel_nb[0], cw, nodes[0].qg, nodes[0].qh);
+        nodes[0].qg = g;
+        nodes[0].qh = h;
     }
 }
 
@@ -3019,13 +3054,48 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
                                    TreeParams tp, double2 const *qscale, LeafPop p, uint32_t cw,
                                    uint64_t const *fgroups)
 {
-    if (threadIdx.x != 0)
-    {
-        return;
-    }
+    __shared__ int64_t qtot_s[4];
+    __shared__ float   tot_s[4];
     if (out->split == 0)
     {
-        ctl->n_cur = 0;
+        if (threadIdx.x == 0)
+        {
+            ctl->n_cur = 0;
+        }
+        return;
+    }
+    // warp c sums child c's first feature
+    uint32_t const wc = threadIdx.x >> 5;
+    if (wc < 2)
+    {
+        if constexpr (Q)
+        {
+            int64_t g, h;
+            warp_qtotals(static_cast<unsigned long long const *>(pool) +
+                             (static_cast<uint64_t>(slot_of[wc]) * total_cells * cw),
+                         sel_nb[0], cw, g, h);
+            if ((threadIdx.x & 31) == 0)
+            {
+                qtot_s[2 * wc]       = g;
+                qtot_s[(2 * wc) + 1] = h;
+            }
+        }
+        else
+        {
+            float g, h;
+            warp_totals(static_cast<float2 const *>(pool) +
+                            (static_cast<uint64_t>(slot_of[wc]) * total_cells),
+                        sel_nb[0], g, h);
+            if ((threadIdx.x & 31) == 0)
+            {
+                tot_s[2 * wc]       = g;
+                tot_s[(2 * wc) + 1] = h;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+    {
         return;
     }
     Node L = next[0];
@@ -3033,11 +3103,10 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
     double gl, hl, gr, hr;
     if constexpr (Q)
     {
-        auto const *h = static_cast<unsigned long long const *>(pool);
-        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells * cw),
-                           sel_nb[0], cw, L.qg, L.qh);
-        qtotals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells * cw),
-                           sel_nb[0], cw, R.qg, R.qh);
+        L.qg             = qtot_s[0];
+        L.qh             = qtot_s[1];
+        R.qg             = qtot_s[2];
+        R.qh             = qtot_s[3];
         double2 const sc = *qscale;
         gl = static_cast<double>(L.qg) * sc.x;
         hl = static_cast<double>(L.qh) * sc.y;
@@ -3046,11 +3115,10 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
     }
     else
     {
-        auto const *h = static_cast<float2 const *>(pool);
-        totals_from_cells(h + (static_cast<uint64_t>(slot_of[0]) * total_cells), sel_nb[0],
-                          L.sum_g, L.sum_h);
-        totals_from_cells(h + (static_cast<uint64_t>(slot_of[1]) * total_cells), sel_nb[0],
-                          R.sum_g, R.sum_h);
+        L.sum_g = tot_s[0];
+        L.sum_h = tot_s[1];
+        R.sum_g = tot_s[2];
+        R.sum_h = tot_s[3];
         gl = L.sum_g;
         hl = L.sum_h;
         gr = R.sum_g;
@@ -3084,19 +3152,23 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
 
 // Each node's best split over the features (the lowest feature wins a gain
 // tie), no split past the depth cap; the nodes and splits go to the host.
-__global__ void leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_sel,
-                                 Node const *nodes, LeafOut *out, uint32_t may_split)
+// grid 2 (a CTA per node) x k_best_thr: each thread scans a stride of the
+// features, then (largest gain, lowest feature) over the block -- the serial
+// scan's choice, whatever the order.
+constexpr uint32_t k_best_thr = 256;
+
+__global__ void __launch_bounds__(k_best_thr)
+    leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_sel, Node const *nodes,
+                     LeafOut *out, uint32_t may_split)
 {
-    uint32_t const w    = threadIdx.x >> 5;
-    uint32_t const lane = threadIdx.x & 31;
-    if (w >= 2)
-    {
-        return;
-    }
-    bool const live = w < ctl->n_cur;
-    double     g    = 0.0;
-    uint32_t   o    = 0xFFFFFFFFu;
-    for (uint32_t j = lane; live && may_split != 0 && j < n_sel; j += 32)
+    __shared__ double   g_s[k_best_thr / 32];
+    __shared__ uint32_t o_s[k_best_thr / 32];
+    uint32_t const      w    = blockIdx.x;
+    uint32_t const      lane = threadIdx.x & 31;
+    bool const          live = w < ctl->n_cur;
+    double              g    = 0.0;
+    uint32_t            o    = 0xFFFFFFFFu;
+    for (uint32_t j = threadIdx.x; live && may_split != 0 && j < n_sel; j += k_best_thr)
     {
         Best const c = cand[(w * n_sel) + j];
         if (c.valid != 0 && (c.gain > g || (c.gain == g && j < o)))
@@ -3108,6 +3180,20 @@ __global__ void leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_se
     warp_best(g, o);
     if (lane == 0)
     {
+        g_s[threadIdx.x >> 5] = g;
+        o_s[threadIdx.x >> 5] = o;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (uint32_t x = 1; x < k_best_thr / 32; ++x)
+        {
+            if (g_s[x] > g || (g_s[x] == g && o_s[x] < o))
+            {
+                g = g_s[x];
+                o = o_s[x];
+            }
+        }
         out->best[w] = o == 0xFFFFFFFFu ? Best{0.0, 0, 0, 1, 0} : cand[(w * n_sel) + o];
         if (live)
         {
@@ -4017,7 +4103,8 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                 tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
         }
         BB_LAUNCH("find_kernel");
-        leaf_best_kernel<<<1, 64, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split ? 1 : 0);
+        leaf_best_kernel<<<2, k_best_thr, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout,
+                                                  may_split ? 1 : 0);
         BB_LAUNCH("leaf_best_kernel");
         BB_CHECK(cudaMemcpyAsync(lh, lout, sizeof(LeafOut), cudaMemcpyDeviceToHost, s));
         BB_CHECK(cudaStreamSynchronize(s));
@@ -4137,7 +4224,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         {
             leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_ * cw_,
                                                         total_cells_ * cw_);
-            leaf_totals_kernel<true><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
+            leaf_totals_kernel<true><<<1, 64, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                       total_cells_, sel_, sel_nb_, mono_, n_mono_,
                                                       tp, qscale_, p, cw_, fgroups_);
         }
@@ -4145,7 +4232,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         {
             leaf_sub_kernel<false><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
                                                          total_cells_);
-            leaf_totals_kernel<false><<<1, 32, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
+            leaf_totals_kernel<false><<<1, 64, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
                                                        total_cells_, sel_, sel_nb_, mono_,
                                                        n_mono_, tp, qscale_, p, 1, fgroups_);
         }
