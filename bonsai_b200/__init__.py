@@ -92,6 +92,11 @@ class TrainParams:
     # (BernoulliSampler, src/sampler.cpp:36-55)
     subsample: float = 1.0
     random_seed: int = 42
+    # tree_config.feature_fraction / feature_seed: a resident booster with
+    # feature_fraction < 1 grows each tree over its own feature sample
+    # (sample_features, src/grower_impl.hpp:163-180)
+    feature_fraction: float = 1.0
+    feature_seed: int = 2
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -110,6 +115,8 @@ class TrainParams:
         c.n_classes = self.n_classes
         c.subsample = self.subsample
         c.random_seed = self.random_seed
+        c.feature_fraction = self.feature_fraction
+        c.feature_seed = self.feature_seed
         c.use_graph = 1 if self.use_graph else 0
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <future>
+#include <iterator>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -622,6 +623,25 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// sample_features (src/grower_impl.hpp:163-180): a sorted draw of
+// max(1, ceil(fraction x n)) distinct feature ids by std::sample over the
+// grower's std::mt19937, the same library calls, so the same features.
+std::vector<uint32_t> sample_features(uint32_t n_features, float fraction, std::mt19937 &rng)
+{
+    std::vector<uint32_t> all(n_features);
+    std::iota(all.begin(), all.end(), 0U);
+    if (fraction >= 1.0F || n_features <= 1)
+    {
+        return all;
+    }
+    auto const k = std::max<size_t>(
+        1, static_cast<size_t>(std::ceil(fraction * static_cast<float>(n_features))));
+    std::vector<uint32_t> selected;
+    selected.reserve(k);
+    std::sample(all.begin(), all.end(), std::back_inserter(selected), k, rng);
+    return selected;
+}
+
 // The host side of the sample: two pinned slots of one round's masks (K trees
 // x words, tree-major). upload() sends the next round's masks and starts
 // drawing the round after into the other slot, once that slot's previous
@@ -771,13 +791,31 @@ struct bb_booster
     uint32_t                   *scount = nullptr; // their number
     uint32_t                   *sbsum  = nullptr; // per mask block: counts, then offsets
     std::vector<uint32_t>       host_counts;      // this round's, per tree
+    // the feature sample (feature_fraction < 1): the grower's std::mt19937
+    std::mt19937                feat_rng;
+    float                       feat_frac = 1.0F;
+    uint32_t                    feat_k    = 0; // features per tree; 0: every feature
 
-    // Sends the next round's masks (before its graph or its eager body).
+    // Sends the next round's masks and feature samples (before its graph or
+    // its eager body).
     void upload_sample()
     {
         if (sampler)
         {
             host_counts = sampler->upload(sbits, stream);
+        }
+        for (uint32_t k = 0; feat_k > 0 && k < n_classes; ++k)
+        {
+            grower->set_selection(k, sample_features(plane->n_feats, feat_frac, feat_rng));
+        }
+    }
+
+    // Class k's tree reads table set k (the one set of a single-output fit).
+    void use_features(uint32_t k)
+    {
+        if (feat_k > 0)
+        {
+            grower->use_set(k);
         }
     }
 
@@ -888,6 +926,7 @@ struct bb_booster
             BB_LAUNCH("softmax_gradient_kernel");
             for (uint32_t k = 0; k < n_classes; ++k)
             {
+                use_features(k);
                 if (sampler)
                 {
                     grow_sampled(k, gh + (k * n), scores + (k * n), nullptr);
@@ -903,6 +942,7 @@ struct bb_booster
             }
             return;
         }
+        use_features(0);
         if (!grower->fuses_next())
         {
             // the leafwise plane stamps from its leaves' segments: gradients
@@ -962,6 +1002,17 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
          "sampler.subsample must be > 0");
     bool const sampled = cfg->subsample > 0.0F && cfg->subsample < 1.0F;
     need(!sampled || red == nullptr, "a sharded fit keeps every row (subsample 1)");
+    need(!(cfg->feature_fraction < 0.0F) && !std::isnan(cfg->feature_fraction),
+         "tree_config.feature_fraction must be > 0");
+    uint32_t const F_all = plane->p.n_feats;
+    uint32_t const feat_k =
+        cfg->feature_fraction > 0.0F && cfg->feature_fraction < 1.0F && F_all > 1
+            ? static_cast<uint32_t>(std::max<size_t>(
+                  1, static_cast<size_t>(
+                         std::ceil(cfg->feature_fraction * static_cast<float>(F_all)))))
+            : 0;
+    need(feat_k == 0 || cfg->selected == nullptr,
+         "feature_fraction < 1 draws each tree's features: pass no `selected`");
     auto           b = std::make_unique<bb_booster>();
     Plane const   &p = plane->p;
     uint64_t const n = p.n_rows;
@@ -1040,7 +1091,17 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     iota_kernel<<<blocks(n), 256, 0, b->stream>>>(b->rows, n);
     BB_LAUNCH("iota_kernel");
     BB_CHECK(cudaMemsetAsync(b->round, 0, 4, b->stream));
-    b->grower = std::make_unique<Grower>(p, grow_config(*cfg), selection(*cfg, p.n_feats),
+    GrowConfig gc = grow_config(*cfg);
+    if (feat_k > 0 && feat_k < p.n_feats)
+    {
+        // every tree draws its own features into table set k (class k)
+        gc.sample_k   = feat_k;
+        gc.sel_sets   = K;
+        b->feat_k     = feat_k;
+        b->feat_frac  = cfg->feature_fraction;
+        b->feat_rng.seed(cfg->feature_seed);
+    }
+    b->grower = std::make_unique<Grower>(p, gc, selection(*cfg, p.n_feats),
                                          static_cast<uint32_t>(n), b->stream);
     b->grower->set_monotone(monotone(*cfg));
     b->grower->set_interaction(interaction(*cfg, p.n_feats));

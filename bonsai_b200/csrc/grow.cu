@@ -21,7 +21,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <limits>
+#include <numeric>
 #include <type_traits>
 
 namespace bb
@@ -1518,6 +1520,7 @@ __global__ void __launch_bounds__(k_threads)
 // unit, so at most 2^62 over 2^24 rows; integer sums are order-free, hence
 // deterministic), a one-CTA kernel turns them into FP64 Newton values, and
 // pass B applies them from the leaf id pass A recorded.
+constexpr uint32_t k_no_sel_tile = 0xFFFFFFFFu; // an unused tile slot of a selection
 constexpr uint32_t k_walk_nodes = 512;     // a depth-8 tree has at most 511
 constexpr uint32_t k_no_tile    = 0xFFFFFFu;
 constexpr double   k_fix_unit   = 274877906944.0; // 2^38
@@ -2245,6 +2248,10 @@ __global__ void __launch_bounds__(k_qthreads, 3)
         return;
     }
     uint32_t const tile  = tile_ids[blockIdx.y];
+    if (tile == k_no_sel_tile)
+    {
+        return; // a tile slot this selection leaves unused
+    }
     uint32_t const cells = per * max_nb;
     int32_t       *hg_s  = hq_s;
     uint32_t      *hh_s  = reinterpret_cast<uint32_t *>(hq_s + cells);
@@ -2472,6 +2479,10 @@ __global__ void __launch_bounds__(k_tthreads, 1)
     auto const    *stg_p = reinterpret_cast<uint4 const *>(
         reinterpret_cast<unsigned char const *>(t_smem) + k_ttable_bytes);
     uint32_t const tile = tile_ids[blockIdx.y];
+    if (tile == k_no_sel_tile)
+    {
+        return; // a tile slot this selection leaves unused
+    }
     if (tid < 32)
     {
         j_s[tid] = tile_j[(blockIdx.y * 32) + tid];
@@ -3220,6 +3231,16 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
                uint32_t max_root_rows, cudaStream_t stream)
     : plane_(plane), cfg_(cfg), sel_h_(std::move(selected)), stream_(stream)
 {
+    if (cfg_.sample_k > 0)
+    {
+        // per-tree samples: the first sample_k features until set_selection
+        if (cfg_.sample_k > plane_.n_feats || cfg_.sel_sets == 0)
+        {
+            throw ConfigError("grower: a feature sample larger than the plane");
+        }
+        sel_h_.resize(cfg_.sample_k);
+        std::iota(sel_h_.begin(), sel_h_.end(), 0U);
+    }
     n_sel_ = static_cast<uint32_t>(sel_h_.size());
     quant_ = cfg_.mode != HistMode::exact;
     if (n_sel_ == 0)
@@ -3266,6 +3287,28 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     }
     total_cells_ = off[n_sel_];
     off_h_       = off;
+    if (cfg_.sample_k > 0)
+    {
+        // bounds over every sample: the largest feature's bins, and per node
+        // the cells of the sample_k largest features (off_h_ is read at the
+        // whole sample and at its first feature only)
+        std::vector<uint32_t> all(plane_.n_feats);
+        for (uint32_t f = 0; f < plane_.n_feats; ++f)
+        {
+            all[f]  = plane_.h_cut_off[f + 1] - plane_.h_cut_off[f];
+            max_nb_ = std::max(max_nb_, all[f]);
+        }
+        std::sort(all.begin(), all.end(), std::greater<>());
+        total_cells_ = std::accumulate(all.begin(), all.begin() + n_sel_, 0U);
+        off_h_.assign(n_sel_ + 1, 0);
+        off_h_[1]      = max_nb_;
+        off_h_[n_sel_] = total_cells_;
+        if (max_nb_ > k_max_bins)
+        {
+            throw ConfigError("grower: a feature has more than 4096 bins; lower "
+                              "bin_mapper.max_bin or use a host grower");
+        }
+    }
     cell_stride_ = ((max_nb_ + 1 + 3) / 4) * 4;
     // leafwise: a pool slot per live leaf plus the one being built; a pop
     // consumes a heap entry (at most 2 per split + the root), two nodes each
@@ -3279,14 +3322,44 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
     max_bchunks_ = ceil_div(max_rows_, crows_) + max_front_;
 
-    cudaStream_t s = stream_;
-    sel_      = dalloc<uint32_t>(n_sel_, s);
-    cell_off_ = dalloc<uint32_t>(n_sel_ + 1, s);
-    sel_nb_   = dalloc<uint32_t>(n_sel_, s);
-    BB_CHECK(cudaMemcpyAsync(sel_, sel_h_.data(), n_sel_ * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(cell_off_, off.data(), (n_sel_ + 1) * 4,
-                             cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(sel_nb_, nb.data(), n_sel_ * 4, cudaMemcpyHostToDevice, s));
+    cudaStream_t   s     = stream_;
+    uint32_t const nsets = std::max(1u, cfg_.sel_sets);
+    sel_base_      = dalloc<uint32_t>(static_cast<size_t>(nsets) * n_sel_, s);
+    cell_off_base_ = dalloc<uint32_t>(static_cast<size_t>(nsets) * (n_sel_ + 1), s);
+    sel_nb_base_   = dalloc<uint32_t>(static_cast<size_t>(nsets) * n_sel_, s);
+    if (quant_)
+    {
+        // the mirror tiles a selection can touch: all selected features (v
+        // 0), and the first one alone (v 1: the last level builds only its
+        // totals); a sampled grower sizes them for any sample
+        uint32_t const per     = k_mirror_bytes / (plane_.u8 ? 1 : 2);
+        uint32_t const n_tiles = ceil_div(plane_.n_feats, per);
+        for (int v = 0; v < 2; ++v)
+        {
+            uint32_t cap = 1;
+            if (v == 0)
+            {
+                cap = 0;
+                for (uint32_t j = 0; j < n_sel_; ++j)
+                {
+                    cap += (j == 0 || sel_h_[j] / per != sel_h_[j - 1] / per) ? 1 : 0;
+                }
+                if (cfg_.sample_k > 0)
+                {
+                    cap = std::min(n_sel_, n_tiles);
+                }
+            }
+            n_tiles_[v]       = cap;
+            tile_ids_base_[v] = dalloc<uint32_t>(static_cast<size_t>(nsets) * cap, s);
+            tile_j_base_[v]   = dalloc<int32_t>(static_cast<size_t>(nsets) * cap * per, s);
+        }
+    }
+    sets_h_.assign(nsets, sel_h_);
+    for (uint32_t k = 0; k < nsets; ++k)
+    {
+        write_tables(k, sel_h_);
+    }
+    use_set(0);
     ctl_      = dalloc<Ctl>(1, s);
     nodes_[0] = dalloc<Node>(max_front_, s);
     nodes_[1] = dalloc<Node>(max_front_, s);
@@ -3336,33 +3409,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         wacc_    = dalloc<unsigned long long>(2 * k_walk_nodes, s);
         leaf16_  = dalloc<uint16_t>(plane_.n_rows, s);
         BB_CHECK(cudaMemsetAsync(done_, 0, 4, s));
-        // the mirror tiles holding the selection: all selected features, and
-        // the first one alone (the last level builds only its totals)
         uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
-        for (int v = 0; v < 2; ++v)
-        {
-            std::vector<uint32_t> ids;
-            std::vector<int32_t>  js;
-            uint32_t const        nfb = v == 0 ? n_sel_ : 1;
-            for (uint32_t j = 0; j < nfb; ++j)
-            {
-                uint32_t const t = sel_h_[j] / per;
-                if (ids.empty() || ids.back() != t)
-                {
-                    ids.push_back(t);
-                    js.insert(js.end(), per, -1);
-                }
-                js[((ids.size() - 1) * per) + (sel_h_[j] % per)] = static_cast<int32_t>(j);
-            }
-            n_tiles_[v]  = static_cast<uint32_t>(ids.size());
-            tile_ids_[v] = dalloc<uint32_t>(ids.size(), s);
-            tile_j_[v]   = dalloc<int32_t>(js.size(), s);
-            BB_CHECK(cudaMemcpyAsync(tile_ids_[v], ids.data(), ids.size() * 4,
-                                     cudaMemcpyHostToDevice, s));
-            BB_CHECK(cudaMemcpyAsync(tile_j_[v], js.data(), js.size() * 4,
-                                     cudaMemcpyHostToDevice, s));
-            BB_CHECK(cudaStreamSynchronize(s));
-        }
         size_t const qsmem = static_cast<size_t>(per) * max_nb_ * 8;
         if (qsmem > 200 * 1024)
         {
@@ -3441,15 +3488,106 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     BB_CHECK(cudaEventCreate(&pev_[1]));
 }
 
+// Set k's tables for the ascending feature ids sel: the ids, each one's
+// first cell and bin count, and (quantised) the mirror tiles holding them
+// with each tile slot's selection index, unused slots marked. The host
+// vectors are pageable, so each copy has left them when it returns.
+void Grower::write_tables(uint32_t set, std::vector<uint32_t> const &sel)
+{
+    cudaStream_t          s = stream_;
+    std::vector<uint32_t> off(n_sel_ + 1, 0);
+    std::vector<uint32_t> nb(n_sel_, 0);
+    for (uint32_t j = 0; j < n_sel_; ++j)
+    {
+        uint32_t const f = sel[j];
+        nb[j]            = plane_.h_cut_off[f + 1] - plane_.h_cut_off[f];
+        off[j + 1]       = off[j] + nb[j];
+    }
+    BB_CHECK(cudaMemcpyAsync(sel_base_ + (static_cast<size_t>(set) * n_sel_), sel.data(),
+                             n_sel_ * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(cell_off_base_ + (static_cast<size_t>(set) * (n_sel_ + 1)),
+                             off.data(), (n_sel_ + 1) * 4, cudaMemcpyHostToDevice, s));
+    BB_CHECK(cudaMemcpyAsync(sel_nb_base_ + (static_cast<size_t>(set) * n_sel_), nb.data(),
+                             n_sel_ * 4, cudaMemcpyHostToDevice, s));
+    if (!quant_)
+    {
+        return;
+    }
+    uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
+    for (int v = 0; v < 2; ++v)
+    {
+        uint32_t const        cap = n_tiles_[v];
+        std::vector<uint32_t> ids;
+        std::vector<int32_t>  js(static_cast<size_t>(cap) * per, -1);
+        uint32_t const        nfb = v == 0 ? n_sel_ : 1;
+        for (uint32_t j = 0; j < nfb; ++j)
+        {
+            uint32_t const t = sel[j] / per;
+            if (ids.empty() || ids.back() != t)
+            {
+                ids.push_back(t);
+            }
+            js[((ids.size() - 1) * per) + (sel[j] % per)] = static_cast<int32_t>(j);
+        }
+        if (ids.size() > cap)
+        {
+            throw std::logic_error("grower: a selection touches more tiles than its tables hold");
+        }
+        ids.resize(cap, k_no_sel_tile);
+        BB_CHECK(cudaMemcpyAsync(tile_ids_base_[v] + (static_cast<size_t>(set) * cap), ids.data(),
+                                 cap * 4, cudaMemcpyHostToDevice, s));
+        BB_CHECK(cudaMemcpyAsync(tile_j_base_[v] + (static_cast<size_t>(set) * cap * per),
+                                 js.data(), js.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+}
+
+void Grower::set_selection(uint32_t set, std::vector<uint32_t> const &sel)
+{
+    if (cfg_.sample_k == 0 || set >= sets_h_.size() || sel.size() != n_sel_)
+    {
+        throw std::logic_error("grower: set_selection outside a sampled grower's sets");
+    }
+    for (size_t j = 0; j < sel.size(); ++j)
+    {
+        if (sel[j] >= plane_.n_feats || (j > 0 && sel[j] <= sel[j - 1]))
+        {
+            throw std::logic_error("grower: a feature sample must be ascending plane features");
+        }
+    }
+    write_tables(set, sel);
+    sets_h_[set] = sel;
+}
+
+void Grower::use_set(uint32_t set)
+{
+    if (set >= sets_h_.size())
+    {
+        throw std::logic_error("grower: no such selection set");
+    }
+    uint32_t const per = k_mirror_bytes / (plane_.u8 ? 1 : 2);
+    sel_      = sel_base_ + (static_cast<size_t>(set) * n_sel_);
+    cell_off_ = cell_off_base_ + (static_cast<size_t>(set) * (n_sel_ + 1));
+    sel_nb_   = sel_nb_base_ + (static_cast<size_t>(set) * n_sel_);
+    for (int v = 0; v < 2; ++v)
+    {
+        if (tile_ids_base_[v] != nullptr)
+        {
+            tile_ids_[v] = tile_ids_base_[v] + (static_cast<size_t>(set) * n_tiles_[v]);
+            tile_j_[v]   = tile_j_base_[v] + (static_cast<size_t>(set) * n_tiles_[v] * per);
+        }
+    }
+    sel_h_ = sets_h_[set];
+}
+
 Grower::~Grower()
 {
-    void *ptrs[] = {sel_,     cell_off_, sel_nb_,  ctl_,      nodes_[0],   nodes_[1],
+    void *ptrs[] = {sel_base_, cell_off_base_, sel_nb_base_, ctl_, nodes_[0], nodes_[1],
                     hist_[0], hist_[1],  cand_,    best_,     pchunks_,    pleft_,
                     prbase_,  dst_,      build_,   bpair_,    brange_,     bchunks_,
                     ccount_,  seg_,      payload_, rows_[0],  rows_[1],    scale_,
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
-                    qgh8_,    partial_,  dtree_,   tile_ids_[0], tile_ids_[1], tile_j_[0],
-                    tile_j_[1], bbase_,   dirs_,    btot_,    done_,    wacc_,
+                    qgh8_,    partial_,  dtree_,   tile_ids_base_[0], tile_ids_base_[1],
+                    tile_j_base_[0], tile_j_base_[1], bbase_, dirs_, btot_, done_, wacc_,
                     leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_};
     for (void *p : ptrs)
     {

@@ -153,6 +153,12 @@ struct GrowConfig
     // node per heap pop, at most tp.max_leaves leaves (<= 512), tp.max_depth
     // caps the depth (<= 255)
     bool       leaf  = false;
+    // > 0: every tree draws its own sample of this many features
+    // (feature_fraction, sample_features, src/grower_impl.hpp:163-180) into one
+    // of sel_sets table sets (set_selection / use_set); the grower is sized
+    // for any such sample, so its launches do not depend on which
+    uint32_t   sample_k = 0;
+    uint32_t   sel_sets = 1;
 };
 
 // All device buffers one tree's growth needs, sized once for a dataset and
@@ -207,6 +213,13 @@ class Grower
     {
         return total_cells_;
     }
+
+    // Per-tree feature samples (GrowConfig::sample_k): writes the tables of
+    // table set `set` for the ascending feature ids sel (sample_k of them),
+    // enqueued on the grower's stream; use_set picks the set the next
+    // grow() reads (a captured grow keeps the set it was captured with).
+    void set_selection(uint32_t set, std::vector<uint32_t> const &sel);
+    void use_set(uint32_t set);
 
     uint32_t max_nodes() const
     {
@@ -302,6 +315,16 @@ class Grower
     uint32_t *tile_ids_[2] = {nullptr, nullptr};
     int32_t  *tile_j_[2]   = {nullptr, nullptr};
     uint32_t  n_tiles_[2]  = {0, 0};
+    // the selection tables of every set (sel_, cell_off_, sel_nb_ and the
+    // tile tables point into set k's part); unused tile slots hold
+    // k_no_sel_tile, so their CTAs exit
+    std::vector<std::vector<uint32_t>> sets_h_;
+    uint32_t *sel_base_      = nullptr;
+    uint32_t *cell_off_base_ = nullptr;
+    uint32_t *sel_nb_base_   = nullptr;
+    uint32_t *tile_ids_base_[2] = {nullptr, nullptr};
+    int32_t  *tile_j_base_[2]   = {nullptr, nullptr};
+    void      write_tables(uint32_t set, std::vector<uint32_t> const &sel);
     Node const     *nodes_cur_ = nullptr;
     uint32_t const *rows_cur_  = nullptr;
     uint32_t const *root_rows_ = nullptr;

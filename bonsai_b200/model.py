@@ -225,6 +225,9 @@ def config_for(params, n_iters: int, max_bin: int = 255, **sections) -> dict:
     for k in ("min_child_hess", "min_gain_to_split", "lambda_l2", "lambda_l1", "max_depth",
               "min_data_in_leaf", "max_leaves"):
         tc[k] = getattr(params, k)
+    frac = params.feature_fraction
+    tc["feature_fraction"] = frac if 0.0 < frac < 1.0 else 1.0
+    tc["feature_seed"] = int(params.feature_seed)
     tc["monotone_constraints"] = [int(v) for v in params.monotone]
     tc["interaction_constraints"] = [
         g if isinstance(g, str) else ",".join(str(int(f)) for f in g)

@@ -161,6 +161,17 @@ typedef struct
      * refused. bb_grow_tree ignores both: its caller passes the rows. */
     float          subsample;
     uint32_t       random_seed;
+    /* tree_config.feature_fraction and .feature_seed (tree_config.hpp:15,19;
+     * the reference's default seed is 2): a resident booster with
+     * 0 < feature_fraction < 1 grows each tree over max(1, ceil(fraction x
+     * n_feats)) features drawn by std::sample from std::mt19937(feature_seed)
+     * as sample_features does (src/grower_impl.hpp:163-180), tree by tree
+     * (class tree by class tree in a softmax round). 0 (a zeroed config) or
+     * >= 1 keeps every feature; negative values and a feature_fraction < 1
+     * with `selected` are refused. bb_grow_tree ignores both: its caller
+     * passes the selection. */
+    float          feature_fraction;
+    uint32_t       feature_seed;
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and

@@ -106,10 +106,12 @@ def test_config_for_writes_every_persisted_key():
             if (section, k) != ("parallel", "n_threads"):
                 assert cfg[section][k] == v, (section, k)
     s = M.config_for(TrainParams(objective="softmax", n_classes=7, grower="oblivious",
-                                 subsample=0.8, monotone=[1, 0, -1],
+                                 subsample=0.8, monotone=[1, 0, -1], feature_fraction=0.5,
+                                 feature_seed=9,
                                  interaction_constraints=[[0, 1], "2,3"]), n_iters=300)
     assert s["dispatch"] == {"objective_name": "softmax", "grower_name": "levelwise",
                              "sampler_name": "bernoulli"}
     assert s["objective"]["n_classes"] == 7 and s["sampler"]["subsample"] == float(np.float32(0.8))
     assert s["tree_config"]["monotone_constraints"] == [1, 0, -1]
+    assert s["tree_config"]["feature_fraction"] == 0.5 and s["tree_config"]["feature_seed"] == 9
     assert s["tree_config"]["interaction_constraints"] == ["0,1", "2,3"]
