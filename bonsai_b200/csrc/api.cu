@@ -831,6 +831,7 @@ struct bb_booster
         BB_LAUNCH("sample_scan_kernel");
         sample_list_kernel<<<nb, k_smp_threads, 0, stream>>>(bits, words, sbsum, srows);
         BB_LAUNCH("sample_list_kernel");
+        round_launches += 3;
         return RootSample{scount, bits};
     }
 
@@ -862,15 +863,26 @@ struct bb_booster
                 scratch.t, scratch.cap, rs.bits, sc, li, lr);
         }
         BB_LAUNCH("route_unsampled_kernel");
+        round_launches += 1;
     }
+
+    uint32_t round_launches = 0; // kernels the last round_body enqueued
 
     void round_body()
     {
+        round_launches = 0;
         grow_round();
         if (vplane != nullptr)
         {
             eval_round();
+            round_launches += 2;
         }
+    }
+
+    // one grow's kernels and the commit after it
+    void count_tree()
+    {
+        round_launches += grower->launches_per_tree() + 1;
     }
 
     void eval_round()
@@ -924,6 +936,7 @@ struct bb_booster
             softmax_gradient_kernel<<<blocks(n), 256, 0, stream>>>(scores, labels, gh, n,
                                                                     n_classes, weights);
             BB_LAUNCH("softmax_gradient_kernel");
+            round_launches += 1;
             for (uint32_t k = 0; k < n_classes; ++k)
             {
                 use_features(k);
@@ -939,6 +952,7 @@ struct bb_booster
                 }
                 commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
                 BB_LAUNCH("commit_tree_kernel");
+                count_tree();
             }
             return;
         }
@@ -961,6 +975,8 @@ struct bb_booster
             }
             commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
             BB_LAUNCH("commit_tree_kernel");
+            count_tree();
+            round_launches += 1; // the gradient pass
             return;
         }
         bb::NextRound const next{objective, labels, gh, weights};
@@ -975,6 +991,7 @@ struct bb_booster
         }
         commit_tree_kernel<<<1, 256, 0, stream>>>(scratch.t, trees.t, trees.cap, round);
         BB_LAUNCH("commit_tree_kernel");
+        count_tree();
     }
 };
 
@@ -1707,7 +1724,7 @@ extern "C"
                 out->hist_bytes   = p.hist_bytes;
                 out->hist_rows    = p.hist_rows;
                 out->hist_builds  = p.hist_builds;
-                out->launches     = b->grower->launches_per_tree() + 2;
+                out->launches     = b->round_launches;
             });
     }
 

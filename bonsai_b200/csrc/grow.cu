@@ -798,6 +798,139 @@ __global__ void __launch_bounds__(k_find_thr)
 }
 
 
+// The quantised form's find with a warp per (node, feature): grid (frontier,
+// ceil(n_sel / k_qfind_warps)), k_qfind_warps warps per CTA, no block
+// barrier. The cut bins go by in 32-bin chunks (lane l holds bin c + l), a
+// group of chunks loaded at once; the exact integer prefix (order-free) is
+// each chunk's warp scan plus the carry, each bin's candidates are scored
+// by its lane, and (largest gain, lowest bin x 2 + direction) over the warp
+// is the choice of the per-(node, feature) CTA above, which one
+// barrier-free warp replaces.
+constexpr uint32_t k_qfind_warps = 8;
+constexpr uint32_t k_qfind_group = 4; // 32-bin chunks in flight per lane
+
+__global__ void __launch_bounds__(k_qfind_warps * 32)
+    qfind_warp_kernel(Ctl const *ctl, Node const *nodes, void const *hist_v,
+                      uint32_t total_cells, uint32_t const *cell_off, uint32_t const *sel_nb,
+                      uint32_t const *sel, uint32_t n_sel, int8_t const *mono, uint32_t n_mono,
+                      TreeParams tp, Best *cand, double2 const *qscale, uint32_t const *slot_of,
+                      uint32_t cw, uint64_t const *fgroups)
+{
+    uint32_t const i = blockIdx.x;
+    if (i >= ctl->n_cur)
+    {
+        return;
+    }
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const j    = (blockIdx.y * k_qfind_warps) + (threadIdx.x >> 5);
+    if (j >= n_sel)
+    {
+        return;
+    }
+    Node const     nd  = nodes[i];
+    uint32_t const nb  = sel_nb[j];
+    Best           out = {0.0, j, 0, 1, 0};
+    if (nd.gcount < 2 * tp.min_data_in_leaf || nb < 2 ||
+        !interaction_allows(nd, fgroups, sel[j]))
+    {
+        if (lane == 0)
+        {
+            cand[(i * n_sel) + j] = out;
+        }
+        return;
+    }
+    uint32_t const n_cut = nb - 2;
+    uint32_t const slot  = slot_of != nullptr ? slot_of[i] : i;
+    auto const    *src   = static_cast<unsigned long long const *>(hist_v) +
+                      (((static_cast<uint64_t>(slot) * total_cells) + cell_off[j]) * cw);
+    double2 const sc = *qscale;
+    int64_t       mqg, mqh;
+    qcell(src, nb - 1, cw, mqg, mqh);
+    double const   l1       = tp.lambda_l1;
+    double const   l2       = tp.lambda_l2;
+    double const   mg       = static_cast<double>(mqg) * sc.x;
+    double const   mh       = static_cast<double>(mqh) * sc.y;
+    double const   node_sc  = split_score(static_cast<double>(nd.qg) * sc.x,
+                                          static_cast<double>(nd.qh) * sc.y, l1, l2);
+    double const   real_g   = static_cast<double>(nd.qg - mqg) * sc.x;
+    double const   real_h   = static_cast<double>(nd.qh - mqh) * sc.y;
+    uint32_t const n_dir    = (mqg == 0 && mqh == 0) ? 1 : 2;
+    uint32_t const f        = sel[j];
+    int const      mc       = (mono != nullptr && f < n_mono) ? mono[f] : 0;
+    double const   min_gain = tp.min_gain_to_split;
+    double         best     = 0.0;
+    uint32_t       order    = 0xFFFFFFFFu;
+    int64_t        carry_g  = 0;
+    int64_t        carry_h  = 0;
+    // 32-bin chunks, a group of them loaded (coalesced, all in flight)
+    // before the group's scans; lane l holds bin c + l of chunk c
+    for (uint32_t c0 = 0; c0 < n_cut; c0 += 32 * k_qfind_group)
+    {
+        int64_t vg[k_qfind_group];
+        int64_t vh[k_qfind_group];
+#pragma unroll
+        for (uint32_t q = 0; q < k_qfind_group; ++q)
+        {
+            uint32_t const b = c0 + (q * 32) + lane;
+            vg[q]            = 0;
+            vh[q]            = 0;
+            if (b < n_cut)
+            {
+                qcell(src, b, cw, vg[q], vh[q]);
+            }
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < k_qfind_group; ++q)
+        {
+            int64_t sg = vg[q];
+            int64_t sh = vh[q];
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1)
+            {
+                int64_t const ug = __shfl_up_sync(0xFFFFFFFFu, sg, o);
+                int64_t const uh = __shfl_up_sync(0xFFFFFFFFu, sh, o);
+                if (lane >= o)
+                {
+                    sg += ug;
+                    sh += uh;
+                }
+            }
+            uint32_t const b = c0 + (q * 32) + lane;
+            if (b < n_cut)
+            {
+                double const lg = static_cast<double>(carry_g + sg) * sc.x;
+                double const lh = static_cast<double>(carry_h + sh) * sc.y;
+                for (uint32_t d = 0; d < n_dir; ++d)
+                {
+                    double gain = 0.0;
+                    if (candidate_gain<double>(lg, lh, mg, mh, real_g, real_h, d == 0, node_sc,
+                                               tp, mc, nd.lo, nd.hi, gain) &&
+                        gain > best && gain >= min_gain)
+                    {
+                        best  = gain;
+                        order = (b * 2) + d;
+                    }
+                }
+            }
+            carry_g += __shfl_sync(0xFFFFFFFFu, sg, 31);
+            carry_h += __shfl_sync(0xFFFFFFFFu, sh, 31);
+        }
+    }
+    warp_best(best, order);
+    if (lane == 0)
+    {
+        if (order != 0xFFFFFFFFu)
+        {
+            out.gain  = best;
+            out.bin   = order >> 1;
+            out.dl    = (order & 1) == 0 ? 1 : 0;
+            out.valid = 1;
+        }
+        cand[(i * n_sel) + j] = out;
+    }
+}
+
+
 // ------------------------------------------------------- level split find ----
 //
 // update_best_for_feature_for_level (src/split.cpp:164-235): one split for
@@ -3853,9 +3986,10 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     else if (quant_)
     {
-        find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
+        qfind_warp_kernel<<<dim3(max_front_, ceil_div(n_sel_, k_qfind_warps)),
+                            k_qfind_warps * 32, 0, s>>>(
             ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_, fgroups_);
+            mono_, n_mono_, cfg_.tp, cand_, qscale_, nullptr, cw_, fgroups_);
     }
     else
     {
@@ -4213,6 +4347,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
                                               build_, t, crows_, n_root, nullptr);
     BB_LAUNCH("root_setup_kernel");
+    n_launch_ += 1;
     build(rows_[0], n_sel_, 0);
     if (quant_)
     {
@@ -4225,14 +4360,16 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                             sel_nb_);
     }
     BB_LAUNCH("root_totals_kernel");
+    n_launch_ += 1;
     auto find = [&](Node const *nodes, uint32_t const *slot_of, bool may_split)
     {
         dim3 const fgrid(2, n_sel_);
         if (quant_)
         {
-            find_kernel<true><<<fgrid, k_find_thr, find_smem, s>>>(
-                ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
+            qfind_warp_kernel<<<dim3(2, ceil_div(n_sel_, k_qfind_warps)), k_qfind_warps * 32, 0,
+                                s>>>(ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_,
+                                     n_sel_, mono_, n_mono_, tp, cand_, qscale_, slot_of, cw_,
+                                     fgroups_);
         }
         else
         {
@@ -4244,6 +4381,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         leaf_best_kernel<<<2, k_best_thr, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout,
                                                   may_split ? 1 : 0);
         BB_LAUNCH("leaf_best_kernel");
+        n_launch_ += 2;
         BB_CHECK(cudaMemcpyAsync(lh, lout, sizeof(LeafOut), cudaMemcpyDeviceToHost, s));
         BB_CHECK(cudaStreamSynchronize(s));
     };
@@ -4351,6 +4489,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
             dirs_, static_cast<unsigned long long *>(pool), build_, total_cells_ * cw_,
             quant_ ? total_cells_ * cw_ : 0);
         BB_LAUNCH("pscatter_kernel");
+        n_launch_ += 4; // setup, count, plan, scatter
         build(rows_[1], n_sel_, 0, true);
         uint32_t const cgrid = std::max(1u, std::min(ceil_div(c.node.count, 256), 148u * 8u));
         leaf_copyback_kernel<<<cgrid, 256, 0, s>>>(lout, rows_[1], rows_[0], c.node.start,
@@ -4375,6 +4514,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                                        n_mono_, tp, qscale_, p, 1, fgroups_);
         }
         BB_LAUNCH("leaf_totals_kernel");
+        n_launch_ += 3; // copy-back, subtraction, totals
         find(nodes_[1], slot_of_, c.depth + 1 < tp.max_depth);
         if (lh->split == 0)
         {
@@ -4433,6 +4573,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     leaf_final_ctl_kernel<<<1, 1, 0, s>>>(ctl_, static_cast<uint32_t>(leaves.size()), n_nodes,
                                           depth);
     BB_LAUNCH("leaf_final_ctl_kernel");
+    n_launch_ += 2; // with final_kernel below
     // write_leaf for every leaf, then (quantised) the FP64 renewal, then the
     // rows' leaf ids and score updates from the leaves' segments
     final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], tp, t, pchunks_, pcr_, nbound_);
@@ -4445,6 +4586,8 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     BB_LAUNCH("stamp_kernel");
     tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
     BB_LAUNCH("tree_counter_kernel");
+    n_launch_ += 2; // stamp, counter
+    launches_ = n_launch_;
     BB_CHECK(cudaStreamSynchronize(s)); // the host tables above are read until here
     ++tree_no_;
 }
