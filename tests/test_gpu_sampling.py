@@ -133,3 +133,38 @@ def test_subsample_refusals(bb):
     cuts, off = bb.fit_cuts(X)
     with pytest.raises(bb.BonsaiError):
         bb.Booster(bb.Plane(X, cuts, off), y, bb.TrainParams(subsample=-0.5))
+
+
+@pytest.mark.parametrize("grower,graph", [("depthwise", True), ("levelwise", True),
+                                          ("leafwise", False)])
+@pytest.mark.parametrize("seed", [0, 5])
+def test_empty_and_single_row_samples_match_reference(bb, ref, grower, graph, seed):
+    """Samples of zero or one row (subsample 0.002 of 300 rows: seed 0 keeps 1, 0
+    and 1 rows over three trees, seed 5 none): the reference grows a root leaf
+    of value -0.0 and cover 0 from an empty sample, and every row still takes
+    each tree's leaf."""
+    rng = np.random.Generator(np.random.PCG64(1))
+    X = rng.standard_normal((300, 4)).astype(np.float32)
+    y = X[:, 0].astype(np.float32)
+    cuts, off = ref.fit_cuts(X)
+    ds = ref.dataset(X, y, cuts, off)
+    tc = dict(grower=grower, max_depth=3, max_leaves=7)
+    m = ref.train(ds, TreeCfg(n_iters=3, subsample=0.002, random_seed=seed, **tc))
+    plane = bb.Plane(X, cuts, off)
+    b = bb.Booster(plane, y, bb.TrainParams(subsample=0.002, random_seed=seed, use_graph=graph,
+                                            **tc), max_trees=3)
+    b.update(3)
+    keep = bernoulli_keep(300, 0.002, seed, 3)
+    for i in range(3):
+        assert int(b.tree(i).covers[0]) == int(keep[i].sum())
+        if grower == "levelwise":
+            for x, z in zip(bb.oblivious_tables(b.tree(i)), m.oblivious(i)):
+                assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(z).view(np.uint8))
+        else:
+            _same(b.tree(i), m.tree(i), f"tree {i}")
+    assert np.array_equal(bb.predict(plane, b.trees(), b.init_score, 0.1).view(np.uint32),
+                          m.predict_binned(ds).view(np.uint32))
+    s = np.full(300, np.float32(b.init_score), np.float32)
+    for t in b.trees():
+        s = (s + np.float32(0.1) * bb.predict(plane, [t], np.float32(0.0), 1.0)).astype(np.float32)
+    assert np.array_equal(b.scores().view(np.uint32), s.view(np.uint32))
