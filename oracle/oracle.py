@@ -41,12 +41,13 @@ class RefCfg(C.Structure):
         ("subsample", C.c_float), ("random_seed", C.c_uint32),
         ("n_threads", C.c_uint32), ("n_classes", C.c_uint32),
         ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
-        ("interaction", C.c_char_p),
+        ("interaction", C.c_char_p), ("quantile_alpha", C.c_float), ("huber_delta", C.c_float),
     ]
 
 
 GROWERS = {"depthwise": 0, "levelwise": 1, "leafwise": 2}
-OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2, "poisson": 3}
+OBJECTIVES = {"mse": 0, "logloss": 1, "softmax": 2, "poisson": 3, "mae": 4, "huber": 5,
+              "quantile": 6}
 
 
 @dataclass
@@ -70,6 +71,8 @@ class TreeCfg:
     random_seed: int = 42
     n_threads: int = 1
     n_classes: int = 3
+    quantile_alpha: float = 0.5
+    huber_delta: float = 1.0
     monotone: list = field(default_factory=list)
     interaction_constraints: list = field(default_factory=list)  # TOML strings, "0,1"
 
@@ -80,7 +83,7 @@ class TreeCfg:
         for k in ("n_iters", "learning_rate", "min_child_hess", "min_gain_to_split",
                   "lambda_l2", "lambda_l1", "feature_fraction", "max_depth",
                   "min_data_in_leaf", "max_leaves", "feature_seed", "subsample",
-                  "random_seed", "n_threads", "n_classes"):
+                  "random_seed", "n_threads", "n_classes", "quantile_alpha", "huber_delta"):
             setattr(c, k, getattr(self, k))
         if self.monotone:
             self._mono = np.asarray(self.monotone, dtype=np.int32)

@@ -133,7 +133,7 @@ FlatTree flatten(DenseTree const &t)
 struct ref_cfg
     {
         int32_t  grower;    // 0 depthwise, 1 levelwise (oblivious), 2 leafwise
-        int32_t  objective; // 0 mse, 1 logloss, 2 softmax
+        int32_t  objective; // 0 mse, 1 logloss, 2 softmax, 3 poisson, 4 mae, 5 huber, 6 quantile
         uint32_t n_iters;
         float    learning_rate;
         float    min_child_hess;
@@ -152,6 +152,8 @@ struct ref_cfg
         int32_t const *monotone;
         uint32_t       n_monotone;
         char const    *interaction; // groups as the TOML strings, ';'-separated, or null
+        float          quantile_alpha;
+        float          huber_delta;
     };
 
     struct RefModel
@@ -203,6 +205,8 @@ namespace
         cfg.booster_config.random_seed   = c.random_seed;
         cfg.sampler.subsample            = c.subsample;
         cfg.objective.n_classes          = c.n_classes;
+        cfg.objective.quantile_alpha     = c.quantile_alpha;
+        cfg.objective.huber_delta        = c.huber_delta;
         return cfg;
     }
 
@@ -219,6 +223,12 @@ namespace
             return std::make_unique<MulticlassBooster<Gr, Sa>>(cfg);
         case 3:
             return std::make_unique<Booster<PoissonObjective, Gr, Sa>>(cfg);
+        case 4:
+            return std::make_unique<Booster<MAEObjective, Gr, Sa>>(cfg);
+        case 5:
+            return std::make_unique<Booster<HuberObjective, Gr, Sa>>(cfg);
+        case 6:
+            return std::make_unique<Booster<QuantileObjective, Gr, Sa>>(cfg);
         default:
             throw std::runtime_error("unknown objective");
         }
@@ -277,6 +287,9 @@ namespace
             ok = go(dynamic_cast<Booster<MSEObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<LogLossObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<PoissonObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<MAEObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<HuberObjective, Gr, BernoulliSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<QuantileObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<MulticlassBooster<Gr, BernoulliSampler> *>(raw));
         }
         else
@@ -284,6 +297,9 @@ namespace
             ok = go(dynamic_cast<Booster<MSEObjective, Gr, AllRowsSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<LogLossObjective, Gr, AllRowsSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<PoissonObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<MAEObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<HuberObjective, Gr, AllRowsSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<QuantileObjective, Gr, AllRowsSampler> *>(raw)) ||
                  go(dynamic_cast<MulticlassBooster<Gr, AllRowsSampler> *>(raw));
         }
         if (!ok)

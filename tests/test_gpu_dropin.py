@@ -65,3 +65,25 @@ def test_reference_booster_over_b200_grower_logloss(dref):
     # host objective on both sides: the same gradients, the same trees
     for i in range(tc.n_iters):
         assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+
+
+@pytest.mark.parametrize("objective,kw", [("mae", {}), ("huber", dict(huber_delta=0.5)),
+                                          ("quantile", dict(quantile_alpha=0.8))])
+@pytest.mark.parametrize("subsample", [1.0, 0.8])
+def test_reference_booster_over_b200_grower_renewed_leaves(dref, objective, kw, subsample):
+    """The host objectives whose booster renews every leaf from its rows'
+    residuals (Booster::renew_leaves, include/bonsai/booster.hpp:561-591,
+    763-785: MAE and quantile take the leaf's residual quantile, Huber its
+    own rule) read each row's leaf id from the grower -- sampled rows from
+    their leaf segments, the rest routed through the finished tree -- so the
+    renewed models agree only if every id does."""
+    X, y = _data(seed=11)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(objective=objective, max_depth=5, n_iters=10, learning_rate=0.2,
+                 subsample=subsample, **kw)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+    assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
