@@ -1,18 +1,22 @@
-// B200DepthwiseGrower: the reference-side binding of the B200 growers.
+// B200DepthwiseGrower, B200ObliviousGrower, B200LeafwiseGrower: the
+// reference-side binding of the B200 growers.
 //
-// A C++ grower satisfying bonsai's TreeGrower concept
+// C++ growers satisfying bonsai's TreeGrower concept
 // (include/bonsai/grower.hpp:54-62) and the booster's grower seams
 // (recycle, resident_begin/end, eval_begin/accumulate; booster.hpp:562-676,
-// 1008-1021), implemented entirely through the C ABI in bonsai_b200.h. It
-// compiles against bonsai's own headers, so a maintainer drops it into
-// include/bonsai/cuda/ and registers it beside CudaDepthwiseGrower
+// 1008-1021), implemented entirely through the C ABI in bonsai_b200.h. They
+// compile against bonsai's own headers, so a maintainer drops this file into
+// include/bonsai/cuda/ and registers each beside its Cuda* twin
 // (include/bonsai/registry/typelists.hpp:19-22). One grow() call is one
-// DepthwiseGrower<CudaHistogramEngine>::grow (src/grower_impl.hpp:465-577):
-// the same feature draw (std::sample over the ids with a mt19937 seeded by
+// grow of the reference's grower -- DepthwiseGrower (src/grower_impl.hpp:
+// 465-577), ObliviousGrower (:579-720) or LeafwiseGrower (:744-850): the same
+// feature draw (std::sample over the ids with a mt19937 seeded by
 // feature_seed, as sample_features does, grower_impl.hpp:165-180), the same
-// DenseTree node table, the same per-row values and leaf ids, rows outside
-// the sample routed through the finished tree in bin space
-// (route_unsampled, grower_impl.hpp:438-461).
+// tree (a DenseTree node table, or the ObliviousTree's level splits, leaf
+// table, level gains and leaf covers), the same per-row values and leaf ids
+// (DenseTree node ids, or leaf-table indices), rows outside the sample
+// routed through the finished tree in bin space (route_unsampled,
+// grower_impl.hpp:438-461; the level walk, :705-725).
 //
 // Status codes rethrow as the reference does: BB_ERR_CONFIG as
 // bonsai::ConfigError, everything else as std::runtime_error.
@@ -29,12 +33,12 @@
 #include <cstdint>
 #include <iterator>
 #include <numeric>
-#include <string>
 #include <optional>
 #include <random>
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace bonsai
@@ -54,18 +58,18 @@ inline void b200_rethrow(int rc)
     throw std::runtime_error(msg);
 }
 
-class B200DepthwiseGrower
+// Kind: bb_train_cfg.grower -- 0 depthwise, 1 levelwise (oblivious), 2 leafwise.
+template <int Kind> class B200Grower
 {
   public:
-    using Tree = DenseTree;
+    using Tree = std::conditional_t<Kind == 1, ObliviousTree, DenseTree>;
 
-    explicit B200DepthwiseGrower(TreeConfig const &cfg)
-        : config_(cfg), feature_rng_(cfg.feature_seed)
+    explicit B200Grower(TreeConfig const &cfg) : config_(cfg), feature_rng_(cfg.feature_seed)
     {
     }
-    B200DepthwiseGrower(B200DepthwiseGrower const &)            = delete;
-    B200DepthwiseGrower &operator=(B200DepthwiseGrower const &) = delete;
-    ~B200DepthwiseGrower()
+    B200Grower(B200Grower const &)            = delete;
+    B200Grower &operator=(B200Grower const &) = delete;
+    ~B200Grower()
     {
         if (plane_ != nullptr)
         {
@@ -81,6 +85,8 @@ class B200DepthwiseGrower
         std::vector<int8_t>         mono(config_.monotone_constraints.begin(),
                                          config_.monotone_constraints.end());
         bb_train_cfg c{};
+        c.grower            = Kind;
+        c.max_leaves        = Kind == 2 ? config_.max_leaves : 0;
         c.objective         = 0;
         c.learning_rate     = 1.0F;
         c.min_child_hess    = config_.min_child_hess;
@@ -116,7 +122,7 @@ class B200DepthwiseGrower
         c.interaction_features = ifeat.empty() ? nullptr : ifeat.data();
         c.interaction_offsets  = ioff.data();
         c.n_interaction_groups = static_cast<uint32_t>(ioff.size() - 1);
-        size_t const cap    = (size_t{2} << config_.max_depth) - 1;
+        size_t const cap    = std::max<uint32_t>(bb_tree_capacity(&c), 1);
         std::vector<uint32_t> feat(cap), left(cap), right(cap), split_bin(cap), meta(3);
         std::vector<float>    value(cap), gain(cap), cover(cap);
         std::vector<uint8_t>  dl(cap);
@@ -130,23 +136,16 @@ class B200DepthwiseGrower
                                   gain.data(), cover.data(), split_bin.data(), meta.data(),
                                   values.data(), leaf_ids.data()));
         size_t const n_nodes = meta[0];
-        Tree::Nodes  nodes(n_nodes);
-        for (size_t i = 0; i < n_nodes; ++i)
+        if constexpr (Kind == 1)
         {
-            nodes[i] = feat[i] == DenseTree::k_leaf_flag
-                           ? DenseTree::leaf(value[i])
-                           : DenseTree::internal(feat[i], value[i], left[i], right[i],
-                                                 dl[i] != 0);
+            return oblivious(ds, rows, all, feat, value, left, dl, gain, cover, split_bin,
+                             std::move(values), std::move(leaf_ids));
         }
-        if (!all)
+        else
         {
-            route_unsampled(ds, nodes, split_bin, rows, values, leaf_ids);
+            return dense(ds, rows, all, n_nodes, meta, feat, value, left, right, dl, gain,
+                         cover, split_bin, std::move(values), std::move(leaf_ids));
         }
-        return {.tree     = Tree(std::move(nodes), {.depth = meta[1], .n_leaves = meta[2]},
-                                 std::vector<float>(gain.begin(), gain.begin() + n_nodes),
-                                 std::vector<float>(cover.begin(), cover.begin() + n_nodes)),
-                .values   = std::move(values),
-                .leaf_ids = std::move(leaf_ids)};
     }
 
     // The booster's seams. The per-row buffers are rebuilt every grow, so
@@ -173,6 +172,93 @@ class B200DepthwiseGrower
     }
 
   private:
+    GrowResult<DenseTree> dense(Dataset const &ds, row_index_view rows, bool all, size_t n_nodes,
+                                std::vector<uint32_t> const &meta,
+                                std::vector<uint32_t> const &feat, std::vector<float> const &value,
+                                std::vector<uint32_t> const &left,
+                                std::vector<uint32_t> const &right,
+                                std::vector<uint8_t> const &dl, std::vector<float> const &gain,
+                                std::vector<float> const     &cover,
+                                std::vector<uint32_t> const  &split_bin,
+                                train_leaf_values values, std::vector<node_id_t> leaf_ids)
+    {
+        DenseTree::Nodes nodes(n_nodes);
+        for (size_t i = 0; i < n_nodes; ++i)
+        {
+            nodes[i] = feat[i] == DenseTree::k_leaf_flag
+                           ? DenseTree::leaf(value[i])
+                           : DenseTree::internal(feat[i], value[i], left[i], right[i],
+                                                 dl[i] != 0);
+        }
+        if (!all)
+        {
+            route_unsampled(ds, nodes, split_bin, rows, values, leaf_ids);
+        }
+        return {.tree     = DenseTree(std::move(nodes), {.depth = meta[1], .n_leaves = meta[2]},
+                                      std::vector<float>(gain.begin(), gain.begin() + n_nodes),
+                                      std::vector<float>(cover.begin(), cover.begin() + n_nodes)),
+                .values   = std::move(values),
+                .leaf_ids = std::move(leaf_ids)};
+    }
+
+    // The levelwise tree comes back perfect and in level order (level L
+    // starts at node 2^L - 1, leaves in the reference's path order): each
+    // level's split, gain and bin from its first node, the leaf table and
+    // leaf covers from the last level; a leaf id becomes its table index.
+    GrowResult<ObliviousTree> oblivious(Dataset const &ds, row_index_view rows, bool all,
+                                        std::vector<uint32_t> const &feat,
+                                        std::vector<float> const    &value,
+                                        std::vector<uint32_t> const &left,
+                                        std::vector<uint8_t> const  &dl,
+                                        std::vector<float> const    &gain,
+                                        std::vector<float> const    &cover,
+                                        std::vector<uint32_t> const &split_bin,
+                                        train_leaf_values values, std::vector<node_id_t> leaf_ids)
+    {
+        ObliviousTree::LevelSplits splits;
+        std::vector<float>         level_gains;
+        std::vector<bin_id_t>      level_bins;
+        size_t                     idx = 0;
+        while (feat[idx] != DenseTree::k_leaf_flag)
+        {
+            splits.push_back({.feature_id   = static_cast<feature_id_t>(feat[idx]),
+                              .threshold    = value[idx],
+                              .default_left = dl[idx] != 0});
+            level_gains.push_back(gain[idx]);
+            level_bins.push_back(static_cast<bin_id_t>(split_bin[idx]));
+            idx = left[idx];
+        }
+        size_t const       first = (size_t{1} << splits.size()) - 1;
+        size_t const       n_lf  = size_t{1} << splits.size();
+        std::vector<float> table(value.begin() + first, value.begin() + first + n_lf);
+        std::vector<float> covers(cover.begin() + first, cover.begin() + first + n_lf);
+        size_t             j = 0;
+        for (size_t r = 0; r < ds.n_rows(); ++r)
+        {
+            if (all || (j < rows.size() && rows[j] == r))
+            {
+                ++j;
+                leaf_ids[r] = static_cast<node_id_t>(leaf_ids[r] - first);
+                continue;
+            }
+            size_t index = 0;
+            for (size_t lvl = 0; lvl < splits.size(); ++lvl)
+            {
+                auto const    &sp   = splits[lvl];
+                auto const     last = static_cast<bin_id_t>(ds.n_bins(sp.feature_id) - 1);
+                bin_id_t const b    = ds.bin_at(sp.feature_id, static_cast<row_id_t>(r));
+                index = (index << 1U) |
+                        (routes_left(b, last, level_bins[lvl], sp.default_left) ? 0U : 1U);
+            }
+            values[r]   = table[index];
+            leaf_ids[r] = static_cast<node_id_t>(index);
+        }
+        return {.tree     = ObliviousTree(std::move(splits), std::move(table),
+                                          std::move(level_gains), std::move(covers)),
+                .values   = std::move(values),
+                .leaf_ids = std::move(leaf_ids)};
+    }
+
     // The device plane for ds, built once per Dataset from its host columns.
     void bind(Dataset const &ds)
     {
@@ -249,7 +335,7 @@ class B200DepthwiseGrower
         return selected;
     }
 
-    static void route_unsampled(Dataset const &ds, Tree::Nodes const &nodes,
+    static void route_unsampled(Dataset const &ds, DenseTree::Nodes const &nodes,
                                 std::vector<uint32_t> const &split_bin, row_index_view rows,
                                 train_leaf_values &values, std::vector<node_id_t> &leaf_ids)
     {
@@ -284,6 +370,12 @@ class B200DepthwiseGrower
     size_t         bound_rows_ = 0;
 };
 
+using B200DepthwiseGrower = B200Grower<0>;
+using B200ObliviousGrower = B200Grower<1>;
+using B200LeafwiseGrower  = B200Grower<2>;
+
 static_assert(TreeGrower<B200DepthwiseGrower>);
+static_assert(TreeGrower<B200ObliviousGrower>);
+static_assert(TreeGrower<B200LeafwiseGrower>);
 
 } // namespace bonsai

@@ -745,33 +745,49 @@ extern "C"
 // on ds; the model handle reads back like ref_train's.
 #include "bonsai_b200_grower.hpp"
 
+namespace
+{
+// The reference's booster over one of the shims (Gr), trained and harvested.
+template <typename Gr> RefModel *b200_train_with(Dataset const &ds, ref_cfg const &c)
+{
+    Config cfg = make_config(c);
+    parallel::set_n_threads(c.n_threads);
+    auto mm     = std::make_unique<RefModel>();
+    mm->grower  = c.grower;
+    mm->booster = make_for_sampler<Gr>(c, cfg);
+    for (uint32_t i = 0; i < c.n_iters; ++i)
+    {
+        mm->booster->update_one_iter(ds);
+    }
+    harvest<Gr>(*mm, c);
+    auto *raw = mm->booster.get();
+    read_init(*mm, dynamic_cast<Booster<MSEObjective, Gr, AllRowsSampler> const *>(raw));
+    read_init(*mm, dynamic_cast<Booster<LogLossObjective, Gr, AllRowsSampler> const *>(raw));
+    read_init(*mm, dynamic_cast<Booster<MSEObjective, Gr, BernoulliSampler> const *>(raw));
+    read_init(*mm, dynamic_cast<Booster<LogLossObjective, Gr, BernoulliSampler> const *>(raw));
+    return mm.release();
+}
+} // namespace
+
 extern "C" void *ref_b200_train(void const *dsp, ref_cfg const *c)
 {
     RefModel *m  = nullptr;
     int const rc = guarded(
         [&]
         {
-            auto const &ds  = *static_cast<Dataset const *>(dsp);
-            Config      cfg = make_config(*c);
-            parallel::set_n_threads(c->n_threads);
-            auto mm         = std::make_unique<RefModel>();
-            mm->grower      = 0;
-            mm->booster     = make_for_sampler<B200DepthwiseGrower>(*c, cfg);
-            for (uint32_t i = 0; i < c->n_iters; ++i)
+            auto const &ds = *static_cast<Dataset const *>(dsp);
+            switch (c->grower)
             {
-                mm->booster->update_one_iter(ds);
+            case 1:
+                m = b200_train_with<B200ObliviousGrower>(ds, *c);
+                break;
+            case 2:
+                m = b200_train_with<B200LeafwiseGrower>(ds, *c);
+                break;
+            default:
+                m = b200_train_with<B200DepthwiseGrower>(ds, *c);
+                break;
             }
-            harvest<B200DepthwiseGrower>(*mm, *c);
-            auto *raw = mm->booster.get();
-            read_init(*mm, dynamic_cast<Booster<MSEObjective, B200DepthwiseGrower,
-                                                AllRowsSampler> const *>(raw));
-            read_init(*mm, dynamic_cast<Booster<LogLossObjective, B200DepthwiseGrower,
-                                                AllRowsSampler> const *>(raw));
-            read_init(*mm, dynamic_cast<Booster<MSEObjective, B200DepthwiseGrower,
-                                                BernoulliSampler> const *>(raw));
-            read_init(*mm, dynamic_cast<Booster<LogLossObjective, B200DepthwiseGrower,
-                                                BernoulliSampler> const *>(raw));
-            m = mm.release();
         });
     return rc == 0 ? m : nullptr;
 }

@@ -87,3 +87,35 @@ def test_reference_booster_over_b200_grower_renewed_leaves(dref, objective, kw, 
     for i in range(tc.n_iters):
         assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
     assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
+
+
+@pytest.mark.parametrize("grower,cfg", [
+    ("leafwise", dict(max_leaves=31, max_depth=12, n_iters=15)),
+    ("leafwise", dict(max_leaves=63, max_depth=255, n_iters=10, subsample=0.8,
+                      feature_fraction=0.5, lambda_l1=0.2)),
+    ("leafwise", dict(max_leaves=31, max_depth=8, n_iters=8, objective="mae", subsample=0.8)),
+    ("levelwise", dict(max_depth=6, n_iters=15)),
+    ("levelwise", dict(max_depth=7, n_iters=10, subsample=0.8, feature_fraction=0.6,
+                       min_child_hess=4.0)),
+    ("levelwise", dict(max_depth=5, n_iters=8, objective="quantile", quantile_alpha=0.3,
+                       subsample=0.8)),
+])
+def test_reference_booster_over_leafwise_and_levelwise_shims(dref, grower, cfg):
+    """The same drop-in check for B200LeafwiseGrower and B200ObliviousGrower
+    (include/bonsai_b200_grower.hpp): the reference's booster over each equals
+    it over the reference's LeafwiseGrower / ObliviousGrower, tree for tree --
+    a levelwise model's ObliviousTree tables too, its leaf ids being leaf-table
+    indices (the quantile objective renews leaves by them)."""
+    X, y = _data(seed=13)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(grower=grower, learning_rate=0.2, **cfg)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    assert cpu.n_trees() == gpu.n_trees() == tc.n_iters
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+        if grower == "levelwise":
+            for a, b in zip(gpu.oblivious(i), cpu.oblivious(i)):
+                assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
