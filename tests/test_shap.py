@@ -287,3 +287,35 @@ def test_shap_plan_long_paths(bb, depth, n):
     phi = bb.ShapPlan(plane, trees, 0.25, 0.2).run(plane)
     ref = shap_numpy(codes.T.astype(np.int64), nb.astype(np.int64) - 1, trees, 0.25, 0.2)
     np.testing.assert_allclose(phi, ref, rtol=RTOL, atol=1e-11)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grower,kw", [
+    ("levelwise", dict(max_depth=6)),
+    ("leafwise", dict(max_leaves=31, max_depth=10)),
+    ("depthwise", dict(max_depth=6, subsample=0.7, feature_fraction=0.6)),
+])
+def test_device_contribs_match_live_reference_per_grower(bb, ref, grower, kw):
+    """Against the live reference's pred_contribs_binned (include/bonsai/
+    booster.hpp:887-924) on the same model: a levelwise ensemble (the reference
+    explains each ObliviousTree through its preorder dense_equivalent, src/
+    tree.cpp:64-117; here the level-order tree the device grew), a leafwise one,
+    and a depthwise one grown over row and feature samples (covers count the
+    sampled rows)."""
+    from oracle import TreeCfg
+    rng = np.random.Generator(np.random.PCG64(41))
+    n, F = 4_000, 7
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    X[rng.random((n, F)) < 0.06] = np.nan
+    x = np.nan_to_num(X)
+    y = (np.sin(2 * x[:, 0]) + x[:, 1] * x[:, 2] + 0.2 * rng.standard_normal(n)).astype(np.float32)
+    cuts, off = ref.fit_cuts(X)
+    ds = ref.dataset(X, y, cuts, off)
+    tc = dict(grower=grower, learning_rate=0.1, **kw)
+    m = ref.train(ds, TreeCfg(n_iters=12, **tc))
+    plane = bb.Plane(X, cuts, off)
+    b = bb.Booster(plane, y, bb.TrainParams(use_graph=grower != "leafwise", **tc), max_trees=12)
+    b.update(12)
+    phi = bb.pred_contribs(plane, b.trees(), b.init_score, 0.1)
+    want = m.contribs_binned(ds)
+    np.testing.assert_allclose(phi, want, rtol=RTOL, atol=ATOL)
