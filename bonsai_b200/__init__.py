@@ -26,7 +26,7 @@ from .binning import cuts_from_sample, fit_cuts, sample_rows
 
 __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
-    "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "oblivious_tables", "fit_cuts",
+    "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "pred_contribs_classes", "oblivious_tables", "fit_cuts",
     "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows", "fit_cuts_device",
     "available", "LEAF",
 ]
@@ -718,6 +718,16 @@ class PredictPlan:
             self.close()
         except Exception:
             pass
+
+
+def pred_contribs_classes(plane: Plane, trees: list, init_scores, lr: float) -> np.ndarray:
+    """TreeSHAP of a softmax ensemble whose trees are round-major (tree r * K + k
+    is class k's): n_rows x K x (n_feats + 1), class k's contributions scaled
+    by lr with its initial score in the bias column, as MulticlassBooster
+    composes them (include/bonsai/multiclass_booster.hpp:411-436)."""
+    K = len(init_scores)
+    return np.stack([pred_contribs(plane, trees[k::K], float(init_scores[k]), lr)
+                     for k in range(K)], axis=1)
 
 
 def predict_classes(plane: Plane, trees: list, init_scores, lr: float) -> np.ndarray:

@@ -313,7 +313,15 @@ class RefModel:
         n = L.ref_model_init_scores(C.c_void_p(self.h), out.ctypes.data, 64)
         return out[:n].copy()
 
-    def contribs_binned(self, ds):
+    def contribs_binned(self, ds, n_classes: int = 1):
+        """n x (F + 1), or n x n_classes x (F + 1) for a multiclass model."""
+        if n_classes > 1:
+            out = np.empty((ds.n, n_classes, ds.F + 1), np.float64)
+            f = self.lib.L.ref_model_contribs_binned_k
+            f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
+            if f(C.c_void_p(self.h), C.c_void_p(ds.h), out.ctypes.data, n_classes):
+                raise RuntimeError(self.lib.err())
+            return out
         out = np.empty((ds.n, ds.F + 1), np.float64)
         if self.lib.L.ref_model_contribs_binned(C.c_void_p(self.h), C.c_void_p(ds.h),
                                                 out.ctypes.data):

@@ -649,6 +649,22 @@ extern "C"
             });
     }
 
+    // The same for a model of n_classes outputs: out holds n x n_classes x (F + 1)
+    // (MulticlassBooster's layout, include/bonsai/multiclass_booster.hpp:411-436).
+    int ref_model_contribs_binned_k(void const *mp, void const *dsp, double *out,
+                                    size_t n_classes)
+    {
+        return guarded(
+            [&]
+            {
+                auto const  *m  = static_cast<RefModel const *>(mp);
+                auto const  &ds = *static_cast<Dataset const *>(dsp);
+                size_t const F  = ds.n_features();
+                m->booster->pred_contribs_binned(ds, {out, ds.n_rows() * n_classes * (F + 1)},
+                                                 F);
+            });
+    }
+
     // Grows ONE depthwise/levelwise/leafwise tree on given grad/hess over the
     // given ascending rows, through the reference's CPU grower. Outputs the
     // per-row leaf values and leaf ids over all ds rows (unsampled rows are

@@ -319,3 +319,32 @@ def test_device_contribs_match_live_reference_per_grower(bb, ref, grower, kw):
     phi = bb.pred_contribs(plane, b.trees(), b.init_score, 0.1)
     want = m.contribs_binned(ds)
     np.testing.assert_allclose(phi, want, rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grower", ["depthwise", "levelwise"])
+def test_softmax_contribs_match_live_reference(bb, ref, grower):
+    """A softmax ensemble's per-class contributions (n x K x (F + 1),
+    MulticlassBooster's layout and composition) on the reference's own model
+    (its trees, split bins recovered from their thresholds; a levelwise model
+    through its preorder dense_equivalent) against the live reference's; each
+    class's contributions sum to its raw score."""
+    from oracle import TreeCfg
+    from bonsai_b200 import synth
+    from bonsai_b200.model import _split_bins
+    K = 3
+    X, y = synth.multiclass_onehot(n=3_000, n_classes=K)
+    cuts, off = ref.fit_cuts(X)
+    ds = ref.dataset(X, y, cuts, off)
+    m = ref.train(ds, TreeCfg(objective="softmax", n_classes=K, grower=grower, max_depth=4,
+                              n_iters=6, learning_rate=0.1))
+    trees = [bb.Tree(feature=t.feature, value=t.value, left=t.left, right=t.right,
+                     default_left=t.default_left, gains=t.gains, covers=t.covers,
+                     split_bin=_split_bins(t.feature, t.value, cuts, off)) for t in m.trees()]
+    plane = bb.Plane(X, cuts, off)
+    init = m.init_scores()
+    phi = bb.pred_contribs_classes(plane, trees, init, 0.1)
+    want = m.contribs_binned(ds, n_classes=K)
+    np.testing.assert_allclose(phi, want, rtol=RTOL, atol=ATOL)
+    raw = bb.predict_classes(plane, trees, init, 0.1).astype(np.float64)
+    np.testing.assert_allclose(phi.sum(axis=2), raw, rtol=0, atol=1e-5)
