@@ -448,3 +448,28 @@ def from_booster(booster, cuts, cut_off, n_iters: int | None = None, feature_nam
                  cut_off=np.asarray(cut_off, np.uint32), trees=trees,
                  init_scores=np.asarray(booster.init_scores, np.float32),
                  feature_names=list(feature_names) if feature_names is not None else [])
+
+
+def warm_start(model: Model, plane, labels, params, max_trees: int, weights=None):
+    """A Booster that continues `model` over `plane` (the reference's warm start,
+    include/bonsai/booster.hpp:512-524): every row's starting score is the
+    model's init + lr x (its trees' leaf values summed in tree order), the
+    reference's rebuilt training score bit for bit, and the new rounds grow
+    from it. Single-output models; params.learning_rate should be the model's.
+    `continued` joins the result back into one model."""
+    from . import Booster, predict
+    if model.objective == "softmax":
+        raise ValueError("warm_start: single-output models only")
+    scores = predict(plane, model.trees, model.init_score, model.learning_rate)
+    return Booster(plane, labels, params, max_trees=max_trees, init_scores=scores,
+                   weights=weights)
+
+
+def continued(model: Model, booster) -> Model:
+    """`model` with the trees a warm-started booster grew appended (its initial
+    score and bin mappers kept; the config counts every round)."""
+    cfg = copy.deepcopy(model.config)
+    trees = list(model.trees) + booster.trees()
+    cfg["booster_config"]["n_iters"] = len(trees) // max(1, model.n_classes)
+    return Model(config=cfg, cuts=model.cuts, cut_off=model.cut_off, trees=trees,
+                 init_scores=model.init_scores, feature_names=list(model.feature_names))

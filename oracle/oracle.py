@@ -178,6 +178,29 @@ class RefLib:
             raise RuntimeError(self.err())
         return RefModel(self, h)
 
+    def warm_train(self, ds, cfg: TreeCfg, trees, init_score):
+        """The reference's depthwise booster loaded with trees and init_score
+        (its warm start), trained cfg.n_iters more rounds; the model holds every
+        tree."""
+        off = np.concatenate([[0], np.cumsum([len(t.feature) for t in trees])]).astype(np.uint32)
+        types = dict(feature=np.uint32, value=np.float32, left=np.uint32, right=np.uint32,
+                     default_left=np.uint8, gains=np.float32, covers=np.float32)
+        # held in names for the call: a temporary's buffer could be freed first
+        cat = {k: np.ascontiguousarray(np.concatenate([np.asarray(getattr(t, k)) for t in trees]),
+                                       dtype=ty) for k, ty in types.items()}
+        depth = np.array([t.depth for t in trees], np.uint32)
+        n_leaves = np.array([t.n_leaves for t in trees], np.uint32)
+        f = self.L.ref_warm_train
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_void_p, C.POINTER(RefCfg), C.c_uint32] + [C.c_void_p] * 10 + [C.c_float]
+        rc = cfg.ref()
+        h = f(C.c_void_p(ds.h), C.byref(rc), len(trees), off.ctypes.data,
+              *(cat[k].ctypes.data for k in types), depth.ctypes.data, n_leaves.ctypes.data,
+              float(init_score))
+        if not h:
+            raise RuntimeError(self.err())
+        return RefModel(self, h)
+
     def train_b200(self, ds, cfg: TreeCfg):
         """The reference's Booster with B200DepthwiseGrower (needs REF_B200_SO)."""
         f = self.L.ref_b200_train

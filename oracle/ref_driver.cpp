@@ -649,6 +649,73 @@ extern "C"
             });
     }
 
+    // Warm start (include/bonsai/booster.hpp:512-524, load_state :1065-1069):
+    // the reference's depthwise booster loaded with n_trees given DenseTrees
+    // (node arrays concatenated, tree t's nodes at [off[t], off[t + 1])) and
+    // init_score, then trained c.n_iters more rounds; the model holds every
+    // tree, the loaded ones first. MSE and logloss, every row.
+    void *ref_warm_train(void const *dsp, ref_cfg const *c, uint32_t n_trees,
+                         uint32_t const *off, uint32_t const *feature, float const *value,
+                         uint32_t const *left, uint32_t const *right,
+                         uint8_t const *default_left, float const *gains,
+                         float const *covers, uint32_t const *depth,
+                         uint32_t const *n_leaves, float init_score)
+    {
+        RefModel *m  = nullptr;
+        int const rc = guarded(
+            [&]
+            {
+                auto const &ds  = *static_cast<Dataset const *>(dsp);
+                Config      cfg = make_config(*c);
+                parallel::set_n_threads(c->n_threads);
+                std::vector<DenseTree> trees;
+                for (uint32_t t = 0; t < n_trees; ++t)
+                {
+                    DenseTree::Nodes nodes;
+                    for (uint32_t i = off[t]; i < off[t + 1]; ++i)
+                    {
+                        nodes.push_back(feature[i] == DenseTree::k_leaf_flag
+                                            ? DenseTree::leaf(value[i])
+                                            : DenseTree::internal(feature[i], value[i],
+                                                                  left[i], right[i],
+                                                                  default_left[i] != 0));
+                    }
+                    trees.emplace_back(std::move(nodes),
+                                       DenseTree::Params{.depth = depth[t], .n_leaves = n_leaves[t]},
+                                       std::vector<float>(gains + off[t], gains + off[t + 1]),
+                                       std::vector<float>(covers + off[t], covers + off[t + 1]));
+                }
+                auto mm    = std::make_unique<RefModel>();
+                mm->grower = 0;
+                auto go    = [&](auto b)
+                {
+                    b->load_state(trees, init_score);
+                    for (uint32_t i = 0; i < c->n_iters; ++i)
+                    {
+                        b->update_one_iter(ds);
+                    }
+                    harvest_dense(*mm, *b);
+                    mm->init_scores = {b->init_score()};
+                    mm->booster     = std::move(b);
+                };
+                if (c->objective == 0)
+                {
+                    go(std::make_unique<Booster<MSEObjective, DepthwiseGrower<>, AllRowsSampler>>(cfg));
+                }
+                else if (c->objective == 1)
+                {
+                    go(std::make_unique<
+                        Booster<LogLossObjective, DepthwiseGrower<>, AllRowsSampler>>(cfg));
+                }
+                else
+                {
+                    throw std::runtime_error("ref_warm_train: mse or logloss");
+                }
+                m = mm.release();
+            });
+        return rc == 0 ? m : nullptr;
+    }
+
     // The same for a model of n_classes outputs: out holds n x n_classes x (F + 1)
     // (MulticlassBooster's layout, include/bonsai/multiclass_booster.hpp:411-436).
     int ref_model_contribs_binned_k(void const *mp, void const *dsp, double *out,
