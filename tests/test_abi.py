@@ -96,3 +96,33 @@ def test_fit_cuts_signed_zeros_match_reference(ref):
     cuts, off = bb.fit_cuts(X)
     assert np.array_equal(off, ro)
     assert np.array_equal(cuts.view(np.uint32), rc.view(np.uint32))
+
+
+@pytest.mark.parametrize("py_name,c_name", [("TrainCfg", "bb_train_cfg"),
+                                             ("Profile", "bb_profile")])
+def test_struct_layout_matches_the_header(tmp_path, py_name, c_name):
+    """The Python binding's structs (bonsai_b200._lib) have the C header's
+    layout: every field at the header's offset, the same size (fields are
+    appended over time; a mismatch would pass wrong values silently)."""
+    import shutil
+    import subprocess
+    from bonsai_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    T = getattr(_lib, py_name)
+    fields = [f[0] for f in T._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"bonsai_b200.h\"\n"
+                   "int main(void) {\n"
+                   + "".join(f'  printf("{f} %zu\\n", offsetof({c_name}, {f}));\n'
+                             for f in fields)
+                   + f'  printf("sizeof %zu\\n", sizeof({c_name}));\n  return 0;\n}}\n')
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = dict(line.split() for line in subprocess.run(
+        [str(exe)], check=True, capture_output=True, text=True).stdout.splitlines())
+    for f in fields:
+        assert int(got[f]) == getattr(T, f).offset, f
+    assert int(got["sizeof"]) == C.sizeof(T)
