@@ -42,6 +42,7 @@ class RefCfg(C.Structure):
         ("n_threads", C.c_uint32), ("n_classes", C.c_uint32),
         ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
         ("interaction", C.c_char_p), ("quantile_alpha", C.c_float), ("huber_delta", C.c_float),
+        ("dart_drop_rate", C.c_float),
     ]
 
 
@@ -73,6 +74,7 @@ class TreeCfg:
     n_classes: int = 3
     quantile_alpha: float = 0.5
     huber_delta: float = 1.0
+    dart_drop_rate: float = 0.0
     monotone: list = field(default_factory=list)
     interaction_constraints: list = field(default_factory=list)  # TOML strings, "0,1"
 
@@ -83,7 +85,8 @@ class TreeCfg:
         for k in ("n_iters", "learning_rate", "min_child_hess", "min_gain_to_split",
                   "lambda_l2", "lambda_l1", "feature_fraction", "max_depth",
                   "min_data_in_leaf", "max_leaves", "feature_seed", "subsample",
-                  "random_seed", "n_threads", "n_classes", "quantile_alpha", "huber_delta"):
+                  "random_seed", "n_threads", "n_classes", "quantile_alpha", "huber_delta",
+                  "dart_drop_rate"):
             setattr(c, k, getattr(self, k))
         if self.monotone:
             self._mono = np.asarray(self.monotone, dtype=np.int32)

@@ -154,6 +154,7 @@ struct ref_cfg
         char const    *interaction; // groups as the TOML strings, ';'-separated, or null
         float          quantile_alpha;
         float          huber_delta;
+        float          dart_drop_rate;
     };
 
     struct RefModel
@@ -207,6 +208,7 @@ namespace
         cfg.objective.n_classes          = c.n_classes;
         cfg.objective.quantile_alpha     = c.quantile_alpha;
         cfg.objective.huber_delta        = c.huber_delta;
+        cfg.booster_config.dart_drop_rate = c.dart_drop_rate;
         return cfg;
     }
 

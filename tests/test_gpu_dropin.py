@@ -119,3 +119,21 @@ def test_reference_booster_over_leafwise_and_levelwise_shims(dref, grower, cfg):
             for a, b in zip(gpu.oblivious(i), cpu.oblivious(i)):
                 assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
     assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
+
+
+@pytest.mark.parametrize("cfg", [dict(dart_drop_rate=0.3),
+                                 dict(dart_drop_rate=0.5, subsample=0.8, feature_fraction=0.7)])
+def test_reference_booster_over_b200_grower_dart(dref, cfg):
+    """DART (booster_config.dart_drop_rate; drop_dart_trees / apply_dart_round,
+    include/bonsai/booster.hpp:535-540,700-760) runs the reference's host round
+    -- trees dropped, gradients against the thinned model, dropped and new
+    trees rescaled -- over the shim as over the CPU grower: the same model."""
+    X, y = _data(seed=17)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(max_depth=5, n_iters=12, learning_rate=0.2, **cfg)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+    assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
