@@ -42,7 +42,8 @@ class RefCfg(C.Structure):
         ("n_threads", C.c_uint32), ("n_classes", C.c_uint32),
         ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
         ("interaction", C.c_char_p), ("quantile_alpha", C.c_float), ("huber_delta", C.c_float),
-        ("dart_drop_rate", C.c_float),
+        ("dart_drop_rate", C.c_float), ("goss_top_rate", C.c_float),
+        ("goss_other_rate", C.c_float),
     ]
 
 
@@ -75,6 +76,8 @@ class TreeCfg:
     quantile_alpha: float = 0.5
     huber_delta: float = 1.0
     dart_drop_rate: float = 0.0
+    goss_top_rate: float = 0.0  # > 0 selects the GOSS sampler
+    goss_other_rate: float = 0.1
     monotone: list = field(default_factory=list)
     interaction_constraints: list = field(default_factory=list)  # TOML strings, "0,1"
 
@@ -86,7 +89,7 @@ class TreeCfg:
                   "lambda_l2", "lambda_l1", "feature_fraction", "max_depth",
                   "min_data_in_leaf", "max_leaves", "feature_seed", "subsample",
                   "random_seed", "n_threads", "n_classes", "quantile_alpha", "huber_delta",
-                  "dart_drop_rate"):
+                  "dart_drop_rate", "goss_top_rate", "goss_other_rate"):
             setattr(c, k, getattr(self, k))
         if self.monotone:
             self._mono = np.asarray(self.monotone, dtype=np.int32)

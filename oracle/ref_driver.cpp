@@ -155,6 +155,8 @@ struct ref_cfg
         float          quantile_alpha;
         float          huber_delta;
         float          dart_drop_rate;
+        float          goss_top_rate;   // > 0 selects the GOSS sampler
+        float          goss_other_rate;
     };
 
     struct RefModel
@@ -209,6 +211,11 @@ namespace
         cfg.objective.quantile_alpha     = c.quantile_alpha;
         cfg.objective.huber_delta        = c.huber_delta;
         cfg.booster_config.dart_drop_rate = c.dart_drop_rate;
+        if (c.goss_top_rate > 0.0F)
+        {
+            cfg.sampler.top_rate   = c.goss_top_rate;
+            cfg.sampler.other_rate = c.goss_other_rate;
+        }
         return cfg;
     }
 
@@ -239,6 +246,10 @@ namespace
     template <typename Gr>
     std::unique_ptr<IBooster> make_for_sampler(ref_cfg const &c, Config const &cfg)
     {
+        if (c.goss_top_rate > 0.0F)
+        {
+            return make_for_objective<Gr, GossSampler>(c, cfg);
+        }
         if (c.subsample < 1.0F)
         {
             return make_for_objective<Gr, BernoulliSampler>(c, cfg);
@@ -284,7 +295,17 @@ namespace
             return true;
         };
         bool ok = false;
-        if (c.subsample < 1.0F)
+        if (c.goss_top_rate > 0.0F)
+        {
+            ok = go(dynamic_cast<Booster<MSEObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<LogLossObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<PoissonObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<MAEObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<HuberObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<Booster<QuantileObjective, Gr, GossSampler> *>(raw)) ||
+                 go(dynamic_cast<MulticlassBooster<Gr, GossSampler> *>(raw));
+        }
+        else if (c.subsample < 1.0F)
         {
             ok = go(dynamic_cast<Booster<MSEObjective, Gr, BernoulliSampler> *>(raw)) ||
                  go(dynamic_cast<Booster<LogLossObjective, Gr, BernoulliSampler> *>(raw)) ||

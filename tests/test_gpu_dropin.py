@@ -137,3 +137,21 @@ def test_reference_booster_over_b200_grower_dart(dref, cfg):
     for i in range(tc.n_iters):
         assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
     assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
+
+
+@pytest.mark.parametrize("grower", ["depthwise", "leafwise", "levelwise"])
+def test_reference_booster_over_b200_grower_goss(dref, grower):
+    """GOSS (GossSampler, src/sampler.cpp:57-125: the top_rate rows by |g| and an
+    amplified other_rate draw of the rest) chooses rows from the gradients and
+    scales theirs, then hands both to the grower: over each shim the same
+    model as over the reference's CPU grower of that kind."""
+    X, y = _data(seed=19)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(grower=grower, max_depth=5, max_leaves=31, n_iters=10, learning_rate=0.2,
+                 goss_top_rate=0.2, goss_other_rate=0.15)
+    cpu = dref.train(ds, tc)
+    gpu = dref.train_b200(ds, tc)
+    for i in range(tc.n_iters):
+        assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+    assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
