@@ -58,12 +58,15 @@ def _sharded(bb, X, y, cuts, off, params, k, rounds, init):
     return boosters
 
 
-@pytest.mark.parametrize("k,grower", [(2, "depthwise"), (3, "levelwise")])
-def test_group_shards_equal_unsharded_fit(bb, k, grower):
+@pytest.mark.parametrize("k,grower,ff", [(2, "depthwise", 1.0), (3, "levelwise", 1.0),
+                                         (2, "depthwise", 0.5), (3, "levelwise", 0.6)])
+def test_group_shards_equal_unsharded_fit(bb, k, grower, ff):
+    # ff < 1: every shard draws each tree's features from the same seed
     X, y = _data(3 + k)
     cuts, off = bb.fit_cuts(X)
     params = bb.TrainParams(objective="logloss", grower=grower, max_depth=6,
-                            hist_mode="int8", seed=9, learning_rate=0.2)
+                            hist_mode="int8", seed=9, learning_rate=0.2, feature_fraction=ff,
+                            feature_seed=4)
     rounds = 6
     full = bb.Booster(bb.Plane(X, cuts, off), y, params, max_trees=rounds)
     full.update(rounds)
