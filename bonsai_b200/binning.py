@@ -21,6 +21,27 @@ from __future__ import annotations
 import numpy as np
 
 FLT_MAX = np.float32(np.finfo(np.float32).max)
+_MID_HI = np.float32(FLT_MAX / np.float32(2.0))                     # halving is exact
+_MID_LO = np.float32(np.finfo(np.float32).tiny) * np.float32(2.0)   # 2 x smallest normal
+
+
+def midpoint(a, b) -> np.float32:
+    """std::midpoint for float (the greedy rule's cut, src/bin_mapper.cpp:95):
+    the correctly rounded half-sum that never overflows. With both magnitudes
+    at most FLT_MAX/2 the sum cannot overflow and (a + b) / 2 is exact up to
+    one rounding; above that each operand is halved before the add, except one
+    so small (below twice the smallest normal) that halving it would round --
+    that one is added whole. These are the cases the C++ standard's midpoint
+    proposal (P0811) states."""
+    a = np.float32(a)
+    b = np.float32(b)
+    if abs(a) <= _MID_HI and abs(b) <= _MID_HI:
+        return np.float32((a + b) / np.float32(2.0))
+    if abs(a) < _MID_LO:
+        return np.float32(a + b / np.float32(2.0))
+    if abs(b) < _MID_LO:
+        return np.float32(a / np.float32(2.0) + b)
+    return np.float32(a / np.float32(2.0) + b / np.float32(2.0))
 
 
 def _greedy(vals: np.ndarray, counts: np.ndarray, n_samples: int, budget: int,
@@ -40,7 +61,7 @@ def _greedy(vals: np.ndarray, counts: np.ndarray, n_samples: int, budget: int,
             rest_sum -= int(counts[i])
         in_bin += int(counts[i])
         if is_big[i] or in_bin >= bin_size or (is_big[i + 1] and in_bin >= bin_size / 2.0):
-            mid = np.float32((vals[i] + vals[i + 1]) / np.float32(2.0))
+            mid = midpoint(vals[i], vals[i + 1])
             if not cuts or cuts[-1] < mid:
                 cuts.append(mid)
             in_bin = 0

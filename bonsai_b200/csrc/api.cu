@@ -2043,7 +2043,10 @@ extern "C"
 // leaves the last ensemble in it: calls whose work overlaps on the GPU (from
 // several host threads, or before the previous call's kernel has run) race
 // on it. The kernel runs on the legacy default stream and the call returns
-// once it is enqueued; synchronise that stream before reading out.
+// once it is enqueued; synchronise that stream before reading out. The
+// plane's device must be the calling thread's current device (refused with
+// BB_ERR_CONFIG otherwise), and a plane with no rows (a request plane before
+// its first refill) returns success without touching the array.
 
 namespace bb
 {
@@ -2172,6 +2175,17 @@ extern "C" int bb_predict_static(bb_plane const *plane, uint32_t n_trees,
                                 b + right[i] < e,
                             "bb_predict_static: a child id must follow its parent in its tree");
             }
+        }
+        int cur = 0;
+        check(cudaGetDevice(&cur), "cudaGetDevice");
+        if (cur != p.device)
+        {
+            throw ConfigError("bb_predict_static: the plane's device must be the current "
+                              "device (cudaSetDevice / bb_select_device first)");
+        }
+        if (p.n_rows == 0)
+        {
+            return; // a request plane before its first refill: nothing to score
         }
         unsigned char *scr = scratch_address();
         auto          *w   = reinterpret_cast<uint32_t *>(scr);

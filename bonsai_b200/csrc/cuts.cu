@@ -46,6 +46,34 @@ __device__ __forceinline__ float value_of(uint32_t k)
     return __uint_as_float((k >> 31) != 0 ? k ^ 0x80000000u : ~k);
 }
 
+// std::midpoint for float, the greedy rule's cut (src/bin_mapper.cpp:95): the
+// correctly rounded half-sum that never overflows. With both magnitudes at
+// most FLT_MAX / 2 the sum cannot overflow; above that each operand is halved
+// before the add, except one below twice the smallest normal (halving it
+// would round), which is added whole -- the cases of the C++ standard's
+// midpoint proposal (P0811). Division by 2 is exact or correctly rounded, and
+// the build keeps denormals (no flush to zero).
+__device__ __forceinline__ float midpoint_f(float a, float b)
+{
+    float const hi = FLT_MAX / 2.0F;
+    float const lo = FLT_MIN * 2.0F;
+    float const aa = fabsf(a);
+    float const ab = fabsf(b);
+    if (aa <= hi && ab <= hi)
+    {
+        return (a + b) / 2.0F;
+    }
+    if (aa < lo)
+    {
+        return a + b / 2.0F;
+    }
+    if (ab < lo)
+    {
+        return a / 2.0F + b;
+    }
+    return a / 2.0F + b / 2.0F;
+}
+
 // The NaN-free values of columns [f0, f0 + nf) of row-major S (n x F) as
 // keys, column c's at keys[c * n + ...] (order within a column is free: the
 // sort makes it canonical); counts[c] ends as the column's count.
@@ -323,7 +351,7 @@ __global__ void __launch_bounds__(k_cut_threads)
             {
                 float const a   = value_of(k[st[j]]);
                 float const b   = value_of(k[st[j + 1]]);
-                float const mid = (a + b) / 2.0F;
+                float const mid = midpoint_f(a, b);
                 if (c == 0 || out[c - 1] < mid)
                 {
                     out[c++] = mid;

@@ -466,7 +466,9 @@ void bb_shap_plan_destroy(bb_shap_plan *plan);
  * resolves the array's address there (make it before any stream capture).
  * All calls share the array: calls whose work overlaps on the GPU race on
  * it. The kernel runs on the legacy default stream; the call returns once it
- * is enqueued, so synchronise before reading out_device. */
+ * is enqueued, so synchronise before reading out_device. The plane's device
+ * must be the current device (BB_ERR_CONFIG otherwise); a plane with no rows
+ * (a request plane before its first refill) returns 0 and runs nothing. */
 int bb_predict_static(bb_plane const *plane, uint32_t n_trees, uint32_t const *roots,
                       uint32_t n_nodes, uint32_t const *feature, uint32_t const *split_bin,
                       uint32_t const *left, uint32_t const *right,

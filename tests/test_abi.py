@@ -126,3 +126,49 @@ def test_struct_layout_matches_the_header(tmp_path, py_name, c_name):
     for f in fields:
         assert int(got[f]) == getattr(T, f).offset, f
     assert int(got["sizeof"]) == C.sizeof(T)
+
+
+def _extreme_columns(rng, n=5000):
+    """Greedy-rule columns (a value heavier than a mean bin) at magnitudes
+    where the cut's midpoint matters: above FLT_MAX / 2, where a plain
+    (a + b) / 2 overflows; mixed huge and subnormal neighbours (one operand
+    added whole); subnormal and near-subnormal runs; the float extremes."""
+    big = rng.uniform(2e38, 3.4e38, n)
+    heavy = rng.random(n) < 0.4
+    tiny = rng.uniform(-1.2e-38, 1.2e-38, n)
+    cols = [
+        np.where(heavy, 2.5e38, big),                                   # huge, one sign
+        np.where(heavy, -2.5e38, -big),                                 # its mirror
+        np.where(heavy, 0.0, rng.choice([-1.0, 1.0], n) * big),         # huge either side of 0
+        np.where(heavy, 1e-42, rng.choice([-1.0, 1.0], n) * big),       # huge next to subnormal
+        np.where(heavy, 1e-39, tiny),                                   # subnormal runs
+        np.where(heavy, -3e-38, rng.uniform(-4e-38, 4e-38, n)),         # near the normal edge
+        np.where(heavy, 1.0, rng.choice([-3.4028235e38, 3.4028235e38, 1.7e38, -1.7e38], n)),
+        np.where(heavy, 3e38, rng.choice([np.inf, -np.inf, 1e38], n)),  # infinities
+    ]
+    return np.stack(cols, 1).astype(np.float32)
+
+
+def test_midpoint_follows_std_midpoint():
+    """The greedy cut's midpoint never overflows and equals the half-sum in
+    float where that is exact."""
+    from bonsai_b200.binning import midpoint
+    f = np.float32
+    fmax = np.finfo(np.float32).max
+    assert midpoint(f(3e38), f(3.2e38)) == f(3.1e38)
+    assert midpoint(fmax, fmax) == fmax
+    assert midpoint(-fmax, fmax) == 0.0
+    assert midpoint(f(1.0), f(2.0)) == f(1.5)
+    d = np.float32(1e-45)                      # the smallest subnormal
+    assert midpoint(d, d) == d
+    assert midpoint(f(-3e38), d) == f(-1.5e38)
+
+
+@pytest.mark.parametrize("max_bin", [16, 255])
+def test_fit_cuts_extreme_magnitudes_match_reference(ref, max_bin):
+    import bonsai_b200 as bb
+    X = _extreme_columns(np.random.Generator(np.random.PCG64(41)))
+    rc, ro = ref.fit_cuts(X, max_bin=max_bin)
+    cuts, off = bb.fit_cuts(X, max_bin=max_bin)
+    assert np.array_equal(off, ro)
+    assert np.array_equal(cuts.view(np.uint32), rc.view(np.uint32))

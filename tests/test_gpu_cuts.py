@@ -71,3 +71,16 @@ def test_device_cuts_many_columns(bb):
     X[rng.random(X.shape) < 0.5] = np.nan
     X[:, ::7] = np.round(X[:, ::7], 0)
     _same(bb.fit_cuts_device(X), bb.fit_cuts(X), "wide")
+
+
+@pytest.mark.parametrize("max_bin", [16, 255])
+def test_device_cuts_extreme_magnitudes(bb, ref, max_bin):
+    """Greedy-rule columns above FLT_MAX / 2, huge values next to subnormal
+    ones, subnormal runs and infinities: the device midpoint is
+    std::midpoint's, so device cuts equal the host restatement's and the
+    reference's bit for bit."""
+    from test_abi import _extreme_columns
+    X = _extreme_columns(np.random.Generator(np.random.PCG64(41)))
+    want = ref.fit_cuts(X, max_bin=max_bin)
+    _same(bb.fit_cuts(X, max_bin=max_bin), want, "host")
+    _same(bb.fit_cuts_device(X, max_bin=max_bin), want, "device")

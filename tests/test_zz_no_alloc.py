@@ -69,3 +69,40 @@ def test_predict_static_matches_predict_on_consecutive_calls(bb):
     rc = _call(L, plane, roots, 600_000, t, 0.0, 0.1, out.data_ptr())
     assert rc == BB_ERR_CONFIG
     assert "524,288" in L.bb_last_error().decode()
+
+
+def test_predict_static_on_u16_codes_and_request_planes(bb):
+    """The 16-bit code kernel (more than 256 bins per feature), and a request
+    plane: before its first refill it holds no rows and the call runs
+    nothing; refilled with a batch whose row count is not a multiple of 64
+    (its column stride differs from an ingest plane's), the scores equal
+    bb_predict's bit for bit, on two refills in a row."""
+    import torch
+
+    from bonsai_b200._lib import check, lib
+    rng = np.random.Generator(np.random.PCG64(78))
+    n, F = 20_000, 5
+    X = rng.standard_normal((n, F)).astype(np.float32)
+    X[rng.random((n, F)) < 0.03] = np.nan
+    y = (X[:, 0] * 2 + np.nan_to_num(X[:, 3]) > 0.5).astype(np.float32)
+    cuts, off = bb.fit_cuts(X, max_bin=700)
+    plane = bb.Plane(X, cuts, off)
+    assert int(max(np.diff(off))) > 256                 # u16 codes
+    b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=7), max_trees=6)
+    b.update(6)
+    trees = b.trees()
+    roots, n_nodes, t = _pack(trees)
+    L = lib()
+    req = bb.Plane.like(plane, 9_000)
+    out = torch.full((9_000,), 7.0, dtype=torch.float32, device="cuda")
+    check(_call(L, req, roots, n_nodes, t, b.init_score, 0.1, out.data_ptr()))
+    torch.cuda.synchronize()
+    assert (out.cpu().numpy() == 7.0).all()             # nothing ran
+    for batch in (None, X[:8_999], X[5:6_006]):
+        use = plane if batch is None else req.refill(batch)
+        m = n if batch is None else len(batch)
+        want = bb.predict(use, trees, b.init_score, 0.1)
+        out = torch.full((m,), float("nan"), dtype=torch.float32, device="cuda")
+        check(_call(L, use, roots, n_nodes, t, b.init_score, 0.1, out.data_ptr()))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
