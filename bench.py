@@ -2,29 +2,33 @@
 """Benchmark: the tall binary-classification fit (10,000,000 rows x 28 float32
 features, logloss, depthwise depth 8, 255 bins, lr 0.1) on B200.
 
-A step is one boosting round (one depth-8 tree over all 10M rows, with the
-resident gradient and score update). The metric is the fit time for 500
-rounds, reported as ms_per_step x 500: device time of K timed rounds (CUDA
-events on the booster's stream, after W warm-up rounds, a barrier and a
-synchronize on both sides, max over ranks). The bins plane (280 MB) and the
-per-row state exceed the 126 MB L2, so no flush is needed between rounds.
+The metric is the fit time for 500 rounds. `value` is the device time of a
+complete 500-round fit (CUDA events on the booster's stream around its 500
+rounds, the binned plane and labels already resident); `e2e` is the wall
+clock of the same fit from pinned host rows (ingest, the rounds, the model and
+training scores back on the host). The plain (exact) form fits the same 500
+rounds on the same plane, and both forms' validation AUC and logloss are
+measured on 1,000,000 rows of the generator's validation seed. A step is one
+boosting round: `ms_per_step` is K device-timed rounds after W warm-up rounds
+(a barrier and a synchronize on both sides, max over ranks). The bins plane
+(280 MB) and the per-row state exceed the 126 MB L2, so no flush is needed
+between rounds. Cut fitting is outside every timed region, on both arms.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode exact|int8|int16]
   python bench.py --impl reference      # the reference's CPU grower, timed
-  python bench.py --workload serve [--impl reference]
+  python bench.py --workload serve|wide|multiclass|many [--impl reference]
 
 The serving workload fits a 1,000-tree depth-8 ensemble (squared error, 255
 bins, lr 0.1) on 20,000 rows x 28 of the ragged-many family, then scores
 request batches of 1 to 1,000,000 rows x 28: predict rows/s through a
 predict plan (device time per launch, L2 flushed between launches, and end
 to end from pinned host rows through a request plane, refilled per batch, to
-host scores) and TreeSHAP
-rows/s with the additivity error against an FP64 recomputation of the
-margin.
+host scores) and TreeSHAP rows/s with the additivity error against an FP64
+recomputation of the margin.
 
-Multi-GPU (torchrun): every rank fits its own replica of the workload (one
-fit per GPU, no collective in the data path); value is the time for all
-ranks' fits, i.e. the max over ranks.
+Multi-GPU (torchrun): the quantised fit is row-sharded -- every rank holds a
+contiguous slice of the same rows and the ranks all-reduce integer histograms
+over NCCL once per level (strong scaling; trees equal the one-GPU fit's).
 """
 
 from __future__ import annotations
@@ -34,6 +38,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -44,7 +49,6 @@ sys.path.insert(0, ROOT)
 METRIC = "10M×28 fit s/500 iters: int-quantised vs plain GPU at ΔAUC≤1e-3; hist GB/s"
 WORKLOAD = "tall binary logloss 10,000,000x28, depthwise depth 8, 255 bins, lr 0.1"
 N_ROUNDS = 500
-CPU_SAMPLE_ROWS = 1_000_000
 
 
 def peaks():
@@ -95,7 +99,8 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(),
+                                 f"bonsai_b200_clocks_{os.getpid()}_{id(self)}.csv")
 
     def __enter__(self):
         try:
@@ -146,13 +151,15 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(X, y, cuts, off, steps, warmup, rows=CPU_SAMPLE_ROWS):
+def cpu_reference(X, y, cuts, off, steps, warmup, rows=None):
     """The reference's own CPU depthwise grower (oracle/_ref, compiled from
-    its sources) on the first `rows` rows, all host threads; per-round time
-    scaled by rows to the full workload. Falls back to the oracle port."""
+    its sources) on all rows (or the first `rows`), all host threads: `steps`
+    timed rounds after `warmup` rounds, the per-round time x 500 (and x the
+    row ratio when sampled). Falls back to the oracle port."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     n_full = X.shape[0]
+    rows = n_full if rows is None else min(rows, n_full)
     Xs, ys = X[:rows], y[:rows]
     threads = len(os.sched_getaffinity(0))
     tc = O.TreeCfg(objective="logloss", max_depth=8, learning_rate=0.1, n_threads=threads)
@@ -185,9 +192,10 @@ def cpu_reference(X, y, cuts, off, steps, warmup, rows=CPU_SAMPLE_ROWS):
         per_round = (time.perf_counter() - t0) / steps
     value = per_round * (n_full / rows) * N_ROUNDS
     return {"value": value, "unit": "s", "cores": threads, "kind": kind,
-            "sample": f"first {rows:,} rows x 28, {steps} timed depth-8 logloss rounds "
-                      f"({warmup} warm-up), per-round time x {n_full / rows:g} (rows) "
-                      f"x {N_ROUNDS} (rounds)"}
+            "sample": (f"all {rows:,} rows x 28" if rows == n_full else
+                       f"first {rows:,} rows x 28 (per-round time x {n_full / rows:g})") +
+                      f", {steps} timed depth-8 logloss rounds after {warmup} warm-up "
+                      f"rounds, per-round time x {N_ROUNDS} (rounds)"}
 
 
 def make_data(rows):
@@ -625,13 +633,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="int8", choices=["exact", "int8", "int16"])
-    ap.add_argument("--compare-steps", type=int, default=5,
-                    help="timed rounds of the plain form for the quantised/plain ratio "
-                         "(0 skips it)")
+    ap.add_argument("--compare-rounds", type=int, default=N_ROUNDS,
+                    help="fit: rounds of the plain form's fit for the quantised/plain ratio "
+                         "and the AUC delta (0 skips it)")
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
-                    help="fit: validation rows for the device validation plane's cost (0 skips)")
+                    help="fit: validation rows for the AUC and logloss (0 skips)")
     ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass", "many"])
     ap.add_argument("--batches", default=",".join(map(str, SERVE_BATCHES)),
                     help="serve: predict request batch sizes")
@@ -673,23 +681,97 @@ def main():
             dist.destroy_process_group()
         return
     if args.impl == "reference":
-        if rank != 0:
-            return
-        X, y, cuts, off = make_data(args.rows)
-        cb = cpu_reference(X, y, cuts, off, K, W)
-        line = {"metric": METRIC, "value": cb["value"], "unit": "s", "impl": "reference",
-                "n_gpus": args.gpus, "steps": K, "warmup": W,
-                "ms_per_step": cb["value"] / N_ROUNDS * 1000.0, "higher_is_better": False,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "rows": args.rows, "features": 28,
-                           "rounds": N_ROUNDS, "host_threads": cb["cores"]},
-                "cpu_baseline": cb,
-                "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        if rank == 0:
+            reference_main(args, W, K)
         return
+    fit_main(args, world, rank, local, W, K)
+
+
+def fit_config(rows):
+    """The workload's config: the same dict on both arms."""
+    return {"workload": WORKLOAD, "rows": rows, "features": 28, "rounds": N_ROUNDS,
+            "l2": "inputs larger than L2 (bins 280 MB, gradient pairs 80 MB)",
+            "excluded": "cut fitting (the same fixed cuts on both arms)"}
+
+
+def reference_main(args, W, K):
+    """The reference arm: the reference's own CPU depthwise grower on all
+    rows, K timed rounds after W warm-up rounds."""
+    X, y, cuts, off = make_data(args.rows)
+    cb = cpu_reference(X, y, cuts, off, K, W)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": K, "warmup": W,
+            "ms_per_step": cb["value"] / N_ROUNDS * 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded HIGGS-shaped stand-in)",
+            "config": fit_config(args.rows), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def auc(y, p):
+    """Area under the ROC curve (ties share their mean rank)."""
+    y = np.asarray(y) > 0.5
+    p = np.asarray(p, np.float64)
+    order = np.argsort(p, kind="stable")
+    ps = p[order]
+    ranks = np.empty(len(p))
+    # mean rank over runs of equal scores
+    starts = np.flatnonzero(np.r_[True, ps[1:] != ps[:-1]])
+    ends = np.r_[starts[1:], len(p)]
+    mean = (starts + ends + 1) / 2.0
+    ranks[order] = np.repeat(mean, ends - starts)
+    n1 = int(y.sum())
+    n0 = len(y) - n1
+    return float((ranks[y].sum() - n1 * (n1 + 1) / 2.0) / (n1 * n0))
+
+
+def logloss(y, margin):
+    m = np.asarray(margin, np.float64)
+    y = np.asarray(y, np.float64)
+    return float(np.mean(np.logaddexp(0.0, m) - y * m))
+
+
+def hist_error(bb, plane, scores, y, seed=7):
+    """The int8 histogram against FP64 sums, over the gradients of the fit's
+    final scores (logloss: g = p - y, h = p (1 - p)) at the root (every row):
+    relative L1 error of the gradient and hessian cells, and the largest cell
+    error in units of the stochastic-rounding spread (scale x sqrt(count))."""
+    s = np.asarray(scores, np.float64)
+    p = 1.0 / (1.0 + np.exp(-s))
+    g = (p - y).astype(np.float32)
+    h = (p * (1.0 - p)).astype(np.float32)
+    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=seed), g, h)
+    codes = plane.bins()
+    nb = np.asarray(plane.n_bins, np.int64)
+    G, H, N = [], [], []
+    for f in range(codes.shape[0]):
+        c = codes[f]
+        G.append(np.bincount(c, weights=g.astype(np.float64), minlength=nb[f]))
+        H.append(np.bincount(c, weights=h.astype(np.float64), minlength=nb[f]))
+        N.append(np.bincount(c, minlength=nb[f]))
+    G, H, N = np.concatenate(G), np.concatenate(H), np.concatenate(N)
+    sg = float(np.abs(g).max()) / 127.0
+    sh = float(h.max()) / 127.0
+    eg = np.abs(q[:, 0] - G)
+    eh = np.abs(q[:, 1] - H)
+    live = N > 0
+    return {"where": "root of the final round's gradients, every row",
+            "g_rel_l1": float(eg.sum() / np.abs(G).sum()),
+            "h_rel_l1": float(eh.sum() / np.abs(H).sum()),
+            "g_max_sigmas": float((eg[live] / (sg * np.sqrt(N[live]))).max()),
+            "h_max_sigmas": float((eh[live] / (sh * np.sqrt(N[live]))).max())}
+
+
+def fit_main(args, world, rank, local, W, K):
+    """The headline: a complete 500-round fit in each form on the 10M x 28
+    data (device time with inputs resident, and wall clock end to end), the
+    validation AUC and logloss of both, and K device-timed rounds."""
+    import torch
 
     import bonsai_b200 as bb
+    from bonsai_b200 import synth
     from bonsai_b200.build import build_library
     if rank == 0:
         build_library()
@@ -698,12 +780,15 @@ def main():
     X, y, cuts, off = make_data(args.rows)
     n_fit, F = X.shape
     # N > 1: the quantised fit is row-sharded -- each rank holds a contiguous
-    # slice of the same 10M rows and the ranks combine integer histograms over
-    # NCCL (strong scaling; trees equal the one-GPU fit's); the exact form's
-    # float cells do not combine exactly, so it runs one replica per GPU
-    sharded = world > 1 and args.mode != "exact"
+    # slice of the same rows and the ranks combine integer histograms over
+    # NCCL (strong scaling; trees equal the one-GPU fit's). The exact form's
+    # float cells do not combine exactly, so N > 1 runs the quantised form only.
+    sharded = world > 1
+    if sharded and args.mode == "exact":
+        raise SystemExit("bench: a row-sharded fit needs --mode int8 or int16")
     comm = None
     row0 = 0
+    init = None
     if sharded:
         from bonsai_b200 import dist as bdist
         row0, row1 = bdist.shard_range(n_fit, world, rank)
@@ -712,80 +797,93 @@ def main():
         init = bdist.sharded_init_score(y, n_fit, "logloss", world, rank)
         comm = bdist.open_comm(world, rank)
     n = X.shape[0]
-
-    # ---- end to end through the C ABI with host buffers: ingest (H2D of the
-    # raw matrix + bin application), labels up, rounds, model + scores down
-    import torch
     Xp = torch.empty((n, F), dtype=torch.float32, pin_memory=True).numpy()
     Xp[...] = X
     yp = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
     yp[...] = y
-    params = bb.TrainParams(objective="logloss", max_depth=8, learning_rate=0.1,
-                            min_data_in_leaf=20, hist_mode=args.mode, use_graph=True)
-    barrier(world)
-    t0 = time.perf_counter()
-    plane = bb.Plane(Xp, cuts, off)
-    if sharded:
-        b = bb.Booster(plane, yp, params, max_trees=W + K + 4, comm=comm, row_offset=row0,
-                       total_rows=n_fit, init_score=init)
-    else:
-        b = bb.Booster(plane, yp, params, max_trees=W + K + 4)
-    torch.cuda.synchronize()
-    t_setup = time.perf_counter() - t0
 
-    # ---- device-timed rounds
+    def params(mode):
+        return bb.TrainParams(objective="logloss", max_depth=8, learning_rate=0.1,
+                              min_data_in_leaf=20, hist_mode=mode, use_graph=True)
+
+    def booster(plane, mode, max_trees):
+        if sharded:
+            return bb.Booster(plane, yp, params(mode), max_trees=max_trees, comm=comm,
+                              row_offset=row0, total_rows=n_fit, init_score=init)
+        return bb.Booster(plane, yp, params(mode), max_trees=max_trees)
+
+    # ---- the complete fit, end to end through the C ABI with host buffers:
+    # pinned X -> ingest (H2D + bin application), labels up, 500 rounds, the
+    # model and the training scores down. `value` is the device time of its
+    # 500 rounds (CUDA events on the booster's stream; inputs resident).
+    barrier(world)
+    with Clocks(local) as clk_fit:
+        t0 = time.perf_counter()
+        plane = bb.Plane(Xp, cuts, off)
+        b = booster(plane, args.mode, N_ROUNDS)
+        t_setup = time.perf_counter() - t0
+        b.update(N_ROUNDS)
+        t_fit = time.perf_counter() - t0 - t_setup
+        fit_ms = b.last_ms
+        t1 = time.perf_counter()
+        trees = b.trees()
+        scores = b.scores()
+        t_down = time.perf_counter() - t1
+        wall = time.perf_counter() - t0
+    fit_ms = max_over_ranks(fit_ms, world)
+    wall = max_over_ranks(wall, world)
+    init_score = b.init_score
+    b.close()
+    tree_bytes = sum(t.feature.nbytes * 8 for t in trees)
+
+    # ---- K device-timed rounds after W warm-up rounds (the per-step figure),
+    # and one profiled round for the phase and per-level histogram figures
+    b = booster(plane, args.mode, W + K + 4)
     b.update(W)
     barrier(world)
     with Clocks(local) as clk:
         b.update(K)
-    ms = b.last_ms / K
-    ms = max_over_ranks(ms, world)
+    ms = max_over_ranks(b.last_ms / K, world)
     barrier(world)
-
-    t1 = time.perf_counter()
-    trees = b.trees()
-    scores = b.scores()
-    t_down = (time.perf_counter() - t1) * (N_ROUNDS / max(1, len(trees)))
-    tree_bytes = sum(t.feature.nbytes * 8 for t in trees) / max(1, len(trees))
-
     prof = b.profile_round()
     b.close()
+
+    # ---- the plain form: a complete 500-round fit on the same plane
+    plain = None
+    plain_trees = None
+    if args.mode != "exact" and args.compare_rounds > 0 and not sharded:
+        bp = booster(plane, "exact", args.compare_rounds)
+        bp.update(args.compare_rounds)
+        pms = bp.last_ms
+        plain_trees = bp.trees()
+        plain_init = bp.init_score
+        bp.close()
+        plain = {"rounds": args.compare_rounds, "device_s": pms / 1000.0,
+                 "ms_per_round": pms / args.compare_rounds,
+                 "quantised_speedup": (pms / args.compare_rounds) / (fit_ms / N_ROUNDS)}
+
+    # ---- accuracy on the validation rows (the generator's seed 10,000,001)
+    accuracy = None
+    if rank == 0 and args.eval_rows > 0:
+        Xv, yv = synth.tall_binary(n=args.eval_rows, seed=10_000_001)
+        pv = bb.Plane(Xv, cuts, off)
+        mq = bb.PredictPlan(pv, trees, init_score, 0.1).run(pv)
+        accuracy = {"valid_rows": args.eval_rows,
+                    args.mode: {"auc": auc(yv, mq), "logloss": logloss(yv, mq)}}
+        if plain_trees is not None:
+            mp = bb.PredictPlan(pv, plain_trees, plain_init, 0.1).run(pv)
+            accuracy["exact"] = {"auc": auc(yv, mp), "logloss": logloss(yv, mp),
+                                 "rounds": len(plain_trees)}
+            if len(plain_trees) == len(trees):
+                accuracy["delta_auc"] = accuracy[args.mode]["auc"] - accuracy["exact"]["auc"]
+                accuracy["delta_logloss"] = (accuracy[args.mode]["logloss"] -
+                                             accuracy["exact"]["logloss"])
+        pv.close()
+        if args.mode == "int8" and not sharded:
+            accuracy["hist_error_vs_fp64"] = hist_error(bb, plane, scores, y)
     if comm is not None:
         comm.close()
 
-    # the plain (exact) form on the same plane, for the headline ratio
-    plain = None
-    if args.mode != "exact" and args.compare_steps > 0 and not sharded:
-        pp = bb.TrainParams(objective="logloss", max_depth=8, learning_rate=0.1,
-                            min_data_in_leaf=20, hist_mode="exact", use_graph=True)
-        bp = bb.Booster(plane, yp, pp, max_trees=W + args.compare_steps + 1)
-        bp.update(W)
-        barrier(world)
-        bp.update(args.compare_steps)
-        pms = max_over_ranks(bp.last_ms / args.compare_steps, world)
-        bp.close()
-        plain = {"value": pms * N_ROUNDS / 1000.0, "unit": "s", "ms_per_step": pms,
-                 "steps": args.compare_steps,
-                 "quantised_speedup": pms / ms}
-    # the device validation plane: the same fit with a validation set of the
-    # workload's generator (seed 10,000,001) armed, every round recording its
-    # validation logloss on the device inside the round's graph
-    vplane = None
-    if args.eval_rows > 0 and not sharded:
-        from bonsai_b200 import synth
-        Xv, yv = synth.tall_binary(n=args.eval_rows, seed=10_000_001)
-        pv = bb.Plane(Xv, cuts, off)
-        be = bb.Booster(plane, yp, params, max_trees=W + K + 4)
-        be.eval_arm(pv, yv)
-        be.update(W)
-        barrier(world)
-        be.update(K)
-        ems = be.last_ms / K
-        losses = be.eval_losses()
-        be.close()
-        pv.close()
-        vplane = {"rows": args.eval_rows, "ms_per_step": ems, "overhead_ms_per_step": ems - ms,
-                  "rounds_recorded": int(len(losses)), "last_logloss": float(losses[-1])}
     peak, peak_kind = peaks()
     hist_gbs = prof["hist_bytes"] / (prof["hist_ms"] * 1e-3) / 1e9
     traffic = None
@@ -794,26 +892,37 @@ def main():
         with open(tpath) as f:
             td = json.load(f)
         traffic = td.get(args.mode, {}).get("dram_bytes_per_tree")
-
-    value = ms * N_ROUNDS / 1000.0
-    e2e = t_setup + value + t_down
+    per_row = F + (2.0 if args.mode == "int8" else 4.0 if args.mode == "int16" else 8.0) + 4.0
+    levels = [{"rows": r, "ms": t, "gbs": (r * per_row) / (t * 1e-3) / 1e9 if t > 0 else None}
+              for r, t in zip(prof["build_rows"], prof["build_ms"])]
+    # partition per level: every row's id and its split-feature code read,
+    # its id written (pass 1 reads, pass 2 reads and writes)
+    part_levels = max(1, len(levels) - 1)
+    part_bytes = part_levels * n * (4 + 1 + 4)
+    value = fit_ms / 1000.0
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f32" if args.mode == "exact" else args.mode,
         "data": "synthetic (seeded HIGGS-shaped stand-in)",
-        "config": {"workload": WORKLOAD, "rows": n_fit, "features": F, "rounds": N_ROUNDS,
-                   "hist_mode": args.mode, "graph": True,
-                   "parallelism": (f"row shards x{world} (NCCL all-reduce of integer "
-                                   "histograms)" if sharded else
-                                   f"replicas x{world}" if world > 1 else "single"),
-                   "rows_per_gpu": n,
-                   "l2": "inputs larger than L2 (bins 280 MB, gh 80 MB)"},
-        "e2e": {"value": e2e, "unit": "s",
+        "config": fit_config(n_fit),
+        "arm": {"hist_mode": args.mode, "graph": True, "rows_per_gpu": n,
+                "parallelism": (f"row shards x{world} (NCCL all-reduce of integer "
+                                "histograms)" if sharded else "single"),
+                "value": f"device time of a complete {N_ROUNDS}-round fit (CUDA events on "
+                         "the booster's stream, plane and labels resident)",
+                "ms_per_step": f"{K} device-timed rounds after {W} warm-up rounds"},
+        "fit": {"rounds": len(trees), "device_s": value, "ms_per_round": fit_ms / N_ROUNDS,
+                "wall_s": wall},
+        "e2e": {"value": wall, "unit": "s",
                 "h2d_bytes_per_step": (X.nbytes + y.nbytes) / N_ROUNDS,
-                "d2h_bytes_per_step": tree_bytes + scores.nbytes / N_ROUNDS,
-                "setup_s": t_setup, "download_s_per_500": t_down},
+                "d2h_bytes_per_step": (tree_bytes + scores.nbytes) / N_ROUNDS,
+                "setup_s": t_setup, "rounds_s": t_fit, "download_s": t_down,
+                "what": f"wall clock: pinned host X and labels -> ingest -> {N_ROUNDS} rounds "
+                        "-> trees and training scores on the host"},
+        "plain_form": plain,
+        "accuracy": accuracy,
         "roofline": {"bound": "hbm",
                      "kernel": ("histogram build (qhist_t_kernel per level)" if args.mode != "exact"
                                 else "histogram build (count+offsets+scatter+chain)"),
@@ -821,15 +930,19 @@ def main():
                      "unit": "GB/s", "frac": hist_gbs / peak, "traffic": traffic,
                      "algorithmic_bytes_per_tree": prof["hist_bytes"],
                      "hist_ms_per_tree": prof["hist_ms"]},
+        "hist_levels": levels,
+        "partition": {"ms_per_tree": prof["partition_ms"],
+                      "algorithmic_bytes_per_tree": part_bytes,
+                      "gbs": part_bytes / (prof["partition_ms"] * 1e-3) / 1e9,
+                      "frac": part_bytes / (prof["partition_ms"] * 1e-3) / 1e9 / peak},
         "phases_ms": {k: prof[k] for k in ("hist_ms", "partition_ms", "find_ms", "other_ms",
                                            "total_ms")},
-        "plain_form": plain,
-        "validation_plane": vplane,
         "gpu_launches": int(prof["launches"]) * K,
         "clocks": clk.summary(),
+        "clocks_fit": clk_fit.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(X, y, cuts, off, steps=2, warmup=1)
+        line["cpu_baseline"] = cpu_reference(X, y, cuts, off, steps=K, warmup=W)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plane.close()

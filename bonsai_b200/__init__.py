@@ -562,7 +562,11 @@ class Booster:
         """One boosting round timed phase by phase (bb_booster_profile_round)."""
         p = _lib.Profile()
         check(lib().bb_booster_profile_round(self.h, C.byref(p)))
-        return {k: getattr(p, k) for k, _ in _lib.Profile._fields_}
+        out = {k: getattr(p, k) for k, _ in _lib.Profile._fields_}
+        n = min(int(p.hist_builds), 16)
+        out["build_ms"] = [float(x) for x in p.build_ms[:n]]
+        out["build_rows"] = [int(x) for x in p.build_rows[:n]]
+        return out
 
     def close(self):
         if getattr(self, "h", None):

@@ -50,6 +50,7 @@ class Profile(C.Structure):
         ("hist_ms", C.c_double), ("partition_ms", C.c_double), ("find_ms", C.c_double),
         ("other_ms", C.c_double), ("total_ms", C.c_double), ("hist_bytes", C.c_double),
         ("hist_rows", C.c_uint64), ("hist_builds", C.c_uint32), ("launches", C.c_uint32),
+        ("build_ms", C.c_double * 16), ("build_rows", C.c_uint64 * 16),
     ]
 
 

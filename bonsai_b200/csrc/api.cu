@@ -1725,6 +1725,11 @@ extern "C"
                 out->hist_rows    = p.hist_rows;
                 out->hist_builds  = p.hist_builds;
                 out->launches     = b->round_launches;
+                for (uint32_t k = 0; k < 16; ++k)
+                {
+                    out->build_ms[k]   = p.build_ms[k];
+                    out->build_rows[k] = p.build_rows[k];
+                }
             });
     }
 

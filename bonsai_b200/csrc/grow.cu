@@ -3931,6 +3931,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
     }
     if (prof_ != nullptr)
     {
+        double const before = prof_->hist_ms;
         phase_end(prof_->hist_ms);
         Ctl c{};
         BB_CHECK(cudaMemcpy(&c, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost));
@@ -3941,6 +3942,11 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         prof_->hist_rows += c.built_rows;
         prof_->hist_bytes += (static_cast<double>(c.built_rows) * per_row) +
                              (static_cast<double>(c.n_build) * off_h_[nfb] * 8.0);
+        if (prof_->hist_builds < Profile::k_prof_builds)
+        {
+            prof_->build_ms[prof_->hist_builds]   = prof_->hist_ms - before;
+            prof_->build_rows[prof_->hist_builds] = c.built_rows;
+        }
         prof_->hist_builds += 1;
     }
 }

@@ -114,6 +114,11 @@ struct Profile
     double   hist_bytes   = 0.0;
     uint64_t hist_rows    = 0;
     uint32_t hist_builds  = 0;
+    // per histogram build of the round, in order (root first): its time and
+    // built rows (the first k_prof_builds builds)
+    static constexpr uint32_t k_prof_builds = 16;
+    double   build_ms[k_prof_builds]   = {};
+    uint64_t build_rows[k_prof_builds] = {};
 };
 
 // Combines a device buffer across the row shards of one fit, in stream

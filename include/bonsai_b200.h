@@ -268,6 +268,10 @@ typedef struct
     uint64_t hist_rows;
     uint32_t hist_builds;
     uint32_t launches; /* this library's kernel launches per round */
+    /* per histogram build of the round in launch order (root first; the
+     * first 16 builds): device time and built rows */
+    double   build_ms[16];
+    uint64_t build_rows[16];
 } bb_profile;
 
 int bb_booster_profile_round(bb_booster *b, bb_profile *out);
