@@ -649,8 +649,12 @@ std::vector<uint32_t> sample_features(uint32_t n_features, float fraction, std::
 class RowSampler
 {
   public:
-    RowSampler(float p, uint32_t seed, uint64_t n, uint32_t trees, int device)
-        : p_(p), rng_(seed), n_(n), trees_(trees), words_((n + 31) / 32), device_(device)
+    // external: the caller supplies each round's rows (set_rows) instead of
+    // the Bernoulli draws
+    RowSampler(float p, uint32_t seed, uint64_t n, uint32_t trees, int device,
+               bool external = false)
+        : p_(p), rng_(seed), n_(n), trees_(trees), words_((n + 31) / 32), device_(device),
+          external_(external)
     {
         for (int j = 0; j < 2; ++j)
         {
@@ -683,9 +687,40 @@ class RowSampler
         return static_cast<size_t>(words_) * trees_ * 4;
     }
 
+    // The caller's rows for the next round (external mode): ascending ids
+    // below n into the current slot's mask, once its last copy has left.
+    void set_rows(uint32_t const *rows, uint64_t m)
+    {
+        need(external_, "bb_booster_set_rows: the booster draws its own rows "
+                        "(create it with external_sample)");
+        need(m <= n_, "bb_booster_set_rows: more rows than the plane holds");
+        BB_CHECK(cudaEventSynchronize(copied_[cur_]));
+        uint32_t *w = slot_[cur_];
+        std::memset(w, 0, bytes());
+        for (uint64_t i = 0; i < m; ++i)
+        {
+            need(rows[i] < n_ && (i == 0 || rows[i - 1] < rows[i]),
+                 "bb_booster_set_rows: row ids must be ascending and below the row count");
+            w[rows[i] >> 5] |= 1u << (rows[i] & 31);
+        }
+        counts_[cur_][0] = static_cast<uint32_t>(m);
+        ready_           = true;
+    }
+
     // The next round's masks into dev (on s); returns each tree's row count.
     std::vector<uint32_t> const &upload(uint32_t *dev, cudaStream_t s)
     {
+        if (external_)
+        {
+            need(ready_, "bb_booster_update: no rows for this round (bb_booster_set_rows "
+                         "before every round of an external_sample booster)");
+            int const done = cur_;
+            BB_CHECK(cudaMemcpyAsync(dev, slot_[done], bytes(), cudaMemcpyHostToDevice, s));
+            BB_CHECK(cudaEventRecord(copied_[done], s));
+            cur_   = done ^ 1;
+            ready_ = false;
+            return counts_[done];
+        }
         if (pending_.valid())
         {
             pending_.get();
@@ -742,6 +777,8 @@ class RowSampler
     std::vector<uint32_t> counts_[2];
     int                   cur_ = 0;
     std::future<void>     pending_;
+    bool                  external_ = false;
+    bool                  ready_    = false;
 };
 
 } // namespace
@@ -1017,8 +1054,11 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     // values >= 1 keep every row
     need(!(cfg->subsample < 0.0F) && !std::isnan(cfg->subsample),
          "sampler.subsample must be > 0");
-    bool const sampled = cfg->subsample > 0.0F && cfg->subsample < 1.0F;
+    bool const external = cfg->external_sample != 0;
+    bool const sampled  = external || (cfg->subsample > 0.0F && cfg->subsample < 1.0F);
     need(!sampled || red == nullptr, "a sharded fit keeps every row (subsample 1)");
+    need(!external || cfg->objective != 2,
+         "external_sample: single-output objectives only (a softmax round draws per class)");
     need(!(cfg->feature_fraction < 0.0F) && !std::isnan(cfg->feature_fraction),
          "tree_config.feature_fraction must be > 0");
     uint32_t const F_all = plane->p.n_feats;
@@ -1109,6 +1149,7 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     BB_LAUNCH("iota_kernel");
     BB_CHECK(cudaMemsetAsync(b->round, 0, 4, b->stream));
     GrowConfig gc = grow_config(*cfg);
+    gc.fit_rows   = red != nullptr ? total_rows : n; // a shard's cells hold the fit's sums
     if (feat_k > 0 && feat_k < p.n_feats)
     {
         // every tree draws its own features into table set k (class k)
@@ -1132,7 +1173,8 @@ bb_booster *create_booster(bb_plane const *plane, float const *labels, float con
     {
         int dev = 0;
         BB_CHECK(cudaGetDevice(&dev));
-        b->sampler = std::make_unique<RowSampler>(cfg->subsample, cfg->random_seed, n, K, dev);
+        b->sampler = std::make_unique<RowSampler>(cfg->subsample, cfg->random_seed, n, K, dev,
+                                                  external);
         uint64_t const words = b->sampler->words();
         b->sbits  = dmalloc<uint32_t>(words * K);
         b->srows  = dmalloc<uint32_t>(n);
@@ -1503,6 +1545,19 @@ extern "C"
                 }
                 *out = create_booster(plane, labels, init_scores, cfg, max_trees,
                                       comm->reducer(), row_offset, total_rows, &init_score);
+            });
+    }
+
+    int bb_booster_set_rows(bb_booster *b, uint32_t const *rows, uint64_t n_rows)
+    {
+        return guarded(
+            [&]
+            {
+                need(b != nullptr && (rows != nullptr || n_rows == 0),
+                     "bb_booster_set_rows: null argument");
+                need(b->sampler != nullptr, "bb_booster_set_rows: the booster keeps every row "
+                                            "(create it with external_sample)");
+                b->sampler->set_rows(rows, n_rows);
             });
     }
 

@@ -1649,14 +1649,14 @@ __global__ void __launch_bounds__(k_threads)
 // leaf ids and, for a resident booster, writes the next round's gradient
 // pairs and their maxima. The quantised form renews its leaves from
 // full-precision gradients first: pass A walks and sums each leaf's
-// (g, h) as exact fixed-point integers (2^38 / max |g| and 2^38 / max h per
-// unit, so at most 2^62 over 2^24 rows; integer sums are order-free, hence
-// deterministic), a one-CTA kernel turns them into FP64 Newton values, and
+// (g, h) as exact fixed-point integers (u / max |g| and u / max h per unit,
+// u = 2^38 up to 2^24 rows and halved per doubling above, so no sum passes
+// 2^62; integer sums are order-free, hence deterministic), a one-CTA kernel
+// turns them into FP64 Newton values, and
 // pass B applies them from the leaf id pass A recorded.
 constexpr uint32_t k_no_sel_tile = 0xFFFFFFFFu; // an unused tile slot of a selection
 constexpr uint32_t k_walk_nodes = 512;     // a depth-8 tree has at most 511
 constexpr uint32_t k_no_tile    = 0xFFFFFFu;
-constexpr double   k_fix_unit   = 274877906944.0; // 2^38
 
 struct WalkArgs
 {
@@ -1875,7 +1875,7 @@ __global__ void __launch_bounds__(k_threads)
                     uint64_t n_rows, uint32_t const *cut_off, uint32_t depth,
                     float2 const *__restrict__ gh, uint32_t const *absmax,
                     uint16_t *__restrict__ leaf16, unsigned long long *acc,
-                    uint32_t const *__restrict__ bits)
+                    uint32_t const *__restrict__ bits, double fix_unit)
 {
     constexpr uint32_t  per = U8 ? 32 : 16;
     __shared__ uint4    node_s[k_walk_nodes];
@@ -1889,8 +1889,8 @@ __global__ void __launch_bounds__(k_threads)
     uint4 const   *mt        = mirror + (static_cast<uint64_t>(root_tile) * n_rows * 2);
     float const    mgx       = __uint_as_float(absmax[0]);
     float const    mhx       = __uint_as_float(absmax[1]);
-    double const   fg        = mgx > 0.0F ? k_fix_unit / static_cast<double>(mgx) : 1.0;
-    double const   fh        = mhx > 0.0F ? k_fix_unit / static_cast<double>(mhx) : 1.0;
+    double const   fg        = mgx > 0.0F ? fix_unit / static_cast<double>(mgx) : 1.0;
+    double const   fh        = mhx > 0.0F ? fix_unit / static_cast<double>(mhx) : 1.0;
     uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
     for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
          r0 < n_rows; r0 += 2 * stride)
@@ -1936,12 +1936,13 @@ __global__ void __launch_bounds__(k_threads)
 // under each leaf's monotone bounds.
 __global__ void __launch_bounds__(k_threads)
     leaf_fix_kernel(Ctl const *ctl, TreeOut t, unsigned long long const *acc,
-                    double2 const *nbound, uint32_t const *absmax, TreeParams tp)
+                    double2 const *nbound, uint32_t const *absmax, TreeParams tp,
+                    double fix_unit)
 {
     float const  mgx = __uint_as_float(absmax[0]);
     float const  mhx = __uint_as_float(absmax[1]);
-    double const fg  = mgx > 0.0F ? k_fix_unit / static_cast<double>(mgx) : 1.0;
-    double const fh  = mhx > 0.0F ? k_fix_unit / static_cast<double>(mhx) : 1.0;
+    double const fg  = mgx > 0.0F ? fix_unit / static_cast<double>(mgx) : 1.0;
+    double const fh  = mhx > 0.0F ? fix_unit / static_cast<double>(mhx) : 1.0;
     uint32_t const n_nodes = min(ctl->n_nodes, k_walk_nodes);
     for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
     {
@@ -2363,7 +2364,7 @@ __global__ void __launch_bounds__(k_threads)
 // W16: int16 codes (a 32-bit word per row) into two-word cells (int64
 // gradient, uint64 hessian sums); a 2,048-row chunk's sums of |q| <= 32767
 // still fit the 32-bit shared words.
-template <typename BinT, bool W16 = false>
+template <typename BinT, bool W16 = false, bool CW2 = W16>
 __global__ void __launch_bounds__(k_qthreads, 3)
     qhist_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
                  uint32_t const *rows, uint4 const *__restrict__ mirror, uint64_t n_rows,
@@ -2452,7 +2453,7 @@ __global__ void __launch_bounds__(k_qthreads, 3)
         }
     }
     __syncthreads();
-    constexpr uint32_t  cw  = W16 ? 2 : 1;
+    constexpr uint32_t  cw  = CW2 ? 2 : 1;
     unsigned long long *dst = hist + (static_cast<uint64_t>(build[ch.node]) * total_cells * cw);
     for (uint32_t x = threadIdx.x; x < cells; x += k_qthreads)
     {
@@ -2462,7 +2463,7 @@ __global__ void __launch_bounds__(k_qthreads, 3)
         if (jj >= 0 && bb < sel_nb[jj] && (hg_s[x] != 0 || hh_s[x] != 0))
         {
             uint64_t const cell = cell_off[jj] + bb;
-            if constexpr (W16)
+            if constexpr (CW2)
             {
                 atomicAdd(&dst[2 * cell],
                           static_cast<unsigned long long>(static_cast<int64_t>(hg_s[x])));
@@ -2503,9 +2504,12 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 // ahead loaded into registers. The shared
 // histogram flushes -- one packed 64-bit global add per touched cell,
 // gradient in the high word (two's complement), hessian in the low word --
-// only when the node changes. The 32-bit words cannot overflow in between:
-// the quantised forms take fewer than 16,909,320 rows and both codes are at
-// most 127 in magnitude, so no cell's sum leaves the int32 range.
+// only when the node changes. The 32-bit shared words cannot overflow in
+// between: a CTA adds a share of one node's rows (fewer than 16,909,320
+// while the grid has a CTA per SM) and both codes are at most 127 in
+// magnitude. Global cells are packed 64-bit words while 127 x the fit's rows
+// stays below 2^31, and two words (int64 gradient, uint64 hessian sums,
+// CW2) beyond that.
 constexpr uint32_t k_ttable_bytes = 256 * 256; // 256 bins x (32 g + 32 h) x 4 B
 
 __device__ __forceinline__ void red_shared_u32(uint32_t addr, uint32_t v)
@@ -2518,6 +2522,7 @@ __device__ __forceinline__ void red_shared_u32_hi(uint32_t addr, uint32_t v)
     asm volatile("red.shared.add.u32 [%0+128], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
+template <bool CW2>
 __device__ __forceinline__ void qflush_t(uint32_t *tbl, uint32_t max_nb, int32_t const *j_s,
                                          uint32_t const *sel_nb, uint32_t const *cell_off,
                                          unsigned long long *dst)
@@ -2533,9 +2538,19 @@ __device__ __forceinline__ void qflush_t(uint32_t *tbl, uint32_t max_nb, int32_t
         int32_t const  j2 = j_s[f];
         if (bb < max_nb && j2 >= 0 && bb < sel_nb[j2] && (g != 0 || h != 0))
         {
-            atomicAdd(&dst[cell_off[j2] + bb],
-                      (static_cast<unsigned long long>(g) << 32) +
-                          static_cast<unsigned long long>(h));
+            uint64_t const cell = cell_off[j2] + bb;
+            if constexpr (CW2)
+            {
+                // two-word cells: the int64 gradient sum, the uint64 hessian sum
+                atomicAdd(&dst[2 * cell], static_cast<unsigned long long>(
+                                              static_cast<int64_t>(static_cast<int32_t>(g))));
+                atomicAdd(&dst[(2 * cell) + 1], static_cast<unsigned long long>(h));
+            }
+            else
+            {
+                atomicAdd(&dst[cell], (static_cast<unsigned long long>(g) << 32) +
+                                          static_cast<unsigned long long>(h));
+            }
         }
         tbl[gi]      = 0;
         tbl[gi + 32] = 0;
@@ -2586,6 +2601,7 @@ __device__ __forceinline__ void cp_async16(uint32_t smem_addr, void const *gsrc)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr), "l"(gsrc));
 }
 
+template <bool CW2>
 __global__ void __launch_bounds__(k_tthreads, 1)
     qhist_t_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *build,
                    uint32_t const *__restrict__ rows, uint4 const *__restrict__ mirror,
@@ -2690,8 +2706,8 @@ __global__ void __launch_bounds__(k_tthreads, 1)
         uint32_t const cnode = bchunks[c].node;
         if (cnode != node)
         {
-            qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
-                     hist + (static_cast<uint64_t>(build[node]) * total_cells));
+            qflush_t<CW2>(tbl, max_nb, j_s, sel_nb, cell_off,
+                          hist + (static_cast<uint64_t>(build[node]) * total_cells * (CW2 ? 2 : 1)));
             node = cnode;
         }
         cp_async_wait<1>(); // this thread's copies of chunk c have landed
@@ -2715,8 +2731,8 @@ __global__ void __launch_bounds__(k_tthreads, 1)
         }
     }
     cp_async_wait<0>();
-    qflush_t(tbl, max_nb, j_s, sel_nb, cell_off,
-             hist + (static_cast<uint64_t>(build[node]) * total_cells));
+    qflush_t<CW2>(tbl, max_nb, j_s, sel_nb, cell_off,
+                  hist + (static_cast<uint64_t>(build[node]) * total_cells * (CW2 ? 2 : 1)));
 }
 
 // The quantised form's node totals: exact integer sums of the first selected
@@ -3397,7 +3413,23 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         throw ConfigError("grower: max_depth above 8 exceeds the level plane's "
                           "512-node frontier; use a host grower");
     }
-    cw_ = cfg_.mode == HistMode::quant16 ? 2 : 1; // int16 sums take two-word cells
+    {
+        uint64_t const fit_rows = std::max<uint64_t>(cfg_.fit_rows, max_root_rows);
+        wide_codes_ = cfg_.mode == HistMode::quant16;
+        // int16 sums always outgrow a packed 32-bit half; int8 sums do once
+        // 127 x rows reaches 2^31 (16,909,320 rows)
+        cw_ = wide_codes_ || (cfg_.mode == HistMode::quant8 && fit_rows * 127ULL >= (1ULL << 31))
+                  ? 2
+                  : 1;
+        // the leaf sums add at most one unit per row: 2^38 up to 2^24 rows,
+        // then one bit less per doubling, so no sum leaves the int64 range
+        uint32_t lg = 24;
+        while (lg < 62 && (uint64_t{1} << lg) < fit_rows)
+        {
+            ++lg;
+        }
+        fix_unit_ = std::ldexp(1.0, 62 - static_cast<int>(lg));
+    }
     std::vector<uint32_t> off(n_sel_ + 1, 0);
     std::vector<uint32_t> nb(n_sel_, 0);
     for (uint32_t j = 0; j < n_sel_; ++j)
@@ -3411,12 +3443,6 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     {
         throw ConfigError("grower: a feature has more than 4096 bins; lower "
                           "bin_mapper.max_bin or use a host grower");
-    }
-    if (cfg_.mode == HistMode::quant8 &&
-        static_cast<uint64_t>(max_root_rows) * 127ULL >= (1ULL << 31))
-    {
-        throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per "
-                          "node; use hist_mode exact");
     }
     total_cells_ = off[n_sel_];
     off_h_       = off;
@@ -3531,7 +3557,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         qscale_  = dalloc<double2>(1, s);
         // +2: the histogram copies whole 4-byte words of codes
         qgh8_    = dalloc<uint16_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 2, s);
-        if (cw_ == 2)
+        if (wide_codes_)
         {
             qgh16_ = dalloc<uint32_t>((max_rows_ > plane_.n_rows ? max_rows_ : plane_.n_rows) + 1,
                                       s);
@@ -3555,11 +3581,17 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(qsmem)));
+        BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint16_t, false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(qsmem)));
         BB_CHECK(cudaFuncSetAttribute(qhist_kernel<uint8_t, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(static_cast<size_t>(32) * max_nb_ * 8)));
         size_t const tsmem = k_tsmem;
-        BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel,
+        BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(tsmem)));
+        BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(tsmem)));
     }
@@ -3770,9 +3802,10 @@ void Grower::set_shard(Reducer *r, uint64_t row_offset, uint64_t total_rows)
         throw ConfigError("grower: a sharded fit needs the quantised form (integer "
                           "histograms combine exactly; float cells would not)");
     }
-    if (r != nullptr && cfg_.mode == HistMode::quant8 && total_rows * 127ULL >= (1ULL << 31))
+    if (r != nullptr && total_rows > std::max<uint64_t>(cfg_.fit_rows, max_rows_))
     {
-        throw ConfigError("grower: int8 histograms hold at most 16,909,320 rows per fit");
+        throw ConfigError("grower: a shard's grower must be sized for the whole fit's rows "
+                          "(GrowConfig::fit_rows)");
     }
     red_        = r;
     row_off_    = row_offset;
@@ -3817,7 +3850,7 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
     }
     uint2 const key = make_uint2(static_cast<uint32_t>(seed_),
                                  static_cast<uint32_t>(seed_ >> 32));
-    if (cw_ == 2)
+    if (wide_codes_)
     {
         quantise_kernel<true><<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh16_,
                                                          qscale_, row_off_);
@@ -3849,7 +3882,7 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         uint32_t const per   = k_mirror_bytes / (plane_.u8 ? 1 : 2);
         size_t const   qsmem = static_cast<size_t>(per) * max_nb_ * 8;
         dim3 const     grid(max_bchunks_, n_tiles_[v]);
-        if (cw_ == 2)
+        if (wide_codes_)
         {
             // int16 codes: the per-chunk kernel with two-word cells
             if (plane_.u8)
@@ -3870,14 +3903,17 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         else if (plane_.u8)
         {
             size_t const tsmem = k_tsmem;
-            qhist_t_kernel<<<dim3(qctas_, n_tiles_[v]), k_tthreads, tsmem, s>>>(
+            auto const kern = cw_ == 2 ? qhist_t_kernel<true> : qhist_t_kernel<false>;
+            kern<<<dim3(qctas_, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);
         }
         else
         {
-            qhist_kernel<uint16_t><<<grid, k_qthreads, qsmem, s>>>(
+            auto const kern =
+                cw_ == 2 ? qhist_kernel<uint16_t, false, true> : qhist_kernel<uint16_t>;
+            kern<<<grid, k_qthreads, qsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);
@@ -4247,7 +4283,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             {
                 kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
                                                 gh_cur_, absmax_, leaf16_, wacc_,
-                                                sample != nullptr ? sample->bits : nullptr);
+                                                sample != nullptr ? sample->bits : nullptr,
+                                                fix_unit_);
             };
             if (plane_.u8)
             {
@@ -4262,7 +4299,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             {
                 red_->sum_u64(wacc_, 2 * static_cast<size_t>(k_walk_nodes), s);
             }
-            leaf_fix_kernel<<<1, k_threads, 0, s>>>(ctl_, t, wacc_, nbound_, absmax_, cfg_.tp);
+            leaf_fix_kernel<<<1, k_threads, 0, s>>>(ctl_, t, wacc_, nbound_, absmax_, cfg_.tp,
+                                                    fix_unit_);
             BB_LAUNCH("leaf_fix_kernel");
             if (next != nullptr)
             {

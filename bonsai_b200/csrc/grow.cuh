@@ -164,6 +164,9 @@ struct GrowConfig
     // for any such sample, so its launches do not depend on which
     uint32_t   sample_k = 0;
     uint32_t   sel_sets = 1;
+    // rows of the whole fit (every shard's, for a row-sharded fit; 0: the
+    // grower's own rows): sizes the quantised cells and fixed-point sums
+    uint64_t   fit_rows = 0;
 };
 
 // All device buffers one tree's growth needs, sized once for a dataset and
@@ -265,7 +268,13 @@ class Grower
     uint32_t              cell_stride_ = 0; // per-(chunk, feature) count stride
     uint32_t              lgroup_      = 1; // nodes per level-finder group
     uint32_t              qctas_       = 1; // u8 quantised histogram CTAs per tile
-    uint32_t              cw_          = 1; // words per quantised cell (2: int16 codes)
+    // words per quantised cell: 2 (an int64 gradient and a uint64 hessian
+    // sum) for int16 codes, and for int8 codes once the fit's rows could carry
+    // a packed 32-bit half past its range (127 x rows >= 2^31)
+    uint32_t              cw_          = 1;
+    bool                  wide_codes_  = false;          // int16 codes (one u32 per row)
+    double                fix_unit_    = 274877906944.0; // fixed-point leaf-sum unit (2^38 at
+                                                         // up to 2^24 rows, halved per doubling)
 
     // device
     uint32_t *sel_      = nullptr; // selected feature ids

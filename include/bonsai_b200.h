@@ -172,6 +172,12 @@ typedef struct
      * passes the selection. */
     float          feature_fraction;
     uint32_t       feature_seed;
+    /* 1: the caller draws each round's rows on the host and hands them over
+     * with bb_booster_set_rows before the round (the rows the reference's
+     * Booster passes to grow() in its resident round, booster.hpp:664-676,
+     * from its own sampler); subsample and random_seed are then unused.
+     * Single-output objectives, unsharded fits. */
+    int32_t        external_sample;
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
@@ -195,6 +201,14 @@ int bb_booster_create(bb_plane const *plane, float const *labels,
  * Before the first round only (BB_ERR_ARG after). A sharded fit sets each
  * shard's weights on its own rank. */
 int bb_booster_set_weights(bb_booster *b, float const *weights);
+
+/* The rows the next round grows over, for a booster created with
+ * external_sample: n_rows ascending row ids (host), every row's score still
+ * taking the tree. Called once before each round (each bb_booster_update of
+ * one round); a round without rows is refused. Replaces the row list the
+ * reference's resident round passes to its grower (Booster::resident_round,
+ * include/bonsai/booster.hpp:664-676). */
+int bb_booster_set_rows(bb_booster *b, uint32_t const *rows, uint64_t n_rows);
 
 /* Runs n_iters more rounds (asynchronous; bb_booster_sync waits). */
 int bb_booster_update(bb_booster *b, uint32_t n_iters);

@@ -43,7 +43,7 @@ class RefCfg(C.Structure):
         ("monotone", C.POINTER(C.c_int32)), ("n_monotone", C.c_uint32),
         ("interaction", C.c_char_p), ("quantile_alpha", C.c_float), ("huber_delta", C.c_float),
         ("dart_drop_rate", C.c_float), ("goss_top_rate", C.c_float),
-        ("goss_other_rate", C.c_float),
+        ("goss_other_rate", C.c_float), ("hist_mode", C.c_int32),
     ]
 
 
@@ -80,6 +80,7 @@ class TreeCfg:
     goss_other_rate: float = 0.1
     monotone: list = field(default_factory=list)
     interaction_constraints: list = field(default_factory=list)  # TOML strings, "0,1"
+    hist_mode: str = "exact"  # the drop-in grower's form: exact, int8, int16
 
     def ref(self):
         c = RefCfg()
@@ -91,6 +92,7 @@ class TreeCfg:
                   "random_seed", "n_threads", "n_classes", "quantile_alpha", "huber_delta",
                   "dart_drop_rate", "goss_top_rate", "goss_other_rate"):
             setattr(c, k, getattr(self, k))
+        c.hist_mode = {"exact": 0, "int8": 1, "int16": 2}[self.hist_mode]
         if self.monotone:
             self._mono = np.asarray(self.monotone, dtype=np.int32)
             c.monotone = _p(self._mono, C.c_int32)
@@ -217,6 +219,22 @@ class RefLib:
         if not h:
             raise RuntimeError(self.err())
         return RefModel(self, h)
+
+    def train_b200_valid(self, ds, valid, cfg: TreeCfg):
+        """train_b200 with a validation set, routed as the reference's fit loop
+        routes a device grower's: returns (model, per-round losses, per-round
+        flags of losses the device plane reported)."""
+        f = self.L.ref_b200_train_valid
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(RefCfg), C.c_void_p, C.c_void_p]
+        rc = cfg.ref()
+        losses = np.zeros(cfg.n_iters, np.float32)
+        dev = np.zeros(cfg.n_iters, np.int32)
+        h = f(C.c_void_p(ds.h), C.c_void_p(valid.h), C.byref(rc), losses.ctypes.data,
+              dev.ctypes.data)
+        if not h:
+            raise RuntimeError(self.err())
+        return RefModel(self, h), losses, dev
 
     def grow_tree(self, ds, cfg: TreeCfg, grad, hess, rows=None):
         n = ds.n

@@ -157,6 +157,7 @@ struct ref_cfg
         float          dart_drop_rate;
         float          goss_top_rate;   // > 0 selects the GOSS sampler
         float          goss_other_rate;
+        int32_t        hist_mode; // the drop-in grower's form: 0 plain, 1 int8, 2 int16
     };
 
     struct RefModel
@@ -875,6 +876,87 @@ template <typename Gr> RefModel *b200_train_with(Dataset const &ds, ref_cfg cons
 }
 } // namespace
 
+namespace
+{
+// The shim of grower kind K in the form c.hist_mode.
+template <int K, typename F> void with_form(ref_cfg const &c, F &&f)
+{
+    switch (c.hist_mode)
+    {
+    case 1:
+        f(static_cast<B200Grower<K, 1> *>(nullptr));
+        break;
+    case 2:
+        f(static_cast<B200Grower<K, 2> *>(nullptr));
+        break;
+    default:
+        f(static_cast<B200Grower<K, 0> *>(nullptr));
+        break;
+    }
+}
+
+template <typename F> void with_shim(ref_cfg const &c, F &&f)
+{
+    switch (c.grower)
+    {
+    case 1:
+        with_form<1>(c, f);
+        break;
+    case 2:
+        with_form<2>(c, f);
+        break;
+    default:
+        with_form<0>(c, f);
+        break;
+    }
+}
+
+// The validation route the reference's fit loop takes with a device grower
+// (src/cli/pipeline.cpp:380-450): after round 0 the booster arms its
+// resident validation plane with the initial scores; every round then asks
+// it to add the round's tree and report the loss, falling back to the host
+// bin-space walk and host loss when it declines.
+template <typename Gr>
+RefModel *b200_train_valid_with(Dataset const &ds, Dataset const &valid, ref_cfg const &c,
+                                float *losses, int32_t *on_device)
+{
+    Config cfg = make_config(c);
+    parallel::set_n_threads(c.n_threads);
+    auto mm     = std::make_unique<RefModel>();
+    mm->grower  = c.grower;
+    mm->booster = make_for_sampler<Gr>(c, cfg);
+    IBooster          &b = *mm->booster;
+    std::vector<float> es;
+    bool               device_eval = false;
+    for (uint32_t i = 0; i < c.n_iters; ++i)
+    {
+        b.update_one_iter(ds);
+        if (i == 0)
+        {
+            auto *raw = mm->booster.get();
+            read_init(*mm, dynamic_cast<Booster<MSEObjective, Gr, AllRowsSampler> const *>(raw));
+            read_init(*mm,
+                      dynamic_cast<Booster<LogLossObjective, Gr, AllRowsSampler> const *>(raw));
+            es.assign(valid.n_rows(), mm->init_scores.at(0));
+            device_eval = b.begin_resident_validation(valid, std::span<float const>{es});
+        }
+        std::optional<float> loss;
+        if (device_eval)
+        {
+            device_eval = b.accumulate_last_round_resident(valid, es, loss);
+        }
+        if (!device_eval)
+        {
+            b.accumulate_last_round_binned(valid, es);
+        }
+        losses[i]    = loss.has_value() ? *loss : b.validation_loss(es, valid.labels());
+        on_device[i] = loss.has_value() ? 1 : 0;
+    }
+    harvest<Gr>(*mm, c);
+    return mm.release();
+}
+} // namespace
+
 extern "C" void *ref_b200_train(void const *dsp, ref_cfg const *c)
 {
     RefModel *m  = nullptr;
@@ -882,18 +964,29 @@ extern "C" void *ref_b200_train(void const *dsp, ref_cfg const *c)
         [&]
         {
             auto const &ds = *static_cast<Dataset const *>(dsp);
-            switch (c->grower)
-            {
-            case 1:
-                m = b200_train_with<B200ObliviousGrower>(ds, *c);
-                break;
-            case 2:
-                m = b200_train_with<B200LeafwiseGrower>(ds, *c);
-                break;
-            default:
-                m = b200_train_with<B200DepthwiseGrower>(ds, *c);
-                break;
-            }
+            with_shim(*c, [&](auto *tag)
+                      { m = b200_train_with<std::remove_pointer_t<decltype(tag)>>(ds, *c); });
+        });
+    return rc == 0 ? m : nullptr;
+}
+
+// ref_b200_train with a validation set: per-round losses, and whether each
+// came from the device plane.
+extern "C" void *ref_b200_train_valid(void const *dsp, void const *vdsp, ref_cfg const *c,
+                                      float *losses, int32_t *on_device)
+{
+    RefModel *m  = nullptr;
+    int const rc = guarded(
+        [&]
+        {
+            auto const &ds = *static_cast<Dataset const *>(dsp);
+            auto const &vs = *static_cast<Dataset const *>(vdsp);
+            with_shim(*c,
+                      [&](auto *tag)
+                      {
+                          m = b200_train_valid_with<std::remove_pointer_t<decltype(tag)>>(
+                              ds, vs, *c, losses, on_device);
+                      });
         });
     return rc == 0 ? m : nullptr;
 }

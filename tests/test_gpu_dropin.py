@@ -54,17 +54,131 @@ def test_reference_booster_over_b200_grower_matches_cpu(dref, cfg):
     assert np.array_equal(gpu.predict_binned(ds), cpu.predict_binned(ds))
 
 
-def test_reference_booster_over_b200_grower_logloss(dref):
+def test_reference_booster_over_b200_grower_logloss(dref, monkeypatch):
     X, y = _data(seed=9)
     yb = (y > np.median(y)).astype(np.float32)
     cuts, off = dref.fit_cuts(X)
     ds = dref.dataset(X, yb, cuts, off)
     tc = TreeCfg(objective="logloss", max_depth=6, n_iters=20)
     cpu = dref.train(ds, tc)
+    # the reference's own escape hatch keeps the host objective (booster.hpp:
+    # 634-636): the same host gradients on both sides, the same trees
+    monkeypatch.setenv("BONSAI_HOST_OBJECTIVE", "1")
     gpu = dref.train_b200(ds, tc)
-    # host objective on both sides: the same gradients, the same trees
     for i in range(tc.n_iters):
         assert_trees_equal(gpu.tree(i), cpu.tree(i), f"round {i}")
+
+
+# ---- the resident round through the reference's own Booster seam
+# (try_resident_round / resident_round, include/bonsai/booster.hpp:630-676):
+# the shim arms it, so grow() runs whole device rounds (bb_booster_*).
+
+def _bb_fit(bb, X, y, cuts, off, n_iters, **kw):
+    plane = bb.Plane(X, cuts, off)
+    b = bb.Booster(plane, y, bb.TrainParams(use_graph=True, **kw), max_trees=n_iters)
+    b.update(n_iters)
+    return b.trees(), plane
+
+
+def _same_tree(a, t, where):
+    """A reference-harvested tree against one of this package's trees."""
+    for k in ("feature", "left", "right", "default_left"):
+        assert np.array_equal(getattr(a, k), getattr(t, k)), f"{where} {k}"
+    for k in ("value", "gains", "covers"):
+        x = getattr(a, k)
+        z = getattr(t, k)
+        assert np.array_equal(x.view(np.uint32), z.view(np.uint32)), f"{where} {k}"
+
+
+@pytest.mark.parametrize("subsample", [1.0, 0.8])
+def test_resident_rounds_through_the_booster_equal_the_host_rounds(dref, monkeypatch,
+                                                                  subsample):
+    """Squared error: the reference's booster arms the shim's resident round
+    (device gradients and fused score updates; a Bernoulli sample's rows handed
+    over each round with bb_booster_set_rows) and its trees equal those of the
+    same booster kept on the host objective, and the CPU grower's, bit for bit."""
+    X, y = _data(seed=21)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    tc = TreeCfg(max_depth=6, n_iters=12, learning_rate=0.2, subsample=subsample,
+                 feature_fraction=0.8)
+    cpu = dref.train(ds, tc)
+    res = dref.train_b200(ds, tc)
+    monkeypatch.setenv("BONSAI_HOST_OBJECTIVE", "1")
+    host = dref.train_b200(ds, tc)
+    for i in range(tc.n_iters):
+        assert_trees_equal(res.tree(i), cpu.tree(i), f"round {i}")
+        assert_trees_equal(host.tree(i), cpu.tree(i), f"round {i}")
+    assert np.array_equal(res.predict_binned(ds), cpu.predict_binned(ds))
+
+
+@pytest.mark.parametrize("mode", ["int8", "int16"])
+@pytest.mark.parametrize("subsample", [1.0, 0.8])
+def test_quantised_resident_round_through_the_booster(bb, dref, mode, subsample):
+    """The quantised form behind the reference's Booster<LogLoss, B200
+    DepthwiseGrowerInt8|Int16, AllRows|Bernoulli>: the resident rounds are
+    this package's quantised rounds -- the same trees as bb_booster_* fitting
+    the same data with the same seed (the sampler's rows are the device
+    booster's own Bernoulli draws from the same seed)."""
+    X, y = _data(seed=23, n=20_000)
+    yb = (y > np.median(y)).astype(np.float32)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, yb, cuts, off)
+    tc = TreeCfg(objective="logloss", max_depth=6, n_iters=10, learning_rate=0.2,
+                 subsample=subsample, hist_mode=mode)
+    got = dref.train_b200(ds, tc)
+    want, _ = _bb_fit(bb, X, yb, cuts, off, tc.n_iters, objective="logloss", max_depth=6,
+                      learning_rate=0.2, hist_mode=mode, seed=0, subsample=subsample,
+                      random_seed=tc.random_seed)
+    assert got.n_trees() == len(want) == tc.n_iters
+    for i in range(tc.n_iters):
+        _same_tree(got.tree(i), want[i], f"round {i}")
+
+
+@pytest.mark.parametrize("grower", ["levelwise", "leafwise"])
+def test_quantised_resident_levelwise_and_leafwise(bb, dref, grower):
+    X, y = _data(seed=25, n=15_000)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    kw = dict(max_depth=5) if grower == "levelwise" else dict(max_depth=10, max_leaves=31)
+    tc = TreeCfg(grower=grower, n_iters=6, learning_rate=0.2, hist_mode="int8", **kw)
+    got = dref.train_b200(ds, tc)
+    want, _ = _bb_fit(bb, X, y, cuts, off, tc.n_iters, grower=grower, learning_rate=0.2,
+                      hist_mode="int8", seed=0, **kw)
+    for i in range(tc.n_iters):
+        if grower == "levelwise":
+            # the reference keeps ObliviousTree tables: levels and leaf table
+            for a, b in zip(got.oblivious(i), bb.oblivious_tables(want[i])):
+                assert np.array_equal(np.asarray(a).view(np.uint8),
+                                      np.asarray(b).view(np.uint8)), f"round {i}"
+        else:
+            _same_tree(got.tree(i), want[i], f"round {i}")
+
+
+def test_resident_validation_plane_through_the_booster(dref, monkeypatch):
+    """The fit loop's device validation route (src/cli/pipeline.cpp:420-450)
+    over the shim: round 0's tree is added on arming and its loss is the
+    host's; every later round's loss comes from the device plane and equals
+    the host route's loss (the same booster kept on the host objective and
+    the host bin-space walk) within float rounding."""
+    X, y = _data(seed=27, n=12_000)
+    Xv, yv = _data(seed=28, n=3_000)
+    cuts, off = dref.fit_cuts(X)
+    ds = dref.dataset(X, y, cuts, off)
+    vs = dref.dataset(Xv, yv, cuts, off)
+    tc = TreeCfg(max_depth=5, n_iters=8, learning_rate=0.2)
+    model, losses, dev = dref.train_b200_valid(ds, vs, tc)
+    assert dev[0] == 0 and (dev[1:] == 1).all()
+    cpu = dref.train(ds, tc)
+    for i in range(tc.n_iters):
+        assert_trees_equal(model.tree(i), cpu.tree(i), f"round {i}")
+    monkeypatch.setenv("BONSAI_HOST_OBJECTIVE", "1")
+    host, host_losses, host_dev = dref.train_b200_valid(ds, vs, tc)
+    assert (host_dev == 0).all()
+    for i in range(tc.n_iters):
+        assert_trees_equal(host.tree(i), cpu.tree(i), f"round {i}")
+    assert losses[0] == host_losses[0]
+    np.testing.assert_allclose(losses, host_losses, rtol=1e-5)
 
 
 @pytest.mark.parametrize("objective,kw", [("mae", {}), ("huber", dict(huber_delta=0.5)),
