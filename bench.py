@@ -483,6 +483,24 @@ def config_main(args, name):
     ms = b.last_ms / K
     prof = b.profile_round()
     b.close()
+    # the quantised build's launch shape for this shape (bonsai_b200.autotune),
+    # then the same K rounds with it
+    autotune = None
+    if args.mode != "exact" and not args.no_tune:
+        t0 = time.perf_counter()
+        tp = bb.tune(plane, y, params, rounds=2)
+        tune_s = time.perf_counter() - t0
+        default_ms = ms
+        if tp.hist_ctas != params.hist_ctas:
+            bt = bb.Booster(plane, y, tp, max_trees=W + K + 2)
+            bt.update(W)
+            with Clocks(0) as clk:
+                bt.update(K)
+            ms = bt.last_ms / K
+            prof = bt.profile_round()
+            bt.close()
+        autotune = {"hist_ctas": tp.hist_ctas, "tune_s": tune_s,
+                    "default_ms_per_step": default_ms, "tuned_ms_per_step": ms}
     value = ms * rounds / 1000.0
     line = {"metric": f"{name} fit s/{rounds} iters", "value": value, "unit": "s", "n_gpus": 1,
             "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": False,
@@ -497,7 +515,8 @@ def config_main(args, name):
                     "setup_s": t_setup},
             "phases_ms": {k: prof[k] for k in ("hist_ms", "partition_ms", "find_ms",
                                                "other_ms", "total_ms")},
-            "gpu_launches": int(prof["launches"]) * K, "clocks": clk.summary()}
+            "gpu_launches": int(prof["launches"]) * K, "clocks": clk.summary(),
+            "autotune": autotune}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = config_reference(name, X, y, cuts, off, rounds)
     print(json.dumps(line), flush=True)
@@ -638,6 +657,8 @@ def main():
                          "and the AUC delta (0 skips it)")
     ap.add_argument("--rows", type=int, default=10_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default histogram launch shape (no autotuning)")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
                     help="fit: validation rows for the AUC and logloss (0 skips)")
     ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass", "many"])
@@ -802,15 +823,35 @@ def fit_main(args, world, rank, local, W, K):
     yp = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
     yp[...] = y
 
-    def params(mode):
+    def params(mode, hist_ctas=0):
         return bb.TrainParams(objective="logloss", max_depth=8, learning_rate=0.1,
-                              min_data_in_leaf=20, hist_mode=mode, use_graph=True)
+                              min_data_in_leaf=20, hist_mode=mode, use_graph=True,
+                              hist_ctas=hist_ctas)
+
+    tuned = {"hist_ctas": 0}
 
     def booster(plane, mode, max_trees):
+        p = params(mode, tuned["hist_ctas"] if mode == args.mode else 0)
         if sharded:
-            return bb.Booster(plane, yp, params(mode), max_trees=max_trees, comm=comm,
+            return bb.Booster(plane, yp, p, max_trees=max_trees, comm=comm,
                               row_offset=row0, total_rows=n_fit, init_score=init)
-        return bb.Booster(plane, yp, params(mode), max_trees=max_trees)
+        return bb.Booster(plane, yp, p, max_trees=max_trees)
+
+    # the quantised build's launch shape for this data, timed once per shape
+    # (bonsai_b200.autotune; cached on disk) before anything is timed
+    autotune = None
+    if args.mode != "exact" and not sharded and not args.no_tune:
+        tplane = bb.Plane(Xp, cuts, off)
+        t0 = time.perf_counter()
+        tp = bb.tune(tplane, yp, params(args.mode))
+        autotune = {"hist_ctas": tp.hist_ctas, "tune_s": time.perf_counter() - t0}
+        from bonsai_b200 import autotune as _at
+        ent = _at.load().get(_at.shape_key(tplane.n_rows, tplane.n_feats, True, tp,
+                                           _at.device_name()))
+        if ent is not None:
+            autotune["ms_per_round"] = ent["ms_per_round"]
+        tplane.close()
+        tuned["hist_ctas"] = tp.hist_ctas
 
     # ---- the complete fit, end to end through the C ABI with host buffers:
     # pinned X -> ingest (H2D + bin application), labels up, 500 rounds, the
@@ -923,6 +964,7 @@ def fit_main(args, world, rank, local, W, K):
                         "-> trees and training scores on the host"},
         "plain_form": plain,
         "accuracy": accuracy,
+        "autotune": autotune,
         "roofline": {"bound": "hbm",
                      "kernel": ("histogram build (qhist_t_kernel per level)" if args.mode != "exact"
                                 else "histogram build (count+offsets+scatter+chain)"),

@@ -28,7 +28,7 @@ __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
     "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "pred_contribs_classes", "oblivious_tables", "fit_cuts",
     "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows", "fit_cuts_device",
-    "available", "LEAF",
+    "available", "LEAF", "tune",
 ]
 
 LEAF = 0xFFFFFFFF
@@ -97,6 +97,10 @@ class TrainParams:
     # (sample_features, src/grower_impl.hpp:163-180)
     feature_fraction: float = 1.0
     feature_seed: int = 2
+    # the quantised histogram build's CTAs per mirror tile (0: the default
+    # launch shape); bonsai_b200.autotune picks it per shape. Results do not
+    # depend on it.
+    hist_ctas: int = 0
 
     def c(self) -> _lib.TrainCfg:
         c = _lib.TrainCfg()
@@ -118,6 +122,7 @@ class TrainParams:
         c.feature_fraction = self.feature_fraction
         c.feature_seed = self.feature_seed
         c.use_graph = 1 if self.use_graph else 0
+        c.hist_ctas = int(self.hist_ctas)
         c.record_leaf_ids = 1 if self.record_leaf_ids else 0
         if self.monotone:
             c._mono = np.ascontiguousarray(self.monotone, dtype=np.int8)
@@ -794,3 +799,10 @@ class ShapPlan:
             self.close()
         except Exception:
             pass
+
+
+def tune(plane, labels, params, **kw):
+    """params with the quantised build's launch shape autotuned for this
+    plane (bonsai_b200.autotune: timed once per shape, cached on disk)."""
+    from .autotune import tune as _tune
+    return _tune(plane, labels, params, **kw)

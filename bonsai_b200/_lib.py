@@ -42,7 +42,7 @@ class TrainCfg(C.Structure):
         ("interaction_offsets", C.POINTER(C.c_uint32)), ("n_interaction_groups", C.c_uint32),
         ("subsample", C.c_float), ("random_seed", C.c_uint32),
         ("feature_fraction", C.c_float), ("feature_seed", C.c_uint32),
-        ("external_sample", C.c_int32),
+        ("external_sample", C.c_int32), ("hist_ctas", C.c_uint32),
     ]
 
 

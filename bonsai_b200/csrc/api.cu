@@ -387,6 +387,7 @@ GrowConfig grow_config(bb_train_cfg const &c)
     g.tp.min_data_in_leaf  = c.min_data_in_leaf;
     g.tp.max_leaves        = c.grower == 2 ? c.max_leaves : 0;
     g.mode                 = static_cast<HistMode>(c.hist_mode);
+    g.hist_ctas            = c.hist_ctas;
     return g;
 }
 

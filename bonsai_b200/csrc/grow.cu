@@ -3477,7 +3477,9 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     crows_       = quant_ ? k_qbuild_rows : k_build_rows;
     // the histogram grid: one CTA per SM for a large fit, about one per four
     // 2,048-row chunks of the root for a small one
-    qctas_       = std::max(1u, std::min(k_qctas, ceil_div(max_rows_, 4 * k_qbuild_rows)));
+    qctas_       = cfg_.hist_ctas > 0
+                       ? std::min(cfg_.hist_ctas, 64u * k_qctas)
+                       : std::max(1u, std::min(k_qctas, ceil_div(max_rows_, 4 * k_qbuild_rows)));
     max_pchunks_ = ceil_div(max_rows_, k_part_rows) + max_front_;
     max_bchunks_ = ceil_div(max_rows_, crows_) + max_front_;
 
@@ -3903,8 +3905,16 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         else if (plane_.u8)
         {
             size_t const tsmem = k_tsmem;
+            // CTAs per tile: the caller's count, else one per SM for a plane of
+            // one tile, and about two waves over all tiles for a wide plane (a
+            // CTA zeroes and flushes a 64 KB table per node, so many tiles
+            // want fewer, longer CTAs each)
+            uint32_t const ctas =
+                cfg_.hist_ctas > 0 ? qctas_
+                                   : std::max(1u, std::min(qctas_, ceil_div(2 * k_qctas,
+                                                                            n_tiles_[v])));
             auto const kern = cw_ == 2 ? qhist_t_kernel<true> : qhist_t_kernel<false>;
-            kern<<<dim3(qctas_, n_tiles_[v]), k_tthreads, tsmem, s>>>(
+            kern<<<dim3(ctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
                 plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
                 static_cast<unsigned long long *>(hist_[dst]), total_cells_);

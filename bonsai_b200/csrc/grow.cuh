@@ -167,6 +167,9 @@ struct GrowConfig
     // rows of the whole fit (every shard's, for a row-sharded fit; 0: the
     // grower's own rows): sizes the quantised cells and fixed-point sums
     uint64_t   fit_rows = 0;
+    // the quantised build's CTAs per mirror tile (0: one per SM, fewer for a
+    // small dataset); a launch shape only -- the cells are order-free sums
+    uint32_t   hist_ctas = 0;
 };
 
 // All device buffers one tree's growth needs, sized once for a dataset and

@@ -178,6 +178,13 @@ typedef struct
      * from its own sampler); subsample and random_seed are then unused.
      * Single-output objectives, unsharded fits. */
     int32_t        external_sample;
+    /* The quantised histogram build's CTAs per mirror tile (a persistent
+     * grid over the level's row chunks): 0 picks the default (one per SM,
+     * fewer for a small dataset); bonsai_b200.autotune times candidates and
+     * caches the fastest per shape. Results do not depend on it (the
+     * quantised cells are order-free integer sums). No reference key: the
+     * reference's launch shapes are fixed. */
+    uint32_t       hist_ctas;
 } bb_train_cfg;
 
 /* A device-resident boosting fit over the plane: labels (host, n_rows) and
