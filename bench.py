@@ -645,6 +645,110 @@ def many_reference(sets, cuts, every=8, steps=3):
                       f"x {total / r:.3g} (rows) x {MANY_ROUNDS} (rounds)"}
 
 
+ACC_ROUNDS = {"wide": 50, "multiclass": 300, "many": 100}
+
+
+def _mse(a, b):
+    return float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+
+
+def _softmax_loss(y, S):
+    S = np.asarray(S, np.float64)
+    S = S - S.max(axis=1, keepdims=True)
+    lse = np.log(np.exp(S).sum(axis=1))
+    return float(np.mean(lse - S[np.arange(len(y)), y.astype(np.int64)]))
+
+
+def _hist_err_mse(bb, plane, scores, y):
+    """The int8 root histogram of the fit's final squared-error gradients
+    (g = score - y, h = 1) against FP64 sums: relative L1 error of the
+    gradient cells (h is constant, so its cells are exact)."""
+    g = (np.asarray(scores, np.float64) - y).astype(np.float32)
+    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=7), g,
+                    np.ones_like(g))
+    codes = plane.bins()
+    G = np.concatenate([np.bincount(codes[f], weights=g.astype(np.float64),
+                                    minlength=int(plane.n_bins[f]))
+                        for f in range(codes.shape[0])])
+    return {"g_rel_l1": float(np.abs(q[:, 0] - G).sum() / np.abs(G).sum())}
+
+
+def accuracy_main(args):
+    """The quantised form against the plain form on held-out rows of each
+    configuration's generator: validation loss (and class accuracy) of both
+    fits and their difference, and the int8 histogram's error against FP64
+    sums. One JSON line per configuration."""
+    import bonsai_b200 as bb
+    from bonsai_b200 import synth
+    from bonsai_b200.binning import fit_cuts
+    from bonsai_b200.build import build_library
+    build_library()
+    out = []
+    # wide sparse leafwise: 1,000,000 training rows and 100,000 held out
+    X, y = synth.wide_sparse(n=1_100_000)
+    Xt, yt, Xv, yv = X[:1_000_000], y[:1_000_000], X[1_000_000:], y[1_000_000:]
+    cuts, off = fit_cuts(Xt, max_bin=256)
+    pt, pv = bb.Plane(Xt, cuts, off), bb.Plane(Xv, cuts, off)
+    R = ACC_ROUNDS["wide"]
+    res = {}
+    for mode in ("int8", "exact"):
+        b = bb.Booster(pt, yt, bb.TrainParams(hist_mode=mode, **config_tc("wide", bb)),
+                       max_trees=R)
+        b.update(R)
+        res[mode] = _mse(bb.predict(pv, b.trees(), b.init_score, 0.1), yv)
+        if mode == "int8":
+            herr = _hist_err_mse(bb, pt, b.scores(), yt)
+        b.close()
+    out.append({"config": "wide", "rounds": R, "valid_rows": len(yv),
+                "valid_mse": res, "delta_mse": res["int8"] - res["exact"],
+                "rel_delta_mse": (res["int8"] - res["exact"]) / res["exact"],
+                "hist_error_vs_fp64": herr})
+    del X, Xt, pt, pv
+    # multiclass levelwise softmax: 581,012 training rows and 100,000 held out
+    X, y = synth.multiclass_onehot(n=681_012)
+    Xt, yt, Xv, yv = X[:581_012], y[:581_012], X[581_012:], y[581_012:]
+    cuts, off = fit_cuts(Xt, max_bin=255)
+    pt, pv = bb.Plane(Xt, cuts, off), bb.Plane(Xv, cuts, off)
+    R = ACC_ROUNDS["multiclass"]
+    res = {}
+    for mode in ("int8", "exact"):
+        b = bb.Booster(pt, yt, bb.TrainParams(hist_mode=mode, use_graph=True,
+                                              **config_tc("multiclass", bb)), max_trees=R)
+        b.update(R)
+        S = bb.predict_classes(pv, b.trees(), b.init_scores, 0.1)
+        res[mode] = {"logloss": _softmax_loss(yv, S),
+                     "accuracy": float(np.mean(np.argmax(S, axis=1) == yv))}
+        b.close()
+    out.append({"config": "multiclass", "rounds": R, "valid_rows": len(yv), "valid": res,
+                "delta_logloss": res["int8"]["logloss"] - res["exact"]["logloss"],
+                "delta_accuracy": res["int8"]["accuracy"] - res["exact"]["accuracy"]})
+    del X, Xt, pt, pv
+    # the 64 ragged datasets: 20% of each dataset's rows held out
+    R = ACC_ROUNDS["many"]
+    deltas, rels = [], []
+    for X, y in synth.ragged_many():
+        k = int(len(y) * 0.8)
+        cuts, off = fit_cuts(X[:k])
+        pt, pv = bb.Plane(X[:k], cuts, off), bb.Plane(X[k:], cuts, off)
+        res = {}
+        for mode in ("int8", "exact"):
+            b = bb.Booster(pt, y[:k], bb.TrainParams(max_depth=6, learning_rate=0.1,
+                                                     hist_mode=mode, use_graph=True),
+                           max_trees=R)
+            b.update(R)
+            res[mode] = _mse(bb.predict(pv, b.trees(), b.init_score, 0.1), y[k:])
+            b.close()
+        deltas.append(res["int8"] - res["exact"])
+        rels.append((res["int8"] - res["exact"]) / res["exact"])
+        pt.close()
+        pv.close()
+    out.append({"config": "many", "rounds": R, "datasets": len(deltas),
+                "rel_delta_mse": {"mean": float(np.mean(rels)), "max": float(np.max(rels)),
+                                  "min": float(np.min(rels))}})
+    for line in out:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -661,7 +765,8 @@ def main():
                     help="keep the default histogram launch shape (no autotuning)")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
                     help="fit: validation rows for the AUC and logloss (0 skips)")
-    ap.add_argument("--workload", default="fit", choices=["fit", "serve", "wide", "multiclass", "many"])
+    ap.add_argument("--workload", default="fit",
+                    choices=["fit", "serve", "wide", "multiclass", "many", "accuracy"])
     ap.add_argument("--batches", default=",".join(map(str, SERVE_BATCHES)),
                     help="serve: predict request batch sizes")
     ap.add_argument("--shap-batches", default=",".join(map(str, SHAP_BATCHES)),
@@ -671,6 +776,11 @@ def main():
     K = max(1, args.steps)
 
     world, rank, local = dist_init(args.gpus)
+    if args.workload == "accuracy":
+        if rank == 0:
+            accuracy_main(args)
+        barrier(world)
+        return
     if args.workload == "many":
         if rank == 0:
             many_main(args)

@@ -3053,29 +3053,6 @@ struct LeafOut
     uint32_t pad[2];
 };
 
-__global__ void __launch_bounds__(k_plan_thr)
-    leaf_setup_kernel(Ctl *ctl, Node *nodes, Best *best, Chunk *pchunks, uint32_t *pcr,
-                      LeafPop p)
-{
-    uint32_t const nch = (p.node.count + k_part_rows - 1) / k_part_rows;
-    if (threadIdx.x == 0)
-    {
-        ctl->n_cur     = 1;
-        ctl->n_pchunks = nch;
-        Node nd        = p.node;
-        nd.flags       = 1;
-        nodes[0]       = nd;
-        best[0]        = p.best;
-        pcr[0]         = 0;
-        pcr[1]         = nch;
-    }
-    for (uint32_t c = threadIdx.x; c < nch; c += k_plan_thr)
-    {
-        uint32_t const b = c * k_part_rows;
-        pchunks[c]       = {0, p.node.start + b, min(k_part_rows, p.node.count - b), 0};
-    }
-}
-
 // After partition pass 1: the chunks' left bases, the node's left count, and
 // either the demotion (a side came out empty) or the two children, the
 // smaller child's build chunks (in the scatter's output, which starts at 0)
@@ -3084,8 +3061,9 @@ __global__ void __launch_bounds__(k_plan_thr)
     leaf_plan_kernel(Ctl *ctl, Chunk const *pchunks, uint32_t *pleft, uint32_t *prbase,
                      uint32_t *nleft, uint32_t *dst, uint32_t *build, uint32_t *brange,
                      uint32_t *bbase, Chunk *bchunks, uint32_t *bpair, Node *nodes, Node *next,
-                     uint32_t *slot_of, LeafOut *out, uint32_t crows, LeafPop p)
+                     uint32_t *slot_of, LeafOut *out, uint32_t crows, LeafPop const *pp)
 {
+    LeafPop const  p    = *pp;
     uint32_t const n_ch = ctl->n_pchunks;
     uint32_t const per  = (n_ch + k_plan_thr - 1) / k_plan_thr;
     uint32_t const c_a  = min(n_ch, threadIdx.x * per);
@@ -3160,12 +3138,14 @@ __global__ void __launch_bounds__(k_plan_thr)
 
 // The partitioned segment back into the row buffer.
 __global__ void leaf_copyback_kernel(LeafOut const *out, uint32_t const *__restrict__ tmp,
-                                     uint32_t *__restrict__ rows, uint32_t start, uint32_t count)
+                                     uint32_t *__restrict__ rows, LeafPop const *pp)
 {
     if (out->split == 0)
     {
         return;
     }
+    uint32_t const start = pp->node.start;
+    uint32_t const count = pp->node.count;
     for (uint32_t k = (blockIdx.x * blockDim.x) + threadIdx.x; k < count;
          k += gridDim.x * blockDim.x)
     {
@@ -3211,8 +3191,8 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
                                    uint32_t const *slot_of, void const *pool,
                                    uint32_t total_cells, uint32_t const *sel,
                                    uint32_t const *sel_nb, int8_t const *mono, uint32_t n_mono,
-                                   TreeParams tp, double2 const *qscale, LeafPop p, uint32_t cw,
-                                   uint64_t const *fgroups)
+                                   TreeParams tp, double2 const *qscale, LeafPop const *pp,
+                                   uint32_t cw, uint64_t const *fgroups)
 {
     __shared__ int64_t qtot_s[4];
     __shared__ float   tot_s[4];
@@ -3258,8 +3238,9 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
     {
         return;
     }
-    Node L = next[0];
-    Node R = next[1];
+    LeafPop const p = *pp;
+    Node          L = next[0];
+    Node          R = next[1];
     double gl, hl, gr, hr;
     if constexpr (Q)
     {
@@ -3319,8 +3300,9 @@ constexpr uint32_t k_best_thr = 256;
 
 __global__ void __launch_bounds__(k_best_thr)
     leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_sel, Node const *nodes,
-                     LeafOut *out, uint32_t may_split)
+                     LeafOut *out, uint32_t const *may_split_p)
 {
+    uint32_t const      may_split = *may_split_p;
     __shared__ double   g_s[k_best_thr / 32];
     __shared__ uint32_t o_s[k_best_thr / 32];
     uint32_t const      w    = blockIdx.x;
@@ -3360,6 +3342,329 @@ __global__ void __launch_bounds__(k_best_thr)
             out->child[w] = nodes[w];
         }
     }
+}
+
+// ---- the leafwise pop loop on the device -----------------------------------
+// LeafwiseGrower::grow's heap loop (src/grower_impl.hpp:744-850): the gain
+// max-heap (ties to the lower node id, so growth is deterministic), the
+// histogram pool's free slots, the node table and the leaf list all live on
+// the device, and one pop is a fixed sequence of launches that a CUDA graph's
+// conditional WHILE node repeats until the heap is empty or the leaf budget
+// is spent -- no host round trip per pop.
+
+struct LeafCand
+{
+    Node     node;
+    Best     best;
+    uint32_t depth;
+    uint32_t slot;
+};
+
+struct LeafLoop
+{
+    LeafPop  pop;        // the current pop
+    uint32_t pop_depth;
+    uint32_t may_split;  // the pop's children may split (depth cap)
+    uint32_t root_may;   // the root may split
+    uint32_t noop;       // this iteration has nothing to pop
+    uint32_t n_cand;
+    uint32_t n_leaves;
+    uint32_t n_nodes;
+    uint32_t live;
+    uint32_t depth;
+    uint32_t n_free;
+    uint32_t error;      // 1: the node table is full, 2: the histogram pool is
+    uint32_t pops;       // pops taken this tree
+};
+
+// After the root's find: the root a candidate (or a leaf), the node table's
+// first entry, every pool slot but the root's free.
+__global__ void __launch_bounds__(k_plan_thr)
+    leaf_loop_init_kernel(LeafLoop *st, LeafCand *cand, Node *leaves, uint32_t *free_slots,
+                          LeafOut const *out, TreeOut const *tp_, uint32_t n_root,
+                          uint32_t max_front, uint32_t max_depth)
+{
+    for (uint32_t k = threadIdx.x; k + 1 < max_front; k += k_plan_thr)
+    {
+        free_slots[k] = max_front - 1 - k; // popped from the top: slot 1 first
+    }
+    if (threadIdx.x != 0)
+    {
+        return;
+    }
+    TreeOut const t   = *tp_;
+    t.feature[0]      = k_leaf_flag;
+    t.left[0]         = 0;
+    t.right[0]        = 0;
+    t.split_bin[0]    = 0;
+    t.value[0]        = 0.0F;
+    t.gain[0]         = 0.0F;
+    t.cover[0]        = static_cast<float>(n_root);
+    t.default_left[0] = 0;
+    LeafCand const root{out->child[0], out->best[0], 0, 0};
+    bool const     ok = root.best.valid != 0 && max_depth > 0;
+    st->n_cand        = ok ? 1 : 0;
+    if (ok)
+    {
+        cand[0] = root;
+    }
+    else
+    {
+        leaves[0] = root.node;
+    }
+    st->n_leaves = ok ? 0 : 1;
+    st->n_nodes  = 1;
+    st->live     = 1;
+    st->depth    = 0;
+    st->n_free   = max_front - 1;
+    st->error    = 0;
+    st->pops     = 0;
+    st->noop     = 0;
+}
+
+// One pop: the best candidate off the heap, commit_split_node
+// (src/grower_impl.hpp:189-206) into the node table, a pool slot for the
+// smaller child, and the popped node's partition chunks (the setup of one
+// pop). With nothing to pop it sets the iteration's no-op flag and leaves
+// no chunks, so the rest of the iteration does nothing.
+constexpr uint32_t k_pop_thr = 256;
+
+__global__ void __launch_bounds__(k_pop_thr)
+    leaf_pop_kernel(LeafLoop *st, LeafCand *cand, uint32_t *free_slots, TreeOut const *tp_,
+                    float const *cuts, uint32_t const *cut_off, uint32_t const *sel,
+                    uint32_t max_leaves, uint32_t max_nodes, uint32_t max_depth, Ctl *ctl,
+                    Node *nodes, Best *best, Chunk *pchunks, uint32_t *pcr)
+{
+    __shared__ double   g_s[k_pop_thr / 32];
+    __shared__ uint32_t id_s[k_pop_thr / 32];
+    __shared__ uint32_t ix_s[k_pop_thr / 32];
+    __shared__ uint32_t go_s;
+    uint32_t const      n    = st->n_cand;
+    uint32_t const      lane = threadIdx.x & 31;
+    if (threadIdx.x == 0)
+    {
+        bool const go = st->error == 0 && n > 0 && (max_leaves == 0 || st->live < max_leaves);
+        go_s          = go ? 1 : 0;
+        st->noop      = go ? 0 : 1;
+        if (!go)
+        {
+            ctl->n_cur     = 0;
+            ctl->n_pchunks = 0;
+            ctl->n_build   = 0;
+            ctl->n_bchunks = 0;
+            pcr[0]         = 0;
+            pcr[1]         = 0;
+            st->pop.node.count = 0;
+        }
+    }
+    __syncthreads();
+    if (go_s == 0)
+    {
+        return;
+    }
+    // the heap's top: the largest gain, then the lowest node id
+    double   g  = -1.0;
+    uint32_t id = 0xFFFFFFFFu;
+    uint32_t ix = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += k_pop_thr)
+    {
+        double const   cg  = cand[i].best.gain;
+        uint32_t const cid = cand[i].node.id;
+        if (cg > g || (cg == g && cid < id))
+        {
+            g  = cg;
+            id = cid;
+            ix = i;
+        }
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        double const   og  = __shfl_xor_sync(0xFFFFFFFFu, g, o);
+        uint32_t const oid = __shfl_xor_sync(0xFFFFFFFFu, id, o);
+        uint32_t const oix = __shfl_xor_sync(0xFFFFFFFFu, ix, o);
+        if (og > g || (og == g && oid < id))
+        {
+            g  = og;
+            id = oid;
+            ix = oix;
+        }
+    }
+    if (lane == 0)
+    {
+        g_s[threadIdx.x >> 5]  = g;
+        id_s[threadIdx.x >> 5] = id;
+        ix_s[threadIdx.x >> 5] = ix;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (uint32_t w = 1; w < k_pop_thr / 32; ++w)
+        {
+            if (g_s[w] > g || (g_s[w] == g && id_s[w] < id))
+            {
+                g  = g_s[w];
+                id = id_s[w];
+                ix = ix_s[w];
+            }
+        }
+        LeafCand const c = cand[ix];
+        cand[ix]         = cand[n - 1];
+        st->n_cand       = n - 1;
+        uint32_t const lid = st->n_nodes;
+        uint32_t const rid = lid + 1;
+        if (rid >= max_nodes || st->n_free == 0)
+        {
+            st->error          = rid >= max_nodes ? 1 : 2;
+            st->noop           = 1;
+            ctl->n_cur         = 0;
+            ctl->n_pchunks     = 0;
+            ctl->n_build       = 0;
+            ctl->n_bchunks     = 0;
+            pcr[0]             = 0;
+            pcr[1]             = 0;
+            st->pop.node.count = 0;
+            go_s               = 0;
+        }
+        else
+        {
+            TreeOut const t = *tp_;
+            for (uint32_t k = lid; k <= rid; ++k)
+            {
+                t.feature[k]      = k_leaf_flag;
+                t.left[k]         = 0;
+                t.right[k]        = 0;
+                t.split_bin[k]    = 0;
+                t.value[k]        = 0.0F;
+                t.gain[k]         = 0.0F;
+                t.cover[k]        = 0.0F;
+                t.default_left[k] = 0;
+            }
+            uint32_t const f     = sel[c.best.feature];
+            uint32_t const nid   = c.node.id;
+            t.feature[nid]       = f;
+            t.value[nid]         = cuts[cut_off[f] + c.best.bin];
+            t.left[nid]          = lid;
+            t.right[nid]         = rid;
+            t.default_left[nid]  = static_cast<uint8_t>(c.best.dl);
+            t.gain[nid]          = static_cast<float>(c.best.gain);
+            t.split_bin[nid]     = c.best.bin;
+            st->n_nodes          = rid + 1;
+            uint32_t const small = free_slots[--st->n_free];
+            st->pop       = LeafPop{c.node, c.best, lid, rid, c.slot, small};
+            st->pop_depth = c.depth;
+            st->may_split = c.depth + 1 < max_depth ? 1 : 0;
+            st->pops += 1;
+            // the pop's setup: the node's partition chunks
+            uint32_t const nch = (c.node.count + k_part_rows - 1) / k_part_rows;
+            ctl->n_cur         = 1;
+            ctl->n_pchunks     = nch;
+            Node nd            = c.node;
+            nd.flags           = 1;
+            nodes[0]           = nd;
+            best[0]            = c.best;
+            pcr[0]             = 0;
+            pcr[1]             = nch;
+        }
+    }
+    __syncthreads();
+    if (go_s == 0)
+    {
+        return;
+    }
+    LeafPop const &p   = st->pop;
+    uint32_t const cnt = p.node.count;
+    uint32_t const nch = (cnt + k_part_rows - 1) / k_part_rows;
+    for (uint32_t c = threadIdx.x; c < nch; c += k_pop_thr)
+    {
+        uint32_t const b = c * k_part_rows;
+        pchunks[c]       = {0, p.node.start + b, min(k_part_rows, cnt - b), 0};
+    }
+}
+
+// The pop's outcome into the loop's state (commit_pop's demotion, or the two
+// children queued: queue_children, src/grower_impl.hpp:405-425), then whether
+// the loop goes on.
+__global__ void leaf_commit_kernel(LeafLoop *st, LeafCand *cand, Node *leaves,
+                                   uint32_t *free_slots, LeafOut const *out,
+                                   TreeOut const *tp_, uint32_t max_leaves, uint32_t max_pops,
+                                   cudaGraphConditionalHandle handle)
+{
+    if (st->noop == 0)
+    {
+        LeafPop const &p = st->pop;
+        TreeOut const  t = *tp_;
+        if (out->split == 0)
+        {
+            // the survivor holds the parent's rows and takes its id and
+            // bounds; the two children stay placeholders
+            t.gain[p.node.id]           = 0.0F;
+            leaves[st->n_leaves++]      = p.node;
+            free_slots[st->n_free++]    = p.small_slot;
+            free_slots[st->n_free++]    = p.parent_slot;
+        }
+        else
+        {
+            Node const     L  = out->child[0];
+            Node const     R  = out->child[1];
+            bool const     sl = out->small_left != 0;
+            uint32_t const d  = st->pop_depth + 1;
+            t.cover[p.left_id]  = static_cast<float>(L.gcount);
+            t.cover[p.right_id] = static_cast<float>(R.gcount);
+            st->live += 1;
+            st->depth = max(st->depth, d);
+            LeafCand const kids[2] = {{L, out->best[0], d, sl ? p.small_slot : p.parent_slot},
+                                      {R, out->best[1], d, sl ? p.parent_slot : p.small_slot}};
+            for (LeafCand const &k : kids)
+            {
+                if (k.best.valid != 0)
+                {
+                    cand[st->n_cand++] = k;
+                }
+                else
+                {
+                    leaves[st->n_leaves++]   = k.node;
+                    free_slots[st->n_free++] = k.slot;
+                }
+            }
+        }
+    }
+    // every pop either adds a leaf or retires a candidate, so at most
+    // 2 x max_leaves pops ever run; past max_pops the loop stops with an error
+    // rather than spin
+    if (st->pops >= max_pops && st->noop == 0)
+    {
+        st->error = 3;
+    }
+    bool const more = st->noop == 0 && st->error == 0 && st->n_cand > 0 &&
+                      (max_leaves == 0 || st->live < max_leaves);
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// The tree's epilogue: every remaining candidate is a leaf; the leaf list,
+// node count and depth go to the level plane's control block.
+__global__ void leaf_loop_end_kernel(LeafLoop *st, LeafCand const *cand, Node *leaves,
+                                     Node *nodes, Ctl *ctl)
+{
+    uint32_t const nl = st->n_leaves;
+    uint32_t const nc = st->n_cand;
+    for (uint32_t i = threadIdx.x; i < nl + nc; i += blockDim.x)
+    {
+        nodes[i] = i < nl ? leaves[i] : cand[i - nl].node;
+    }
+    if (threadIdx.x == 0)
+    {
+        ctl->n_cur    = nl + nc;
+        ctl->n_nodes  = st->n_nodes;
+        ctl->depth    = st->depth;
+        ctl->n_leaves = 0;
+    }
+}
+
+__global__ void leaf_set_tree_kernel(TreeOut *dst, TreeOut t, LeafLoop *st, uint32_t root_may)
+{
+    *dst          = t;
+    st->root_may  = root_may;
 }
 
 __global__ void tree_counter_kernel(uint32_t *tree_no)
@@ -3546,9 +3851,14 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     nbound_   = dalloc<double2>(std::max<uint32_t>(max_nodes_, k_walk_nodes), s);
     if (cfg_.leaf)
     {
-        lout_    = dalloc<LeafOut>(1, s);
-        slot_of_ = dalloc<uint32_t>(2, s);
-        BB_CHECK(cudaMallocHost(&lout_h_, sizeof(LeafOut)));
+        lout_      = dalloc<LeafOut>(1, s);
+        slot_of_   = dalloc<uint32_t>(2, s);
+        loop_      = dalloc<LeafLoop>(1, s);
+        cand_heap_ = dalloc<LeafCand>(max_front_ + 2, s);
+        leaves_    = dalloc<Node>(max_front_ + 2, s);
+        free_      = dalloc<uint32_t>(max_front_ + 2, s);
+        tree_dev_  = dalloc<TreeOut>(1, s);
+        BB_CHECK(cudaMallocHost(&lout_h_, sizeof(LeafLoop)));
     }
     nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
     dtree_    = dalloc<uint32_t>(1, s);
@@ -3767,6 +4077,19 @@ Grower::~Grower()
     {
         cudaFreeAsync(lout_, stream_);
         cudaFreeAsync(slot_of_, stream_);
+        cudaFreeAsync(loop_, stream_);
+        cudaFreeAsync(cand_heap_, stream_);
+        cudaFreeAsync(leaves_, stream_);
+        cudaFreeAsync(free_, stream_);
+        cudaFreeAsync(tree_dev_, stream_);
+    }
+    if (loop_x_ != nullptr)
+    {
+        cudaGraphExecDestroy(loop_x_);
+    }
+    if (loop_g_ != nullptr)
+    {
+        cudaGraphDestroy(loop_g_);
     }
     cudaStreamSynchronize(stream_);
     if (lout_h_ != nullptr)
@@ -4363,22 +4686,6 @@ namespace
 
 // A leaf awaiting expansion (Candidate, src/step/primitives.hpp:440-450): its
 // node, its best split, its depth and the pool slot holding its histograms.
-struct HeapEntry
-{
-    Node     node;
-    Best     best;
-    uint32_t depth;
-    uint32_t slot;
-};
-
-__global__ void leaf_final_ctl_kernel(Ctl *ctl, uint32_t n_leaves, uint32_t n_nodes,
-                                      uint32_t depth)
-{
-    ctl->n_cur    = n_leaves;
-    ctl->n_nodes  = n_nodes;
-    ctl->depth    = depth;
-    ctl->n_leaves = 0;
-}
 
 } // namespace
 
@@ -4394,14 +4701,20 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     TreeParams const &tp        = cfg_.tp;
     size_t const      find_smem = max_nb_ * (sizeof(double2) + (sizeof(unsigned long long) * cw_));
     auto             *lout      = static_cast<LeafOut *>(lout_);
-    auto             *lh        = static_cast<LeafOut *>(lout_h_);
+    auto             *st        = static_cast<LeafLoop *>(loop_);
+    auto             *cand      = static_cast<LeafCand *>(cand_heap_);
+    auto             *tdev      = static_cast<TreeOut *>(tree_dev_);
+    LeafPop const    *pp        = &st->pop;
     void             *pool      = hist_[0];
+    uint32_t          launches  = 0;
     BB_CHECK(cudaMemcpyAsync(rows_[0], root_rows, size_t{n_root} * 4, cudaMemcpyDeviceToDevice,
                              s));
+    leaf_set_tree_kernel<<<1, 1, 0, s>>>(tdev, t, st, tp.max_depth > 0 ? 1u : 0u);
+    BB_LAUNCH("leaf_set_tree_kernel");
     root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
                                               build_, t, crows_, n_root, nullptr);
     BB_LAUNCH("root_setup_kernel");
-    n_launch_ += 1;
+    launches += 2;
     build(rows_[0], n_sel_, 0);
     if (quant_)
     {
@@ -4414,8 +4727,10 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                                             sel_nb_);
     }
     BB_LAUNCH("root_totals_kernel");
-    n_launch_ += 1;
-    auto find = [&](Node const *nodes, uint32_t const *slot_of, bool may_split)
+    launches += 1;
+    // each node's best split, then the pair's outcome (the children and their
+    // bests) into lout; may_split: the depth cap's verdict, on the device
+    auto find = [&](Node const *nodes, uint32_t const *slot_of, uint32_t const *may_split)
     {
         dim3 const fgrid(2, n_sel_);
         if (quant_)
@@ -4432,217 +4747,162 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
                 tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
         }
         BB_LAUNCH("find_kernel");
-        leaf_best_kernel<<<2, k_best_thr, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout,
-                                                  may_split ? 1 : 0);
+        leaf_best_kernel<<<2, k_best_thr, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split);
         BB_LAUNCH("leaf_best_kernel");
-        n_launch_ += 2;
-        BB_CHECK(cudaMemcpyAsync(lh, lout, sizeof(LeafOut), cudaMemcpyDeviceToHost, s));
-        BB_CHECK(cudaStreamSynchronize(s));
     };
-    find(nodes_[0], nullptr, tp.max_depth > 0);
+    find(nodes_[0], nullptr, &st->root_may);
+    leaf_loop_init_kernel<<<1, k_plan_thr, 0, s>>>(st, cand, leaves_, free_, lout, tdev, n_root,
+                                                   max_front_, tp.max_depth);
+    BB_LAUNCH("leaf_loop_init_kernel");
+    launches += 3;
 
-    // the tree as the host assembles it (DenseTree nodes, gains, covers)
-    std::vector<uint32_t> feat{k_leaf_flag};
-    std::vector<uint32_t> left{0};
-    std::vector<uint32_t> right{0};
-    std::vector<uint32_t> sbin{0};
-    std::vector<float>    value{0.0F};
-    std::vector<float>    gain{0.0F};
-    std::vector<float>    cover{static_cast<float>(n_root)};
-    std::vector<uint8_t>  dl{0};
-    auto                  push_leaf = [&]
+    // one pop as a fixed sequence of launches, repeated by the loop graph's
+    // WHILE node until leaf_commit_kernel says the heap is done; captured
+    // once (the loop's buffers and the tree's device record do not move)
+    if (loop_x_ == nullptr)
     {
-        feat.push_back(k_leaf_flag);
-        left.push_back(0);
-        right.push_back(0);
-        sbin.push_back(0);
-        value.push_back(0.0F);
-        gain.push_back(0.0F);
-        cover.push_back(0.0F);
-        dl.push_back(0);
-    };
-    std::vector<uint32_t> free_slots;
-    for (uint32_t k = max_front_; k-- > 1;)
-    {
-        free_slots.push_back(k); // slot 0 holds the root
-    }
-    auto gain_less = [](HeapEntry const &a, HeapEntry const &b)
-    {
-        if (a.best.gain != b.best.gain)
+        Profile *const saved = prof_;
+        prof_                = nullptr; // no per-phase events inside the loop graph
+        BB_CHECK(cudaGraphCreate(&loop_g_, 0));
+        cudaGraphConditionalHandle handle{};
+        BB_CHECK(cudaGraphConditionalHandleCreate(&handle, loop_g_, 1,
+                                                  cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type               = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type   = cudaGraphCondTypeWhile;
+        cp.conditional.size   = 1;
+        cudaGraphNode_t cnode{};
+        BB_CHECK(cudaGraphAddNode(&cnode, loop_g_, nullptr, 0, &cp));
+        cudaGraph_t const body = cp.conditional.phGraph_out[0];
+        BB_CHECK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        uint32_t const n0 = n_launch_;
+        try
         {
-            return a.best.gain < b.best.gain;
-        }
-        return a.node.id > b.node.id;
-    };
-    std::vector<HeapEntry> heap;
-    std::vector<HeapEntry> pending;
-    std::vector<Node>      leaves; // demoted splits, as they happen
-    HeapEntry const        root{lh->child[0], lh->best[0], 0, 0};
-    if (root.best.valid != 0 && tp.max_depth > 0)
-    {
-        heap.push_back(root);
-    }
-    else
-    {
-        pending.push_back(root);
-    }
-    uint32_t live  = 1;
-    uint32_t depth = 0;
-    while (!heap.empty() && (tp.max_leaves == 0 || live < tp.max_leaves))
-    {
-        std::pop_heap(heap.begin(), heap.end(), gain_less);
-        HeapEntry const c = heap.back();
-        heap.pop_back();
-        // commit_split_node (src/grower_impl.hpp:189-206)
-        uint32_t const id  = c.node.id;
-        uint32_t const lid = static_cast<uint32_t>(feat.size());
-        uint32_t const rid = lid + 1;
-        if (rid >= max_nodes_)
-        {
-            throw ConfigError("grower: leafwise tree outgrew its node table");
-        }
-        push_leaf();
-        push_leaf();
-        uint32_t const f = sel_h_[c.best.feature];
-        feat[id]         = f;
-        value[id]        = plane_.h_cuts[plane_.h_cut_off[f] + c.best.bin];
-        left[id]         = lid;
-        right[id]        = rid;
-        dl[id]           = static_cast<uint8_t>(c.best.dl);
-        gain[id]         = static_cast<float>(c.best.gain);
-        sbin[id]         = c.best.bin;
-        if (free_slots.empty())
-        {
-            throw ConfigError("grower: leafwise histogram pool exhausted");
-        }
-        uint32_t const small = free_slots.back();
-        free_slots.pop_back();
-        LeafPop const p{c.node, c.best, lid, rid, c.slot, small};
-        leaf_setup_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], best_, pchunks_, pcr_, p);
-        BB_LAUNCH("leaf_setup_kernel");
-        if (plane_.u8)
-        {
-            pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
-                ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
-                sel_nb_, pleft_, dirs_);
-        }
-        else
-        {
-            pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
-                ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
-                sel_nb_, pleft_, dirs_);
-        }
-        BB_LAUNCH("pcount_kernel");
-        leaf_plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pchunks_, pleft_, prbase_, nleft_, dst_,
-                                                  build_, brange_, bbase_, bchunks_, bpair_,
-                                                  nodes_[0], nodes_[1], slot_of_, lout, crows_,
-                                                  p);
-        BB_LAUNCH("leaf_plan_kernel");
-        pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
-            ctl_, pchunks_, nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0], rows_[1],
-            dirs_, static_cast<unsigned long long *>(pool), build_, total_cells_ * cw_,
-            quant_ ? total_cells_ * cw_ : 0);
-        BB_LAUNCH("pscatter_kernel");
-        n_launch_ += 4; // setup, count, plan, scatter
-        build(rows_[1], n_sel_, 0, true);
-        uint32_t const cgrid = std::max(1u, std::min(ceil_div(c.node.count, 256), 148u * 8u));
-        leaf_copyback_kernel<<<cgrid, 256, 0, s>>>(lout, rows_[1], rows_[0], c.node.start,
-                                                   c.node.count);
-        BB_LAUNCH("leaf_copyback_kernel");
-        uint32_t const sgrid =
-            std::max(1u, std::min(ceil_div(total_cells_ * cw_, 256), 148u * 8u));
-        if (quant_)
-        {
-            leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_ * cw_,
-                                                        total_cells_ * cw_);
-            leaf_totals_kernel<true><<<1, 64, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
-                                                      total_cells_, sel_, sel_nb_, mono_, n_mono_,
-                                                      tp, qscale_, p, cw_, fgroups_);
-        }
-        else
-        {
-            leaf_sub_kernel<false><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
-                                                         total_cells_);
-            leaf_totals_kernel<false><<<1, 64, 0, s>>>(ctl_, lout, nodes_[1], slot_of_, pool,
-                                                       total_cells_, sel_, sel_nb_, mono_,
-                                                       n_mono_, tp, qscale_, p, 1, fgroups_);
-        }
-        BB_LAUNCH("leaf_totals_kernel");
-        n_launch_ += 3; // copy-back, subtraction, totals
-        find(nodes_[1], slot_of_, c.depth + 1 < tp.max_depth);
-        if (lh->split == 0)
-        {
-            // commit_pop's demotion: the survivor holds the parent's rows and
-            // takes its id and bounds; the two children stay placeholders
-            gain[id] = 0.0F;
-            leaves.push_back(c.node);
-            free_slots.push_back(small);
-            free_slots.push_back(c.slot);
-            continue;
-        }
-        Node const     L  = lh->child[0];
-        Node const     R  = lh->child[1];
-        bool const     sl = lh->small_left != 0;
-        cover[lid]        = static_cast<float>(L.gcount);
-        cover[rid]        = static_cast<float>(R.gcount);
-        ++live;
-        depth = std::max(depth, c.depth + 1);
-        HeapEntry const kids[2] = {{L, lh->best[0], c.depth + 1, sl ? small : c.slot},
-                                   {R, lh->best[1], c.depth + 1, sl ? c.slot : small}};
-        for (HeapEntry const &k : kids)
-        {
-            // queue_children (src/grower_impl.hpp:405-425)
-            if (k.best.valid != 0)
+            leaf_pop_kernel<<<1, k_pop_thr, 0, s>>>(
+                st, cand, free_, tdev, plane_.cuts, plane_.cut_off, sel_, tp.max_leaves,
+                max_nodes_, tp.max_depth, ctl_, nodes_[0], best_, pchunks_, pcr_);
+            BB_LAUNCH("leaf_pop_kernel");
+            if (plane_.u8)
             {
-                heap.push_back(k);
-                std::push_heap(heap.begin(), heap.end(), gain_less);
+                pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
+                    ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                    sel_nb_, pleft_, dirs_);
             }
             else
             {
-                pending.push_back(k);
-                free_slots.push_back(k.slot);
+                pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
+                    ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                    sel_nb_, pleft_, dirs_);
             }
+            BB_LAUNCH("pcount_kernel");
+            leaf_plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pchunks_, pleft_, prbase_, nleft_,
+                                                      dst_, build_, brange_, bbase_, bchunks_,
+                                                      bpair_, nodes_[0], nodes_[1], slot_of_, lout,
+                                                      crows_, pp);
+            BB_LAUNCH("leaf_plan_kernel");
+            pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
+                ctl_, pchunks_, nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0],
+                rows_[1], dirs_, static_cast<unsigned long long *>(pool), build_,
+                total_cells_ * cw_, quant_ ? total_cells_ * cw_ : 0);
+            BB_LAUNCH("pscatter_kernel");
+            n_launch_ = 0;
+            build(rows_[1], n_sel_, 0, true);
+            uint32_t const nb = n_launch_;
+            leaf_copyback_kernel<<<148u * 8u, 256, 0, s>>>(lout, rows_[1], rows_[0], pp);
+            BB_LAUNCH("leaf_copyback_kernel");
+            uint32_t const sgrid =
+                std::max(1u, std::min(ceil_div(total_cells_ * cw_, 256), 148u * 8u));
+            if (quant_)
+            {
+                leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool,
+                                                            total_cells_ * cw_,
+                                                            total_cells_ * cw_);
+                leaf_totals_kernel<true><<<1, 64, 0, s>>>(
+                    ctl_, lout, nodes_[1], slot_of_, pool, total_cells_, sel_, sel_nb_, mono_,
+                    n_mono_, tp, qscale_, pp, cw_, fgroups_);
+            }
+            else
+            {
+                leaf_sub_kernel<false><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
+                                                             total_cells_);
+                leaf_totals_kernel<false><<<1, 64, 0, s>>>(
+                    ctl_, lout, nodes_[1], slot_of_, pool, total_cells_, sel_, sel_nb_, mono_,
+                    n_mono_, tp, qscale_, pp, 1, fgroups_);
+            }
+            BB_LAUNCH("leaf_totals_kernel");
+            find(nodes_[1], slot_of_, &st->may_split);
+            leaf_commit_kernel<<<1, 1, 0, s>>>(st, cand, leaves_, free_, lout, tdev,
+                                               tp.max_leaves, 4 * max_front_ + 8, handle);
+            BB_LAUNCH("leaf_commit_kernel");
+            // pop, count, plan, scatter, the build, copy-back, subtraction,
+            // totals, find, best, commit
+            body_launches_ = 4 + nb + 3 + 2 + 1;
         }
+        catch (...)
+        {
+            cudaGraph_t dummy{};
+            cudaStreamEndCapture(s, &dummy);
+            prof_     = saved;
+            n_launch_ = n0;
+            throw;
+        }
+        cudaGraph_t captured{};
+        BB_CHECK(cudaStreamEndCapture(s, &captured));
+        BB_CHECK(cudaGraphInstantiate(&loop_x_, loop_g_, 0));
+        prof_     = saved;
+        n_launch_ = n0;
     }
-    // the tree epilogue: every remaining candidate and pending node is a leaf
-    for (HeapEntry const &h : heap)
+    if (prof_ != nullptr)
     {
-        leaves.push_back(h.node);
+        phase_begin();
     }
-    for (HeapEntry const &h : pending)
+    BB_CHECK(cudaGraphLaunch(loop_x_, s));
+    if (prof_ != nullptr)
     {
-        leaves.push_back(h.node);
+        phase_end(prof_->other_ms);
     }
-    uint32_t const n_nodes = static_cast<uint32_t>(feat.size());
-    BB_CHECK(cudaMemcpyAsync(t.feature, feat.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.value, value.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.left, left.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.right, right.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.default_left, dl.data(), n_nodes, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.gain, gain.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.cover, cover.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(t.split_bin, sbin.data(), n_nodes * 4, cudaMemcpyHostToDevice, s));
-    BB_CHECK(cudaMemcpyAsync(nodes_[0], leaves.data(), leaves.size() * sizeof(Node),
-                             cudaMemcpyHostToDevice, s));
-    leaf_final_ctl_kernel<<<1, 1, 0, s>>>(ctl_, static_cast<uint32_t>(leaves.size()), n_nodes,
-                                          depth);
-    BB_LAUNCH("leaf_final_ctl_kernel");
-    n_launch_ += 2; // with final_kernel below
+    leaf_loop_end_kernel<<<1, k_plan_thr, 0, s>>>(st, cand, leaves_, nodes_[0], ctl_);
+    BB_LAUNCH("leaf_loop_end_kernel");
+    launches += 1;
     // write_leaf for every leaf, then (quantised) the FP64 renewal, then the
     // rows' leaf ids and score updates from the leaves' segments
     final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], tp, t, pchunks_, pcr_, nbound_);
     BB_LAUNCH("final_kernel");
+    launches += 1;
     nodes_cur_ = nodes_[0];
     rows_cur_  = rows_[0];
+    uint32_t const before = n_launch_;
     leaf_values(t, true);
+    launches += n_launch_ - before;
     stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[0], rows_[0], t,
                                                     leaf_id, scores, lr);
     BB_LAUNCH("stamp_kernel");
     tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
     BB_LAUNCH("tree_counter_kernel");
-    n_launch_ += 2; // stamp, counter
+    launches += 2;
+    // the loop's verdict: a full node table or pool is the reference's
+    // capacity refusal
+    auto *lh = static_cast<LeafLoop *>(lout_h_);
+    BB_CHECK(cudaMemcpyAsync(lh, st, sizeof(LeafLoop), cudaMemcpyDeviceToHost, s));
+    BB_CHECK(cudaStreamSynchronize(s));
+    if (lh->error == 1)
+    {
+        throw ConfigError("grower: leafwise tree outgrew its node table");
+    }
+    if (lh->error == 2)
+    {
+        throw ConfigError("grower: leafwise histogram pool exhausted");
+    }
+    if (lh->error == 3)
+    {
+        throw std::runtime_error("grower: leafwise pop loop exceeded its pop bound");
+    }
+    // every pop ran the body, and the last iteration found nothing to pop
+    // (or stopped at the budget) -- one graph launch on the host's side
+    n_launch_ += launches + (lh->pops + (lh->noop != 0 ? 1 : 0)) * body_launches_;
     launches_ = n_launch_;
-    BB_CHECK(cudaStreamSynchronize(s)); // the host tables above are read until here
     ++tree_no_;
 }
 

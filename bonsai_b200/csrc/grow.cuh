@@ -324,8 +324,19 @@ class Grower
     double2  *nbound_   = nullptr; // per tree node: monotone bounds (lo, hi)
     // leafwise
     void     *lout_     = nullptr; // the pop's results (device)
-    void     *lout_h_   = nullptr; // ... read back (pinned host)
+    void     *lout_h_   = nullptr; // the loop's state read back after a tree (pinned host)
     uint32_t *slot_of_  = nullptr; // the children's pool slots
+    // the device-side pop loop: its state (the candidate heap, free pool
+    // slots, the leaves, the node count), the tree being grown, and the
+    // loop's graph (a conditional WHILE node over one pop's launches)
+    void            *loop_      = nullptr;
+    void            *cand_heap_ = nullptr;
+    Node            *leaves_    = nullptr;
+    uint32_t        *free_      = nullptr;
+    void            *tree_dev_  = nullptr;
+    cudaGraph_t      loop_g_    = nullptr;
+    cudaGraphExec_t  loop_x_    = nullptr;
+    uint32_t         body_launches_ = 0;
     uint32_t  crows_    = 0;       // rows per histogram-build chunk
     bool      quant_    = false;
     uint32_t *dtree_    = nullptr; // device tree counter (the rounding stream)
