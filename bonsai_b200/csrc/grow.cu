@@ -2886,6 +2886,56 @@ __global__ void __launch_bounds__(k_threads)
 // Exact integer totals of the smaller children when no histogram is built
 // for them (the last level): per build chunk, the sums of its rows' codes,
 // added into the chunk's build slot.
+// The last level of a walked quantised tree: each built (smaller) child's
+// exact integer totals straight from its parent's cells of the split
+// feature -- the bins routes_left sends left (b <= split bin, and the missing
+// bin when it defaults left), or the parent's totals minus them -- so the
+// level needs neither the row scatter nor a gather of the children's codes.
+// The parent's cells are the fit's (a sharded fit reduced them already).
+// A warp per built child.
+__global__ void qsplit_totals_kernel(Ctl const *ctl, uint32_t const *bpair, Node const *cur,
+                                     Best const *best, unsigned long long const *hist_cur,
+                                     uint32_t total_cells, uint32_t const *cell_off,
+                                     uint32_t const *sel_nb, uint32_t cw, int64_t *btot)
+{
+    uint32_t const k = (blockIdx.x * (blockDim.x / 32)) + (threadIdx.x >> 5);
+    if (k >= ctl->n_splits)
+    {
+        return;
+    }
+    uint32_t const i       = bpair[3 * k];
+    bool const     left_sm = (bpair[(3 * k) + 1] & 1u) == 0;
+    Best const     b       = best[i];
+    uint32_t const nb      = sel_nb[b.feature];
+    uint32_t const last    = nb - 1;
+    auto const    *cells   = hist_cur + (static_cast<uint64_t>(i) * total_cells * cw) +
+                      (static_cast<uint64_t>(cell_off[b.feature]) * cw);
+    int64_t lg = 0;
+    int64_t lh = 0;
+    for (uint32_t x = threadIdx.x & 31; x < nb; x += 32)
+    {
+        if (x == last ? b.dl != 0 : x <= b.bin)
+        {
+            int64_t cg, ch;
+            qcell(cells, x, cw, cg, ch);
+            lg += cg;
+            lh += ch;
+        }
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1)
+    {
+        lg += __shfl_xor_sync(0xFFFFFFFFu, lg, o);
+        lh += __shfl_xor_sync(0xFFFFFFFFu, lh, o);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        Node const nd  = cur[i];
+        btot[2 * k]     = left_sm ? lg : nd.qg - lg;
+        btot[(2 * k) + 1] = left_sm ? lh : nd.qh - lh;
+    }
+}
+
 __global__ void __launch_bounds__(k_threads)
     qbuilt_totals_kernel(Ctl const *ctl, Chunk const *bchunks, uint32_t const *rows,
                          uint16_t const *__restrict__ qgh, uint32_t const *__restrict__ qgh16,
@@ -4424,6 +4474,32 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     bool const     last     = (L + 1) == cfg_.tp.max_depth;
     uint32_t const nfb      = last ? 1 : n_sel_;
     uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] * cw_ : 0;
+    if (quant_ && last && walk_)
+    {
+        // a walked tree's last level: the leaves' rows are never listed (the
+        // walk routes every row) and their exact totals come from the
+        // parents' split cells
+        if (prof_ != nullptr)
+        {
+            phase_end(prof_->partition_ms);
+        }
+        phase_begin();
+        qsplit_totals_kernel<<<ceil_div(max_front_, 8), 256, 0, s>>>(
+            ctl_, bpair_, nodes_[cur], best_, static_cast<unsigned long long const *>(hist_[cur]),
+            total_cells_, cell_off_, sel_nb_, cw_, btot_);
+        BB_LAUNCH("qsplit_totals_kernel");
+        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
+            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
+            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
+            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
+        BB_LAUNCH("qsubtract_totals_kernel");
+        n_launch_ += 6; // count, plan2, the two totals kernels (+ find, plan)
+        if (prof_ != nullptr)
+        {
+            phase_end(prof_->other_ms);
+        }
+        return;
+    }
     pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
         ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
         dirs_, static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_, n_zcells);
