@@ -597,6 +597,24 @@ def many_main(args):
     launches = sum(int(b.profile_round()["launches"]) for b in boosters) * MANY_ROUNDS
     for b in boosters:
         b.close()
+    # the same rounds as one graph launch per round for the whole batch
+    # (bb_batch: every booster's round graph a child of one parent graph)
+    one_launch = None
+    if not args.no_batch:
+        planes, boosters = fits()
+        group = bb.BoosterBatch(boosters)
+        group.update(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        group.update(MANY_ROUNDS - 1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        one_launch = {"s_per_100_rounds": wall * MANY_ROUNDS / (MANY_ROUNDS - 1),
+                      "device_ms_per_round": group.last_ms / (MANY_ROUNDS - 1),
+                      "graph_launches_per_round": 1}
+        group.close()
+        for b in boosters:
+            b.close()
     planes, boosters = fits()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -614,6 +632,7 @@ def many_main(args):
             "config": {"workload": MANY_WORKLOAD, "datasets": len(sets), "rows": rows,
                        "hist_mode": args.mode, "timing": "wall clock, synchronized"},
             "one_at_a_time_s": serial, "concurrency_speedup": serial / batch,
+            "one_graph_launch": one_launch,
             "e2e": {"value": batch, "unit": "s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "gpu_launches": launches, "clocks": clk.summary()}
@@ -763,6 +782,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default histogram launch shape (no autotuning)")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="many: skip the one-launch batch (bb_batch) leg")
     ap.add_argument("--eval-rows", type=int, default=1_000_000,
                     help="fit: validation rows for the AUC and logloss (0 skips)")
     ap.add_argument("--workload", default="fit",

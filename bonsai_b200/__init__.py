@@ -28,7 +28,7 @@ __all__ = [
     "BonsaiError", "ConfigError", "TrainParams", "Plane", "Booster", "Tree",
     "grow_tree", "populate", "predict", "PredictPlan", "ShapPlan", "predict_classes", "pred_contribs", "pred_contribs_classes", "oblivious_tables", "fit_cuts",
     "Comm", "early_stop_round", "fit_early_stopping", "shard_range", "init_score", "label_sum", "init_score_from_sum", "cuts_from_sample", "sample_rows", "fit_cuts_device",
-    "available", "LEAF", "tune",
+    "available", "LEAF", "tune", "BoosterBatch",
 ]
 
 LEAF = 0xFFFFFFFF
@@ -583,6 +583,43 @@ class Booster:
             self.close()
         except Exception:
             pass  # interpreter shutdown: the library may be gone already
+
+
+class BoosterBatch:
+    """Many boosters, one graph launch per round (bb_batch_*): every
+    booster's round graph is a child of one parent graph, so a round of the
+    whole batch is one launch and the boosters run concurrently. Boosters
+    must use CUDA graphs, without row or feature sampling; they must outlive
+    the batch. Their trees and scores read as usual afterwards."""
+
+    def __init__(self, boosters):
+        self.boosters = list(boosters)
+        arr = (C.c_void_p * len(self.boosters))(*[b.h for b in self.boosters])
+        h = C.c_void_p()
+        check(lib().bb_batch_create(arr, len(self.boosters), C.byref(h)))
+        self.h = h.value
+
+    def update(self, n_rounds: int = 1, sync: bool = True):
+        check(lib().bb_batch_update(self.h, n_rounds))
+        if sync:
+            check(lib().bb_batch_sync(self.h))
+
+    @property
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        check(lib().bb_batch_last_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def early_stop_round(losses, patience: int):

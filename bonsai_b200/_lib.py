@@ -78,6 +78,13 @@ def lib() -> C.CDLL:
         L.bb_booster_create.argtypes = [vp, vp, vp, C.POINTER(TrainCfg), C.c_uint32,
                                         C.POINTER(vp)]
         L.bb_booster_update.argtypes = [vp, C.c_uint32]
+        L.bb_booster_set_rows.argtypes = [vp, vp, C.c_uint64]
+        L.bb_batch_create.argtypes = [vp, C.c_uint32, C.POINTER(vp)]
+        L.bb_batch_update.argtypes = [vp, C.c_uint32]
+        L.bb_batch_sync.argtypes = [vp]
+        L.bb_batch_last_ms.argtypes = [vp, C.POINTER(C.c_float)]
+        L.bb_batch_destroy.argtypes = [vp]
+        L.bb_batch_destroy.restype = None
         L.bb_booster_sync.argtypes = [vp]
         L.bb_booster_set_weights.argtypes = [vp, vp]
         L.bb_booster_n_trees.argtypes = [vp, C.POINTER(C.c_uint32)]

@@ -1607,6 +1607,160 @@ extern "C"
             });
     }
 
+    // ---- many boosters, one graph launch per round -----------------------
+    // Every booster's round graph becomes a child node of one parent graph
+    // with no edges between them, so a round of the whole batch is one
+    // cudaGraphLaunch and the boosters' kernels run concurrently.
+    struct bb_batch_impl
+    {
+        std::vector<bb_booster *> boosters;
+        cudaGraphExec_t           exec = nullptr;
+        cudaStream_t              stream{};
+        cudaEvent_t               ev0{}, ev1{};
+        std::vector<cudaEvent_t>  ready;
+    };
+
+    int bb_batch_create(bb_booster *const *boosters, uint32_t n, bb_batch **out)
+    {
+        return guarded(
+            [&]
+            {
+                need(boosters != nullptr && out != nullptr && n > 0,
+                     "bb_batch_create: null argument");
+                auto        bt = std::make_unique<bb_batch_impl>();
+                cudaGraph_t parent{};
+                BB_CHECK(cudaGraphCreate(&parent, 0));
+                try
+                {
+                    for (uint32_t i = 0; i < n; ++i)
+                    {
+                        bb_booster *b = boosters[i];
+                        need(b != nullptr, "bb_batch_create: null booster");
+                        if (!b->use_graph || b->sampler != nullptr || b->feat_k > 0 ||
+                            b->sharded || b->truncated)
+                        {
+                            throw ConfigError(
+                                "bb_batch_create: a batch takes graph-captured boosters without "
+                                "row or feature sampling, unsharded and not truncated (a "
+                                "leafwise round is not captured)");
+                        }
+                        cudaGraph_t g{};
+                        BB_CHECK(cudaStreamBeginCapture(b->stream,
+                                                        cudaStreamCaptureModeThreadLocal));
+                        try
+                        {
+                            b->round_body();
+                        }
+                        catch (...)
+                        {
+                            cudaStreamEndCapture(b->stream, &g);
+                            throw;
+                        }
+                        BB_CHECK(cudaStreamEndCapture(b->stream, &g));
+                        cudaGraphNode_t node{};
+                        cudaError_t const e = cudaGraphAddChildGraphNode(&node, parent, nullptr,
+                                                                         0, g);
+                        cudaGraphDestroy(g);
+                        check(e, "cudaGraphAddChildGraphNode");
+                        bt->boosters.push_back(b);
+                        cudaEvent_t ev{};
+                        BB_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                        bt->ready.push_back(ev);
+                    }
+                    BB_CHECK(cudaGraphInstantiate(&bt->exec, parent, 0));
+                }
+                catch (...)
+                {
+                    cudaGraphDestroy(parent);
+                    for (cudaEvent_t ev : bt->ready)
+                    {
+                        cudaEventDestroy(ev);
+                    }
+                    throw;
+                }
+                BB_CHECK(cudaGraphDestroy(parent));
+                BB_CHECK(cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking));
+                BB_CHECK(cudaEventCreate(&bt->ev0));
+                BB_CHECK(cudaEventCreate(&bt->ev1));
+                *out = reinterpret_cast<bb_batch *>(bt.release());
+            });
+    }
+
+    int bb_batch_update(bb_batch *batch, uint32_t n_rounds)
+    {
+        return guarded(
+            [&]
+            {
+                need(batch != nullptr, "bb_batch_update: null batch");
+                auto *bt = reinterpret_cast<bb_batch_impl *>(batch);
+                for (bb_booster *b : bt->boosters)
+                {
+                    need(b->n_trees + (n_rounds * b->n_classes) <= b->trees.n,
+                         "bb_batch_update: a booster's tree capacity");
+                    need(!b->truncated, "bb_batch_update: a booster was truncated");
+                }
+                // the batch runs after every booster's queued work ...
+                for (size_t i = 0; i < bt->boosters.size(); ++i)
+                {
+                    BB_CHECK(cudaEventRecord(bt->ready[i], bt->boosters[i]->stream));
+                    BB_CHECK(cudaStreamWaitEvent(bt->stream, bt->ready[i], 0));
+                }
+                BB_CHECK(cudaEventRecord(bt->ev0, bt->stream));
+                for (uint32_t r = 0; r < n_rounds; ++r)
+                {
+                    BB_CHECK(cudaGraphLaunch(bt->exec, bt->stream));
+                }
+                BB_CHECK(cudaEventRecord(bt->ev1, bt->stream));
+                // ... and before anything later on each booster's stream
+                for (bb_booster *b : bt->boosters)
+                {
+                    BB_CHECK(cudaStreamWaitEvent(b->stream, bt->ev1, 0));
+                    b->n_trees += n_rounds * b->n_classes;
+                }
+            });
+    }
+
+    int bb_batch_sync(bb_batch *batch)
+    {
+        return guarded(
+            [&]
+            {
+                need(batch != nullptr, "bb_batch_sync: null batch");
+                BB_CHECK(cudaStreamSynchronize(reinterpret_cast<bb_batch_impl *>(batch)->stream));
+            });
+    }
+
+    int bb_batch_last_ms(bb_batch const *batch, float *ms)
+    {
+        return guarded(
+            [&]
+            {
+                need(batch != nullptr && ms != nullptr, "bb_batch_last_ms: null argument");
+                auto const *bt = reinterpret_cast<bb_batch_impl const *>(batch);
+                BB_CHECK(cudaEventSynchronize(bt->ev1));
+                BB_CHECK(cudaEventElapsedTime(ms, bt->ev0, bt->ev1));
+            });
+    }
+
+    void bb_batch_destroy(bb_batch *batch)
+    {
+        if (batch == nullptr)
+        {
+            return;
+        }
+        auto *bt = reinterpret_cast<bb_batch_impl *>(batch);
+        cudaStreamSynchronize(bt->stream);
+        cudaGraphExecDestroy(bt->exec);
+        for (cudaEvent_t ev : bt->ready)
+        {
+            cudaEventDestroy(ev);
+        }
+        cudaEventDestroy(bt->ev0);
+        cudaEventDestroy(bt->ev1);
+        cudaStreamDestroy(bt->stream);
+        delete bt;
+    }
+
     int bb_booster_set_weights(bb_booster *b, float const *weights)
     {
         return guarded(

@@ -2497,11 +2497,12 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 // Persistent: a grid of up to k_qctas CTAs per tile (one per SM; fewer for a
 // small dataset, so several fits share the GPU), each walking a
 // contiguous range of the level's chunks (node-ordered), so no wave tail.
-// The gathers are software-pipelined: while a chunk's rows are added, every
-// thread's cp.async copies of the next chunk's 32-byte tiles are in flight
-// into its own slots of a double-buffered staging area (so no barrier guards
-// them), with the next chunk's gradient codes and the row ids two chunks
-// ahead loaded into registers. The shared
+// The gathers are software-pipelined through registers: while a chunk's rows
+// are added, the thread's loads of the next chunk's row ids, gradient codes
+// and 32-byte tiles (two 16-byte non-coherent loads per row) are in flight,
+// the loop unrolled by two so the prefetched registers are never moved (a
+// move would wait for its load); with no shared staging the load/store path
+// carries only the reductions. The shared
 // histogram flushes -- one packed 64-bit global add per touched cell,
 // gradient in the high word (two's complement), hessian in the low word --
 // only when the node changes. The 32-bit shared words cannot overflow in
@@ -2558,7 +2559,7 @@ __device__ __forceinline__ void qflush_t(uint32_t *tbl, uint32_t max_nb, int32_t
     __syncthreads();
 }
 
-// One row's 32 (feature, bin) cells: w is the row's 32-byte tile.
+// One row's 32 (feature, bin) cells: va, vb are the row's 32-byte tile.
 __device__ __forceinline__ void qrow_t(uint32_t base, uint32_t lane4, uint32_t wsel,
                                        uint32_t const sel[4], uint4 va, uint4 vb, uint32_t q)
 {
@@ -2592,14 +2593,9 @@ __device__ __forceinline__ void qrow_t(uint32_t base, uint32_t lane4, uint32_t w
 }
 
 constexpr uint32_t k_tper   = k_qbuild_rows / k_tthreads; // rows per thread per chunk
-constexpr uint32_t k_tstage = 2 * 2 * k_qbuild_rows * 16; // 2 buffers x 2 halves x rows x 16 B
-constexpr uint32_t k_tsmem  = k_ttable_bytes + k_tstage;
+constexpr uint32_t k_tsmem  = k_ttable_bytes;               // the table
 constexpr uint32_t k_no_row = 0xFFFFFFFFu;
-
-__device__ __forceinline__ void cp_async16(uint32_t smem_addr, void const *gsrc)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr), "l"(gsrc));
-}
+static_assert(k_tper == 2, "the prefetch holds two rows per thread");
 
 template <bool CW2>
 __global__ void __launch_bounds__(k_tthreads, 1)
@@ -2618,20 +2614,15 @@ __global__ void __launch_bounds__(k_tthreads, 1)
     {
         return;
     }
-    uint32_t const tid  = threadIdx.x;
-    uint32_t const lane = tid & 31;
-    auto          *tbl  = reinterpret_cast<uint32_t *>(t_smem);
-    uint32_t const base = static_cast<uint32_t>(__cvta_generic_to_shared(tbl));
-    // staging after the table: [buffer][half][row slot] x 16 B; a thread
-    // uses only its own slots
-    uint32_t const stg   = base + k_ttable_bytes;
-    auto const    *stg_p = reinterpret_cast<uint4 const *>(
-        reinterpret_cast<unsigned char const *>(t_smem) + k_ttable_bytes);
     uint32_t const tile = tile_ids[blockIdx.y];
     if (tile == k_no_sel_tile)
     {
         return; // a tile slot this selection leaves unused
     }
+    uint32_t const tid  = threadIdx.x;
+    uint32_t const lane = tid & 31;
+    auto          *tbl  = reinterpret_cast<uint32_t *>(t_smem);
+    uint32_t const base = static_cast<uint32_t>(__cvta_generic_to_shared(tbl));
     if (tid < 32)
     {
         j_s[tid] = tile_j[(blockIdx.y * 32) + tid];
@@ -2650,87 +2641,76 @@ __global__ void __launch_bounds__(k_tthreads, 1)
     uint32_t const lane4 = lane * 4;
     uint32_t const wsel  = lane >> 2;
     uint4 const   *mt    = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
-    // the thread's row ids of chunk c (k_no_row past the chunk's end)
-    auto ids_of = [&](uint32_t c, uint32_t (&out)[k_tper])
+    // one chunk's share of this thread: two rows, their codes and tiles
+    struct Stage
+    {
+        uint32_t id[k_tper];
+        uint32_t q[k_tper];
+        uint4    a[k_tper];
+        uint4    b[k_tper];
+        uint32_t node;
+    };
+    auto load = [&](uint32_t c, Stage &S)
     {
         Chunk const ch = c < c_b ? bchunks[c] : Chunk{0, 0, 0, 0};
+        S.node         = ch.node;
 #pragma unroll
         for (uint32_t m = 0; m < k_tper; ++m)
         {
             uint32_t const k = (m * k_tthreads) + tid;
-            out[m] = k < ch.count ? (rows != nullptr ? rows[ch.begin + k] : ch.begin + k)
-                                  : k_no_row;
+            S.id[m] = k < ch.count ? (rows != nullptr ? rows[ch.begin + k] : ch.begin + k)
+                                   : k_no_row;
         }
-    };
-    // the copies of those rows' tiles into buffer buf, as one group
-    auto issue = [&](uint32_t const (&id)[k_tper], uint32_t buf)
-    {
 #pragma unroll
         for (uint32_t m = 0; m < k_tper; ++m)
         {
-            if (id[m] != k_no_row)
+            if (S.id[m] != k_no_row)
             {
-                uint32_t const slot = (m * k_tthreads) + tid;
-                uint4 const   *src  = mt + (static_cast<uint64_t>(id[m]) * 2);
-                cp_async16(stg + ((((buf * 2) + 0) * k_qbuild_rows) + slot) * 16, src);
-                cp_async16(stg + ((((buf * 2) + 1) * k_qbuild_rows) + slot) * 16, src + 1);
+                uint4 const *src = mt + (static_cast<uint64_t>(S.id[m]) * 2);
+                S.q[m]           = qgh[S.id[m]];
+                S.a[m]           = __ldg(src);
+                S.b[m]           = __ldg(src + 1);
+            }
+            else
+            {
+                S.q[m] = 0;
+                S.a[m] = make_uint4(0, 0, 0, 0);
+                S.b[m] = make_uint4(0, 0, 0, 0);
             }
         }
-        cp_async_commit();
     };
-    auto codes_of = [&](uint32_t const (&id)[k_tper], uint32_t (&q)[k_tper])
-    {
-#pragma unroll
-        for (uint32_t m = 0; m < k_tper; ++m)
-        {
-            q[m] = id[m] != k_no_row ? static_cast<uint32_t>(qgh[id[m]]) : 0u;
-        }
-    };
-    uint32_t id_c[k_tper];
-    uint32_t id_n[k_tper];
-    uint32_t id_nn[k_tper];
-    uint32_t q_c[k_tper];
-    uint32_t q_n[k_tper];
-    ids_of(c_a, id_c);
-    issue(id_c, 0);
-    codes_of(id_c, q_c);
-    ids_of(c_a + 1, id_n);
     uint32_t node = bchunks[c_a].node;
-    for (uint32_t c = c_a; c < c_b; ++c)
+    auto     run  = [&](Stage const &S)
     {
-        uint32_t const buf = (c - c_a) & 1;
-        // next chunk's copies and codes, the ids after it
-        issue(id_n, buf ^ 1);
-        codes_of(id_n, q_n);
-        ids_of(c + 2, id_nn);
-        uint32_t const cnode = bchunks[c].node;
-        if (cnode != node)
+        if (S.node != node)
         {
             qflush_t<CW2>(tbl, max_nb, j_s, sel_nb, cell_off,
                           hist + (static_cast<uint64_t>(build[node]) * total_cells * (CW2 ? 2 : 1)));
-            node = cnode;
+            node = S.node;
         }
-        cp_async_wait<1>(); // this thread's copies of chunk c have landed
 #pragma unroll
         for (uint32_t m = 0; m < k_tper; ++m)
         {
-            if (id_c[m] != k_no_row)
+            if (S.id[m] != k_no_row)
             {
-                uint32_t const slot = (m * k_tthreads) + tid;
-                uint4 const    va   = stg_p[((buf * 2) * k_qbuild_rows) + slot];
-                uint4 const    vb   = stg_p[(((buf * 2) + 1) * k_qbuild_rows) + slot];
-                qrow_t(base, lane4, wsel, sel, va, vb, q_c[m]);
+                qrow_t(base, lane4, wsel, sel, S.a[m], S.b[m], S.q[m]);
             }
         }
-#pragma unroll
-        for (uint32_t m = 0; m < k_tper; ++m)
+    };
+    Stage s0;
+    Stage s1;
+    load(c_a, s0);
+    for (uint32_t c = c_a; c < c_b; c += 2)
+    {
+        load(c + 1, s1);
+        run(s0);
+        if (c + 1 >= c_b)
         {
-            id_c[m] = id_n[m];
-            id_n[m] = id_nn[m];
-            q_c[m]  = q_n[m];
+            break;
         }
+        load(c + 2, s0);
+        run(s1);
     }
-    cp_async_wait<0>();
     qflush_t<CW2>(tbl, max_nb, j_s, sel_nb, cell_off,
                   hist + (static_cast<uint64_t>(build[node]) * total_cells * (CW2 ? 2 : 1)));
 }

@@ -217,6 +217,26 @@ int bb_booster_set_weights(bb_booster *b, float const *weights);
  * include/bonsai/booster.hpp:664-676). */
 int bb_booster_set_rows(bb_booster *b, uint32_t const *rows, uint64_t n_rows);
 
+/* Many boosters, one launch per round: the boosters' round graphs become
+ * the child graphs of one parent graph with no edges between them, so one
+ * cudaGraphLaunch runs a round of every booster, concurrently. Each booster
+ * must run its rounds as a CUDA graph (use_graph; a leafwise round is not
+ * captured) with no row or feature sampling, unsharded and not truncated;
+ * others are refused (BB_ERR_CONFIG). The boosters must outlive the batch.
+ * bb_batch_update runs n_rounds rounds of every booster after any work
+ * already queued on their streams, and orders their later calls after it;
+ * their trees and scores are read with bb_booster_tree / bb_booster_scores
+ * as usual, and equal the same rounds run booster by booster. No
+ * counterpart in the reference, which fits one booster per device
+ * (include/bonsai/config/sections/parallel.hpp:10-12). */
+typedef struct bb_batch bb_batch;
+int  bb_batch_create(bb_booster *const *boosters, uint32_t n, bb_batch **out);
+int  bb_batch_update(bb_batch *batch, uint32_t n_rounds);
+int  bb_batch_sync(bb_batch *batch);
+/* Device time of the last bb_batch_update, in milliseconds. */
+int  bb_batch_last_ms(bb_batch const *batch, float *ms);
+void bb_batch_destroy(bb_batch *batch);
+
 /* Runs n_iters more rounds (asynchronous; bb_booster_sync waits). */
 int bb_booster_update(bb_booster *b, uint32_t n_iters);
 int bb_booster_sync(bb_booster *b);

@@ -53,3 +53,53 @@ def test_concurrent_fits_equal_sequential(bb, mode):
             for f in TREE_FIELDS:
                 assert np.array_equal(getattr(ta, f).view(np.uint8),
                                       getattr(tc, f).view(np.uint8)), (i, t, f)
+
+
+@pytest.mark.parametrize("mode,grower", [("exact", "depthwise"), ("int8", "depthwise"),
+                                         ("int8", "levelwise")])
+def test_one_launch_batch_equals_sequential(bb, mode, grower):
+    """bb_batch: every booster's round graph a child of one parent graph, one
+    launch per round for the whole batch; the fits equal the same fits run one
+    at a time, and a batch round can follow ordinary rounds of its boosters."""
+    sets = _datasets(10, seed=65)
+    params = bb.TrainParams(max_depth=5, learning_rate=0.1, hist_mode=mode, grower=grower,
+                            use_graph=True)
+    rounds = 8
+
+    def make():
+        out = []
+        for X, y in sets:
+            cuts, off = bb.fit_cuts(X)
+            out.append(bb.Booster(bb.Plane(X, cuts, off), y, params, max_trees=rounds))
+        return out
+
+    seq = make()
+    for b in seq:
+        b.update(rounds)
+    bat = make()
+    bat[0].update(2)                 # ordinary rounds first, then the batch
+    batch = bb.BoosterBatch(bat[1:])
+    batch.update(rounds)
+    bat[0].update(rounds - 2)
+    assert batch.last_ms > 0
+    batch.close()
+    for i, (a, c) in enumerate(zip(seq, bat)):
+        assert c.n_trees == rounds, i
+        assert np.array_equal(a.scores(), c.scores()), i
+        for t in range(rounds):
+            ta, tc = a.tree(t), c.tree(t)
+            for f in TREE_FIELDS:
+                assert np.array_equal(getattr(ta, f).view(np.uint8),
+                                      getattr(tc, f).view(np.uint8)), (i, t, f)
+
+
+def test_batch_refuses_sampled_and_leafwise(bb):
+    (X, y), = _datasets(1, seed=66)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    for kw in (dict(subsample=0.8), dict(grower="leafwise", max_leaves=15),
+               dict(feature_fraction=0.5)):
+        b = bb.Booster(plane, y, bb.TrainParams(use_graph=True, **kw), max_trees=2)
+        with pytest.raises(bb.ConfigError):
+            bb.BoosterBatch([b])
+        b.close()
