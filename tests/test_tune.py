@@ -54,6 +54,9 @@ def test_ties_keep_the_default_and_exact_is_untouched(tmp_path):
     path = str(tmp_path / "t.json")
     params = TrainParams(hist_mode="int8")
     assert T.tune(_plane(), None, params, path=path, timer=lambda p: 1.0).hist_ctas == 0
+    # within the noise margin of the default: the default stays
+    assert T.pick({0: 1.00, 148: 0.99, 4: 1.5}) == 0
+    assert T.pick({0: 1.00, 148: 0.97, 4: 1.5}) == 148
     exact = TrainParams(hist_mode="exact")
     assert T.tune(_plane(), None, exact, path=path, timer=lambda p: 1 / 0) is exact
 
