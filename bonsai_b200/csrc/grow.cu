@@ -45,6 +45,40 @@ constexpr uint32_t k_chain_nst  = 4;    // cp.async stages per lane
 constexpr uint32_t k_max_bins   = 4096; // per feature, this engine's ceiling
 constexpr uint32_t k_plan_thr   = 512;  // plan kernels: one thread per node
 
+// L2 eviction hints (createpolicy): the mirror's tiles, which a pass reads
+// once, are evict-first, so that the arrays every pass of a tree reads again
+// (gradient codes, row lists, gradients) stay in L2.
+__device__ __forceinline__ uint64_t l2_policy_first()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint64_t l2_policy_last()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// A read-only 16-byte load that skips L1 and carries an L2 policy.
+__device__ __forceinline__ uint4 ld_nc_v4(uint4 const *src, uint64_t pol)
+{
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(src), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_nc_u16(uint16_t const *src, uint64_t pol)
+{
+    uint16_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(src), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt()
 {
     uint32_t m;
@@ -1188,15 +1222,33 @@ __global__ void __launch_bounds__(k_lfind_thr)
     }
 }
 
-// Cuts n row segments into chunks of `rows` rows with the whole block:
-// segment i owns chunks [range[i], range[i + 1]); chunk c finds its segment
-// by binary search (range is in global memory, written before a barrier).
-// seg(i, start, count, aux) describes segment i.
+// Cuts n row segments (n <= k_plan_thr) into chunks of `rows` rows with the
+// whole block: segment i owns chunks [range[i], range[i + 1]), and
+// seg(i, start, count, aux) describes it. One thread per segment stages its
+// chunk origin and description in shared memory first (range and what seg
+// reads are in global memory, written before a barrier), so a chunk's binary
+// search and lookup read no global memory.
 template <typename Seg>
 __device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *range,
                                                  uint32_t total, uint32_t rows, Seg seg,
                                                  Chunk *out)
 {
+    __shared__ uint32_t range_s[k_plan_thr];
+    __shared__ uint32_t start_s[k_plan_thr];
+    __shared__ uint32_t count_s[k_plan_thr];
+    __shared__ uint32_t aux_s[k_plan_thr];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        uint32_t st  = 0;
+        uint32_t cnt = 0;
+        uint32_t aux = 0;
+        seg(i, st, cnt, aux);
+        range_s[i] = range[i];
+        start_s[i] = st;
+        count_s[i] = cnt;
+        aux_s[i]   = aux;
+    }
+    __syncthreads();
     for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
     {
         uint32_t lo = 0;
@@ -1204,7 +1256,7 @@ __device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *ran
         while (hi - lo > 1)
         {
             uint32_t const mid = (lo + hi) >> 1;
-            if (range[mid] <= c)
+            if (range_s[mid] <= c)
             {
                 lo = mid;
             }
@@ -1213,12 +1265,8 @@ __device__ __forceinline__ void fill_chunk_table(uint32_t n, uint32_t const *ran
                 hi = mid;
             }
         }
-        uint32_t start = 0;
-        uint32_t count = 0;
-        uint32_t aux   = 0;
-        seg(lo, start, count, aux);
-        uint32_t const b = (c - range[lo]) * rows;
-        out[c]           = {lo, start + b, min(rows, count - b), aux};
+        uint32_t const b = (c - range_s[lo]) * rows;
+        out[c]           = {lo, start_s[lo] + b, min(rows, count_s[lo] - b), aux_s[lo]};
     }
 }
 
@@ -1397,6 +1445,8 @@ __global__ void __launch_bounds__(k_threads)
         uint32_t const k = k0 + (32 * i);
         r[i]             = k < ch.count ? rows[ch.begin + k] : k_leaf_flag;
     }
+    // (plain loads: nodes splitting on the same feature share the column's
+    // sectors, which an evict-first hint would give up early)
     uint32_t b[steps];
 #pragma unroll
     for (uint32_t i = 0; i < steps; ++i)
@@ -1461,6 +1511,9 @@ __global__ void __launch_bounds__(k_plan_thr)
                  uint64_t const *gleft, uint64_t const *fgroups)
 {
     __shared__ uint32_t grand_s;
+    __shared__ uint32_t flags_s[k_plan_thr]; // per node: flags, start, prefix origin
+    __shared__ uint32_t start_s[k_plan_thr];
+    __shared__ uint32_t p0_s[k_plan_thr];
     uint32_t const      n_cur = ctl->n_cur;
     uint32_t const      n_ch  = ctl->n_pchunks;
     // A. exclusive prefix of the chunks' left counts over the whole level
@@ -1520,19 +1573,21 @@ __global__ void __launch_bounds__(k_plan_thr)
     }
     if (live)
     {
-        dst[i] = p0; // the node's prefix origin, consumed by C below
+        flags_s[i] = nd.flags;
+        start_s[i] = nd.start;
+        p0_s[i]    = p0; // the node's prefix origin, consumed by C below
     }
     __syncthreads();
     // C. per chunk of a split node: its left and right write bases
     for (uint32_t c = threadIdx.x; c < n_ch; c += k_plan_thr)
     {
-        Chunk const ch = pchunks[c];
-        Node const  nx = nodes[ch.node];
-        if ((nx.flags & 1) != 0 && (nx.flags & 2) == 0)
+        Chunk const    ch = pchunks[c];
+        uint32_t const fl = flags_s[ch.node];
+        if ((fl & 1) != 0 && (fl & 2) == 0)
         {
-            uint32_t const lb = pleft[c] - dst[ch.node];
+            uint32_t const lb = pleft[c] - p0_s[ch.node];
             pleft[c]          = lb;
-            prbase[c]         = (ch.begin - nx.start) - lb;
+            prbase[c]         = (ch.begin - start_s[ch.node]) - lb;
         }
     }
     __syncthreads();
@@ -1833,16 +1888,17 @@ __global__ void __launch_bounds__(k_threads)
     float          mg        = 0.0F;
     float          mh        = 0.0F;
     uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
+    uint64_t const pol       = l2_policy_first();
     for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
          r0 < n_rows; r0 += 2 * stride)
     {
         uint64_t const r1  = r0 + stride;
         bool const     two = r1 < n_rows;
         uint64_t const rb  = two ? r1 : r0;
-        uint4 const    a0  = mt[r0 * 2];
-        uint4 const    b0  = mt[(r0 * 2) + 1];
-        uint4 const    a1  = mt[rb * 2];
-        uint4 const    b1  = mt[(rb * 2) + 1];
+        uint4 const    a0  = ld_nc_v4(mt + (r0 * 2), pol);
+        uint4 const    b0  = ld_nc_v4(mt + (r0 * 2) + 1, pol);
+        uint4 const    a1  = ld_nc_v4(mt + (rb * 2), pol);
+        uint4 const    b1  = ld_nc_v4(mt + (rb * 2) + 1, pol);
         float const    s0  = a.scores != nullptr ? a.scores[r0] : 0.0F;
         float const    s1  = a.scores != nullptr ? a.scores[rb] : 0.0F;
         float const    y0  = a.gh != nullptr ? a.labels[r0] : 0.0F;
@@ -1892,16 +1948,17 @@ __global__ void __launch_bounds__(k_threads)
     double const   fg        = mgx > 0.0F ? fix_unit / static_cast<double>(mgx) : 1.0;
     double const   fh        = mhx > 0.0F ? fix_unit / static_cast<double>(mhx) : 1.0;
     uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
+    uint64_t const pol       = l2_policy_first();
     for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
          r0 < n_rows; r0 += 2 * stride)
     {
         uint64_t const r1  = r0 + stride;
         bool const     two = r1 < n_rows;
         uint64_t const rb  = two ? r1 : r0;
-        uint4 const    a0  = mt[r0 * 2];
-        uint4 const    b0  = mt[(r0 * 2) + 1];
-        uint4 const    a1  = mt[rb * 2];
-        uint4 const    b1  = mt[(rb * 2) + 1];
+        uint4 const    a0  = ld_nc_v4(mt + (r0 * 2), pol);
+        uint4 const    b0  = ld_nc_v4(mt + (r0 * 2) + 1, pol);
+        uint4 const    a1  = ld_nc_v4(mt + (rb * 2), pol);
+        uint4 const    b1  = ld_nc_v4(mt + (rb * 2) + 1, pol);
         // a row outside this tree's sample takes its leaf but adds nothing
         float2 const   g0  = in_sample(bits, r0) ? gh[r0] : make_float2(0.0F, 0.0F);
         float2 const   g1  = in_sample(bits, rb) ? gh[rb] : make_float2(0.0F, 0.0F);
@@ -2506,12 +2563,20 @@ __global__ void __launch_bounds__(k_qthreads, 3)
 // histogram flushes -- one packed 64-bit global add per touched cell,
 // gradient in the high word (two's complement), hessian in the low word --
 // only when the node changes. The 32-bit shared words cannot overflow in
-// between: a CTA adds a share of one node's rows (fewer than 16,909,320
-// while the grid has a CTA per SM) and both codes are at most 127 in
-// magnitude. Global cells are packed 64-bit words while 127 x the fit's rows
-// stays below 2^31, and two words (int64 gradient, uint64 hessian sums,
-// CW2) beyond that.
+// between: a CTA adds at most k_tshare_chunks chunks of 2,048 rows (the
+// launch raises its CTA count to keep every share within that), so a word
+// sums at most 16,908,288 codes of magnitude at most 127, below 2^31.
+// Global cells are packed 64-bit words while 127 x the fit's rows stays
+// below 2^31, and two words (int64 gradient, uint64 hessian sums, CW2)
+// beyond that.
+//
+// The loads carry L2 eviction hints: the tiles are read once per build
+// (evict-first), the 2-byte gradient codes by every build of the tree
+// (evict-last), so below the root the codes are L2 hits instead of one
+// random DRAM sector per built row.
 constexpr uint32_t k_ttable_bytes = 256 * 256; // 256 bins x (32 g + 32 h) x 4 B
+constexpr uint32_t k_tshare_chunks = 0x7FFFFFFFu / (127u * 2048u);
+
 
 __device__ __forceinline__ void red_shared_u32(uint32_t addr, uint32_t v)
 {
@@ -2641,6 +2706,8 @@ __global__ void __launch_bounds__(k_tthreads, 1)
     uint32_t const lane4 = lane * 4;
     uint32_t const wsel  = lane >> 2;
     uint4 const   *mt    = mirror + (static_cast<uint64_t>(tile) * n_rows * 2);
+    uint64_t const pol_t = l2_policy_first();
+    uint64_t const pol_q = l2_policy_last();
     // one chunk's share of this thread: two rows, their codes and tiles
     struct Stage
     {
@@ -2667,9 +2734,9 @@ __global__ void __launch_bounds__(k_tthreads, 1)
             if (S.id[m] != k_no_row)
             {
                 uint4 const *src = mt + (static_cast<uint64_t>(S.id[m]) * 2);
-                S.q[m]           = qgh[S.id[m]];
-                S.a[m]           = __ldg(src);
-                S.b[m]           = __ldg(src + 1);
+                S.q[m]           = ld_nc_u16(qgh + S.id[m], pol_q);
+                S.a[m]           = ld_nc_v4(src, pol_t);
+                S.b[m]           = ld_nc_v4(src + 1, pol_t);
             }
             else
             {
@@ -4262,10 +4329,13 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
             // one tile, and about two waves over all tiles for a wide plane (a
             // CTA zeroes and flushes a 64 KB table per node, so many tiles
             // want fewer, longer CTAs each)
-            uint32_t const ctas =
-                cfg_.hist_ctas > 0 ? qctas_
-                                   : std::max(1u, std::min(qctas_, ceil_div(2 * k_qctas,
-                                                                            n_tiles_[v])));
+            // (at least enough CTAs that no CTA's share of the chunks can
+            // overflow its 32-bit shared words)
+            uint32_t const ctas = std::max(
+                ceil_div(max_bchunks_, k_tshare_chunks),
+                cfg_.hist_ctas > 0
+                    ? qctas_
+                    : std::max(1u, std::min(qctas_, ceil_div(2 * k_qctas, n_tiles_[v]))));
             auto const kern = cw_ == 2 ? qhist_t_kernel<true> : qhist_t_kernel<false>;
             kern<<<dim3(ctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
                 ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),

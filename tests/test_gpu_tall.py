@@ -16,9 +16,12 @@ pytestmark = pytest.mark.gpu
 N_TALL = 20_000_000
 
 
-def test_int8_cells_past_the_packed_range(bb):
+@pytest.mark.parametrize("hist_ctas", [0, 1])
+def test_int8_cells_past_the_packed_range(bb, hist_ctas):
     """One bin holding all 20M rows with the largest code: 20M x 127 would
-    wrap a packed 32-bit half; the two-word cell sums it exactly."""
+    wrap a packed 32-bit half; the two-word cell sums it exactly. With one
+    CTA asked for, the build still spreads the rows over enough CTAs that no
+    CTA's 32-bit shared words sum more than 16,908,288 codes."""
     rng = np.random.Generator(np.random.PCG64(5))
     X = np.empty((N_TALL, 2), np.float32)
     X[:, 0] = 1.0                                  # every row in one bin
@@ -27,7 +30,8 @@ def test_int8_cells_past_the_packed_range(bb):
     plane = bb.Plane(X, cuts, off)
     g = np.ones(N_TALL, np.float32)
     h = np.full(N_TALL, 0.25, np.float32)
-    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=1), g, h)
+    q = bb.populate(plane, bb.TrainParams(hist_mode="int8", seed=1, hist_ctas=hist_ctas),
+                    g, h)
     nb0 = int(off[1] - off[0])
     cells = q[:nb0]
     assert cells[:, 0].max() == N_TALL            # 20M codes of 127 x scale 1/127
