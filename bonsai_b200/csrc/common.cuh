@@ -44,6 +44,40 @@ void set_last_error(char const *msg);
 #define BB_CHECK(call) ::bb::check((call), #call)
 #define BB_LAUNCH(what) ::bb::check(cudaGetLastError(), what)
 
+// Programmatic dependent launch. A kernel launched with the programmatic
+// stream-serialization attribute may be scheduled while the kernel before it
+// in the stream still runs; its first statement waits for that kernel's
+// completion and memory (griddepcontrol.wait: a no-op for a kernel launched
+// without the attribute), then lets the kernel after it be scheduled in turn.
+// Nothing is read or written before the wait, so the order of effects is the
+// plain stream order; what overlaps is the next grid's launch and the
+// scheduling of its CTAs.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches kernel k like k<<<grid, block, smem, s>>>(args...), with the
+// programmatic stream-serialization attribute when pdl is set (k must open
+// with pdl_enter()).
+template <typename... P, typename... A>
+inline void launch_k(bool pdl, void (*k)(P...), dim3 grid, dim3 block, size_t smem,
+                     cudaStream_t s, A &&...args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim          = grid;
+    cfg.blockDim         = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream           = s;
+    cudaLaunchAttribute at[1];
+    at[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs                                        = pdl ? at : nullptr;
+    cfg.numAttrs                                     = pdl ? 1 : 0;
+    check(cudaLaunchKernelEx(&cfg, k, static_cast<A &&>(args)...), "cudaLaunchKernelEx");
+}
+
 // ---- split math, restated from include/bonsai/split.hpp:112-158 ----------
 // Double precision, IEEE round-to-nearest, no contraction (-fmad=false).
 

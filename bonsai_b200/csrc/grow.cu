@@ -167,6 +167,7 @@ __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk 
                                   uint32_t *brange, uint32_t *build, TreeOut t,
                                   uint32_t crows, uint32_t g_root, uint32_t const *n_root_dev)
 {
+    pdl_enter();
     if (n_root_dev != nullptr)
     {
         n_root = *n_root_dev;
@@ -231,6 +232,7 @@ __device__ __forceinline__ void warp_totals(float2 const *cells, uint32_t nb, fl
 
 __global__ void root_totals_kernel(Node *nodes, float2 const *hist, uint32_t const *sel_nb)
 {
+    pdl_enter();
     float g, h;
     warp_totals(hist, sel_nb[0], g, h);
     if (threadIdx.x == 0)
@@ -252,6 +254,7 @@ __global__ void __launch_bounds__(k_threads)
                  void const *bins, uint64_t n_pad, uint32_t const *sel,
                  uint32_t const *sel_nb, uint32_t nfb, uint32_t *ccount, uint32_t cs)
 {
+    pdl_enter();
     extern __shared__ uint32_t cnt_s[]; // [k_warps_feat][cs]
     uint32_t const             c = blockIdx.x;
     if (c >= ctl->n_bchunks)
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(k_threads)
                    uint32_t *seg, uint32_t const *sel_nb, uint32_t nfb, uint32_t cs,
                    Chunk const *bchunks)
 {
+    pdl_enter();
     __shared__ uint32_t tot_s[k_max_bins];
     __shared__ uint32_t carry_s;
     uint32_t const      i = blockIdx.x;
@@ -367,6 +371,7 @@ __global__ void __launch_bounds__(k_threads)
                    uint32_t const *ccount, uint32_t cs, float2 *payload,
                    uint64_t p_stride)
 {
+    pdl_enter();
     extern __shared__ unsigned char smem_raw[];
     uint32_t const c = blockIdx.x;
     if (c >= ctl->n_bchunks)
@@ -452,6 +457,7 @@ __global__ void __launch_bounds__(32)
                  uint64_t p_stride, uint32_t const *sel_nb, uint32_t const *cell_off,
                  uint32_t nfb, uint32_t cs, float2 *hist, uint32_t total_cells)
 {
+    pdl_enter();
     extern __shared__ float2 ring_s[];
     uint32_t const i = blockIdx.x;
     if (i >= ctl->n_build)
@@ -651,6 +657,7 @@ __global__ void __launch_bounds__(k_find_thr)
                 TreeParams tp, Best *cand, uint32_t max_nb, double2 const *qscale,
                 uint32_t const *slot_of, uint32_t cw, uint64_t const *fgroups)
 {
+    pdl_enter();
     extern __shared__ unsigned char smem_raw[];
     __shared__ double   bg_s[k_find_thr / 32];
     __shared__ uint32_t bo_s[k_find_thr / 32];
@@ -850,6 +857,7 @@ __global__ void __launch_bounds__(k_qfind_warps * 32)
                       TreeParams tp, Best *cand, double2 const *qscale, uint32_t const *slot_of,
                       uint32_t cw, uint64_t const *fgroups)
 {
+    pdl_enter();
     uint32_t const i = blockIdx.x;
     if (i >= ctl->n_cur)
     {
@@ -1016,6 +1024,7 @@ __global__ void __launch_bounds__(k_lfind_thr)
                       uint32_t n_sel, TreeParams tp, Best *cand, uint32_t max_nb,
                       uint32_t group, double2 const *qscale, uint32_t cw)
 {
+    pdl_enter();
     extern __shared__ unsigned char smem_raw[];
     __shared__ LevelNode ln_s[k_lfind_thr / 32];
     __shared__ double    bg_s[k_lfind_thr / 32];
@@ -1278,6 +1287,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                 TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound,
                 bool level)
 {
+    pdl_enter();
     __shared__ Best    level_s;
     uint32_t const n_cur = ctl->n_cur;
     uint32_t const lane  = threadIdx.x & 31;
@@ -1412,6 +1422,7 @@ __global__ void __launch_bounds__(k_threads)
                   uint32_t const *sel_nb, uint32_t *__restrict__ pleft,
                   uint32_t *__restrict__ dirs)
 {
+    pdl_enter();
     __shared__ uint32_t wsum[k_threads / 32];
     uint32_t const      c = blockIdx.x;
     if (c >= ctl->n_pchunks)
@@ -1487,6 +1498,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     node_left_kernel(Ctl const *ctl, uint32_t const *pcr, uint32_t const *pleft,
                      uint64_t *gleft, uint32_t n_slots)
 {
+    pdl_enter();
     uint32_t const n_cur = ctl->n_cur;
     for (uint32_t i = threadIdx.x; i < n_slots; i += k_plan_thr)
     {
@@ -1510,6 +1522,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  TreeOut t, uint32_t crows, uint32_t *bbase, bool level,
                  uint64_t const *gleft, uint64_t const *fgroups)
 {
+    pdl_enter();
     __shared__ uint32_t grand_s;
     __shared__ uint32_t flags_s[k_plan_thr]; // per node: flags, start, prefix origin
     __shared__ uint32_t start_s[k_plan_thr];
@@ -1666,6 +1679,7 @@ __global__ void __launch_bounds__(k_threads)
                  uint32_t const *rows, TreeOut t, uint32_t *leaf_id, float *scores,
                  float lr)
 {
+    pdl_enter();
     uint32_t const c = blockIdx.x;
     if (c >= ctl->n_pchunks)
     {
@@ -1749,59 +1763,55 @@ __device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
     }
 }
 
-__device__ __forceinline__ uint32_t walk_step(uint4 const e, uint32_t code)
+// The walked tree as a complete binary heap of its decision levels, built
+// once per tree (final_kernel): slot h's children are 2h + 1 and 2h + 2, so a
+// step reads one 8-byte entry -- x = tile << 8 | position, y = split bin |
+// missing bin << 16 | default_left << 31 -- and no child ids. A leaf above
+// the last level repeats down its left spine (split bin 0xFFFF sends every
+// code left, missing bin 0x7FFF matches no code, no tile), and the slot a
+// row ends in after `depth` steps names its leaf through leafmap.
+constexpr uint32_t k_heap_slots = 255;         // decision slots of a depth-8 heap
+constexpr uint32_t k_heap_pass  = 0x7FFFFFFFu; // a leaf's entry: always left
+
+__device__ __forceinline__ uint32_t heap_step(uint2 const e, uint32_t code, uint32_t h)
 {
-    bool const left = code == (e.y >> 16) ? ((e.z >> 24) & 1u) != 0 : code <= (e.y & 0xFFFFu);
-    return left ? (e.z & 0xFFFu) : ((e.z >> 12) & 0xFFFu);
+    bool const left = code == ((e.y >> 16) & 0x7FFFu) ? (e.y >> 31) != 0 : code <= (e.y & 0xFFFFu);
+    return (2 * h) + (left ? 1u : 2u);
 }
 
-// The tree as one 16-byte entry per node: x = tile << 8 | position (a leaf:
-// no tile), y = split bin | missing bin << 16, z = left | right << 12 |
-// default_left << 24, w = value bits.
-__device__ __forceinline__ uint32_t load_node_table(uint4 *node_s, Ctl const *ctl,
-                                                    TreeOut const &t, uint32_t const *cut_off,
-                                                    uint32_t per)
+// The heap's entries and leaf map, staged in shared memory by the block.
+__device__ __forceinline__ void load_heap(uint2 *heap_s, uint16_t *leaf_s, uint2 const *heap,
+                                          uint16_t const *leafmap, uint32_t depth)
 {
-    uint32_t const n_nodes = min(ctl->n_nodes, k_walk_nodes);
-    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    uint32_t const n_int = (1u << depth) - 1;
+    for (uint32_t i = threadIdx.x; i < n_int; i += blockDim.x)
     {
-        uint32_t const f = t.feature[i];
-        uint4          e;
-        e.w = __float_as_uint(t.value[i]);
-        if (f == k_leaf_flag)
-        {
-            e.x = k_no_tile << 8;
-            e.y = 0xFFFFFFFFu;
-            e.z = i | (i << 12);
-        }
-        else
-        {
-            e.x = ((f / per) << 8) | (f % per);
-            e.y = t.split_bin[i] | ((cut_off[f + 1] - cut_off[f] - 1) << 16);
-            e.z = t.left[i] | (t.right[i] << 12) |
-                  (static_cast<uint32_t>(t.default_left[i] != 0) << 24);
-        }
-        node_s[i] = e;
+        heap_s[i] = heap[i];
+    }
+    for (uint32_t i = threadIdx.x; i <= n_int; i += blockDim.x)
+    {
+        leaf_s[i] = leafmap[i];
     }
     __syncthreads();
-    return n_nodes;
 }
 
-// Row r's leaf: its tile of the root's feature is passed in; with MULTI the
-// walk fetches another tile when a node's feature lives there.
+// Row r's last-level slot (leaf_s names its leaf): its tile of the root's
+// feature is passed in; with MULTI the walk fetches another tile when a
+// slot's feature lives there.
 template <bool U8, bool MULTI>
-__device__ __forceinline__ uint32_t walk_row(uint4 const *node_s, uint4 const *__restrict__ mirror,
-                                             uint64_t n_rows, uint64_t r, uint32_t depth,
-                                             uint4 ta, uint4 tb, uint32_t held)
+__device__ __forceinline__ uint32_t walk_heap(uint2 const *heap_s,
+                                              uint4 const *__restrict__ mirror, uint64_t n_rows,
+                                              uint64_t r, uint32_t depth, uint4 ta, uint4 tb,
+                                              uint32_t held)
 {
     uint32_t w[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
-    uint32_t n    = 0;
+    uint32_t h    = 0;
 #pragma unroll
     for (uint32_t d = 0; d < 8; ++d)
     {
         if (d < depth)
         {
-            uint4 const e = node_s[n];
+            uint2 const e = heap_s[h];
             if constexpr (MULTI)
             {
                 uint32_t const tile = e.x >> 8;
@@ -1815,10 +1825,17 @@ __device__ __forceinline__ uint32_t walk_row(uint4 const *node_s, uint4 const *_
                     held = tile;
                 }
             }
-            n = walk_step(e, tile_code<U8>(w, e.x & 0xFFu));
+            h = heap_step(e, tile_code<U8>(w, e.x & 0xFFu), h);
         }
     }
-    return n;
+    return h - ((1u << depth) - 1); // the row's slot among the last level's 2^depth
+}
+
+// The tile that holds the root's feature (0 when the root is a leaf).
+__device__ __forceinline__ uint32_t heap_root_tile(uint2 const *heap_s, uint32_t depth)
+{
+    uint32_t const t = depth > 0 ? heap_s[0].x >> 8 : k_no_tile;
+    return t == k_no_tile ? 0u : t;
 }
 
 // Block maxima of |g| and h into the quantiser's two words.
@@ -1878,12 +1895,19 @@ __device__ __forceinline__ void apply_leaf(WalkArgs const &a, uint64_t r, uint32
 template <bool U8, bool MULTI>
 __global__ void __launch_bounds__(k_threads)
     walk_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror, uint64_t n_rows,
-                uint32_t const *cut_off, uint32_t depth, WalkArgs a)
+                uint2 const *heap, uint16_t const *leafmap, uint32_t depth, WalkArgs a)
 {
-    constexpr uint32_t per = U8 ? 32 : 16;
-    __shared__ uint4   node_s[k_walk_nodes];
-    load_node_table(node_s, ctl, t, cut_off, per);
-    uint32_t const root_tile = (node_s[0].x >> 8) == k_no_tile ? 0u : node_s[0].x >> 8;
+    pdl_enter();
+    __shared__ uint2    heap_s[k_heap_slots];
+    __shared__ uint16_t leaf_s[k_heap_slots + 1];
+    __shared__ float    val_s[k_walk_nodes];
+    uint32_t const      n_nodes = min(ctl->n_nodes, k_walk_nodes);
+    for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
+    {
+        val_s[i] = t.value[i];
+    }
+    load_heap(heap_s, leaf_s, heap, leafmap, depth);
+    uint32_t const root_tile = heap_root_tile(heap_s, depth);
     uint4 const   *mt        = mirror + (static_cast<uint64_t>(root_tile) * n_rows * 2);
     float          mg        = 0.0F;
     float          mh        = 0.0F;
@@ -1903,12 +1927,14 @@ __global__ void __launch_bounds__(k_threads)
         float const    s1  = a.scores != nullptr ? a.scores[rb] : 0.0F;
         float const    y0  = a.gh != nullptr ? a.labels[r0] : 0.0F;
         float const    y1  = a.gh != nullptr ? a.labels[rb] : 0.0F;
-        uint32_t const n0 = walk_row<U8, MULTI>(node_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
-        uint32_t const n1 = walk_row<U8, MULTI>(node_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
-        apply_leaf(a, r0, n0, s0, y0, __uint_as_float(node_s[n0].w), mg, mh);
+        uint32_t const n0 =
+            leaf_s[walk_heap<U8, MULTI>(heap_s, mirror, n_rows, r0, depth, a0, b0, root_tile)];
+        uint32_t const n1 =
+            leaf_s[walk_heap<U8, MULTI>(heap_s, mirror, n_rows, rb, depth, a1, b1, root_tile)];
+        apply_leaf(a, r0, n0, s0, y0, val_s[n0], mg, mh);
         if (two)
         {
-            apply_leaf(a, r1, n1, s1, y1, __uint_as_float(node_s[n1].w), mg, mh);
+            apply_leaf(a, r1, n1, s1, y1, val_s[n1], mg, mh);
         }
     }
     if (a.absmax != nullptr)
@@ -1924,32 +1950,52 @@ __device__ __forceinline__ bool in_sample(uint32_t const *bits, uint64_t r)
 
 // Pass A of the quantised form: each row's leaf (as 16 bits) and every
 // leaf's exact fixed-point (g, h) sums -- shared-memory 64-bit integer adds,
-// then one global add per touched leaf and CTA.
+// then one global add per touched leaf and CTA. The shared sums are kept in
+// k_wsum_copies lane-interleaved copies per last-level slot, laid out
+// [slot][g, h][copy], so a warp's 64-bit adds -- copy = lane & 15 -- touch
+// 16 distinct 8-byte words per half warp whatever slots its rows reach: two
+// conflict-free wavefronts per add instead of one pass per row sharing a
+// leaf. (Dynamic shared memory: 2^depth x 2 x 16 x 8 B.)
+constexpr uint32_t k_wsum_thr    = 512;
+constexpr uint32_t k_wsum_copies = 16;
+
 template <bool U8, bool MULTI>
-__global__ void __launch_bounds__(k_threads)
-    walk_sum_kernel(Ctl const *ctl, TreeOut t, uint4 const *__restrict__ mirror,
-                    uint64_t n_rows, uint32_t const *cut_off, uint32_t depth,
+__global__ void __launch_bounds__(k_wsum_thr)
+    walk_sum_kernel(Ctl const *ctl, uint4 const *__restrict__ mirror, uint64_t n_rows,
+                    uint2 const *heap, uint16_t const *leafmap, uint32_t depth,
                     float2 const *__restrict__ gh, uint32_t const *absmax,
                     uint16_t *__restrict__ leaf16, unsigned long long *acc,
                     uint32_t const *__restrict__ bits, double fix_unit)
 {
-    constexpr uint32_t  per = U8 ? 32 : 16;
-    __shared__ uint4    node_s[k_walk_nodes];
-    __shared__ unsigned long long acc_s[2 * k_walk_nodes];
-    for (uint32_t i = threadIdx.x; i < 2 * k_walk_nodes; i += k_threads)
+    pdl_enter();
+    extern __shared__ unsigned long long acc_s[];
+    __shared__ uint2    heap_s[k_heap_slots];
+    __shared__ uint16_t leaf_s[k_heap_slots + 1];
+    uint32_t const      n_slot = 1u << depth;
+    for (uint32_t i = threadIdx.x; i < n_slot * 2 * k_wsum_copies; i += k_wsum_thr)
     {
         acc_s[i] = 0ULL;
     }
-    uint32_t const n_nodes   = load_node_table(node_s, ctl, t, cut_off, per);
-    uint32_t const root_tile = (node_s[0].x >> 8) == k_no_tile ? 0u : node_s[0].x >> 8;
+    load_heap(heap_s, leaf_s, heap, leafmap, depth);
+    uint32_t const root_tile = heap_root_tile(heap_s, depth);
     uint4 const   *mt        = mirror + (static_cast<uint64_t>(root_tile) * n_rows * 2);
     float const    mgx       = __uint_as_float(absmax[0]);
     float const    mhx       = __uint_as_float(absmax[1]);
     double const   fg        = mgx > 0.0F ? fix_unit / static_cast<double>(mgx) : 1.0;
     double const   fh        = mhx > 0.0F ? fix_unit / static_cast<double>(mhx) : 1.0;
-    uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_threads;
+    uint64_t const stride    = static_cast<uint64_t>(gridDim.x) * k_wsum_thr;
     uint64_t const pol       = l2_policy_first();
-    for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x;
+    uint32_t const cp        = threadIdx.x & (k_wsum_copies - 1);
+    auto           add       = [&](uint32_t o, float2 g)
+    {
+        uint32_t const x = (o * 2 * k_wsum_copies) + cp;
+        atomicAdd(&acc_s[x],
+                  static_cast<unsigned long long>(llrint(static_cast<double>(g.x) * fg)));
+        atomicAdd(&acc_s[x + k_wsum_copies],
+                  static_cast<unsigned long long>(
+                      llrint(static_cast<double>(fmaxf(g.y, 0.0F)) * fh)));
+    };
+    for (uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * k_wsum_thr) + threadIdx.x;
          r0 < n_rows; r0 += 2 * stride)
     {
         uint64_t const r1  = r0 + stride;
@@ -1962,29 +2008,32 @@ __global__ void __launch_bounds__(k_threads)
         // a row outside this tree's sample takes its leaf but adds nothing
         float2 const   g0  = in_sample(bits, r0) ? gh[r0] : make_float2(0.0F, 0.0F);
         float2 const   g1  = in_sample(bits, rb) ? gh[rb] : make_float2(0.0F, 0.0F);
-        uint32_t const n0 = walk_row<U8, MULTI>(node_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
-        uint32_t const n1 = walk_row<U8, MULTI>(node_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
-        leaf16[r0] = static_cast<uint16_t>(n0);
-        atomicAdd(&acc_s[2 * n0], static_cast<unsigned long long>(
-                                      llrint(static_cast<double>(g0.x) * fg)));
-        atomicAdd(&acc_s[(2 * n0) + 1], static_cast<unsigned long long>(
-                                            llrint(static_cast<double>(fmaxf(g0.y, 0.0F)) * fh)));
+        uint32_t const o0 =
+            walk_heap<U8, MULTI>(heap_s, mirror, n_rows, r0, depth, a0, b0, root_tile);
+        uint32_t const o1 =
+            walk_heap<U8, MULTI>(heap_s, mirror, n_rows, rb, depth, a1, b1, root_tile);
+        leaf16[r0] = leaf_s[o0];
+        add(o0, g0);
         if (two)
         {
-            leaf16[r1] = static_cast<uint16_t>(n1);
-            atomicAdd(&acc_s[2 * n1], static_cast<unsigned long long>(
-                                          llrint(static_cast<double>(g1.x) * fg)));
-            atomicAdd(&acc_s[(2 * n1) + 1],
-                      static_cast<unsigned long long>(
-                          llrint(static_cast<double>(fmaxf(g1.y, 0.0F)) * fh)));
+            leaf16[r1] = leaf_s[o1];
+            add(o1, g1);
         }
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < 2 * n_nodes; i += k_threads)
+    // slot o's (g, h) over the copies, into its leaf's global sums (slots
+    // that no row reaches hold zeros)
+    for (uint32_t x = threadIdx.x; x < 2 * n_slot; x += k_wsum_thr)
     {
-        if (acc_s[i] != 0ULL)
+        unsigned long long v = 0ULL;
+#pragma unroll
+        for (uint32_t k = 0; k < k_wsum_copies; ++k)
         {
-            atomicAdd(&acc[i], acc_s[i]);
+            v += acc_s[(x * k_wsum_copies) + k];
+        }
+        if (v != 0ULL)
+        {
+            atomicAdd(&acc[(2 * leaf_s[x >> 1]) + (x & 1)], v);
         }
     }
 }
@@ -1996,6 +2045,7 @@ __global__ void __launch_bounds__(k_threads)
                     double2 const *nbound, uint32_t const *absmax, TreeParams tp,
                     double fix_unit)
 {
+    pdl_enter();
     float const  mgx = __uint_as_float(absmax[0]);
     float const  mhx = __uint_as_float(absmax[1]);
     double const fg  = mgx > 0.0F ? fix_unit / static_cast<double>(mgx) : 1.0;
@@ -2020,6 +2070,7 @@ __global__ void __launch_bounds__(k_threads)
     walk_apply_kernel(Ctl const *ctl, TreeOut t, uint64_t n_rows,
                       uint16_t const *__restrict__ leaf16, WalkArgs a)
 {
+    pdl_enter();
     __shared__ float val_s[k_walk_nodes];
     uint32_t const   n_nodes = min(ctl->n_nodes, k_walk_nodes);
     for (uint32_t i = threadIdx.x; i < n_nodes; i += k_threads)
@@ -2056,6 +2107,7 @@ __global__ void __launch_bounds__(k_threads)
                     uint32_t const *__restrict__ dirs, unsigned long long *zhist,
                     uint32_t const *build, uint32_t total_cells, uint32_t n_zcells)
 {
+    pdl_enter();
     __shared__ uint32_t wsum[k_threads / 32];
     uint32_t const      c = blockIdx.x;
     // the quantised build that follows adds into zeroed cells: every CTA
@@ -2150,6 +2202,7 @@ __global__ void __launch_bounds__(k_threads)
                            uint32_t const *sel, uint32_t const *sel_nb,
                            int8_t const *mono, uint32_t n_mono, TreeParams tp)
 {
+    pdl_enter();
     uint32_t const k = blockIdx.x;
     if (k == 0 && threadIdx.x == 0)
     {
@@ -2226,8 +2279,11 @@ __global__ void __launch_bounds__(k_threads)
 // (and, quantised, the leaf renewal) run chunk by chunk as on any level.
 __global__ void __launch_bounds__(k_plan_thr)
     final_kernel(Ctl *ctl, Node *nodes, TreeParams tp, TreeOut t, Chunk *pchunks,
-                 uint32_t *pcr, double2 *nbound)
+                 uint32_t *pcr, double2 *nbound, uint2 *heap, uint16_t *leafmap,
+                 uint32_t depth, uint32_t per, uint32_t const *cut_off)
 {
+    pdl_enter();
+    __shared__ uint16_t hnode_s[2 * (k_heap_slots + 1)];
     uint32_t const n    = ctl->n_cur;
     uint32_t const i    = threadIdx.x;
     bool const     live = i < n;
@@ -2266,6 +2322,46 @@ __global__ void __launch_bounds__(k_plan_thr)
             aux           = 0;
         },
         pchunks);
+    if (heap == nullptr)
+    {
+        return;
+    }
+    // the walk's heap (depth <= 8), level by level from the finished tables
+    // (this block's leaf writes above are visible after its barriers)
+    if (i == 0)
+    {
+        hnode_s[0] = 0;
+    }
+    __syncthreads();
+    for (uint32_t d = 0; d <= depth; ++d)
+    {
+        uint32_t const b = (1u << d) - 1;
+        for (uint32_t h = b + i; h < (2 * b) + 1; h += k_plan_thr)
+        {
+            uint32_t const nd_id = hnode_s[h];
+            if (d == depth)
+            {
+                leafmap[h - b] = static_cast<uint16_t>(nd_id);
+                continue;
+            }
+            uint32_t const f = t.feature[nd_id];
+            uint32_t       l = nd_id;
+            uint32_t       r = nd_id;
+            uint2          e = make_uint2(k_no_tile << 8, k_heap_pass);
+            if (f != k_leaf_flag)
+            {
+                e.x = ((f / per) << 8) | (f % per);
+                e.y = t.split_bin[nd_id] | ((cut_off[f + 1] - cut_off[f] - 1) << 16) |
+                      (static_cast<uint32_t>(t.default_left[nd_id] != 0) << 31);
+                l = t.left[nd_id];
+                r = t.right[nd_id];
+            }
+            heap[h]                = e;
+            hnode_s[(2 * h) + 1] = static_cast<uint16_t>(l);
+            hnode_s[(2 * h) + 2] = static_cast<uint16_t>(r);
+        }
+        __syncthreads();
+    }
 }
 
 
@@ -2305,6 +2401,7 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 __global__ void __launch_bounds__(k_threads)
     absmax_kernel(float2 const *__restrict__ gh, uint32_t n, uint32_t *absmax)
 {
+    pdl_enter();
     __shared__ float sg[k_threads / 32];
     __shared__ float sh[k_threads / 32];
     float            mg = 0.0F;
@@ -2350,6 +2447,7 @@ __global__ void __launch_bounds__(k_threads)
                     uint32_t const *__restrict__ tree_no, void *__restrict__ qout,
                     double2 *__restrict__ scale, uint64_t row_off)
 {
+    pdl_enter();
     constexpr double qmax = W16 ? 32767.0 : 127.0;
     constexpr int    imax = W16 ? 32767 : 127;
     double const mg = __uint_as_float(absmax[0]);
@@ -2399,6 +2497,7 @@ __global__ void __launch_bounds__(k_threads)
     zero_build_kernel(Ctl const *ctl, uint32_t const *build, unsigned long long *hist,
                       uint32_t total_cells, uint32_t n_cells)
 {
+    pdl_enter();
     uint32_t const i = blockIdx.x;
     if (i >= ctl->n_build)
     {
@@ -2429,6 +2528,7 @@ __global__ void __launch_bounds__(k_qthreads, 3)
                  int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
                  uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
+    pdl_enter();
     constexpr uint32_t per = k_mirror_bytes / sizeof(BinT);
     constexpr uint32_t U   = 2; // rows in flight per thread
     extern __shared__ int32_t hq_s[]; // [per][max_nb] gradient words, then hessian words
@@ -2670,6 +2770,7 @@ __global__ void __launch_bounds__(k_tthreads, 1)
                    int32_t const *tile_j, uint32_t const *sel_nb, uint32_t const *cell_off,
                    uint32_t max_nb, unsigned long long *hist, uint32_t total_cells)
 {
+    pdl_enter();
     extern __shared__ uint4 t_smem[];
     __shared__ int32_t      j_s[32];
     uint32_t const          total = ctl->n_bchunks;
@@ -2809,6 +2910,7 @@ __device__ __forceinline__ void warp_qtotals(unsigned long long const *cells, ui
 __global__ void qroot_totals_kernel(Node *nodes, unsigned long long const *hist,
                                     uint32_t const *sel_nb, uint32_t cw)
 {
+    pdl_enter();
     int64_t g, h;
     warp_qtotals(hist, sel_nb[0], cw, g, h);
     if (threadIdx.x == 0)
@@ -2832,6 +2934,7 @@ __global__ void __launch_bounds__(k_threads)
                             TreeParams tp, double2 const *qscale, int64_t const *btot,
                             uint32_t cw)
 {
+    pdl_enter();
     uint32_t const k = blockIdx.x;
     if (k == 0 && blockIdx.y == 0 && threadIdx.x == 0)
     {
@@ -2945,6 +3048,7 @@ __global__ void qsplit_totals_kernel(Ctl const *ctl, uint32_t const *bpair, Node
                                      uint32_t total_cells, uint32_t const *cell_off,
                                      uint32_t const *sel_nb, uint32_t cw, int64_t *btot)
 {
+    pdl_enter();
     uint32_t const k = (blockIdx.x * (blockDim.x / 32)) + (threadIdx.x >> 5);
     if (k >= ctl->n_splits)
     {
@@ -2988,6 +3092,7 @@ __global__ void __launch_bounds__(k_threads)
                          uint16_t const *__restrict__ qgh, uint32_t const *__restrict__ qgh16,
                          int64_t *btot)
 {
+    pdl_enter();
     uint32_t const c = blockIdx.x;
     if (c >= ctl->n_bchunks)
     {
@@ -3037,6 +3142,7 @@ __global__ void __launch_bounds__(k_threads)
                    double2 *partial, uint32_t const *pcr, TreeParams tp, TreeOut t,
                    uint32_t *done)
 {
+    pdl_enter();
     __shared__ double sg_s[k_threads / 32];
     __shared__ double sh_s[k_threads / 32];
     __shared__ bool   last_s;
@@ -3160,6 +3266,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                      uint32_t *bbase, Chunk *bchunks, uint32_t *bpair, Node *nodes, Node *next,
                      uint32_t *slot_of, LeafOut *out, uint32_t crows, LeafPop const *pp)
 {
+    pdl_enter();
     LeafPop const  p    = *pp;
     uint32_t const n_ch = ctl->n_pchunks;
     uint32_t const per  = (n_ch + k_plan_thr - 1) / k_plan_thr;
@@ -3237,6 +3344,7 @@ __global__ void __launch_bounds__(k_plan_thr)
 __global__ void leaf_copyback_kernel(LeafOut const *out, uint32_t const *__restrict__ tmp,
                                      uint32_t *__restrict__ rows, LeafPop const *pp)
 {
+    pdl_enter();
     if (out->split == 0)
     {
         return;
@@ -3256,6 +3364,7 @@ template <bool Q>
 __global__ void leaf_sub_kernel(LeafOut const *out, uint32_t const *bpair, void *pool,
                                 uint32_t total_cells, uint32_t n_cells)
 {
+    pdl_enter();
     // quantised: total_cells and n_cells count words (cw per cell)
     if (out->split == 0)
     {
@@ -3291,6 +3400,7 @@ __global__ void leaf_totals_kernel(Ctl *ctl, LeafOut const *out, Node *next,
                                    TreeParams tp, double2 const *qscale, LeafPop const *pp,
                                    uint32_t cw, uint64_t const *fgroups)
 {
+    pdl_enter();
     __shared__ int64_t qtot_s[4];
     __shared__ float   tot_s[4];
     if (out->split == 0)
@@ -3399,6 +3509,7 @@ __global__ void __launch_bounds__(k_best_thr)
     leaf_best_kernel(Ctl const *ctl, Best const *cand, uint32_t n_sel, Node const *nodes,
                      LeafOut *out, uint32_t const *may_split_p)
 {
+    pdl_enter();
     uint32_t const      may_split = *may_split_p;
     __shared__ double   g_s[k_best_thr / 32];
     __shared__ uint32_t o_s[k_best_thr / 32];
@@ -3481,6 +3592,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                           LeafOut const *out, TreeOut const *tp_, uint32_t n_root,
                           uint32_t max_front, uint32_t max_depth)
 {
+    pdl_enter();
     for (uint32_t k = threadIdx.x; k + 1 < max_front; k += k_plan_thr)
     {
         free_slots[k] = max_front - 1 - k; // popped from the top: slot 1 first
@@ -3532,6 +3644,7 @@ __global__ void __launch_bounds__(k_pop_thr)
                     uint32_t max_leaves, uint32_t max_nodes, uint32_t max_depth, Ctl *ctl,
                     Node *nodes, Best *best, Chunk *pchunks, uint32_t *pcr)
 {
+    pdl_enter();
     __shared__ double   g_s[k_pop_thr / 32];
     __shared__ uint32_t id_s[k_pop_thr / 32];
     __shared__ uint32_t ix_s[k_pop_thr / 32];
@@ -3687,6 +3800,7 @@ __global__ void leaf_commit_kernel(LeafLoop *st, LeafCand *cand, Node *leaves,
                                    TreeOut const *tp_, uint32_t max_leaves, uint32_t max_pops,
                                    cudaGraphConditionalHandle handle)
 {
+    pdl_enter();
     if (st->noop == 0)
     {
         LeafPop const &p = st->pop;
@@ -3743,6 +3857,7 @@ __global__ void leaf_commit_kernel(LeafLoop *st, LeafCand *cand, Node *leaves,
 __global__ void leaf_loop_end_kernel(LeafLoop *st, LeafCand const *cand, Node *leaves,
                                      Node *nodes, Ctl *ctl)
 {
+    pdl_enter();
     uint32_t const nl = st->n_leaves;
     uint32_t const nc = st->n_cand;
     for (uint32_t i = threadIdx.x; i < nl + nc; i += blockDim.x)
@@ -3760,12 +3875,14 @@ __global__ void leaf_loop_end_kernel(LeafLoop *st, LeafCand const *cand, Node *l
 
 __global__ void leaf_set_tree_kernel(TreeOut *dst, TreeOut t, LeafLoop *st, uint32_t root_may)
 {
+    pdl_enter();
     *dst          = t;
     st->root_may  = root_may;
 }
 
 __global__ void tree_counter_kernel(uint32_t *tree_no)
 {
+    pdl_enter();
     *tree_no += 1;
 }
 
@@ -3946,6 +4063,8 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
     rows_[1]  = dalloc<uint32_t>(max_rows_, s);
     pcr_      = dalloc<uint32_t>(max_front_ + 2, s);
     nbound_   = dalloc<double2>(std::max<uint32_t>(max_nodes_, k_walk_nodes), s);
+    heap_     = dalloc<uint2>(k_heap_slots, s);
+    leafmap_  = dalloc<uint16_t>(k_heap_slots + 1, s);
     if (cfg_.leaf)
     {
         lout_      = dalloc<LeafOut>(1, s);
@@ -4003,6 +4122,16 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaFuncSetAttribute(qhist_t_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(tsmem)));
+        // the summing walk's accumulator copies at depth 8
+        int const wsmem = static_cast<int>((size_t{2} << 8) * k_wsum_copies * 8);
+        BB_CHECK(cudaFuncSetAttribute(walk_sum_kernel<true, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, wsmem));
+        BB_CHECK(cudaFuncSetAttribute(walk_sum_kernel<true, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, wsmem));
+        BB_CHECK(cudaFuncSetAttribute(walk_sum_kernel<false, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, wsmem));
+        BB_CHECK(cudaFuncSetAttribute(walk_sum_kernel<false, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, wsmem));
     }
     else
     {
@@ -4162,7 +4291,7 @@ Grower::~Grower()
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_base_[0], tile_ids_base_[1],
                     tile_j_base_[0], tile_j_base_[1], bbase_, dirs_, btot_, done_, wacc_,
-                    leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_};
+                    leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_, heap_, leafmap_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -4250,7 +4379,7 @@ void Grower::seed_absmax(float2 const *gh)
     uint32_t const grid = std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_threads),
                                              148u * 8u);
     BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
-    absmax_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_);
+    launch_k(pdl_, absmax_kernel, grid, k_threads, 0, s, gh, n, absmax_);
     BB_LAUNCH("absmax_kernel");
 }
 
@@ -4262,7 +4391,7 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
     if (!have_absmax)
     {
         BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
-        absmax_kernel<<<grid, k_threads, 0, s>>>(gh, n, absmax_);
+        launch_k(pdl_, absmax_kernel, grid, k_threads, 0, s, gh, n, absmax_);
         BB_LAUNCH("absmax_kernel");
         n_launch_ += 1;
     }
@@ -4274,13 +4403,13 @@ void Grower::quantise(float2 const *gh, uint32_t n, bool have_absmax)
                                  static_cast<uint32_t>(seed_ >> 32));
     if (wide_codes_)
     {
-        quantise_kernel<true><<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh16_,
-                                                         qscale_, row_off_);
+        launch_k(pdl_, quantise_kernel<true>, grid, k_threads, 0, s, gh, n, absmax_, key, dtree_,
+                 qgh16_, qscale_, row_off_);
     }
     else
     {
-        quantise_kernel<false><<<grid, k_threads, 0, s>>>(gh, n, absmax_, key, dtree_, qgh8_,
-                                                          qscale_, row_off_);
+        launch_k(pdl_, quantise_kernel<false>, grid, k_threads, 0, s, gh, n, absmax_, key, dtree_,
+                 qgh8_, qscale_, row_off_);
     }
     BB_LAUNCH("quantise_kernel");
     n_launch_ += 1;
@@ -4295,9 +4424,9 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         int const v = nfb == n_sel_ ? 0 : 1;
         if (!zeroed)
         {
-            zero_build_kernel<<<max_front_, k_threads, 0, s>>>(
-                ctl_, build_, static_cast<unsigned long long *>(hist_[dst]), total_cells_ * cw_,
-                off_h_[nfb] * cw_);
+            launch_k(pdl_, zero_build_kernel, max_front_, k_threads, 0, s, ctl_, build_,
+                     static_cast<unsigned long long *>(hist_[dst]), total_cells_ * cw_,
+                     off_h_[nfb] * cw_);
             BB_LAUNCH("zero_build_kernel");
             n_launch_ += 1;
         }
@@ -4309,17 +4438,17 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
             // int16 codes: the per-chunk kernel with two-word cells
             if (plane_.u8)
             {
-                qhist_kernel<uint8_t, true><<<grid, k_qthreads, qsmem, s>>>(
-                    ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
-                    plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
-                    static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+                launch_k(pdl_, qhist_kernel<uint8_t, true>, grid, k_qthreads, qsmem, s, ctl_,
+                         bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                         plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_,
+                         max_nb_, static_cast<unsigned long long *>(hist_[dst]), total_cells_);
             }
             else
             {
-                qhist_kernel<uint16_t, true><<<grid, k_qthreads, qsmem, s>>>(
-                    ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
-                    plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
-                    static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+                launch_k(pdl_, qhist_kernel<uint16_t, true>, grid, k_qthreads, qsmem, s, ctl_,
+                         bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
+                         plane_.n_rows, qgh16_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_,
+                         max_nb_, static_cast<unsigned long long *>(hist_[dst]), total_cells_);
             }
         }
         else if (plane_.u8)
@@ -4337,19 +4466,19 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
                     ? qctas_
                     : std::max(1u, std::min(qctas_, ceil_div(2 * k_qctas, n_tiles_[v]))));
             auto const kern = cw_ == 2 ? qhist_t_kernel<true> : qhist_t_kernel<false>;
-            kern<<<dim3(ctas, n_tiles_[v]), k_tthreads, tsmem, s>>>(
-                ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
-                plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
-                static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+            launch_k(pdl_, kern, dim3(ctas, n_tiles_[v]), k_tthreads, tsmem, s, ctl_, bchunks_,
+                     build_, rows, static_cast<uint4 const *>(plane_.mirror), plane_.n_rows, qgh8_,
+                     tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                     static_cast<unsigned long long *>(hist_[dst]), total_cells_);
         }
         else
         {
             auto const kern =
                 cw_ == 2 ? qhist_kernel<uint16_t, false, true> : qhist_kernel<uint16_t>;
-            kern<<<grid, k_qthreads, qsmem, s>>>(
-                ctl_, bchunks_, build_, rows, static_cast<uint4 const *>(plane_.mirror),
-                plane_.n_rows, qgh8_, tile_ids_[v], tile_j_[v], sel_nb_, cell_off_, max_nb_,
-                static_cast<unsigned long long *>(hist_[dst]), total_cells_);
+            launch_k(pdl_, kern, grid, k_qthreads, qsmem, s, ctl_, bchunks_, build_, rows,
+                     static_cast<uint4 const *>(plane_.mirror), plane_.n_rows, qgh8_, tile_ids_[v],
+                     tile_j_[v], sel_nb_, cell_off_, max_nb_,
+                     static_cast<unsigned long long *>(hist_[dst]), total_cells_);
         }
         BB_LAUNCH("qhist_kernel");
         n_launch_ += 1;
@@ -4364,37 +4493,35 @@ void Grower::build(uint32_t const *rows, uint32_t nfb, int dst, bool zeroed)
         uint32_t const *crow = rows != nullptr ? rows : root_rows_;
         if (plane_.u8)
         {
-            count_kernel<uint8_t><<<gcs, k_threads, cnt_smem, s>>>(
-                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
-                cell_stride_);
+            launch_k(pdl_, count_kernel<uint8_t>, gcs, k_threads, cnt_smem, s, ctl_, bchunks_, crow,
+                     plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_, cell_stride_);
         }
         else
         {
-            count_kernel<uint16_t><<<gcs, k_threads, cnt_smem, s>>>(
-                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_,
-                cell_stride_);
+            launch_k(pdl_, count_kernel<uint16_t>, gcs, k_threads, cnt_smem, s, ctl_, bchunks_,
+                     crow, plane_.bins, plane_.n_pad, sel_, sel_nb_, nfb, ccount_, cell_stride_);
         }
         BB_LAUNCH("count_kernel");
-        offsets_kernel<<<dim3(max_front_, nfb), k_threads, 0, s>>>(
-            ctl_, brange_, ccount_, seg_, sel_nb_, nfb, cell_stride_, bchunks_);
+        launch_k(pdl_, offsets_kernel, dim3(max_front_, nfb), k_threads, 0, s, ctl_, brange_,
+                 ccount_, seg_, sel_nb_, nfb, cell_stride_, bchunks_);
         BB_LAUNCH("offsets_kernel");
         if (plane_.u8)
         {
-            scatter_kernel<uint8_t><<<gcs, k_threads, sc_smem, s>>>(
-                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
-                ccount_, cell_stride_, payload_, max_rows_);
+            launch_k(pdl_, scatter_kernel<uint8_t>, gcs, k_threads, sc_smem, s, ctl_, bchunks_,
+                     crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb, ccount_,
+                     cell_stride_, payload_, max_rows_);
         }
         else
         {
-            scatter_kernel<uint16_t><<<gcs, k_threads, sc_smem, s>>>(
-                ctl_, bchunks_, crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb,
-                ccount_, cell_stride_, payload_, max_rows_);
+            launch_k(pdl_, scatter_kernel<uint16_t>, gcs, k_threads, sc_smem, s, ctl_, bchunks_,
+                     crow, plane_.bins, plane_.n_pad, gh_cur_, sel_, sel_nb_, nfb, ccount_,
+                     cell_stride_, payload_, max_rows_);
         }
         BB_LAUNCH("scatter_kernel");
         size_t const chain_smem = 32 * k_chain_stg * k_chain_nst * sizeof(float2);
-        chain_kernel<<<dim3(max_front_, nfb, ceil_div(max_nb_, 32)), 32, chain_smem, s>>>(
-            ctl_, build_, bchunks_, brange_, seg_, payload_, max_rows_, sel_nb_, cell_off_,
-            nfb, cell_stride_, static_cast<float2 *>(hist_[dst]), total_cells_);
+        launch_k(pdl_, chain_kernel, dim3(max_front_, nfb, ceil_div(max_nb_, 32)), 32, chain_smem,
+                 s, ctl_, build_, bchunks_, brange_, seg_, payload_, max_rows_, sel_nb_, cell_off_,
+                 nfb, cell_stride_, static_cast<float2 *>(hist_[dst]), total_cells_);
         BB_LAUNCH("chain_kernel");
         n_launch_ += 4;
     }
@@ -4427,9 +4554,8 @@ void Grower::leaf_values(TreeOut const &t, bool)
         return;
     }
     cudaStream_t s = stream_;
-    leafsum_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_cur_, rows_cur_,
-                                                      gh_cur_, partial_, pcr_, cfg_.tp, t,
-                                                      done_);
+    launch_k(pdl_, leafsum_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_cur_,
+             rows_cur_, gh_cur_, partial_, pcr_, cfg_.tp, t, done_);
     BB_LAUNCH("leafsum_kernel");
     n_launch_ += 1;
 }
@@ -4448,34 +4574,33 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         size_t const lsmem = static_cast<size_t>(lgroup_) * max_nb_ * sizeof(double2);
         if (quant_)
         {
-            level_find_kernel<true><<<n_sel_, k_lfind_thr, lsmem, s>>>(
-                ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
-                cand_, max_nb_, lgroup_, qscale_, cw_);
+            launch_k(pdl_, level_find_kernel<true>, n_sel_, k_lfind_thr, lsmem, s, ctl_,
+                     nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
+                     cand_, max_nb_, lgroup_, qscale_, cw_);
         }
         else
         {
-            level_find_kernel<false><<<n_sel_, k_lfind_thr, lsmem, s>>>(
-                ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
-                cand_, max_nb_, lgroup_, qscale_, cw_);
+            launch_k(pdl_, level_find_kernel<false>, n_sel_, k_lfind_thr, lsmem, s, ctl_,
+                     nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, n_sel_, cfg_.tp,
+                     cand_, max_nb_, lgroup_, qscale_, cw_);
         }
     }
     else if (quant_)
     {
-        qfind_warp_kernel<<<dim3(max_front_, ceil_div(n_sel_, k_qfind_warps)),
-                            k_qfind_warps * 32, 0, s>>>(
-            ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, qscale_, nullptr, cw_, fgroups_);
+        launch_k(pdl_, qfind_warp_kernel, dim3(max_front_, ceil_div(n_sel_, k_qfind_warps)),
+                 k_qfind_warps * 32, 0, s, ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_,
+                 sel_nb_, sel_, n_sel_, mono_, n_mono_, cfg_.tp, cand_, qscale_, nullptr, cw_,
+                 fgroups_);
     }
     else
     {
-        find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
-            ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_,
-            mono_, n_mono_, cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_, fgroups_);
+        launch_k(pdl_, find_kernel<false>, fgrid, k_find_thr, find_smem, s, ctl_, nodes_[cur],
+                 hist_[cur], total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
+                 cfg_.tp, cand_, max_nb_, qscale_, nullptr, cw_, fgroups_);
     }
     BB_LAUNCH("find_kernel");
-    plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
-                                         plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_,
-                                         pcr_, nbound_, cfg_.level);
+    launch_k(pdl_, plan_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
+             plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_, pcr_, nbound_, cfg_.level);
     BB_LAUNCH("plan_kernel");
     if (prof_ != nullptr)
     {
@@ -4484,29 +4609,28 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     phase_begin();
     if (plane_.u8)
     {
-        pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
-            ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
-            sel_nb_, pleft_, dirs_);
+        launch_k(pdl_, pcount_kernel<uint8_t>, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+                 nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
+                 dirs_);
     }
     else
     {
-        pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
-            ctl_, pchunks_, nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_,
-            sel_nb_, pleft_, dirs_);
+        launch_k(pdl_, pcount_kernel<uint16_t>, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+                 nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
+                 dirs_);
     }
     BB_LAUNCH("pcount_kernel");
     if (red_ != nullptr)
     {
-        node_left_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pcr_, pleft_, gleft_, max_front_);
+        launch_k(pdl_, node_left_kernel, 1, k_plan_thr, 0, s, ctl_, pcr_, pleft_, gleft_,
+                 max_front_);
         BB_LAUNCH("node_left_kernel");
         red_->sum_u64(gleft_, max_front_, s);
         n_launch_ += 1;
     }
-    plan2_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[cur], nodes_[nxt], best_, pchunks_,
-                                          pcr_, pleft_, prbase_, nleft_, dst_, bpair_,
-                                          build_, brange_, bchunks_, cfg_.tp, t, crows_,
-                                          bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr,
-                                          fgroups_);
+    launch_k(pdl_, plan2_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], nodes_[nxt], best_,
+             pchunks_, pcr_, pleft_, prbase_, nleft_, dst_, bpair_, build_, brange_, bchunks_,
+             cfg_.tp, t, crows_, bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr, fgroups_);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -4516,8 +4640,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     if (!walk_)
     {
-        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[cur], rows_in,
-                                                        t, leaf_id, scores, lr);
+        launch_k(pdl_, stamp_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur],
+                 rows_in, t, leaf_id, scores, lr);
         BB_LAUNCH("stamp_kernel");
         n_launch_ += 1;
     }
@@ -4534,14 +4658,14 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             phase_end(prof_->partition_ms);
         }
         phase_begin();
-        qsplit_totals_kernel<<<ceil_div(max_front_, 8), 256, 0, s>>>(
-            ctl_, bpair_, nodes_[cur], best_, static_cast<unsigned long long const *>(hist_[cur]),
-            total_cells_, cell_off_, sel_nb_, cw_, btot_);
+        launch_k(pdl_, qsplit_totals_kernel, ceil_div(max_front_, 8), 256, 0, s, ctl_, bpair_,
+                 nodes_[cur], best_, static_cast<unsigned long long const *>(hist_[cur]),
+                 total_cells_, cell_off_, sel_nb_, cw_, btot_);
         BB_LAUNCH("qsplit_totals_kernel");
-        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
-            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
-            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
-            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
+        launch_k(pdl_, qsubtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+                 static_cast<unsigned long long const *>(hist_[cur]),
+                 static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
+                 nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
         BB_LAUNCH("qsubtract_totals_kernel");
         n_launch_ += 6; // count, plan2, the two totals kernels (+ find, plan)
         if (prof_ != nullptr)
@@ -4550,9 +4674,9 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         }
         return;
     }
-    pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
-        ctl_, pchunks_, nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out,
-        dirs_, static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_, n_zcells);
+    launch_k(pdl_, pscatter_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur],
+             best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out, dirs_,
+             static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_, n_zcells);
     BB_LAUNCH("pscatter_kernel");
     if (prof_ != nullptr)
     {
@@ -4565,17 +4689,17 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         // exact totals only (monotone bounds), not their histograms
         phase_begin();
         BB_CHECK(cudaMemsetAsync(btot_, 0, sizeof(int64_t) * 2 * max_front_, s));
-        qbuilt_totals_kernel<<<max_bchunks_, k_threads, 0, s>>>(ctl_, bchunks_, rows_out,
-                                                                 qgh8_, qgh16_, btot_);
+        launch_k(pdl_, qbuilt_totals_kernel, max_bchunks_, k_threads, 0, s, ctl_, bchunks_,
+                 rows_out, qgh8_, qgh16_, btot_);
         BB_LAUNCH("qbuilt_totals_kernel");
         if (red_ != nullptr)
         {
             red_->sum_u64(btot_, 2 * static_cast<size_t>(max_front_), s);
         }
-        qsubtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
-            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
-            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
-            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
+        launch_k(pdl_, qsubtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+                 static_cast<unsigned long long const *>(hist_[cur]),
+                 static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
+                 nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
         BB_LAUNCH("qsubtract_totals_kernel");
         n_launch_ += 2;
         if (prof_ != nullptr)
@@ -4596,21 +4720,19 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     phase_begin();
     if (quant_)
     {
-        qsubtract_totals_kernel<<<dim3(max_front_,
-                                       std::max(1u, ceil_div(n_cells * cw_, k_sub_cells))),
-                                  k_threads, 0, s>>>(
-            ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
-            static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells,
-            nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_,
-            nullptr, cw_);
+        launch_k(pdl_, qsubtract_totals_kernel,
+                 dim3(max_front_, std::max(1u, ceil_div(n_cells * cw_, k_sub_cells))), k_threads, 0,
+                 s, ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
+                 static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells, nodes_[cur],
+                 nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, nullptr, cw_);
         BB_LAUNCH("qsubtract_totals_kernel");
     }
     else
     {
-        subtract_totals_kernel<<<max_front_, k_threads, 0, s>>>(
-            ctl_, bpair_, static_cast<float2 const *>(hist_[cur]),
-            static_cast<float2 *>(hist_[nxt]), total_cells_, n_cells, nodes_[cur],
-            nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp);
+        launch_k(pdl_, subtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+                 static_cast<float2 const *>(hist_[cur]), static_cast<float2 *>(hist_[nxt]),
+                 total_cells_, n_cells, nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_,
+                 n_mono_, cfg_.tp);
         BB_LAUNCH("subtract_totals_kernel");
     }
     n_launch_ += 1;
@@ -4673,9 +4795,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         }
     }
     uint32_t const g_root = red_ != nullptr ? static_cast<uint32_t>(total_rows_) : n_root;
-    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t, crows_, g_root,
-                                              sample != nullptr ? sample->count : nullptr);
+    launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n_root, bchunks_,
+             brange_, build_, t, crows_, g_root, sample != nullptr ? sample->count : nullptr);
     BB_LAUNCH("root_setup_kernel");
     n_launch_ += 1;
     // the root's rows: the quantised build reads an identity list implicitly
@@ -4688,14 +4809,14 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     phase_begin();
     if (quant_)
     {
-        qroot_totals_kernel<<<1, 32, 0, s>>>(
-            nodes_[0], static_cast<unsigned long long const *>(hist_[0]), sel_nb_, cw_);
+        launch_k(pdl_, qroot_totals_kernel, 1, 32, 0, s, nodes_[0],
+                 static_cast<unsigned long long const *>(hist_[0]), sel_nb_, cw_);
         BB_LAUNCH("qroot_totals_kernel");
     }
     else
     {
-        root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(hist_[0]),
-                                            sel_nb_);
+        launch_k(pdl_, root_totals_kernel, 1, 32, 0, s, nodes_[0],
+                 static_cast<float2 const *>(hist_[0]), sel_nb_);
         BB_LAUNCH("root_totals_kernel");
     }
     n_launch_ += 1;
@@ -4712,8 +4833,9 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     }
     phase_begin();
     int const fin = static_cast<int>(cfg_.tp.max_depth & 1);
-    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_,
-                                          nbound_);
+    launch_k(pdl_, final_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_,
+             nbound_, walk_ ? heap_ : nullptr, leafmap_, cfg_.tp.max_depth,
+             k_mirror_bytes / (plane_.u8 ? 1u : 2u), plane_.cut_off);
     BB_LAUNCH("final_kernel");
     nodes_cur_ = nodes_[fin];
     rows_cur_  = rows_in;
@@ -4740,10 +4862,12 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             BB_CHECK(cudaMemsetAsync(wacc_, 0, sizeof(unsigned long long) * 2 * k_walk_nodes, s));
             auto sum = [&](auto kern)
             {
-                kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
-                                                gh_cur_, absmax_, leaf16_, wacc_,
-                                                sample != nullptr ? sample->bits : nullptr,
-                                                fix_unit_);
+                uint32_t const wgrid =
+                    std::min<uint32_t>(ceil_div(std::max<uint32_t>(n, 1), k_wsum_thr), 148u * 2u);
+                launch_k(pdl_, kern, wgrid, k_wsum_thr,
+                         (size_t{2} << depth) * k_wsum_copies * sizeof(unsigned long long), s,
+                         ctl_, mir, plane_.n_rows, heap_, leafmap_, depth, gh_cur_, absmax_,
+                         leaf16_, wacc_, sample != nullptr ? sample->bits : nullptr, fix_unit_);
             };
             if (plane_.u8)
             {
@@ -4758,14 +4882,15 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
             {
                 red_->sum_u64(wacc_, 2 * static_cast<size_t>(k_walk_nodes), s);
             }
-            leaf_fix_kernel<<<1, k_threads, 0, s>>>(ctl_, t, wacc_, nbound_, absmax_, cfg_.tp,
-                                                    fix_unit_);
+            launch_k(pdl_, leaf_fix_kernel, 1, k_threads, 0, s, ctl_, t, wacc_, nbound_, absmax_,
+                     cfg_.tp, fix_unit_);
             BB_LAUNCH("leaf_fix_kernel");
             if (next != nullptr)
             {
                 BB_CHECK(cudaMemsetAsync(absmax_, 0, 8, s));
             }
-            walk_apply_kernel<<<grid, k_threads, 0, s>>>(ctl_, t, plane_.n_rows, leaf16_, a);
+            launch_k(pdl_, walk_apply_kernel, grid, k_threads, 0, s, ctl_, t, plane_.n_rows,
+                     leaf16_, a);
             BB_LAUNCH("walk_apply_kernel");
             n_launch_ += 3;
         }
@@ -4773,8 +4898,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
         {
             auto walk = [&](auto kern)
             {
-                kern<<<grid, k_threads, 0, s>>>(ctl_, t, mir, plane_.n_rows, plane_.cut_off, depth,
-                                                a);
+                launch_k(pdl_, kern, grid, k_threads, 0, s, ctl_, t, mir, plane_.n_rows, heap_,
+                         leafmap_, depth, a);
             };
             if (plane_.u8)
             {
@@ -4791,12 +4916,12 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     else
     {
         leaf_values(t, true);
-        stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[fin], rows_in, t,
-                                                        leaf_id, scores, lr);
+        launch_k(pdl_, stamp_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[fin],
+                 rows_in, t, leaf_id, scores, lr);
         BB_LAUNCH("stamp_kernel");
         n_launch_ += 1;
     }
-    tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
+    launch_k(pdl_, tree_counter_kernel, 1, 1, 0, s, dtree_);
     BB_LAUNCH("tree_counter_kernel");
     n_launch_ += 2;
     if (prof_ != nullptr)
@@ -4835,22 +4960,22 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     uint32_t          launches  = 0;
     BB_CHECK(cudaMemcpyAsync(rows_[0], root_rows, size_t{n_root} * 4, cudaMemcpyDeviceToDevice,
                              s));
-    leaf_set_tree_kernel<<<1, 1, 0, s>>>(tdev, t, st, tp.max_depth > 0 ? 1u : 0u);
+    launch_k(pdl_, leaf_set_tree_kernel, 1, 1, 0, s, tdev, t, st, tp.max_depth > 0 ? 1u : 0u);
     BB_LAUNCH("leaf_set_tree_kernel");
-    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n_root, bchunks_, brange_,
-                                              build_, t, crows_, n_root, nullptr);
+    launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n_root, bchunks_,
+             brange_, build_, t, crows_, n_root, nullptr);
     BB_LAUNCH("root_setup_kernel");
     launches += 2;
     build(rows_[0], n_sel_, 0);
     if (quant_)
     {
-        qroot_totals_kernel<<<1, 32, 0, s>>>(
-            nodes_[0], static_cast<unsigned long long const *>(pool), sel_nb_, cw_);
+        launch_k(pdl_, qroot_totals_kernel, 1, 32, 0, s, nodes_[0],
+                 static_cast<unsigned long long const *>(pool), sel_nb_, cw_);
     }
     else
     {
-        root_totals_kernel<<<1, 32, 0, s>>>(nodes_[0], static_cast<float2 const *>(pool),
-                                            sel_nb_);
+        launch_k(pdl_, root_totals_kernel, 1, 32, 0, s, nodes_[0],
+                 static_cast<float2 const *>(pool), sel_nb_);
     }
     BB_LAUNCH("root_totals_kernel");
     launches += 1;
@@ -4861,24 +4986,24 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         dim3 const fgrid(2, n_sel_);
         if (quant_)
         {
-            qfind_warp_kernel<<<dim3(2, ceil_div(n_sel_, k_qfind_warps)), k_qfind_warps * 32, 0,
-                                s>>>(ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_,
-                                     n_sel_, mono_, n_mono_, tp, cand_, qscale_, slot_of, cw_,
-                                     fgroups_);
+            launch_k(pdl_, qfind_warp_kernel, dim3(2, ceil_div(n_sel_, k_qfind_warps)),
+                     k_qfind_warps * 32, 0, s, ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_,
+                     sel_, n_sel_, mono_, n_mono_, tp, cand_, qscale_, slot_of, cw_, fgroups_);
         }
         else
         {
-            find_kernel<false><<<fgrid, k_find_thr, find_smem, s>>>(
-                ctl_, nodes, pool, total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_,
-                tp, cand_, max_nb_, qscale_, slot_of, cw_, fgroups_);
+            launch_k(pdl_, find_kernel<false>, fgrid, k_find_thr, find_smem, s, ctl_, nodes, pool,
+                     total_cells_, cell_off_, sel_nb_, sel_, n_sel_, mono_, n_mono_, tp, cand_,
+                     max_nb_, qscale_, slot_of, cw_, fgroups_);
         }
         BB_LAUNCH("find_kernel");
-        leaf_best_kernel<<<2, k_best_thr, 0, s>>>(ctl_, cand_, n_sel_, nodes, lout, may_split);
+        launch_k(pdl_, leaf_best_kernel, 2, k_best_thr, 0, s, ctl_, cand_, n_sel_, nodes, lout,
+                 may_split);
         BB_LAUNCH("leaf_best_kernel");
     };
     find(nodes_[0], nullptr, &st->root_may);
-    leaf_loop_init_kernel<<<1, k_plan_thr, 0, s>>>(st, cand, leaves_, free_, lout, tdev, n_root,
-                                                   max_front_, tp.max_depth);
+    launch_k(pdl_, leaf_loop_init_kernel, 1, k_plan_thr, 0, s, st, cand, leaves_, free_, lout, tdev,
+             n_root, max_front_, tp.max_depth);
     BB_LAUNCH("leaf_loop_init_kernel");
     launches += 3;
 
@@ -4906,61 +5031,59 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
         uint32_t const n0 = n_launch_;
         try
         {
-            leaf_pop_kernel<<<1, k_pop_thr, 0, s>>>(
-                st, cand, free_, tdev, plane_.cuts, plane_.cut_off, sel_, tp.max_leaves,
-                max_nodes_, tp.max_depth, ctl_, nodes_[0], best_, pchunks_, pcr_);
+            launch_k(pdl_, leaf_pop_kernel, 1, k_pop_thr, 0, s, st, cand, free_, tdev, plane_.cuts,
+                     plane_.cut_off, sel_, tp.max_leaves, max_nodes_, tp.max_depth, ctl_, nodes_[0],
+                     best_, pchunks_, pcr_);
             BB_LAUNCH("leaf_pop_kernel");
             if (plane_.u8)
             {
-                pcount_kernel<uint8_t><<<max_pchunks_, k_threads, 0, s>>>(
-                    ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
-                    sel_nb_, pleft_, dirs_);
+                launch_k(pdl_, pcount_kernel<uint8_t>, max_pchunks_, k_threads, 0, s, ctl_,
+                         pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                         sel_nb_, pleft_, dirs_);
             }
             else
             {
-                pcount_kernel<uint16_t><<<max_pchunks_, k_threads, 0, s>>>(
-                    ctl_, pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
-                    sel_nb_, pleft_, dirs_);
+                launch_k(pdl_, pcount_kernel<uint16_t>, max_pchunks_, k_threads, 0, s, ctl_,
+                         pchunks_, nodes_[0], best_, rows_[0], plane_.bins, plane_.n_pad, sel_,
+                         sel_nb_, pleft_, dirs_);
             }
             BB_LAUNCH("pcount_kernel");
-            leaf_plan_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, pchunks_, pleft_, prbase_, nleft_,
-                                                      dst_, build_, brange_, bbase_, bchunks_,
-                                                      bpair_, nodes_[0], nodes_[1], slot_of_, lout,
-                                                      crows_, pp);
+            launch_k(pdl_, leaf_plan_kernel, 1, k_plan_thr, 0, s, ctl_, pchunks_, pleft_, prbase_,
+                     nleft_, dst_, build_, brange_, bbase_, bchunks_, bpair_, nodes_[0], nodes_[1],
+                     slot_of_, lout, crows_, pp);
             BB_LAUNCH("leaf_plan_kernel");
-            pscatter_kernel<<<max_pchunks_, k_threads, 0, s>>>(
-                ctl_, pchunks_, nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0],
-                rows_[1], dirs_, static_cast<unsigned long long *>(pool), build_,
-                total_cells_ * cw_, quant_ ? total_cells_ * cw_ : 0);
+            launch_k(pdl_, pscatter_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+                     nodes_[0], best_, pleft_, prbase_, nleft_, dst_, rows_[0], rows_[1], dirs_,
+                     static_cast<unsigned long long *>(pool), build_, total_cells_ * cw_,
+                     quant_ ? total_cells_ * cw_ : 0);
             BB_LAUNCH("pscatter_kernel");
             n_launch_ = 0;
             build(rows_[1], n_sel_, 0, true);
             uint32_t const nb = n_launch_;
-            leaf_copyback_kernel<<<148u * 8u, 256, 0, s>>>(lout, rows_[1], rows_[0], pp);
+            launch_k(pdl_, leaf_copyback_kernel, 148u * 8u, 256, 0, s, lout, rows_[1], rows_[0], pp);
             BB_LAUNCH("leaf_copyback_kernel");
             uint32_t const sgrid =
                 std::max(1u, std::min(ceil_div(total_cells_ * cw_, 256), 148u * 8u));
             if (quant_)
             {
-                leaf_sub_kernel<true><<<sgrid, 256, 0, s>>>(lout, bpair_, pool,
-                                                            total_cells_ * cw_,
-                                                            total_cells_ * cw_);
-                leaf_totals_kernel<true><<<1, 64, 0, s>>>(
-                    ctl_, lout, nodes_[1], slot_of_, pool, total_cells_, sel_, sel_nb_, mono_,
-                    n_mono_, tp, qscale_, pp, cw_, fgroups_);
+                launch_k(pdl_, leaf_sub_kernel<true>, sgrid, 256, 0, s, lout, bpair_, pool,
+                         total_cells_ * cw_, total_cells_ * cw_);
+                launch_k(pdl_, leaf_totals_kernel<true>, 1, 64, 0, s, ctl_, lout, nodes_[1],
+                         slot_of_, pool, total_cells_, sel_, sel_nb_, mono_, n_mono_, tp, qscale_,
+                         pp, cw_, fgroups_);
             }
             else
             {
-                leaf_sub_kernel<false><<<sgrid, 256, 0, s>>>(lout, bpair_, pool, total_cells_,
-                                                             total_cells_);
-                leaf_totals_kernel<false><<<1, 64, 0, s>>>(
-                    ctl_, lout, nodes_[1], slot_of_, pool, total_cells_, sel_, sel_nb_, mono_,
-                    n_mono_, tp, qscale_, pp, 1, fgroups_);
+                launch_k(pdl_, leaf_sub_kernel<false>, sgrid, 256, 0, s, lout, bpair_, pool,
+                         total_cells_, total_cells_);
+                launch_k(pdl_, leaf_totals_kernel<false>, 1, 64, 0, s, ctl_, lout, nodes_[1],
+                         slot_of_, pool, total_cells_, sel_, sel_nb_, mono_, n_mono_, tp, qscale_,
+                         pp, 1, fgroups_);
             }
             BB_LAUNCH("leaf_totals_kernel");
             find(nodes_[1], slot_of_, &st->may_split);
-            leaf_commit_kernel<<<1, 1, 0, s>>>(st, cand, leaves_, free_, lout, tdev,
-                                               tp.max_leaves, 4 * max_front_ + 8, handle);
+            launch_k(pdl_, leaf_commit_kernel, 1, 1, 0, s, st, cand, leaves_, free_, lout, tdev,
+                     tp.max_leaves, 4 * max_front_ + 8, handle);
             BB_LAUNCH("leaf_commit_kernel");
             // pop, count, plan, scatter, the build, copy-back, subtraction,
             // totals, find, best, commit
@@ -4989,12 +5112,13 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     {
         phase_end(prof_->other_ms);
     }
-    leaf_loop_end_kernel<<<1, k_plan_thr, 0, s>>>(st, cand, leaves_, nodes_[0], ctl_);
+    launch_k(pdl_, leaf_loop_end_kernel, 1, k_plan_thr, 0, s, st, cand, leaves_, nodes_[0], ctl_);
     BB_LAUNCH("leaf_loop_end_kernel");
     launches += 1;
     // write_leaf for every leaf, then (quantised) the FP64 renewal, then the
     // rows' leaf ids and score updates from the leaves' segments
-    final_kernel<<<1, k_plan_thr, 0, s>>>(ctl_, nodes_[0], tp, t, pchunks_, pcr_, nbound_);
+    launch_k(pdl_, final_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[0], tp, t, pchunks_, pcr_,
+             nbound_, static_cast<uint2 *>(nullptr), leafmap_, 0u, 1u, plane_.cut_off);
     BB_LAUNCH("final_kernel");
     launches += 1;
     nodes_cur_ = nodes_[0];
@@ -5002,10 +5126,10 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     uint32_t const before = n_launch_;
     leaf_values(t, true);
     launches += n_launch_ - before;
-    stamp_kernel<<<max_pchunks_, k_threads, 0, s>>>(ctl_, pchunks_, nodes_[0], rows_[0], t,
-                                                    leaf_id, scores, lr);
+    launch_k(pdl_, stamp_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[0], rows_[0],
+             t, leaf_id, scores, lr);
     BB_LAUNCH("stamp_kernel");
-    tree_counter_kernel<<<1, 1, 0, s>>>(dtree_);
+    launch_k(pdl_, tree_counter_kernel, 1, 1, 0, s, dtree_);
     BB_LAUNCH("tree_counter_kernel");
     launches += 2;
     // the loop's verdict: a full node table or pool is the reference's
@@ -5049,8 +5173,8 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
         quantise(gh, static_cast<uint32_t>(plane_.n_rows), false);
     }
     walk_ = false;
-    root_setup_kernel<<<1, k_threads, 0, s>>>(ctl_, nodes_[0], n, bchunks_, brange_, build_,
-                                              t, crows_, n, nullptr);
+    launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n, bchunks_, brange_,
+             build_, t, crows_, n, nullptr);
     BB_LAUNCH("root_setup_kernel");
     build(rows, n_sel_, 0);
     std::vector<double2> cells(total_cells_);

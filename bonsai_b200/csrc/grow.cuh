@@ -322,6 +322,8 @@ class Grower
     unsigned long long *wacc_ = nullptr; // per tree node: fixed-point (G, H) of the walk
     uint16_t *leaf16_   = nullptr; // per row: its leaf, from the walk
     double2  *nbound_   = nullptr; // per tree node: monotone bounds (lo, hi)
+    uint2    *heap_     = nullptr; // the walked tree's decision heap (final_kernel)
+    uint16_t *leafmap_  = nullptr; // its last heap level's leaf node ids
     // leafwise
     void     *lout_     = nullptr; // the pop's results (device)
     void     *lout_h_   = nullptr; // the loop's state read back after a tree (pinned host)
@@ -397,6 +399,10 @@ class Grower
     Profile    *prof_     = nullptr;
     uint32_t    launches_ = 0;
     uint32_t    n_launch_ = 0;
+    // every kernel opens with pdl_enter(): launched with programmatic
+    // stream serialization, a kernel's CTAs are scheduled while its
+    // predecessor drains
+    bool        pdl_      = true;
     cudaEvent_t pev_[2]   = {nullptr, nullptr};
     void        phase_begin();
     void        phase_end(double &acc);
