@@ -45,6 +45,48 @@ constexpr uint32_t k_chain_nst  = 4;    // cp.async stages per lane
 constexpr uint32_t k_max_bins   = 4096; // per feature, this engine's ceiling
 constexpr uint32_t k_plan_thr   = 512;  // plan kernels: one thread per node
 
+// The walked tree's decision heap (depthwise trees, depth <= 8): slot h's
+// children are 2h + 1 and 2h + 2; an entry is x = tile << 8 | position,
+// y = split bin | missing bin << 16 | default_left << 31. The plan kernels
+// fill it as the tree grows (a node carries its slot): a split node's entry,
+// and for a leaf above the last level the leaf map entry of its leftmost
+// last-level descendant; every other slot keeps the always-left entry the
+// tree starts from (split bin 0xFFFF takes every code, missing bin 0x7FFF
+// matches none, no tile).
+constexpr uint32_t k_no_tile    = 0xFFFFFFu;
+constexpr uint32_t k_heap_slots = 255;         // decision slots of a depth-8 heap
+constexpr uint32_t k_heap_pass  = 0x7FFFFFFFu; // an always-left entry's y
+
+struct HeapOut
+{
+    uint2    *heap;    // k_heap_slots entries, or null: no heap for this tree
+    uint16_t *leafmap; // 2^depth last-level slots -> leaf node id
+    uint32_t  depth;
+    uint32_t  per;     // codes per 32-byte mirror tile
+};
+
+__device__ __forceinline__ uint2 heap_entry(uint32_t f, uint32_t per, uint32_t split,
+                                            uint32_t last, bool dl)
+{
+    return make_uint2(((f / per) << 8) | (f % per),
+                      split | (last << 16) | (static_cast<uint32_t>(dl) << 31));
+}
+
+// Slot h holds a leaf: its leftmost last-level descendant names it.
+__device__ __forceinline__ void heap_leaf(HeapOut const &ho, uint32_t h, uint32_t id)
+{
+    uint32_t const lvl = 31 - __clz(h + 1);
+    if (ho.heap == nullptr || lvl > ho.depth)
+    {
+        return;
+    }
+    if (h < k_heap_slots)
+    {
+        ho.heap[h] = make_uint2(k_no_tile << 8, k_heap_pass);
+    }
+    ho.leafmap[((h + 1) << (ho.depth - lvl)) - (1u << ho.depth)] = static_cast<uint16_t>(id);
+}
+
 // L2 eviction hints (createpolicy): the mirror's tiles, which a pass reads
 // once, are evict-first, so that the arrays every pass of a tree reads again
 // (gradient codes, row lists, gradients) stay in L2.
@@ -165,9 +207,14 @@ __device__ __forceinline__ float leaf_value(Node const &nd, TreeParams const &tp
 // same number.
 __global__ void root_setup_kernel(Ctl *ctl, Node *nodes, uint32_t n_root, Chunk *bchunks,
                                   uint32_t *brange, uint32_t *build, TreeOut t,
-                                  uint32_t crows, uint32_t g_root, uint32_t const *n_root_dev)
+                                  uint32_t crows, uint32_t g_root, uint32_t const *n_root_dev,
+                                  uint2 *heap)
 {
     pdl_enter();
+    for (uint32_t i = threadIdx.x; heap != nullptr && i < k_heap_slots; i += blockDim.x)
+    {
+        heap[i] = make_uint2(k_no_tile << 8, k_heap_pass);
+    }
     if (n_root_dev != nullptr)
     {
         n_root = *n_root_dev;
@@ -1285,7 +1332,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     plan_kernel(Ctl *ctl, Node *nodes, Best const *cand, Best *best, uint32_t n_sel,
                 uint32_t const *sel, float const *cuts, uint32_t const *cut_off,
                 TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound,
-                bool level)
+                bool level, HeapOut ho)
 {
     pdl_enter();
     __shared__ Best    level_s;
@@ -1372,9 +1419,15 @@ __global__ void __launch_bounds__(k_plan_thr)
             t.cover[left]  = 0.0F;
             t.cover[right] = 0.0F;
             nd.flags       = 1;
+            if (ho.heap != nullptr && nd.heap < k_heap_slots)
+            {
+                ho.heap[nd.heap] = heap_entry(f, ho.per, bs.bin,
+                                              cut_off[f + 1] - cut_off[f] - 1, bs.dl != 0);
+            }
         }
         else
         {
+            heap_leaf(ho, nd.heap, nd.id);
             write_leaf_node(t, nd.id, leaf_value(nd, tp));
             nd.flags = 0;
         }
@@ -1520,7 +1573,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
                  TreeOut t, uint32_t crows, uint32_t *bbase, bool level,
-                 uint64_t const *gleft, uint64_t const *fgroups)
+                 uint64_t const *gleft, uint64_t const *fgroups, HeapOut ho)
 {
     pdl_enter();
     __shared__ uint32_t grand_s;
@@ -1578,6 +1631,7 @@ __global__ void __launch_bounds__(k_plan_thr)
             write_leaf_node(t, nd.id, leaf_value(nd, tp));
             t.gain[nd.id] = 0.0F;
             nodes[i]      = nd;
+            heap_leaf(ho, nd.heap, nd.id);
         }
         else
         {
@@ -1620,6 +1674,8 @@ __global__ void __launch_bounds__(k_plan_thr)
         uint32_t const rid  = t.right[nd.id];
         Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0, 0};
         Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0, 0};
+        L.heap              = (2 * nd.heap) + 1;
+        R.heap              = (2 * nd.heap) + 2;
         interaction_children(nd, fgroups, t.feature[nd.id], L, R);
         next[2 * k]         = L;
         next[(2 * k) + 1]   = R;
@@ -1725,7 +1781,6 @@ __global__ void __launch_bounds__(k_threads)
 // pass B applies them from the leaf id pass A recorded.
 constexpr uint32_t k_no_sel_tile = 0xFFFFFFFFu; // an unused tile slot of a selection
 constexpr uint32_t k_walk_nodes = 512;     // a depth-8 tree has at most 511
-constexpr uint32_t k_no_tile    = 0xFFFFFFu;
 
 struct WalkArgs
 {
@@ -1770,8 +1825,6 @@ __device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
 // the last level repeats down its left spine (split bin 0xFFFF sends every
 // code left, missing bin 0x7FFF matches no code, no tile), and the slot a
 // row ends in after `depth` steps names its leaf through leafmap.
-constexpr uint32_t k_heap_slots = 255;         // decision slots of a depth-8 heap
-constexpr uint32_t k_heap_pass  = 0x7FFFFFFFu; // a leaf's entry: always left
 
 __device__ __forceinline__ uint32_t heap_step(uint2 const e, uint32_t code, uint32_t h)
 {
@@ -2279,11 +2332,9 @@ __global__ void __launch_bounds__(k_threads)
 // (and, quantised, the leaf renewal) run chunk by chunk as on any level.
 __global__ void __launch_bounds__(k_plan_thr)
     final_kernel(Ctl *ctl, Node *nodes, TreeParams tp, TreeOut t, Chunk *pchunks,
-                 uint32_t *pcr, double2 *nbound, uint2 *heap, uint16_t *leafmap,
-                 uint32_t depth, uint32_t per, uint32_t const *cut_off)
+                 uint32_t *pcr, double2 *nbound, HeapOut ho)
 {
     pdl_enter();
-    __shared__ uint16_t hnode_s[2 * (k_heap_slots + 1)];
     uint32_t const n    = ctl->n_cur;
     uint32_t const i    = threadIdx.x;
     bool const     live = i < n;
@@ -2294,6 +2345,7 @@ __global__ void __launch_bounds__(k_plan_thr)
         write_leaf_node(t, nd.id, leaf_value(nd, tp));
         nd.flags = 0;
         nodes[i] = nd;
+        heap_leaf(ho, nd.heap, nd.id);
     }
     uint32_t const nch   = live ? (nd.count + k_part_rows - 1) / k_part_rows : 0;
     uint32_t       total = 0;
@@ -2322,46 +2374,6 @@ __global__ void __launch_bounds__(k_plan_thr)
             aux           = 0;
         },
         pchunks);
-    if (heap == nullptr)
-    {
-        return;
-    }
-    // the walk's heap (depth <= 8), level by level from the finished tables
-    // (this block's leaf writes above are visible after its barriers)
-    if (i == 0)
-    {
-        hnode_s[0] = 0;
-    }
-    __syncthreads();
-    for (uint32_t d = 0; d <= depth; ++d)
-    {
-        uint32_t const b = (1u << d) - 1;
-        for (uint32_t h = b + i; h < (2 * b) + 1; h += k_plan_thr)
-        {
-            uint32_t const nd_id = hnode_s[h];
-            if (d == depth)
-            {
-                leafmap[h - b] = static_cast<uint16_t>(nd_id);
-                continue;
-            }
-            uint32_t const f = t.feature[nd_id];
-            uint32_t       l = nd_id;
-            uint32_t       r = nd_id;
-            uint2          e = make_uint2(k_no_tile << 8, k_heap_pass);
-            if (f != k_leaf_flag)
-            {
-                e.x = ((f / per) << 8) | (f % per);
-                e.y = t.split_bin[nd_id] | ((cut_off[f + 1] - cut_off[f] - 1) << 16) |
-                      (static_cast<uint32_t>(t.default_left[nd_id] != 0) << 31);
-                l = t.left[nd_id];
-                r = t.right[nd_id];
-            }
-            heap[h]                = e;
-            hnode_s[(2 * h) + 1] = static_cast<uint16_t>(l);
-            hnode_s[(2 * h) + 2] = static_cast<uint16_t>(r);
-        }
-        __syncthreads();
-    }
 }
 
 
@@ -4600,7 +4612,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     BB_LAUNCH("find_kernel");
     launch_k(pdl_, plan_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
-             plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_, pcr_, nbound_, cfg_.level);
+             plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_, pcr_, nbound_, cfg_.level,
+             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)});
     BB_LAUNCH("plan_kernel");
     if (prof_ != nullptr)
     {
@@ -4630,7 +4643,8 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     launch_k(pdl_, plan2_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], nodes_[nxt], best_,
              pchunks_, pcr_, pleft_, prbase_, nleft_, dst_, bpair_, build_, brange_, bchunks_,
-             cfg_.tp, t, crows_, bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr, fgroups_);
+             cfg_.tp, t, crows_, bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr, fgroups_,
+             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)});
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -4796,7 +4810,8 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     }
     uint32_t const g_root = red_ != nullptr ? static_cast<uint32_t>(total_rows_) : n_root;
     launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n_root, bchunks_,
-             brange_, build_, t, crows_, g_root, sample != nullptr ? sample->count : nullptr);
+             brange_, build_, t, crows_, g_root, sample != nullptr ? sample->count : nullptr,
+             heap_);
     BB_LAUNCH("root_setup_kernel");
     n_launch_ += 1;
     // the root's rows: the quantised build reads an identity list implicitly
@@ -4834,8 +4849,7 @@ void Grower::grow(float2 const *gh, uint32_t const *root_rows, uint32_t n_root,
     phase_begin();
     int const fin = static_cast<int>(cfg_.tp.max_depth & 1);
     launch_k(pdl_, final_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[fin], cfg_.tp, t, pchunks_, pcr_,
-             nbound_, walk_ ? heap_ : nullptr, leafmap_, cfg_.tp.max_depth,
-             k_mirror_bytes / (plane_.u8 ? 1u : 2u), plane_.cut_off);
+             nbound_, HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)});
     BB_LAUNCH("final_kernel");
     nodes_cur_ = nodes_[fin];
     rows_cur_  = rows_in;
@@ -4963,7 +4977,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     launch_k(pdl_, leaf_set_tree_kernel, 1, 1, 0, s, tdev, t, st, tp.max_depth > 0 ? 1u : 0u);
     BB_LAUNCH("leaf_set_tree_kernel");
     launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n_root, bchunks_,
-             brange_, build_, t, crows_, n_root, nullptr);
+             brange_, build_, t, crows_, n_root, nullptr, static_cast<uint2 *>(nullptr));
     BB_LAUNCH("root_setup_kernel");
     launches += 2;
     build(rows_[0], n_sel_, 0);
@@ -5118,7 +5132,7 @@ void Grower::grow_leafwise(uint32_t const *root_rows, uint32_t n_root, TreeOut c
     // write_leaf for every leaf, then (quantised) the FP64 renewal, then the
     // rows' leaf ids and score updates from the leaves' segments
     launch_k(pdl_, final_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[0], tp, t, pchunks_, pcr_,
-             nbound_, static_cast<uint2 *>(nullptr), leafmap_, 0u, 1u, plane_.cut_off);
+             nbound_, HeapOut{nullptr, nullptr, 0, 1});
     BB_LAUNCH("final_kernel");
     launches += 1;
     nodes_cur_ = nodes_[0];
@@ -5174,7 +5188,7 @@ void Grower::populate(float2 const *gh, uint32_t const *rows, uint32_t n, double
     }
     walk_ = false;
     launch_k(pdl_, root_setup_kernel, 1, k_threads, 0, s, ctl_, nodes_[0], n, bchunks_, brange_,
-             build_, t, crows_, n, nullptr);
+             build_, t, crows_, n, nullptr, heap_);
     BB_LAUNCH("root_setup_kernel");
     build(rows, n_sel_, 0);
     std::vector<double2> cells(total_cells_);

@@ -35,6 +35,7 @@ struct Node
     // feature when it is 1, << 2; and the groups that contain the whole path
     uint32_t ipath;
     uint64_t icover;
+    uint32_t heap; // depthwise: the node's slot in the walked tree's decision heap
 };
 
 // SplitOutput (include/bonsai/split.hpp:62-69), one per (node, feature)
