@@ -1332,7 +1332,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     plan_kernel(Ctl *ctl, Node *nodes, Best const *cand, Best *best, uint32_t n_sel,
                 uint32_t const *sel, float const *cuts, uint32_t const *cut_off,
                 TreeParams tp, TreeOut t, Chunk *pchunks, uint32_t *pcr, double2 *nbound,
-                bool level, HeapOut ho)
+                bool level, HeapOut ho, uint32_t *nleft, uint32_t *nright)
 {
     pdl_enter();
     __shared__ Best    level_s;
@@ -1399,6 +1399,8 @@ __global__ void __launch_bounds__(k_plan_thr)
     Node           nd       = live ? nodes[i] : Node{};
     if (live)
     {
+        nleft[i]      = 0; // the one-pass partition's per-node counters
+        nright[i]     = 0;
         nbound[nd.id] = make_double2(nd.lo, nd.hi); // for a later leaf renewal
         if (split)
         {
@@ -1445,6 +1447,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     {
         pcr[n_cur]      = total;
         ctl->n_pchunks  = total;
+        ctl->n_psplit   = n_split_total;
         ctl->n_nodes    = n_nodes0 + (2 * n_split_total);
         ctl->n_leaves  += n_cur - n_split_total;
     }
@@ -1573,7 +1576,7 @@ __global__ void __launch_bounds__(k_plan_thr)
                  uint32_t *prbase, uint32_t *nleft, uint32_t *dst, uint32_t *bpair,
                  uint32_t *build, uint32_t *brange, Chunk *bchunks, TreeParams tp,
                  TreeOut t, uint32_t crows, uint32_t *bbase, bool level,
-                 uint64_t const *gleft, uint64_t const *fgroups, HeapOut ho)
+                 uint64_t const *gleft, uint64_t const *fgroups, HeapOut ho, bool fused)
 {
     pdl_enter();
     __shared__ uint32_t grand_s;
@@ -1584,7 +1587,8 @@ __global__ void __launch_bounds__(k_plan_thr)
     uint32_t const      n_ch  = ctl->n_pchunks;
     // A. exclusive prefix of the chunks' left counts over the whole level
     //    (leaf chunks count zero), each thread a contiguous run of chunks
-    uint32_t const per = (n_ch + k_plan_thr - 1) / k_plan_thr;
+    //    (the one-pass partition placed its rows already: no chunk runs)
+    uint32_t const per = fused ? 0 : (n_ch + k_plan_thr - 1) / k_plan_thr;
     uint32_t const c_a = min(n_ch, threadIdx.x * per);
     uint32_t const c_b = min(n_ch, c_a + per);
     uint32_t       sum = 0;
@@ -1615,13 +1619,20 @@ __global__ void __launch_bounds__(k_plan_thr)
     uint32_t       p0   = 0;
     if (live && (nd.flags & 1) != 0)
     {
-        uint32_t const c0 = pcr[i];
-        uint32_t const c1 = pcr[i + 1];
-        // a node without chunks (a level split of an empty node) past the
-        // last chunk: its prefix origin is the grand total
-        p0                = c0 < n_ch ? pleft[c0] : grand_s;
-        nl                = (c1 < n_ch ? pleft[c1] : grand_s) - p0;
-        nleft[i]          = nl;
+        if (fused)
+        {
+            nl = nleft[i]; // the one-pass partition's left counter
+        }
+        else
+        {
+            uint32_t const c0 = pcr[i];
+            uint32_t const c1 = pcr[i + 1];
+            // a node without chunks (a level split of an empty node) past
+            // the last chunk: its prefix origin is the grand total
+            p0       = c0 < n_ch ? pleft[c0] : grand_s;
+            nl       = (c1 < n_ch ? pleft[c1] : grand_s) - p0;
+            nleft[i] = nl;
+        }
         gnl               = gleft != nullptr ? static_cast<uint32_t>(gleft[i]) : nl;
         if (!level && (gnl == 0 || gnl == nd.gcount))
         {
@@ -1646,7 +1657,7 @@ __global__ void __launch_bounds__(k_plan_thr)
     }
     __syncthreads();
     // C. per chunk of a split node: its left and right write bases
-    for (uint32_t c = threadIdx.x; c < n_ch; c += k_plan_thr)
+    for (uint32_t c = threadIdx.x; !fused && c < n_ch; c += k_plan_thr)
     {
         Chunk const    ch = pchunks[c];
         uint32_t const fl = flags_s[ch.node];
@@ -1667,13 +1678,16 @@ __global__ void __launch_bounds__(k_plan_thr)
     uint32_t small_count = 0;
     if (surv)
     {
-        dst[i]              = start;
+        // the children's rows: compacted by pscatter, or where the one-pass
+        // partition left them (the parent's segment, lefts first)
+        uint32_t const s0   = fused ? nd.start : start;
+        dst[i]              = s0;
         uint32_t const nr   = nd.count - nl;
         uint32_t const gnr  = nd.gcount - gnl;
         uint32_t const lid  = t.left[nd.id];
         uint32_t const rid  = t.right[nd.id];
-        Node           L{start, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0, 0};
-        Node           R{start + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0, 0};
+        Node           L{s0, nl, lid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnl, 0, 0};
+        Node           R{s0 + nl, nr, rid, 0, 0.0F, 0.0F, nd.lo, nd.hi, 0, 0, gnr, 0, 0};
         L.heap              = (2 * nd.heap) + 1;
         R.heap              = (2 * nd.heap) + 2;
         interaction_children(nd, fgroups, t.feature[nd.id], L, R);
@@ -2243,6 +2257,139 @@ __global__ void __launch_bounds__(k_threads)
         }
         lo += __popc(lm);
         ro += nvalid - __popc(lm);
+    }
+}
+
+// The partition in one pass, for trees the final walk stamps in the
+// quantised form, whose every consumer of the row lists is order-free (the
+// histogram build adds exact integers; the next partition routes row by
+// row). Each chunk routes its rows as pcount_kernel does, then reserves its
+// lefts' and rights' places in the node's own segment with one atomic add per
+// side on per-node counters (zeroed by plan_kernel): lefts fill the segment
+// from its start, rights from its end backwards, so pass 2, its re-read of the
+// row ids and the chunk prefix sums in plan2_kernel fall away. Which chunk's
+// rows come first inside a child depends on the order chunks finish; the
+// histograms, splits and leaves do not. With SCATTER false (the last level,
+// whose rows are never listed) only the left counts are taken. Also zeroes
+// the next level's histogram slots [0, 2 x splits) for the build's adds.
+template <typename BinT, bool SCATTER>
+__global__ void __launch_bounds__(k_threads)
+    psplit_kernel(Ctl const *ctl, Chunk const *pchunks, Node const *nodes, Best const *best,
+                  uint32_t const *__restrict__ rows, uint32_t *__restrict__ rows_out,
+                  void const *__restrict__ bins, uint64_t n_pad, uint32_t const *sel,
+                  uint32_t const *sel_nb, uint32_t *nleft, uint32_t *nright,
+                  unsigned long long *zhist, uint32_t total_cells, uint32_t n_zcells)
+{
+    pdl_enter();
+    __shared__ uint32_t wsum[k_threads / 32];
+    __shared__ uint32_t base_s[2];
+    uint32_t const      c = blockIdx.x;
+    if constexpr (SCATTER)
+    {
+        uint64_t const nz = 2ULL * ctl->n_psplit * n_zcells;
+        for (uint64_t x = (static_cast<uint64_t>(c) * k_threads) + threadIdx.x; x < nz;
+             x += static_cast<uint64_t>(gridDim.x) * k_threads)
+        {
+            uint64_t const i = x / n_zcells;
+            zhist[(i * total_cells) + (x - (i * n_zcells))] = 0ULL;
+        }
+    }
+    if (c >= ctl->n_pchunks)
+    {
+        return;
+    }
+    Chunk const ch = pchunks[c];
+    Node const  nd = nodes[ch.node];
+    if ((nd.flags & 1) == 0)
+    {
+        return; // a leaf's chunk routes nothing
+    }
+    Best const     bs   = best[ch.node];
+    uint32_t const f    = sel[bs.feature];
+    uint32_t const last = sel_nb[bs.feature] - 1;
+    BinT const    *col  = static_cast<BinT const *>(bins) + (static_cast<uint64_t>(f) * n_pad);
+    uint32_t const lane = threadIdx.x & 31;
+    uint32_t const w    = threadIdx.x >> 5;
+    uint32_t const w0   = w * k_warp_rows;
+    constexpr uint32_t steps = k_warp_rows / 32;
+    uint32_t           r[steps];
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        uint32_t const k = w0 + (32 * i) + lane;
+        r[i]             = k < ch.count ? rows[ch.begin + k] : k_leaf_flag;
+    }
+    uint32_t b[steps];
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        b[i] = r[i] != k_leaf_flag ? static_cast<uint32_t>(col[r[i]]) : 0u;
+    }
+    uint32_t mword = 0; // lane i: step i's direction bits
+    uint32_t n     = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        bool const     lf = r[i] != k_leaf_flag && routes_left(b[i], last, bs.bin, bs.dl != 0);
+        uint32_t const m  = __ballot_sync(0xFFFFFFFFu, lf);
+        mword             = lane == i ? m : mword;
+        n += __popc(m);
+    }
+    if (lane == 0)
+    {
+        wsum[w] = n;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t lc = 0;
+        for (uint32_t x = 0; x < k_threads / 32; ++x)
+        {
+            lc += wsum[x];
+        }
+        uint32_t const rc = ch.count - lc;
+        base_s[0]         = lc != 0 ? atomicAdd(&nleft[ch.node], lc) : 0u;
+        base_s[1]         = SCATTER && rc != 0 ? atomicAdd(&nright[ch.node], rc) : 0u;
+    }
+    if constexpr (!SCATTER)
+    {
+        return;
+    }
+    __syncthreads();
+    uint32_t lb = 0;
+    for (uint32_t x = 0; x < w; ++x)
+    {
+        lb += wsum[x];
+    }
+    uint32_t       lo  = nd.start + base_s[0] + lb;                       // next left
+    uint32_t       rk  = base_s[1] + (min(w0, ch.count) - lb);            // next right's rank
+    uint32_t const top = nd.start + nd.count - 1;                          // rights count down
+    uint32_t const ltm = (1u << lane) - 1u;
+#pragma unroll
+    for (uint32_t i = 0; i < steps; ++i)
+    {
+        uint32_t const base = w0 + (32 * i);
+        if (base >= ch.count)
+        {
+            break;
+        }
+        uint32_t const m      = __shfl_sync(0xFFFFFFFFu, mword, i);
+        uint32_t const nvalid = min(32u, ch.count - base);
+        uint32_t const vm     = nvalid == 32 ? 0xFFFFFFFFu : ((1u << nvalid) - 1u);
+        uint32_t const lm     = m & vm;
+        if (lane < nvalid)
+        {
+            if ((m >> lane) & 1u)
+            {
+                rows_out[lo + __popc(lm & ltm)] = r[i];
+            }
+            else
+            {
+                rows_out[top - (rk + __popc(~lm & vm & ltm))] = r[i];
+            }
+        }
+        lo += __popc(lm);
+        rk += __popc(~lm & vm);
     }
 }
 
@@ -4089,6 +4236,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
         BB_CHECK(cudaMallocHost(&lout_h_, sizeof(LeafLoop)));
     }
     nleft_    = dalloc<uint32_t>(max_front_ + 1, s);
+    nright_   = dalloc<uint32_t>(max_front_ + 1, s);
     dtree_    = dalloc<uint32_t>(1, s);
     BB_CHECK(cudaMemsetAsync(dtree_, 0, 4, s));
     if (quant_)
@@ -4303,7 +4451,7 @@ Grower::~Grower()
                     absmax_,  qgh_,      pcr_,     nleft_,    mono_,       qscale_,
                     qgh8_,    partial_,  dtree_,   tile_ids_base_[0], tile_ids_base_[1],
                     tile_j_base_[0], tile_j_base_[1], bbase_, dirs_, btot_, done_, wacc_,
-                    leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_, heap_, leafmap_};
+                    leaf16_,  nbound_,  gleft_,   qgh16_,   fgroups_, heap_, leafmap_, nright_};
     for (void *p : ptrs)
     {
         if (p != nullptr)
@@ -4613,14 +4761,31 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     BB_LAUNCH("find_kernel");
     launch_k(pdl_, plan_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], cand_, best_, n_sel_, sel_,
              plane_.cuts, plane_.cut_off, cfg_.tp, t, pchunks_, pcr_, nbound_, cfg_.level,
-             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)});
+             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)}, nleft_, nright_);
     BB_LAUNCH("plan_kernel");
     if (prof_ != nullptr)
     {
         phase_end(prof_->find_ms);
     }
     phase_begin();
-    if (plane_.u8)
+    bool const     last     = (L + 1) == cfg_.tp.max_depth;
+    uint32_t const nfb      = last ? 1 : n_sel_;
+    uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] * cw_ : 0;
+    // a walked quantised tree (unsharded) partitions in one pass: nothing
+    // downstream of its row lists depends on the rows' order inside a node
+    bool const     fused    = quant_ && walk_ && red_ == nullptr;
+    if (fused)
+    {
+        auto const kern = plane_.u8 ? (last ? psplit_kernel<uint8_t, false>
+                                            : psplit_kernel<uint8_t, true>)
+                                    : (last ? psplit_kernel<uint16_t, false>
+                                            : psplit_kernel<uint16_t, true>);
+        launch_k(pdl_, kern, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur], best_,
+                 rows_in, rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_, nleft_, nright_,
+                 static_cast<unsigned long long *>(hist_[nxt]), total_cells_ * cw_, n_zcells);
+        BB_LAUNCH("psplit_kernel");
+    }
+    else if (plane_.u8)
     {
         launch_k(pdl_, pcount_kernel<uint8_t>, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
                  nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
@@ -4632,7 +4797,10 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
                  nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
                  dirs_);
     }
-    BB_LAUNCH("pcount_kernel");
+    if (!fused)
+    {
+        BB_LAUNCH("pcount_kernel");
+    }
     if (red_ != nullptr)
     {
         launch_k(pdl_, node_left_kernel, 1, k_plan_thr, 0, s, ctl_, pcr_, pleft_, gleft_,
@@ -4644,7 +4812,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     launch_k(pdl_, plan2_kernel, 1, k_plan_thr, 0, s, ctl_, nodes_[cur], nodes_[nxt], best_,
              pchunks_, pcr_, pleft_, prbase_, nleft_, dst_, bpair_, build_, brange_, bchunks_,
              cfg_.tp, t, crows_, bbase_, cfg_.level, red_ != nullptr ? gleft_ : nullptr, fgroups_,
-             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)});
+             HeapOut{heap_, leafmap_, cfg_.tp.max_depth, k_mirror_bytes / (plane_.u8 ? 1u : 2u)}, fused);
     BB_LAUNCH("plan2_kernel");
     nodes_cur_ = nodes_[cur];
     rows_cur_  = rows_in;
@@ -4659,9 +4827,6 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         BB_LAUNCH("stamp_kernel");
         n_launch_ += 1;
     }
-    bool const     last     = (L + 1) == cfg_.tp.max_depth;
-    uint32_t const nfb      = last ? 1 : n_sel_;
-    uint32_t const n_zcells = quant_ && !last ? off_h_[nfb] * cw_ : 0;
     if (quant_ && last && walk_)
     {
         // a walked tree's last level: the leaves' rows are never listed (the
@@ -4688,15 +4853,19 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         }
         return;
     }
-    launch_k(pdl_, pscatter_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur],
-             best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out, dirs_,
-             static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_, n_zcells);
-    BB_LAUNCH("pscatter_kernel");
+    if (!fused)
+    {
+        launch_k(pdl_, pscatter_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+                 nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out, dirs_,
+                 static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_,
+                 n_zcells);
+        BB_LAUNCH("pscatter_kernel");
+    }
     if (prof_ != nullptr)
     {
         phase_end(prof_->partition_ms);
     }
-    n_launch_ += 5;
+    n_launch_ += fused ? 4 : 5;
     if (quant_ && last)
     {
         // the last level's nodes are leaves: the quantised form needs their

@@ -71,7 +71,8 @@ struct Ctl
     uint32_t n_build;    // nodes whose histograms are built this level
     uint32_t n_splits;   // surviving splits this level
     uint32_t built_rows; // rows across the built nodes
-    uint32_t pad[6];
+    uint32_t n_psplit;   // splits plan_kernel committed at the current level
+    uint32_t pad[5];
 };
 
 // A row sample on the device: its size and one bit per dataset row (bit r of
@@ -323,7 +324,8 @@ class Grower
     unsigned long long *wacc_ = nullptr; // per tree node: fixed-point (G, H) of the walk
     uint16_t *leaf16_   = nullptr; // per row: its leaf, from the walk
     double2  *nbound_   = nullptr; // per tree node: monotone bounds (lo, hi)
-    uint2    *heap_     = nullptr; // the walked tree's decision heap (final_kernel)
+    uint32_t *nright_   = nullptr; // per frontier node: rights placed (one-pass partition)
+    uint2    *heap_     = nullptr; // the walked tree's decision heap (plan kernels)
     uint16_t *leafmap_  = nullptr; // its last heap level's leaf node ids
     // leafwise
     void     *lout_     = nullptr; // the pop's results (device)

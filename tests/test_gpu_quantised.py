@@ -89,6 +89,37 @@ def test_quantised_seeded_and_deterministic(bb):
 
 
 @pytest.mark.parametrize("mono", [False, True])
+@pytest.mark.parametrize("grower", ["depthwise", "levelwise"])
+def test_one_pass_partition_leaves_fits_deterministic(bb, grower):
+    """A walked quantised tree partitions each level in one pass: chunks
+    place their rows in a child in the order they finish, so row lists
+    differ from run to run. Everything built from them (exact integer
+    histograms, per-row routing) is order-free: three fits of 2,000,000 rows
+    (hundreds of chunks per node) give the same trees and scores bit for
+    bit, with and without CUDA graphs."""
+    X, g, h = _data(21, 2_000_000, F=12)
+    cuts, off = bb.fit_cuts(X)
+    plane = bb.Plane(X, cuts, off)
+    y = (g + np.nan_to_num(X[:, 0]) > 0).astype(np.float32)
+
+    def fit(graph):
+        b = bb.Booster(plane, y, bb.TrainParams(objective="logloss", max_depth=8,
+                                                 hist_mode="int8", seed=5, grower=grower,
+                                                 use_graph=graph), max_trees=12)
+        b.update(12)
+        out = b.scores(), [b.tree(i) for i in range(12)]
+        b.close()
+        return out
+
+    s0, t0 = fit(True)
+    for graph in (True, False):
+        s1, t1 = fit(graph)
+        assert np.array_equal(s0, s1)
+        for a, c in zip(t0, t1):
+            for k in ("feature", "split_bin", "left", "right", "value", "cover"):
+                assert np.array_equal(getattr(a, k), getattr(c, k)), k
+
+
 def test_quantised_leaf_values_renew_from_full_gradients(bb, mono):
     """Every leaf's value is the FP64 Newton step of its rows' full-precision
     (g, h) -- not of the quantised codes -- under its monotone bounds, and the
