@@ -116,7 +116,7 @@ def test_one_pass_partition_leaves_fits_deterministic(bb, grower):
         s1, t1 = fit(graph)
         assert np.array_equal(s0, s1)
         for a, c in zip(t0, t1):
-            for k in ("feature", "split_bin", "left", "right", "value", "cover"):
+            for k in ("feature", "split_bin", "left", "right", "value", "covers"):
                 assert np.array_equal(getattr(a, k), getattr(c, k)), k
 
 
