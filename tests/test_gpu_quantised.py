@@ -88,7 +88,6 @@ def test_quantised_seeded_and_deterministic(bb):
     assert not np.array_equal(s1, s3)
 
 
-@pytest.mark.parametrize("mono", [False, True])
 @pytest.mark.parametrize("grower", ["depthwise", "levelwise"])
 def test_one_pass_partition_leaves_fits_deterministic(bb, grower):
     """A walked quantised tree partitions each level in one pass: chunks
@@ -120,6 +119,7 @@ def test_one_pass_partition_leaves_fits_deterministic(bb, grower):
                 assert np.array_equal(getattr(a, k), getattr(c, k)), k
 
 
+@pytest.mark.parametrize("mono", [False, True])
 def test_quantised_leaf_values_renew_from_full_gradients(bb, mono):
     """Every leaf's value is the FP64 Newton step of its rows' full-precision
     (g, h) -- not of the quantised codes -- under its monotone bounds, and the
