@@ -4058,6 +4058,7 @@ Grower::Grower(Plane const &plane, GrowConfig const &cfg, std::vector<uint32_t> 
                uint32_t max_root_rows, cudaStream_t stream)
     : plane_(plane), cfg_(cfg), sel_h_(std::move(selected)), stream_(stream)
 {
+    pdl_ = plane_.n_rows >= (uint64_t{1} << 19);
     if (cfg_.sample_k > 0)
     {
         // per-tree samples: the first sample_k features until set_selection

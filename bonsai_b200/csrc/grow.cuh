@@ -404,8 +404,11 @@ class Grower
     uint32_t    n_launch_ = 0;
     // every kernel opens with pdl_enter(): launched with programmatic
     // stream serialization, a kernel's CTAs are scheduled while its
-    // predecessor drains
-    bool        pdl_      = true;
+    // predecessor drains. Set for planes of 2^19 rows or more, whose kernels
+    // each fill the GPU; small planes are the ones several boosters fit at
+    // once, where CTAs waiting for their predecessor would hold SM resources
+    // the other boosters' kernels could use.
+    bool        pdl_      = false;
     cudaEvent_t pev_[2]   = {nullptr, nullptr};
     void        phase_begin();
     void        phase_end(double &acc);
