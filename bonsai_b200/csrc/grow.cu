@@ -114,11 +114,31 @@ __device__ __forceinline__ uint4 ld_nc_v4(uint4 const *src, uint64_t pol)
     return v;
 }
 
+// A 4-byte load with an L2 policy, through the coherent path.
+__device__ __forceinline__ uint32_t ld_hint_b32(void const *src, uint64_t pol)
+{
+    uint32_t v;
+    asm volatile("ld.global.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(src), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ uint32_t ld_nc_u16(uint16_t const *src, uint64_t pol)
 {
     uint16_t v;
     asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(src), "l"(pol));
     return v;
+}
+
+__device__ __forceinline__ uint32_t ld_nc_code(uint8_t const *src, uint64_t pol)
+{
+    uint16_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(v) : "l"(src), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_nc_code(uint16_t const *src, uint64_t pol)
+{
+    return ld_nc_u16(src, pol);
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt()
@@ -2148,12 +2168,15 @@ __global__ void __launch_bounds__(k_threads)
     float          mg     = 0.0F;
     float          mh     = 0.0F;
     uint64_t const stride = static_cast<uint64_t>(gridDim.x) * k_threads;
+    uint64_t const pol    = l2_policy_first(); // leaf ids, scores, labels: once a round
     for (uint64_t r = (static_cast<uint64_t>(blockIdx.x) * k_threads) + threadIdx.x; r < n_rows;
          r += stride)
     {
-        uint32_t const n = leaf16[r];
-        float const    s = a.scores != nullptr ? a.scores[r] : 0.0F;
-        float const    y = a.gh != nullptr ? a.labels[r] : 0.0F;
+        uint32_t const n = ld_nc_u16(leaf16 + r, pol);
+        float const    s = a.scores != nullptr ? __uint_as_float(ld_hint_b32(a.scores + r, pol))
+                                               : 0.0F;
+        float const    y = a.gh != nullptr ? __uint_as_float(ld_hint_b32(a.labels + r, pol))
+                                           : 0.0F;
         apply_leaf(a, r, n, s, y, val_s[n], mg, mh);
     }
     if (a.absmax != nullptr)
@@ -2312,18 +2335,21 @@ __global__ void __launch_bounds__(k_threads)
     uint32_t const w    = threadIdx.x >> 5;
     uint32_t const w0   = w * k_warp_rows;
     constexpr uint32_t steps = k_warp_rows / 32;
+    // the level's list and the split column's codes: read once here (the
+    // gradient codes and the next lists are what the level reads again)
+    uint64_t const     pol   = l2_policy_first();
     uint32_t           r[steps];
 #pragma unroll
     for (uint32_t i = 0; i < steps; ++i)
     {
         uint32_t const k = w0 + (32 * i) + lane;
-        r[i]             = k < ch.count ? rows[ch.begin + k] : k_leaf_flag;
+        r[i]             = k < ch.count ? ld_hint_b32(rows + ch.begin + k, pol) : k_leaf_flag;
     }
     uint32_t b[steps];
 #pragma unroll
     for (uint32_t i = 0; i < steps; ++i)
     {
-        b[i] = r[i] != k_leaf_flag ? static_cast<uint32_t>(col[r[i]]) : 0u;
+        b[i] = r[i] != k_leaf_flag ? ld_nc_code(col + r[i], pol) : 0u;
     }
     uint32_t mword = 0; // lane i: step i's direction bits
     uint32_t n     = 0;
