@@ -1058,19 +1058,25 @@ def fit_main(args, world, rank, local, W, K):
 
     peak, peak_kind = peaks()
     hist_gbs = prof["hist_bytes"] / (prof["hist_ms"] * 1e-3) / 1e9
-    traffic = None
+    # DRAM bytes of the build: the measured bytes per algorithmic byte of a
+    # full-size tree (one ncu pass per launch, the L2 as the fit leaves it),
+    # times this tree's algorithmic bytes
+    traffic = traffic_ratio = None
     tpath = os.path.join(ROOT, "profiles", "qhist_t_tall_binary_int8_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             td = json.load(f)
-        traffic = td.get(args.mode, {}).get("dram_bytes_per_tree")
+        traffic_ratio = td.get(args.mode, {}).get("dram_per_algorithmic_byte")
+        if traffic_ratio is not None:
+            traffic = traffic_ratio * prof["hist_bytes"]
     per_row = F + (2.0 if args.mode == "int8" else 4.0 if args.mode == "int16" else 8.0) + 4.0
     levels = [{"rows": r, "ms": t, "gbs": (r * per_row) / (t * 1e-3) / 1e9 if t > 0 else None}
               for r, t in zip(prof["build_rows"], prof["build_ms"])]
     # partition per level: every row's id and its split-feature code read,
-    # its id written (pass 1 reads, pass 2 reads and writes)
+    # its id written; the last level (whose rows are never listed) counts
+    # its left rows only
     part_levels = max(1, len(levels) - 1)
-    part_bytes = part_levels * n * (4 + 1 + 4)
+    part_bytes = part_levels * n * (4 + 1 + 4) + n * (4 + 1)
     value = fit_ms / 1000.0
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": K,
@@ -1101,6 +1107,7 @@ def fit_main(args, world, rank, local, W, K):
                                 else "histogram build (count+offsets+scatter+chain)"),
                      "achieved": hist_gbs, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": hist_gbs / peak, "traffic": traffic,
+                     "traffic_per_algorithmic_byte": traffic_ratio,
                      "algorithmic_bytes_per_tree": prof["hist_bytes"],
                      "hist_ms_per_tree": prof["hist_ms"]},
         "hist_levels": levels,
