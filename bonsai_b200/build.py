@@ -73,13 +73,16 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-def build_oracle() -> None:
+def build_oracle(ref: str | None = None) -> None:
     """Compiles the oracle checkers (test infrastructure): the C restatement
-    always, the reference's own CPU grower when its sources are present."""
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
-    if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver.o")):
+    always, the reference's own CPU grower when `ref` (or BONSAI_REFERENCE)
+    names its source tree."""
+    ref = ref or os.environ.get("BONSAI_REFERENCE", "")
+    args = [f"REF={ref}"] if ref else []
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", *args], check=True)
+    if ref and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver.o")):
         # the drop-in check links the product library: build it after
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin"],
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "dropin", *args],
                        check=True)
 
 

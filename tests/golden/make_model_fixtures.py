@@ -14,7 +14,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_model_fixtures.py <reference source tree>")
+    ref = sys.argv[1]
     for kind in ("regressor", "softmax"):
         shutil.copyfile(os.path.join(ref, "tests", "data", f"fixture_v7_{kind}.bonsai"),
                         os.path.join(HERE, f"model_v7_{kind}.bonsai"))
