@@ -47,15 +47,15 @@ constexpr uint32_t k_plan_thr   = 512;  // plan kernels: one thread per node
 
 // The walked tree's decision heap (depthwise trees, depth <= 8): slot h's
 // children are 2h + 1 and 2h + 2; an entry is x = tile << 8 | position,
-// y = split bin | missing bin << 16 | default_left << 31. The plan kernels
-// fill it as the tree grows (a node carries its slot): a split node's entry,
-// and for a leaf above the last level the leaf map entry of its leftmost
-// last-level descendant; every other slot keeps the always-left entry the
-// tree starts from (split bin 0xFFFF takes every code, missing bin 0x7FFF
-// matches none, no tile).
+// y = split bin | (the missing bin if missing rows go left, else 0xFFFF)
+// << 16. The plan kernels fill it as the tree grows (a node carries its
+// slot): a split node's entry, and for a leaf above the last level the leaf
+// map entry of its leftmost last-level descendant; every other slot keeps
+// the always-left entry the tree starts from (split bin 0xFFFF takes every
+// code, no tile).
 constexpr uint32_t k_no_tile    = 0xFFFFFFu;
 constexpr uint32_t k_heap_slots = 255;         // decision slots of a depth-8 heap
-constexpr uint32_t k_heap_pass  = 0x7FFFFFFFu; // an always-left entry's y
+constexpr uint32_t k_heap_pass  = 0xFFFFFFFFu; // an always-left entry's y
 
 struct HeapOut
 {
@@ -65,11 +65,13 @@ struct HeapOut
     uint32_t  per;     // codes per 32-byte mirror tile
 };
 
+// y = split bin | (the missing bin when missing rows go left, else 0xFFFF,
+// which no code equals) << 16: routes_left is then code <= split bin or code
+// == y >> 16, since the split bin is below the missing bin
 __device__ __forceinline__ uint2 heap_entry(uint32_t f, uint32_t per, uint32_t split,
                                             uint32_t last, bool dl)
 {
-    return make_uint2(((f / per) << 8) | (f % per),
-                      split | (last << 16) | (static_cast<uint32_t>(dl) << 31));
+    return make_uint2(((f / per) << 8) | (f % per), split | ((dl ? last : 0xFFFFu) << 16));
 }
 
 // Slot h holds a leaf: its leftmost last-level descendant names it.
@@ -1852,17 +1854,15 @@ __device__ __forceinline__ uint32_t tile_code(uint32_t const w[8], uint32_t pos)
     }
 }
 
-// The walked tree as a complete binary heap of its decision levels, built
-// once per tree (final_kernel): slot h's children are 2h + 1 and 2h + 2, so a
-// step reads one 8-byte entry -- x = tile << 8 | position, y = split bin |
-// missing bin << 16 | default_left << 31 -- and no child ids. A leaf above
-// the last level repeats down its left spine (split bin 0xFFFF sends every
-// code left, missing bin 0x7FFF matches no code, no tile), and the slot a
-// row ends in after `depth` steps names its leaf through leafmap.
+// The walk steps through the tree's decision heap (filled by the plan
+// kernels): slot h's children are 2h + 1 and 2h + 2, so a step reads one
+// 8-byte entry and no child ids. A leaf above the last level repeats down
+// its left spine, and the slot a row ends in after `depth` steps names its
+// leaf through leafmap.
 
 __device__ __forceinline__ uint32_t heap_step(uint2 const e, uint32_t code, uint32_t h)
 {
-    bool const left = code == ((e.y >> 16) & 0x7FFFu) ? (e.y >> 31) != 0 : code <= (e.y & 0xFFFFu);
+    bool const left = code <= (e.y & 0xFFFFu) || code == (e.y >> 16);
     return (2 * h) + (left ? 1u : 2u);
 }
 
@@ -4753,9 +4753,13 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     cudaStream_t s   = stream_;
     int const    cur = static_cast<int>(L & 1);
     int const    nxt = cur ^ 1;
+    // grids sized for this level: at most 2^L frontier nodes, and at most one
+    // partial partition chunk per node beyond the rows' whole chunks
+    uint32_t const front = std::min(max_front_, 1u << std::min(L, 30u));
+    uint32_t const pch   = std::min(max_pchunks_, ceil_div(max_rows_, k_part_rows) + front);
     size_t const find_smem = max_nb_ * (sizeof(double2) + (sizeof(unsigned long long) * cw_));
     phase_begin();
-    dim3 const fgrid(max_front_, n_sel_);
+    dim3 const fgrid(front, n_sel_);
     if (cfg_.level)
     {
         size_t const lsmem = static_cast<size_t>(lgroup_) * max_nb_ * sizeof(double2);
@@ -4774,7 +4778,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     else if (quant_)
     {
-        launch_k(pdl_, qfind_warp_kernel, dim3(max_front_, ceil_div(n_sel_, k_qfind_warps)),
+        launch_k(pdl_, qfind_warp_kernel, dim3(front, ceil_div(n_sel_, k_qfind_warps)),
                  k_qfind_warps * 32, 0, s, ctl_, nodes_[cur], hist_[cur], total_cells_, cell_off_,
                  sel_nb_, sel_, n_sel_, mono_, n_mono_, cfg_.tp, cand_, qscale_, nullptr, cw_,
                  fgroups_);
@@ -4807,20 +4811,20 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
                                             : psplit_kernel<uint8_t, true>)
                                     : (last ? psplit_kernel<uint16_t, false>
                                             : psplit_kernel<uint16_t, true>);
-        launch_k(pdl_, kern, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur], best_,
+        launch_k(pdl_, kern, pch, k_threads, 0, s, ctl_, pchunks_, nodes_[cur], best_,
                  rows_in, rows_out, plane_.bins, plane_.n_pad, sel_, sel_nb_, nleft_, nright_,
                  static_cast<unsigned long long *>(hist_[nxt]), total_cells_ * cw_, n_zcells);
         BB_LAUNCH("psplit_kernel");
     }
     else if (plane_.u8)
     {
-        launch_k(pdl_, pcount_kernel<uint8_t>, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+        launch_k(pdl_, pcount_kernel<uint8_t>, pch, k_threads, 0, s, ctl_, pchunks_,
                  nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
                  dirs_);
     }
     else
     {
-        launch_k(pdl_, pcount_kernel<uint16_t>, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+        launch_k(pdl_, pcount_kernel<uint16_t>, pch, k_threads, 0, s, ctl_, pchunks_,
                  nodes_[cur], best_, rows_in, plane_.bins, plane_.n_pad, sel_, sel_nb_, pleft_,
                  dirs_);
     }
@@ -4849,7 +4853,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     if (!walk_)
     {
-        launch_k(pdl_, stamp_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_, nodes_[cur],
+        launch_k(pdl_, stamp_kernel, pch, k_threads, 0, s, ctl_, pchunks_, nodes_[cur],
                  rows_in, t, leaf_id, scores, lr);
         BB_LAUNCH("stamp_kernel");
         n_launch_ += 1;
@@ -4864,11 +4868,11 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
             phase_end(prof_->partition_ms);
         }
         phase_begin();
-        launch_k(pdl_, qsplit_totals_kernel, ceil_div(max_front_, 8), 256, 0, s, ctl_, bpair_,
+        launch_k(pdl_, qsplit_totals_kernel, ceil_div(std::min(max_front_, 2 * front), 8u), 256, 0, s, ctl_, bpair_,
                  nodes_[cur], best_, static_cast<unsigned long long const *>(hist_[cur]),
                  total_cells_, cell_off_, sel_nb_, cw_, btot_);
         BB_LAUNCH("qsplit_totals_kernel");
-        launch_k(pdl_, qsubtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+        launch_k(pdl_, qsubtract_totals_kernel, front, k_threads, 0, s, ctl_, bpair_,
                  static_cast<unsigned long long const *>(hist_[cur]),
                  static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
                  nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
@@ -4882,7 +4886,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     if (!fused)
     {
-        launch_k(pdl_, pscatter_kernel, max_pchunks_, k_threads, 0, s, ctl_, pchunks_,
+        launch_k(pdl_, pscatter_kernel, pch, k_threads, 0, s, ctl_, pchunks_,
                  nodes_[cur], best_, pleft_, prbase_, nleft_, dst_, rows_in, rows_out, dirs_,
                  static_cast<unsigned long long *>(hist_[nxt]), build_, total_cells_ * cw_,
                  n_zcells);
@@ -4906,7 +4910,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
         {
             red_->sum_u64(btot_, 2 * static_cast<size_t>(max_front_), s);
         }
-        launch_k(pdl_, qsubtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+        launch_k(pdl_, qsubtract_totals_kernel, front, k_threads, 0, s, ctl_, bpair_,
                  static_cast<unsigned long long const *>(hist_[cur]),
                  static_cast<unsigned long long *>(hist_[nxt]), total_cells_, 0, nodes_[cur],
                  nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, btot_, cw_);
@@ -4931,7 +4935,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     if (quant_)
     {
         launch_k(pdl_, qsubtract_totals_kernel,
-                 dim3(max_front_, std::max(1u, ceil_div(n_cells * cw_, k_sub_cells))), k_threads, 0,
+                 dim3(front, std::max(1u, ceil_div(n_cells * cw_, k_sub_cells))), k_threads, 0,
                  s, ctl_, bpair_, static_cast<unsigned long long const *>(hist_[cur]),
                  static_cast<unsigned long long *>(hist_[nxt]), total_cells_, n_cells, nodes_[cur],
                  nodes_[nxt], best_, sel_, sel_nb_, mono_, n_mono_, cfg_.tp, qscale_, nullptr, cw_);
@@ -4939,7 +4943,7 @@ void Grower::level(uint32_t L, uint32_t const *rows_in, uint32_t *rows_out,
     }
     else
     {
-        launch_k(pdl_, subtract_totals_kernel, max_front_, k_threads, 0, s, ctl_, bpair_,
+        launch_k(pdl_, subtract_totals_kernel, front, k_threads, 0, s, ctl_, bpair_,
                  static_cast<float2 const *>(hist_[cur]), static_cast<float2 *>(hist_[nxt]),
                  total_cells_, n_cells, nodes_[cur], nodes_[nxt], best_, sel_, sel_nb_, mono_,
                  n_mono_, cfg_.tp);
