@@ -498,7 +498,17 @@ class Booster:
         return _finish(a, meta)
 
     def trees(self) -> list:
-        return [self.tree(t) for t in range(self.n_trees)]
+        """Every tree, copied from the device in one transfer per array
+        (bb_booster_trees)."""
+        n = self.n_trees
+        if n == 0:
+            return []
+        cap = int(lib().bb_booster_tree_capacity(self.h))
+        a = _tree_arrays(cap * n)
+        meta = np.zeros(3 * n, np.uint32)
+        check(lib().bb_booster_trees(self.h, 0, n, *(ptr(a[k]) for k in _ORDER), ptr(meta)))
+        return [_finish({k: v[i * cap:(i + 1) * cap] for k, v in a.items()},
+                        meta[3 * i:3 * i + 3]) for i in range(n)]
 
     @property
     def n_classes(self) -> int:

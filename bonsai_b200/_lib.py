@@ -91,6 +91,7 @@ def lib() -> C.CDLL:
         L.bb_booster_init_score.argtypes = [vp]
         L.bb_booster_tree_capacity.argtypes = [vp]
         L.bb_booster_tree.argtypes = [vp, C.c_uint32] + [vp] * 9
+        L.bb_booster_trees.argtypes = [vp, C.c_uint32, C.c_uint32] + [vp] * 9
         L.bb_booster_scores.argtypes = [vp, vp]
         L.bb_booster_leaf_ids.argtypes = [vp, vp]
         L.bb_booster_last_ms.argtypes = [vp, C.POINTER(C.c_float)]

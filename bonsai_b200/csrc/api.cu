@@ -339,20 +339,22 @@ struct TreeStore
         }
         t = {};
     }
+    // slots [slot, slot + count), each array's entries back to back
     void download(uint32_t slot, uint32_t *feature, float *value, uint32_t *left,
                   uint32_t *right, uint8_t *dl, float *gain, float *cover,
-                  uint32_t *split_bin, uint32_t *meta) const
+                  uint32_t *split_bin, uint32_t *meta, uint32_t count = 1) const
     {
         size_t const o = static_cast<size_t>(slot) * cap;
-        BB_CHECK(cudaMemcpy(feature, t.feature + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(value, t.value + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(left, t.left + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(right, t.right + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(dl, t.default_left + o, cap, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(gain, t.gain + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(cover, t.cover + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(split_bin, t.split_bin + o, cap * 4, cudaMemcpyDeviceToHost));
-        BB_CHECK(cudaMemcpy(meta, t.meta + (3 * static_cast<size_t>(slot)), 12,
+        size_t const m = static_cast<size_t>(count) * cap;
+        BB_CHECK(cudaMemcpy(feature, t.feature + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(value, t.value + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(left, t.left + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(right, t.right + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(dl, t.default_left + o, m, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(gain, t.gain + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(cover, t.cover + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(split_bin, t.split_bin + o, m * 4, cudaMemcpyDeviceToHost));
+        BB_CHECK(cudaMemcpy(meta, t.meta + (3 * static_cast<size_t>(slot)), 12 * count,
                             cudaMemcpyDeviceToHost));
     }
 };
@@ -1839,6 +1841,26 @@ extern "C"
                 BB_CHECK(cudaStreamSynchronize(b->stream));
                 b->trees.download(t, feature, value, left, right, default_left, gain, cover,
                                   split_bin, meta);
+            });
+    }
+
+    int bb_booster_trees(bb_booster const *b, uint32_t first, uint32_t count,
+                         uint32_t *feature, float *value, uint32_t *left, uint32_t *right,
+                         uint8_t *default_left, float *gain, float *cover, uint32_t *split_bin,
+                         uint32_t *meta)
+    {
+        return guarded(
+            [&]
+            {
+                need(first <= b->n_trees && count <= b->n_trees - first,
+                     "bb_booster_trees: tree range out of range");
+                if (count == 0)
+                {
+                    return;
+                }
+                BB_CHECK(cudaStreamSynchronize(b->stream));
+                b->trees.download(first, feature, value, left, right, default_left, gain, cover,
+                                  split_bin, meta, count);
             });
     }
 

@@ -254,6 +254,15 @@ int bb_booster_tree(bb_booster const *b, uint32_t t, uint32_t *feature, float *v
                     uint32_t *left, uint32_t *right, uint8_t *default_left,
                     float *gain, float *cover, uint32_t *split_bin, uint32_t *meta);
 
+/* Trees first .. first + count - 1 at once (one copy per array): tree
+ * first + i in entries [i * capacity, (i + 1) * capacity) of each array and
+ * its meta in [3 i, 3 i + 3). The model download of a whole fit (the
+ * reference's save after training, src/io/model.cpp:158-387) in nine copies
+ * instead of nine per tree. */
+int bb_booster_trees(bb_booster const *b, uint32_t first, uint32_t count, uint32_t *feature,
+                     float *value, uint32_t *left, uint32_t *right, uint8_t *default_left,
+                     float *gain, float *cover, uint32_t *split_bin, uint32_t *meta);
+
 /* The training scores (host, n_rows). Replaces resident_end
  * (histogram_engine.hpp:262). */
 int bb_booster_scores(bb_booster const *b, float *out);

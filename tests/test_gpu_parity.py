@@ -143,7 +143,11 @@ def test_booster_100_trees_bit_exact_vs_reference(bb, orc, use_graph):
     gold = unpack_trees(d)
     for i in range(100):
         assert_trees_equal(b.tree(i), gold[i], f"tree {i}")
-    trees = b.trees()
+    trees = b.trees()                      # all 100 in one transfer per array
+    for i in range(100):
+        assert_trees_equal(trees[i], gold[i], f"bulk tree {i}")
+    assert [len(t.feature) for t in b.trees()[40:]] == [len(b.tree(i).feature)
+                                                        for i in range(40, 100)]
     pred = bb.predict(plane, trees, b.init_score, 0.1)
     assert np.array_equal(pred, d["pred"])
     # the fused training-score update: scores[r] += lr * leaf, round by round
