@@ -1217,36 +1217,52 @@ __global__ void __launch_bounds__(k_lfind_thr)
         }
         __syncthreads();
         uint32_t const gn = min(group, n_cur - g0);
+        // every (node, bin) pair's two terms, all threads at once (the FP64
+        // divisions are independent), in place of the pair's prefix
+        for (uint32_t x = tid; x < gn * n_cut; x += k_lfind_thr)
+        {
+            uint32_t const  q    = x / n_cut;
+            uint32_t const  b    = x - (q * n_cut);
+            LevelNode const l    = ln_s[q];
+            double2        *cell = pref + ((static_cast<uint64_t>(q) * max_nb) + b);
+            double2 const   p2   = *cell;
+            double          t0;
+            double          t1;
+            if constexpr (Q)
+            {
+                t0 = level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g, l.real_h, true,
+                                        l.score, tp);
+                t1 = level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g, l.real_h, false,
+                                        l.score, tp);
+            }
+            else
+            {
+                float const mg = static_cast<float>(l.mg);
+                float const mh = static_cast<float>(l.mh);
+                t0 = level_term<float>(p2.x, p2.y, mg, mh, l.real_g, l.real_h, true, l.score,
+                                       tp);
+                t1 = level_term<float>(p2.x, p2.y, mg, mh, l.real_g, l.real_h, false, l.score,
+                                       tp);
+            }
+            *cell = make_double2(t0, t1);
+        }
+        __syncthreads();
+        // then each bin adds the group's terms in frontier order
         for (uint32_t q = 0; q < gn; ++q)
         {
-            LevelNode const l  = ln_s[q];
-            double2 const  *pr = pref + (static_cast<uint64_t>(q) * max_nb);
+            double2 const *pr = pref + (static_cast<uint64_t>(q) * max_nb);
 #pragma unroll
             for (uint32_t x = 0; x < k_bins_per_thr; ++x)
             {
                 uint32_t const b = tid + (x * k_lfind_thr);
                 if (b < n_cut)
                 {
-                    double2 const p2 = pr[b];
-                    if constexpr (Q)
-                    {
-                        acc[2 * x] += level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g,
-                                                         l.real_h, true, l.score, tp);
-                        acc[(2 * x) + 1] += level_term<double>(p2.x, p2.y, l.mg, l.mh, l.real_g,
-                                                               l.real_h, false, l.score, tp);
-                    }
-                    else
-                    {
-                        float const mg = static_cast<float>(l.mg);
-                        float const mh = static_cast<float>(l.mh);
-                        acc[2 * x] += level_term<float>(p2.x, p2.y, mg, mh, l.real_g, l.real_h,
-                                                        true, l.score, tp);
-                        acc[(2 * x) + 1] += level_term<float>(p2.x, p2.y, mg, mh, l.real_g,
-                                                              l.real_h, false, l.score, tp);
-                    }
+                    double2 const t2 = pr[b];
+                    acc[2 * x] += t2.x;
+                    acc[(2 * x) + 1] += t2.y;
                 }
             }
-            parent_sum += l.score;
+            parent_sum += ln_s[q].score;
         }
         __syncthreads();
     }
