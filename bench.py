@@ -113,7 +113,14 @@ class Clocks:
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
+            # the timed region starts once the sampler has started up and
+            # written its first sample (its start-up holds the driver)
+            t_end = time.perf_counter() + 10.0
+            while time.perf_counter() < t_end and self.proc.poll() is None:
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.05)
+            time.sleep(0.2)
         except Exception:
             self.proc = None
         return self
