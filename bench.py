@@ -115,7 +115,7 @@ class Clocks:
                 stdout=self.f, stderr=subprocess.DEVNULL)
             # the timed region starts once the sampler has started up and
             # written its first sample (its start-up holds the driver)
-            t_end = time.perf_counter() + 10.0
+            t_end = time.perf_counter() + 3.0
             while time.perf_counter() < t_end and self.proc.poll() is None:
                 if os.path.getsize(self.path) > 0:
                     break
