@@ -1054,7 +1054,7 @@ __global__ void __launch_bounds__(k_qfind_warps * 32)
 // exact form's serial FP64 chain, the quantised form's exact integer scan),
 // then every thread adds the group's nodes for its bins in frontier order,
 // so the FP64 sums follow the reference's order bit for bit.
-constexpr uint32_t k_lfind_thr = 512;
+constexpr uint32_t k_lfind_thr = 1024;
 
 struct LevelNode
 {
