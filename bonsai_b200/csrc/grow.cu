@@ -1819,9 +1819,9 @@ __global__ void __launch_bounds__(k_threads)
 // with the partition's own rule (routes_left on the split bin, the last bin
 // following default_left), so it reaches the leaf whose segment held it --
 // and rows read in order are coalesced, where the partitioned rows are a
-// gather. The walk takes a fixed number of steps: leaves loop to themselves
-// (missing bin 0xFFFF never matches, split bin 0xFFFF sends every code left,
-// both children are the leaf). One pass (exact form) updates
+// gather. The walk takes a fixed number of steps through the tree's
+// decision heap (a leaf above the last level repeats down its left spine, and
+// the last level's slot names the leaf). One pass (exact form) updates
 // scores[r] = scores[r] + lr * value -- the stamp's arithmetic -- and the
 // leaf ids and, for a resident booster, writes the next round's gradient
 // pairs and their maxima. The quantised form renews its leaves from
