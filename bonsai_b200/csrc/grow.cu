@@ -4564,6 +4564,12 @@ void Grower::set_shard(Reducer *r, uint64_t row_offset, uint64_t total_rows)
     red_        = r;
     row_off_    = row_offset;
     total_rows_ = total_rows;
+    if (r != nullptr)
+    {
+        // a shard's rounds put NCCL's kernels between this grower's: plain
+        // stream order there
+        pdl_ = false;
+    }
     if (gleft_ == nullptr)
     {
         gleft_ = dalloc<uint64_t>(max_front_, stream_);
