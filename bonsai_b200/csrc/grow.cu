@@ -2299,6 +2299,79 @@ __global__ void __launch_bounds__(k_threads)
     }
 }
 
+constexpr uint32_t k_psteps = k_warp_rows / 32; // 32-row steps of a partition warp
+
+// One warp's 512 rows of a one-pass partition chunk: their ids (the level's
+// list and the split column's codes are read once here, evict-first: the
+// gradient codes and the next lists are what the level reads again), their
+// codes of the split feature, their directions (lane i keeps step i's bits).
+template <bool FULL, typename BinT>
+__device__ __forceinline__ void psplit_route(Chunk const &ch, uint32_t const *__restrict__ rows,
+                                             BinT const *col, uint32_t last, Best const &bs,
+                                             uint32_t w0, uint32_t lane, uint32_t (&r)[k_psteps],
+                                             uint32_t &mword, uint32_t &n)
+{
+    uint64_t const pol = l2_policy_first();
+#pragma unroll
+    for (uint32_t i = 0; i < k_psteps; ++i)
+    {
+        uint32_t const k = w0 + (32 * i) + lane;
+        r[i]             = FULL || k < ch.count ? ld_hint_b32(rows + ch.begin + k, pol)
+                                                : k_leaf_flag;
+    }
+    uint32_t b[k_psteps];
+#pragma unroll
+    for (uint32_t i = 0; i < k_psteps; ++i)
+    {
+        b[i] = FULL || r[i] != k_leaf_flag ? ld_nc_code(col + r[i], pol) : 0u;
+    }
+#pragma unroll
+    for (uint32_t i = 0; i < k_psteps; ++i)
+    {
+        bool const lf =
+            (FULL || r[i] != k_leaf_flag) && routes_left(b[i], last, bs.bin, bs.dl != 0);
+        uint32_t const m = __ballot_sync(0xFFFFFFFFu, lf);
+        mword            = lane == i ? m : mword;
+        n += __popc(m);
+    }
+}
+
+// ... and their places: lefts from lo up, rights from top down (rank rk on).
+template <bool FULL>
+__device__ __forceinline__ void psplit_place(Chunk const &ch, uint32_t w0, uint32_t lane,
+                                             uint32_t const (&r)[k_psteps], uint32_t mword,
+                                             uint32_t lo, uint32_t rk, uint32_t top,
+                                             uint32_t *__restrict__ rows_out)
+{
+    uint32_t const ltm = (1u << lane) - 1u;
+#pragma unroll
+    for (uint32_t i = 0; i < k_psteps; ++i)
+    {
+        uint32_t const base = w0 + (32 * i);
+        if (!FULL && base >= ch.count)
+        {
+            break;
+        }
+        uint32_t const m      = __shfl_sync(0xFFFFFFFFu, mword, i);
+        uint32_t const nvalid = FULL ? 32u : min(32u, ch.count - base);
+        uint32_t const vm     = FULL || nvalid == 32 ? 0xFFFFFFFFu : ((1u << nvalid) - 1u);
+        uint32_t const lm     = m & vm;
+        if (FULL || lane < nvalid)
+        {
+            if ((m >> lane) & 1u)
+            {
+                rows_out[lo + __popc(lm & ltm)] = r[i];
+            }
+            else
+            {
+                rows_out[top - (rk + __popc(~lm & vm & ltm))] = r[i];
+            }
+        }
+        lo += __popc(lm);
+        rk += __popc(~lm & vm);
+    }
+}
+
 // The partition in one pass, for trees the final walk stamps in the
 // quantised form, whose every consumer of the row lists is order-free (the
 // histogram build adds exact integers; the next partition routes row by
@@ -2350,32 +2423,19 @@ __global__ void __launch_bounds__(k_threads)
     uint32_t const lane = threadIdx.x & 31;
     uint32_t const w    = threadIdx.x >> 5;
     uint32_t const w0   = w * k_warp_rows;
-    constexpr uint32_t steps = k_warp_rows / 32;
-    // the level's list and the split column's codes: read once here (the
-    // gradient codes and the next lists are what the level reads again)
-    uint64_t const     pol   = l2_policy_first();
-    uint32_t           r[steps];
-#pragma unroll
-    for (uint32_t i = 0; i < steps; ++i)
+    // a warp whose 512 rows all lie in the chunk (the common case) skips the
+    // per-row range checks
+    bool const     full = w0 + k_warp_rows <= ch.count;
+    uint32_t       r[k_psteps];
+    uint32_t       mword = 0; // lane i: step i's direction bits
+    uint32_t       n     = 0;
+    if (full)
     {
-        uint32_t const k = w0 + (32 * i) + lane;
-        r[i]             = k < ch.count ? ld_hint_b32(rows + ch.begin + k, pol) : k_leaf_flag;
+        psplit_route<true>(ch, rows, col, last, bs, w0, lane, r, mword, n);
     }
-    uint32_t b[steps];
-#pragma unroll
-    for (uint32_t i = 0; i < steps; ++i)
+    else
     {
-        b[i] = r[i] != k_leaf_flag ? ld_nc_code(col + r[i], pol) : 0u;
-    }
-    uint32_t mword = 0; // lane i: step i's direction bits
-    uint32_t n     = 0;
-#pragma unroll
-    for (uint32_t i = 0; i < steps; ++i)
-    {
-        bool const     lf = r[i] != k_leaf_flag && routes_left(b[i], last, bs.bin, bs.dl != 0);
-        uint32_t const m  = __ballot_sync(0xFFFFFFFFu, lf);
-        mword             = lane == i ? m : mword;
-        n += __popc(m);
+        psplit_route<false>(ch, rows, col, last, bs, w0, lane, r, mword, n);
     }
     if (lane == 0)
     {
@@ -2403,35 +2463,16 @@ __global__ void __launch_bounds__(k_threads)
     {
         lb += wsum[x];
     }
-    uint32_t       lo  = nd.start + base_s[0] + lb;                       // next left
-    uint32_t       rk  = base_s[1] + (min(w0, ch.count) - lb);            // next right's rank
+    uint32_t const lo  = nd.start + base_s[0] + lb;                       // next left
+    uint32_t const rk  = base_s[1] + (min(w0, ch.count) - lb);            // next right's rank
     uint32_t const top = nd.start + nd.count - 1;                          // rights count down
-    uint32_t const ltm = (1u << lane) - 1u;
-#pragma unroll
-    for (uint32_t i = 0; i < steps; ++i)
+    if (full)
     {
-        uint32_t const base = w0 + (32 * i);
-        if (base >= ch.count)
-        {
-            break;
-        }
-        uint32_t const m      = __shfl_sync(0xFFFFFFFFu, mword, i);
-        uint32_t const nvalid = min(32u, ch.count - base);
-        uint32_t const vm     = nvalid == 32 ? 0xFFFFFFFFu : ((1u << nvalid) - 1u);
-        uint32_t const lm     = m & vm;
-        if (lane < nvalid)
-        {
-            if ((m >> lane) & 1u)
-            {
-                rows_out[lo + __popc(lm & ltm)] = r[i];
-            }
-            else
-            {
-                rows_out[top - (rk + __popc(~lm & vm & ltm))] = r[i];
-            }
-        }
-        lo += __popc(lm);
-        rk += __popc(~lm & vm);
+        psplit_place<true>(ch, w0, lane, r, mword, lo, rk, top, rows_out);
+    }
+    else
+    {
+        psplit_place<false>(ch, w0, lane, r, mword, lo, rk, top, rows_out);
     }
 }
 
